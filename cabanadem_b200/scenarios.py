@@ -1,0 +1,264 @@
+"""Scenario builders: the reference's example set-ups and the seeded benchmark workloads.
+
+Each builder returns a :class:`Scenario` (initial particle/wall state plus force model,
+time step, step count and neighbour parameters).  The example builders restate the
+init functors of the reference's example programs (file:line cited per function); the
+workload builders generate seeded synthetic inputs with the shapes, sizes and value
+distributions of the benchmark configurations:
+
+* ``random_box``      4,096 monodisperse spheres, rejection sampled in a 5 cm walled cube
+* ``hcp_box``         2,000,000 polydisperse spheres on a jittered HCP lattice
+* ``bonded_bar``      256x64x8 simple-cubic bonded bar pulled at both ends
+* ``batched_scenes``  1,024 independent clusters fired at one wall each
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .inputs import Inputs
+from .state import BondState, ParticleState, WallState
+
+# Reference quirk flags (bit set = reproduce the reference's behaviour).
+Q1_VELJ_USES_UI = 0x01
+Q2_ETA_T_ZERO = 0x02
+Q3_NO_PP_TORQUE = 0x04
+Q4_UNIT_HISTORY = 0x08
+Q5_WALL_FT_TYPO = 0x10
+REF_COMPAT = 0x1F
+
+
+@dataclass
+class Scenario:
+    name: str
+    state: ParticleState
+    walls: WallState
+    params: dict
+    dt: float
+    nsteps: int
+    delta: float = 0.0          # uniform neighbour cutoff (reference: 3 r); 0 = per-pair r_i + r_j + skin
+    skin: float = 0.0
+    gravity: tuple = (0.0, 0.0, 0.0)
+    output_frequency: int = 0
+    extra: dict = field(default_factory=dict)
+
+
+def _force_params(cor_pp, cor_pw, mu_pp, mu_pw, quirks=REF_COMPAT):
+    return dict(cor_pp=float(cor_pp), cor_pw=float(cor_pw), mu_pp=float(mu_pp), mu_pw=float(mu_pw),
+                quirks=int(quirks))
+
+
+def _material(state, inp, prefix="particle_"):
+    state.rho[:] = inp[prefix + "density"]
+    state.rad[:] = inp[prefix + "radius"]
+    state.E[:] = inp[prefix + "youngs_modulus"]
+    state.G[:] = inp[prefix + "shear_modulus"]
+    state.nu[:] = inp[prefix + "poissons_ratio"]
+    _mass(state, float(inp[prefix + "radius"]), float(inp[prefix + "density"]))
+
+
+def _mass(state, radius, rho):
+    # examples/01_elastic_normal_impact_of_two_identical_particles.cpp:106-107 (scalar form)
+    m_p_i = 4. / 3. * math.pi * radius * radius * radius * rho
+    I_p_i = 2. / 5. * m_p_i * radius * radius
+    state.m[:] = m_p_i
+    state.I[:] = I_p_i
+
+
+def _one_wall(inp, x, normal):
+    w = WallState.create(1)
+    w.x[0] = x
+    w.normal[0] = normal
+    w.E[0] = inp["wall_youngs_modulus"]
+    w.G[0] = inp["wall_shear_modulus"]
+    w.nu[0] = inp["wall_poissons_ratio"]
+    return w
+
+
+def example01(inp: Inputs) -> Scenario:
+    """examples/01_elastic_normal_impact_of_two_identical_particles.cpp:103-188."""
+    r, v = float(inp["particle_radius"]), float(inp["velocity_p"])
+    s = ParticleState.create(2, max_cnts=6, max_walls=1)
+    _material(s, inp)
+    for pid in range(2):
+        s.x[pid, 0] = -r + pid * (2. * r) + pid * r / 100.
+    s.u[0, 0], s.u[1, 0] = v, -v
+    w = _one_wall(inp, (0., -3. * r, 0.), (0., 1., 0.))
+    fp = _force_params(inp["coefficient_of_restitution_pp"], inp["coefficient_of_restitution_pw"],
+                       inp["friction_pp"], inp["friction_pw"])
+    return Scenario("example01", s, w, fp, float(inp["timestep"]), inp["num_steps"] + 1, delta=3. * r,
+                    output_frequency=int(inp["output_frequency"]))
+
+
+def _single_over_wall(inp, name, ux, uy, cor_pw=None):
+    r = float(inp["particle_radius"])
+    s = ParticleState.create(1, max_cnts=6, max_walls=1)
+    _material(s, inp)
+    s.x[0, 1] = r + r / 1000000.
+    s.u[0, 0], s.u[0, 1] = ux, uy
+    w = _one_wall(inp, (0., 0., 0.), (0., 1., 0.))
+    fp = _force_params(inp["coefficient_of_restitution_pp"],
+                       cor_pw if cor_pw is not None else inp["coefficient_of_restitution_pw"],
+                       inp["friction_pp"], inp["friction_pw"])
+    return Scenario(name, s, w, fp, float(inp["timestep"]), inp["num_steps"] + 1, delta=3. * r,
+                    output_frequency=int(inp["output_frequency"]))
+
+
+def example02(inp: Inputs) -> Scenario:
+    """examples/02_elastic_normal_impact_of_particle_wall.cpp:99-171."""
+    return _single_over_wall(inp, "example02", 0.0, -float(inp["velocity_p"]))
+
+
+def example03(inp: Inputs, cor_pw: float) -> Scenario:
+    """examples/03_normal_particle_wall_different_cor.cpp:105-174 (cor_pw from --cor_pw=)."""
+    return _single_over_wall(inp, "example03", 0.0, -float(inp["velocity_p"]), cor_pw=cor_pw)
+
+
+def example04(inp: Inputs, incident_angle: float) -> Scenario:
+    """examples/04_oblique_particle_wall_different_angles.cpp:117-195 (angle from --angle=)."""
+    angle = incident_angle / 180. * math.pi
+    v = float(inp["velocity_p"])
+    return _single_over_wall(inp, "example04", v * math.sin(angle), -v * math.cos(angle))
+
+
+def tst03(inp: Inputs) -> Scenario:
+    """examples/tst_03_multiple_particles_contacts.cpp:103-193 (wall normal is zero)."""
+    r, v = float(inp["particle_radius"]), float(inp["velocity_p"])
+    s = ParticleState.create(3, max_cnts=6, max_walls=1)
+    _material(s, inp)
+    for pid in range(3):
+        s.x[pid, 0] = -r + pid * (2. * r) + pid * r / 100.
+        s.x[pid, 1] = 0.
+        if pid == 1:
+            s.x[pid, 0] = -r + 1 * (1.5 * r) + 1 * r / 100.
+            s.x[pid, 1] = r + r / 2.
+        if pid == 2:
+            s.x[pid, 0] = -r + 1 * (1.5 * r) + 1 * r / 100.
+            s.x[pid, 1] = - r - r / 2.
+    s.u[0, 0] = v
+    w = _one_wall(inp, (0., -3. * r, 0.), (0., 0., 0.))
+    fp = _force_params(inp["coefficient_of_restitution_pp"], inp["coefficient_of_restitution_pw"],
+                       inp["friction_pp"], inp["friction_pw"])
+    return Scenario("tst03", s, w, fp, float(inp["timestep"]), inp["num_steps"] + 1, delta=3. * r,
+                    output_frequency=int(inp["output_frequency"]))
+
+
+def bdem_two_particles():
+    """examples/tst_01_BDEM_two_particles_tensile_3D.cpp:162-302: two bonded spheres
+    pulled apart by +-1e3 N, particle 0's force zeroed after the bond pass."""
+    radius, rho, E, G, nu = 0.5, 2000., 1e4, 1e3, 0.25
+    s = ParticleState.create(2, max_cnts=1, max_walls=1)
+    for i in range(2):
+        s.x[i, 0] = -radius + i * (2. * radius)
+    s.rad[:], s.rho[:], s.E[:], s.G[:], s.nu[:] = radius, rho, E, G, nu
+    _mass(s, radius, rho)
+    b = BondState.create(2, 27)
+    ext = np.zeros((2, 3))
+    ext[0, 0], ext[1, 0] = -1e3, 1e3
+    fix = np.zeros(2, dtype=np.uint8)
+    fix[0] = 1  # zero force (not torque) of particle 0
+    dt = 1e-4
+    return dict(state=s, bonds=b, dt=dt, nsteps=int(4. / dt) + 1, ext_force=ext, fix_flags=fix,
+                bond_factor=3.0, search_cutoff=4. * radius,
+                bparams=dict(quirks=0x07, beta=0.1, radius_factor=1.0, kn=0.0, kt=0.0, break_strain=0.0))
+
+
+# ----------------------------------------------------------------------------------------
+# Seeded benchmark workloads
+# ----------------------------------------------------------------------------------------
+GLASS = dict(rho=2600.0, E=70e9, nu=0.25)  # G = E / (2 (1 + nu)) = 28 GPa
+
+
+def _box_walls(lo, hi, E, nu, G):
+    """Six planes bounding [lo, hi]^3, normals pointing inwards."""
+    w = WallState.create(6)
+    k = 0
+    for d in range(3):
+        for side, (pt, sgn) in enumerate(((lo, 1.0), (hi, -1.0))):
+            w.x[k, d] = pt[d]
+            w.normal[k, d] = sgn
+            k += 1
+    w.E[:], w.nu[:], w.G[:] = E, nu, G
+    return w
+
+
+def _apply_glass(s, rad):
+    E, nu, rho = GLASS["E"], GLASS["nu"], GLASS["rho"]
+    s.rad[:] = rad
+    s.rho[:] = rho
+    s.E[:], s.nu[:], s.G[:] = E, nu, E / (2.0 * (1.0 + nu))
+    s.m[:] = 4. / 3. * math.pi * s.rad * s.rad * s.rad * s.rho
+    s.I[:] = 2. / 5. * s.m * s.rad * s.rad
+
+
+def random_box(n=4096, radius=1e-3, side=0.05, seed=1, vmax=0.1, max_cnts=16, quirks=REF_COMPAT,
+               dt=1e-7, nsteps=10_000):
+    """4,096 monodisperse r = 1 mm glass spheres, non-overlapping by uniform rejection
+    sampling in a 5 cm cube with 6 walls; v ~ U[-0.1, 0.1]^3, gravity -z, dt = 1e-7,
+    Verlet skin 0.1 r, mu = 0.3, e = 0.8."""
+    rng = np.random.default_rng(seed)
+    pos = np.zeros((n, 3))
+    cell = 2.0 * radius
+    grid = {}
+    k = 0
+    while k < n:
+        p = rng.uniform(radius, side - radius, size=3)
+        c = tuple((p // cell).astype(int))
+        ok = True
+        for dx in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dz in (-1, 0, 1):
+                    for q in grid.get((c[0] + dx, c[1] + dy, c[2] + dz), ()):
+                        if np.sum((pos[q] - p) ** 2) < (2.0 * radius) ** 2:
+                            ok = False
+                            break
+                    if not ok:
+                        break
+                if not ok:
+                    break
+            if not ok:
+                break
+        if ok:
+            pos[k] = p
+            grid.setdefault(c, []).append(k)
+            k += 1
+    s = ParticleState.create(n, max_cnts=max_cnts, max_walls=6)
+    s.x[:] = pos
+    s.u[:] = rng.uniform(-vmax, vmax, size=(n, 3))
+    _apply_glass(s, radius)
+    w = _box_walls((0.0, 0.0, 0.0), (side, side, side), GLASS["E"], GLASS["nu"], s.G[0])
+    return Scenario("random_box_4096", s, w, _force_params(0.8, 0.8, 0.3, 0.3, quirks), dt, nsteps,
+                    skin=0.1 * radius, gravity=(0.0, 0.0, -9.81))
+
+
+def hcp_box(n=2_000_000, rmin=0.8e-3, rmax=1.2e-3, seed=2, vmax=0.1, max_cnts=16, quirks=REF_COMPAT,
+            dt=5e-8, nsteps=2000, jitter=0.05):
+    """Polydisperse spheres (r ~ U[0.8, 1.2] mm) on a hexagonal-close-packed lattice of
+    pitch a = 2 r_max, each site jittered by U(-1, 1) * 0.05 * (a/2 - r_i) per axis (no
+    initial overlap), inside a walled box; v ~ U[-0.1, 0.1]^3, gravity -z, dt = 5e-8,
+    skin 0.1 r_mean, neighbour rebuild when the displacement bound exceeds skin / 2."""
+    rng = np.random.default_rng(seed)
+    a = 2.0 * rmax
+    side = (n * a ** 3 / math.sqrt(2.0)) ** (1.0 / 3.0)
+    nx = max(1, int(round(side / a)))
+    ny = max(1, int(round(side / (a * math.sqrt(3.0) / 2.0))))
+    nz = int(math.ceil(n / (nx * ny)))
+    k = np.arange(n)
+    ix, iy, iz = k % nx, (k // nx) % ny, k // (nx * ny)
+    px = a * (ix + 0.5 * ((iy + iz) % 2))
+    py = a * math.sqrt(3.0) / 2.0 * (iy + (iz % 2) / 3.0)
+    pz = a * math.sqrt(2.0 / 3.0) * iz
+    rad = rng.uniform(rmin, rmax, size=n)
+    pos = np.stack([px, py, pz], axis=1)
+    pos += rng.uniform(-1.0, 1.0, size=(n, 3)) * (jitter * (a / 2.0 - rad))[:, None]
+    pos += a  # margin from the walls
+    s = ParticleState.create(n, max_cnts=max_cnts, max_walls=6)
+    s.x[:] = pos
+    s.u[:] = rng.uniform(-vmax, vmax, size=(n, 3))
+    _apply_glass(s, rad)
+    hi = pos.max(axis=0) + a
+    w = _box_walls((0.0, 0.0, 0.0), tuple(hi), GLASS["E"], GLASS["nu"], s.G[0])
+    return Scenario("hcp_box_%d" % n, s, w, _force_params(0.8, 0.8, 0.3, 0.3, quirks), dt, nsteps,
+                    skin=0.1 * 0.5 * (rmin + rmax), gravity=(0.0, 0.0, -9.81))
