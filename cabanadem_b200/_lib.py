@@ -1,0 +1,114 @@
+"""ctypes binding of libb200dem.so (the C ABI declared in include/b200dem.h).
+
+There is no CPU fallback: importing a solver without the built library raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libb200dem.so")
+
+DEM_OK = 0
+ERR = {
+    0x001: "DEM_ERR_INVALID", 0x002: "DEM_ERR_CUDA", 0x004: "DEM_ERR_CONTACT_OVERFLOW",
+    0x008: "DEM_ERR_NEIGHBOR_OVERFLOW", 0x010: "DEM_ERR_NAN", 0x020: "DEM_ERR_TIMEOUT",
+    0x040: "DEM_ERR_BOND_OVERFLOW", 0x080: "DEM_ERR_NOMEM", 0x100: "DEM_ERR_UNSUPPORTED",
+}
+DEM_ERR_CONTACT_OVERFLOW = 0x004
+DEM_ERR_TIMEOUT = 0x020
+
+# enum dem_field
+F = {name: k for k, name in enumerate(
+    ["x", "u", "omega", "force", "torque", "m", "rho", "rad", "I", "E", "nu", "G", "tng_idx", "tng_ss_x",
+     "tng_ss_y", "tng_ss_z", "tng_count", "tng_sw_x", "tng_sw_y", "tng_sw_z", "fix", "ext_force"])}
+W = {name: k for k, name in enumerate(["x", "u", "omega", "normal", "E", "nu", "G"])}
+DEM_FP64, DEM_MIXED = 0, 1
+
+
+class ForceParams(C.Structure):
+    _fields_ = [("cor_pp", C.c_double), ("cor_pw", C.c_double), ("mu_pp", C.c_double), ("mu_pw", C.c_double),
+                ("quirks", C.c_uint)]
+
+
+class SolverParams(C.Structure):
+    _fields_ = [("dt", C.c_double), ("delta", C.c_double), ("skin", C.c_double), ("rebuild_every_step", C.c_int),
+                ("precision", C.c_int), ("gravity", C.c_double * 3), ("max_neighbors", C.c_int),
+                ("steps_per_launch", C.c_int)]
+
+
+class RunStats(C.Structure):
+    _fields_ = [("steps", C.c_long), ("rebuilds", C.c_long), ("max_neighbors", C.c_int),
+                ("neighbor_capacity", C.c_int), ("status", C.c_int), ("disp_bound", C.c_double)]
+
+
+class DemError(RuntimeError):
+    pass
+
+
+_lib = None
+
+_VP = C.c_void_p
+_PROTOS = {
+    "dem_version": ([], C.c_int),
+    "dem_ctx_create": ([C.c_int, C.POINTER(_VP)], C.c_int),
+    "dem_ctx_destroy": ([_VP], C.c_int),
+    "dem_ctx_sync": ([_VP], C.c_int),
+    "dem_last_error": ([_VP], C.c_char_p),
+    "dem_particles_create": ([_VP, C.c_int, C.c_int, C.c_int, C.POINTER(_VP)], C.c_int),
+    "dem_particles_destroy": ([_VP], C.c_int),
+    "dem_particles_set": ([_VP, C.c_int, _VP, C.c_long], C.c_int),
+    "dem_particles_get": ([_VP, C.c_int, _VP, C.c_long], C.c_int),
+    "dem_particles_size": ([_VP], C.c_int),
+    "dem_walls_create": ([_VP, C.c_int, C.POINTER(_VP)], C.c_int),
+    "dem_walls_destroy": ([_VP], C.c_int),
+    "dem_walls_set": ([_VP, C.c_int, _VP, C.c_long], C.c_int),
+    "dem_solver_create": ([_VP, _VP, _VP, C.POINTER(ForceParams), C.POINTER(SolverParams), C.POINTER(_VP)],
+                          C.c_int),
+    "dem_solver_destroy": ([_VP], C.c_int),
+    "dem_solver_run": ([_VP, C.c_int], C.c_int),
+    "dem_solver_stats": ([_VP, C.POINTER(RunStats)], C.c_int),
+    "dem_stage1": ([_VP], C.c_int),
+    "dem_stage2": ([_VP], C.c_int),
+    "dem_stage3": ([_VP], C.c_int),
+    "dem_build_neighbors": ([_VP], C.c_int),
+    "dem_compute_force": ([_VP], C.c_int),
+    "dem_neighbors_get": ([_VP, _VP, _VP, C.POINTER(C.c_long)], C.c_int),
+    "dem_energy": ([_VP, C.POINTER(C.c_double)], C.c_int),
+}
+
+
+def exported_symbols():
+    """Names the C ABI header declares (checked against the library's exports)."""
+    return sorted(_PROTOS)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise DemError("libb200dem.so is not built (run __graft_entry__.build() or make -C cabanadem_b200/csrc); "
+                           "there is no CPU fallback")
+        L = C.CDLL(LIB_PATH)
+        for name, (args, res) in _PROTOS.items():
+            fn = getattr(L, name, None)
+            if fn is None:
+                continue
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def check(st, ctx=None, what="", allow=0):
+    if st & ~allow:
+        msg = ", ".join(v for k, v in ERR.items() if st & k) or str(st)
+        detail = ""
+        if ctx is not None:
+            try:
+                detail = lib().dem_last_error(ctx).decode()
+            except Exception:
+                pass
+        raise DemError(f"{what}: {msg} {detail}".strip())
+    return st

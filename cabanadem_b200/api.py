@@ -1,0 +1,320 @@
+"""Python mirror of the reference's operator interface, running on libb200dem.so.
+
+Names, argument meaning and step semantics follow the reference:
+
+=========================================  ================================================
+reference (file:line)                      here
+=========================================  ================================================
+Particles<Mem,3,MaxCnts,MaxNoWalls>        :class:`Particles` (capacities at run time)
+  (src/CabanaDEM_Particles.hpp:22-71)
+  slicePosition() ... (:99-271)            ``slicePosition()`` ... (host copies),
+                                           ``set(field, array)`` / ``get(field)``
+  updateParticles(exec, functor) (:91-97)  ``updateParticles(functor)`` (host functor on a
+                                           ParticleState, then upload)
+Wall<Mem,3> (src/CabanaDEM_Wall.hpp:22)    :class:`Wall`
+Force(cor_pp, cor_pw, mu_pp, mu_pw)        :class:`Force`
+  (src/CabanaDEM_Force.hpp:23-35)
+Integrator(dt).stage1/2/3                  :class:`Integrator` (bound to a solver)
+  (src/CabanaDEM_Integrator.hpp:16-102)
+computeForceParticleParticleInfiniteWall   :func:`computeForceParticleParticleInfiniteWall`
+  (src/CabanaDEM_Force.hpp:700-710)
+createSolverDEM / SolverDEM::run           :func:`createSolverDEM`, :meth:`SolverDEM.run`
+  (src/CabanaDEM_Solver.hpp:66-138)        (num_steps + 1 steps, as the reference loop)
+=========================================  ================================================
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import DemError, F, W, check, lib
+from .inputs import Inputs
+from .state import ParticleState, WallState
+
+REF_COMPAT = 0x1F
+
+_F_DTYPE = {"tng_idx": np.int32, "tng_count": np.int32, "fix": np.uint8}
+
+
+def _shape(field, n, mc, mw):
+    if field in ("x", "u", "omega", "force", "torque", "ext_force"):
+        return (n, 3)
+    if field in ("tng_idx", "tng_ss_x", "tng_ss_y", "tng_ss_z"):
+        return (n, mc)
+    if field in ("tng_sw_x", "tng_sw_y", "tng_sw_z"):
+        return (n, mw)
+    return (n,)
+
+
+class Context:
+    """One device + one CUDA stream (dem_ctx)."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        st = lib().dem_ctx_create(int(device), C.byref(h))
+        if st:
+            raise DemError("dem_ctx_create failed (status %d): no usable CUDA device" % st)
+        self.h = h
+
+    def sync(self):
+        check(lib().dem_ctx_sync(self.h), self.h, "dem_ctx_sync")
+
+    def close(self):
+        """Destroy the context; close every object created on it first."""
+        if self.h:
+            lib().dem_ctx_destroy(self.h)
+            self.h = None
+
+
+_default_ctx = None
+
+
+def default_context():
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+class Particles:
+    def __init__(self, n: int, max_cnts: int = 6, max_walls: int = 1, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        self.n, self.max_cnts, self.max_walls = int(n), int(max_cnts), int(max_walls)
+        h = C.c_void_p()
+        check(lib().dem_particles_create(self.ctx.h, self.n, self.max_cnts, self.max_walls, C.byref(h)),
+              self.ctx.h, "dem_particles_create")
+        self.h = h
+
+    # ---- field access
+    def set(self, field: str, arr):
+        dt = _F_DTYPE.get(field, np.float64)
+        a = np.ascontiguousarray(arr, dtype=dt)
+        exp = _shape(field, self.n, self.max_cnts, self.max_walls)
+        if a.size != int(np.prod(exp)):
+            raise DemError("set(%s): expected shape %s, got %s" % (field, exp, a.shape))
+        check(lib().dem_particles_set(self.h, F[field], a.ctypes.data, a.size), self.ctx.h, "set " + field)
+
+    def get(self, field: str):
+        dt = _F_DTYPE.get(field, np.float64)
+        a = np.empty(_shape(field, self.n, self.max_cnts, self.max_walls), dtype=dt)
+        check(lib().dem_particles_get(self.h, F[field], a.ctypes.data, a.size), self.ctx.h, "get " + field)
+        return a
+
+    def upload(self, s: ParticleState):
+        for f in ("rad", "x", "u", "omega", "force", "torque", "m", "I", "rho", "E", "nu", "G",
+                  "tng_idx", "tng_ss_x", "tng_ss_y", "tng_ss_z", "tng_count"):
+            self.set(f, getattr(s, f))
+        if self.max_walls > 0:
+            for f in ("tng_sw_x", "tng_sw_y", "tng_sw_z"):
+                self.set(f, getattr(s, f)[:, : self.max_walls])
+
+    def download(self) -> ParticleState:
+        s = ParticleState.create(self.n, self.max_cnts, max(self.max_walls, 1))
+        for f in ("x", "u", "omega", "force", "torque", "m", "I", "rho", "rad", "E", "nu", "G",
+                  "tng_idx", "tng_ss_x", "tng_ss_y", "tng_ss_z", "tng_count"):
+            setattr(s, f, self.get(f))
+        if self.max_walls > 0:
+            for f in ("tng_sw_x", "tng_sw_y", "tng_sw_z"):
+                setattr(s, f, self.get(f))
+        return s
+
+    def updateParticles(self, functor):
+        """Run a host functor over a ParticleState copy, then upload it."""
+        s = self.download()
+        for pid in range(self.n):
+            functor(s, pid)
+        self.upload(s)
+
+    # reference-named accessors (host copies)
+    def slicePosition(self): return self.get("x")
+    def sliceVelocity(self): return self.get("u")
+    def sliceOmega(self): return self.get("omega")
+    def sliceForce(self): return self.get("force")
+    def sliceTorque(self): return self.get("torque")
+    def sliceMass(self): return self.get("m")
+    def sliceDensity(self): return self.get("rho")
+    def sliceRadius(self): return self.get("rad")
+    def sliceMomentOfInertia(self): return self.get("I")
+    def sliceYoungsMod(self): return self.get("E")
+    def slicePoissonsRatio(self): return self.get("nu")
+    def sliceShearMod(self): return self.get("G")
+    def sliceTangentialDispIdx(self): return self.get("tng_idx")
+    def sliceTangentialDispSSx(self): return self.get("tng_ss_x")
+    def sliceTangentialDispSSy(self): return self.get("tng_ss_y")
+    def sliceTangentialDispSSz(self): return self.get("tng_ss_z")
+    def sliceTotalNoTangentialContacts(self): return self.get("tng_count")
+    def sliceTangentialDispSWx(self): return self.get("tng_sw_x")
+    def sliceTangentialDispSWy(self): return self.get("tng_sw_y")
+    def sliceTangentialDispSWz(self): return self.get("tng_sw_z")
+
+    def close(self):
+        if self.h:
+            lib().dem_particles_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Wall:
+    def __init__(self, n: int, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        self.n = int(n)
+        h = C.c_void_p()
+        check(lib().dem_walls_create(self.ctx.h, self.n, C.byref(h)), self.ctx.h, "dem_walls_create")
+        self.h = h
+
+    def set(self, field, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        check(lib().dem_walls_set(self.h, W[field], a.ctypes.data, a.size), self.ctx.h, "wall set " + field)
+
+    def upload(self, w: WallState):
+        for f in ("x", "u", "omega", "normal", "E", "nu", "G"):
+            self.set(f, getattr(w, f))
+
+    def close(self):
+        if self.h:
+            lib().dem_walls_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Force:
+    """Force(cor_pp, cor_pw, friction_pp, friction_pw) (src/CabanaDEM_Force.hpp:23-35)."""
+
+    def __init__(self, cor_pp, cor_pw, friction_pp, friction_pw, quirks=REF_COMPAT):
+        self.cor_pp, self.cor_pw = float(cor_pp), float(cor_pw)
+        self.friction_pp, self.friction_pw = float(friction_pp), float(friction_pw)
+        self.quirks = int(quirks)
+
+    def params(self):
+        return _lib.ForceParams(self.cor_pp, self.cor_pw, self.friction_pp, self.friction_pw, self.quirks)
+
+
+class SolverDEM:
+    """SolverDEM (src/CabanaDEM_Solver.hpp:13-122) on the device."""
+
+    def __init__(self, particles: Particles, wall: Wall | None, force: Force, dt: float, delta: float = 0.0,
+                 skin: float = 0.0, rebuild_every_step: bool = False, gravity=(0.0, 0.0, 0.0),
+                 precision: int = _lib.DEM_FP64, num_steps: int = 0, output_frequency: int = 0,
+                 max_neighbors: int = 0, steps_per_launch: int = 0):
+        self.particles, self.wall, self.force = particles, wall, force
+        self.dt, self.num_steps, self.output_frequency = float(dt), int(num_steps), int(output_frequency)
+        sp = _lib.SolverParams()
+        sp.dt, sp.delta, sp.skin = float(dt), float(delta), float(skin)
+        sp.rebuild_every_step = 1 if rebuild_every_step else 0
+        sp.precision = int(precision)
+        sp.gravity = (C.c_double * 3)(*gravity)
+        sp.max_neighbors = int(max_neighbors)
+        sp.steps_per_launch = int(steps_per_launch)
+        fp = force.params()
+        h = C.c_void_p()
+        check(lib().dem_solver_create(particles.ctx.h, particles.h, wall.h if wall else None, C.byref(fp),
+                                      C.byref(sp), C.byref(h)), particles.ctx.h, "dem_solver_create")
+        self.h = h
+        self.integrator = Integrator(self)
+        self.last_status = 0
+
+    def run(self):
+        """Reference loop: for step in 0..num_steps inclusive (Solver.hpp:79)."""
+        return self.run_steps(self.num_steps + 1)
+
+    def run_steps(self, nsteps: int, allow=_lib.DEM_ERR_CONTACT_OVERFLOW):
+        st = lib().dem_solver_run(self.h, int(nsteps))
+        self.last_status = st
+        return check(st, self.particles.ctx.h, "dem_solver_run", allow=allow)
+
+    def stats(self):
+        s = _lib.RunStats()
+        check(lib().dem_solver_stats(self.h, C.byref(s)), self.particles.ctx.h, "dem_solver_stats")
+        return {k: getattr(s, k) for k, _ in s._fields_}
+
+    def build_neighbors(self):
+        check(lib().dem_build_neighbors(self.h), self.particles.ctx.h, "dem_build_neighbors")
+
+    def compute_force(self):
+        return check(lib().dem_compute_force(self.h), self.particles.ctx.h, "dem_compute_force",
+                     allow=_lib.DEM_ERR_CONTACT_OVERFLOW)
+
+    def neighbors(self):
+        n = self.particles.n
+        off = np.zeros(n + 1, dtype=np.int32)
+        tot = C.c_long(0)
+        check(lib().dem_neighbors_get(self.h, off.ctypes.data, None, C.byref(tot)), self.particles.ctx.h, "nbr")
+        idx = np.zeros(max(tot.value, 1), dtype=np.int32)
+        check(lib().dem_neighbors_get(self.h, off.ctypes.data, idx.ctypes.data, C.byref(tot)),
+              self.particles.ctx.h, "nbr")
+        return off, idx[: tot.value]
+
+    def energy(self):
+        out = (C.c_double * 4)()
+        check(lib().dem_energy(self.h, out), self.particles.ctx.h, "dem_energy")
+        return np.array(out[:])
+
+    def close(self):
+        if self.h:
+            lib().dem_solver_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Integrator:
+    """Integrator::stage1/2/3 (src/CabanaDEM_Integrator.hpp:31-102) on a solver's particles."""
+
+    def __init__(self, solver: SolverDEM):
+        self._s = solver
+
+    def stage1(self, particles=None):
+        check(lib().dem_stage1(self._s.h), self._s.particles.ctx.h, "stage1")
+
+    def stage2(self, particles=None):
+        check(lib().dem_stage2(self._s.h), self._s.particles.ctx.h, "stage2")
+
+    def stage3(self, particles=None):
+        check(lib().dem_stage3(self._s.h), self._s.particles.ctx.h, "stage3")
+
+
+def computeForceParticleParticleInfiniteWall(solver: SolverDEM):
+    """src/CabanaDEM_Force.hpp:700-710: zero, compact contacts, pp force, wall force."""
+    return solver.compute_force()
+
+
+def createSolverDEM(inputs: Inputs, particles: Particles, wall: Wall, force: Force, delta: float, **kw):
+    """createSolverDEM<Mem>(inputs, particles, wall, force, delta) (src/CabanaDEM_Solver.hpp:129-138).
+    The reference rebuilds the list every step with cutoff delta; that is the default here."""
+    kw.setdefault("rebuild_every_step", True)
+    return SolverDEM(particles, wall, force, float(inputs["timestep"]), delta=delta,
+                     num_steps=int(inputs["num_steps"]), output_frequency=int(inputs["output_frequency"]), **kw)
+
+
+def from_scenario(sc, ctx: Context | None = None, rebuild_every_step=False, precision=_lib.DEM_FP64,
+                  steps_per_launch=0, max_neighbors=0):
+    """Particles + Wall + SolverDEM on the device for a scenarios.Scenario."""
+    st = sc.state
+    p = Particles(st.n, st.max_cnts, sc.walls.n if sc.walls is not None else 0, ctx=ctx)
+    p.upload(st)
+    w = None
+    if sc.walls is not None and sc.walls.n > 0:
+        w = Wall(sc.walls.n, ctx=p.ctx)
+        w.upload(sc.walls)
+    prm = sc.params
+    f = Force(prm["cor_pp"], prm["cor_pw"], prm["mu_pp"], prm["mu_pw"], prm.get("quirks", REF_COMPAT))
+    s = SolverDEM(p, w, f, sc.dt, delta=sc.delta, skin=sc.skin, rebuild_every_step=rebuild_every_step,
+                  gravity=sc.gravity, precision=precision, steps_per_launch=steps_per_launch,
+                  max_neighbors=max_neighbors)
+    return s

@@ -1,0 +1,921 @@
+// dem_api.cu -- the C ABI of libb200dem.so (declared in include/b200dem.h).
+//
+// Host side of the library: device allocation, caller-order <-> Morton-order staging,
+// material/pair constant tables, and the solver loop.  The loop replaces
+// SolverDEM::run (src/CabanaDEM_Solver.hpp:66-98): a prologue kernel does stage1+stage2
+// of the first step, then chunks of fused step kernels run as one CUDA graph launch;
+// the neighbour list is rebuilt on the device when the displacement bound since the
+// last build reaches skin/2 (or before every step when rebuild_every_step is set).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "b200dem.h"
+#include "dem_internal.cuh"
+
+using namespace b200dem;
+
+struct dem_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+};
+
+struct dem_particles {
+    dem_ctx *ctx = nullptr;
+    Particles P{};
+    Particles alt{};   // scratch for re-sorting
+    Ctl *ctl = nullptr;
+    std::vector<double> rho, E, nu, G;   // caller order, host copies
+    double rmax = 0.0;
+    bool dirty = true;       // state changed through set(): list must be rebuilt
+    bool mat_dirty = true;   // E, nu, G changed: tables must be rebuilt
+    std::vector<uint8_t> mat;   // caller order
+    std::vector<std::tuple<double, double, double>> mats;
+};
+
+struct dem_walls {
+    dem_ctx *ctx = nullptr;
+    int n = 0;
+    std::vector<double> x, u, omega, normal, E, nu, G;
+};
+
+struct dem_solver {
+    dem_ctx *ctx = nullptr;
+    dem_particles *p = nullptr;
+    dem_walls *w = nullptr;
+    dem_force_params fp{};
+    dem_solver_params sp{};
+    ForceConsts fc{};
+    PairConst *d_pp = nullptr, *d_pw = nullptr;
+    WallGeom *d_walls = nullptr;
+    NbrList L{};
+    BuildBuffers B{};
+    double *d_epart = nullptr, *d_eout = nullptr;
+    int nparts = 0;
+    bool built = false;
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+    long graph_version = -1;
+    long version = 0;   // bumps when anything baked into the graph changes
+};
+
+namespace {
+
+int fail(dem_ctx *ctx, int code, const std::string &msg) {
+    if (ctx) ctx->err = msg;
+    return code;
+}
+
+int cuda_check(dem_ctx *ctx, cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return DEM_OK;
+    return fail(ctx, e == cudaErrorMemoryAllocation ? DEM_ERR_NOMEM : DEM_ERR_CUDA,
+                std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                                  \
+    do {                                                          \
+        int _st = cuda_check(ctx, (call), #call);                 \
+        if (_st) return _st;                                      \
+    } while (0)
+
+template <class T>
+cudaError_t dalloc(T **p, size_t count) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    return cudaMalloc((void **)p, count * sizeof(T));
+}
+
+// ---- staging kernels (caller order <-> sorted order) --------------------------------
+__global__ void k_scatter_d(const double *src, double *dst, int n, int ncomp, int cap, const int *rank) {
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < (long)n * ncomp; t += (long)gridDim.x * blockDim.x) {
+        const int c = (int)(t / ncomp), k = (int)(t % ncomp);
+        dst[(long)k * cap + rank[c]] = src[t];
+    }
+}
+__global__ void k_gather_d(const double *src, double *dst, int n, int ncomp, int cap, const int *rank) {
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < (long)n * ncomp; t += (long)gridDim.x * blockDim.x) {
+        const int c = (int)(t / ncomp), k = (int)(t % ncomp);
+        dst[t] = src[(long)k * cap + rank[c]];
+    }
+}
+// mode 0: partner ids (caller -> sorted via rank), 1: plain
+__global__ void k_scatter_i(const int *src, int *dst, int n, int ncomp, int cap, const int *rank, int remap) {
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < (long)n * ncomp; t += (long)gridDim.x * blockDim.x) {
+        const int c = (int)(t / ncomp), k = (int)(t % ncomp);
+        int v = src[t];
+        if (remap && v >= 0 && v < n) v = rank[v];
+        dst[(long)k * cap + rank[c]] = v;
+    }
+}
+__global__ void k_gather_i(const int *src, int *dst, int n, int ncomp, int cap, const int *rank, const int *perm,
+                           int remap) {
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < (long)n * ncomp; t += (long)gridDim.x * blockDim.x) {
+        const int c = (int)(t / ncomp), k = (int)(t % ncomp);
+        int v = src[(long)k * cap + rank[c]];
+        if (remap && v >= 0 && v < n) v = perm[v];
+        dst[t] = v;
+    }
+}
+__global__ void k_scatter_pos(const double *src, double4 *pos, int n, const int *rank, int rad) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        double4 &p = pos[rank[c]];
+        if (rad) p.w = src[c];
+        else {
+            p.x = src[3 * c];
+            p.y = src[3 * c + 1];
+            p.z = src[3 * c + 2];
+        }
+    }
+}
+__global__ void k_gather_pos(const double4 *pos, double *dst, int n, const int *rank, int rad) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        const double4 p = pos[rank[c]];
+        if (rad) dst[c] = p.w;
+        else {
+            dst[3 * c] = p.x;
+            dst[3 * c + 1] = p.y;
+            dst[3 * c + 2] = p.z;
+        }
+    }
+}
+__global__ void k_scatter_mI(const double *src, double2 *mI, int n, const int *rank, int which) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        double2 &v = mI[rank[c]];
+        if (which) v.y = src[c];
+        else v.x = src[c];
+    }
+}
+__global__ void k_gather_mI(const double2 *mI, double *dst, int n, const int *rank, int which) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        const double2 v = mI[rank[c]];
+        dst[c] = which ? v.y : v.x;
+    }
+}
+__global__ void k_scatter_u8(const uint8_t *src, uint8_t *dst, int n, const int *rank) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) dst[rank[c]] = src[c];
+}
+__global__ void k_gather_u8(const uint8_t *src, uint8_t *dst, int n, const int *rank) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) dst[c] = src[rank[c]];
+}
+__global__ void k_scatter_count(const int *src, int *cstate, int n, const int *rank) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        const int p = rank[c];
+        cstate[p] = (cstate[p] & ~0xff) | (src[c] & 0xff);
+    }
+}
+__global__ void k_gather_count(const int *cstate, int *dst, int n, const int *rank) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) dst[c] = cstate[rank[c]] & 0xff;
+}
+// wall-history-active bits = any stored component nonzero
+__global__ void k_sw_mask(Particles P) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += gridDim.x * blockDim.x) {
+        unsigned m = 0;
+        for (int w = 0; w < P.mw; ++w)
+            for (int d = 0; d < 3; ++d)
+                if (P.sw[((long)d * P.mw + w) * P.cap + i] != 0.0) m |= 1u << w;
+        P.cstate[i] = (P.cstate[i] & 0xff) | (int)(m << 8);
+    }
+}
+__global__ void k_init_particles(Particles P) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += gridDim.x * blockDim.x) {
+        P.perm[i] = i;
+        P.rank[i] = i;
+        for (int k = 0; k < P.mc; ++k) P.tidx[(long)k * P.cap + i] = -1;
+    }
+}
+__global__ void k_run_begin(Ctl *ctl, int target, double half_skin) {
+    if (threadIdx.x == 0) {
+        ctl->steps_done = 0;
+        ctl->target = target;
+        ctl->half_skin = half_skin;
+        ctl->ticket = 0u;
+        ctl->vmax2 = 0ull;
+    }
+}
+__global__ void k_invalidate(Ctl *ctl) {
+    if (threadIdx.x == 0) ctl->disp = 1e300;
+}
+
+constexpr int kGS = 148 * 4;
+constexpr int kTB = 256;
+
+bool field_layout(const dem_particles *p, int field, long *count, int *esize) {
+    const long n = p->P.n;
+    switch (field) {
+        case DEM_F_X: case DEM_F_U: case DEM_F_OMEGA: case DEM_F_FORCE: case DEM_F_TORQUE: case DEM_F_EXT_FORCE:
+            *count = 3 * n; *esize = 8; return true;
+        case DEM_F_M: case DEM_F_RHO: case DEM_F_RAD: case DEM_F_I: case DEM_F_E: case DEM_F_NU: case DEM_F_G:
+            *count = n; *esize = 8; return true;
+        case DEM_F_TNG_IDX: *count = n * p->P.mc; *esize = 4; return true;
+        case DEM_F_TNG_SS_X: case DEM_F_TNG_SS_Y: case DEM_F_TNG_SS_Z: *count = n * p->P.mc; *esize = 8; return true;
+        case DEM_F_TNG_COUNT: *count = n; *esize = 4; return true;
+        case DEM_F_TNG_SW_X: case DEM_F_TNG_SW_Y: case DEM_F_TNG_SW_Z: *count = n * p->P.mw; *esize = 8; return true;
+        case DEM_F_FIX: *count = n; *esize = 1; return true;
+        default: return false;
+    }
+}
+
+int host_cur(dem_particles *p) {
+    int cur = 0;
+    cudaMemcpyAsync(&cur, &p->ctl->cur, sizeof(int), cudaMemcpyDeviceToHost, p->ctx->stream);
+    cudaStreamSynchronize(p->ctx->stream);
+    return cur;
+}
+
+}  // namespace
+
+// =====================================================================================
+extern "C" int dem_version(void) { return 1; }
+
+extern "C" int dem_ctx_create(int device, dem_ctx **out) {
+    if (!out) return DEM_ERR_INVALID;
+    *out = nullptr;
+    dem_ctx *ctx = new dem_ctx();
+    ctx->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete ctx;
+        return DEM_ERR_CUDA;
+    }
+    *out = ctx;
+    return DEM_OK;
+}
+
+extern "C" int dem_ctx_destroy(dem_ctx *ctx) {
+    if (!ctx) return DEM_ERR_INVALID;
+    cudaStreamSynchronize(ctx->stream);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return DEM_OK;
+}
+
+extern "C" int dem_ctx_sync(dem_ctx *ctx) {
+    if (!ctx) return DEM_ERR_INVALID;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return DEM_OK;
+}
+
+extern "C" const char *dem_last_error(dem_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+// ---- particles ----------------------------------------------------------------------
+static cudaError_t alloc_particles(Particles &P, int n, int mc, int mw, bool pingpong) {
+    cudaError_t e = cudaSuccess;
+    auto A = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
+    P.n = n;
+    P.cap = n;
+    P.mc = mc;
+    P.mw = mw;
+    const size_t cap = n;
+    for (int b = 0; b < (pingpong ? 2 : 1); ++b) {
+        A(dalloc(&P.pos[b], cap));
+        A(dalloc(&P.vel[b], 3 * cap));
+        A(dalloc(&P.omg[b], 3 * cap));
+    }
+    A(dalloc(&P.force, 3 * cap));
+    A(dalloc(&P.torque, 3 * cap));
+    A(dalloc(&P.mI, cap));
+    A(dalloc(&P.mat, cap));
+    A(dalloc(&P.cstate, cap));
+    A(dalloc(&P.tidx, (size_t)std::max(mc, 1) * cap));
+    A(dalloc(&P.th, 3 * (size_t)std::max(mc, 1) * cap));
+    A(dalloc(&P.sw, 3 * (size_t)std::max(mw, 1) * cap));
+    A(dalloc(&P.fix, cap));
+    A(dalloc(&P.perm, cap));
+    A(dalloc(&P.rank, cap));
+    P.ext = nullptr;
+    return e;
+}
+
+static void free_particles(Particles &P) {
+    for (int b = 0; b < 2; ++b) {
+        cudaFree(P.pos[b]);
+        cudaFree(P.vel[b]);
+        cudaFree(P.omg[b]);
+    }
+    cudaFree(P.force); cudaFree(P.torque); cudaFree(P.mI); cudaFree(P.mat); cudaFree(P.cstate);
+    cudaFree(P.tidx); cudaFree(P.th); cudaFree(P.sw); cudaFree(P.fix); cudaFree(P.perm); cudaFree(P.rank);
+    cudaFree(P.ext);
+    P = Particles{};
+}
+
+extern "C" int dem_particles_create(dem_ctx *ctx, int n, int max_contacts, int max_walls, dem_particles **out) {
+    if (!ctx || !out || n <= 0 || max_contacts < 0 || max_contacts > 255 || max_walls < 0 || max_walls > kMaxWalls)
+        return fail(ctx, DEM_ERR_INVALID, "dem_particles_create: n > 0, 0 <= max_contacts <= 255, max_walls <= 24");
+    *out = nullptr;
+    dem_particles *p = new dem_particles();
+    p->ctx = ctx;
+    cudaError_t e = alloc_particles(p->P, n, max_contacts, max_walls, true);
+    if (e == cudaSuccess) e = alloc_particles(p->alt, n, max_contacts, max_walls, false);
+    if (e == cudaSuccess) e = dalloc(&p->ctl, 1);
+    if (e != cudaSuccess) {
+        free_particles(p->P);
+        free_particles(p->alt);
+        cudaFree(p->ctl);
+        delete p;
+        return cuda_check(ctx, e, "dem_particles_create");
+    }
+    cudaStream_t s = ctx->stream;
+    const Particles &P = p->P;
+    for (int b = 0; b < 2; ++b) {
+        cudaMemsetAsync(P.pos[b], 0, sizeof(double4) * n, s);
+        cudaMemsetAsync(P.vel[b], 0, sizeof(double) * 3 * n, s);
+        cudaMemsetAsync(P.omg[b], 0, sizeof(double) * 3 * n, s);
+    }
+    cudaMemsetAsync(P.force, 0, sizeof(double) * 3 * n, s);
+    cudaMemsetAsync(P.torque, 0, sizeof(double) * 3 * n, s);
+    cudaMemsetAsync(P.mI, 0, sizeof(double2) * n, s);
+    cudaMemsetAsync(P.mat, 0, n, s);
+    cudaMemsetAsync(P.cstate, 0, sizeof(int) * n, s);
+    cudaMemsetAsync(P.th, 0, sizeof(double) * 3 * std::max(max_contacts, 1) * (size_t)n, s);
+    cudaMemsetAsync(P.sw, 0, sizeof(double) * 3 * std::max(max_walls, 1) * (size_t)n, s);
+    cudaMemsetAsync(P.fix, 0, n, s);
+    cudaMemsetAsync(p->ctl, 0, sizeof(Ctl), s);
+    k_init_particles<<<kGS, kTB, 0, s>>>(p->P);
+    p->rho.assign(n, 0.0);
+    p->E.assign(n, 0.0);
+    p->nu.assign(n, 0.0);
+    p->G.assign(n, 0.0);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s));
+    *out = p;
+    return DEM_OK;
+}
+
+extern "C" int dem_particles_destroy(dem_particles *p) {
+    if (!p) return DEM_ERR_INVALID;
+    cudaStreamSynchronize(p->ctx->stream);
+    free_particles(p->P);
+    free_particles(p->alt);
+    cudaFree(p->ctl);
+    delete p;
+    return DEM_OK;
+}
+
+extern "C" int dem_particles_size(dem_particles *p) { return p ? p->P.n : -1; }
+
+extern "C" int dem_particles_set(dem_particles *p, int field, const void *host, long count) {
+    if (!p || !host) return DEM_ERR_INVALID;
+    dem_ctx *ctx = p->ctx;
+    long need;
+    int es;
+    if (!field_layout(p, field, &need, &es) || count != need)
+        return fail(ctx, DEM_ERR_INVALID, "dem_particles_set: unknown field or wrong element count");
+    const int n = p->P.n;
+    cudaStream_t s = ctx->stream;
+    Particles &P = p->P;
+    if (field == DEM_F_RHO || field == DEM_F_E || field == DEM_F_NU || field == DEM_F_G) {
+        std::vector<double> &dst = field == DEM_F_RHO ? p->rho : field == DEM_F_E ? p->E : field == DEM_F_NU ? p->nu : p->G;
+        std::memcpy(dst.data(), host, sizeof(double) * n);
+        if (field != DEM_F_RHO) p->mat_dirty = true;
+        return DEM_OK;
+    }
+    void *tmp = nullptr;
+    CK(cudaMalloc(&tmp, (size_t)need * es));
+    CK(cudaMemcpyAsync(tmp, host, (size_t)need * es, cudaMemcpyHostToDevice, s));
+    const int cur = host_cur(p);
+    switch (field) {
+        case DEM_F_X: k_scatter_pos<<<kGS, kTB, 0, s>>>((double *)tmp, P.pos[cur], n, P.rank, 0); break;
+        case DEM_F_RAD: {
+            k_scatter_pos<<<kGS, kTB, 0, s>>>((double *)tmp, P.pos[cur], n, P.rank, 1);
+            const double *r = (const double *)host;
+            p->rmax = 0.0;
+            for (int i = 0; i < n; ++i) p->rmax = std::max(p->rmax, r[i]);
+            break;
+        }
+        case DEM_F_U: k_scatter_d<<<kGS, kTB, 0, s>>>((double *)tmp, P.vel[cur], n, 3, P.cap, P.rank); break;
+        case DEM_F_OMEGA: k_scatter_d<<<kGS, kTB, 0, s>>>((double *)tmp, P.omg[cur], n, 3, P.cap, P.rank); break;
+        case DEM_F_FORCE: k_scatter_d<<<kGS, kTB, 0, s>>>((double *)tmp, P.force, n, 3, P.cap, P.rank); break;
+        case DEM_F_TORQUE: k_scatter_d<<<kGS, kTB, 0, s>>>((double *)tmp, P.torque, n, 3, P.cap, P.rank); break;
+        case DEM_F_EXT_FORCE:
+            if (!P.ext) {
+                CK(dalloc(&P.ext, 3 * (size_t)P.cap));
+                CK(dalloc(&p->alt.ext, 3 * (size_t)P.cap));
+            }
+            k_scatter_d<<<kGS, kTB, 0, s>>>((double *)tmp, P.ext, n, 3, P.cap, P.rank);
+            break;
+        case DEM_F_M: k_scatter_mI<<<kGS, kTB, 0, s>>>((double *)tmp, P.mI, n, P.rank, 0); break;
+        case DEM_F_I: k_scatter_mI<<<kGS, kTB, 0, s>>>((double *)tmp, P.mI, n, P.rank, 1); break;
+        case DEM_F_TNG_IDX: k_scatter_i<<<kGS, kTB, 0, s>>>((int *)tmp, P.tidx, n, P.mc, P.cap, P.rank, 1); break;
+        case DEM_F_TNG_SS_X: case DEM_F_TNG_SS_Y: case DEM_F_TNG_SS_Z:
+            k_scatter_d<<<kGS, kTB, 0, s>>>((double *)tmp, P.th + (long)(field - DEM_F_TNG_SS_X) * P.mc * P.cap, n, P.mc,
+                                            P.cap, P.rank);
+            break;
+        case DEM_F_TNG_COUNT: k_scatter_count<<<kGS, kTB, 0, s>>>((int *)tmp, P.cstate, n, P.rank); break;
+        case DEM_F_TNG_SW_X: case DEM_F_TNG_SW_Y: case DEM_F_TNG_SW_Z:
+            k_scatter_d<<<kGS, kTB, 0, s>>>((double *)tmp, P.sw + (long)(field - DEM_F_TNG_SW_X) * P.mw * P.cap, n, P.mw,
+                                            P.cap, P.rank);
+            k_sw_mask<<<kGS, kTB, 0, s>>>(P);
+            break;
+        case DEM_F_FIX: k_scatter_u8<<<kGS, kTB, 0, s>>>((uint8_t *)tmp, P.fix, n, P.rank); break;
+    }
+    cudaError_t e = cudaGetLastError();
+    cudaStreamSynchronize(s);
+    cudaFree(tmp);
+    CK(e);
+    p->dirty = true;
+    k_invalidate<<<1, 32, 0, s>>>(p->ctl);
+    return DEM_OK;
+}
+
+extern "C" int dem_particles_get(dem_particles *p, int field, void *host, long count) {
+    if (!p || !host) return DEM_ERR_INVALID;
+    dem_ctx *ctx = p->ctx;
+    long need;
+    int es;
+    if (!field_layout(p, field, &need, &es) || count != need)
+        return fail(ctx, DEM_ERR_INVALID, "dem_particles_get: unknown field or wrong element count");
+    const int n = p->P.n;
+    cudaStream_t s = ctx->stream;
+    Particles &P = p->P;
+    if (field == DEM_F_RHO || field == DEM_F_E || field == DEM_F_NU || field == DEM_F_G) {
+        const std::vector<double> &src = field == DEM_F_RHO ? p->rho : field == DEM_F_E ? p->E : field == DEM_F_NU ? p->nu : p->G;
+        std::memcpy(host, src.data(), sizeof(double) * n);
+        return DEM_OK;
+    }
+    if (field == DEM_F_EXT_FORCE && !P.ext) {
+        std::memset(host, 0, sizeof(double) * 3 * n);
+        return DEM_OK;
+    }
+    void *tmp = nullptr;
+    CK(cudaMalloc(&tmp, (size_t)need * es));
+    const int cur = host_cur(p);
+    switch (field) {
+        case DEM_F_X: k_gather_pos<<<kGS, kTB, 0, s>>>(P.pos[cur], (double *)tmp, n, P.rank, 0); break;
+        case DEM_F_RAD: k_gather_pos<<<kGS, kTB, 0, s>>>(P.pos[cur], (double *)tmp, n, P.rank, 1); break;
+        case DEM_F_U: k_gather_d<<<kGS, kTB, 0, s>>>(P.vel[cur], (double *)tmp, n, 3, P.cap, P.rank); break;
+        case DEM_F_OMEGA: k_gather_d<<<kGS, kTB, 0, s>>>(P.omg[cur], (double *)tmp, n, 3, P.cap, P.rank); break;
+        case DEM_F_FORCE: k_gather_d<<<kGS, kTB, 0, s>>>(P.force, (double *)tmp, n, 3, P.cap, P.rank); break;
+        case DEM_F_TORQUE: k_gather_d<<<kGS, kTB, 0, s>>>(P.torque, (double *)tmp, n, 3, P.cap, P.rank); break;
+        case DEM_F_EXT_FORCE: k_gather_d<<<kGS, kTB, 0, s>>>(P.ext, (double *)tmp, n, 3, P.cap, P.rank); break;
+        case DEM_F_M: k_gather_mI<<<kGS, kTB, 0, s>>>(P.mI, (double *)tmp, n, P.rank, 0); break;
+        case DEM_F_I: k_gather_mI<<<kGS, kTB, 0, s>>>(P.mI, (double *)tmp, n, P.rank, 1); break;
+        case DEM_F_TNG_IDX: k_gather_i<<<kGS, kTB, 0, s>>>(P.tidx, (int *)tmp, n, P.mc, P.cap, P.rank, P.perm, 1); break;
+        case DEM_F_TNG_SS_X: case DEM_F_TNG_SS_Y: case DEM_F_TNG_SS_Z:
+            k_gather_d<<<kGS, kTB, 0, s>>>(P.th + (long)(field - DEM_F_TNG_SS_X) * P.mc * P.cap, (double *)tmp, n, P.mc,
+                                           P.cap, P.rank);
+            break;
+        case DEM_F_TNG_COUNT: k_gather_count<<<kGS, kTB, 0, s>>>(P.cstate, (int *)tmp, n, P.rank); break;
+        case DEM_F_TNG_SW_X: case DEM_F_TNG_SW_Y: case DEM_F_TNG_SW_Z:
+            k_gather_d<<<kGS, kTB, 0, s>>>(P.sw + (long)(field - DEM_F_TNG_SW_X) * P.mw * P.cap, (double *)tmp, n, P.mw,
+                                           P.cap, P.rank);
+            break;
+        case DEM_F_FIX: k_gather_u8<<<kGS, kTB, 0, s>>>(P.fix, (uint8_t *)tmp, n, P.rank); break;
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(host, tmp, (size_t)need * es, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(tmp);
+    CK(e);
+    return DEM_OK;
+}
+
+// ---- walls --------------------------------------------------------------------------
+extern "C" int dem_walls_create(dem_ctx *ctx, int n, dem_walls **out) {
+    if (!ctx || !out || n < 0 || n > kMaxWalls) return fail(ctx, DEM_ERR_INVALID, "dem_walls_create: 0 <= n <= 24");
+    dem_walls *w = new dem_walls();
+    w->ctx = ctx;
+    w->n = n;
+    w->x.assign(3 * n, 0.0);
+    w->u.assign(3 * n, 0.0);
+    w->omega.assign(3 * n, 0.0);
+    w->normal.assign(3 * n, 0.0);
+    w->E.assign(n, 0.0);
+    w->nu.assign(n, 0.0);
+    w->G.assign(n, 0.0);
+    *out = w;
+    return DEM_OK;
+}
+
+extern "C" int dem_walls_destroy(dem_walls *w) {
+    if (!w) return DEM_ERR_INVALID;
+    delete w;
+    return DEM_OK;
+}
+
+extern "C" int dem_walls_set(dem_walls *w, int field, const double *host, long count) {
+    if (!w || !host) return DEM_ERR_INVALID;
+    std::vector<double> *dst = nullptr;
+    long need = w->n;
+    switch (field) {
+        case DEM_W_X: dst = &w->x; need = 3L * w->n; break;
+        case DEM_W_U: dst = &w->u; need = 3L * w->n; break;
+        case DEM_W_OMEGA: dst = &w->omega; need = 3L * w->n; break;
+        case DEM_W_NORMAL: dst = &w->normal; need = 3L * w->n; break;
+        case DEM_W_E: dst = &w->E; break;
+        case DEM_W_NU: dst = &w->nu; break;
+        case DEM_W_G: dst = &w->G; break;
+        default: return fail(w->ctx, DEM_ERR_INVALID, "dem_walls_set: unknown field");
+    }
+    if (count != need) return fail(w->ctx, DEM_ERR_INVALID, "dem_walls_set: wrong element count");
+    std::copy(host, host + count, dst->begin());
+    return DEM_OK;
+}
+
+// ---- solver -------------------------------------------------------------------------
+namespace {
+
+// Host-side constants, each in the reference's expression order.
+PairConst pair_const(double E_i, double nu_i, double G_i, double E_j, double nu_j, double G_j) {
+    PairConst c{};
+    double tmp_1 = (1. - (nu_i * nu_i)) / E_i;   // Force.hpp:196-198
+    double tmp_2 = (1. - (nu_j * nu_j)) / E_j;
+    const double E_eff = 1. / (tmp_1 + tmp_2);
+    tmp_1 = (2. - nu_i) / G_i;                    // Force.hpp:218-220
+    tmp_2 = (2. - nu_j) / G_j;
+    const double G_eff = 1. / (tmp_1 + tmp_2);
+    c.c_kn = 4. / 3. * E_eff;
+    c.c_Sn = 2. * E_eff;
+    c.c_kt = 8. * G_eff;
+    return c;
+}
+
+double beta_of(double cor) {   // Force.hpp:206-210
+    const double tmp_1 = std::log(cor);
+    const double tmp_2 = tmp_1 * tmp_1 + M_PI * M_PI;
+    return tmp_1 / std::sqrt(tmp_2);
+}
+
+int prepare(dem_solver *s) {
+    dem_ctx *ctx = s->ctx;
+    dem_particles *p = s->p;
+    cudaStream_t st = ctx->stream;
+    const int n = p->P.n;
+    if (p->mat_dirty) {
+        std::map<std::tuple<double, double, double>, int> ids;
+        p->mats.clear();
+        p->mat.assign(n, 0);
+        for (int i = 0; i < n; ++i) {
+            auto key = std::make_tuple(p->E[i], p->nu[i], p->G[i]);
+            auto it = ids.find(key);
+            if (it == ids.end()) {
+                if ((int)p->mats.size() >= kMaxMat)
+                    return fail(ctx, DEM_ERR_UNSUPPORTED, "more than 32 distinct (E, nu, G) materials");
+                it = ids.emplace(key, (int)p->mats.size()).first;
+                p->mats.push_back(key);
+            }
+            p->mat[i] = (uint8_t)it->second;
+        }
+        uint8_t *tmp = nullptr;
+        CK(cudaMalloc(&tmp, n));
+        CK(cudaMemcpyAsync(tmp, p->mat.data(), n, cudaMemcpyHostToDevice, st));
+        k_scatter_u8<<<kGS, kTB, 0, st>>>(tmp, p->P.mat, n, p->P.rank);
+        CK(cudaStreamSynchronize(st));
+        cudaFree(tmp);
+        p->mat_dirty = false;
+        s->built = false;
+    }
+    const int nm = (int)p->mats.size();
+    const int nw = s->w ? s->w->n : 0;
+    std::vector<PairConst> pp((size_t)nm * nm), pw((size_t)nm * std::max(nw, 1));
+    for (int a = 0; a < nm; ++a) {
+        const auto &A = p->mats[a];
+        for (int b = 0; b < nm; ++b) {
+            const auto &B = p->mats[b];
+            pp[(size_t)a * nm + b] = pair_const(std::get<0>(A), std::get<1>(A), std::get<2>(A), std::get<0>(B),
+                                                std::get<1>(B), std::get<2>(B));
+        }
+        for (int w = 0; w < nw; ++w)
+            pw[(size_t)a * nw + w] = pair_const(std::get<0>(A), std::get<1>(A), std::get<2>(A), s->w->E[w], s->w->nu[w],
+                                                s->w->G[w]);
+    }
+    std::vector<WallGeom> wg(std::max(nw, 1));
+    for (int w = 0; w < nw; ++w)
+        for (int d = 0; d < 3; ++d) {
+            wg[w].x[d] = s->w->x[3 * w + d];
+            wg[w].n[d] = s->w->normal[3 * w + d];
+        }
+    cudaFree(s->d_pp);
+    cudaFree(s->d_pw);
+    cudaFree(s->d_walls);
+    CK(dalloc(&s->d_pp, pp.size()));
+    CK(dalloc(&s->d_pw, pw.size()));
+    CK(dalloc(&s->d_walls, wg.size()));
+    CK(cudaMemcpyAsync(s->d_pp, pp.data(), pp.size() * sizeof(PairConst), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(s->d_pw, pw.data(), pw.size() * sizeof(PairConst), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(s->d_walls, wg.data(), wg.size() * sizeof(WallGeom), cudaMemcpyHostToDevice, st));
+    ForceConsts &fc = s->fc;
+    fc = ForceConsts{};
+    const unsigned q = s->fp.quirks;
+    const double bpp = beta_of(s->fp.cor_pp), bpw = beta_of(s->fp.cor_pw);
+    fc.K_n_pp = -2. * std::sqrt(5. / 6.) * bpp;             // Force.hpp:215
+    fc.K_n_pw = -2. * std::sqrt(5. / 6.) * bpw;             // Force.hpp:580
+    fc.K_t_pp = (q & DEM_Q2_ETA_T_ZERO) ? -2 * std::sqrt((double)(5 / 6)) * bpp : fc.K_n_pp;   // :224
+    fc.K_t_pw = (q & DEM_Q2_ETA_T_ZERO) ? -2 * std::sqrt((double)(5 / 6)) * bpw : fc.K_n_pw;   // :618
+    fc.mu_pp = s->fp.mu_pp;
+    fc.mu_pw = s->fp.mu_pw;
+    fc.dt = s->sp.dt;
+    fc.half_dt = 0.5 * s->sp.dt;                             // Integrator.hpp:25
+    for (int d = 0; d < 3; ++d) fc.g[d] = s->sp.gravity[d];
+    fc.has_gravity = (fc.g[0] != 0.0 || fc.g[1] != 0.0 || fc.g[2] != 0.0) ? 1 : 0;
+    fc.quirks = q;
+    fc.nmat = nm;
+    fc.nwall = nw;
+    fc.has_ext = p->P.ext ? 1 : 0;
+    fc.has_fix = 1;
+    CK(cudaStreamSynchronize(st));
+    s->version++;
+    return DEM_OK;
+}
+
+int alloc_lists(dem_solver *s, int maxnb) {
+    dem_ctx *ctx = s->ctx;
+    cudaFree(s->L.nn);
+    cudaFree(s->L.idx);
+    s->L.maxnb = maxnb;
+    CK(dalloc(&s->L.nn, s->p->P.cap));
+    CK(dalloc(&s->L.idx, (size_t)maxnb * s->p->P.cap));
+    CK(cudaMemsetAsync(s->L.nn, 0, sizeof(int) * s->p->P.cap, ctx->stream));
+    s->version++;
+    s->built = false;
+    return DEM_OK;
+}
+
+Ctl read_ctl(dem_solver *s) {
+    Ctl c{};
+    cudaMemcpyAsync(&c, s->p->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s->ctx->stream);
+    cudaStreamSynchronize(s->ctx->stream);
+    return c;
+}
+
+__global__ void k_clear_status(Ctl *ctl, int bits) {
+    if (threadIdx.x == 0) ctl->status &= ~bits;
+}
+
+bool ref_mode(const dem_solver *s) { return s->sp.rebuild_every_step != 0; }
+
+// Build with overflow handling (host-driven; re-sorts into Morton order).
+int build_now(dem_solver *s, bool resort) {
+    dem_ctx *ctx = s->ctx;
+    for (int attempt = 0; attempt < 8; ++attempt) {
+        launch_build(s->p->P, s->p->alt, s->L, s->B, s->p->ctl, s->sp.delta, s->sp.skin, resort, false,
+                     ctx->stream);
+        CK(cudaGetLastError());
+        Ctl c = read_ctl(s);
+        CK(cudaGetLastError());
+        if (!(c.status & DEM_ERR_NEIGHBOR_OVERFLOW)) {
+            s->built = true;
+            s->p->dirty = false;
+            return DEM_OK;
+        }
+        const int want = std::min(std::max(2 * s->L.maxnb, c.max_nbr + 8), 128);
+        if (c.max_nbr > 128) return fail(ctx, DEM_ERR_NEIGHBOR_OVERFLOW, "more than 128 neighbours per particle");
+        int st = alloc_lists(s, want);
+        if (st) return st;
+        k_clear_status<<<1, 32, 0, ctx->stream>>>(s->p->ctl, DEM_ERR_NEIGHBOR_OVERFLOW);
+        resort = false;
+    }
+    return fail(ctx, DEM_ERR_NEIGHBOR_OVERFLOW, "neighbour list did not converge");
+}
+
+int capture_graph(dem_solver *s, int steps) {
+    dem_ctx *ctx = s->ctx;
+    if (s->graph) {
+        cudaGraphExecDestroy(s->graph);
+        s->graph = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < steps; ++k) {
+        if (ref_mode(s))
+            launch_build(s->p->P, s->p->alt, s->L, s->B, s->p->ctl, s->sp.delta, s->sp.skin, false, true, ctx->stream);
+        launch_step(s->p->P, s->L, s->p->ctl, s->fc, s->d_pp, s->d_pw, s->d_walls, MODE_FUSED, ctx->stream);
+    }
+    CK(cudaStreamEndCapture(ctx->stream, &g));
+    cudaError_t e = cudaGraphInstantiate(&s->graph, g, 0);
+    cudaGraphDestroy(g);
+    CK(e);
+    s->graph_steps = steps;
+    s->graph_version = s->version;
+    return DEM_OK;
+}
+
+}  // namespace
+
+extern "C" int dem_solver_create(dem_ctx *ctx, dem_particles *p, dem_walls *w, const dem_force_params *fp,
+                                 const dem_solver_params *sp, dem_solver **out) {
+    if (!ctx || !p || !fp || !sp || !out || !(sp->dt > 0.0))
+        return fail(ctx, DEM_ERR_INVALID, "dem_solver_create: null argument or dt <= 0");
+    if (sp->precision != DEM_FP64 && sp->precision != DEM_MIXED)
+        return fail(ctx, DEM_ERR_INVALID, "dem_solver_create: unknown precision");
+    if (w && w->n > p->P.mw && w->n > 0)
+        return fail(ctx, DEM_ERR_INVALID, "dem_solver_create: more walls than MaxNoWalls history slots");
+    if (sp->delta <= 0.0 && sp->skin < 0.0) return fail(ctx, DEM_ERR_INVALID, "dem_solver_create: skin < 0");
+    dem_solver *s = new dem_solver();
+    s->ctx = ctx;
+    s->p = p;
+    s->w = w;
+    s->fp = *fp;
+    s->sp = *sp;
+    if (s->sp.steps_per_launch <= 0) s->sp.steps_per_launch = 32;
+    const int n = p->P.cap;
+    BuildBuffers &B = s->B;
+    B.cell_cap = std::min<long>(std::max<long>(8L * n, 32768L), 1L << 28);
+    cudaError_t e = cudaSuccess;
+    auto A = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
+    A(dalloc(&B.grid, 1));
+    A(dalloc(&B.key, n));
+    A(dalloc(&B.cell_start, (size_t)B.cell_cap + 1));
+    A(dalloc(&B.cell_fill, (size_t)B.cell_cap + 1));
+    A(dalloc(&B.cell_items, n));
+    A(dalloc(&B.block_sums, (size_t)B.cell_cap / 2048 + 2));
+    A(dalloc(&B.bbox, 8));
+    A(dalloc(&B.src, n));
+    A(dalloc(&B.dst, n));
+    s->nparts = (p->P.n + 127) / 128;
+    A(dalloc(&s->d_epart, 4 * (size_t)s->nparts));
+    A(dalloc(&s->d_eout, 4));
+    if (e != cudaSuccess) {
+        dem_solver_destroy(s);
+        return cuda_check(ctx, e, "dem_solver_create");
+    }
+    int st = alloc_lists(s, sp->max_neighbors > 0 ? std::min(sp->max_neighbors, 128) : 32);
+    if (!st) st = prepare(s);
+    if (st) {
+        dem_solver_destroy(s);
+        return st;
+    }
+    *out = s;
+    return DEM_OK;
+}
+
+extern "C" int dem_solver_destroy(dem_solver *s) {
+    if (!s) return DEM_ERR_INVALID;
+    cudaStreamSynchronize(s->ctx->stream);
+    if (s->graph) cudaGraphExecDestroy(s->graph);
+    cudaFree(s->d_pp); cudaFree(s->d_pw); cudaFree(s->d_walls);
+    cudaFree(s->L.nn); cudaFree(s->L.idx);
+    BuildBuffers &B = s->B;
+    cudaFree(B.grid); cudaFree(B.key); cudaFree(B.cell_start); cudaFree(B.cell_fill); cudaFree(B.cell_items);
+    cudaFree(B.block_sums); cudaFree(B.bbox); cudaFree(B.src); cudaFree(B.dst);
+    cudaFree(s->d_epart); cudaFree(s->d_eout);
+    delete s;
+    return DEM_OK;
+}
+
+extern "C" int dem_solver_run(dem_solver *s, int nsteps) {
+    if (!s) return DEM_ERR_INVALID;
+    if (nsteps <= 0) return DEM_OK;
+    dem_ctx *ctx = s->ctx;
+    if (s->p->mat_dirty || (s->p->P.ext != nullptr) != (s->fc.has_ext != 0)) {
+        int st = prepare(s);
+        if (st) return st;
+    }
+    cudaStream_t st = ctx->stream;
+    double half_skin;
+    if (ref_mode(s)) half_skin = 1e300;
+    else if (s->sp.delta > 0.0) half_skin = std::max(0.0, s->sp.delta - 2.0 * s->p->rmax) / 2.0;
+    else half_skin = s->sp.skin / 2.0;
+    k_run_begin<<<1, 32, 0, st>>>(s->p->ctl, nsteps, half_skin);
+    launch_prologue(s->p->P, s->p->ctl, s->fc, st);
+    CK(cudaGetLastError());
+    const int chunk = s->sp.steps_per_launch;
+    if (ref_mode(s)) {
+        // rebuild before every force pass, inside the graph (no re-sort)
+        for (;;) {
+            if (!s->graph || s->graph_version != s->version || s->graph_steps != chunk) {
+                int e = capture_graph(s, chunk);
+                if (e) return e;
+            }
+            Ctl c{};
+            int done_before = -1;
+            for (;;) {
+                CK(cudaGraphLaunch(s->graph, st));
+                c = read_ctl(s);
+                if (c.steps_done >= c.target || (c.status & DEM_ERR_NEIGHBOR_OVERFLOW) || c.steps_done == done_before)
+                    break;
+                done_before = c.steps_done;
+            }
+            if (c.status & DEM_ERR_NEIGHBOR_OVERFLOW) {
+                const int want = std::min(std::max(2 * s->L.maxnb, c.max_nbr + 8), 128);
+                if (c.max_nbr > 128) return fail(ctx, DEM_ERR_NEIGHBOR_OVERFLOW, "more than 128 neighbours");
+                int e = alloc_lists(s, want);
+                if (e) return e;
+                k_clear_status<<<1, 32, 0, st>>>(s->p->ctl, DEM_ERR_NEIGHBOR_OVERFLOW);
+                continue;
+            }
+            if (c.steps_done >= c.target) break;
+            return fail(ctx, DEM_ERR_CUDA, "solver made no progress");
+        }
+    } else {
+        if (!s->built || s->p->dirty) {
+            int e = build_now(s, true);
+            if (e) return e;
+        }
+        for (int guard = 0;; ++guard) {
+            if (!s->graph || s->graph_version != s->version || s->graph_steps != chunk) {
+                int e = capture_graph(s, chunk);
+                if (e) return e;
+            }
+            CK(cudaGraphLaunch(s->graph, st));
+            Ctl c = read_ctl(s);
+            CK(cudaGetLastError());
+            if (c.steps_done >= c.target) break;
+            if (!(c.disp < c.half_skin)) {
+                int e = build_now(s, true);
+                if (e) return e;
+            }
+            if (guard > 4 * (nsteps + 4)) return fail(ctx, DEM_ERR_CUDA, "solver made no progress");
+        }
+    }
+    Ctl c = read_ctl(s);
+    CK(cudaGetLastError());
+    return c.status & (DEM_ERR_CONTACT_OVERFLOW | DEM_ERR_NAN);
+}
+
+extern "C" int dem_solver_stats(dem_solver *s, dem_run_stats *out) {
+    if (!s || !out) return DEM_ERR_INVALID;
+    Ctl c = read_ctl(s);
+    out->steps = c.total_steps;
+    out->rebuilds = c.rebuilds;
+    out->max_neighbors = c.max_nbr;
+    out->neighbor_capacity = s->L.maxnb;
+    out->status = c.status;
+    out->disp_bound = c.disp;
+    return DEM_OK;
+}
+
+extern "C" int dem_stage1(dem_solver *s) {
+    if (!s) return DEM_ERR_INVALID;
+    dem_ctx *ctx = s->ctx;
+    launch_stage(s->p->P, s->p->ctl, s->fc, 1, ctx->stream);
+    CK(cudaGetLastError());
+    return DEM_OK;
+}
+extern "C" int dem_stage2(dem_solver *s) {
+    if (!s) return DEM_ERR_INVALID;
+    dem_ctx *ctx = s->ctx;
+    launch_stage(s->p->P, s->p->ctl, s->fc, 2, ctx->stream);
+    k_invalidate<<<1, 32, 0, ctx->stream>>>(s->p->ctl);
+    CK(cudaGetLastError());
+    return DEM_OK;
+}
+extern "C" int dem_stage3(dem_solver *s) {
+    if (!s) return DEM_ERR_INVALID;
+    dem_ctx *ctx = s->ctx;
+    launch_stage(s->p->P, s->p->ctl, s->fc, 3, ctx->stream);
+    CK(cudaGetLastError());
+    return DEM_OK;
+}
+extern "C" int dem_build_neighbors(dem_solver *s) {
+    if (!s) return DEM_ERR_INVALID;
+    if (s->p->mat_dirty || (s->p->P.ext != nullptr) != (s->fc.has_ext != 0)) {
+        int st = prepare(s);
+        if (st) return st;
+    }
+    int st = build_now(s, false);
+    if (st) return st;
+    return DEM_OK;
+}
+extern "C" int dem_compute_force(dem_solver *s) {
+    if (!s) return DEM_ERR_INVALID;
+    dem_ctx *ctx = s->ctx;
+    if (s->p->mat_dirty || (s->p->P.ext != nullptr) != (s->fc.has_ext != 0)) {
+        int st = prepare(s);
+        if (st) return st;
+    }
+    if (!s->built) return fail(ctx, DEM_ERR_INVALID, "dem_compute_force: build the neighbour list first");
+    launch_step(s->p->P, s->L, s->p->ctl, s->fc, s->d_pp, s->d_pw, s->d_walls, MODE_FORCE_ONLY, ctx->stream);
+    CK(cudaGetLastError());
+    Ctl c = read_ctl(s);
+    return c.status & (DEM_ERR_CONTACT_OVERFLOW | DEM_ERR_NAN);
+}
+
+extern "C" int dem_neighbors_get(dem_solver *s, int *offsets, int *idx, long *total) {
+    if (!s || !offsets) return DEM_ERR_INVALID;
+    dem_ctx *ctx = s->ctx;
+    const int n = s->p->P.n, cap = s->p->P.cap, mb = s->L.maxnb;
+    std::vector<int> nn(n), li((size_t)mb * cap), perm(n), rank(n);
+    cudaStream_t st = ctx->stream;
+    CK(cudaMemcpyAsync(nn.data(), s->L.nn, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(li.data(), s->L.idx, sizeof(int) * li.size(), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(perm.data(), s->p->P.perm, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(rank.data(), s->p->P.rank, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    offsets[0] = 0;
+    for (int c = 0; c < n; ++c) offsets[c + 1] = offsets[c] + nn[rank[c]];
+    if (total) *total = offsets[n];
+    if (idx)
+        for (int c = 0; c < n; ++c) {
+            const int p = rank[c];
+            for (int k = 0; k < nn[p]; ++k) idx[offsets[c] + k] = perm[li[(size_t)k * cap + p]];
+        }
+    return DEM_OK;
+}
+
+extern "C" int dem_energy(dem_solver *s, double out[4]) {
+    if (!s || !out) return DEM_ERR_INVALID;
+    dem_ctx *ctx = s->ctx;
+    launch_energy(s->p->P, s->L, s->p->ctl, s->fc, s->d_pp, s->d_pw, s->d_walls, s->d_epart, s->nparts, s->d_eout,
+                  ctx->stream);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, s->d_eout, 4 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return DEM_OK;
+}

@@ -1,0 +1,126 @@
+// dem_internal.cuh -- device data layout and launcher declarations shared by the
+// translation units of libb200dem.so.
+//
+// HBM layout (particles in Morton-sorted order, capacity `cap` = n):
+//   pos[2]    double4 (x, y, z, r)      ping-pong; neighbour gathers read one 32 B sector
+//   vel[2]    double  [3][cap]           ping-pong SoA (ux | uy | uz)
+//   omg[2]    double  [3][cap]           ping-pong SoA
+//   force, torque double [3][cap]        written by the last fused step / unfused force pass
+//   mI        double2 (m, I)
+//   mat       uint8 material id          (E, nu, G) deduplicated into pair tables
+//   cstate    int: pp contact count (bits 0-7) | wall-history-active mask (bits 8-31)
+//   tidx      int    [MaxCnts][cap]      partner (sorted index), slot-major
+//   th        double [3][MaxCnts][cap]   tangential history x|y|z, slot-major
+//   sw        double [3][MaxNoWalls][cap] wall tangential history
+//   fix       uint8 flags, ext double [3][cap] (optional)
+//   perm      sorted index -> caller index; rank: caller index -> sorted index
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace b200dem {
+
+constexpr int kMaxWalls = 24;
+constexpr int kMaxMat = 32;
+
+struct Ctl {
+    int cur;                  // current ping-pong buffer
+    int steps_done;           // fused steps executed in the current run
+    int target;               // fused steps requested in the current run
+    unsigned ticket;          // last-block election
+    unsigned long long vmax2; // max |u|^2 of the drift in the running kernel (double bits)
+    double disp;              // displacement bound since the last build
+    double half_skin;         // stale threshold (list invalid once disp >= half_skin)
+    int status;               // sticky DEM_ERR_* bits
+    int max_nbr;              // longest neighbour list seen at the last build
+    long long total_steps;
+    long long rebuilds;
+};
+
+struct Particles {
+    int n, cap, mc, mw;
+    double4 *pos[2];
+    double *vel[2];
+    double *omg[2];
+    double *force, *torque;
+    double2 *mI;
+    uint8_t *mat;
+    int *cstate;
+    int *tidx;
+    double *th;
+    double *sw;
+    uint8_t *fix;
+    double *ext;   // may be null
+    int *perm, *rank;
+};
+
+struct PairConst {   // per (material a, material b) or (material a, wall w)
+    double c_kn;     // 4./3. * E_eff            (Force.hpp:203, :568)
+    double c_Sn;     // 2. * E_eff               (Force.hpp:211, :576)
+    double c_kt;     // 8. * G_eff               (Force.hpp:222, :616)
+    double pad;
+};
+
+struct WallGeom {
+    double x[3];
+    double n[3];
+};
+
+struct ForceConsts {
+    double K_n_pp, K_t_pp;     // eta = K * sqrt(S * m_eff)       (Force.hpp:215, :224)
+    double K_n_pw, K_t_pw;     //                                  (Force.hpp:580, :618)
+    double mu_pp, mu_pw;
+    double dt, half_dt;
+    double g[3];
+    unsigned quirks;
+    int nmat, nwall;
+    int has_gravity;
+    int has_ext;
+    int has_fix;
+};
+
+struct NbrList {
+    int *nn;     // [cap] list length
+    int *idx;    // [maxnb][cap] sorted indices, ascending caller id
+    int maxnb;
+};
+
+struct Grid {                 // computed on the device at every build
+    double lo[3];
+    double cell, inv_cell;
+    int dims[3];
+    int bits;                 // Morton bits per axis (0: linear cell index)
+    int ncodes;               // number of cell keys
+    double rmax;
+    int overflow;             // cell keys exceeded the table
+};
+
+struct BuildBuffers {
+    Grid *grid;               // device
+    int *key;                 // [cap]
+    int *cell_start;          // [cell_cap + 1]
+    int *cell_fill;           // [cell_cap]
+    int *cell_items;          // [cap] sorted-order index per cell slot
+    int *block_sums;          // scan scratch
+    int cell_cap;
+    unsigned long long *bbox; // 7 ordered-int words: lo[3], hi[3], rmax
+    int *src, *dst;           // permutation at re-sort
+};
+
+// ---- launchers (dem_step.cu) ------------------------------------------------------
+enum StepMode { MODE_FUSED = 0, MODE_FORCE_ONLY = 1 };
+void launch_prologue(const Particles &P, Ctl *ctl, const ForceConsts &fc, cudaStream_t s);
+void launch_step(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
+                 const PairConst *pw, const WallGeom *walls, int mode, cudaStream_t s);
+void launch_stage(const Particles &P, Ctl *ctl, const ForceConsts &fc, int stage, cudaStream_t s);
+void launch_energy(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
+                   const PairConst *pw, const WallGeom *walls, double *partials, int nparts, double *out,
+                   cudaStream_t s);
+
+// ---- launchers (dem_nbr.cu) -------------------------------------------------------
+// Builds the neighbour list of the current order; with `resort` the particles are first
+// re-ordered by Morton cell key (state permuted, contact partners remapped).
+void launch_build(const Particles &P, Particles &alt, const NbrList &L, BuildBuffers &B, Ctl *ctl, double delta,
+                  double skin, bool resort, bool check_run, cudaStream_t s);
+
+}  // namespace b200dem

@@ -1,0 +1,405 @@
+// dem_nbr.cu -- cell-list Verlet neighbour build on sm_100a (replaces Cabana's
+// VerletList<FullNeighborTag, VerletLayout2D> used at src/CabanaDEM_Solver.hpp:61-63,
+// :87-88 and src/CabanaBondedDEM_Particles.hpp:155-157).
+//
+// Pipeline (all on the device, no host round trip, so it can sit in a CUDA graph):
+//   bbox      min/max of positions and max radius (ordered-integer atomics)
+//   grid      cell size >= largest cutoff, Morton cell keys when they fit the table
+//   count     particles per cell key;  scan  exclusive prefix sum (3 kernels)
+//   fill      particle slots per cell; per-cell insertion sort by caller index
+//   [resort]  permute all particle state into cell-key (Morton) order, remap partners
+//   list      per particle: 27-cell stencil, keep j != i with |x_i - x_j| <= cutoff,
+//             sorted by caller index (the oracle's summation order)
+// Built with --fmad=false so that the distance test matches the oracle's.
+#include "dem_internal.cuh"
+#include "b200dem.h"
+
+namespace b200dem {
+
+namespace {
+
+constexpr int kB = 256;
+constexpr int kScanItems = 8;                 // per thread
+constexpr int kScanTile = kB * kScanItems;    // 2048 keys per block
+constexpr int kMaxCand = 128;                 // candidates kept per particle while sorting
+
+struct __align__(32) D4 {
+    double x, y, z, w;
+};
+__device__ __forceinline__ D4 ld4(const double4 *p, int i) { return reinterpret_cast<const D4 *>(p)[i]; }
+
+__device__ __forceinline__ unsigned long long ord(double x) {
+    const unsigned long long b = (unsigned long long)__double_as_longlong(x);
+    return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double unord(unsigned long long o) {
+    const unsigned long long b = (o & 0x8000000000000000ull) ? (o & 0x7fffffffffffffffull) : ~o;
+    return __longlong_as_double((long long)b);
+}
+
+__device__ __forceinline__ unsigned part1by2(unsigned x) {
+    x &= 0x3ff;
+    x = (x | (x << 16)) & 0x030000FF;
+    x = (x | (x << 8)) & 0x0300F00F;
+    x = (x | (x << 4)) & 0x030C30C3;
+    x = (x | (x << 2)) & 0x09249249;
+    return x;
+}
+
+__device__ __forceinline__ int cell_key(const Grid &g, int cx, int cy, int cz) {
+    if (g.bits > 0) return (int)(part1by2((unsigned)cx) | (part1by2((unsigned)cy) << 1) | (part1by2((unsigned)cz) << 2));
+    return (cz * g.dims[1] + cy) * g.dims[0] + cx;
+}
+
+__device__ __forceinline__ void cell_of(const Grid &g, const D4 &p, int c[3]) {
+    const double xs[3] = {p.x, p.y, p.z};
+    for (int d = 0; d < 3; ++d) {
+        int v = (int)floor((xs[d] - g.lo[d]) * g.inv_cell);
+        v = v < 0 ? 0 : (v >= g.dims[d] ? g.dims[d] - 1 : v);
+        c[d] = v;
+    }
+}
+
+__global__ void k_bbox_init(unsigned long long *bb) {
+    if (threadIdx.x < 3) bb[threadIdx.x] = ord(1e300);
+    else if (threadIdx.x < 6) bb[threadIdx.x] = ord(-1e300);
+    else if (threadIdx.x == 6) bb[6] = ord(0.0);
+}
+
+__global__ void k_bbox(Particles P, const Ctl *ctl, unsigned long long *bb) {
+    __shared__ unsigned long long s[7];
+    if (threadIdx.x < 7) s[threadIdx.x] = threadIdx.x < 3 ? ord(1e300) : (threadIdx.x < 6 ? ord(-1e300) : ord(0.0));
+    __syncthreads();
+    const int cur = ctl->cur;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += gridDim.x * blockDim.x) {
+        const D4 p = ld4(P.pos[cur], i);
+        atomicMin(&s[0], ord(p.x));
+        atomicMin(&s[1], ord(p.y));
+        atomicMin(&s[2], ord(p.z));
+        atomicMax(&s[3], ord(p.x));
+        atomicMax(&s[4], ord(p.y));
+        atomicMax(&s[5], ord(p.z));
+        atomicMax(&s[6], ord(p.w));
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) atomicMin(&bb[threadIdx.x], s[threadIdx.x]);
+    else if (threadIdx.x < 7) atomicMax(&bb[threadIdx.x], s[threadIdx.x]);
+}
+
+__global__ void k_grid(const unsigned long long *bb, Grid *g, int cell_cap, double delta, double skin) {
+    if (threadIdx.x != 0) return;
+    Grid G;
+    double lo[3], hi[3];
+    for (int d = 0; d < 3; ++d) {
+        lo[d] = unord(bb[d]);
+        hi[d] = unord(bb[3 + d]);
+        if (!(hi[d] >= lo[d])) hi[d] = lo[d];
+    }
+    G.rmax = unord(bb[6]);
+    const double cut = delta > 0.0 ? delta : 2.0 * G.rmax + skin;
+    double cell = cut > 0.0 ? cut : 1.0;
+    G.overflow = 0;
+    for (int it = 0; it < 200; ++it) {
+        double tot = 1.0;
+        int dmax = 1;
+        for (int d = 0; d < 3; ++d) {
+            const double e = floor((hi[d] - lo[d]) / cell) + 1.0;
+            G.dims[d] = (int)fmin(e, 1e9);
+            tot *= e;
+            dmax = max(dmax, G.dims[d]);
+        }
+        int bits = 0;
+        while ((1 << bits) < dmax) ++bits;
+        if (bits <= 10 && (double)(1LL << (3 * bits)) <= (double)cell_cap) {
+            G.bits = bits > 0 ? bits : 1;
+            G.ncodes = 1 << (3 * G.bits);
+            break;
+        }
+        if (tot <= (double)cell_cap) {
+            G.bits = 0;
+            G.ncodes = (int)tot;
+            break;
+        }
+        cell *= 1.26;
+    }
+    for (int d = 0; d < 3; ++d) G.lo[d] = lo[d];
+    G.cell = cell;
+    G.inv_cell = 1.0 / cell;
+    *g = G;
+}
+
+__global__ void k_zero(int *a, const Grid *g) {
+    const int n = g->ncodes + 1;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = 0;
+}
+
+__global__ void k_count(Particles P, const Ctl *ctl, const Grid *g, int *key, int *cnt) {
+    const Grid G = *g;
+    const int cur = ctl->cur;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += gridDim.x * blockDim.x) {
+        int c[3];
+        cell_of(G, ld4(P.pos[cur], i), c);
+        const int k = cell_key(G, c[0], c[1], c[2]);
+        key[i] = k;
+        atomicAdd(&cnt[k], 1);
+    }
+}
+
+// Exclusive scan of cnt[0..ncodes) into start[0..ncodes]; 3 passes.
+__global__ void k_scan_tiles(const int *cnt, int *start, int *sums, const Grid *g) {
+    __shared__ int s[kB];
+    const int n = g->ncodes;
+    const long base = (long)blockIdx.x * kScanTile;
+    if (base >= n) return;
+    int v[kScanItems];
+    int t = 0;
+    for (int k = 0; k < kScanItems; ++k) {
+        const long idx = base + (long)threadIdx.x * kScanItems + k;
+        v[k] = idx < n ? cnt[idx] : 0;
+        t += v[k];
+    }
+    s[threadIdx.x] = t;
+    __syncthreads();
+    for (int o = 1; o < kB; o <<= 1) {
+        const int a = threadIdx.x >= o ? s[threadIdx.x - o] : 0;
+        __syncthreads();
+        s[threadIdx.x] += a;
+        __syncthreads();
+    }
+    int run = s[threadIdx.x] - t;
+    for (int k = 0; k < kScanItems; ++k) {
+        const long idx = base + (long)threadIdx.x * kScanItems + k;
+        if (idx < n) start[idx] = run;
+        run += v[k];
+    }
+    if (threadIdx.x == kB - 1) sums[blockIdx.x] = s[kB - 1];
+}
+
+__global__ void k_scan_sums(int *sums, const Grid *g, int *start) {
+    // single block of kB threads; tiles <= kB * kScanItems * ... handled by a serial outer loop
+    __shared__ int s[kB];
+    const int n = g->ncodes;
+    const int tiles = (n + kScanTile - 1) / kScanTile;
+    int carry = 0;
+    for (int base = 0; base < tiles; base += kB) {
+        const int idx = base + threadIdx.x;
+        const int v = idx < tiles ? sums[idx] : 0;
+        s[threadIdx.x] = v;
+        __syncthreads();
+        for (int o = 1; o < kB; o <<= 1) {
+            const int a = threadIdx.x >= o ? s[threadIdx.x - o] : 0;
+            __syncthreads();
+            s[threadIdx.x] += a;
+            __syncthreads();
+        }
+        if (idx < tiles) sums[idx] = carry + s[threadIdx.x] - v;
+        const int tot = s[kB - 1];
+        __syncthreads();
+        carry += tot;
+    }
+    if (threadIdx.x == 0) start[n] = carry;
+}
+
+__global__ void k_scan_add(int *start, int *fill, const int *sums, const Grid *g) {
+    const int n = g->ncodes;
+    const long base = (long)blockIdx.x * kScanTile;
+    if (base >= n) return;
+    const int add = sums[blockIdx.x];
+    for (int k = threadIdx.x; k < kScanTile; k += blockDim.x) {
+        const long idx = base + k;
+        if (idx < n) {
+            const int v = start[idx] + add;
+            start[idx] = v;
+            fill[idx] = v;
+        }
+    }
+}
+
+__global__ void k_fill(int n, const int *key, int *fill, int *items) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int slot = atomicAdd(&fill[key[i]], 1);
+        items[slot] = i;
+    }
+}
+
+// Deterministic order inside each cell: ascending caller index.
+__global__ void k_cell_sort(const int *start, int *items, const int *perm, const Grid *g) {
+    const int n = g->ncodes;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        const int b = start[c], e = start[c + 1];
+        for (int a = b + 1; a < e; ++a) {
+            const int v = items[a];
+            const int kv = perm[v];
+            int t = a - 1;
+            while (t >= b && perm[items[t]] > kv) {
+                items[t + 1] = items[t];
+                --t;
+            }
+            items[t + 1] = v;
+        }
+    }
+}
+
+// Re-sort: new index p takes old particle src[p] = items[p].
+__global__ void k_make_dst(int n, const int *items, int *dst) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) dst[items[p]] = p;
+}
+
+__global__ void k_permute(Particles P, Particles A, const Ctl *ctl, const int *items, const int *dst) {
+    const int n = P.n, cap = P.cap, cur = ctl->cur, nxt = cur ^ 1;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const int q = items[p];
+        reinterpret_cast<D4 *>(P.pos[nxt])[p] = ld4(P.pos[cur], q);
+        for (int d = 0; d < 3; ++d) {
+            P.vel[nxt][d * cap + p] = P.vel[cur][d * cap + q];
+            P.omg[nxt][d * cap + p] = P.omg[cur][d * cap + q];
+            A.force[d * cap + p] = P.force[d * cap + q];
+            A.torque[d * cap + p] = P.torque[d * cap + q];
+            if (P.ext) A.ext[d * cap + p] = P.ext[d * cap + q];
+        }
+        A.mI[p] = P.mI[q];
+        A.mat[p] = P.mat[q];
+        A.fix[p] = P.fix[q];
+        A.cstate[p] = P.cstate[q];
+        for (int k = 0; k < P.mc; ++k) {
+            const int t = P.tidx[(long)k * cap + q];
+            A.tidx[(long)k * cap + p] = (t >= 0 && t < n) ? dst[t] : t;
+        }
+        for (long k = 0; k < 3L * P.mc; ++k) A.th[k * cap + p] = P.th[k * cap + q];
+        for (long k = 0; k < 3L * P.mw; ++k) A.sw[k * cap + p] = P.sw[k * cap + q];
+        const int orig = P.perm[q];
+        A.perm[p] = orig;
+        P.rank[orig] = p;
+    }
+}
+
+__global__ void k_identity(int n, int *items) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) items[p] = p;
+}
+
+__global__ void k_flip(Ctl *ctl) {
+    if (threadIdx.x == 0) ctl->cur ^= 1;
+}
+
+__global__ void __launch_bounds__(128) k_list(Particles P, NbrList L, Ctl *ctl, const Grid *g, const int *start,
+                                              const int *items, double delta, double skin) {
+    const Grid G = *g;
+    const int cur = ctl->cur, cap = P.cap;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int count = 0;
+    if (i < P.n) {
+        const double4 *pc = P.pos[cur];
+        const D4 pi = ld4(pc, i);
+        int c[3];
+        cell_of(G, pi, c);
+        int cand[kMaxCand];
+        int ckey[kMaxCand];
+        for (int dz = -1; dz <= 1; ++dz) {
+            const int z = c[2] + dz;
+            if (z < 0 || z >= G.dims[2]) continue;
+            for (int dy = -1; dy <= 1; ++dy) {
+                const int y = c[1] + dy;
+                if (y < 0 || y >= G.dims[1]) continue;
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const int x = c[0] + dx;
+                    if (x < 0 || x >= G.dims[0]) continue;
+                    const int key = cell_key(G, x, y, z);
+                    const int e = start[key + 1];
+                    for (int s = start[key]; s < e; ++s) {
+                        const int j = items[s];
+                        if (j == i) continue;
+                        const D4 pj = ld4(pc, j);
+                        const double px = pi.x - pj.x, py = pi.y - pj.y, pz = pi.z - pj.z;
+                        const double r2 = px * px + py * py + pz * pz;
+                        const double cut = delta > 0.0 ? delta : pi.w + pj.w + skin;
+                        if (r2 <= cut * cut) {
+                            if (count < kMaxCand) {
+                                // insertion by caller index
+                                const int kj = P.perm[j];
+                                int t = count - 1;
+                                while (t >= 0 && ckey[t] > kj) {
+                                    ckey[t + 1] = ckey[t];
+                                    cand[t + 1] = cand[t];
+                                    --t;
+                                }
+                                ckey[t + 1] = kj;
+                                cand[t + 1] = j;
+                            }
+                            ++count;
+                        }
+                    }
+                }
+            }
+        }
+        const int keep = count < L.maxnb ? count : L.maxnb;
+        for (int k = 0; k < keep; ++k) L.idx[(long)k * cap + i] = cand[k];
+        L.nn[i] = keep;
+    }
+    // block max of the list length
+    __shared__ int smax;
+    if (threadIdx.x == 0) smax = 0;
+    __syncthreads();
+    atomicMax(&smax, count);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        atomicMax(&ctl->max_nbr, smax);
+        if (smax > L.maxnb) atomicOr(&ctl->status, DEM_ERR_NEIGHBOR_OVERFLOW);
+    }
+}
+
+__global__ void k_build_begin(Ctl *ctl) {
+    if (threadIdx.x == 0) ctl->max_nbr = 0;
+}
+
+__global__ void k_build_end(Ctl *ctl) {
+    if (threadIdx.x == 0) {
+        ctl->disp = 0.0;
+        ctl->rebuilds += 1;
+    }
+}
+
+}  // namespace
+
+void launch_build(const Particles &P, Particles &alt, const NbrList &L, BuildBuffers &B, Ctl *ctl, double delta,
+                  double skin, bool resort, bool check_run, cudaStream_t s) {
+    (void)check_run;
+    const int n = P.n;
+    const int gs = 148 * 8;
+    const int tiles = (B.cell_cap + kScanTile) / kScanTile;
+    k_build_begin<<<1, 32, 0, s>>>(ctl);
+    k_bbox_init<<<1, 32, 0, s>>>(B.bbox);
+    k_bbox<<<gs, kB, 0, s>>>(P, ctl, B.bbox);
+    k_grid<<<1, 32, 0, s>>>(B.bbox, B.grid, B.cell_cap, delta, skin);
+    k_zero<<<gs, kB, 0, s>>>(B.cell_start, B.grid);
+    k_count<<<gs, kB, 0, s>>>(P, ctl, B.grid, B.key, B.cell_start);
+    // cell_start holds counts now; scan into cell_fill (as start) then swap roles
+    k_scan_tiles<<<tiles, kB, 0, s>>>(B.cell_start, B.cell_fill, B.block_sums, B.grid);
+    k_scan_sums<<<1, kB, 0, s>>>(B.block_sums, B.grid, B.cell_fill);
+    k_scan_add<<<tiles, kB, 0, s>>>(B.cell_fill, B.cell_start, B.block_sums, B.grid);
+    // now cell_fill = exclusive start (with [ncodes] = n), cell_start = running cursor
+    k_fill<<<gs, kB, 0, s>>>(n, B.key, B.cell_start, B.cell_items);
+    k_cell_sort<<<gs, kB, 0, s>>>(B.cell_fill, B.cell_items, P.perm, B.grid);
+    if (resort) {
+        k_make_dst<<<gs, kB, 0, s>>>(n, B.cell_items, B.dst);
+        k_permute<<<gs, kB, 0, s>>>(P, alt, ctl, B.cell_items, B.dst);
+        const size_t cap = (size_t)P.cap;
+        cudaMemcpyAsync(P.force, alt.force, 3 * cap * sizeof(double), cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(P.torque, alt.torque, 3 * cap * sizeof(double), cudaMemcpyDeviceToDevice, s);
+        if (P.ext) cudaMemcpyAsync(P.ext, alt.ext, 3 * cap * sizeof(double), cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(P.mI, alt.mI, cap * sizeof(double2), cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(P.mat, alt.mat, cap, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(P.fix, alt.fix, cap, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(P.cstate, alt.cstate, cap * sizeof(int), cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(P.tidx, alt.tidx, (size_t)P.mc * cap * sizeof(int), cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(P.th, alt.th, 3 * (size_t)P.mc * cap * sizeof(double), cudaMemcpyDeviceToDevice, s);
+        if (P.mw > 0)
+            cudaMemcpyAsync(P.sw, alt.sw, 3 * (size_t)P.mw * cap * sizeof(double), cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(P.perm, alt.perm, cap * sizeof(int), cudaMemcpyDeviceToDevice, s);
+        k_flip<<<1, 32, 0, s>>>(ctl);
+        k_identity<<<gs, kB, 0, s>>>(n, B.cell_items);
+    }
+    k_list<<<(n + 127) / 128, 128, 0, s>>>(P, L, ctl, B.grid, B.cell_fill, B.cell_items, delta, skin);
+    k_build_end<<<1, 32, 0, s>>>(ctl);
+}
+
+}  // namespace b200dem

@@ -1,0 +1,171 @@
+/*
+ * b200dem.h -- C ABI of the B200-native DEM contact step (libb200dem.so).
+ *
+ * The library replaces the Kokkos/Cabana path of CabanaDEM on one GPU: particle storage
+ * (Particles.hpp), walls (Wall.hpp), the Hertz-Mindlin force (Force.hpp), the
+ * velocity-Verlet integrator (Integrator.hpp), the Verlet neighbour list and the time loop
+ * (Solver.hpp), and the bonded-DEM force (CabanaBondedDEM_*.hpp).  Each declaration cites
+ * the reference interface it stands in for (paths relative to the reference repository).
+ *
+ * Conventions
+ *  - Every call returns an int status: 0 (DEM_OK) or DEM_ERR_* bits.  Nothing aborts or
+ *    traps; dem_last_error() returns a message for the last failure on a context.
+ *  - The library owns all device memory.  Host arrays are caller-owned and copied.
+ *  - Host arrays use the reference's layout and particle order: vectors [n][3],
+ *    tangential history [n][MaxCnts], wall history [n][MaxNoWalls]; contact partner ids
+ *    are the caller's particle indices.  Internally particles are re-ordered along a
+ *    Morton curve; that order never shows through this interface.
+ *  - One dem_ctx owns one CUDA stream; calls on it are stream-ordered, *_get and
+ *    dem_ctx_sync synchronise.  A context is used by one host thread at a time.
+ */
+#ifndef B200DEM_H
+#define B200DEM_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status bits --------------------------------------------------------------- */
+#define DEM_OK                    0
+#define DEM_ERR_INVALID           0x001 /* bad argument                                  */
+#define DEM_ERR_CUDA              0x002 /* CUDA runtime error                             */
+#define DEM_ERR_CONTACT_OVERFLOW  0x004 /* more than MaxCnts contacts (ref: OOB write)    */
+#define DEM_ERR_NEIGHBOR_OVERFLOW 0x008 /* neighbour list capacity exceeded (internal)    */
+#define DEM_ERR_NAN               0x010 /* non-finite state detected                      */
+#define DEM_ERR_TIMEOUT           0x020 /* bounded device wait gave up                    */
+#define DEM_ERR_BOND_OVERFLOW     0x040 /* more than MaxBonds bonds                       */
+#define DEM_ERR_NOMEM             0x080 /* device allocation failed                       */
+#define DEM_ERR_UNSUPPORTED       0x100 /* option not supported                           */
+
+/* ---- reference behaviours (bit set = reproduce the reference) ------------------ */
+#define DEM_Q1_VELJ_USES_UI  0x01u /* src/CabanaDEM_Force.hpp:133-137                    */
+#define DEM_Q2_ETA_T_ZERO    0x02u /* src/CabanaDEM_Force.hpp:224, :618                  */
+#define DEM_Q3_NO_PP_TORQUE  0x04u /* src/CabanaDEM_Force.hpp:324-326                    */
+#define DEM_Q4_UNIT_HISTORY  0x08u /* src/CabanaDEM_Force.hpp:310-319                    */
+#define DEM_Q5_WALL_FT_TYPO  0x10u /* src/CabanaDEM_Force.hpp:624                        */
+#define DEM_REF_COMPAT       0x1Fu
+
+/* ---- particle fields for dem_particles_set/get (Particles.hpp:99-271) ------------ */
+enum dem_field {
+    DEM_F_X = 0,        /* double [n][3]  slicePosition          */
+    DEM_F_U,            /* double [n][3]  sliceVelocity          */
+    DEM_F_OMEGA,        /* double [n][3]  sliceOmega             */
+    DEM_F_FORCE,        /* double [n][3]  sliceForce             */
+    DEM_F_TORQUE,       /* double [n][3]  sliceTorque            */
+    DEM_F_M,            /* double [n]     sliceMass              */
+    DEM_F_RHO,          /* double [n]     sliceDensity           */
+    DEM_F_RAD,          /* double [n]     sliceRadius            */
+    DEM_F_I,            /* double [n]     sliceMomentOfInertia   */
+    DEM_F_E,            /* double [n]     sliceYoungsMod         */
+    DEM_F_NU,           /* double [n]     slicePoissonsRatio     */
+    DEM_F_G,            /* double [n]     sliceShearMod          */
+    DEM_F_TNG_IDX,      /* int    [n][MaxCnts]    sliceTangentialDispIdx          */
+    DEM_F_TNG_SS_X,     /* double [n][MaxCnts]    sliceTangentialDispSSx          */
+    DEM_F_TNG_SS_Y,
+    DEM_F_TNG_SS_Z,
+    DEM_F_TNG_COUNT,    /* int    [n]             sliceTotalNoTangentialContacts  */
+    DEM_F_TNG_SW_X,     /* double [n][MaxNoWalls] sliceTangentialDispSWx          */
+    DEM_F_TNG_SW_Y,
+    DEM_F_TNG_SW_Z,
+    DEM_F_FIX,          /* uint8  [n]  DEM_FIX_* flags (boundary-condition hook)      */
+    DEM_F_EXT_FORCE,    /* double [n][3] external force added before the pair forces  */
+    DEM_F_COUNT_
+};
+#define DEM_FIX_FORCE  0x1 /* zero F after the force pass (tst_01_BDEM:19-67)           */
+#define DEM_FIX_TORQUE 0x2 /* zero torque after the force pass                          */
+
+enum dem_wall_field { DEM_W_X = 0, DEM_W_U, DEM_W_OMEGA, DEM_W_NORMAL, DEM_W_E, DEM_W_NU, DEM_W_G };
+
+enum dem_precision { DEM_FP64 = 0, DEM_MIXED = 1 };
+
+typedef struct dem_ctx dem_ctx;
+typedef struct dem_particles dem_particles;
+typedef struct dem_walls dem_walls;
+typedef struct dem_solver dem_solver;
+typedef struct dem_bonds dem_bonds;
+
+/* Force model, replaces Force(cor_pp, cor_pw, friction_pp, friction_pw)
+ * (src/CabanaDEM_Force.hpp:23-35) plus the quirk selection. */
+typedef struct dem_force_params {
+    double cor_pp, cor_pw, mu_pp, mu_pw;
+    unsigned quirks;
+} dem_force_params;
+
+/* Solver options, replaces SolverDEM's inputs (timestep) and the hard-coded neighbour
+ * settings (delta, cell_ratio; src/CabanaDEM_Solver.hpp:43-63). */
+typedef struct dem_solver_params {
+    double dt;
+    double delta;          /* > 0: uniform cutoff as the reference (3 r); 0: r_i + r_j + skin */
+    double skin;           /* Verlet skin (used when delta == 0)                              */
+    int rebuild_every_step;/* 1: rebuild before every force pass (Solver.hpp:87-88)           */
+    int precision;         /* DEM_FP64 or DEM_MIXED                                           */
+    double gravity[3];     /* body acceleration, added after the pair forces                 */
+    int max_neighbors;     /* initial neighbour-list capacity per particle (0 = 32)          */
+    int steps_per_launch;  /* fused steps per captured graph (0 = 32)                        */
+} dem_solver_params;
+
+typedef struct dem_run_stats {
+    long steps;            /* fused steps executed since creation          */
+    long rebuilds;         /* neighbour builds since creation              */
+    int max_neighbors;     /* largest list length at the last build        */
+    int neighbor_capacity; /* current per-particle capacity                */
+    int status;            /* sticky DEM_ERR_* bits seen on the device     */
+    double disp_bound;     /* displacement bound since the last build (m)  */
+} dem_run_stats;
+
+/* ---- context ------------------------------------------------------------------- */
+int dem_ctx_create(int device, dem_ctx **out);
+int dem_ctx_destroy(dem_ctx *ctx);
+int dem_ctx_sync(dem_ctx *ctx);
+const char *dem_last_error(dem_ctx *ctx);
+int dem_version(void);
+
+/* ---- particles: Particles<Mem,3,MaxCnts,MaxNoWalls>(exec, n, out) ----------------
+ * (src/CabanaDEM_Particles.hpp:22-71; template parameters become runtime capacities) */
+int dem_particles_create(dem_ctx *ctx, int n, int max_contacts, int max_walls, dem_particles **out);
+int dem_particles_destroy(dem_particles *p);
+/* slice*() + updateParticles (src/CabanaDEM_Particles.hpp:91-271): SoA upload/download.
+ * count = number of elements in `host` (e.g. 3*n for DEM_F_X). */
+int dem_particles_set(dem_particles *p, int field, const void *host, long count);
+int dem_particles_get(dem_particles *p, int field, void *host, long count);
+int dem_particles_size(dem_particles *p);
+
+/* ---- walls: Wall<Mem,3>(exec, n, out) (src/CabanaDEM_Wall.hpp:22-153) ------------- */
+int dem_walls_create(dem_ctx *ctx, int n, dem_walls **out);
+int dem_walls_destroy(dem_walls *w);
+int dem_walls_set(dem_walls *w, int field, const double *host, long count);
+
+/* ---- solver: createSolverDEM<Mem>(inputs, particles, wall, force, delta) ----------
+ * (src/CabanaDEM_Solver.hpp:129-138; ctor :32-64) */
+int dem_solver_create(dem_ctx *ctx, dem_particles *p, dem_walls *w, const dem_force_params *fp,
+                      const dem_solver_params *sp, dem_solver **out);
+int dem_solver_destroy(dem_solver *s);
+/* SolverDEM::run() body for nsteps steps (src/CabanaDEM_Solver.hpp:79-97): fused
+ * force + integration kernels, graph-captured, neighbour rebuild when the
+ * displacement bound exceeds skin/2 (or every step when rebuild_every_step). */
+int dem_solver_run(dem_solver *s, int nsteps);
+int dem_solver_stats(dem_solver *s, dem_run_stats *out);
+
+/* Reference-order phases, one launch each, for callers that drive the loop themselves:
+ * Integrator::stage1/2/3 (src/CabanaDEM_Integrator.hpp:31-102), neighbors->build
+ * (src/CabanaDEM_Solver.hpp:87-88) and computeForceParticleParticleInfiniteWall
+ * (src/CabanaDEM_Force.hpp:700-710: zero, compact contacts, pp force, wall force). */
+int dem_stage1(dem_solver *s);
+int dem_stage2(dem_solver *s);
+int dem_stage3(dem_solver *s);
+int dem_build_neighbors(dem_solver *s);
+int dem_compute_force(dem_solver *s);
+
+/* Neighbour list of the last build in caller order, CSR: offsets[n+1], idx[total]
+ * (ascending partner id).  Pass idx=NULL to get the total in *total. */
+int dem_neighbors_get(dem_solver *s, int *offsets, int *idx, long *total);
+
+/* Energy totals (no reference counterpart): out[0] translational kinetic, out[1]
+ * rotational kinetic, out[2] Hertz elastic energy of pp contacts, out[3] of wall
+ * contacts.  Fixed-order reduction, so repeated calls are bitwise identical. */
+int dem_energy(dem_solver *s, double out[4]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

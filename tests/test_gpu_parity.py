@@ -1,0 +1,188 @@
+"""GPU parity: the fused FP64 step (libb200dem.so, called through its C ABI) against the CPU
+oracle on the same seeded inputs.
+
+With the oracle's pow handling set to the device arithmetic (x^1.5 = x*sqrt(x)), FP64
+results must be bit-identical, including the contact slot layout.  Against the oracle's
+libm pow (the reference's literal arithmetic) the bar is 1e-10 relative.
+"""
+import numpy as np
+import pytest
+
+from cabanadem_b200 import api, scenarios as S
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+STATE_F = ("x", "u", "omega", "force", "torque")
+HIST_F = ("tng_idx", "tng_ss_x", "tng_ss_y", "tng_ss_z", "tng_count")
+WALL_F = ("tng_sw_x", "tng_sw_y", "tng_sw_z")
+
+
+def _assert_bitwise(got, ref, fields=STATE_F + HIST_F + WALL_F, where=""):
+    for f in fields:
+        a, b = getattr(got, f), getattr(ref, f)
+        if f.startswith("tng_sw"):
+            a, b = a[:, : b.shape[1]], b[:, : a.shape[1]]
+        if f in ("tng_idx", "tng_ss_x", "tng_ss_y", "tng_ss_z"):
+            # slots beyond the count are not part of the state
+            mask = np.arange(a.shape[1])[None, :] < ref.tng_count[:, None]
+            a, b = np.where(mask, a, 0), np.where(mask, b, 0)
+        if not np.array_equal(a, b):
+            d = np.abs(np.asarray(a, float) - np.asarray(b, float))
+            raise AssertionError("%s %s differs: max |d| = %g at %s" % (where, f, d.max(), np.unravel_index(d.argmax(), d.shape)))
+
+
+def _rel_close(got, ref, tol, fields=STATE_F):
+    for f in fields:
+        a, b = getattr(got, f), getattr(ref, f)
+        scale = max(np.abs(b).max(), 1e-300)
+        err = np.abs(a - b).max() / scale
+        assert err <= tol, (f, err)
+
+
+def _gpu_run(sc, nsteps, rebuild_every_step, chunks=1, **kw):
+    s = api.from_scenario(sc, rebuild_every_step=rebuild_every_step, **kw)
+    per = nsteps // chunks
+    for c in range(chunks):
+        s.run_steps(per if c < chunks - 1 else nsteps - per * (chunks - 1))
+    return s, s.particles.download()
+
+
+def _oracle(sc, nsteps, pow_mode=O.POW_SQRT):
+    ref = sc.state.copy()
+    st = O.run(ref, sc.walls, sc.params, sc.dt, nsteps, delta=sc.delta, skin=sc.skin, gravity=sc.gravity,
+               pow_mode=pow_mode)
+    return ref, st
+
+
+EXAMPLES = [
+    ("example01", lambda I: S.example01(I["01_elastic_normal_impact_of_two_identical_particles"])),
+    ("example02", lambda I: S.example02(I["02_elastic_normal_impact_of_particle_wall"])),
+    ("example03_cor0.4", lambda I: S.example03(I["03_normal_particle_wall_different_cor"], 0.4)),
+    ("example04_30deg", lambda I: S.example04(I["04_oblique_particle_wall_different_angles"], 30.0)),
+    ("example04_60deg", lambda I: S.example04(I["04_oblique_particle_wall_different_angles"], 60.0)),
+    ("tst03", lambda I: S.tst03(I["tst_03_multiple_particles_contacts"])),
+]
+
+
+@pytest.mark.parametrize("name,make", EXAMPLES, ids=[e[0] for e in EXAMPLES])
+@pytest.mark.parametrize("ref_mode", [True, False], ids=["rebuild_every_step", "skin"])
+def test_reference_examples_bitwise(example_inputs, name, make, ref_mode):
+    sc = make(example_inputs)
+    if not ref_mode:
+        sc.delta, sc.skin = 0.0, 0.1 * float(sc.state.rad.max())
+    n = min(sc.nsteps, 3001)
+    ref, _ = _oracle(sc, n)
+    _, got = _gpu_run(sc, n, ref_mode, chunks=3)
+    _assert_bitwise(got, ref, where=name)
+
+
+@pytest.mark.parametrize("name,make", EXAMPLES[:4], ids=[e[0] for e in EXAMPLES[:4]])
+def test_reference_examples_vs_libm_pow(example_inputs, name, make):
+    sc = make(example_inputs)
+    ref, _ = _oracle(sc, sc.nsteps, pow_mode=O.POW_LIBM)
+    _, got = _gpu_run(sc, sc.nsteps, True)
+    _rel_close(got, ref, 1e-10)
+
+
+@pytest.mark.parametrize("quirks", [S.REF_COMPAT, 0x00], ids=["ref_compat", "fixed"])
+def test_random_box_bitwise(quirks):
+    """4,096 spheres in a walled 5 cm cube, gravity, friction: 300 steps, denser start so
+    that many contacts form (positions compressed towards the box centre)."""
+    sc = S.random_box(n=4096, quirks=quirks, nsteps=300)
+    c = sc.state.x.mean(axis=0)
+    sc.state.x[:] = c + (sc.state.x - c) * 0.9       # overlapping start: many contacts at once
+    sc.state.rad[:] = 1e-3
+    ref, _ = _oracle(sc, 300)
+    s, got = _gpu_run(sc, 300, False, chunks=2)
+    assert ref.tng_count.sum() > 100
+    _assert_bitwise(got, ref, where="random_box")
+    st = s.stats()
+    assert st["rebuilds"] >= 1
+
+
+def test_unfused_phases_match_fused(example_inputs):
+    sc = S.tst03(example_inputs["tst_03_multiple_particles_contacts"])
+    steps = 400
+    _, fused = _gpu_run(sc, steps, True)
+    s = api.from_scenario(sc, rebuild_every_step=True)
+    for _ in range(steps):
+        s.integrator.stage1()
+        s.integrator.stage2()
+        s.build_neighbors()
+        api.computeForceParticleParticleInfiniteWall(s)
+        s.integrator.stage3()
+    _assert_bitwise(s.particles.download(), fused, where="unfused")
+
+
+def test_split_runs_equal_one_run():
+    sc = S.random_box(n=2048, nsteps=200)
+    _, one = _gpu_run(sc, 200, False, chunks=1)
+    _, split = _gpu_run(sc, 200, False, chunks=7)
+    _assert_bitwise(split, one, where="split")
+
+
+def test_deterministic_repeat():
+    sc = S.random_box(n=4096, nsteps=100)
+    c = sc.state.x.mean(axis=0)
+    sc.state.x[:] = c + (sc.state.x - c) * 0.55
+    _, a = _gpu_run(sc, 100, False)
+    _, b = _gpu_run(sc, 100, False)
+    _assert_bitwise(a, b, where="repeat")
+
+
+@pytest.mark.parametrize("delta", [0.0, 3e-3])
+def test_neighbor_list_matches_oracle(delta):
+    sc = S.random_box(n=4096)
+    s = api.from_scenario(sc, rebuild_every_step=delta > 0)
+    if delta > 0:
+        s.close()
+        sc.delta = delta
+        s = api.from_scenario(sc, rebuild_every_step=True)
+    s.build_neighbors()
+    off, idx = s.neighbors()
+    roff, ridx = O.neighbor_list(sc.state, delta=sc.delta, skin=sc.skin)
+    assert np.array_equal(off, roff)
+    assert np.array_equal(idx, ridx)
+
+
+def test_contact_overflow_reported():
+    """More overlapping partners than MaxCnts: the reference writes out of bounds
+    (Force.hpp:186-188); here the extra contacts are not stored and the status says so,
+    exactly as in the oracle."""
+    sc = S.random_box(n=512, max_cnts=2, nsteps=5)
+    c = sc.state.x.mean(axis=0)
+    sc.state.x[:] = c + (sc.state.x - c) * 0.3
+    ref, st = _oracle(sc, 5)
+    assert st & 0x1
+    s = api.from_scenario(sc)
+    s.run_steps(5)
+    assert s.last_status & 0x004
+    _assert_bitwise(s.particles.download(), ref, where="overflow")
+
+
+def test_energy_matches_oracle():
+    sc = S.random_box(n=4096, nsteps=50)
+    s, got = _gpu_run(sc, 50, False)
+    e = s.energy()
+    assert abs(e[0] + e[1] - O.kinetic_energy(got)) <= 1e-12 * O.kinetic_energy(got)
+    assert np.array_equal(e, s.energy())
+
+
+def test_set_get_roundtrip_after_resort():
+    sc = S.random_box(n=4096, nsteps=10)
+    s, _ = _gpu_run(sc, 10, False)
+    p = s.particles
+    x = p.get("x")
+    u = np.random.default_rng(5).normal(size=x.shape)
+    p.set("u", u)
+    assert np.array_equal(p.get("u"), u)
+    assert np.array_equal(p.get("rad"), sc.state.rad)
+
+
+def test_hcp_full_size_one_step_bitwise():
+    """Full benchmark size (2,000,000 spheres): 2 fused steps bit-identical to the oracle."""
+    sc = S.hcp_box()
+    ref, _ = _oracle(sc, 2)
+    _, got = _gpu_run(sc, 2, False)
+    _assert_bitwise(got, ref, fields=STATE_F + ("tng_count",), where="hcp")
