@@ -1,0 +1,299 @@
+#!/usr/bin/env python
+"""Throughput of the DEM contact step on one or more B200s (particle-steps/s).
+
+Workload: 2,000,000 polydisperse glass spheres (r ~ U[0.8, 1.2] mm) on a jittered
+hexagonal-close-packed lattice in a 6-wall box, gravity on, dt = 5e-8 s, 2,000 steps,
+Verlet skin 0.1 r_mean with rebuild when the displacement bound reaches skin/2
+(seeded synthetic input, `cabanadem_b200.scenarios.hcp_box`).
+
+  python bench.py [--gpus N --steps K --warmup W] [--precision fp64|mixed]
+  python bench.py --impl reference ...   # the reference algorithm on the host cores
+
+Prints one JSON line (rank 0).  `value` is device-timed (CUDA events on the library's
+stream, inputs resident in HBM); `e2e` is the same metric through the C ABI with host
+buffers (state upload + steps + state download inside the timed region);
+`roofline` is the fused step kernel's algorithmic bytes per launch over its
+CUDA-event-timed mean launch duration; `cpu_baseline` is the CPU oracle (a C++
+restatement of the reference's step, run in the reference's rebuild-every-step mode) on
+a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "particle-steps/s"
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "fused_step_fp64_hcp.md")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--n", type=int, default=2_000_000)
+    ap.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-steps", type=int, default=50)
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS_FILE) as f:
+            pk = json.load(f)
+        return float(pk["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def traffic_per_particle_step():
+    """DRAM bytes per particle-step of the fused kernel from the committed ncu summary."""
+    try:
+        for line in open(TRAFFIC_FILE):
+            if line.strip().startswith("dram_bytes_per_particle_step:"):
+                return float(line.split(":", 1)[1].split()[0])
+    except Exception:
+        pass
+    return None
+
+
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join("/tmp", "bench_clocks_%d_%d.csv" % (os.getpid(), device))
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def workload(n, seed=2):
+    from cabanadem_b200 import scenarios as S
+    return S.hcp_box(n=n, seed=seed)
+
+
+def algorithmic_bytes(sc, state, off):
+    """Per-particle-step bytes of the fused step: 168 (read x,u,omega + write x,u,omega +
+    read r, m, I, all FP64) + 4 n_nbr + 56 n_c + 48 n_wc."""
+    n = state.n
+    n_nbr = float(off[-1]) / n
+    n_c = float(state.tng_count.sum()) / n
+    w = sc.walls
+    d = (state.x[:, None, :] - w.x[None, :, :]) * w.normal[None, :, :]
+    n_wc = float(((state.rad[:, None] - d.sum(axis=2)) > 0).sum()) / n
+    b = 168.0 + 4.0 * n_nbr + 56.0 * n_c + 48.0 * n_wc
+    return b, dict(n_nbr=round(n_nbr, 4), n_contacts=round(n_c, 6), n_wall_contacts=round(n_wc, 6))
+
+
+def cpu_baseline(n, budget_s, max_steps=None):
+    """The oracle (reference algorithm: rebuild every step with delta = 3 r_max) on the
+    host cores; steps until the time budget is used."""
+    from oracle import oracle as O
+    sc = workload(n)
+    delta = 3.0 * float(sc.state.rad.max())
+    st = sc.state
+    O.run(st, sc.walls, sc.params, sc.dt, 1, delta=delta, gravity=sc.gravity)   # warm-up step
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        O.run(st, sc.walls, sc.params, sc.dt, 1, delta=delta, gravity=sc.gravity)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= budget_s or (max_steps and steps >= max_steps):
+            break
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return dict(value=n * steps / el, unit=METRIC, cores=cores, kind="port",
+                sample="%d reference steps (rebuild every step, delta = 3 r_max) of the %d-sphere workload, %.1f s"
+                % (steps, n, el))
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    n = args.n
+    budget = max(5.0, min(args.cpu_seconds, 120.0))
+    cb = cpu_baseline(n, budget, max_steps=max(1, args.steps))
+    line = {"metric": METRIC, "value": cb["value"], "unit": METRIC, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "impl": "reference", "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "hcp_box_%d: %d polydisperse spheres r~U[0.8,1.2] mm, jittered HCP, 6 walls, "
+                                   "gravity, dt 5e-8 s" % (n, n)},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    ws, rank, local = dist_env()
+    import torch
+    if ws > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    from cabanadem_b200 import api
+    from cabanadem_b200._lib import DEM_FP64, DEM_MIXED
+
+    prec = DEM_FP64 if args.precision == "fp64" else DEM_MIXED
+    sc = workload(args.n, seed=2 + rank)
+    ctx = api.Context(local)
+    solver = api.from_scenario(sc, ctx=ctx, precision=prec)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=torch.device("cuda", local))
+
+    def barrier():
+        if ws > 1:
+            torch.distributed.barrier()
+
+    clocks = ClockSampler(local)
+    solver.run_steps(max(3, args.warmup))
+    clocks.start()
+    kernel_ms = solver.profile_steps(args.profile_steps)
+    stats0 = solver.stats()
+    barrier()
+    torch.cuda.synchronize(local)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    solver.run_steps(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize(local)
+    barrier()
+    ck = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    stats1 = solver.stats()
+    if ws > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    n = args.n
+    value = ws * n * args.steps / (ms / 1e3)
+
+    # roofline of the fused step kernel
+    state = solver.particles.download()
+    off, _ = solver.neighbors()
+    b_step, occ = algorithmic_bytes(sc, state, off)
+    peak, peak_kind = hbm_peak()
+    achieved = n * b_step / (kernel_ms / 1e3) / 1e9
+    tpps = traffic_per_particle_step()
+    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "traffic": (round(tpps * n) if tpps else None),
+            "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+            "kernel": "k_step<MODE_FUSED> (fused FP64 force + integration)", "kernel_ms": round(kernel_ms, 5),
+            "bytes_per_particle_step": round(b_step, 2), **occ}
+
+    # end to end through the C ABI with host buffers
+    barrier()
+    host = sc.state.copy()
+    h2d = sum(getattr(host, f).nbytes for f in ("rad", "x", "u", "omega", "force", "torque", "m", "I", "rho", "E",
+                                                 "nu", "G", "tng_idx", "tng_ss_x", "tng_ss_y", "tng_ss_z",
+                                                 "tng_count", "tng_sw_x", "tng_sw_y", "tng_sw_z"))
+    torch.cuda.synchronize(local)
+    t0 = time.perf_counter()
+    a0 = torch.cuda.Event(enable_timing=True)
+    a1 = torch.cuda.Event(enable_timing=True)
+    a0.record(stream)
+    solver.particles.upload(host)
+    solver.run_steps(args.steps)
+    out = {f: solver.particles.get(f) for f in ("x", "u", "omega", "force", "torque")}
+    a1.record(stream)
+    a1.synchronize()
+    e2e_ms = a0.elapsed_time(a1)
+    wall_ms = (time.perf_counter() - t0) * 1e3
+    d2h = sum(v.nbytes for v in out.values())
+    if ws > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = {"value": ws * n * args.steps / (e2e_ms / 1e3), "unit": METRIC,
+           "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
+           "wall_ms": round(wall_ms, 2)}
+
+    rebuilds = stats1["rebuilds"] - stats0["rebuilds"]
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if prec == DEM_FP64 else "f64 state / f32 force",
+            "data": "synthetic",
+            "config": {"workload": "hcp_box_%d: %d polydisperse spheres r~U[0.8,1.2] mm, jittered HCP, 6 walls, "
+                                   "gravity, dt 5e-8 s, skin 0.1 r_mean" % (n, n),
+                       "precision": args.precision, "parallelism": "replicas" if ws > 1 else "single",
+                       "l2": "inputs larger than L2 (device state ~%.2f GB)" % (n * 330 / 1e9),
+                       "rebuilds_in_timed_region": rebuilds, "neighbors_per_particle": occ["n_nbr"]},
+            "roofline": roof, "e2e": e2e, "clocks": ck,
+            "gpu_launches": int(stats1["launches"] - stats0["launches"])}
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(n, args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

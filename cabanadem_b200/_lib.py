@@ -40,7 +40,8 @@ class SolverParams(C.Structure):
 
 class RunStats(C.Structure):
     _fields_ = [("steps", C.c_long), ("rebuilds", C.c_long), ("max_neighbors", C.c_int),
-                ("neighbor_capacity", C.c_int), ("status", C.c_int), ("disp_bound", C.c_double)]
+                ("neighbor_capacity", C.c_int), ("status", C.c_int), ("disp_bound", C.c_double),
+                ("launches", C.c_long)]
 
 
 class DemError(RuntimeError):
@@ -69,6 +70,8 @@ _PROTOS = {
     "dem_solver_destroy": ([_VP], C.c_int),
     "dem_solver_run": ([_VP, C.c_int], C.c_int),
     "dem_solver_stats": ([_VP, C.POINTER(RunStats)], C.c_int),
+    "dem_solver_profile": ([_VP, C.c_int, C.POINTER(C.c_double)], C.c_int),
+    "dem_ctx_stream": ([_VP], C.c_void_p),
     "dem_stage1": ([_VP], C.c_int),
     "dem_stage2": ([_VP], C.c_int),
     "dem_stage3": ([_VP], C.c_int),

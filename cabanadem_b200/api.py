@@ -61,6 +61,10 @@ class Context:
     def sync(self):
         check(lib().dem_ctx_sync(self.h), self.h, "dem_ctx_sync")
 
+    def stream_ptr(self) -> int:
+        """cudaStream_t of this context (for CUDA events on the library's stream)."""
+        return int(lib().dem_ctx_stream(self.h) or 0)
+
     def close(self):
         """Destroy the context; close every object created on it first."""
         if self.h:
@@ -238,6 +242,14 @@ class SolverDEM:
         s = _lib.RunStats()
         check(lib().dem_solver_stats(self.h, C.byref(s)), self.particles.ctx.h, "dem_solver_stats")
         return {k: getattr(s, k) for k, _ in s._fields_}
+
+    def profile_steps(self, nsteps: int) -> float:
+        """Run nsteps fused steps launched one by one between CUDA events; returns the
+        mean duration (ms) of one fused step launch."""
+        ms = C.c_double(0.0)
+        check(lib().dem_solver_profile(self.h, int(nsteps), C.byref(ms)), self.particles.ctx.h,
+              "dem_solver_profile", allow=_lib.DEM_ERR_CONTACT_OVERFLOW)
+        return ms.value
 
     def build_neighbors(self):
         check(lib().dem_build_neighbors(self.h), self.particles.ctx.h, "dem_build_neighbors")

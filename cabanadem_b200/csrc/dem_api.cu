@@ -63,6 +63,8 @@ struct dem_solver {
     int graph_steps = 0;
     long graph_version = -1;
     long version = 0;   // bumps when anything baked into the graph changes
+    long launches = 0;  // kernels launched (graph nodes counted per replay)
+    long graph_nodes = 0;
 };
 
 namespace {
@@ -263,6 +265,8 @@ extern "C" int dem_ctx_sync(dem_ctx *ctx) {
 }
 
 extern "C" const char *dem_last_error(dem_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+extern "C" void *dem_ctx_stream(dem_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
 
 // ---- particles ----------------------------------------------------------------------
 static cudaError_t alloc_particles(Particles &P, int n, int mc, int mw, bool pingpong) {
@@ -628,9 +632,11 @@ int alloc_lists(dem_solver *s, int maxnb) {
     dem_ctx *ctx = s->ctx;
     cudaFree(s->L.nn);
     cudaFree(s->L.idx);
+    cudaFree(s->L.defer);
     s->L.maxnb = maxnb;
     CK(dalloc(&s->L.nn, s->p->P.cap));
     CK(dalloc(&s->L.idx, (size_t)maxnb * s->p->P.cap));
+    CK(dalloc(&s->L.defer, s->p->P.cap));
     CK(cudaMemsetAsync(s->L.nn, 0, sizeof(int) * s->p->P.cap, ctx->stream));
     s->version++;
     s->built = false;
@@ -650,12 +656,16 @@ __global__ void k_clear_status(Ctl *ctl, int bits) {
 
 bool ref_mode(const dem_solver *s) { return s->sp.rebuild_every_step != 0; }
 
+// kernels issued by one launch_build (see dem_nbr.cu)
+long build_kernel_count(bool resort) { return 13 + (resort ? 4 : 0); }
+
 // Build with overflow handling (host-driven; re-sorts into Morton order).
 int build_now(dem_solver *s, bool resort) {
     dem_ctx *ctx = s->ctx;
     for (int attempt = 0; attempt < 8; ++attempt) {
         launch_build(s->p->P, s->p->alt, s->L, s->B, s->p->ctl, s->sp.delta, s->sp.skin, resort, false,
                      ctx->stream);
+        s->launches += build_kernel_count(resort);
         CK(cudaGetLastError());
         Ctl c = read_ctl(s);
         CK(cudaGetLastError());
@@ -688,6 +698,7 @@ int capture_graph(dem_solver *s, int steps) {
         launch_step(s->p->P, s->L, s->p->ctl, s->fc, s->d_pp, s->d_pw, s->d_walls, MODE_FUSED, ctx->stream);
     }
     CK(cudaStreamEndCapture(ctx->stream, &g));
+    s->graph_nodes = (long)steps * (kernels_per_step() + (ref_mode(s) ? build_kernel_count(false) : 0));
     cudaError_t e = cudaGraphInstantiate(&s->graph, g, 0);
     cudaGraphDestroy(g);
     CK(e);
@@ -750,7 +761,7 @@ extern "C" int dem_solver_destroy(dem_solver *s) {
     cudaStreamSynchronize(s->ctx->stream);
     if (s->graph) cudaGraphExecDestroy(s->graph);
     cudaFree(s->d_pp); cudaFree(s->d_pw); cudaFree(s->d_walls);
-    cudaFree(s->L.nn); cudaFree(s->L.idx);
+    cudaFree(s->L.nn); cudaFree(s->L.idx); cudaFree(s->L.defer);
     BuildBuffers &B = s->B;
     cudaFree(B.grid); cudaFree(B.key); cudaFree(B.cell_start); cudaFree(B.cell_fill); cudaFree(B.cell_items);
     cudaFree(B.block_sums); cudaFree(B.bbox); cudaFree(B.src); cudaFree(B.dst);
@@ -774,6 +785,7 @@ extern "C" int dem_solver_run(dem_solver *s, int nsteps) {
     else half_skin = s->sp.skin / 2.0;
     k_run_begin<<<1, 32, 0, st>>>(s->p->ctl, nsteps, half_skin);
     launch_prologue(s->p->P, s->p->ctl, s->fc, st);
+    s->launches += 2;
     CK(cudaGetLastError());
     const int chunk = s->sp.steps_per_launch;
     if (ref_mode(s)) {
@@ -787,6 +799,7 @@ extern "C" int dem_solver_run(dem_solver *s, int nsteps) {
             int done_before = -1;
             for (;;) {
                 CK(cudaGraphLaunch(s->graph, st));
+                s->launches += s->graph_nodes;
                 c = read_ctl(s);
                 if (c.steps_done >= c.target || (c.status & DEM_ERR_NEIGHBOR_OVERFLOW) || c.steps_done == done_before)
                     break;
@@ -814,6 +827,7 @@ extern "C" int dem_solver_run(dem_solver *s, int nsteps) {
                 if (e) return e;
             }
             CK(cudaGraphLaunch(s->graph, st));
+            s->launches += s->graph_nodes;
             Ctl c = read_ctl(s);
             CK(cudaGetLastError());
             if (c.steps_done >= c.target) break;
@@ -838,7 +852,60 @@ extern "C" int dem_solver_stats(dem_solver *s, dem_run_stats *out) {
     out->neighbor_capacity = s->L.maxnb;
     out->status = c.status;
     out->disp_bound = c.disp;
+    out->launches = s->launches;
     return DEM_OK;
+}
+
+extern "C" int dem_solver_profile(dem_solver *s, int nsteps, double *kernel_ms) {
+    if (!s || !kernel_ms) return DEM_ERR_INVALID;
+    *kernel_ms = 0.0;
+    if (nsteps <= 0) return DEM_OK;
+    dem_ctx *ctx = s->ctx;
+    if (ref_mode(s)) return fail(ctx, DEM_ERR_UNSUPPORTED, "dem_solver_profile: skin mode only");
+    if (s->p->mat_dirty || (s->p->P.ext != nullptr) != (s->fc.has_ext != 0)) {
+        int st = prepare(s);
+        if (st) return st;
+    }
+    cudaStream_t st = ctx->stream;
+    const double half_skin = s->sp.delta > 0.0 ? std::max(0.0, s->sp.delta - 2.0 * s->p->rmax) / 2.0 : s->sp.skin / 2.0;
+    k_run_begin<<<1, 32, 0, st>>>(s->p->ctl, nsteps, half_skin);
+    launch_prologue(s->p->P, s->p->ctl, s->fc, st);
+    s->launches += 2;
+    if (!s->built || s->p->dirty) {
+        int e = build_now(s, true);
+        if (e) return e;
+    }
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    double sum = 0.0;
+    long timed = 0;
+    int done = 0;
+    for (int guard = 0; guard < 4 * (nsteps + 4); ++guard) {
+        CK(cudaEventRecord(e0, st));
+        launch_step(s->p->P, s->L, s->p->ctl, s->fc, s->d_pp, s->d_pw, s->d_walls, MODE_FUSED, st);
+        CK(cudaEventRecord(e1, st));
+        s->launches += kernels_per_step();
+        CK(cudaEventSynchronize(e1));
+        const Ctl c = read_ctl(s);
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        if (c.steps_done > done) {   // the launch did a step (a stale list makes it a no-op)
+            sum += ms;
+            ++timed;
+            done = c.steps_done;
+        }
+        if (c.steps_done >= c.target) break;
+        if (!(c.disp < c.half_skin)) {
+            int e = build_now(s, true);
+            if (e) return e;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *kernel_ms = timed ? sum / timed : 0.0;
+    Ctl c = read_ctl(s);
+    return c.status & (DEM_ERR_CONTACT_OVERFLOW | DEM_ERR_NAN);
 }
 
 extern "C" int dem_stage1(dem_solver *s) {

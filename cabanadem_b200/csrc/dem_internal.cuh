@@ -33,6 +33,7 @@ struct Ctl {
     double half_skin;         // stale threshold (list invalid once disp >= half_skin)
     int status;               // sticky DEM_ERR_* bits
     int max_nbr;              // longest neighbour list seen at the last build
+    int ndefer;               // particles handed from the streaming to the contact kernel
     long long total_steps;
     long long rebuilds;
 };
@@ -83,6 +84,7 @@ struct NbrList {
     int *nn;     // [cap] list length
     int *idx;    // [maxnb][cap] sorted indices, ascending caller id
     int maxnb;
+    int *defer;  // [cap] particles deferred to the contact kernel in the current step
 };
 
 struct Grid {                 // computed on the device at every build
@@ -108,7 +110,10 @@ struct BuildBuffers {
 };
 
 // ---- launchers (dem_step.cu) ------------------------------------------------------
+// MODE_FUSED launches the streaming kernel and the contact kernel (kernels_per_step());
+// MODE_FORCE_ONLY one force-only kernel.
 enum StepMode { MODE_FUSED = 0, MODE_FORCE_ONLY = 1 };
+int kernels_per_step();
 void launch_prologue(const Particles &P, Ctl *ctl, const ForceConsts &fc, cudaStream_t s);
 void launch_step(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
                  const PairConst *pw, const WallGeom *walls, int mode, cudaStream_t s);

@@ -111,6 +111,7 @@ typedef struct dem_run_stats {
     int neighbor_capacity; /* current per-particle capacity                */
     int status;            /* sticky DEM_ERR_* bits seen on the device     */
     double disp_bound;     /* displacement bound since the last build (m)  */
+    long launches;         /* kernels launched by this solver (graph nodes counted per replay) */
 } dem_run_stats;
 
 /* ---- context ------------------------------------------------------------------- */
@@ -119,6 +120,9 @@ int dem_ctx_destroy(dem_ctx *ctx);
 int dem_ctx_sync(dem_ctx *ctx);
 const char *dem_last_error(dem_ctx *ctx);
 int dem_version(void);
+/* The context's CUDA stream (cudaStream_t), so that callers can order their own work
+ * after the library's and time it with CUDA events (no reference counterpart). */
+void *dem_ctx_stream(dem_ctx *ctx);
 
 /* ---- particles: Particles<Mem,3,MaxCnts,MaxNoWalls>(exec, n, out) ----------------
  * (src/CabanaDEM_Particles.hpp:22-71; template parameters become runtime capacities) */
@@ -145,6 +149,10 @@ int dem_solver_destroy(dem_solver *s);
  * displacement bound exceeds skin/2 (or every step when rebuild_every_step). */
 int dem_solver_run(dem_solver *s, int nsteps);
 int dem_solver_stats(dem_solver *s, dem_run_stats *out);
+/* Same steps as dem_solver_run, but each fused step kernel is launched on its own between
+ * two CUDA events; *kernel_ms receives the mean duration of one fused step launch
+ * (rebuilds excluded).  For roofline measurement; no reference counterpart. */
+int dem_solver_profile(dem_solver *s, int nsteps, double *kernel_ms);
 
 /* Reference-order phases, one launch each, for callers that drive the loop themselves:
  * Integrator::stage1/2/3 (src/CabanaDEM_Integrator.hpp:31-102), neighbors->build
