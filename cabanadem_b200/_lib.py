@@ -79,7 +79,9 @@ _PROTOS = {
     "dem_compute_force": ([_VP], C.c_int),
     "dem_neighbors_get": ([_VP, _VP, _VP, C.POINTER(C.c_long)], C.c_int),
     "dem_energy": ([_VP, C.POINTER(C.c_double)], C.c_int),
+    "dem_neighbor_list_noalloc": ([_VP, _VP, C.c_int, C.c_double, C.c_double, C.c_int, _VP, _VP, _VP], C.c_int),
 }
+NOALLOC_MAX_PARTICLES = 32768
 
 
 def exported_symbols():

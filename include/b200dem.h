@@ -168,6 +168,29 @@ int dem_compute_force(dem_solver *s);
  * (ascending partner id).  Pass idx=NULL to get the total in *total. */
 int dem_neighbors_get(dem_solver *s, int *offsets, int *idx, long *total);
 
+/* ---- neighbour list without allocation ---------------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device memory at the
+ * point where they need a neighbour list: code whose device memory belongs to another
+ * allocator (a framework's caching pool, a budget fixed up front), code in a time loop that
+ * must not stall the GPU (cudaMalloc and cudaFree can synchronise the device), and code that
+ * may not call an allocation API at all.  Builds the list dem_build_neighbors builds, for
+ * particles held in the caller's device arrays, with its scratch taken from a fixed array
+ * inside the library (about 2.4 MB on every GPU that loads it, held until the process exits).
+ *   x[n][3], rad[n]               device inputs: positions and radii
+ *   delta > 0: uniform cutoff; otherwise cutoff r_i + r_j + skin
+ *   nn[n], idx[max_neighbors][n]  device outputs: list length, partner indices in ascending
+ *                                 order, slot-major (partner k of particle i at idx[k*n + i])
+ *   stream                        cudaStream_t (NULL: default stream); synchronised on return
+ * Returns DEM_ERR_INVALID when n > DEM_NOALLOC_MAX_PARTICLES and DEM_ERR_NEIGHBOR_OVERFLOW when
+ * a particle has more than max_neighbors partners (its list is cut at max_neighbors).
+ * All calls share the scratch array and it keeps the last call's contents: calls that could
+ * overlap on the GPU race and must be ordered by the caller.  The first call on a device looks
+ * up the array's address (with that device current); make that call before any stream
+ * capture. */
+#define DEM_NOALLOC_MAX_PARTICLES 32768
+int dem_neighbor_list_noalloc(const double *x, const double *rad, int n, double delta, double skin,
+                              int max_neighbors, int *nn, int *idx, void *stream);
+
 /* Energy totals (no reference counterpart): out[0] translational kinetic, out[1]
  * rotational kinetic, out[2] Hertz elastic energy of pp contacts, out[3] of wall
  * contacts.  Fixed-order reduction, so repeated calls are bitwise identical. */
