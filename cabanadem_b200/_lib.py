@@ -38,6 +38,15 @@ class SolverParams(C.Structure):
                 ("steps_per_launch", C.c_int)]
 
 
+class BondParams(C.Structure):
+    _fields_ = [("quirks", C.c_uint), ("beta", C.c_double), ("radius_factor", C.c_double), ("kn", C.c_double),
+                ("kt", C.c_double), ("break_strain", C.c_double)]
+
+
+BFIELD = {name: k for k, name in enumerate(
+    ["idx", "init_len", "count", "ft_x", "ft_y", "ft_z", "mn_x", "mn_y", "mn_z", "mt_x", "mt_y", "mt_z", "broken"])}
+
+
 class RunStats(C.Structure):
     _fields_ = [("steps", C.c_long), ("rebuilds", C.c_long), ("max_neighbors", C.c_int),
                 ("neighbor_capacity", C.c_int), ("status", C.c_int), ("disp_bound", C.c_double),
@@ -79,6 +88,12 @@ _PROTOS = {
     "dem_compute_force": ([_VP], C.c_int),
     "dem_neighbors_get": ([_VP, _VP, _VP, C.POINTER(C.c_long)], C.c_int),
     "dem_energy": ([_VP, C.POINTER(C.c_double)], C.c_int),
+    "dem_bonds_create": ([_VP, C.c_int, C.POINTER(BondParams), C.POINTER(_VP)], C.c_int),
+    "dem_bonds_destroy": ([_VP], C.c_int),
+    "dem_bonds_setup": ([_VP, C.c_double, C.c_double], C.c_int),
+    "dem_bonds_get": ([_VP, C.c_int, _VP, C.c_long], C.c_int),
+    "dem_bonds_broken": ([_VP, C.POINTER(C.c_long)], C.c_int),
+    "dem_bonded_run": ([_VP, C.c_int], C.c_int),
     "dem_neighbor_list_noalloc": ([_VP, _VP, C.c_int, C.c_double, C.c_double, C.c_int, _VP, _VP, _VP], C.c_int),
 }
 NOALLOC_MAX_PARTICLES = 32768

@@ -330,3 +330,75 @@ def from_scenario(sc, ctx: Context | None = None, rebuild_every_step=False, prec
                   gravity=sc.gravity, precision=precision, steps_per_launch=steps_per_launch,
                   max_neighbors=max_neighbors)
     return s
+
+
+class Bonds:
+    """ParticlesBondedDEM's bond slots (src/CabanaBondedDEM_Particles.hpp:29-293) on a solver's
+    particles, with setupBonds (:86-171) and the bonded loop (tst_01_BDEM:295-306)."""
+
+    def __init__(self, solver: SolverDEM, max_bonds: int, quirks=0x07, beta=0.1, radius_factor=1.0, kn=0.0,
+                 kt=0.0, break_strain=0.0):
+        self.solver = solver
+        self.max_bonds = int(max_bonds)
+        bp = _lib.BondParams(int(quirks), float(beta), float(radius_factor), float(kn), float(kt),
+                             float(break_strain))
+        h = C.c_void_p()
+        check(lib().dem_bonds_create(solver.h, self.max_bonds, C.byref(bp), C.byref(h)), solver.particles.ctx.h,
+              "dem_bonds_create")
+        self.h = h
+
+    def setupBonds(self, factor=3.0, search_cutoff=0.0):
+        check(lib().dem_bonds_setup(self.h, float(factor), float(search_cutoff)), self.solver.particles.ctx.h,
+              "dem_bonds_setup")
+
+    def get(self, field):
+        n = self.solver.particles.n
+        if field == "count":
+            a = np.empty(n, dtype=np.int32)
+        elif field == "idx":
+            a = np.empty((n, self.max_bonds), dtype=np.int32)
+        elif field == "broken":
+            a = np.empty((n, self.max_bonds), dtype=np.uint8)
+        else:
+            a = np.empty((n, self.max_bonds))
+        check(lib().dem_bonds_get(self.h, _lib.BFIELD[field], a.ctypes.data, a.size), self.solver.particles.ctx.h,
+              "dem_bonds_get " + field)
+        return a
+
+    def broken(self) -> int:
+        """Broken bond ends (each bond of a symmetric pair is counted at both particles)."""
+        c = C.c_long(0)
+        check(lib().dem_bonds_broken(self.h, C.byref(c)), self.solver.particles.ctx.h, "dem_bonds_broken")
+        return c.value
+
+    def run_steps(self, nsteps: int):
+        return check(lib().dem_bonded_run(self.h, int(nsteps)), self.solver.particles.ctx.h, "dem_bonded_run")
+
+    def close(self):
+        if self.h:
+            lib().dem_bonds_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def bonded_from_case(case: dict, ctx: Context | None = None, steps_per_launch=0):
+    """Particles + SolverDEM + Bonds on the device for a scenarios.bonded_bar /
+    bdem_two_particles case (bonds set up)."""
+    st = case["state"]
+    p = Particles(st.n, max(st.max_cnts, 1), 0, ctx=ctx)
+    p.upload(st)
+    if case.get("ext_force") is not None:
+        p.set("ext_force", case["ext_force"])
+    if case.get("fix_flags") is not None:
+        p.set("fix", case["fix_flags"])
+    s = SolverDEM(p, None, Force(1.0, 1.0, 0.0, 0.0), case["dt"], skin=0.0, steps_per_launch=steps_per_launch)
+    bp = case["bparams"]
+    b = Bonds(s, case["bonds"].max_bonds, quirks=bp["quirks"], beta=bp["beta"], radius_factor=bp["radius_factor"],
+              kn=bp["kn"], kt=bp["kt"], break_strain=bp["break_strain"])
+    b.setupBonds(case["bond_factor"], case["search_cutoff"])
+    return b

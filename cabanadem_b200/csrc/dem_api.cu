@@ -35,6 +35,7 @@ struct dem_particles {
     double rmax = 0.0;
     bool dirty = true;       // state changed through set(): list must be rebuilt
     bool mat_dirty = true;   // E, nu, G changed: tables must be rebuilt
+    bool has_bonds = false;  // bond slots hold sorted indices: no re-sort from now on
     std::vector<uint8_t> mat;   // caller order
     std::vector<std::tuple<double, double, double>> mats;
 };
@@ -65,6 +66,17 @@ struct dem_solver {
     long version = 0;   // bumps when anything baked into the graph changes
     long launches = 0;  // kernels launched (graph nodes counted per replay)
     long graph_nodes = 0;
+};
+
+struct dem_bonds {
+    dem_solver *s = nullptr;
+    Bonds B{};
+    BondConsts bc{};
+    unsigned long long *d_count = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+    long graph_version = -1;
+    bool set_up = false;
 };
 
 namespace {
@@ -164,6 +176,15 @@ __global__ void k_scatter_u8(const uint8_t *src, uint8_t *dst, int n, const int 
 }
 __global__ void k_gather_u8(const uint8_t *src, uint8_t *dst, int n, const int *rank) {
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) dst[c] = src[rank[c]];
+}
+__global__ void k_gather_u8n(const uint8_t *src, uint8_t *dst, int n, int ncomp, int cap, const int *rank) {
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < (long)n * ncomp; t += (long)gridDim.x * blockDim.x) {
+        const int c = (int)(t / ncomp), k = (int)(t % ncomp);
+        dst[t] = src[(long)k * cap + rank[c]];
+    }
+}
+__global__ void k_fill_i(int *a, long count, int v) {
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < count; t += (long)gridDim.x * blockDim.x) a[t] = v;
 }
 __global__ void k_scatter_count(const int *src, int *cstate, int n, const int *rank) {
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
@@ -623,6 +644,7 @@ int prepare(dem_solver *s) {
     fc.nwall = nw;
     fc.has_ext = p->P.ext ? 1 : 0;
     fc.has_fix = 1;
+    fc.mixed = s->sp.precision == DEM_MIXED ? 1 : 0;
     CK(cudaStreamSynchronize(st));
     s->version++;
     return DEM_OK;
@@ -660,11 +682,14 @@ bool ref_mode(const dem_solver *s) { return s->sp.rebuild_every_step != 0; }
 long build_kernel_count(bool resort) { return 13 + (resort ? 4 : 0); }
 
 // Build with overflow handling (host-driven; re-sorts into Morton order).
-int build_now(dem_solver *s, bool resort) {
+int build_with(dem_solver *s, bool resort, double delta, double skin);
+int build_now(dem_solver *s, bool resort) { return build_with(s, resort, s->sp.delta, s->sp.skin); }
+
+int build_with(dem_solver *s, bool resort, double delta, double skin) {
     dem_ctx *ctx = s->ctx;
+    if (s->p->has_bonds) resort = false;
     for (int attempt = 0; attempt < 8; ++attempt) {
-        launch_build(s->p->P, s->p->alt, s->L, s->B, s->p->ctl, s->sp.delta, s->sp.skin, resort, false,
-                     ctx->stream);
+        launch_build(s->p->P, s->p->alt, s->L, s->B, s->p->ctl, delta, skin, resort, false, ctx->stream);
         s->launches += build_kernel_count(resort);
         CK(cudaGetLastError());
         Ctl c = read_ctl(s);
@@ -985,4 +1010,172 @@ extern "C" int dem_energy(dem_solver *s, double out[4]) {
     CK(cudaMemcpyAsync(out, s->d_eout, 4 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     return DEM_OK;
+}
+
+// ---- bonded DEM ---------------------------------------------------------------------
+extern "C" int dem_bonds_create(dem_solver *s, int max_bonds, const dem_bond_params *bp, dem_bonds **out) {
+    if (!s || !bp || !out || max_bonds <= 0 || max_bonds > 64) return DEM_ERR_INVALID;
+    dem_ctx *ctx = s->ctx;
+    dem_bonds *b = new dem_bonds();
+    b->s = s;
+    const int cap = s->p->P.cap;
+    Bonds &B = b->B;
+    B.mb = max_bonds;
+    B.cap = cap;
+    cudaError_t e = cudaSuccess;
+    auto A = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
+    A(dalloc(&B.idx, (size_t)max_bonds * cap));
+    A(dalloc(&B.init_len, (size_t)max_bonds * cap));
+    A(dalloc(&B.count, cap));
+    A(dalloc(&B.hist, 9 * (size_t)max_bonds * cap));
+    A(dalloc(&B.broken, (size_t)max_bonds * cap));
+    A(dalloc(&B.E, cap));
+    A(dalloc(&B.G, cap));
+    A(dalloc(&b->d_count, 1));
+    if (e != cudaSuccess) {
+        dem_bonds_destroy(b);
+        return cuda_check(ctx, e, "dem_bonds_create");
+    }
+    cudaStream_t st = ctx->stream;
+    k_fill_i<<<kGS, kTB, 0, st>>>(B.idx, (long)max_bonds * cap, -1);
+    cudaMemsetAsync(B.init_len, 0, sizeof(double) * max_bonds * (size_t)cap, st);
+    cudaMemsetAsync(B.count, 0, sizeof(int) * cap, st);
+    cudaMemsetAsync(B.hist, 0, sizeof(double) * 9 * max_bonds * (size_t)cap, st);
+    cudaMemsetAsync(B.broken, 0, (size_t)max_bonds * cap, st);
+    b->bc.quirks = bp->quirks;
+    b->bc.beta = bp->beta;
+    b->bc.radius_factor = bp->radius_factor;
+    b->bc.kn = bp->kn;
+    b->bc.kt = bp->kt;
+    b->bc.break_strain = bp->break_strain;
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(st));
+    *out = b;
+    return DEM_OK;
+}
+
+extern "C" int dem_bonds_destroy(dem_bonds *b) {
+    if (!b) return DEM_ERR_INVALID;
+    cudaStreamSynchronize(b->s->ctx->stream);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    Bonds &B = b->B;
+    cudaFree(B.idx); cudaFree(B.init_len); cudaFree(B.count); cudaFree(B.hist); cudaFree(B.broken);
+    cudaFree(B.E); cudaFree(B.G); cudaFree(b->d_count);
+    delete b;
+    return DEM_OK;
+}
+
+extern "C" int dem_bonds_setup(dem_bonds *b, double factor, double search_cutoff) {
+    if (!b || !(factor > 0.0)) return DEM_ERR_INVALID;
+    dem_solver *s = b->s;
+    dem_ctx *ctx = s->ctx;
+    dem_particles *p = s->p;
+    if (p->mat_dirty || (p->P.ext != nullptr) != (s->fc.has_ext != 0)) {
+        int st = prepare(s);
+        if (st) return st;
+    }
+    if (!(search_cutoff > 0.0)) search_cutoff = factor * p->rmax;
+    int st = build_with(s, true, search_cutoff, 0.0);
+    if (st) return st;
+    cudaStream_t cs = ctx->stream;
+    launch_bond_setup(p->P, s->L, b->B, p->ctl, factor, cs);
+    // per-particle moduli in the (now fixed) particle order
+    double *tmp = nullptr;
+    const int n = p->P.n;
+    CK(cudaMalloc(&tmp, sizeof(double) * n));
+    CK(cudaMemcpyAsync(tmp, p->E.data(), sizeof(double) * n, cudaMemcpyHostToDevice, cs));
+    k_scatter_d<<<kGS, kTB, 0, cs>>>(tmp, b->B.E, n, 1, p->P.cap, p->P.rank);
+    CK(cudaStreamSynchronize(cs));
+    CK(cudaMemcpyAsync(tmp, p->G.data(), sizeof(double) * n, cudaMemcpyHostToDevice, cs));
+    k_scatter_d<<<kGS, kTB, 0, cs>>>(tmp, b->B.G, n, 1, p->P.cap, p->P.rank);
+    CK(cudaStreamSynchronize(cs));
+    cudaFree(tmp);
+    CK(cudaGetLastError());
+    p->has_bonds = true;
+    s->built = false;   // the list was built with the bond search cutoff
+    b->set_up = true;
+    Ctl c = read_ctl(s);
+    return c.status & DEM_ERR_BOND_OVERFLOW;
+}
+
+extern "C" int dem_bonds_get(dem_bonds *b, int field, void *host, long count) {
+    if (!b || !host) return DEM_ERR_INVALID;
+    dem_solver *s = b->s;
+    dem_ctx *ctx = s->ctx;
+    const Particles &P = s->p->P;
+    const Bonds &B = b->B;
+    const int n = P.n, mb = B.mb;
+    const long per = (field == DEM_B_COUNT) ? n : (long)n * mb;
+    const int es = (field == DEM_B_IDX || field == DEM_B_COUNT) ? 4 : (field == DEM_B_BROKEN ? 1 : 8);
+    if (field < DEM_B_IDX || field > DEM_B_BROKEN || count != per)
+        return fail(ctx, DEM_ERR_INVALID, "dem_bonds_get: unknown field or wrong element count");
+    cudaStream_t st = ctx->stream;
+    void *tmp = nullptr;
+    CK(cudaMalloc(&tmp, (size_t)per * es));
+    switch (field) {
+        case DEM_B_IDX: k_gather_i<<<kGS, kTB, 0, st>>>(B.idx, (int *)tmp, n, mb, P.cap, P.rank, P.perm, 1); break;
+        case DEM_B_INIT_LEN: k_gather_d<<<kGS, kTB, 0, st>>>(B.init_len, (double *)tmp, n, mb, P.cap, P.rank); break;
+        case DEM_B_COUNT: k_gather_i<<<kGS, kTB, 0, st>>>(B.count, (int *)tmp, n, 1, P.cap, P.rank, P.perm, 0); break;
+        case DEM_B_BROKEN: k_gather_u8n<<<kGS, kTB, 0, st>>>(B.broken, (uint8_t *)tmp, n, mb, P.cap, P.rank); break;
+        default:
+            k_gather_d<<<kGS, kTB, 0, st>>>(B.hist + (long)(field - DEM_B_FT_X) * mb * P.cap, (double *)tmp, n, mb,
+                                           P.cap, P.rank);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(host, tmp, (size_t)per * es, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(tmp);
+    CK(e);
+    return DEM_OK;
+}
+
+extern "C" int dem_bonds_broken(dem_bonds *b, long *count) {
+    if (!b || !count) return DEM_ERR_INVALID;
+    dem_ctx *ctx = b->s->ctx;
+    launch_bond_broken_count(b->B, b->s->p->P.n, b->d_count, ctx->stream);
+    unsigned long long c = 0;
+    CK(cudaMemcpyAsync(&c, b->d_count, sizeof(c), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    *count = (long)c;
+    return DEM_OK;
+}
+
+extern "C" int dem_bonded_run(dem_bonds *b, int nsteps) {
+    if (!b) return DEM_ERR_INVALID;
+    if (nsteps <= 0) return DEM_OK;
+    dem_solver *s = b->s;
+    dem_ctx *ctx = s->ctx;
+    if (!b->set_up) return fail(ctx, DEM_ERR_INVALID, "dem_bonded_run: call dem_bonds_setup first");
+    if (s->p->mat_dirty || (s->p->P.ext != nullptr) != (s->fc.has_ext != 0)) {
+        int st = prepare(s);
+        if (st) return st;
+    }
+    cudaStream_t st = ctx->stream;
+    k_run_begin<<<1, 32, 0, st>>>(s->p->ctl, nsteps, 1e300);
+    launch_prologue(s->p->P, s->p->ctl, s->fc, st);
+    s->launches += 2;
+    CK(cudaGetLastError());
+    const int chunk = s->sp.steps_per_launch;
+    if (!b->graph || b->graph_version != s->version || b->graph_steps != chunk) {
+        if (b->graph) {
+            cudaGraphExecDestroy(b->graph);
+            b->graph = nullptr;
+        }
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        for (int k = 0; k < chunk; ++k) launch_bond_step(s->p->P, b->B, s->p->ctl, s->fc, b->bc, st);
+        CK(cudaStreamEndCapture(st, &g));
+        cudaError_t e = cudaGraphInstantiate(&b->graph, g, 0);
+        cudaGraphDestroy(g);
+        CK(e);
+        b->graph_steps = chunk;
+        b->graph_version = s->version;
+    }
+    for (int guard = 0; guard < 4 * (nsteps / chunk + 4); ++guard) {
+        CK(cudaGraphLaunch(b->graph, st));
+        s->launches += chunk;
+        Ctl c = read_ctl(s);
+        if (c.steps_done >= c.target) return c.status & (DEM_ERR_BOND_OVERFLOW | DEM_ERR_NAN);
+    }
+    return fail(ctx, DEM_ERR_CUDA, "dem_bonded_run made no progress");
 }

@@ -1,0 +1,294 @@
+// dem_bonded.cu -- bonded-DEM bond build and fused bond-force step on sm_100a (FP64,
+// built with --fmad=false; the expressions follow the reference's order).
+//
+//   k_bond_setup   setupBonds (src/CabanaBondedDEM_Particles.hpp:118-137): over the
+//                  neighbour list (ascending caller index) bond every j with
+//                  rij < factor * rad(i), rest length = rij
+//   k_bond_step    one bonded step in the order of tst_01_BDEM:295-306: force reset, external
+//                  force, computeBondedForce (src/CabanaBondedDEM_Force.hpp:86-341), boundary
+//                  hook, stage3, then stage1 + stage2 of the next step (ping-pong buffers)
+//
+// Bond slots are slot-major per particle: partner (sorted index), rest length, and the 9 live
+// history components (tangential force, normal and tangential moments; the reference's
+// bond_fn_* arrays are never written, :69-71).  Breakage (no reference counterpart): a bond
+// whose FP64 strain (rij - L0) / L0 exceeds the threshold is flagged and skipped from then on;
+// both ends compute the same strain bit for bit, so they break in the same step.
+#include "dem_particle.cuh"
+
+namespace b200dem {
+
+namespace {
+
+constexpr int kBondBlock = 128;
+
+__global__ void k_bond_setup(Particles P, NbrList L, Bonds B, Ctl *ctl, double factor) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n) return;
+    const int cur = ctl->cur, cap = P.cap;
+    const D4 pi = ld4(P.pos[cur], i);
+    int cnt = 0;
+    int status = 0;
+    for (int kk = 0; kk < L.nn[i]; ++kk) {
+        const int j = L.idx[(long)kk * cap + i];
+        const D4 pj = ld4(P.pos[cur], j);
+        const double px = pi.x - pj.x, py = pi.y - pj.y, pz = pi.z - pj.z;
+        const double r2ij = px * px + py * py + pz * pz;
+        const double rij = sqrt(r2ij);
+        const double bond_cond = factor * pi.w;
+        if (rij < bond_cond) {
+            if (cnt >= B.mb) {
+                status |= DEM_ERR_BOND_OVERFLOW;
+                continue;
+            }
+            B.idx[(long)cnt * cap + i] = j;
+            B.init_len[(long)cnt * cap + i] = rij;
+            ++cnt;
+        }
+    }
+    B.count[i] = cnt;
+    for (int k = cnt; k < B.mb; ++k) B.idx[(long)k * cap + i] = -1;
+    if (status) atomicOr(&ctl->status, status);
+}
+
+__global__ void __launch_bounds__(kBondBlock) k_bond_step(Particles P, Bonds B, Ctl *ctl, ForceConsts fc, BondConsts bc) {
+    const CtlSnap cs_ = read_ctl(ctl, true);
+    if (!cs_.go) return;
+    const int cur = cs_.cur, nxt = cur ^ 1;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int cap = P.cap;
+    double vmax2 = 0.0;
+    int status = 0;
+    if (i < P.n) {
+        const double4 *__restrict__ pc = P.pos[cur];
+        const double *__restrict__ vc = P.vel[cur];
+        const double *__restrict__ wc = P.omg[cur];
+        const D4 pi = ld4(pc, i);
+        double ui0 = vc[i], ui1 = vc[cap + i], ui2 = vc[2 * cap + i];
+        double wi0 = wc[i], wi1 = wc[cap + i], wi2 = wc[2 * cap + i];
+        const double2 mIi = P.mI[i];
+        double F0 = 0., F1 = 0., F2 = 0., T0 = 0., T1 = 0., T2 = 0.;
+        if (fc.has_ext) {   // applyTensileForce (tst_01_BDEM:101-111) before the bond pass
+            F0 += P.ext[i];
+            F1 += P.ext[cap + i];
+            F2 += P.ext[2 * cap + i];
+        }
+        const double Ei = B.E[i], Gi = B.G[i];
+        const int no_bonds_i = B.count[i];
+        for (int k = 0; k < no_bonds_i; k++) {
+            const long slot = (long)k * cap + i;
+            const int j = B.idx[slot];
+            if (j < 0 || B.broken[slot]) continue;
+            long hs = slot;
+            if (bc.quirks & BQ10_INDEX_BY_J) {
+                const int jc = P.perm[j];
+                if (jc >= B.mb) {
+                    status |= DEM_ERR_BOND_OVERFLOW;
+                    continue;
+                }
+                hs = (long)jc * cap + i;
+            }
+            const D4 pj = ld4(pc, j);
+            const double px = pi.x - pj.x, py = pi.y - pj.y, pz = pi.z - pj.z;
+            const double r2ij = px * px + py * py + pz * pz;
+            const double rij = sqrt(r2ij);
+            const double L0 = B.init_len[hs];
+            if (bc.break_strain > 0.0) {
+                const double strain = (rij - L0) / L0;
+                if (strain > bc.break_strain) {
+                    B.broken[slot] = 1;
+                    continue;
+                }
+            }
+            const double g_c = rij - pi.w - pj.w;
+            const double a_i = pi.w + g_c / 2.;
+            const double a_j = pj.w + g_c / 2.;
+            const double n0 = px / rij, n1 = py / rij, n2 = pz / rij;
+            const double uj0 = vc[j];
+            const double uj1 = (bc.quirks & BQ1_VELJ_USES_UI) ? ui1 : vc[cap + j];
+            const double uj2 = (bc.quirks & BQ1_VELJ_USES_UI) ? ui2 : vc[2 * cap + j];
+            const double wj0 = wc[j], wj1 = wc[cap + j], wj2 = wc[2 * cap + j];
+            const double vi0 = ui0 + (wi1 * n2 - wi2 * n1) * a_i;
+            const double vi1 = ui1 + (wi2 * n0 - wi0 * n2) * a_i;
+            const double vi2 = ui2 + (wi0 * n1 - wi1 * n0) * a_i;
+            const double vj0 = uj0 + (-wj1 * n2 + wj2 * n1) * a_j;
+            const double vj1 = uj1 + (-wj2 * n0 + wj0 * n2) * a_j;
+            const double vj2 = uj2 + (-wj0 * n1 + wj1 * n0) * a_j;
+            const double vr0 = vi0 - vj0, vr1 = vi1 - vj1, vr2 = vi2 - vj2;
+            const double vdp = vr0 * n0 + vr1 * n1 + vr2 * n2;
+            const double vn0 = vdp * n0, vn1 = vdp * n1, vn2 = vdp * n2;
+            const double vt0 = vr0 - vn0, vt1 = vr1 - vn1, vt2 = vr2 - vn2;
+            const double wr0 = wi0 - wj0, wr1 = wi1 - wj1, wr2 = wi2 - wj2;
+            const double wdp = wr0 * n0 + wr1 * n1 + wr2 * n2;
+            const double wn0 = wdp * n0, wn1 = wdp * n1, wn2 = wdp * n2;
+            const double wt0 = wr0 - wn0, wt1 = wr1 - wn1, wt2 = wr2 - wn2;
+            const double rad_sum = pi.w + pj.w;
+            const double beta_bond = bc.beta;
+            const double bond_rad = (pi.w < pj.w ? pi.w : pj.w) * bc.radius_factor;
+            const double A_bond = M_PI * (bond_rad * bond_rad);
+            const double I_bond = M_PI * ((bond_rad * bond_rad) * (bond_rad * bond_rad)) / 4.0;
+            const double I_p_bond = I_bond * 2.0;
+            double k_n_bond, k_t_bond, k_tor_bond, k_ben_bond;
+            if (bc.quirks & BQ11_HARDCODED_K) {
+                k_n_bond = Ei * A_bond / rad_sum;
+                k_t_bond = Gi * A_bond / rad_sum;
+                k_tor_bond = Gi * I_p_bond / rad_sum;
+                k_ben_bond = Ei * I_bond / rad_sum;
+            } else {
+                k_n_bond = bc.kn;
+                k_t_bond = bc.kt;
+                k_tor_bond = bc.kt * I_p_bond / A_bond;
+                k_ben_bond = bc.kn * I_bond / A_bond;
+            }
+            // normal bond force (:205-222)
+            const double overlap_n = rij - L0;
+            const double fn0 = -k_n_bond * overlap_n * n0;
+            const double fn1 = -k_n_bond * overlap_n * n1;
+            const double fn2 = -k_n_bond * overlap_n * n2;
+            double mX = (vn0 >= 0.0) ? 1.0 : -1.0;
+            double mY = (vn1 >= 0.0) ? 1.0 : -1.0;
+            double mZ = (vn2 >= 0.0) ? 1.0 : -1.0;
+            const double fd0 = fn0 + beta_bond * fabs(fn0) * mX;
+            const double fd1 = fn1 + beta_bond * fabs(fn1) * mY;
+            const double fd2 = fn2 + beta_bond * fabs(fn2) * mZ;
+            // tangential bond force (:231-260)
+            double ft0 = B.hist[(0L * B.mb) * cap + hs], ft1 = B.hist[(1L * B.mb) * cap + hs],
+                   ft2 = B.hist[(2L * B.mb) * cap + hs];
+            const double fdp = ft0 * n0 + ft1 * n1 + ft2 * n2;
+            ft0 -= fdp * n0;
+            ft1 -= fdp * n1;
+            ft2 -= fdp * n2;
+            double tmp = k_t_bond * fc.dt;
+            ft0 += -vt0 * tmp;
+            ft1 += -vt1 * tmp;
+            ft2 += -vt2 * tmp;
+            mX = (vt0 >= 0.0) ? 1.0 : -1.0;
+            mY = (vt1 >= 0.0) ? 1.0 : -1.0;
+            mZ = (vt2 >= 0.0) ? 1.0 : -1.0;
+            const double ftd0 = ft0 - beta_bond * fabs(ft0) * mX;
+            const double ftd1 = ft1 - beta_bond * fabs(ft1) * mY;
+            const double ftd2 = ft2 - beta_bond * fabs(ft2) * mZ;
+            B.hist[(0L * B.mb) * cap + hs] = ftd0;
+            B.hist[(1L * B.mb) * cap + hs] = ftd1;
+            B.hist[(2L * B.mb) * cap + hs] = ftd2;
+            // twisting moment (:267-291)
+            double tn0 = B.hist[(3L * B.mb) * cap + hs], tn1 = B.hist[(4L * B.mb) * cap + hs],
+                   tn2 = B.hist[(5L * B.mb) * cap + hs];
+            double tdp = tn0 * n0 + tn1 * n1 + tn2 * n2;
+            tn0 = tdp * n0;
+            tn1 = tdp * n1;
+            tn2 = tdp * n2;
+            tmp = k_tor_bond * fc.dt;
+            tn0 += -wn0 * tmp;
+            tn1 += -wn1 * tmp;
+            tn2 += -wn2 * tmp;
+            mX = (wn0 >= 0.0) ? 1.0 : -1.0;
+            mY = (wn1 >= 0.0) ? 1.0 : -1.0;
+            mZ = (wn2 >= 0.0) ? 1.0 : -1.0;
+            const double nd0 = tn0 - beta_bond * fabs(tn0) * mX;
+            const double nd1 = tn1 - beta_bond * fabs(tn1) * mY;
+            const double nd2 = tn2 - beta_bond * fabs(tn2) * mZ;
+            B.hist[(3L * B.mb) * cap + hs] = nd0;
+            B.hist[(4L * B.mb) * cap + hs] = nd1;
+            B.hist[(5L * B.mb) * cap + hs] = nd2;
+            // bending moment (:298-322)
+            double tt0 = B.hist[(6L * B.mb) * cap + hs], tt1 = B.hist[(7L * B.mb) * cap + hs],
+                   tt2 = B.hist[(8L * B.mb) * cap + hs];
+            tdp = tt0 * n0 + tt1 * n1 + tt2 * n2;
+            tt0 -= tdp * n0;
+            tt1 -= tdp * n1;
+            tt2 -= tdp * n2;
+            tmp = k_ben_bond * fc.dt;
+            tt0 += -wt0 * tmp;
+            tt1 += -wt1 * tmp;
+            tt2 += -wt2 * tmp;
+            mX = (wt0 >= 0.0) ? 1.0 : -1.0;
+            mY = (wt1 >= 0.0) ? 1.0 : -1.0;
+            mZ = (wt2 >= 0.0) ? 1.0 : -1.0;
+            const double td0 = tt0 - beta_bond * fabs(tt0) * mX;
+            const double td1 = tt1 - beta_bond * fabs(tt1) * mY;
+            const double td2 = tt2 - beta_bond * fabs(tt2) * mZ;
+            B.hist[(6L * B.mb) * cap + hs] = td0;
+            B.hist[(7L * B.mb) * cap + hs] = td1;
+            B.hist[(8L * B.mb) * cap + hs] = td2;
+            const double cri = rij * 1. / pi.w * 1. / (pi.w + pj.w);
+            F0 += fd0 + ftd0;
+            F1 += fd1 + ftd1;
+            F2 += fd2 + ftd2;
+            T0 += nd0 + td0 - cri * 0.0;
+            T1 += nd1 + td1 - cri * 0.0;
+            T2 += nd2 + td2 - cri * 0.0;
+        }
+        if (fc.has_gravity) {
+            F0 += mIi.x * fc.g[0];
+            F1 += mIi.x * fc.g[1];
+            F2 += mIi.x * fc.g[2];
+        }
+        if (fc.has_fix) {   // applyBoundaryConditions (tst_01_BDEM:50-60)
+            const int f = P.fix[i];
+            if (f & DEM_FIX_FORCE) F0 = F1 = F2 = 0.;
+            if (f & DEM_FIX_TORQUE) T0 = T1 = T2 = 0.;
+        }
+        const double m_inverse = 1. / mIi.x, I_inverse = 1. / mIi.y, h = fc.half_dt;
+        ui0 += h * F0 * m_inverse;
+        ui1 += h * F1 * m_inverse;
+        ui2 += h * F2 * m_inverse;
+        wi0 += h * T0 * I_inverse;
+        wi1 += h * T1 * I_inverse;
+        wi2 += h * T2 * I_inverse;
+        D4 pn = pi;
+        if (cs_.last) {
+            P.force[i] = F0;
+            P.force[cap + i] = F1;
+            P.force[2 * cap + i] = F2;
+            P.torque[i] = T0;
+            P.torque[cap + i] = T1;
+            P.torque[2 * cap + i] = T2;
+        } else {
+            ui0 += h * F0 * m_inverse;
+            ui1 += h * F1 * m_inverse;
+            ui2 += h * F2 * m_inverse;
+            wi0 += h * T0 * I_inverse;
+            wi1 += h * T1 * I_inverse;
+            wi2 += h * T2 * I_inverse;
+            pn.x += fc.dt * ui0;
+            pn.y += fc.dt * ui1;
+            pn.z += fc.dt * ui2;
+            vmax2 = ui0 * ui0 + ui1 * ui1 + ui2 * ui2;
+        }
+        st4(P.pos[nxt], i, pn);
+        double *vn = P.vel[nxt], *wn = P.omg[nxt];
+        vn[i] = ui0;
+        vn[cap + i] = ui1;
+        vn[2 * cap + i] = ui2;
+        wn[i] = wi0;
+        wn[cap + i] = wi1;
+        wn[2 * cap + i] = wi2;
+    }
+    finish_step(ctl, vmax2, fc.dt, status, true);
+}
+
+__global__ void k_bond_broken_count(Bonds B, int n, unsigned long long *out) {
+    unsigned long long c = 0;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < (long)B.mb * B.cap; t += (long)gridDim.x * blockDim.x)
+        c += B.broken[t] ? 1 : 0;
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
+}
+
+}  // namespace
+
+void launch_bond_setup(const Particles &P, const NbrList &L, const Bonds &B, Ctl *ctl, double factor, cudaStream_t s) {
+    k_bond_setup<<<(P.n + 127) / 128, 128, 0, s>>>(P, L, B, ctl, factor);
+}
+
+void launch_bond_step(const Particles &P, const Bonds &B, Ctl *ctl, const ForceConsts &fc, const BondConsts &bc,
+                      cudaStream_t s) {
+    k_bond_step<<<(P.n + kBondBlock - 1) / kBondBlock, kBondBlock, 0, s>>>(P, B, ctl, fc, bc);
+}
+
+void launch_bond_broken_count(const Bonds &B, int n, unsigned long long *out, cudaStream_t s) {
+    cudaMemsetAsync(out, 0, sizeof(unsigned long long), s);
+    k_bond_broken_count<<<148 * 4, 256, 0, s>>>(B, n, out);
+}
+
+}  // namespace b200dem

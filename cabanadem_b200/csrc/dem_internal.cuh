@@ -78,6 +78,7 @@ struct ForceConsts {
     int has_gravity;
     int has_ext;
     int has_fix;
+    int mixed;                 // 1: FP32 contact forces (dem_mixed.cu)
 };
 
 struct NbrList {
@@ -109,6 +110,32 @@ struct BuildBuffers {
     int *src, *dst;           // permutation at re-sort
 };
 
+// Bond slots (bonded DEM), slot-major like the contact history.
+constexpr unsigned BQ10_INDEX_BY_J = 0x01u;   // history(i, partner id), BondedDEM_Force.hpp:207, :231-322
+constexpr unsigned BQ11_HARDCODED_K = 0x02u;  // k from E, G and bond area, BondedDEM_Force.hpp:186-198
+constexpr unsigned BQ1_VELJ_USES_UI = 0x04u;  // BondedDEM_Force.hpp:142-146
+
+struct Bonds {
+    int mb, cap;
+    int *idx;          // [mb][cap] partner (sorted index), -1 empty
+    double *init_len;  // [mb][cap]
+    int *count;        // [cap]
+    double *hist;      // [9][mb][cap]: ft x|y|z, mn x|y|z, mt x|y|z
+    uint8_t *broken;   // [mb][cap]
+    double *E, *G;     // [cap] per-particle moduli (sorted order)
+};
+
+struct BondConsts {
+    unsigned quirks;
+    double beta, radius_factor, kn, kt, break_strain;
+};
+
+// ---- launchers (dem_bonded.cu) ----------------------------------------------------
+void launch_bond_setup(const Particles &P, const NbrList &L, const Bonds &B, Ctl *ctl, double factor, cudaStream_t s);
+void launch_bond_step(const Particles &P, const Bonds &B, Ctl *ctl, const ForceConsts &fc, const BondConsts &bc,
+                      cudaStream_t s);
+void launch_bond_broken_count(const Bonds &B, int n, unsigned long long *out, cudaStream_t s);
+
 // ---- launchers (dem_step.cu) ------------------------------------------------------
 // MODE_FUSED launches the streaming kernel and the contact kernel (kernels_per_step());
 // MODE_FORCE_ONLY one force-only kernel.
@@ -118,6 +145,12 @@ void launch_prologue(const Particles &P, Ctl *ctl, const ForceConsts &fc, cudaSt
 void launch_step(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
                  const PairConst *pw, const WallGeom *walls, int mode, cudaStream_t s);
 void launch_stage(const Particles &P, Ctl *ctl, const ForceConsts &fc, int stage, cudaStream_t s);
+// dem_mixed.cu
+void launch_contact_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
+                          const PairConst *pw, const WallGeom *walls, int blocks, cudaStream_t s);
+void launch_force_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
+                        const PairConst *pw, const WallGeom *walls, cudaStream_t s);
+const void *contact_mixed_kernel();
 void launch_energy(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
                    const PairConst *pw, const WallGeom *walls, double *partials, int nparts, double *out,
                    cudaStream_t s);

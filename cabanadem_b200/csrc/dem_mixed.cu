@@ -1,0 +1,67 @@
+// dem_mixed.cu -- mixed-precision contact kernels (built with FMA contraction).
+//
+// Same per-particle step as the FP64 path (dem_particle.cuh), instantiated with FP32
+// normal/tangential force arithmetic: pair offset, distance and overlap are formed in FP64
+// from the FP64 positions (the subtraction that cancels), then the Hertz/Mindlin forces,
+// damping and Coulomb limit are evaluated in FP32; tangential history is accumulated and
+// stored in FP64, per-particle force sums and the velocity-Verlet update stay FP64.  The
+// streaming kernel (particles with no possible contact) is shared with the FP64 path.
+#include "dem_particle.cuh"
+
+namespace b200dem {
+
+namespace {
+
+__global__ void __launch_bounds__(kBlock) k_contact_mixed(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
+                                                          const PairConst *__restrict__ pp,
+                                                          const PairConst *__restrict__ pw,
+                                                          const WallGeom *__restrict__ walls) {
+    if (ctl->steps_done >= ctl->target || (ctl->status & DEM_ERR_NEIGHBOR_OVERFLOW) || !(ctl->disp < ctl->half_skin))
+        return;
+    const int nd = ctl->ndefer;
+    if ((long)blockIdx.x * blockDim.x >= nd) {
+        finish_step_idle(ctl, fc.dt);
+        return;
+    }
+    CtlSnap cs_;
+    cs_.cur = ctl->cur;
+    cs_.last = ctl->steps_done + 1 >= ctl->target;
+    double vmax2 = 0.0;
+    int status = 0;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nd; t += gridDim.x * blockDim.x) {
+        double v2 = 0.0;
+        particle_full<MODE_FUSED, true>(P, L, fc, pp, pw, walls, cs_.cur, cs_.cur ^ 1, cs_.last, L.defer[t], v2,
+                                        status);
+        vmax2 = fmax(vmax2, v2);
+    }
+    finish_step(ctl, vmax2, fc.dt, status, true);
+}
+
+__global__ void __launch_bounds__(kBlock) k_force_mixed(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
+                                                        const PairConst *__restrict__ pp,
+                                                        const PairConst *__restrict__ pw,
+                                                        const WallGeom *__restrict__ walls) {
+    const CtlSnap cs_ = read_ctl(ctl, false);
+    if (!cs_.go) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double vmax2 = 0.0;
+    int status = 0;
+    if (i < P.n) particle_full<MODE_FORCE_ONLY, true>(P, L, fc, pp, pw, walls, cs_.cur, cs_.cur ^ 1, 1, i, vmax2, status);
+    if (status) atomicOr(&ctl->status, status);
+}
+
+}  // namespace
+
+void launch_contact_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
+                          const PairConst *pw, const WallGeom *walls, int blocks, cudaStream_t s) {
+    k_contact_mixed<<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+}
+
+void launch_force_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
+                        const PairConst *pw, const WallGeom *walls, cudaStream_t s) {
+    k_force_mixed<<<(P.n + kBlock - 1) / kBlock, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+}
+
+const void *contact_mixed_kernel() { return (const void *)k_contact_mixed; }
+
+}  // namespace b200dem

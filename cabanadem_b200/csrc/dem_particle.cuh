@@ -1,0 +1,656 @@
+// dem_particle.cuh -- per-particle DEM step shared by the FP64 and mixed-precision
+// translation units.  dem_step.cu (built with --fmad=false) instantiates the FP64 body,
+// whose every expression keeps the reference's order; dem_mixed.cu (built with FMA)
+// instantiates the mixed body: contact geometry (pair distance and overlap) in FP64 on the
+// FP64 positions, normal/tangential forces in FP32 on the resulting offsets, tangential
+// history accumulation, force sums and integration in FP64.
+#pragma once
+#include "b200dem.h"
+#include "dem_internal.cuh"
+
+namespace b200dem {
+
+namespace {
+
+constexpr int kBlock = 128;
+constexpr int kStreamBlock = 256;
+
+struct __align__(32) D4 {
+    double x, y, z, w;
+};
+
+__device__ __forceinline__ D4 ld4(const double4 *p, int i) {
+    const D4 *q = reinterpret_cast<const D4 *>(p);
+    return q[i];
+}
+__device__ __forceinline__ void st4(double4 *p, int i, D4 v) { reinterpret_cast<D4 *>(p)[i] = v; }
+
+// Read-only loads issued where they are written: volatile asm is neither sunk into a later
+// branch nor merged, so all of a particle's loads are in flight together.
+__device__ __forceinline__ double ld_early(const double *p) {
+    double v;
+    asm volatile("ld.global.nc.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ double2 ld_early2(const void *p) {
+    double2 v;
+    asm volatile("ld.global.nc.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ int ld_early_i(const int *p) {
+    int v;
+    asm volatile("ld.global.nc.b32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ D4 ld4_early(const double4 *p, int i) {
+    const double2 a = ld_early2(reinterpret_cast<const double2 *>(p) + 2 * (long)i);
+    const double2 b = ld_early2(reinterpret_cast<const double2 *>(p) + 2 * (long)i + 1);
+    D4 r;
+    r.x = a.x;
+    r.y = a.y;
+    r.z = b.x;
+    r.w = b.y;
+    return r;
+}
+
+// Last-block election without a block barrier, for a block that has no work: it adds no
+// vmax or status, only its ticket; the last ticket finalises the step.
+__device__ __forceinline__ void finish_step_idle(Ctl *ctl, double dt) {
+    if (threadIdx.x != 0) return;
+    __threadfence();
+    const unsigned t = atomicAdd(&ctl->ticket, 1u);
+    if (t == gridDim.x - 1) {
+        __threadfence();
+        const double v2 = __longlong_as_double((long long)atomicAdd(&ctl->vmax2, 0ull));
+        ctl->disp = ctl->disp + dt * sqrt(v2) * (1.0 + 1e-9);
+        ctl->vmax2 = 0ull;
+        ctl->ndefer = 0;
+        ctl->cur ^= 1;
+        ctl->steps_done += 1;
+        ctl->total_steps += 1;
+        __threadfence();
+        ctl->ticket = 0u;
+    }
+}
+
+struct CtlSnap {
+    int cur, go, last;
+};
+
+// Block-uniform gate on the device control word.  Every block evaluates the same
+// condition from values finalised by the previous launch.
+__device__ __forceinline__ CtlSnap read_ctl(const Ctl *ctl, bool gated) {
+    __shared__ CtlSnap s;
+    if (threadIdx.x == 0) {
+        CtlSnap c;
+        c.cur = ctl->cur;
+        if (gated) {
+            const bool stale = !(ctl->disp < ctl->half_skin);
+            c.go = (ctl->steps_done < ctl->target) && !(ctl->status & DEM_ERR_NEIGHBOR_OVERFLOW) && !stale;
+            c.last = (ctl->steps_done + 1 >= ctl->target);
+        } else {
+            c.go = !(ctl->status & DEM_ERR_NEIGHBOR_OVERFLOW);
+            c.last = 1;
+        }
+        s = c;
+    }
+    __syncthreads();
+    return s;
+}
+
+// Block max of |u|^2, then the last block to finish advances the control word:
+// disp += dt*|u|max (conservative displacement bound), flips the ping-pong buffer.
+__device__ __forceinline__ void finish_step(Ctl *ctl, double vmax2, double dt, int status, bool count_step) {
+    __shared__ double red[kBlock / 32];
+    __shared__ bool am_last;
+    for (int o = 16; o > 0; o >>= 1) vmax2 = fmax(vmax2, __shfl_xor_sync(0xffffffffu, vmax2, o));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (status) atomicOr(&ctl->status, status);
+    if (lane == 0) red[warp] = vmax2;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = red[0];
+        for (int w = 1; w < kBlock / 32; ++w) m = fmax(m, red[w]);
+        atomicMax(&ctl->vmax2, (unsigned long long)__double_as_longlong(m));
+        __threadfence();
+        const unsigned t = atomicAdd(&ctl->ticket, 1u);
+        am_last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (am_last && threadIdx.x == 0) {
+        __threadfence();
+        const double v2 = __longlong_as_double((long long)atomicAdd(&ctl->vmax2, 0ull));
+        ctl->disp = ctl->disp + dt * sqrt(v2) * (1.0 + 1e-9);
+        ctl->vmax2 = 0ull;
+        ctl->ndefer = 0;
+        ctl->cur ^= 1;
+        if (count_step) {
+            ctl->steps_done += 1;
+            ctl->total_steps += 1;
+        }
+        __threadfence();
+        ctl->ticket = 0u;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Full per-particle step (contact compaction, pp and wall forces, hooks, integration).
+// MODE_FORCE_ONLY writes F and tau in place and leaves x, u, omega untouched (the
+// unfused reference-order path); MODE_FUSED integrates into the next buffer.
+// ---------------------------------------------------------------------------------------
+template <int MODE, bool MIXED>
+__device__ __forceinline__ void particle_full(const Particles &P, const NbrList &L, const ForceConsts &fc,
+                                              const PairConst *__restrict__ pp, const PairConst *__restrict__ pw,
+                                              const WallGeom *__restrict__ walls, const int cur, const int nxt,
+                                              const int last, const int i, double &vmax2, int &status) {
+    const int cap = P.cap;
+    const unsigned q = fc.quirks;
+    const double4 *__restrict__ pc = P.pos[cur];
+    const double *__restrict__ vc = P.vel[cur];
+    const double *__restrict__ wc = P.omg[cur];
+    const D4 pi = ld4(pc, i);
+    double ui0 = vc[i], ui1 = vc[cap + i], ui2 = vc[2 * cap + i];
+    double wi0 = wc[i], wi1 = wc[cap + i], wi2 = wc[2 * cap + i];
+    const double2 mIi = P.mI[i];
+    const int mi = fc.nmat > 1 ? (int)P.mat[i] : 0;
+    const int cs0 = P.cstate[i];
+    int cnt = cs0 & 0xff;
+    unsigned wmask = (unsigned)cs0 >> 8;
+    int *tidx = P.tidx + i;
+    double *thx = P.th + i;
+    double *thy = P.th + (long)P.mc * cap + i;
+    double *thz = P.th + 2L * P.mc * cap + i;
+    double F0 = 0., F1 = 0., F2 = 0., T0 = 0., T1 = 0., T2 = 0.;
+    if (fc.has_ext) {
+        F0 += P.ext[i];
+        F1 += P.ext[cap + i];
+        F2 += P.ext[2 * cap + i];
+    }
+    // ---- update_tangential_contacts (Force.hpp:364-441)
+    if (cnt > 0) {
+        int count = 0, k = 0;
+        const int total = cnt;
+        int last_idx_tmp = cnt - 1;
+        while (count < total) {
+            const int sidx = tidx[(long)k * cap];
+            if (sidx == -1) break;
+            const D4 pj = ld4(pc, sidx);
+            const double px = pi.x - pj.x, py = pi.y - pj.y, pz = pi.z - pj.z;
+            const double r2ij = px * px + py * py + pz * pz;
+            const double rij = sqrt(r2ij);
+            const double overlap = pi.w + pj.w - rij;
+            if (overlap <= 0.) {
+                const long a = (long)k * cap, b = (long)last_idx_tmp * cap;
+                if (k == last_idx_tmp) {
+                    tidx[a] = -1;
+                    thx[a] = 0.;
+                    thy[a] = 0.;
+                    thz[a] = 0.;
+                } else {
+                    tidx[a] = tidx[b];
+                    tidx[b] = -1;
+                    thx[a] = thx[b];
+                    thx[b] = 0.;
+                    thy[a] = thy[b];
+                    thy[b] = 0.;
+                    thz[a] = thz[b];
+                    thz[b] = 0.;
+                    last_idx_tmp -= 1;
+                }
+                cnt -= 1;
+            } else {
+                k = k + 1;
+            }
+            count += 1;
+        }
+    }
+    // ---- particle-particle (Force.hpp:73-329), list in ascending caller index
+    const int nn = L.nn[i];
+    const int *__restrict__ lidx = L.idx + i;
+    for (int kk = 0; kk < nn; ++kk) {
+        const int j = lidx[(long)kk * cap];
+        const D4 pj = ld4(pc, j);
+        const double px = pi.x - pj.x, py = pi.y - pj.y, pz = pi.z - pj.z;
+        const double r2ij = px * px + py * py + pz * pz;
+        const double sr = pi.w + pj.w;
+        // exact early-out: r2 >= s^2 (1 + 1e-10) implies sqrt(r2) >= s, overlap <= 0
+        if (r2ij >= sr * sr * 1.0000000001) continue;
+        const double rij = sqrt(r2ij);
+        const double overlap = sr - rij;
+        if (!(overlap > 0.)) continue;
+        const double a_i = pi.w - overlap / 2.;
+        const double a_j = pj.w - overlap / 2.;
+        const double nx = px / rij, ny = py / rij, nz = pz / rij;
+        const double uj0 = vc[j];
+        const double uj1 = (q & DEM_Q1_VELJ_USES_UI) ? ui1 : vc[cap + j];
+        const double uj2 = (q & DEM_Q1_VELJ_USES_UI) ? ui2 : vc[2 * cap + j];
+        const double wj0 = wc[j], wj1 = wc[cap + j], wj2 = wc[2 * cap + j];
+        const double vi0 = ui0 + (wi1 * nz - wi2 * ny) * a_i;
+        const double vi1 = ui1 + (wi2 * nx - wi0 * nz) * a_i;
+        const double vi2 = ui2 + (wi0 * ny - wi1 * nx) * a_i;
+        const double vj0 = uj0 + (-wj1 * nz + wj2 * ny) * a_j;
+        const double vj1 = uj1 + (-wj2 * nx + wj0 * nz) * a_j;
+        const double vj2 = uj2 + (-wj0 * ny + wj1 * nx) * a_j;
+        const double v0 = vi0 - vj0, v1 = vi1 - vj1, v2 = vi2 - vj2;
+        const double vdn = v0 * nx + v1 * ny + v2 * nz;
+        const double vn0 = vdn * nx, vn1 = vdn * ny, vn2 = vdn * nz;
+        const double vt0 = v0 - vn0, vt1 = v1 - vn1, vt2 = v2 - vn2;
+        // slot lookup / insert (Force.hpp:166-192)
+        int found_at = -1;
+        for (int s = 0; s < cnt; ++s)
+            if (tidx[(long)s * cap] == j) found_at = s;
+        double h0 = 0., h1 = 0., h2 = 0.;
+        if (found_at < 0) {
+            if (cnt < P.mc) {
+                found_at = cnt;
+                cnt += 1;
+                const long a = (long)found_at * cap;
+                tidx[a] = j;
+                thx[a] = 0.;
+                thy[a] = 0.;
+                thz[a] = 0.;
+            } else {
+                status |= DEM_ERR_CONTACT_OVERFLOW;
+            }
+        } else {
+            const long a = (long)found_at * cap;
+            h0 = thx[a];
+            h1 = thy[a];
+            h2 = thz[a];
+        }
+        const int mj = fc.nmat > 1 ? (int)P.mat[j] : 0;
+        const PairConst c = pp[mi * fc.nmat + mj];
+        if constexpr (MIXED) {
+            // Kinematics in FP64 (multiplies and adds only: the normal, the relative contact
+            // velocity and its normal/tangential split, where cancellation would cost FP32 its
+            // accuracy); force magnitudes -- square roots, divisions, x^1.5, Coulomb limit --
+            // in FP32; history accumulation and force sums in FP64.
+            const float ov = (float)overlap;
+            const double inv_r = 1.0 / rij;
+            const double dnx = px * inv_r, dny = py * inv_r, dnz = pz * inv_r;
+            const double da_i = pi.w - 0.5 * overlap, da_j = pj.w - 0.5 * overlap;
+            const double uj0 = vc[j];
+            const double uj1 = (q & DEM_Q1_VELJ_USES_UI) ? ui1 : vc[cap + j];
+            const double uj2 = (q & DEM_Q1_VELJ_USES_UI) ? ui2 : vc[2 * cap + j];
+            const double wj0 = wc[j], wj1 = wc[cap + j], wj2 = wc[2 * cap + j];
+            const double dv0 = (ui0 + (wi1 * dnz - wi2 * dny) * da_i) - (uj0 + (-wj1 * dnz + wj2 * dny) * da_j);
+            const double dv1 = (ui1 + (wi2 * dnx - wi0 * dnz) * da_i) - (uj1 + (-wj2 * dnx + wj0 * dnz) * da_j);
+            const double dv2 = (ui2 + (wi0 * dny - wi1 * dnx) * da_i) - (uj2 + (-wj0 * dny + wj1 * dnx) * da_j);
+            const double dvdn = dv0 * dnx + dv1 * dny + dv2 * dnz;
+            const float fnx = (float)dnx, fny = (float)dny, fnz = (float)dnz;
+            const float fa_i = (float)da_i;
+            const float ri = (float)pi.w, rj = (float)pj.w;
+            const float v0 = (float)dv0, v1 = (float)dv1, v2 = (float)dv2;
+            const float vdn = (float)dvdn;
+            const float vt0 = (float)(dv0 - dvdn * dnx), vt1 = (float)(dv1 - dvdn * dny), vt2 = (float)(dv2 - dvdn * dnz);
+            const float R_eff = 1.f / (1.f / ri + 1.f / rj);
+            const float m_eff = 1.f / (1.f / (float)mIi.x + 1.f / (float)P.mI[j].x);
+            const float sro = sqrtf(R_eff * ov);
+            const float kn = (float)c.c_kn * sqrtf(R_eff);
+            const float S_n = (float)c.c_Sn * sro;
+            const float eta_n = (float)fc.K_n_pp * sqrtf(S_n * m_eff);
+            const float kt = (float)c.c_kt * sro;
+            const float eta_t = (float)fc.K_t_pp * sqrtf(kt * m_eff);
+            const float fn = kn * ov * sqrtf(ov);
+            const float fn0 = fn * fnx - eta_n * (vdn * fnx);
+            const float fn1 = fn * fny - eta_n * (vdn * fny);
+            const float fn2 = fn * fnz - eta_n * (vdn * fnz);
+            float tf0 = 0.f, tf1 = 0.f, tf2 = 0.f;
+            const float vij_magn = sqrtf(v0 * v0 + v1 * v1 + v2 * v2);
+            if (vij_magn < 1e-12f) {
+                h0 = 0.;
+                h1 = 0.;
+                h2 = 0.;
+            } else {
+                const float ti_magn = sqrtf(vt0 * vt0 + vt1 * vt1 + vt2 * vt2);
+                float ti0 = 0.f, ti1 = 0.f, ti2 = 0.f;
+                if (ti_magn > 1e-12f) {
+                    const float inv_t = 1.f / ti_magn;
+                    ti0 = vt0 * inv_t;
+                    ti1 = vt1 * inv_t;
+                    ti2 = vt2 * inv_t;
+                }
+                const double dl0 = h0 + dv0 * fc.dt, dl1 = h1 + dv1 * fc.dt, dl2 = h2 + dv2 * fc.dt;
+                const double dld = dl0 * (double)ti0 + dl1 * (double)ti1 + dl2 * (double)ti2;
+                h0 = dld * (double)ti0;
+                h1 = dld * (double)ti1;
+                h2 = dld * (double)ti2;
+                const float ft0 = -kt * (float)h0 - eta_t * vt0;
+                const float ft1 = -kt * (float)h1 - eta_t * vt1;
+                const float ft2 = -kt * (float)h2 - eta_t * vt2;
+                const float ft_magn = sqrtf(ft0 * ft0 + ft1 * ft1 + ft2 * ft2);
+                const float fn_magn = sqrtf(fn0 * fn0 + fn1 * fn1 + fn2 * fn2);
+                const float lim = (float)fc.mu_pp * fn_magn;
+                const float fms = ft_magn > lim ? lim : ft_magn;
+                tf0 = -fms * ti0;
+                tf1 = -fms * ti1;
+                tf2 = -fms * ti2;
+                const float md0 = -tf0 / kt, md1 = -tf1 / kt, md2 = -tf2 / kt;
+                if (q & DEM_Q4_UNIT_HISTORY) {
+                    const float lt = sqrtf(md0 * md0 + md1 * md1 + md2 * md2);
+                    if (lt > 1e-12f) {
+                        h0 = (double)(md0 / lt);
+                        h1 = (double)(md1 / lt);
+                        h2 = (double)(md2 / lt);
+                    } else {
+                        h0 = 0.;
+                        h1 = 0.;
+                        h2 = 0.;
+                    }
+                } else {
+                    h0 = (double)md0;
+                    h1 = (double)md1;
+                    h2 = (double)md2;
+                }
+            }
+            if (found_at >= 0) {
+                const long a = (long)found_at * cap;
+                thx[a] = h0;
+                thy[a] = h1;
+                thz[a] = h2;
+            }
+            F0 += (double)(fn0 + tf0);
+            F1 += (double)(fn1 + tf1);
+            F2 += (double)(fn2 + tf2);
+            if (!(q & DEM_Q3_NO_PP_TORQUE)) {
+                T0 += (double)((fny * tf2 - fnz * tf1) * fa_i);
+                T1 += (double)((fnz * tf0 - fnx * tf2) * fa_i);
+                T2 += (double)((fnx * tf1 - fny * tf0) * fa_i);
+            }
+            continue;
+        }
+        const double tmp_3 = 1. / pi.w;
+        const double tmp_4 = 1. / pj.w;
+        const double R_eff = 1. / (tmp_3 + tmp_4);
+        const double kn = c.c_kn * sqrt(R_eff);
+        const double S_n = c.c_Sn * sqrt(R_eff * overlap);
+        const double m_eff = 1. / (1. / mIi.x + 1. / P.mI[j].x);
+        const double eta_n = fc.K_n_pp * sqrt(S_n * m_eff);
+        const double kt = c.c_kt * sqrt(R_eff * overlap);
+        const double eta_t = fc.K_t_pp * sqrt(kt * m_eff);
+        const double fn = kn * (overlap * sqrt(overlap));
+        const double fn0 = fn * nx - eta_n * vn0;
+        const double fn1 = fn * ny - eta_n * vn1;
+        const double fn2 = fn * nz - eta_n * vn2;
+        double tf0 = 0., tf1 = 0., tf2 = 0.;
+        const double vij_magn = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+        if (vij_magn < 1e-12) {
+            h0 = 0.;
+            h1 = 0.;
+            h2 = 0.;
+        } else {
+            const double tx = v0 - nx * vdn, ty = v1 - ny * vdn, tz = v2 - nz * vdn;
+            const double ti_magn = sqrt(tx * tx + ty * ty + tz * tz);
+            double ti0 = 0., ti1 = 0., ti2 = 0.;
+            if (ti_magn > 1e-12) {
+                ti0 = tx / ti_magn;
+                ti1 = ty / ti_magn;
+                ti2 = tz / ti_magn;
+            }
+            const double dl0 = h0 + v0 * fc.dt, dl1 = h1 + v1 * fc.dt, dl2 = h2 + v2 * fc.dt;
+            const double dld = (dl0 * ti0 + dl1 * ti1 + dl2 * ti2);
+            h0 = dld * ti0;
+            h1 = dld * ti1;
+            h2 = dld * ti2;
+            const double ft0 = -kt * h0 - eta_t * vt0;
+            const double ft1 = -kt * h1 - eta_t * vt1;
+            const double ft2 = -kt * h2 - eta_t * vt2;
+            const double ft_magn = sqrt(ft0 * ft0 + ft1 * ft1 + ft2 * ft2);
+            const double fn_magn = sqrt(fn0 * fn0 + fn1 * fn1 + fn2 * fn2);
+            double fms = ft_magn;
+            if (fms > fc.mu_pp * fn_magn) fms = fc.mu_pp * fn_magn;
+            tf0 = -fms * ti0;
+            tf1 = -fms * ti1;
+            tf2 = -fms * ti2;
+            const double md0 = -tf0 / kt, md1 = -tf1 / kt, md2 = -tf2 / kt;
+            if (q & DEM_Q4_UNIT_HISTORY) {
+                const double lt = sqrt(md0 * md0 + md1 * md1 + md2 * md2);
+                if (lt > 1e-12) {
+                    h0 = md0 / lt;
+                    h1 = md1 / lt;
+                    h2 = md2 / lt;
+                } else {
+                    h0 = 0.;
+                    h1 = 0.;
+                    h2 = 0.;
+                }
+            } else {
+                h0 = md0;
+                h1 = md1;
+                h2 = md2;
+            }
+        }
+        if (found_at >= 0) {
+            const long a = (long)found_at * cap;
+            thx[a] = h0;
+            thy[a] = h1;
+            thz[a] = h2;
+        }
+        F0 += fn0 + tf0;
+        F1 += fn1 + tf1;
+        F2 += fn2 + tf2;
+        if (!(q & DEM_Q3_NO_PP_TORQUE)) {
+            T0 += (ny * tf2 - nz * tf1) * a_i;
+            T1 += (nz * tf0 - nx * tf2) * a_i;
+            T2 += (nx * tf1 - ny * tf0) * a_i;
+        }
+    }
+    // ---- particle-infinite wall (Force.hpp:475-673)
+    for (int w = 0; w < fc.nwall; ++w) {
+        const WallGeom g = walls[w];
+        const double px = pi.x - g.x[0], py = pi.y - g.x[1], pz = pi.z - g.x[2];
+        const double nx = g.n[0], ny = g.n[1], nz = g.n[2];
+        const double tmp = px * nx + py * ny + pz * nz;
+        const double overlap = pi.w - tmp;
+        const unsigned bit = 1u << w;
+        double *swx = P.sw + (long)w * cap + i;
+        double *swy = P.sw + (long)(P.mw + w) * cap + i;
+        double *swz = P.sw + (long)(2 * P.mw + w) * cap + i;
+        if (MIXED && overlap > 0.) {
+            const float ov = (float)overlap;
+            const double da_i = pi.w - 0.5 * overlap;
+            const double dv0 = ui0 + (wi1 * nz - wi2 * ny) * da_i;
+            const double dv1 = ui1 + (wi2 * nx - wi0 * nz) * da_i;
+            const double dv2 = ui2 + (wi0 * ny - wi1 * nx) * da_i;
+            const double dvdn = dv0 * nx + dv1 * ny + dv2 * nz;
+            const float fa_i = (float)da_i;
+            const float gx = (float)nx, gy = (float)ny, gz = (float)nz;
+            const float v0 = (float)dv0, v1 = (float)dv1, v2 = (float)dv2;
+            const float vdn = (float)dvdn;
+            const float vt0 = (float)(dv0 - dvdn * nx), vt1 = (float)(dv1 - dvdn * ny), vt2 = (float)(dv2 - dvdn * nz);
+            const PairConst c = pw[mi * fc.nwall + w];
+            const float R_eff = (float)pi.w;
+            const float m_eff = (float)mIi.x;
+            const float sro = sqrtf(R_eff * ov);
+            const float kn = (float)c.c_kn * sqrtf(R_eff);
+            const float S_n = (float)c.c_Sn * sro;
+            const float eta_n = (float)fc.K_n_pw * sqrtf(S_n * m_eff);
+            const float fn = kn * ov * sqrtf(ov);
+            const float fn0 = fn * gx - eta_n * (vdn * gx);
+            const float fn1 = fn * gy - eta_n * (vdn * gy);
+            const float fn2 = fn * gz - eta_n * (vdn * gz);
+            float ft0 = 0.f, ft1 = 0.f, ft2 = 0.f;
+            const float vij_magn = sqrtf(v0 * v0 + v1 * v1 + v2 * v2);
+            if (vij_magn < 1e-12f) {
+                *swx = 0.;
+                *swy = 0.;
+                *swz = 0.;
+            } else {
+                double s0 = 0., s1 = 0., s2 = 0.;
+                if (wmask & bit) {
+                    s0 = *swx;
+                    s1 = *swy;
+                    s2 = *swz;
+                }
+                s0 += (dv0 - dvdn * nx) * fc.dt;
+                s1 += (dv1 - dvdn * ny) * fc.dt;
+                s2 += (dv2 - dvdn * nz) * fc.dt;
+                const float kt = (float)c.c_kt * sro;
+                const float eta_t = (float)fc.K_t_pw * sqrtf(kt * m_eff);
+                const float fx = -kt * (float)s0 - eta_t * vt0;
+                const float fy = -kt * (float)s1 - eta_t * vt1;
+                const float fz = -kt * (float)s2 - eta_t * vt2;
+                const float ft_magn = (q & DEM_Q5_WALL_FT_TYPO) ? sqrtf(fx * fx + fy * fy + fz * fy)
+                                                                 : sqrtf(fx * fx + fy * fy + fz * fz);
+                float ti0 = 0.f, ti1 = 0.f, ti2 = 0.f;
+                if (ft_magn > 1e-12f) {
+                    ti0 = fx / ft_magn;
+                    ti1 = fy / ft_magn;
+                    ti2 = fz / ft_magn;
+                }
+                const float fn_magn = sqrtf(fn0 * fn0 + fn1 * fn1 + fn2 * fn2);
+                const float lim = (float)fc.mu_pw * fn_magn;
+                const float fms = (ft_magn < lim) ? ft_magn : lim;
+                ft0 = fms * ti0 + eta_t * vt0;
+                ft1 = fms * ti1 + eta_t * vt1;
+                ft2 = fms * ti2 + eta_t * vt2;
+                *swx = (double)(-ft0 / kt);
+                *swy = (double)(-ft1 / kt);
+                *swz = (double)(-ft2 / kt);
+            }
+            wmask |= bit;
+            F0 += (double)(fn0 + ft0);
+            F1 += (double)(fn1 + ft1);
+            F2 += (double)(fn2 + ft2);
+            T0 += (double)((gy * ft2 - gz * ft1) * fa_i);
+            T1 += (double)((gz * ft0 - gx * ft2) * fa_i);
+            T2 += (double)((gx * ft1 - gy * ft0) * fa_i);
+        } else if (overlap > 0.) {
+            const double a_i = pi.w - overlap / 2.;
+            const double v0 = ui0 + (wi1 * nz - wi2 * ny) * a_i;
+            const double v1 = ui1 + (wi2 * nx - wi0 * nz) * a_i;
+            const double v2 = ui2 + (wi0 * ny - wi1 * nx) * a_i;
+            const double vdn = v0 * nx + v1 * ny + v2 * nz;
+            const double vt0 = v0 - vdn * nx, vt1 = v1 - vdn * ny, vt2 = v2 - vdn * nz;
+            const PairConst c = pw[mi * fc.nwall + w];
+            const double R_eff = 1. / (1. / pi.w + 0.);
+            const double kn = c.c_kn * sqrt(R_eff);
+            const double S_n = c.c_Sn * sqrt(R_eff * overlap);
+            const double m_eff = 1. / (1. / mIi.x + 0.);
+            const double eta_n = fc.K_n_pw * sqrt(S_n * m_eff);
+            const double fn = kn * (overlap * sqrt(overlap));
+            const double fn0 = fn * nx - eta_n * (vdn * nx);
+            const double fn1 = fn * ny - eta_n * (vdn * ny);
+            const double fn2 = fn * nz - eta_n * (vdn * nz);
+            double ft0 = 0., ft1 = 0., ft2 = 0.;
+            const double vij_magn = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+            if (vij_magn < 1e-12) {
+                *swx = 0.;
+                *swy = 0.;
+                *swz = 0.;
+            } else {
+                double s0 = 0., s1 = 0., s2 = 0.;
+                if (wmask & bit) {
+                    s0 = *swx;
+                    s1 = *swy;
+                    s2 = *swz;
+                }
+                s0 += vt0 * fc.dt;
+                s1 += vt1 * fc.dt;
+                s2 += vt2 * fc.dt;
+                const double kt = c.c_kt * sqrt(R_eff * overlap);
+                const double eta_t = fc.K_t_pw * sqrt(kt * m_eff);
+                const double fx = -kt * s0 - eta_t * vt0;
+                const double fy = -kt * s1 - eta_t * vt1;
+                const double fz = -kt * s2 - eta_t * vt2;
+                const double ft_magn = (q & DEM_Q5_WALL_FT_TYPO) ? sqrt(fx * fx + fy * fy + fz * fy)
+                                                                  : sqrt(fx * fx + fy * fy + fz * fz);
+                double ti0 = 0., ti1 = 0., ti2 = 0.;
+                if (ft_magn > 1e-12) {
+                    ti0 = fx / ft_magn;
+                    ti1 = fy / ft_magn;
+                    ti2 = fz / ft_magn;
+                }
+                const double fn_magn = sqrt(fn0 * fn0 + fn1 * fn1 + fn2 * fn2);
+                const double lim = fc.mu_pw * fn_magn;
+                const double fms = (ft_magn < lim) ? ft_magn : lim;  // std::min(lim, ft_magn)
+                ft0 = fms * ti0;
+                ft1 = fms * ti1;
+                ft2 = fms * ti2;
+                ft0 += eta_t * vt0;
+                ft1 += eta_t * vt1;
+                ft2 += eta_t * vt2;
+                *swx = -ft0 / kt;
+                *swy = -ft1 / kt;
+                *swz = -ft2 / kt;
+            }
+            wmask |= bit;
+            F0 += fn0 + ft0;
+            F1 += fn1 + ft1;
+            F2 += fn2 + ft2;
+            T0 += (ny * ft2 - nz * ft1) * a_i;
+            T1 += (nz * ft0 - nx * ft2) * a_i;
+            T2 += (nx * ft1 - ny * ft0) * a_i;
+        } else if (wmask & bit) {
+            *swx = 0.;
+            *swy = 0.;
+            *swz = 0.;
+            wmask &= ~bit;
+        }
+    }
+    const int cs1 = cnt | (int)(wmask << 8);
+    if (cs1 != cs0) P.cstate[i] = cs1;
+    // ---- hooks after the pair forces
+    if (fc.has_gravity) {
+        F0 += mIi.x * fc.g[0];
+        F1 += mIi.x * fc.g[1];
+        F2 += mIi.x * fc.g[2];
+    }
+    if (fc.has_fix) {
+        const int f = P.fix[i];
+        if (f & DEM_FIX_FORCE) F0 = F1 = F2 = 0.;
+        if (f & DEM_FIX_TORQUE) T0 = T1 = T2 = 0.;
+    }
+    if (MODE == MODE_FORCE_ONLY) {
+        P.force[i] = F0;
+        P.force[cap + i] = F1;
+        P.force[2 * cap + i] = F2;
+        P.torque[i] = T0;
+        P.torque[cap + i] = T1;
+        P.torque[2 * cap + i] = T2;
+    } else {
+        const double m_inverse = 1. / mIi.x;
+        const double I_inverse = 1. / mIi.y;
+        const double h = fc.half_dt;
+        // stage3 of this step
+        ui0 += h * F0 * m_inverse;
+        ui1 += h * F1 * m_inverse;
+        ui2 += h * F2 * m_inverse;
+        wi0 += h * T0 * I_inverse;
+        wi1 += h * T1 * I_inverse;
+        wi2 += h * T2 * I_inverse;
+        D4 pn = pi;
+        if (last) {
+            P.force[i] = F0;
+            P.force[cap + i] = F1;
+            P.force[2 * cap + i] = F2;
+            P.torque[i] = T0;
+            P.torque[cap + i] = T1;
+            P.torque[2 * cap + i] = T2;
+        } else {
+            // stage1 + stage2 of the next step
+            ui0 += h * F0 * m_inverse;
+            ui1 += h * F1 * m_inverse;
+            ui2 += h * F2 * m_inverse;
+            wi0 += h * T0 * I_inverse;
+            wi1 += h * T1 * I_inverse;
+            wi2 += h * T2 * I_inverse;
+            pn.x += fc.dt * ui0;
+            pn.y += fc.dt * ui1;
+            pn.z += fc.dt * ui2;
+            vmax2 = ui0 * ui0 + ui1 * ui1 + ui2 * ui2;
+        }
+        st4(P.pos[nxt], i, pn);
+        double *vn = P.vel[nxt], *wn = P.omg[nxt];
+        vn[i] = ui0;
+        vn[cap + i] = ui1;
+        vn[2 * cap + i] = ui2;
+        wn[i] = wi0;
+        wn[cap + i] = wi1;
+        wn[2 * cap + i] = wi2;
+    }
+    }
+
+
+}  // namespace
+}  // namespace b200dem

@@ -145,6 +145,32 @@ def tst03(inp: Inputs) -> Scenario:
                     output_frequency=int(inp["output_frequency"]))
 
 
+def bonded_bar(nx=256, ny=64, nz=8, radius=0.5e-3, pull=0.05, dt=2e-8, nsteps=50_000, kn=1e7, kt=4e6,
+               break_strain=0.01, max_bonds=8, bond_quirks=0x04):
+    """Simple-cubic bar of nx*ny*nz spheres (r = 0.5 mm, pitch 1 mm), every pair within
+    1.05 diameters bonded (normal stiffness 1e7 N/m, shear 4e6 N/m, bond radius 0.5 r,
+    breakage at 1% strain).  The two end layers along x move apart at +-0.05 m/s (force and
+    torque zeroed each step); dt = 2e-8 s, 50,000 steps.  Bond history is slot-indexed and the
+    stiffness explicit (the reference's partner-indexed history and hard-coded stiffness,
+    BondedDEM_Force.hpp:186-207, do not define this case); vel_j keeps the reference's form."""
+    n = nx * ny * nz
+    k = np.arange(n)
+    ix, iy, iz = k % nx, (k // nx) % ny, k // (nx * ny)
+    pitch = 2.0 * radius
+    s = ParticleState.create(n, max_cnts=1, max_walls=1)
+    s.x[:, 0], s.x[:, 1], s.x[:, 2] = (ix + 0.5) * pitch, (iy + 0.5) * pitch, (iz + 0.5) * pitch
+    _apply_glass(s, radius)
+    fix = np.zeros(n, dtype=np.uint8)
+    left, right = ix == 0, ix == nx - 1
+    fix[left | right] = 0x3
+    s.u[left, 0], s.u[right, 0] = -pull, pull
+    b = BondState.create(n, max_bonds)
+    return dict(state=s, bonds=b, dt=dt, nsteps=nsteps, ext_force=None, fix_flags=fix, bond_factor=2.1,
+                search_cutoff=1.1 * pitch, length=(nx - 1) * pitch, area=ny * nz * pitch * pitch,
+                bparams=dict(quirks=bond_quirks, beta=0.1, radius_factor=0.5, kn=kn, kt=kt,
+                             break_strain=break_strain))
+
+
 def bdem_two_particles():
     """examples/tst_01_BDEM_two_particles_tensile_3D.cpp:162-302: two bonded spheres
     pulled apart by +-1e3 N, particle 0's force zeroed after the bond pass."""

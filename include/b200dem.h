@@ -168,6 +168,47 @@ int dem_compute_force(dem_solver *s);
  * (ascending partner id).  Pass idx=NULL to get the total in *total. */
 int dem_neighbors_get(dem_solver *s, int *offsets, int *idx, long *total);
 
+/* ---- bonded DEM: ParticlesBondedDEM<Mem,Dim,MaxBonds> bond slots ---------------------
+ * (src/CabanaBondedDEM_Particles.hpp:29-293) and computeBondedForce
+ * (src/CabanaBondedDEM_Force.hpp:53-348).  Reference behaviours, bit set = reproduce: */
+#define DEM_BQ10_INDEX_BY_J   0x01u /* history indexed by partner id (BondedDEM_Force.hpp:207, :231-322) */
+#define DEM_BQ11_HARDCODED_K  0x02u /* stiffness from E, G, bond area (BondedDEM_Force.hpp:186-198)     */
+#define DEM_BQ1_VELJ_USES_UI  0x04u /* vel_j y,z use u(i,.) (BondedDEM_Force.hpp:142-146)               */
+#define DEM_BOND_REF_COMPAT   0x07u
+
+typedef struct dem_bond_params {
+    unsigned quirks;
+    double beta;           /* sign-damping factor (reference: 0.1, BondedDEM_Force.hpp:186)   */
+    double radius_factor;  /* bond radius = min(r_i, r_j) * factor (reference: 1, :187)        */
+    double kn, kt;         /* explicit normal / shear stiffness, used when BQ11 is clear       */
+    double break_strain;   /* > 0: a bond breaks once (rij - L0) / L0 exceeds it (no reference
+                              counterpart)                                                    */
+} dem_bond_params;
+
+enum dem_bond_field {
+    DEM_B_IDX = 0,     /* int    [n][MaxBonds] sliceBondIdx (caller indices, -1 empty) */
+    DEM_B_INIT_LEN,    /* double [n][MaxBonds] sliceBondInitLen                       */
+    DEM_B_COUNT,       /* int    [n]           sliceTotalNoBonds                      */
+    DEM_B_FT_X, DEM_B_FT_Y, DEM_B_FT_Z,   /* double [n][MaxBonds] sliceBondFt*        */
+    DEM_B_MN_X, DEM_B_MN_Y, DEM_B_MN_Z,   /* double [n][MaxBonds] sliceBondMn*        */
+    DEM_B_MT_X, DEM_B_MT_Y, DEM_B_MT_Z,   /* double [n][MaxBonds] sliceBondMt*        */
+    DEM_B_BROKEN       /* uint8  [n][MaxBonds] 1 once the bond has broken             */
+};
+
+/* Bond storage for the solver's particles (ParticlesBondedDEM ctor, :52-60). */
+int dem_bonds_create(dem_solver *s, int max_bonds, const dem_bond_params *bp, dem_bonds **out);
+int dem_bonds_destroy(dem_bonds *b);
+/* setupBonds<Exec>() (src/CabanaBondedDEM_Particles.hpp:86-171): bond every j != i with
+ * rij < factor * rad(i) among the candidates within search_cutoff, in ascending j; rest
+ * length = rij.  The reference uses factor 3 and search cutoff 4 rad(0). */
+int dem_bonds_setup(dem_bonds *b, double factor, double search_cutoff);
+int dem_bonds_get(dem_bonds *b, int field, void *host, long count);
+int dem_bonds_broken(dem_bonds *b, long *count);
+/* nsteps of the bonded loop (tst_01_BDEM:295-306): stage1, stage2, force reset, external
+ * force (DEM_F_EXT_FORCE), computeBondedForce, boundary hook (DEM_F_FIX), stage3 -- fused
+ * into one kernel per step, graph-captured. */
+int dem_bonded_run(dem_bonds *b, int nsteps);
+
 /* ---- neighbour list without allocation ---------------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device memory at the
  * point where they need a neighbour list: code whose device memory belongs to another

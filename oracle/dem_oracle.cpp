@@ -653,8 +653,11 @@ extern "C" int orc_bonded_force(orc_particles *p, orc_bonds *b, const orc_bond_p
             double beta_bond = bp->beta;
             double bond_radius_factor = bp->radius_factor;
             double bond_rad = std::min(rad[i], rad[j]) * bond_radius_factor;
-            double A_bond = M_PI * std::pow(bond_rad, 2.);
-            double I_bond = M_PI * std::pow(bond_rad, 4.) / 4.0;
+            const double b2 = bp->pow_mode == ORC_POW_SQRT ? bond_rad * bond_rad : std::pow(bond_rad, 2.);
+            const double b4 = bp->pow_mode == ORC_POW_SQRT ? (bond_rad * bond_rad) * (bond_rad * bond_rad)
+                                                           : std::pow(bond_rad, 4.);
+            double A_bond = M_PI * b2;
+            double I_bond = M_PI * b4 / 4.0;
             double I_p_bond = I_bond * 2.0;
             double k_n_bond, k_t_bond, k_tor_bond, k_ben_bond;
             if (q & ORC_BQ11_HARDCODED_K) {

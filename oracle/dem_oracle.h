@@ -135,6 +135,7 @@ typedef struct orc_bond_params {
     double radius_factor;   /* bond radius = min(r_i,r_j)*factor (ref: 1)       */
     double kn, kt;          /* explicit stiffnesses when BQ11 is clear          */
     double break_strain;    /* > 0: bond breaks when (rij-L0)/L0 > break_strain */
+    int pow_mode;           /* ORC_POW_LIBM: pow(b,2.), pow(b,4.) as the reference; ORC_POW_SQRT: b*b */
 } orc_bond_params;
 
 /* setupBonds: bond every j != i with rij < factor * rad(i) among the neighbour

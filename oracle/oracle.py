@@ -61,7 +61,7 @@ class _Bonds(C.Structure):
 
 class _BondParams(C.Structure):
     _fields_ = [("quirks", C.c_uint), ("beta", C.c_double), ("radius_factor", C.c_double), ("kn", C.c_double),
-                ("kt", C.c_double), ("break_strain", C.c_double)]
+                ("kt", C.c_double), ("break_strain", C.c_double), ("pow_mode", C.c_int)]
 
 
 _lib = None
@@ -186,10 +186,10 @@ def _bonds(b):
     return c
 
 
-def _bp(bparams):
+def _bp(bparams, pow_mode=POW_LIBM):
     return _BondParams(int(bparams.get("quirks", BOND_REF_COMPAT)), float(bparams.get("beta", 0.1)),
                        float(bparams.get("radius_factor", 1.0)), float(bparams.get("kn", 0.0)),
-                       float(bparams.get("kt", 0.0)), float(bparams.get("break_strain", 0.0)))
+                       float(bparams.get("kt", 0.0)), float(bparams.get("break_strain", 0.0)), int(pow_mode))
 
 
 def setup_bonds(bonds, state, factor, search_cutoff=0.0):
@@ -197,8 +197,9 @@ def setup_bonds(bonds, state, factor, search_cutoff=0.0):
                                  float(search_cutoff))
 
 
-def bonded_run(state, bonds, bparams, dt, nsteps, gravity=(0.0, 0.0, 0.0), ext_force=None, fix_flags=None):
-    p, b, bp = _particles(state), _bonds(bonds), _bp(bparams)
+def bonded_run(state, bonds, bparams, dt, nsteps, gravity=(0.0, 0.0, 0.0), ext_force=None, fix_flags=None,
+               pow_mode=POW_LIBM):
+    p, b, bp = _particles(state), _bonds(bonds), _bp(bparams, pow_mode)
     h = _HookHolder(gravity, ext_force, fix_flags)
     st = 0
     L = lib()
