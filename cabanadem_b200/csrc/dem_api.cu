@@ -36,6 +36,7 @@ struct dem_particles {
     bool dirty = true;       // state changed through set(): list must be rebuilt
     bool mat_dirty = true;   // E, nu, G changed: tables must be rebuilt
     bool has_bonds = false;  // bond slots hold sorted indices: no re-sort from now on
+    bool any_fix = false;    // some particle carries a DEM_FIX_* flag
     std::vector<uint8_t> mat;   // caller order
     std::vector<std::tuple<double, double, double>> mats;
 };
@@ -244,11 +245,12 @@ bool field_layout(const dem_particles *p, int field, long *count, int *esize) {
     }
 }
 
-int host_cur(dem_particles *p) {
-    int cur = 0;
-    cudaMemcpyAsync(&cur, &p->ctl->cur, sizeof(int), cudaMemcpyDeviceToHost, p->ctx->stream);
+int host_cur(dem_particles *p, int *vcur) {
+    int cv[2] = {0, 0};
+    cudaMemcpyAsync(cv, &p->ctl->cur, 2 * sizeof(int), cudaMemcpyDeviceToHost, p->ctx->stream);
     cudaStreamSynchronize(p->ctx->stream);
-    return cur;
+    *vcur = cv[1];
+    return cv[0];
 }
 
 }  // namespace
@@ -294,10 +296,10 @@ static cudaError_t alloc_particles(Particles &P, int n, int mc, int mw, bool pin
     cudaError_t e = cudaSuccess;
     auto A = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
     P.n = n;
-    P.cap = n;
+    P.cap = (n + 63) / 64 * 64;   // component rows of the SoA arrays start 512-byte aligned
     P.mc = mc;
     P.mw = mw;
-    const size_t cap = n;
+    const size_t cap = P.cap;
     for (int b = 0; b < (pingpong ? 2 : 1); ++b) {
         A(dalloc(&P.pos[b], cap));
         A(dalloc(&P.vel[b], 3 * cap));
@@ -314,6 +316,8 @@ static cudaError_t alloc_particles(Particles &P, int n, int mc, int mw, bool pin
     A(dalloc(&P.fix, cap));
     A(dalloc(&P.perm, cap));
     A(dalloc(&P.rank, cap));
+    A(dalloc(&P.vslots, 32 * kVmaxSlots));
+    if (e == cudaSuccess) e = cudaMemset(P.vslots, 0, sizeof(unsigned long long) * 32 * kVmaxSlots);
     P.ext = nullptr;
     return e;
 }
@@ -326,6 +330,7 @@ static void free_particles(Particles &P) {
     }
     cudaFree(P.force); cudaFree(P.torque); cudaFree(P.mI); cudaFree(P.mat); cudaFree(P.cstate);
     cudaFree(P.tidx); cudaFree(P.th); cudaFree(P.sw); cudaFree(P.fix); cudaFree(P.perm); cudaFree(P.rank);
+    cudaFree(P.vslots);
     cudaFree(P.ext);
     P = Particles{};
 }
@@ -348,19 +353,20 @@ extern "C" int dem_particles_create(dem_ctx *ctx, int n, int max_contacts, int m
     }
     cudaStream_t s = ctx->stream;
     const Particles &P = p->P;
+    const size_t cn = (size_t)P.cap;
     for (int b = 0; b < 2; ++b) {
-        cudaMemsetAsync(P.pos[b], 0, sizeof(double4) * n, s);
-        cudaMemsetAsync(P.vel[b], 0, sizeof(double) * 3 * n, s);
-        cudaMemsetAsync(P.omg[b], 0, sizeof(double) * 3 * n, s);
+        cudaMemsetAsync(P.pos[b], 0, sizeof(double4) * cn, s);
+        cudaMemsetAsync(P.vel[b], 0, sizeof(double) * 3 * cn, s);
+        cudaMemsetAsync(P.omg[b], 0, sizeof(double) * 3 * cn, s);
     }
-    cudaMemsetAsync(P.force, 0, sizeof(double) * 3 * n, s);
-    cudaMemsetAsync(P.torque, 0, sizeof(double) * 3 * n, s);
-    cudaMemsetAsync(P.mI, 0, sizeof(double2) * n, s);
-    cudaMemsetAsync(P.mat, 0, n, s);
-    cudaMemsetAsync(P.cstate, 0, sizeof(int) * n, s);
-    cudaMemsetAsync(P.th, 0, sizeof(double) * 3 * std::max(max_contacts, 1) * (size_t)n, s);
-    cudaMemsetAsync(P.sw, 0, sizeof(double) * 3 * std::max(max_walls, 1) * (size_t)n, s);
-    cudaMemsetAsync(P.fix, 0, n, s);
+    cudaMemsetAsync(P.force, 0, sizeof(double) * 3 * cn, s);
+    cudaMemsetAsync(P.torque, 0, sizeof(double) * 3 * cn, s);
+    cudaMemsetAsync(P.mI, 0, sizeof(double2) * cn, s);
+    cudaMemsetAsync(P.mat, 0, cn, s);
+    cudaMemsetAsync(P.cstate, 0, sizeof(int) * cn, s);
+    cudaMemsetAsync(P.th, 0, sizeof(double) * 3 * std::max(max_contacts, 1) * cn, s);
+    cudaMemsetAsync(P.sw, 0, sizeof(double) * 3 * std::max(max_walls, 1) * cn, s);
+    cudaMemsetAsync(P.fix, 0, cn, s);
     cudaMemsetAsync(p->ctl, 0, sizeof(Ctl), s);
     k_init_particles<<<kGS, kTB, 0, s>>>(p->P);
     p->rho.assign(n, 0.0);
@@ -404,7 +410,8 @@ extern "C" int dem_particles_set(dem_particles *p, int field, const void *host, 
     void *tmp = nullptr;
     CK(cudaMalloc(&tmp, (size_t)need * es));
     CK(cudaMemcpyAsync(tmp, host, (size_t)need * es, cudaMemcpyHostToDevice, s));
-    const int cur = host_cur(p);
+    int vcur = 0;
+    const int cur = host_cur(p, &vcur);
     switch (field) {
         case DEM_F_X: k_scatter_pos<<<kGS, kTB, 0, s>>>((double *)tmp, P.pos[cur], n, P.rank, 0); break;
         case DEM_F_RAD: {
@@ -414,8 +421,8 @@ extern "C" int dem_particles_set(dem_particles *p, int field, const void *host, 
             for (int i = 0; i < n; ++i) p->rmax = std::max(p->rmax, r[i]);
             break;
         }
-        case DEM_F_U: k_scatter_d<<<kGS, kTB, 0, s>>>((double *)tmp, P.vel[cur], n, 3, P.cap, P.rank); break;
-        case DEM_F_OMEGA: k_scatter_d<<<kGS, kTB, 0, s>>>((double *)tmp, P.omg[cur], n, 3, P.cap, P.rank); break;
+        case DEM_F_U: k_scatter_d<<<kGS, kTB, 0, s>>>((double *)tmp, P.vel[vcur], n, 3, P.cap, P.rank); break;
+        case DEM_F_OMEGA: k_scatter_d<<<kGS, kTB, 0, s>>>((double *)tmp, P.omg[vcur], n, 3, P.cap, P.rank); break;
         case DEM_F_FORCE: k_scatter_d<<<kGS, kTB, 0, s>>>((double *)tmp, P.force, n, 3, P.cap, P.rank); break;
         case DEM_F_TORQUE: k_scatter_d<<<kGS, kTB, 0, s>>>((double *)tmp, P.torque, n, 3, P.cap, P.rank); break;
         case DEM_F_EXT_FORCE:
@@ -438,7 +445,15 @@ extern "C" int dem_particles_set(dem_particles *p, int field, const void *host, 
                                             P.cap, P.rank);
             k_sw_mask<<<kGS, kTB, 0, s>>>(P);
             break;
-        case DEM_F_FIX: k_scatter_u8<<<kGS, kTB, 0, s>>>((uint8_t *)tmp, P.fix, n, P.rank); break;
+        case DEM_F_FIX: {
+            k_scatter_u8<<<kGS, kTB, 0, s>>>((uint8_t *)tmp, P.fix, n, P.rank);
+            const uint8_t *f = (const uint8_t *)host;
+            bool any = false;
+            for (int i = 0; i < n && !any; ++i) any = f[i] != 0;
+            p->any_fix = any;
+            p->mat_dirty = true;   // re-derive the force constants (has_fix)
+            break;
+        }
     }
     cudaError_t e = cudaGetLastError();
     cudaStreamSynchronize(s);
@@ -470,12 +485,13 @@ extern "C" int dem_particles_get(dem_particles *p, int field, void *host, long c
     }
     void *tmp = nullptr;
     CK(cudaMalloc(&tmp, (size_t)need * es));
-    const int cur = host_cur(p);
+    int vcur = 0;
+    const int cur = host_cur(p, &vcur);
     switch (field) {
         case DEM_F_X: k_gather_pos<<<kGS, kTB, 0, s>>>(P.pos[cur], (double *)tmp, n, P.rank, 0); break;
         case DEM_F_RAD: k_gather_pos<<<kGS, kTB, 0, s>>>(P.pos[cur], (double *)tmp, n, P.rank, 1); break;
-        case DEM_F_U: k_gather_d<<<kGS, kTB, 0, s>>>(P.vel[cur], (double *)tmp, n, 3, P.cap, P.rank); break;
-        case DEM_F_OMEGA: k_gather_d<<<kGS, kTB, 0, s>>>(P.omg[cur], (double *)tmp, n, 3, P.cap, P.rank); break;
+        case DEM_F_U: k_gather_d<<<kGS, kTB, 0, s>>>(P.vel[vcur], (double *)tmp, n, 3, P.cap, P.rank); break;
+        case DEM_F_OMEGA: k_gather_d<<<kGS, kTB, 0, s>>>(P.omg[vcur], (double *)tmp, n, 3, P.cap, P.rank); break;
         case DEM_F_FORCE: k_gather_d<<<kGS, kTB, 0, s>>>(P.force, (double *)tmp, n, 3, P.cap, P.rank); break;
         case DEM_F_TORQUE: k_gather_d<<<kGS, kTB, 0, s>>>(P.torque, (double *)tmp, n, 3, P.cap, P.rank); break;
         case DEM_F_EXT_FORCE: k_gather_d<<<kGS, kTB, 0, s>>>(P.ext, (double *)tmp, n, 3, P.cap, P.rank); break;
@@ -643,7 +659,7 @@ int prepare(dem_solver *s) {
     fc.nmat = nm;
     fc.nwall = nw;
     fc.has_ext = p->P.ext ? 1 : 0;
-    fc.has_fix = 1;
+    fc.has_fix = p->any_fix ? 1 : 0;
     fc.mixed = s->sp.precision == DEM_MIXED ? 1 : 0;
     CK(cudaStreamSynchronize(st));
     s->version++;
@@ -655,10 +671,14 @@ int alloc_lists(dem_solver *s, int maxnb) {
     cudaFree(s->L.nn);
     cudaFree(s->L.idx);
     cudaFree(s->L.defer);
+    cudaFree(s->L.defer_v);
+    cudaFree(s->L.defer_w);
     s->L.maxnb = maxnb;
     CK(dalloc(&s->L.nn, s->p->P.cap));
     CK(dalloc(&s->L.idx, (size_t)maxnb * s->p->P.cap));
     CK(dalloc(&s->L.defer, s->p->P.cap));
+    CK(dalloc(&s->L.defer_v, 3 * (size_t)s->p->P.cap));
+    CK(dalloc(&s->L.defer_w, 3 * (size_t)s->p->P.cap));
     CK(cudaMemsetAsync(s->L.nn, 0, sizeof(int) * s->p->P.cap, ctx->stream));
     s->version++;
     s->built = false;
@@ -786,7 +806,7 @@ extern "C" int dem_solver_destroy(dem_solver *s) {
     cudaStreamSynchronize(s->ctx->stream);
     if (s->graph) cudaGraphExecDestroy(s->graph);
     cudaFree(s->d_pp); cudaFree(s->d_pw); cudaFree(s->d_walls);
-    cudaFree(s->L.nn); cudaFree(s->L.idx); cudaFree(s->L.defer);
+    cudaFree(s->L.nn); cudaFree(s->L.idx); cudaFree(s->L.defer); cudaFree(s->L.defer_v); cudaFree(s->L.defer_w);
     BuildBuffers &B = s->B;
     cudaFree(B.grid); cudaFree(B.key); cudaFree(B.cell_start); cudaFree(B.cell_fill); cudaFree(B.cell_items);
     cudaFree(B.block_sums); cudaFree(B.bbox); cudaFree(B.src); cudaFree(B.dst);

@@ -53,15 +53,15 @@ __global__ void k_bond_setup(Particles P, NbrList L, Bonds B, Ctl *ctl, double f
 __global__ void __launch_bounds__(kBondBlock) k_bond_step(Particles P, Bonds B, Ctl *ctl, ForceConsts fc, BondConsts bc) {
     const CtlSnap cs_ = read_ctl(ctl, true);
     if (!cs_.go) return;
-    const int cur = cs_.cur, nxt = cur ^ 1;
+    const int cur = cs_.cur, nxt = cur ^ 1, vcur = ctl->vcur;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int cap = P.cap;
     double vmax2 = 0.0;
     int status = 0;
     if (i < P.n) {
         const double4 *__restrict__ pc = P.pos[cur];
-        const double *__restrict__ vc = P.vel[cur];
-        const double *__restrict__ wc = P.omg[cur];
+        const double *__restrict__ vc = P.vel[vcur];
+        const double *__restrict__ wc = P.omg[vcur];
         const D4 pi = ld4(pc, i);
         double ui0 = vc[i], ui1 = vc[cap + i], ui2 = vc[2 * cap + i];
         double wi0 = wc[i], wi1 = wc[cap + i], wi2 = wc[2 * cap + i];
@@ -256,7 +256,7 @@ __global__ void __launch_bounds__(kBondBlock) k_bond_step(Particles P, Bonds B, 
             vmax2 = ui0 * ui0 + ui1 * ui1 + ui2 * ui2;
         }
         st4(P.pos[nxt], i, pn);
-        double *vn = P.vel[nxt], *wn = P.omg[nxt];
+        double *vn = P.vel[vcur ^ 1], *wn = P.omg[vcur ^ 1];
         vn[i] = ui0;
         vn[cap + i] = ui1;
         vn[2 * cap + i] = ui2;
@@ -264,7 +264,7 @@ __global__ void __launch_bounds__(kBondBlock) k_bond_step(Particles P, Bonds B, 
         wn[cap + i] = wi1;
         wn[2 * cap + i] = wi2;
     }
-    finish_step(ctl, vmax2, fc.dt, status, true);
+    finish_step(ctl, P.vslots, vmax2, fc.dt, status, true, true);
 }
 
 __global__ void k_bond_broken_count(Bonds B, int n, unsigned long long *out) {

@@ -2,9 +2,10 @@
 // translation units of libb200dem.so.
 //
 // HBM layout (particles in Morton-sorted order, capacity `cap` = n):
-//   pos[2]    double4 (x, y, z, r)      ping-pong; neighbour gathers read one 32 B sector
-//   vel[2]    double  [3][cap]           ping-pong SoA (ux | uy | uz)
-//   omg[2]    double  [3][cap]           ping-pong SoA
+//   pos[2]    double4 (x, y, z, r)      ping-pong (Ctl::cur); neighbour gathers read one 32 B sector
+//   vel[2]    double  [3][cap]           SoA (ux | uy | uz); current buffer Ctl::vcur.  The
+//   omg[2]    double  [3][cap]           contact step updates them in place (see dem_step.cu);
+//                                        the bonded step and re-sorting use the second buffer
 //   force, torque double [3][cap]        written by the last fused step / unfused force pass
 //   mI        double2 (m, I)
 //   mat       uint8 material id          (E, nu, G) deduplicated into pair tables
@@ -24,7 +25,8 @@ constexpr int kMaxWalls = 24;
 constexpr int kMaxMat = 32;
 
 struct Ctl {
-    int cur;                  // current ping-pong buffer
+    int cur;                  // current position buffer
+    int vcur;                 // current velocity / angular-velocity buffer
     int steps_done;           // fused steps executed in the current run
     int target;               // fused steps requested in the current run
     unsigned ticket;          // last-block election
@@ -53,7 +55,10 @@ struct Particles {
     uint8_t *fix;
     double *ext;   // may be null
     int *perm, *rank;
+    unsigned long long *vslots;   // kVmaxSlots x 32 words: per-step max |u|^2, spread over L2 lines
 };
+
+constexpr int kVmaxSlots = 32;   // blocks fold their max into slot blockIdx % 32 (word 32 * slot)
 
 struct PairConst {   // per (material a, material b) or (material a, wall w)
     double c_kn;     // 4./3. * E_eff            (Force.hpp:203, :568)
@@ -86,6 +91,7 @@ struct NbrList {
     int *idx;    // [maxnb][cap] sorted indices, ascending caller id
     int maxnb;
     int *defer;  // [cap] particles deferred to the contact kernel in the current step
+    double *defer_v, *defer_w;  // [3][cap] new u, omega of deferred particle t (slot t)
 };
 
 struct Grid {                 // computed on the device at every build

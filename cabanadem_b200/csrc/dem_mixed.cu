@@ -19,34 +19,29 @@ __global__ void __launch_bounds__(kBlock) k_contact_mixed(Particles P, NbrList L
     if (ctl->steps_done >= ctl->target || (ctl->status & DEM_ERR_NEIGHBOR_OVERFLOW) || !(ctl->disp < ctl->half_skin))
         return;
     const int nd = ctl->ndefer;
-    if ((long)blockIdx.x * blockDim.x >= nd) {
-        finish_step_idle(ctl, fc.dt);
-        return;
-    }
-    CtlSnap cs_;
-    cs_.cur = ctl->cur;
-    cs_.last = ctl->steps_done + 1 >= ctl->target;
+    if ((long)blockIdx.x * blockDim.x >= nd) return;
+    const int cur = ctl->cur, vcur = ctl->vcur;
+    const int last = ctl->steps_done + 1 >= ctl->target;
     double vmax2 = 0.0;
     int status = 0;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nd; t += gridDim.x * blockDim.x) {
         double v2 = 0.0;
-        particle_full<MODE_FUSED, true>(P, L, fc, pp, pw, walls, cs_.cur, cs_.cur ^ 1, cs_.last, L.defer[t], v2,
-                                        status);
+        particle_full<MODE_FUSED, true>(P, L, fc, pp, pw, walls, cur, cur ^ 1, vcur, last, L.defer[t], t, v2, status);
         vmax2 = fmax(vmax2, v2);
     }
-    finish_step(ctl, vmax2, fc.dt, status, true);
+    block_vmax(ctl, P.vslots, vmax2, status);
 }
 
 __global__ void __launch_bounds__(kBlock) k_force_mixed(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
                                                         const PairConst *__restrict__ pp,
                                                         const PairConst *__restrict__ pw,
                                                         const WallGeom *__restrict__ walls) {
-    const CtlSnap cs_ = read_ctl(ctl, false);
-    if (!cs_.go) return;
+    if (ctl->status & DEM_ERR_NEIGHBOR_OVERFLOW) return;
+    const int cur = ctl->cur, vcur = ctl->vcur;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double vmax2 = 0.0;
     int status = 0;
-    if (i < P.n) particle_full<MODE_FORCE_ONLY, true>(P, L, fc, pp, pw, walls, cs_.cur, cs_.cur ^ 1, 1, i, vmax2, status);
+    if (i < P.n) particle_full<MODE_FORCE_ONLY, true>(P, L, fc, pp, pw, walls, cur, cur ^ 1, vcur, 1, i, 0, vmax2, status);
     if (status) atomicOr(&ctl->status, status);
 }
 

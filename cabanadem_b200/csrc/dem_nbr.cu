@@ -246,13 +246,13 @@ __global__ void k_make_dst(int n, const int *items, int *dst) {
 }
 
 __global__ void k_permute(Particles P, Particles A, const Ctl *ctl, const int *items, const int *dst) {
-    const int n = P.n, cap = P.cap, cur = ctl->cur, nxt = cur ^ 1;
+    const int n = P.n, cap = P.cap, cur = ctl->cur, nxt = cur ^ 1, vcur = ctl->vcur, vnxt = vcur ^ 1;
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
         const int q = items[p];
         reinterpret_cast<D4 *>(P.pos[nxt])[p] = ld4(P.pos[cur], q);
         for (int d = 0; d < 3; ++d) {
-            P.vel[nxt][d * cap + p] = P.vel[cur][d * cap + q];
-            P.omg[nxt][d * cap + p] = P.omg[cur][d * cap + q];
+            P.vel[vnxt][d * cap + p] = P.vel[vcur][d * cap + q];
+            P.omg[vnxt][d * cap + p] = P.omg[vcur][d * cap + q];
             A.force[d * cap + p] = P.force[d * cap + q];
             A.torque[d * cap + p] = P.torque[d * cap + q];
             if (P.ext) A.ext[d * cap + p] = P.ext[d * cap + q];
@@ -278,7 +278,10 @@ __global__ void k_identity(int n, int *items) {
 }
 
 __global__ void k_flip(Ctl *ctl) {
-    if (threadIdx.x == 0) ctl->cur ^= 1;
+    if (threadIdx.x == 0) {
+        ctl->cur ^= 1;
+        ctl->vcur ^= 1;
+    }
 }
 
 __global__ void __launch_bounds__(128) k_list(Particles P, NbrList L, Ctl *ctl, const Grid *g, const int *start,

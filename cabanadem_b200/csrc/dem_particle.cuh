@@ -13,7 +13,11 @@ namespace b200dem {
 namespace {
 
 constexpr int kBlock = 128;
-constexpr int kStreamBlock = 256;
+#ifndef STREAM_BLOCK
+#define STREAM_BLOCK 128   // small blocks: a warp stuck on a neighbour loop holds fewer others
+#endif
+constexpr int kStreamBlock = STREAM_BLOCK;
+constexpr int kApplyBlock = 256;
 
 struct __align__(32) D4 {
     double x, y, z, w;
@@ -53,24 +57,13 @@ __device__ __forceinline__ D4 ld4_early(const double4 *p, int i) {
     return r;
 }
 
-// Last-block election without a block barrier, for a block that has no work: it adds no
-// vmax or status, only its ticket; the last ticket finalises the step.
-__device__ __forceinline__ void finish_step_idle(Ctl *ctl, double dt) {
-    if (threadIdx.x != 0) return;
-    __threadfence();
-    const unsigned t = atomicAdd(&ctl->ticket, 1u);
-    if (t == gridDim.x - 1) {
-        __threadfence();
-        const double v2 = __longlong_as_double((long long)atomicAdd(&ctl->vmax2, 0ull));
-        ctl->disp = ctl->disp + dt * sqrt(v2) * (1.0 + 1e-9);
-        ctl->vmax2 = 0ull;
-        ctl->ndefer = 0;
-        ctl->cur ^= 1;
-        ctl->steps_done += 1;
-        ctl->total_steps += 1;
-        __threadfence();
-        ctl->ticket = 0u;
-    }
+// L2 prefetch of a contiguous range with the TMA bulk-prefetch instruction (no registers,
+// no completion to wait for).  The range is clipped to 16-byte granules inside [p, p+bytes).
+__device__ __forceinline__ void prefetch_l2(const void *p, long bytes) {
+    const unsigned long long a = (unsigned long long)p;
+    const unsigned long long a0 = (a + 15ull) & ~15ull;
+    const unsigned long long e = (a + (unsigned long long)bytes) & ~15ull;
+    if (e > a0) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a0), "r"((unsigned)(e - a0)) : "memory");
 }
 
 struct CtlSnap {
@@ -98,10 +91,26 @@ __device__ __forceinline__ CtlSnap read_ctl(const Ctl *ctl, bool gated) {
     return s;
 }
 
-// Block max of |u|^2, then the last block to finish advances the control word:
-// disp += dt*|u|max (conservative displacement bound), flips the ping-pong buffer.
-__device__ __forceinline__ void finish_step(Ctl *ctl, double vmax2, double dt, int status, bool count_step) {
-    __shared__ double red[kBlock / 32];
+__device__ __forceinline__ void vmax_fold(unsigned long long *slots, double m) {
+    if (m > 0.0) atomicMax(&slots[(blockIdx.x % kVmaxSlots) * 32], (unsigned long long)__double_as_longlong(m));
+}
+
+// Max over the slots, clearing them for the next step (called by one thread).
+__device__ __forceinline__ double vmax_collect(unsigned long long *slots) {
+    unsigned long long m = 0ull;
+    for (int s = 0; s < kVmaxSlots; ++s) {
+        const unsigned long long v = atomicExch(&slots[s * 32], 0ull);
+        m = v > m ? v : m;
+    }
+    return __longlong_as_double((long long)m);
+}
+
+// Block max of |u|^2 folded into its slot, then the last block to finish advances the
+// control word: disp += dt*|u|max (conservative displacement bound), flips the position
+// buffer (and the velocity buffer when the kernel wrote the other one).
+__device__ __forceinline__ void finish_step(Ctl *ctl, unsigned long long *slots, double vmax2, double dt, int status,
+                                            bool count_step, bool flip_v = false) {
+    __shared__ double red[32];
     __shared__ bool am_last;
     for (int o = 16; o > 0; o >>= 1) vmax2 = fmax(vmax2, __shfl_xor_sync(0xffffffffu, vmax2, o));
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -110,8 +119,8 @@ __device__ __forceinline__ void finish_step(Ctl *ctl, double vmax2, double dt, i
     __syncthreads();
     if (threadIdx.x == 0) {
         double m = red[0];
-        for (int w = 1; w < kBlock / 32; ++w) m = fmax(m, red[w]);
-        atomicMax(&ctl->vmax2, (unsigned long long)__double_as_longlong(m));
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, red[w]);
+        vmax_fold(slots, m);
         __threadfence();
         const unsigned t = atomicAdd(&ctl->ticket, 1u);
         am_last = (t == gridDim.x - 1);
@@ -119,11 +128,11 @@ __device__ __forceinline__ void finish_step(Ctl *ctl, double vmax2, double dt, i
     __syncthreads();
     if (am_last && threadIdx.x == 0) {
         __threadfence();
-        const double v2 = __longlong_as_double((long long)atomicAdd(&ctl->vmax2, 0ull));
+        const double v2 = vmax_collect(slots);
         ctl->disp = ctl->disp + dt * sqrt(v2) * (1.0 + 1e-9);
-        ctl->vmax2 = 0ull;
         ctl->ndefer = 0;
         ctl->cur ^= 1;
+        if (flip_v) ctl->vcur ^= 1;
         if (count_step) {
             ctl->steps_done += 1;
             ctl->total_steps += 1;
@@ -132,6 +141,21 @@ __device__ __forceinline__ void finish_step(Ctl *ctl, double vmax2, double dt, i
         ctl->ticket = 0u;
     }
 }
+
+// Fold the block's largest |u|^2 into its slot (and OR its status bits).
+__device__ __forceinline__ void block_vmax(Ctl *ctl, unsigned long long *slots, double vmax2, int status) {
+    __shared__ double red[32];
+    for (int o = 16; o > 0; o >>= 1) vmax2 = fmax(vmax2, __shfl_xor_sync(0xffffffffu, vmax2, o));
+    if (status) atomicOr(&ctl->status, status);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = vmax2;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = red[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, red[w]);
+        vmax_fold(slots, m);
+    }
+}
+
 
 // ---------------------------------------------------------------------------------------
 // Full per-particle step (contact compaction, pp and wall forces, hooks, integration).
@@ -142,12 +166,13 @@ template <int MODE, bool MIXED>
 __device__ __forceinline__ void particle_full(const Particles &P, const NbrList &L, const ForceConsts &fc,
                                               const PairConst *__restrict__ pp, const PairConst *__restrict__ pw,
                                               const WallGeom *__restrict__ walls, const int cur, const int nxt,
-                                              const int last, const int i, double &vmax2, int &status) {
+                                              const int vcur, const int last, const int i, const int slot,
+                                              double &vmax2, int &status) {
     const int cap = P.cap;
     const unsigned q = fc.quirks;
     const double4 *__restrict__ pc = P.pos[cur];
-    const double *__restrict__ vc = P.vel[cur];
-    const double *__restrict__ wc = P.omg[cur];
+    const double *__restrict__ vc = P.vel[vcur];
+    const double *__restrict__ wc = P.omg[vcur];
     const D4 pi = ld4(pc, i);
     double ui0 = vc[i], ui1 = vc[cap + i], ui2 = vc[2 * cap + i];
     double wi0 = wc[i], wi1 = wc[cap + i], wi2 = wc[2 * cap + i];
@@ -640,14 +665,16 @@ __device__ __forceinline__ void particle_full(const Particles &P, const NbrList 
             pn.z += fc.dt * ui2;
             vmax2 = ui0 * ui0 + ui1 * ui1 + ui2 * ui2;
         }
+        // positions go to the next buffer; u and omega to this particle's scratch slot,
+        // committed by the apply kernel once no thread reads the current values any more
         st4(P.pos[nxt], i, pn);
-        double *vn = P.vel[nxt], *wn = P.omg[nxt];
-        vn[i] = ui0;
-        vn[cap + i] = ui1;
-        vn[2 * cap + i] = ui2;
-        wn[i] = wi0;
-        wn[cap + i] = wi1;
-        wn[2 * cap + i] = wi2;
+        double *vn = L.defer_v, *wn = L.defer_w;
+        vn[slot] = ui0;
+        vn[cap + slot] = ui1;
+        vn[2 * cap + slot] = ui2;
+        wn[slot] = wi0;
+        wn[cap + slot] = wi1;
+        wn[2 * cap + slot] = wi2;
     }
     }
 

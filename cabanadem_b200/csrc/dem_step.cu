@@ -19,56 +19,78 @@
 
 namespace b200dem {
 
-template <int MODE>
-__global__ void __launch_bounds__(kBlock) k_step(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
-                                                 const PairConst *__restrict__ pp, const PairConst *__restrict__ pw,
-                                                 const WallGeom *__restrict__ walls) {
-    const CtlSnap cs_ = read_ctl(ctl, MODE == MODE_FUSED);
-    if (!cs_.go) return;
+// Unfused force pass (MODE_FORCE_ONLY): F and tau written in place.
+__global__ void __launch_bounds__(kBlock) k_force(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
+                                                  const PairConst *__restrict__ pp, const PairConst *__restrict__ pw,
+                                                  const WallGeom *__restrict__ walls) {
+    if (ctl->status & DEM_ERR_NEIGHBOR_OVERFLOW) return;
+    const int cur = ctl->cur, vcur = ctl->vcur;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double vmax2 = 0.0;
     int status = 0;
-    if (i < P.n) particle_full<MODE, false>(P, L, fc, pp, pw, walls, cs_.cur, cs_.cur ^ 1, cs_.last, i, vmax2, status);
-    if (MODE == MODE_FUSED) {
-        finish_step(ctl, vmax2, fc.dt, status, true);
-    } else if (status) {
-        atomicOr(&ctl->status, status);
-    }
+    if (i < P.n)
+        particle_full<MODE_FORCE_ONLY, false>(P, L, fc, pp, pw, walls, cur, cur ^ 1, vcur, 1, i, 0, vmax2, status);
+    if (status) atomicOr(&ctl->status, status);
+}
+
+__device__ __forceinline__ bool step_gate(const Ctl *ctl) {
+    return ctl->steps_done < ctl->target && !(ctl->status & DEM_ERR_NEIGHBOR_OVERFLOW) && ctl->disp < ctl->half_skin;
 }
 
 // ---------------------------------------------------------------------------------------
-// Fused step, part 1: streaming kernel.  A particle with no tracked contact, no active
-// wall history, no neighbour within r_i + r_j (1 + 5e-11) and no wall overlap has zero
-// pair force; its step reduces to hooks + integration, done here with few registers so
-// the kernel runs at high occupancy.  Every other particle is appended to L.defer and
-// handled by the contact kernel with the full arithmetic.  Persistent grid-stride loop;
-// each thread reads the control word itself (no block barrier before the work).
+// Fused step, kernel 1 of 3: streaming.  A particle with no tracked contact, no active wall
+// history, no neighbour within r_i + r_j (1 + 5e-11) and no wall overlap has zero pair
+// force and zero torque.  Its step is then: hooks, velocity half-kicks and drift -- done
+// here with few registers so that the kernel runs at high occupancy.  Its angular
+// velocity is unchanged (tau = 0), so omega is neither read nor written, and u is updated
+// in place (no other thread reads the velocity of a particle without contacts: the pair
+// terms that read a partner's velocity only run for overlapping pairs, and both partners
+// of such a pair are deferred).  Positions still go to the next buffer because every
+// neighbour reads them.  Every other particle is appended to L.defer for kernel 2.
+// Each thread reads the control word itself (no block barrier before the work).
 // ---------------------------------------------------------------------------------------
 #ifndef STREAM_MIN_BLOCKS
-#define STREAM_MIN_BLOCKS 1
+#define STREAM_MIN_BLOCKS 10  // <= 48 registers: 10 blocks of 128 per SM (B200 sweep of block size
+                              // 64/128/256 and 4..16 blocks: 128 x 10 fastest on the 2M lattice)
 #endif
-__global__ void __launch_bounds__(kStreamBlock, STREAM_MIN_BLOCKS) k_stream(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
-                                                        const WallGeom *__restrict__ walls) {
-    const int cur = ctl->cur;
-    const bool stale = !(ctl->disp < ctl->half_skin);
-    const int steps_done = ctl->steps_done, target = ctl->target;
-    if (steps_done >= target || (ctl->status & DEM_ERR_NEIGHBOR_OVERFLOW) || stale) return;
-    const bool last = steps_done + 1 >= target;
+__global__ void __launch_bounds__(kStreamBlock, STREAM_MIN_BLOCKS) k_stream(Particles P, NbrList L, Ctl *ctl,
+                                                                           ForceConsts fc,
+                                                                           const WallGeom *__restrict__ walls) {
+    if (!step_gate(ctl)) return;
+    const int cur = ctl->cur, vcur = ctl->vcur;
+    const bool last = ctl->steps_done + 1 >= ctl->target;
     const int nxt = cur ^ 1, cap = P.cap;
     const double4 *__restrict__ pc = P.pos[cur];
-    const double *__restrict__ vc = P.vel[cur];
-    const double *__restrict__ wc = P.omg[cur];
+    double *vc = P.vel[vcur];
     double vmax2 = 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += gridDim.x * blockDim.x) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < P.n) {
         // all own-state loads first (one memory round trip per particle)
         const D4 pi = ld4_early(pc, i);
         const int cs = ld_early_i(P.cstate + i);
         const int nn = ld_early_i(L.nn + i);
-        const double2 mIi = ld_early2(P.mI + i);
+        const double m = ld_early(&P.mI[i].x);
         double ui0 = ld_early(vc + i), ui1 = ld_early(vc + cap + i), ui2 = ld_early(vc + 2 * cap + i);
-        double wi0 = ld_early(wc + i), wi1 = ld_early(wc + cap + i), wi2 = ld_early(wc + 2 * cap + i);
+        // the first two list slots are read with the own state (in bounds for every i; the
+        // value is only used below the list length), so that most warps need one more
+        // round trip (the partners' positions) instead of two per neighbour
+        const int j0 = L.maxnb > 0 ? ld_early_i(L.idx + i) : 0;
+        const int j1 = L.maxnb > 1 ? ld_early_i(L.idx + cap + i) : 0;
         bool defer = cs != 0;
-        for (int kk = 0; kk < nn && !defer; ++kk) {
+        if (!defer && nn > 0) {
+            const D4 pa = ld4(pc, j0);
+            D4 pb = pa;
+            if (nn > 1) pb = ld4(pc, j1);
+            const double ax = pi.x - pa.x, ay = pi.y - pa.y, az = pi.z - pa.z;
+            const double sa = pi.w + pa.w;
+            defer = !(ax * ax + ay * ay + az * az >= sa * sa * 1.0000000001);
+            if (nn > 1) {
+                const double bx = pi.x - pb.x, by = pi.y - pb.y, bz = pi.z - pb.z;
+                const double sb = pi.w + pb.w;
+                defer = defer || !(bx * bx + by * by + bz * bz >= sb * sb * 1.0000000001);
+            }
+        }
+        for (int kk = 2; kk < nn && !defer; ++kk) {
             const int j = L.idx[(long)kk * cap + i];
             const D4 pj = ld4(pc, j);
             const double px = pi.x - pj.x, py = pi.y - pj.y, pz = pi.z - pj.z;
@@ -89,117 +111,127 @@ __global__ void __launch_bounds__(kStreamBlock, STREAM_MIN_BLOCKS) k_stream(Part
             if (lane == leader) base = atomicAdd(&ctl->ndefer, __popc(dmask));
             base = __shfl_sync(dmask, base, leader);
             L.defer[base + __popc(dmask & ((1u << lane) - 1u))] = i;
-            continue;
-        }
-        // no pair force: F = ext (added to zero), then the post-force hooks
-        double F0 = 0., F1 = 0., F2 = 0., T0 = 0., T1 = 0., T2 = 0.;
-        if (fc.has_ext) {
-            F0 += P.ext[i];
-            F1 += P.ext[cap + i];
-            F2 += P.ext[2 * cap + i];
-        }
-        if (fc.has_gravity) {
-            F0 += mIi.x * fc.g[0];
-            F1 += mIi.x * fc.g[1];
-            F2 += mIi.x * fc.g[2];
-        }
-        if (fc.has_fix) {
-            const int f = P.fix[i];
-            if (f & DEM_FIX_FORCE) F0 = F1 = F2 = 0.;
-            if (f & DEM_FIX_TORQUE) T0 = T1 = T2 = 0.;
-        }
-        const double m_inverse = 1. / mIi.x;
-        const double I_inverse = 1. / mIi.y;
-        const double h = fc.half_dt;
-        ui0 += h * F0 * m_inverse;
-        ui1 += h * F1 * m_inverse;
-        ui2 += h * F2 * m_inverse;
-        wi0 += h * T0 * I_inverse;
-        wi1 += h * T1 * I_inverse;
-        wi2 += h * T2 * I_inverse;
-        D4 pn = pi;
-        if (last) {
-            P.force[i] = F0;
-            P.force[cap + i] = F1;
-            P.force[2 * cap + i] = F2;
-            P.torque[i] = T0;
-            P.torque[cap + i] = T1;
-            P.torque[2 * cap + i] = T2;
         } else {
+            // no pair force: F = ext (added to zero), then the post-force hooks; tau = 0
+            double F0 = 0., F1 = 0., F2 = 0.;
+            if (fc.has_ext) {
+                F0 += P.ext[i];
+                F1 += P.ext[cap + i];
+                F2 += P.ext[2 * cap + i];
+            }
+            if (fc.has_gravity) {
+                F0 += m * fc.g[0];
+                F1 += m * fc.g[1];
+                F2 += m * fc.g[2];
+            }
+            if (fc.has_fix && (P.fix[i] & DEM_FIX_FORCE)) F0 = F1 = F2 = 0.;
+            const double m_inverse = 1. / m;
+            const double h = fc.half_dt;
             ui0 += h * F0 * m_inverse;
             ui1 += h * F1 * m_inverse;
             ui2 += h * F2 * m_inverse;
-            wi0 += h * T0 * I_inverse;
-            wi1 += h * T1 * I_inverse;
-            wi2 += h * T2 * I_inverse;
-            pn.x += fc.dt * ui0;
-            pn.y += fc.dt * ui1;
-            pn.z += fc.dt * ui2;
-            vmax2 = fmax(vmax2, ui0 * ui0 + ui1 * ui1 + ui2 * ui2);
+            D4 pn = pi;
+            if (last) {
+                P.force[i] = F0;
+                P.force[cap + i] = F1;
+                P.force[2 * cap + i] = F2;
+                P.torque[i] = 0.;
+                P.torque[cap + i] = 0.;
+                P.torque[2 * cap + i] = 0.;
+            } else {
+                ui0 += h * F0 * m_inverse;
+                ui1 += h * F1 * m_inverse;
+                ui2 += h * F2 * m_inverse;
+                pn.x += fc.dt * ui0;
+                pn.y += fc.dt * ui1;
+                pn.z += fc.dt * ui2;
+                vmax2 = ui0 * ui0 + ui1 * ui1 + ui2 * ui2;
+            }
+            st4(P.pos[nxt], i, pn);
+            vc[i] = ui0;
+            vc[cap + i] = ui1;
+            vc[2 * cap + i] = ui2;
         }
-        st4(P.pos[nxt], i, pn);
-        double *vn = P.vel[nxt], *wn = P.omg[nxt];
-        vn[i] = ui0;
-        vn[cap + i] = ui1;
-        vn[2 * cap + i] = ui2;
-        wn[i] = wi0;
-        wn[cap + i] = wi1;
-        wn[2 * cap + i] = wi2;
     }
-    // one atomic per block
-    __shared__ double red[kStreamBlock / 32];
-    for (int o = 16; o > 0; o >>= 1) vmax2 = fmax(vmax2, __shfl_xor_sync(0xffffffffu, vmax2, o));
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = vmax2;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double m = red[0];
-        for (int w = 1; w < kStreamBlock / 32; ++w) m = fmax(m, red[w]);
-        if (m > 0.0) atomicMax(&ctl->vmax2, (unsigned long long)__double_as_longlong(m));
-    }
+    block_vmax(ctl, P.vslots, vmax2, 0);
 }
 
-// Fused step, part 2: the full arithmetic for the deferred particles, then the last block
-// finalises the step (displacement bound, buffer flip, step counter, list reset).
+// Fused step, kernel 2 of 3: the full arithmetic for the deferred particles.  New u and
+// omega go to scratch slot t (their current values are still read by contact partners).
 __global__ void __launch_bounds__(kBlock) k_contact(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
                                                     const PairConst *__restrict__ pp, const PairConst *__restrict__ pw,
                                                     const WallGeom *__restrict__ walls) {
-    // gate read by every thread (no barrier); a block with no deferred particle only votes
-    if (ctl->steps_done >= ctl->target || (ctl->status & DEM_ERR_NEIGHBOR_OVERFLOW) || !(ctl->disp < ctl->half_skin))
-        return;
+    if (!step_gate(ctl)) return;
     const int nd = ctl->ndefer;
-    if ((long)blockIdx.x * blockDim.x >= nd) {
-        finish_step_idle(ctl, fc.dt);
-        return;
-    }
-    CtlSnap cs_;
-    cs_.cur = ctl->cur;
-    cs_.last = ctl->steps_done + 1 >= ctl->target;
+    if ((long)blockIdx.x * blockDim.x >= nd) return;
+    const int cur = ctl->cur, vcur = ctl->vcur;
+    const int last = ctl->steps_done + 1 >= ctl->target;
     double vmax2 = 0.0;
     int status = 0;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nd; t += gridDim.x * blockDim.x) {
         double v2 = 0.0;
-        particle_full<MODE_FUSED, false>(P, L, fc, pp, pw, walls, cs_.cur, cs_.cur ^ 1, cs_.last, L.defer[t], v2, status);
+        particle_full<MODE_FUSED, false>(P, L, fc, pp, pw, walls, cur, cur ^ 1, vcur, last, L.defer[t], t, v2,
+                                         status);
         vmax2 = fmax(vmax2, v2);
     }
-    finish_step(ctl, vmax2, fc.dt, status, true);
+    block_vmax(ctl, P.vslots, vmax2, status);
+}
+
+// Fused step, kernel 3 of 3: commit the deferred particles' u and omega, then the last
+// block to take a ticket finalises the step (displacement bound, position-buffer flip,
+// step counter, deferred-list reset).  Each block copies ndefer before its ticket, so the
+// reset cannot cut another block's copy short.
+__global__ void __launch_bounds__(kApplyBlock) k_apply(Particles P, NbrList L, Ctl *ctl, ForceConsts fc) {
+    __shared__ int s_nd, s_go;
+    if (threadIdx.x == 0) {
+        s_go = step_gate(ctl);
+        s_nd = ctl->ndefer;
+    }
+    __syncthreads();
+    if (!s_go) return;
+    const int nd = s_nd, cap = P.cap, vcur = ctl->vcur;
+    double *vc = P.vel[vcur], *wc = P.omg[vcur];
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nd; t += gridDim.x * blockDim.x) {
+        const int i = L.defer[t];
+        for (int d = 0; d < 3; ++d) {
+            vc[d * cap + i] = L.defer_v[d * cap + t];
+            wc[d * cap + i] = L.defer_w[d * cap + t];
+        }
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned tk = atomicAdd(&ctl->ticket, 1u);
+        if (tk == gridDim.x - 1) {
+            __threadfence();
+            const double v2 = vmax_collect(P.vslots);
+            ctl->disp = ctl->disp + fc.dt * sqrt(v2) * (1.0 + 1e-9);
+            ctl->ndefer = 0;
+            ctl->cur ^= 1;
+            ctl->steps_done += 1;
+            ctl->total_steps += 1;
+            __threadfence();
+            ctl->ticket = 0u;
+        }
+    }
 }
 
 // Prologue of a run: stage1 + stage2 of its first step with the stored F, tau
-// (src/CabanaDEM_Integrator.hpp:31-74).  Writes the next buffer and flips.
+// (src/CabanaDEM_Integrator.hpp:31-74).  u and omega in place; positions to the next
+// buffer, which becomes current.
 __global__ void __launch_bounds__(kBlock) k_prologue(Particles P, Ctl *ctl, ForceConsts fc) {
-    const CtlSnap cs_ = read_ctl(ctl, false);
-    const int cur = cs_.cur, nxt = cur ^ 1;
+    const int cur = ctl->cur, nxt = cur ^ 1, vcur = ctl->vcur;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int cap = P.cap;
     double vmax2 = 0.0;
     if (i < P.n) {
         const double2 mIi = P.mI[i];
         const double m_inverse = 1. / mIi.x, I_inverse = 1. / mIi.y, h = fc.half_dt;
-        const double *vc = P.vel[cur], *wc = P.omg[cur];
-        double u[3], w[3];
+        double *vc = P.vel[vcur], *wc = P.omg[vcur];
+        double u[3];
         for (int d = 0; d < 3; ++d) {
             u[d] = vc[d * cap + i] + h * P.force[d * cap + i] * m_inverse;
-            w[d] = wc[d * cap + i] + h * P.torque[d * cap + i] * I_inverse;
+            vc[d * cap + i] = u[d];
+            wc[d * cap + i] = wc[d * cap + i] + h * P.torque[d * cap + i] * I_inverse;
         }
         D4 p = ld4(P.pos[cur], i);
         p.x += fc.dt * u[0];
@@ -207,32 +239,29 @@ __global__ void __launch_bounds__(kBlock) k_prologue(Particles P, Ctl *ctl, Forc
         p.z += fc.dt * u[2];
         vmax2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
         st4(P.pos[nxt], i, p);
-        for (int d = 0; d < 3; ++d) {
-            P.vel[nxt][d * cap + i] = u[d];
-            P.omg[nxt][d * cap + i] = w[d];
-        }
     }
-    finish_step(ctl, vmax2, fc.dt, 0, false);
+    finish_step(ctl, P.vslots, vmax2, fc.dt, 0, false);
 }
 
 // Unfused Integrator stages, in place on the current buffer.
 __global__ void k_stage(Particles P, Ctl *ctl, ForceConsts fc, int stage) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.n) return;
-    const int cur = ctl->cur, cap = P.cap;
+    const int cur = ctl->cur, vcur = ctl->vcur, cap = P.cap;
+    double *vc = P.vel[vcur], *wc = P.omg[vcur];
     if (stage == 2) {
         D4 p = ld4(P.pos[cur], i);
-        p.x += fc.dt * P.vel[cur][i];
-        p.y += fc.dt * P.vel[cur][cap + i];
-        p.z += fc.dt * P.vel[cur][2 * cap + i];
+        p.x += fc.dt * vc[i];
+        p.y += fc.dt * vc[cap + i];
+        p.z += fc.dt * vc[2 * cap + i];
         st4(P.pos[cur], i, p);
         return;
     }
     const double2 mIi = P.mI[i];
     const double m_inverse = 1. / mIi.x, I_inverse = 1. / mIi.y, h = fc.half_dt;
     for (int d = 0; d < 3; ++d) {
-        P.vel[cur][d * cap + i] += h * P.force[d * cap + i] * m_inverse;
-        P.omg[cur][d * cap + i] += h * P.torque[d * cap + i] * I_inverse;
+        vc[d * cap + i] += h * P.force[d * cap + i] * m_inverse;
+        wc[d * cap + i] += h * P.torque[d * cap + i] * I_inverse;
     }
 }
 
@@ -241,15 +270,16 @@ __global__ void k_stage(Particles P, Ctl *ctl, ForceConsts fc, int stage) {
 __global__ void __launch_bounds__(kBlock) k_energy_partials(Particles P, NbrList L, ForceConsts fc,
                                                             const PairConst *__restrict__ pp,
                                                             const PairConst *__restrict__ pw,
-                                                            const WallGeom *__restrict__ walls, int cur,
+                                                            const WallGeom *__restrict__ walls, const Ctl *ctl,
                                                             double *partials) {
+    const int cur = ctl->cur, vcur = ctl->vcur;
     __shared__ double red[4][kBlock];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int cap = P.cap;
     double e[4] = {0., 0., 0., 0.};
     if (i < P.n) {
         const double2 mIi = P.mI[i];
-        const double *vc = P.vel[cur], *wc = P.omg[cur];
+        const double *vc = P.vel[vcur], *wc = P.omg[vcur];
         const double u0 = vc[i], u1 = vc[cap + i], u2 = vc[2 * cap + i];
         const double w0 = wc[i], w1 = wc[cap + i], w2 = wc[2 * cap + i];
         e[0] = 0.5 * mIi.x * (u0 * u0 + u1 * u1 + u2 * u2);
@@ -302,7 +332,7 @@ void launch_prologue(const Particles &P, Ctl *ctl, const ForceConsts &fc, cudaSt
     k_prologue<<<nblocks(P.n), kBlock, 0, s>>>(P, ctl, fc);
 }
 
-int kernels_per_step() { return 2; }
+int kernels_per_step() { return 3; }
 
 static int persistent_blocks(const void *kernel, int block, int n) {
     static int sms = 0;
@@ -322,22 +352,23 @@ static int persistent_blocks(const void *kernel, int block, int n) {
 void launch_step(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
                  const PairConst *pw, const WallGeom *walls, int mode, cudaStream_t s) {
     if (mode == MODE_FUSED) {
-        static int gs = 0, gc = 0, gm = 0, last_n = -1;
+        static int gc = 0, gm = 0, ga = 0, last_n = -1;
         if (last_n != P.n) {
-            gs = persistent_blocks((const void *)k_stream, kStreamBlock, P.n);
             gc = persistent_blocks((const void *)k_contact, kBlock, P.n);
             gm = persistent_blocks(contact_mixed_kernel(), kBlock, P.n);
+            ga = 148;   // few deferred particles in the common case, one ticket per block
             last_n = P.n;
         }
-        k_stream<<<gs, kStreamBlock, 0, s>>>(P, L, ctl, fc, walls);
+        k_stream<<<(P.n + kStreamBlock - 1) / kStreamBlock, kStreamBlock, 0, s>>>(P, L, ctl, fc, walls);
         if (fc.mixed)
             launch_contact_mixed(P, L, ctl, fc, pp, pw, walls, gm, s);
         else
             k_contact<<<gc, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+        k_apply<<<ga, kApplyBlock, 0, s>>>(P, L, ctl, fc);
     } else if (fc.mixed) {
         launch_force_mixed(P, L, ctl, fc, pp, pw, walls, s);
     } else {
-        k_step<MODE_FORCE_ONLY><<<nblocks(P.n), kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+        k_force<<<nblocks(P.n), kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
     }
 }
 
@@ -348,12 +379,7 @@ void launch_stage(const Particles &P, Ctl *ctl, const ForceConsts &fc, int stage
 void launch_energy(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
                    const PairConst *pw, const WallGeom *walls, double *partials, int nparts, double *out,
                    cudaStream_t s) {
-    (void)ctl;
-    // `cur` is read on the host by the caller and passed through fc-independent path
-    int cur = 0;
-    cudaMemcpyAsync(&cur, &ctl->cur, sizeof(int), cudaMemcpyDeviceToHost, s);
-    cudaStreamSynchronize(s);
-    k_energy_partials<<<nparts, kBlock, 0, s>>>(P, L, fc, pp, pw, walls, cur, partials);
+    k_energy_partials<<<nparts, kBlock, 0, s>>>(P, L, fc, pp, pw, walls, ctl, partials);
     k_energy_final<<<1, 32, 0, s>>>(partials, nparts, out);
 }
 
