@@ -243,7 +243,7 @@ def main():
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "traffic": (round(tpps * n) if tpps else None),
             "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
-            "kernel": "k_step<MODE_FUSED> (fused FP64 force + integration)", "kernel_ms": round(kernel_ms, 5),
+            "kernel": "fused step: k_stream + k_contact + k_apply (FP64 force + integration)", "kernel_ms": round(kernel_ms, 5),
             "bytes_per_particle_step": round(b_step, 2), **occ}
 
     # end to end through the C ABI with host buffers

@@ -37,6 +37,8 @@ struct dem_particles {
     bool mat_dirty = true;   // E, nu, G changed: tables must be rebuilt
     bool has_bonds = false;  // bond slots hold sorted indices: no re-sort from now on
     bool any_fix = false;    // some particle carries a DEM_FIX_* flag
+    void *stage = nullptr;   // device staging buffer for set/get (largest field)
+    size_t stage_bytes = 0;
     std::vector<uint8_t> mat;   // caller order
     std::vector<std::tuple<double, double, double>> mats;
 };
@@ -344,10 +346,15 @@ extern "C" int dem_particles_create(dem_ctx *ctx, int n, int max_contacts, int m
     cudaError_t e = alloc_particles(p->P, n, max_contacts, max_walls, true);
     if (e == cudaSuccess) e = alloc_particles(p->alt, n, max_contacts, max_walls, false);
     if (e == cudaSuccess) e = dalloc(&p->ctl, 1);
+    if (e == cudaSuccess) {
+        p->stage_bytes = sizeof(double) * (size_t)p->P.cap * std::max(3, std::max(max_contacts, max_walls));
+        e = cudaMalloc(&p->stage, p->stage_bytes);
+    }
     if (e != cudaSuccess) {
         free_particles(p->P);
         free_particles(p->alt);
         cudaFree(p->ctl);
+        cudaFree(p->stage);
         delete p;
         return cuda_check(ctx, e, "dem_particles_create");
     }
@@ -385,6 +392,7 @@ extern "C" int dem_particles_destroy(dem_particles *p) {
     free_particles(p->P);
     free_particles(p->alt);
     cudaFree(p->ctl);
+    cudaFree(p->stage);
     delete p;
     return DEM_OK;
 }
@@ -407,8 +415,7 @@ extern "C" int dem_particles_set(dem_particles *p, int field, const void *host, 
         if (field != DEM_F_RHO) p->mat_dirty = true;
         return DEM_OK;
     }
-    void *tmp = nullptr;
-    CK(cudaMalloc(&tmp, (size_t)need * es));
+    void *tmp = p->stage;
     CK(cudaMemcpyAsync(tmp, host, (size_t)need * es, cudaMemcpyHostToDevice, s));
     int vcur = 0;
     const int cur = host_cur(p, &vcur);
@@ -456,8 +463,6 @@ extern "C" int dem_particles_set(dem_particles *p, int field, const void *host, 
         }
     }
     cudaError_t e = cudaGetLastError();
-    cudaStreamSynchronize(s);
-    cudaFree(tmp);
     CK(e);
     p->dirty = true;
     k_invalidate<<<1, 32, 0, s>>>(p->ctl);
@@ -483,8 +488,7 @@ extern "C" int dem_particles_get(dem_particles *p, int field, void *host, long c
         std::memset(host, 0, sizeof(double) * 3 * n);
         return DEM_OK;
     }
-    void *tmp = nullptr;
-    CK(cudaMalloc(&tmp, (size_t)need * es));
+    void *tmp = p->stage;
     int vcur = 0;
     const int cur = host_cur(p, &vcur);
     switch (field) {
@@ -512,7 +516,6 @@ extern "C" int dem_particles_get(dem_particles *p, int field, void *host, long c
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(host, tmp, (size_t)need * es, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    cudaFree(tmp);
     CK(e);
     return DEM_OK;
 }

@@ -354,9 +354,12 @@ void launch_step(const Particles &P, const NbrList &L, Ctl *ctl, const ForceCons
     if (mode == MODE_FUSED) {
         static int gc = 0, gm = 0, ga = 0, last_n = -1;
         if (last_n != P.n) {
-            gc = persistent_blocks((const void *)k_contact, kBlock, P.n);
-            gm = persistent_blocks(contact_mixed_kernel(), kBlock, P.n);
-            ga = 148;   // few deferred particles in the common case, one ticket per block
+            // two contact blocks per SM: enough for dense packings, little fixed cost when
+            // only a few particles are deferred; the apply kernel copies 48 B per deferred
+            // particle and takes one ticket per block
+            gc = min(persistent_blocks((const void *)k_contact, kBlock, P.n), 2 * 148);
+            gm = min(persistent_blocks(contact_mixed_kernel(), kBlock, P.n), 2 * 148);
+            ga = 32;
             last_n = P.n;
         }
         k_stream<<<(P.n + kStreamBlock - 1) / kStreamBlock, kStreamBlock, 0, s>>>(P, L, ctl, fc, walls);

@@ -1,0 +1,524 @@
+// CabanaDEM_B200.hpp -- C++ interface with the reference's class names, over the C ABI of
+// libb200dem.so (b200dem.h).  A CabanaDEM example ports by swapping the include and the
+// Kokkos lambdas for ordinary lambdas:
+//
+//   reference (CabanaDEM.hpp)                       here
+//   CabanaDEM::Inputs (Input.hpp:41-82)             CabanaDEM::Inputs (flat JSON reader)
+//   CabanaDEM::Particles<Mem,3,MaxCnts,MaxWalls>    same template; slices are host mirrors
+//     (Particles.hpp:22-297)                        committed by updateParticles()/commit()
+//   CabanaDEM::Wall<Mem,3> (Wall.hpp:22-153)         same
+//   CabanaDEM::Force<Exec>(cor_pp,cor_pw,mu_pp,mu_pw) same (+ optional quirk bits)
+//   CabanaDEM::createSolverDEM<Mem>(...)->run()     same: num_steps + 1 steps
+//     (Solver.hpp:66-138)
+//   CabanaBondedDEM::ParticlesBondedDEM<Mem,3,MaxBonds>::setupBonds (BondedDEM_Particles.hpp:86)
+//                                                    BondedDEM<Mem,3,MaxBonds> (setupBonds, run)
+//
+// Slices: slicePosition() etc. return a HostSlice, a shared host copy of one field taken at
+// the call; writing through it marks the field dirty, and updateParticles(exec, functor)
+// (or commit()) uploads every dirty field.  Reading a slice after a run downloads fresh data.
+// Errors throw CabanaDEM::Error with the library's message.
+#pragma once
+
+#include <array>
+#include <cctype>
+#include <cmath>
+#include <cstdio>
+#include <fstream>
+#include <functional>
+#include <iostream>
+#include <map>
+#include <memory>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "b200dem.h"
+
+namespace CabanaDEM {
+
+struct DeviceSpace {
+    using memory_space = DeviceSpace;
+    using execution_space = DeviceSpace;
+};
+using DefaultExecutionSpace = DeviceSpace;
+
+class Error : public std::runtime_error {
+  public:
+    explicit Error(const std::string &m) : std::runtime_error(m) {}
+};
+
+class Context {
+  public:
+    explicit Context(int device = 0) {
+        if (dem_ctx_create(device, &h_)) throw Error("dem_ctx_create: no usable CUDA device");
+    }
+    ~Context() { dem_ctx_destroy(h_); }
+    Context(const Context &) = delete;
+    Context &operator=(const Context &) = delete;
+    dem_ctx *handle() const { return h_; }
+    void check(int st, const char *what, int allow = 0) const {
+        if (st & ~allow) throw Error(std::string(what) + ": " + dem_last_error(h_) + " (status " + std::to_string(st) + ")");
+    }
+    static std::shared_ptr<Context> get_default() {
+        static std::shared_ptr<Context> c = std::make_shared<Context>(0);
+        return c;
+    }
+
+  private:
+    dem_ctx *h_ = nullptr;
+};
+
+// ---------------------------------------------------------------------------------------
+// Flat JSON reader for {"key": {"value": v, "unit"/"units": u}} (Input.hpp:41-82).
+// ---------------------------------------------------------------------------------------
+class JsonValue {
+  public:
+    enum Kind { Null, Number, String, Bool, Array, Object };
+    Kind kind = Null;
+    double num = 0.0;
+    std::string str;
+    std::vector<JsonValue> arr;
+    std::map<std::string, JsonValue> obj;
+    operator double() const { return num; }
+    operator int() const { return static_cast<int>(num); }
+    const JsonValue &operator[](const std::string &k) const {
+        auto it = obj.find(k);
+        if (it == obj.end()) throw Error("missing key " + k);
+        return it->second;
+    }
+    const JsonValue &operator[](const char *k) const { return (*this)[std::string(k)]; }
+    bool contains(const std::string &k) const { return obj.count(k) != 0; }
+
+    static JsonValue parse(const std::string &text) {
+        size_t i = 0;
+        JsonValue v = value(text, i);
+        return v;
+    }
+
+  private:
+    static void ws(const std::string &s, size_t &i) {
+        while (i < s.size() && std::isspace(static_cast<unsigned char>(s[i]))) ++i;
+    }
+    static JsonValue value(const std::string &s, size_t &i) {
+        ws(s, i);
+        if (i >= s.size()) throw Error("json: unexpected end");
+        JsonValue v;
+        const char c = s[i];
+        if (c == '{') {
+            v.kind = Object;
+            ++i;
+            ws(s, i);
+            if (s[i] == '}') { ++i; return v; }
+            for (;;) {
+                ws(s, i);
+                const std::string key = string(s, i);
+                ws(s, i);
+                if (s[i++] != ':') throw Error("json: expected ':'");
+                v.obj[key] = value(s, i);
+                ws(s, i);
+                if (s[i] == ',') { ++i; continue; }
+                if (s[i] == '}') { ++i; break; }
+                throw Error("json: expected ',' or '}'");
+            }
+        } else if (c == '[') {
+            v.kind = Array;
+            ++i;
+            ws(s, i);
+            if (s[i] == ']') { ++i; return v; }
+            for (;;) {
+                v.arr.push_back(value(s, i));
+                ws(s, i);
+                if (s[i] == ',') { ++i; continue; }
+                if (s[i] == ']') { ++i; break; }
+                throw Error("json: expected ',' or ']'");
+            }
+        } else if (c == '"') {
+            v.kind = String;
+            v.str = string(s, i);
+        } else if (s.compare(i, 4, "true") == 0) {
+            v.kind = Bool; v.num = 1; i += 4;
+        } else if (s.compare(i, 5, "false") == 0) {
+            v.kind = Bool; v.num = 0; i += 5;
+        } else if (s.compare(i, 4, "null") == 0) {
+            i += 4;
+        } else {
+            v.kind = Number;
+            size_t used = 0;
+            v.num = std::stod(s.substr(i), &used);
+            i += used;
+        }
+        return v;
+    }
+    static std::string string(const std::string &s, size_t &i) {
+        if (s[i] != '"') throw Error("json: expected string");
+        std::string out;
+        for (++i; i < s.size() && s[i] != '"'; ++i) {
+            if (s[i] == '\\' && i + 1 < s.size()) ++i;
+            out += s[i];
+        }
+        ++i;
+        return out;
+    }
+};
+
+inline std::vector<std::string> splitString(const std::string &str, char delimiter) {   // Input.hpp:24-38
+    std::vector<std::string> result;
+    size_t start = 0, end = str.find(delimiter);
+    while (end != std::string::npos) {
+        result.push_back(str.substr(start, end - start));
+        start = end + 1;
+        end = str.find(delimiter, start);
+    }
+    result.push_back(str.substr(start));
+    return result;
+}
+
+class Inputs {
+  public:
+    explicit Inputs(const std::string &filename) {
+        std::ifstream f(filename);
+        if (!f) throw Error("cannot open " + filename);
+        std::stringstream ss;
+        ss << f.rdbuf();
+        inputs_ = JsonValue::parse(ss.str());
+        const double tf = inputs_["final_time"]["value"];
+        const double dt = inputs_["timestep"]["value"];
+        const int num_steps = tf / dt;   // Input.hpp:53, truncation as the reference
+        JsonValue ns;
+        ns.kind = JsonValue::Object;
+        JsonValue v;
+        v.kind = JsonValue::Number;
+        v.num = num_steps;
+        ns.obj["value"] = v;
+        inputs_.obj["num_steps"] = ns;
+    }
+    const JsonValue &operator[](const std::string &label) const { return inputs_[label]["value"]; }
+    const JsonValue &operator[](const char *label) const { return (*this)[std::string(label)]; }
+    std::string units(const std::string &label) const {
+        return inputs_[label].contains("units") ? inputs_[label]["units"].str : std::string();
+    }
+    bool contains(const std::string &label) const { return inputs_.contains(label); }
+
+  private:
+    JsonValue inputs_;
+};
+
+// ---------------------------------------------------------------------------------------
+// Host mirror of one field.
+// ---------------------------------------------------------------------------------------
+template <class T>
+struct Mirror {
+    std::vector<T> data;
+    int ncomp = 1;
+    bool dirty = false;
+    bool fresh = false;
+};
+
+template <class T>
+class HostSlice {
+  public:
+    HostSlice() = default;
+    explicit HostSlice(std::shared_ptr<Mirror<T>> m) : m_(std::move(m)) {}
+    T &operator()(int i, int d = 0) const {
+        m_->dirty = true;
+        return m_->data[static_cast<size_t>(i) * m_->ncomp + d];
+    }
+    std::size_t size() const { return m_->data.size() / m_->ncomp; }
+    const T *data() const { return m_->data.data(); }
+
+  private:
+    std::shared_ptr<Mirror<T>> m_;
+};
+
+// ---------------------------------------------------------------------------------------
+// Particles<MemorySpace, Dim, MaxCnts, MaxNoWalls> (Particles.hpp:22-71)
+// ---------------------------------------------------------------------------------------
+template <class MemorySpace, int Dimension, int MaxCnts, int MaxNoWalls>
+class Particles {
+  public:
+    static constexpr int dim = Dimension;
+    std::array<double, 3> mesh_lo{}, mesh_hi{};   // kept for source compatibility: the device grid
+                                                  // follows the particles' bounding box
+
+    template <class ExecSpace>
+    Particles(const ExecSpace &, std::size_t n, const std::string &output_folder = "",
+              std::shared_ptr<Context> ctx = nullptr)
+        : n_(static_cast<int>(n)), out_(output_folder), ctx_(ctx ? ctx : Context::get_default()) {
+        ctx_->check(dem_particles_create(ctx_->handle(), n_, MaxCnts, MaxNoWalls, &h_), "dem_particles_create");
+    }
+    ~Particles() { dem_particles_destroy(h_); }
+    Particles(const Particles &) = delete;
+    Particles &operator=(const Particles &) = delete;
+
+    HostSlice<double> slicePosition() { return slice_d(DEM_F_X, 3); }
+    HostSlice<double> sliceVelocity() { return slice_d(DEM_F_U, 3); }
+    HostSlice<double> sliceOmega() { return slice_d(DEM_F_OMEGA, 3); }
+    HostSlice<double> sliceForce() { return slice_d(DEM_F_FORCE, 3); }
+    HostSlice<double> sliceTorque() { return slice_d(DEM_F_TORQUE, 3); }
+    HostSlice<double> sliceMass() { return slice_d(DEM_F_M, 1); }
+    HostSlice<double> sliceDensity() { return slice_d(DEM_F_RHO, 1); }
+    HostSlice<double> sliceRadius() { return slice_d(DEM_F_RAD, 1); }
+    HostSlice<double> sliceMomentOfInertia() { return slice_d(DEM_F_I, 1); }
+    HostSlice<double> sliceYoungsMod() { return slice_d(DEM_F_E, 1); }
+    HostSlice<double> slicePoissonsRatio() { return slice_d(DEM_F_NU, 1); }
+    HostSlice<double> sliceShearMod() { return slice_d(DEM_F_G, 1); }
+    HostSlice<double> sliceTangentialDispSSx() { return slice_d(DEM_F_TNG_SS_X, MaxCnts); }
+    HostSlice<double> sliceTangentialDispSSy() { return slice_d(DEM_F_TNG_SS_Y, MaxCnts); }
+    HostSlice<double> sliceTangentialDispSSz() { return slice_d(DEM_F_TNG_SS_Z, MaxCnts); }
+    HostSlice<double> sliceTangentialDispSWx() { return slice_d(DEM_F_TNG_SW_X, MaxNoWalls); }
+    HostSlice<double> sliceTangentialDispSWy() { return slice_d(DEM_F_TNG_SW_Y, MaxNoWalls); }
+    HostSlice<double> sliceTangentialDispSWz() { return slice_d(DEM_F_TNG_SW_Z, MaxNoWalls); }
+    HostSlice<int> sliceTangentialDispIdx() { return slice_i(DEM_F_TNG_IDX, MaxCnts); }
+    HostSlice<int> sliceTotalNoTangentialContacts() { return slice_i(DEM_F_TNG_COUNT, 1); }
+
+    // updateParticles(exec, functor) (Particles.hpp:91-97): functor(pid) on the host for every
+    // particle, then every slice written through is uploaded.
+    template <class ExecSpace, class Functor>
+    void updateParticles(const ExecSpace &, const Functor &f) {
+        for (int pid = 0; pid < n_; ++pid) f(pid);
+        commit();
+    }
+
+    void commit() {
+        for (auto &kv : md_)
+            if (kv.second->dirty) {
+                ctx_->check(dem_particles_set(h_, kv.first, kv.second->data.data(), (long)kv.second->data.size()),
+                            "dem_particles_set");
+                kv.second->dirty = false;
+            }
+        for (auto &kv : mi_)
+            if (kv.second->dirty) {
+                ctx_->check(dem_particles_set(h_, kv.first, kv.second->data.data(), (long)kv.second->data.size()),
+                            "dem_particles_set");
+                kv.second->dirty = false;
+            }
+    }
+    // device -> mirrors (called by the solver after it advances the state)
+    void invalidate() {
+        for (auto &kv : md_) kv.second->fresh = false;
+        for (auto &kv : mi_) kv.second->fresh = false;
+    }
+
+    std::size_t size() const { return static_cast<std::size_t>(n_); }
+    dem_particles *handle() { return h_; }
+    Context &context() { return *ctx_; }
+    std::shared_ptr<Context> context_ptr() { return ctx_; }
+
+  private:
+    HostSlice<double> slice_d(int field, int nc) {
+        auto &m = md_[field];
+        if (!m) {
+            m = std::make_shared<Mirror<double>>();
+            m->ncomp = nc;
+            m->data.assign(static_cast<size_t>(n_) * nc, 0.0);
+        }
+        if (!m->fresh && !m->dirty && nc > 0) {
+            ctx_->check(dem_particles_get(h_, field, m->data.data(), (long)m->data.size()), "dem_particles_get");
+            m->fresh = true;
+        }
+        return HostSlice<double>(m);
+    }
+    HostSlice<int> slice_i(int field, int nc) {
+        auto &m = mi_[field];
+        if (!m) {
+            m = std::make_shared<Mirror<int>>();
+            m->ncomp = nc;
+            m->data.assign(static_cast<size_t>(n_) * nc, 0);
+        }
+        if (!m->fresh && !m->dirty && nc > 0) {
+            ctx_->check(dem_particles_get(h_, field, m->data.data(), (long)m->data.size()), "dem_particles_get");
+            m->fresh = true;
+        }
+        return HostSlice<int>(m);
+    }
+
+    int n_;
+    std::string out_;
+    std::shared_ptr<Context> ctx_;
+    dem_particles *h_ = nullptr;
+    std::map<int, std::shared_ptr<Mirror<double>>> md_;
+    std::map<int, std::shared_ptr<Mirror<int>>> mi_;
+};
+
+// ---------------------------------------------------------------------------------------
+// Wall<MemorySpace, Dim> (Wall.hpp:22-153)
+// ---------------------------------------------------------------------------------------
+template <class MemorySpace, int Dimension>
+class Wall {
+  public:
+    template <class ExecSpace>
+    Wall(const ExecSpace &, std::size_t n, const std::string & = "", std::shared_ptr<Context> ctx = nullptr)
+        : n_(static_cast<int>(n)), ctx_(ctx ? ctx : Context::get_default()) {
+        ctx_->check(dem_walls_create(ctx_->handle(), n_, &h_), "dem_walls_create");
+        for (int f = DEM_W_X; f <= DEM_W_G; ++f) {
+            auto m = std::make_shared<Mirror<double>>();
+            m->ncomp = f <= DEM_W_NORMAL ? 3 : 1;
+            m->data.assign(static_cast<size_t>(n_) * m->ncomp, 0.0);
+            m_[f] = m;
+        }
+    }
+    ~Wall() { dem_walls_destroy(h_); }
+    HostSlice<double> slicePosition() { return HostSlice<double>(m_[DEM_W_X]); }
+    HostSlice<double> sliceVelocity() { return HostSlice<double>(m_[DEM_W_U]); }
+    HostSlice<double> sliceOmega() { return HostSlice<double>(m_[DEM_W_OMEGA]); }
+    HostSlice<double> sliceNormal() { return HostSlice<double>(m_[DEM_W_NORMAL]); }
+    HostSlice<double> sliceYoungsMod() { return HostSlice<double>(m_[DEM_W_E]); }
+    HostSlice<double> slicePoissonsRatio() { return HostSlice<double>(m_[DEM_W_NU]); }
+    HostSlice<double> sliceShearMod() { return HostSlice<double>(m_[DEM_W_G]); }
+    template <class ExecSpace, class Functor>
+    void updateParticles(const ExecSpace &, const Functor &f) {
+        for (int pid = 0; pid < n_; ++pid) f(pid);
+        commit();
+    }
+    void commit() {
+        for (auto &kv : m_)
+            ctx_->check(dem_walls_set(h_, kv.first, kv.second->data.data(), (long)kv.second->data.size()),
+                        "dem_walls_set");
+    }
+    std::size_t size() const { return static_cast<std::size_t>(n_); }
+    dem_walls *handle() { return h_; }
+
+  private:
+    int n_;
+    std::shared_ptr<Context> ctx_;
+    dem_walls *h_ = nullptr;
+    std::map<int, std::shared_ptr<Mirror<double>>> m_;
+};
+
+// Force<ExecutionSpace>(cor_pp, cor_pw, friction_pp, friction_pw) (Force.hpp:16-35)
+template <class ExecutionSpace>
+class Force {
+  public:
+    double cor_pp, cor_pw, friction_pp, friction_pw;
+    unsigned quirks;
+    Force(double cpp, double cpw, double fpp, double fpw, unsigned q = DEM_REF_COMPAT)
+        : cor_pp(cpp), cor_pw(cpw), friction_pp(fpp), friction_pw(fpw), quirks(q) {}
+    dem_force_params params() const { return dem_force_params{cor_pp, cor_pw, friction_pp, friction_pw, quirks}; }
+};
+
+// SolverDEM (Solver.hpp:13-122): the reference rebuilds the neighbour list every step with
+// cutoff delta; that is the default here.  set_skin() switches to the Verlet-skin mode.
+template <class MemorySpace, class InputType, class ParticleType, class WallType, class ForceModel>
+class SolverDEM {
+  public:
+    SolverDEM(const InputType &inputs, std::shared_ptr<ParticleType> particles, std::shared_ptr<WallType> wall,
+              std::shared_ptr<ForceModel> force, double delta, double skin = 0.0, int precision = DEM_FP64,
+              std::array<double, 3> gravity = {0.0, 0.0, 0.0})
+        : particles_(particles), wall_(wall), force_(force) {
+        num_steps = inputs["num_steps"];
+        output_frequency = inputs.contains("output_frequency") ? (int)inputs["output_frequency"] : 0;
+        dt = inputs["timestep"];
+        particles_->commit();
+        if (wall_) wall_->commit();
+        dem_solver_params sp{};
+        sp.dt = dt;
+        sp.delta = skin > 0.0 ? 0.0 : delta;
+        sp.skin = skin;
+        sp.rebuild_every_step = skin > 0.0 ? 0 : 1;
+        sp.precision = precision;
+        for (int d = 0; d < 3; ++d) sp.gravity[d] = gravity[d];
+        const dem_force_params fp = force_->params();
+        particles_->context().check(dem_solver_create(particles_->context().handle(), particles_->handle(),
+                                                      wall_ ? wall_->handle() : nullptr, &fp, &sp, &h_),
+                                    "dem_solver_create");
+    }
+    ~SolverDEM() { dem_solver_destroy(h_); }
+
+    void set_output(std::function<void(int, double)> f) { out_ = std::move(f); }
+
+    // Solver.hpp:79-97: steps 0..num_steps inclusive, output after every step divisible by
+    // output_frequency; the steps between two outputs run as one fused device run
+    void run() {
+        int step = 0;
+        while (step <= num_steps) {
+            int stop = num_steps;
+            if (output_frequency > 0) {
+                const int next_out = (step + output_frequency - 1) / output_frequency * output_frequency;
+                if (next_out < stop) stop = next_out;
+            }
+            run_steps(stop - step + 1);
+            output(stop);
+            step = stop + 1;
+        }
+    }
+    void run_steps(int n) {
+        particles_->commit();
+        particles_->context().check(dem_solver_run(h_, n), "dem_solver_run", DEM_ERR_CONTACT_OVERFLOW);
+        particles_->invalidate();
+    }
+    void output(int step) {
+        if (output_frequency > 0 && step % output_frequency == 0) {
+            std::cout << "We are at " << step << " / " << num_steps << std::endl;
+            if (out_) out_(step, step * dt);
+        }
+    }
+    dem_solver *handle() { return h_; }
+
+    int num_steps = 0;
+    int output_frequency = 0;
+    double dt = 0.0;
+
+  private:
+    std::shared_ptr<ParticleType> particles_;
+    std::shared_ptr<WallType> wall_;
+    std::shared_ptr<ForceModel> force_;
+    dem_solver *h_ = nullptr;
+    std::function<void(int, double)> out_;
+};
+
+// createSolverDEM<MemorySpace>(inputs, particles, wall, force, delta) (Solver.hpp:127-138)
+template <class MemorySpace, class InputsType, class ParticleType, class WallType, class ForceModel>
+auto createSolverDEM(const InputsType &inputs, std::shared_ptr<ParticleType> particles,
+                     std::shared_ptr<WallType> wall, std::shared_ptr<ForceModel> force, double delta) {
+    return std::make_shared<SolverDEM<MemorySpace, InputsType, ParticleType, WallType, ForceModel>>(
+        inputs, particles, wall, force, delta);
+}
+
+}  // namespace CabanaDEM
+
+namespace CabanaBondedDEM {
+
+// Bond slots and the bonded loop on a particle set (ParticlesBondedDEM, BondedDEM_Particles.hpp:29-293;
+// computeBondedForce, BondedDEM_Force.hpp:53-348; loop of tst_01_BDEM:295-306).
+template <class MemorySpace, int Dimension, int MaxBonds>
+class BondedDEM {
+  public:
+    template <class ParticleType>
+    BondedDEM(std::shared_ptr<ParticleType> particles, double dt, const dem_bond_params &bp)
+        : ctx_(particles->context_ptr()) {
+        particles->commit();
+        dem_solver_params sp{};
+        sp.dt = dt;
+        const dem_force_params fp{1.0, 1.0, 0.0, 0.0, DEM_REF_COMPAT};
+        ctx_->check(dem_solver_create(ctx_->handle(), particles->handle(), nullptr, &fp, &sp, &s_), "dem_solver_create");
+        ctx_->check(dem_bonds_create(s_, MaxBonds, &bp, &b_), "dem_bonds_create");
+        invalidate_ = [particles]() { particles->invalidate(); };
+    }
+    ~BondedDEM() {
+        dem_bonds_destroy(b_);
+        dem_solver_destroy(s_);
+    }
+    // setupBonds (BondedDEM_Particles.hpp:86-171): reference factor 3, search cutoff 4 rad(0)
+    void setupBonds(double factor = 3.0, double search_cutoff = 0.0) {
+        ctx_->check(dem_bonds_setup(b_, factor, search_cutoff), "dem_bonds_setup");
+    }
+    void run_steps(int n) {
+        ctx_->check(dem_bonded_run(b_, n), "dem_bonded_run");
+        invalidate_();
+    }
+    long broken() {
+        long c = 0;
+        ctx_->check(dem_bonds_broken(b_, &c), "dem_bonds_broken");
+        return c;
+    }
+    dem_bonds *handle() { return b_; }
+
+  private:
+    std::shared_ptr<CabanaDEM::Context> ctx_;
+    dem_solver *s_ = nullptr;
+    dem_bonds *b_ = nullptr;
+    std::function<void()> invalidate_;
+};
+
+}  // namespace CabanaBondedDEM
