@@ -22,7 +22,7 @@ DEM_ERR_TIMEOUT = 0x020
 # enum dem_field
 F = {name: k for k, name in enumerate(
     ["x", "u", "omega", "force", "torque", "m", "rho", "rad", "I", "E", "nu", "G", "tng_idx", "tng_ss_x",
-     "tng_ss_y", "tng_ss_z", "tng_count", "tng_sw_x", "tng_sw_y", "tng_sw_z", "fix", "ext_force"])}
+     "tng_ss_y", "tng_ss_z", "tng_count", "tng_sw_x", "tng_sw_y", "tng_sw_z", "fix", "ext_force", "scene"])}
 W = {name: k for k, name in enumerate(["x", "u", "omega", "normal", "E", "nu", "G"])}
 DEM_FP64, DEM_MIXED = 0, 1
 
@@ -35,7 +35,11 @@ class ForceParams(C.Structure):
 class SolverParams(C.Structure):
     _fields_ = [("dt", C.c_double), ("delta", C.c_double), ("skin", C.c_double), ("rebuild_every_step", C.c_int),
                 ("precision", C.c_int), ("gravity", C.c_double * 3), ("max_neighbors", C.c_int),
-                ("steps_per_launch", C.c_int)]
+                ("steps_per_launch", C.c_int), ("stream_block", C.c_int)]
+
+
+class SceneParams(C.Structure):
+    _fields_ = [("cor_pp", C.c_double), ("cor_pw", C.c_double), ("mu_pp", C.c_double), ("mu_pw", C.c_double)]
 
 
 class BondParams(C.Structure):
@@ -88,6 +92,7 @@ _PROTOS = {
     "dem_compute_force": ([_VP], C.c_int),
     "dem_neighbors_get": ([_VP, _VP, _VP, C.POINTER(C.c_long)], C.c_int),
     "dem_energy": ([_VP, C.POINTER(C.c_double)], C.c_int),
+    "dem_solver_set_scenes": ([_VP, _VP, C.c_int, C.c_int], C.c_int),
     "dem_bonds_create": ([_VP, C.c_int, C.POINTER(BondParams), C.POINTER(_VP)], C.c_int),
     "dem_bonds_destroy": ([_VP], C.c_int),
     "dem_bonds_setup": ([_VP, C.c_double, C.c_double], C.c_int),

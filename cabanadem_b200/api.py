@@ -35,7 +35,7 @@ from .state import ParticleState, WallState
 
 REF_COMPAT = 0x1F
 
-_F_DTYPE = {"tng_idx": np.int32, "tng_count": np.int32, "fix": np.uint8}
+_F_DTYPE = {"tng_idx": np.int32, "tng_count": np.int32, "fix": np.uint8, "scene": np.int32}
 
 
 def _shape(field, n, mc, mw):
@@ -211,7 +211,7 @@ class SolverDEM:
     def __init__(self, particles: Particles, wall: Wall | None, force: Force, dt: float, delta: float = 0.0,
                  skin: float = 0.0, rebuild_every_step: bool = False, gravity=(0.0, 0.0, 0.0),
                  precision: int = _lib.DEM_FP64, num_steps: int = 0, output_frequency: int = 0,
-                 max_neighbors: int = 0, steps_per_launch: int = 0):
+                 max_neighbors: int = 0, steps_per_launch: int = 0, stream_block: int = 0):
         self.particles, self.wall, self.force = particles, wall, force
         self.dt, self.num_steps, self.output_frequency = float(dt), int(num_steps), int(output_frequency)
         sp = _lib.SolverParams()
@@ -221,6 +221,7 @@ class SolverDEM:
         sp.gravity = (C.c_double * 3)(*gravity)
         sp.max_neighbors = int(max_neighbors)
         sp.steps_per_launch = int(steps_per_launch)
+        sp.stream_block = int(stream_block)
         fp = force.params()
         h = C.c_void_p()
         check(lib().dem_solver_create(particles.ctx.h, particles.h, wall.h if wall else None, C.byref(fp),
@@ -242,6 +243,13 @@ class SolverDEM:
         s = _lib.RunStats()
         check(lib().dem_solver_stats(self.h, C.byref(s)), self.particles.ctx.h, "dem_solver_stats")
         return {k: getattr(s, k) for k, _ in s._fields_}
+
+    def set_scenes(self, params, walls_per_scene: int):
+        """Batched independent scenes: params is a sequence of (cor_pp, cor_pw, mu_pp, mu_pw)
+        per scene; the particles' "scene" field assigns them (dem_solver_set_scenes)."""
+        arr = (_lib.SceneParams * len(params))(*[_lib.SceneParams(*map(float, p)) for p in params])
+        check(lib().dem_solver_set_scenes(self.h, arr, len(params), int(walls_per_scene)), self.particles.ctx.h,
+              "dem_solver_set_scenes")
 
     def profile_steps(self, nsteps: int) -> float:
         """Run nsteps fused steps launched one by one between CUDA events; returns the
@@ -315,10 +323,13 @@ def createSolverDEM(inputs: Inputs, particles: Particles, wall: Wall, force: For
 
 
 def from_scenario(sc, ctx: Context | None = None, rebuild_every_step=False, precision=_lib.DEM_FP64,
-                  steps_per_launch=0, max_neighbors=0):
+                  steps_per_launch=0, max_neighbors=0, stream_block=0):
     """Particles + Wall + SolverDEM on the device for a scenarios.Scenario."""
     st = sc.state
-    p = Particles(st.n, st.max_cnts, sc.walls.n if sc.walls is not None else 0, ctx=ctx)
+    nwalls = sc.walls.n if sc.walls is not None else 0
+    if sc.extra.get("scene") is not None:
+        nwalls = sc.extra["walls_per_scene"]
+    p = Particles(st.n, st.max_cnts, nwalls, ctx=ctx)
     p.upload(st)
     w = None
     if sc.walls is not None and sc.walls.n > 0:
@@ -328,7 +339,10 @@ def from_scenario(sc, ctx: Context | None = None, rebuild_every_step=False, prec
     f = Force(prm["cor_pp"], prm["cor_pw"], prm["mu_pp"], prm["mu_pw"], prm.get("quirks", REF_COMPAT))
     s = SolverDEM(p, w, f, sc.dt, delta=sc.delta, skin=sc.skin, rebuild_every_step=rebuild_every_step,
                   gravity=sc.gravity, precision=precision, steps_per_launch=steps_per_launch,
-                  max_neighbors=max_neighbors)
+                  max_neighbors=max_neighbors, stream_block=stream_block)
+    if sc.extra.get("scene") is not None:
+        p.set("scene", sc.extra["scene"])
+        s.set_scenes(sc.extra["scene_params"], sc.extra["walls_per_scene"])
     return s
 
 

@@ -1,0 +1,99 @@
+"""Autotuner for the launch configuration of a workload.
+
+Three settings change speed but not results (the neighbour list is always a superset of the
+overlapping pairs and is summed in caller-index order, whatever its cutoff or the re-sort):
+
+* ``stream_block``      block size of the streaming kernel (64, 128, 256)
+* ``steps_per_launch``  fused steps per captured CUDA graph (host round trip per graph)
+* ``skin``              Verlet skin, i.e. the rebuild cadence
+
+``tune`` times short runs of the caller's workload for each candidate, one setting at a time
+(coordinate search from the defaults), and caches the winner per size bucket
+(log2 of the particle count, precision, batched or not) in a JSON file
+(``$CABANADEM_B200_TUNE_CACHE``, default ``~/.cache/cabanadem_b200/autotune.json``).
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+import time
+
+from . import api
+
+DEFAULTS = dict(stream_block=128, steps_per_launch=32, skin_factor=1.0)
+CANDIDATES = dict(stream_block=(64, 128, 256), steps_per_launch=(16, 32, 64), skin_factor=(0.5, 1.0, 2.0))
+
+
+def cache_path():
+    return os.environ.get("CABANADEM_B200_TUNE_CACHE",
+                          os.path.join(os.path.expanduser("~"), ".cache", "cabanadem_b200", "autotune.json"))
+
+
+def bucket(sc, precision):
+    batched = sc.extra.get("scene") is not None
+    return "n2^%d|p%d|%s" % (int(math.log2(max(sc.state.n, 1))), int(precision), "batched" if batched else "single")
+
+
+def _load():
+    try:
+        with open(cache_path()) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def _store(table):
+    path = cache_path()
+    os.makedirs(os.path.dirname(path), exist_ok=True)
+    with open(path, "w") as f:
+        json.dump(table, f, indent=1, sort_keys=True)
+
+
+def time_config(sc, cfg, precision, warmup, steps, ctx=None):
+    """Seconds per step of `steps` fused steps after `warmup` steps."""
+    base_skin = sc.skin
+    sc.skin = base_skin * cfg["skin_factor"]
+    try:
+        s = api.from_scenario(sc, ctx=ctx, precision=precision, stream_block=cfg["stream_block"],
+                              steps_per_launch=cfg["steps_per_launch"])
+        s.run_steps(warmup)
+        t0 = time.perf_counter()
+        s.run_steps(steps)      # returns after the device finished (status read-back)
+        dt = (time.perf_counter() - t0) / steps
+        s.close()
+        s.particles.close()
+    finally:
+        sc.skin = base_skin
+    return dt
+
+
+def tune(sc, precision=0, warmup=20, steps=200, use_cache=True, ctx=None):
+    """Best {stream_block, steps_per_launch, skin_factor} for this workload's bucket."""
+    key = bucket(sc, precision)
+    table = _load() if use_cache else {}
+    if use_cache and key in table:
+        return dict(table[key]["config"])
+    best = dict(DEFAULTS)
+    best_t = time_config(sc, best, precision, warmup, steps, ctx)
+    trials = [(dict(best), best_t)]
+    for name in ("stream_block", "steps_per_launch", "skin_factor"):
+        for v in CANDIDATES[name]:
+            if v == best[name]:
+                continue
+            cfg = dict(best)
+            cfg[name] = v
+            t = time_config(sc, cfg, precision, warmup, steps, ctx)
+            trials.append((cfg, t))
+            if t < best_t:
+                best, best_t = cfg, t
+    table[key] = {"config": best, "s_per_step": best_t, "trials": [[c, t] for c, t in trials]}
+    if use_cache:
+        _store(table)
+    return dict(best)
+
+
+def apply(sc, cfg):
+    """Scenario settings for a tuned configuration (skin) and from_scenario keyword arguments."""
+    sc.skin = sc.skin * cfg["skin_factor"]
+    return dict(stream_block=cfg["stream_block"], steps_per_launch=cfg["steps_per_launch"])

@@ -37,6 +37,7 @@ struct dem_particles {
     bool mat_dirty = true;   // E, nu, G changed: tables must be rebuilt
     bool has_bonds = false;  // bond slots hold sorted indices: no re-sort from now on
     bool any_fix = false;    // some particle carries a DEM_FIX_* flag
+    int nscenes = 1;         // 1 + largest DEM_F_SCENE value
     void *stage = nullptr;   // device staging buffer for set/get (largest field)
     size_t stage_bytes = 0;
     std::vector<uint8_t> mat;   // caller order
@@ -58,6 +59,9 @@ struct dem_solver {
     ForceConsts fc{};
     PairConst *d_pp = nullptr, *d_pw = nullptr;
     WallGeom *d_walls = nullptr;
+    SceneConst *d_scenes = nullptr;
+    int nscenes = 0, wps = 0;
+    bool walls_ok = true;
     NbrList L{};
     BuildBuffers B{};
     double *d_epart = nullptr, *d_eout = nullptr;
@@ -243,6 +247,7 @@ bool field_layout(const dem_particles *p, int field, long *count, int *esize) {
         case DEM_F_TNG_COUNT: *count = n; *esize = 4; return true;
         case DEM_F_TNG_SW_X: case DEM_F_TNG_SW_Y: case DEM_F_TNG_SW_Z: *count = n * p->P.mw; *esize = 8; return true;
         case DEM_F_FIX: *count = n; *esize = 1; return true;
+        case DEM_F_SCENE: *count = n; *esize = 4; return true;
         default: return false;
     }
 }
@@ -319,6 +324,7 @@ static cudaError_t alloc_particles(Particles &P, int n, int mc, int mw, bool pin
     A(dalloc(&P.perm, cap));
     A(dalloc(&P.rank, cap));
     A(dalloc(&P.vslots, 32 * kVmaxSlots));
+    P.scene = nullptr;
     if (e == cudaSuccess) e = cudaMemset(P.vslots, 0, sizeof(unsigned long long) * 32 * kVmaxSlots);
     P.ext = nullptr;
     return e;
@@ -333,6 +339,7 @@ static void free_particles(Particles &P) {
     cudaFree(P.force); cudaFree(P.torque); cudaFree(P.mI); cudaFree(P.mat); cudaFree(P.cstate);
     cudaFree(P.tidx); cudaFree(P.th); cudaFree(P.sw); cudaFree(P.fix); cudaFree(P.perm); cudaFree(P.rank);
     cudaFree(P.vslots);
+    cudaFree(P.scene);
     cudaFree(P.ext);
     P = Particles{};
 }
@@ -452,6 +459,22 @@ extern "C" int dem_particles_set(dem_particles *p, int field, const void *host, 
                                             P.cap, P.rank);
             k_sw_mask<<<kGS, kTB, 0, s>>>(P);
             break;
+        case DEM_F_SCENE: {
+            const int *sc = (const int *)host;
+            int mx = 0;
+            for (int i = 0; i < n; ++i) {
+                if (sc[i] < 0 || sc[i] > (1 << 24)) return fail(ctx, DEM_ERR_INVALID, "scene index out of range");
+                mx = std::max(mx, sc[i]);
+            }
+            if (!P.scene) {
+                CK(dalloc(&P.scene, (size_t)P.cap));
+                CK(dalloc(&p->alt.scene, (size_t)P.cap));
+            }
+            k_scatter_i<<<kGS, kTB, 0, s>>>((int *)tmp, P.scene, n, 1, P.cap, P.rank, 0);
+            p->nscenes = mx + 1;
+            p->mat_dirty = true;
+            break;
+        }
         case DEM_F_FIX: {
             k_scatter_u8<<<kGS, kTB, 0, s>>>((uint8_t *)tmp, P.fix, n, P.rank);
             const uint8_t *f = (const uint8_t *)host;
@@ -512,6 +535,10 @@ extern "C" int dem_particles_get(dem_particles *p, int field, void *host, long c
                                            P.cap, P.rank);
             break;
         case DEM_F_FIX: k_gather_u8<<<kGS, kTB, 0, s>>>(P.fix, (uint8_t *)tmp, n, P.rank); break;
+        case DEM_F_SCENE:
+            if (P.scene) k_gather_i<<<kGS, kTB, 0, s>>>(P.scene, (int *)tmp, n, 1, P.cap, P.rank, P.perm, 0);
+            else cudaMemsetAsync(tmp, 0, sizeof(int) * n, s);
+            break;
     }
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(host, tmp, (size_t)need * es, cudaMemcpyDeviceToHost, s);
@@ -522,7 +549,7 @@ extern "C" int dem_particles_get(dem_particles *p, int field, void *host, long c
 
 // ---- walls --------------------------------------------------------------------------
 extern "C" int dem_walls_create(dem_ctx *ctx, int n, dem_walls **out) {
-    if (!ctx || !out || n < 0 || n > kMaxWalls) return fail(ctx, DEM_ERR_INVALID, "dem_walls_create: 0 <= n <= 24");
+    if (!ctx || !out || n < 0 || n > (1 << 20)) return fail(ctx, DEM_ERR_INVALID, "dem_walls_create: 0 <= n <= 2^20");
     dem_walls *w = new dem_walls();
     w->ctx = ctx;
     w->n = n;
@@ -617,6 +644,12 @@ int prepare(dem_solver *s) {
     }
     const int nm = (int)p->mats.size();
     const int nw = s->w ? s->w->n : 0;
+    // wall history slots: checked when the solver runs (scenes may be assigned after creation)
+    s->walls_ok = s->wps == 0 ? nw <= p->P.mw : (s->wps <= p->P.mw && nw >= s->nscenes * s->wps);
+    if (s->nscenes > 0 && p->nscenes > s->nscenes)
+        return fail(ctx, DEM_ERR_INVALID, "a particle's scene index has no scene parameters");
+    if (std::max(p->nscenes, s->nscenes) > s->B.cell_cap)   // every scene takes at least one cell key
+        return fail(ctx, DEM_ERR_INVALID, "more scenes than cell keys (8 per particle slot)");
     std::vector<PairConst> pp((size_t)nm * nm), pw((size_t)nm * std::max(nw, 1));
     for (int a = 0; a < nm; ++a) {
         const auto &A = p->mats[a];
@@ -664,6 +697,17 @@ int prepare(dem_solver *s) {
     fc.has_ext = p->P.ext ? 1 : 0;
     fc.has_fix = p->any_fix ? 1 : 0;
     fc.mixed = s->sp.precision == DEM_MIXED ? 1 : 0;
+    fc.stream_block = (s->sp.stream_block == 64 || s->sp.stream_block == 256) ? s->sp.stream_block : 128;
+    fc.scenes = s->nscenes > 0 ? s->d_scenes : nullptr;
+    fc.wps = s->nscenes > 0 ? s->wps : 0;
+    if (s->B.nscenes < p->nscenes) {   // per-scene grid descriptors and bounding boxes
+        cudaFree(s->B.grid);
+        cudaFree(s->B.bbox);
+        CK(dalloc(&s->B.grid, (size_t)p->nscenes));
+        CK(dalloc(&s->B.bbox, 8 * (size_t)p->nscenes));
+        s->B.nscenes = p->nscenes;
+        s->version++;
+    }
     CK(cudaStreamSynchronize(st));
     s->version++;
     return DEM_OK;
@@ -700,6 +744,13 @@ __global__ void k_clear_status(Ctl *ctl, int bits) {
 }
 
 bool ref_mode(const dem_solver *s) { return s->sp.rebuild_every_step != 0; }
+
+int check_walls(dem_solver *s) {
+    if (s->walls_ok) return DEM_OK;
+    return fail(s->ctx, DEM_ERR_INVALID,
+                "more walls than MaxNoWalls history slots per particle (assign per-scene walls with "
+                "dem_solver_set_scenes) or too few walls for the scenes");
+}
 
 // kernels issued by one launch_build (see dem_nbr.cu)
 long build_kernel_count(bool resort) { return 13 + (resort ? 4 : 0); }
@@ -763,8 +814,6 @@ extern "C" int dem_solver_create(dem_ctx *ctx, dem_particles *p, dem_walls *w, c
         return fail(ctx, DEM_ERR_INVALID, "dem_solver_create: null argument or dt <= 0");
     if (sp->precision != DEM_FP64 && sp->precision != DEM_MIXED)
         return fail(ctx, DEM_ERR_INVALID, "dem_solver_create: unknown precision");
-    if (w && w->n > p->P.mw && w->n > 0)
-        return fail(ctx, DEM_ERR_INVALID, "dem_solver_create: more walls than MaxNoWalls history slots");
     if (sp->delta <= 0.0 && sp->skin < 0.0) return fail(ctx, DEM_ERR_INVALID, "dem_solver_create: skin < 0");
     dem_solver *s = new dem_solver();
     s->ctx = ctx;
@@ -779,6 +828,8 @@ extern "C" int dem_solver_create(dem_ctx *ctx, dem_particles *p, dem_walls *w, c
     cudaError_t e = cudaSuccess;
     auto A = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
     A(dalloc(&B.grid, 1));
+    A(dalloc(&B.total, 1));
+    B.nscenes = 1;
     A(dalloc(&B.key, n));
     A(dalloc(&B.cell_start, (size_t)B.cell_cap + 1));
     A(dalloc(&B.cell_fill, (size_t)B.cell_cap + 1));
@@ -808,10 +859,10 @@ extern "C" int dem_solver_destroy(dem_solver *s) {
     if (!s) return DEM_ERR_INVALID;
     cudaStreamSynchronize(s->ctx->stream);
     if (s->graph) cudaGraphExecDestroy(s->graph);
-    cudaFree(s->d_pp); cudaFree(s->d_pw); cudaFree(s->d_walls);
+    cudaFree(s->d_pp); cudaFree(s->d_pw); cudaFree(s->d_walls); cudaFree(s->d_scenes);
     cudaFree(s->L.nn); cudaFree(s->L.idx); cudaFree(s->L.defer); cudaFree(s->L.defer_v); cudaFree(s->L.defer_w);
     BuildBuffers &B = s->B;
-    cudaFree(B.grid); cudaFree(B.key); cudaFree(B.cell_start); cudaFree(B.cell_fill); cudaFree(B.cell_items);
+    cudaFree(B.grid); cudaFree(B.total); cudaFree(B.key); cudaFree(B.cell_start); cudaFree(B.cell_fill); cudaFree(B.cell_items);
     cudaFree(B.block_sums); cudaFree(B.bbox); cudaFree(B.src); cudaFree(B.dst);
     cudaFree(s->d_epart); cudaFree(s->d_eout);
     delete s;
@@ -825,6 +876,10 @@ extern "C" int dem_solver_run(dem_solver *s, int nsteps) {
     if (s->p->mat_dirty || (s->p->P.ext != nullptr) != (s->fc.has_ext != 0)) {
         int st = prepare(s);
         if (st) return st;
+    }
+    {
+        const int wst = check_walls(s);
+        if (wst) return wst;
     }
     cudaStream_t st = ctx->stream;
     double half_skin;
@@ -904,6 +959,30 @@ extern "C" int dem_solver_stats(dem_solver *s, dem_run_stats *out) {
     return DEM_OK;
 }
 
+extern "C" int dem_solver_set_scenes(dem_solver *s, const dem_scene_params *params, int nscenes, int walls_per_scene) {
+    if (!s || !params || nscenes <= 0 || walls_per_scene < 0) return DEM_ERR_INVALID;
+    dem_ctx *ctx = s->ctx;
+    std::vector<SceneConst> sc(nscenes);
+    for (int k = 0; k < nscenes; ++k) {
+        const double bpp = beta_of(params[k].cor_pp), bpw = beta_of(params[k].cor_pw);
+        const unsigned q = s->fp.quirks;
+        sc[k].K_n_pp = -2. * std::sqrt(5. / 6.) * bpp;
+        sc[k].K_n_pw = -2. * std::sqrt(5. / 6.) * bpw;
+        sc[k].K_t_pp = (q & DEM_Q2_ETA_T_ZERO) ? -2 * std::sqrt((double)(5 / 6)) * bpp : sc[k].K_n_pp;
+        sc[k].K_t_pw = (q & DEM_Q2_ETA_T_ZERO) ? -2 * std::sqrt((double)(5 / 6)) * bpw : sc[k].K_n_pw;
+        sc[k].mu_pp = params[k].mu_pp;
+        sc[k].mu_pw = params[k].mu_pw;
+    }
+    cudaFree(s->d_scenes);
+    s->d_scenes = nullptr;
+    CK(dalloc(&s->d_scenes, (size_t)nscenes));
+    CK(cudaMemcpy(s->d_scenes, sc.data(), sizeof(SceneConst) * nscenes, cudaMemcpyHostToDevice));
+    s->nscenes = nscenes;
+    s->wps = walls_per_scene;
+    s->built = false;
+    return prepare(s);
+}
+
 extern "C" int dem_solver_profile(dem_solver *s, int nsteps, double *kernel_ms) {
     if (!s || !kernel_ms) return DEM_ERR_INVALID;
     *kernel_ms = 0.0;
@@ -913,6 +992,10 @@ extern "C" int dem_solver_profile(dem_solver *s, int nsteps, double *kernel_ms) 
     if (s->p->mat_dirty || (s->p->P.ext != nullptr) != (s->fc.has_ext != 0)) {
         int st = prepare(s);
         if (st) return st;
+    }
+    {
+        const int wst = check_walls(s);
+        if (wst) return wst;
     }
     cudaStream_t st = ctx->stream;
     const double half_skin = s->sp.delta > 0.0 ? std::max(0.0, s->sp.delta - 2.0 * s->p->rmax) / 2.0 : s->sp.skin / 2.0;
@@ -994,6 +1077,10 @@ extern "C" int dem_compute_force(dem_solver *s) {
     if (s->p->mat_dirty || (s->p->P.ext != nullptr) != (s->fc.has_ext != 0)) {
         int st = prepare(s);
         if (st) return st;
+    }
+    {
+        const int wst = check_walls(s);
+        if (wst) return wst;
     }
     if (!s->built) return fail(ctx, DEM_ERR_INVALID, "dem_compute_force: build the neighbour list first");
     launch_step(s->p->P, s->L, s->p->ctl, s->fc, s->d_pp, s->d_pw, s->d_walls, MODE_FORCE_ONLY, ctx->stream);

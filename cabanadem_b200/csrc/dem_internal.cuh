@@ -56,6 +56,7 @@ struct Particles {
     double *ext;   // may be null
     int *perm, *rank;
     unsigned long long *vslots;   // kVmaxSlots x 32 words: per-step max |u|^2, spread over L2 lines
+    int *scene;                   // [cap] scene of each particle, null when all share scene 0
 };
 
 constexpr int kVmaxSlots = 32;   // blocks fold their max into slot blockIdx % 32 (word 32 * slot)
@@ -84,6 +85,15 @@ struct ForceConsts {
     int has_ext;
     int has_fix;
     int mixed;                 // 1: FP32 contact forces (dem_mixed.cu)
+    int stream_block;          // k_stream block size: 64, 128 or 256
+    const struct SceneConst *scenes;   // per-scene damping/friction, null: the scalars above
+    int wps;                   // walls per scene (> 0 with scenes): scene s owns [s*wps, s*wps+wps)
+};
+
+// Per-scene force constants of batched independent scenes.
+struct SceneConst {
+    double K_n_pp, K_t_pp, K_n_pw, K_t_pw;
+    double mu_pp, mu_pw;
 };
 
 struct NbrList {
@@ -94,25 +104,27 @@ struct NbrList {
     double *defer_v, *defer_w;  // [3][cap] new u, omega of deferred particle t (slot t)
 };
 
-struct Grid {                 // computed on the device at every build
+struct Grid {                 // one per scene, computed on the device at every build
     double lo[3];
     double cell, inv_cell;
     int dims[3];
     int bits;                 // Morton bits per axis (0: linear cell index)
-    int ncodes;               // number of cell keys
+    int ncodes;               // number of cell keys of this scene
+    int base;                 // first key of this scene
     double rmax;
-    int overflow;             // cell keys exceeded the table
 };
 
 struct BuildBuffers {
-    Grid *grid;               // device
+    Grid *grid;               // device, [nscenes]
+    int *total;               // device: total cell keys over all scenes
+    int nscenes;              // scenes the grid array holds
     int *key;                 // [cap]
     int *cell_start;          // [cell_cap + 1]
     int *cell_fill;           // [cell_cap]
     int *cell_items;          // [cap] sorted-order index per cell slot
     int *block_sums;          // scan scratch
     int cell_cap;
-    unsigned long long *bbox; // 7 ordered-int words: lo[3], hi[3], rmax
+    unsigned long long *bbox; // 8 ordered-int words per scene: lo[3], hi[3], rmax
     int *src, *dst;           // permutation at re-sort
 };
 

@@ -47,8 +47,9 @@ __device__ __forceinline__ unsigned part1by2(unsigned x) {
 }
 
 __device__ __forceinline__ int cell_key(const Grid &g, int cx, int cy, int cz) {
-    if (g.bits > 0) return (int)(part1by2((unsigned)cx) | (part1by2((unsigned)cy) << 1) | (part1by2((unsigned)cz) << 2));
-    return (cz * g.dims[1] + cy) * g.dims[0] + cx;
+    if (g.bits > 0)
+        return g.base + (int)(part1by2((unsigned)cx) | (part1by2((unsigned)cy) << 1) | (part1by2((unsigned)cz) << 2));
+    return g.base + (cz * g.dims[1] + cy) * g.dims[0] + cx;
 }
 
 __device__ __forceinline__ void cell_of(const Grid &g, const D4 &p, int c[3]) {
@@ -60,83 +61,178 @@ __device__ __forceinline__ void cell_of(const Grid &g, const D4 &p, int c[3]) {
     }
 }
 
-__global__ void k_bbox_init(unsigned long long *bb) {
-    if (threadIdx.x < 3) bb[threadIdx.x] = ord(1e300);
-    else if (threadIdx.x < 6) bb[threadIdx.x] = ord(-1e300);
-    else if (threadIdx.x == 6) bb[6] = ord(0.0);
+__device__ __forceinline__ int scene_of(const Particles &P, int i) { return P.scene ? P.scene[i] : 0; }
+
+// 8 ordered-integer words per scene: lo[3], hi[3], rmax, unused
+__global__ void k_bbox_init(unsigned long long *bb, int nscenes) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 8 * nscenes; t += gridDim.x * blockDim.x) {
+        const int k = t & 7;
+        bb[t] = k < 3 ? ord(1e300) : (k < 6 ? ord(-1e300) : ord(0.0));
+    }
 }
 
 __global__ void k_bbox(Particles P, const Ctl *ctl, unsigned long long *bb) {
-    __shared__ unsigned long long s[7];
-    if (threadIdx.x < 7) s[threadIdx.x] = threadIdx.x < 3 ? ord(1e300) : (threadIdx.x < 6 ? ord(-1e300) : ord(0.0));
-    __syncthreads();
     const int cur = ctl->cur;
+    if (!P.scene) {   // one scene: block reduction, one atomic per word per block
+        __shared__ unsigned long long s[7];
+        if (threadIdx.x < 7) s[threadIdx.x] = threadIdx.x < 3 ? ord(1e300) : (threadIdx.x < 6 ? ord(-1e300) : ord(0.0));
+        __syncthreads();
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += gridDim.x * blockDim.x) {
+            const D4 p = ld4(P.pos[cur], i);
+            atomicMin(&s[0], ord(p.x));
+            atomicMin(&s[1], ord(p.y));
+            atomicMin(&s[2], ord(p.z));
+            atomicMax(&s[3], ord(p.x));
+            atomicMax(&s[4], ord(p.y));
+            atomicMax(&s[5], ord(p.z));
+            atomicMax(&s[6], ord(p.w));
+        }
+        __syncthreads();
+        if (threadIdx.x < 3) atomicMin(&bb[threadIdx.x], s[threadIdx.x]);
+        else if (threadIdx.x < 7) atomicMax(&bb[threadIdx.x], s[threadIdx.x]);
+        return;
+    }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += gridDim.x * blockDim.x) {
         const D4 p = ld4(P.pos[cur], i);
-        atomicMin(&s[0], ord(p.x));
-        atomicMin(&s[1], ord(p.y));
-        atomicMin(&s[2], ord(p.z));
-        atomicMax(&s[3], ord(p.x));
-        atomicMax(&s[4], ord(p.y));
-        atomicMax(&s[5], ord(p.z));
-        atomicMax(&s[6], ord(p.w));
+        unsigned long long *w = bb + 8L * P.scene[i];
+        atomicMin(&w[0], ord(p.x));
+        atomicMin(&w[1], ord(p.y));
+        atomicMin(&w[2], ord(p.z));
+        atomicMax(&w[3], ord(p.x));
+        atomicMax(&w[4], ord(p.y));
+        atomicMax(&w[5], ord(p.z));
+        atomicMax(&w[6], ord(p.w));
+    }
+}
+
+// Per-scene grids: cell >= the largest cutoff of the scene, Morton keys when every scene's
+// Morton range fits the table, else linear keys, else larger cells; scene s's keys start at
+// grid[s].base.  One block.  A non-finite extent (a blown-up state) or a table that no cell
+// size fits gives every scene one cell and raises DEM_ERR_NAN; the cell sort and the list
+// kernels then skip their work, so the build stays bounded.
+__device__ bool scene_dims(const unsigned long long *w, double cell, double lo[3], int dims[3], int &bits,
+                           long long &morton_codes, long long &linear_codes) {
+    double hi[3];
+    bool ok = true;
+    for (int d = 0; d < 3; ++d) {
+        lo[d] = unord(w[d]);
+        hi[d] = unord(w[3 + d]);
+        if (isnan(lo[d]) || isnan(hi[d]) || isinf(hi[d] - lo[d])) ok = false;
+        if (!(hi[d] >= lo[d]) || !ok) lo[d] = hi[d] = 0.0;   // empty scene, or no usable extent
+    }
+    int dmax = 1;
+    linear_codes = 1;
+    for (int d = 0; d < 3; ++d) {
+        const double e = floor((hi[d] - lo[d]) / cell) + 1.0;
+        dims[d] = (int)fmin(e, 1e9);
+        dims[d] = dims[d] < 1 ? 1 : dims[d];
+        dmax = max(dmax, dims[d]);
+        linear_codes *= dims[d];
+        if (linear_codes > (1LL << 40)) linear_codes = 1LL << 40;
+    }
+    bits = 1;
+    while ((1 << bits) < dmax) ++bits;
+    morton_codes = bits <= 10 ? (1LL << (3 * bits)) : (1LL << 40);
+    return ok;
+}
+
+__global__ void k_grid(const unsigned long long *bb, Grid *grid, int *total, int nscenes, int cell_cap, double delta,
+                       double skin, Ctl *ctl) {
+    __shared__ long long sm[256], sl[256];
+    __shared__ int bad[256];
+    __shared__ double factor;
+    __shared__ int use_morton, done, invalid;
+    if (threadIdx.x == 0) {
+        factor = 1.0;
+        done = 0;
+        use_morton = 0;
+        invalid = 0;
     }
     __syncthreads();
-    if (threadIdx.x < 3) atomicMin(&bb[threadIdx.x], s[threadIdx.x]);
-    else if (threadIdx.x < 7) atomicMax(&bb[threadIdx.x], s[threadIdx.x]);
-}
-
-__global__ void k_grid(const unsigned long long *bb, Grid *g, int cell_cap, double delta, double skin) {
-    if (threadIdx.x != 0) return;
-    Grid G;
-    double lo[3], hi[3];
-    for (int d = 0; d < 3; ++d) {
-        lo[d] = unord(bb[d]);
-        hi[d] = unord(bb[3 + d]);
-        if (!(hi[d] >= lo[d])) hi[d] = lo[d];
+    for (int it = 0; it < 200 && !done; ++it) {
+        long long tm = 0, tl = 0;
+        int nb = 0;
+        for (int sc = threadIdx.x; sc < nscenes; sc += blockDim.x) {
+            const double rmax = unord(bb[8L * sc + 6]);
+            const double cut = delta > 0.0 ? delta : 2.0 * rmax + skin;
+            const double cell = (cut > 0.0 ? cut : 1.0) * factor;
+            double lo[3];
+            int dims[3], bits;
+            long long mc, lc;
+            if (!scene_dims(bb + 8L * sc, cell, lo, dims, bits, mc, lc) || !(cell < 1e300)) ++nb;
+            tm += mc;
+            tl += lc;
+        }
+        sm[threadIdx.x] = tm;
+        sl[threadIdx.x] = tl;
+        bad[threadIdx.x] = nb;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            long long a = 0, b = 0;
+            int nbad = 0;
+            for (int t = 0; t < (int)blockDim.x; ++t) {
+                a += sm[t];
+                b += sl[t];
+                nbad += bad[t];
+            }
+            if (nbad > 0 && it == 0) {   // non-finite extent: no cell size helps
+                invalid = 1;
+                done = 1;
+            } else if (a <= cell_cap) {
+                use_morton = 1;
+                done = 1;
+            } else if (b <= cell_cap) {
+                use_morton = 0;
+                done = 1;
+            } else {
+                factor *= 1.26;
+            }
+        }
+        __syncthreads();
     }
-    G.rmax = unord(bb[6]);
-    const double cut = delta > 0.0 ? delta : 2.0 * G.rmax + skin;
-    double cell = cut > 0.0 ? cut : 1.0;
-    G.overflow = 0;
-    for (int it = 0; it < 200; ++it) {
-        double tot = 1.0;
-        int dmax = 1;
-        for (int d = 0; d < 3; ++d) {
-            const double e = floor((hi[d] - lo[d]) / cell) + 1.0;
-            G.dims[d] = (int)fmin(e, 1e9);
-            tot *= e;
-            dmax = max(dmax, G.dims[d]);
-        }
-        int bits = 0;
-        while ((1 << bits) < dmax) ++bits;
-        if (bits <= 10 && (double)(1LL << (3 * bits)) <= (double)cell_cap) {
-            G.bits = bits > 0 ? bits : 1;
-            G.ncodes = 1 << (3 * G.bits);
-            break;
-        }
-        if (tot <= (double)cell_cap) {
+    if (threadIdx.x == 0 && !done) invalid = 1;
+    __syncthreads();
+    for (int sc = threadIdx.x; sc < nscenes; sc += blockDim.x) {
+        Grid G;
+        const double rmax = unord(bb[8L * sc + 6]);
+        const double cut = delta > 0.0 ? delta : 2.0 * rmax + skin;
+        G.cell = (cut > 0.0 ? cut : 1.0) * factor;
+        G.inv_cell = 1.0 / G.cell;
+        G.rmax = rmax;
+        long long mc, lc;
+        int bits;
+        scene_dims(bb + 8L * sc, G.cell, G.lo, G.dims, bits, mc, lc);
+        G.bits = use_morton ? bits : 0;
+        G.ncodes = (int)(use_morton ? mc : lc);
+        if (invalid) {
+            G.dims[0] = G.dims[1] = G.dims[2] = 1;
             G.bits = 0;
-            G.ncodes = (int)tot;
-            break;
+            G.ncodes = 1;
         }
-        cell *= 1.26;
+        G.base = 0;
+        grid[sc] = G;
     }
-    for (int d = 0; d < 3; ++d) G.lo[d] = lo[d];
-    G.cell = cell;
-    G.inv_cell = 1.0 / cell;
-    *g = G;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int run = 0;
+        for (int sc = 0; sc < nscenes; ++sc) {
+            grid[sc].base = run;
+            run += grid[sc].ncodes;
+        }
+        *total = run;
+        if (invalid) atomicOr(&ctl->status, DEM_ERR_NAN);
+    }
 }
 
-__global__ void k_zero(int *a, const Grid *g) {
-    const int n = g->ncodes + 1;
+__global__ void k_zero(int *a, const int *total) {
+    const int n = *total + 1;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = 0;
 }
 
-__global__ void k_count(Particles P, const Ctl *ctl, const Grid *g, int *key, int *cnt) {
-    const Grid G = *g;
+__global__ void k_count(Particles P, const Ctl *ctl, const Grid *grid, int *key, int *cnt) {
     const int cur = ctl->cur;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += gridDim.x * blockDim.x) {
+        const Grid &G = grid[scene_of(P, i)];
         int c[3];
         cell_of(G, ld4(P.pos[cur], i), c);
         const int k = cell_key(G, c[0], c[1], c[2]);
@@ -145,10 +241,10 @@ __global__ void k_count(Particles P, const Ctl *ctl, const Grid *g, int *key, in
     }
 }
 
-// Exclusive scan of cnt[0..ncodes) into start[0..ncodes]; 3 passes.
-__global__ void k_scan_tiles(const int *cnt, int *start, int *sums, const Grid *g) {
+// Exclusive scan of cnt[0..total) into start[0..total]; 3 passes.
+__global__ void k_scan_tiles(const int *cnt, int *start, int *sums, const int *total) {
     __shared__ int s[kB];
-    const int n = g->ncodes;
+    const int n = *total;
     const long base = (long)blockIdx.x * kScanTile;
     if (base >= n) return;
     int v[kScanItems];
@@ -175,10 +271,10 @@ __global__ void k_scan_tiles(const int *cnt, int *start, int *sums, const Grid *
     if (threadIdx.x == kB - 1) sums[blockIdx.x] = s[kB - 1];
 }
 
-__global__ void k_scan_sums(int *sums, const Grid *g, int *start) {
-    // single block of kB threads; tiles <= kB * kScanItems * ... handled by a serial outer loop
+__global__ void k_scan_sums(int *sums, const int *total, int *start) {
+    // single block of kB threads; the tile sums are scanned kB at a time
     __shared__ int s[kB];
-    const int n = g->ncodes;
+    const int n = *total;
     const int tiles = (n + kScanTile - 1) / kScanTile;
     int carry = 0;
     for (int base = 0; base < tiles; base += kB) {
@@ -200,8 +296,8 @@ __global__ void k_scan_sums(int *sums, const Grid *g, int *start) {
     if (threadIdx.x == 0) start[n] = carry;
 }
 
-__global__ void k_scan_add(int *start, int *fill, const int *sums, const Grid *g) {
-    const int n = g->ncodes;
+__global__ void k_scan_add(int *start, int *fill, const int *sums, const int *total) {
+    const int n = *total;
     const long base = (long)blockIdx.x * kScanTile;
     if (base >= n) return;
     const int add = sums[blockIdx.x];
@@ -223,8 +319,9 @@ __global__ void k_fill(int n, const int *key, int *fill, int *items) {
 }
 
 // Deterministic order inside each cell: ascending caller index.
-__global__ void k_cell_sort(const int *start, int *items, const int *perm, const Grid *g) {
-    const int n = g->ncodes;
+__global__ void k_cell_sort(const int *start, int *items, const int *perm, const int *total, const Ctl *ctl) {
+    if (ctl->status & DEM_ERR_NAN) return;   // one cell per scene: the list is not built
+    const int n = *total;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
         const int b = start[c], e = start[c + 1];
         for (int a = b + 1; a < e; ++a) {
@@ -259,6 +356,7 @@ __global__ void k_permute(Particles P, Particles A, const Ctl *ctl, const int *i
         }
         A.mI[p] = P.mI[q];
         A.mat[p] = P.mat[q];
+        if (P.scene) A.scene[p] = P.scene[q];
         A.fix[p] = P.fix[q];
         A.cstate[p] = P.cstate[q];
         for (int k = 0; k < P.mc; ++k) {
@@ -286,11 +384,13 @@ __global__ void k_flip(Ctl *ctl) {
 
 __global__ void __launch_bounds__(128) k_list(Particles P, NbrList L, Ctl *ctl, const Grid *g, const int *start,
                                               const int *items, double delta, double skin) {
-    const Grid G = *g;
     const int cur = ctl->cur, cap = P.cap;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool invalid = (ctl->status & DEM_ERR_NAN) != 0;
     int count = 0;
-    if (i < P.n) {
+    if (i < P.n && invalid) L.nn[i] = 0;
+    if (i < P.n && !invalid) {
+        const Grid G = g[scene_of(P, i)];
         const double4 *pc = P.pos[cur];
         const D4 pi = ld4(pc, i);
         int c[3];
@@ -370,18 +470,18 @@ void launch_build(const Particles &P, Particles &alt, const NbrList &L, BuildBuf
     const int gs = 148 * 8;
     const int tiles = (B.cell_cap + kScanTile) / kScanTile;
     k_build_begin<<<1, 32, 0, s>>>(ctl);
-    k_bbox_init<<<1, 32, 0, s>>>(B.bbox);
+    k_bbox_init<<<(8 * B.nscenes + 255) / 256, 256, 0, s>>>(B.bbox, B.nscenes);
     k_bbox<<<gs, kB, 0, s>>>(P, ctl, B.bbox);
-    k_grid<<<1, 32, 0, s>>>(B.bbox, B.grid, B.cell_cap, delta, skin);
-    k_zero<<<gs, kB, 0, s>>>(B.cell_start, B.grid);
+    k_grid<<<1, 256, 0, s>>>(B.bbox, B.grid, B.total, B.nscenes, B.cell_cap, delta, skin, ctl);
+    k_zero<<<gs, kB, 0, s>>>(B.cell_start, B.total);
     k_count<<<gs, kB, 0, s>>>(P, ctl, B.grid, B.key, B.cell_start);
     // cell_start holds counts now; scan into cell_fill (as start) then swap roles
-    k_scan_tiles<<<tiles, kB, 0, s>>>(B.cell_start, B.cell_fill, B.block_sums, B.grid);
-    k_scan_sums<<<1, kB, 0, s>>>(B.block_sums, B.grid, B.cell_fill);
-    k_scan_add<<<tiles, kB, 0, s>>>(B.cell_fill, B.cell_start, B.block_sums, B.grid);
+    k_scan_tiles<<<tiles, kB, 0, s>>>(B.cell_start, B.cell_fill, B.block_sums, B.total);
+    k_scan_sums<<<1, kB, 0, s>>>(B.block_sums, B.total, B.cell_fill);
+    k_scan_add<<<tiles, kB, 0, s>>>(B.cell_fill, B.cell_start, B.block_sums, B.total);
     // now cell_fill = exclusive start (with [ncodes] = n), cell_start = running cursor
     k_fill<<<gs, kB, 0, s>>>(n, B.key, B.cell_start, B.cell_items);
-    k_cell_sort<<<gs, kB, 0, s>>>(B.cell_fill, B.cell_items, P.perm, B.grid);
+    k_cell_sort<<<gs, kB, 0, s>>>(B.cell_fill, B.cell_items, P.perm, B.total, ctl);
     if (resort) {
         k_make_dst<<<gs, kB, 0, s>>>(n, B.cell_items, B.dst);
         k_permute<<<gs, kB, 0, s>>>(P, alt, ctl, B.cell_items, B.dst);
@@ -398,6 +498,7 @@ void launch_build(const Particles &P, Particles &alt, const NbrList &L, BuildBuf
         if (P.mw > 0)
             cudaMemcpyAsync(P.sw, alt.sw, 3 * (size_t)P.mw * cap * sizeof(double), cudaMemcpyDeviceToDevice, s);
         cudaMemcpyAsync(P.perm, alt.perm, cap * sizeof(int), cudaMemcpyDeviceToDevice, s);
+        if (P.scene) cudaMemcpyAsync(P.scene, alt.scene, cap * sizeof(int), cudaMemcpyDeviceToDevice, s);
         k_flip<<<1, 32, 0, s>>>(ctl);
         k_identity<<<gs, kB, 0, s>>>(n, B.cell_items);
     }

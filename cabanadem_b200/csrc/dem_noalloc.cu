@@ -36,7 +36,8 @@ constexpr int kNoAllocCellCap = 4 * DEM_NOALLOC_MAX_PARTICLES;
 constexpr size_t al(size_t x) { return (x + 255) & ~(size_t)255; }
 constexpr size_t kOffCtl = 0;
 constexpr size_t kOffGrid = al(kOffCtl + sizeof(Ctl));
-constexpr size_t kOffBbox = al(kOffGrid + sizeof(Grid));
+constexpr size_t kOffTotal = al(kOffGrid + sizeof(Grid));
+constexpr size_t kOffBbox = al(kOffTotal + sizeof(int));
 constexpr size_t kOffPos = al(kOffBbox + 8 * sizeof(unsigned long long));
 constexpr size_t kOffPerm = al(kOffPos + sizeof(double4) * DEM_NOALLOC_MAX_PARTICLES);
 constexpr size_t kOffKey = al(kOffPerm + sizeof(int) * DEM_NOALLOC_MAX_PARTICLES);
@@ -94,6 +95,8 @@ extern "C" int dem_neighbor_list_noalloc(const double *x, const double *rad, int
     Ctl *ctl = reinterpret_cast<Ctl *>(b + kOffCtl);
     BuildBuffers B{};
     B.grid = reinterpret_cast<Grid *>(b + kOffGrid);
+    B.total = reinterpret_cast<int *>(b + kOffTotal);
+    B.nscenes = 1;
     B.bbox = reinterpret_cast<unsigned long long *>(b + kOffBbox);
     B.key = reinterpret_cast<int *>(b + kOffKey);
     B.cell_items = reinterpret_cast<int *>(b + kOffItems);
@@ -116,5 +119,5 @@ extern "C" int dem_neighbor_list_noalloc(const double *x, const double *rad, int
     if (cudaMemcpyAsync(&status, &ctl->status, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess)
         return DEM_ERR_CUDA;
     if (cudaStreamSynchronize(s) != cudaSuccess) return DEM_ERR_CUDA;
-    return status & DEM_ERR_NEIGHBOR_OVERFLOW;
+    return status & (DEM_ERR_NEIGHBOR_OVERFLOW | DEM_ERR_NAN);
 }

@@ -13,10 +13,6 @@ namespace b200dem {
 namespace {
 
 constexpr int kBlock = 128;
-#ifndef STREAM_BLOCK
-#define STREAM_BLOCK 128   // small blocks: a warp stuck on a neighbour loop holds fewer others
-#endif
-constexpr int kStreamBlock = STREAM_BLOCK;
 constexpr int kApplyBlock = 256;
 
 struct __align__(32) D4 {
@@ -170,6 +166,14 @@ __device__ __forceinline__ void particle_full(const Particles &P, const NbrList 
                                               double &vmax2, int &status) {
     const int cap = P.cap;
     const unsigned q = fc.quirks;
+    // batched scenes: this particle's scene supplies damping, friction and its walls
+    const int scene_i = P.scene ? P.scene[i] : 0;
+    const SceneConst *scn = fc.scenes ? fc.scenes + scene_i : nullptr;
+    const double K_n_pp = scn ? scn->K_n_pp : fc.K_n_pp, K_t_pp = scn ? scn->K_t_pp : fc.K_t_pp;
+    const double K_n_pw = scn ? scn->K_n_pw : fc.K_n_pw, K_t_pw = scn ? scn->K_t_pw : fc.K_t_pw;
+    const double mu_pp = scn ? scn->mu_pp : fc.mu_pp, mu_pw = scn ? scn->mu_pw : fc.mu_pw;
+    const int wall0 = fc.wps ? scene_i * fc.wps : 0;
+    const int wall1 = fc.wps ? wall0 + fc.wps : fc.nwall;
     const double4 *__restrict__ pc = P.pos[cur];
     const double *__restrict__ vc = P.vel[vcur];
     const double *__restrict__ wc = P.omg[vcur];
@@ -313,9 +317,9 @@ __device__ __forceinline__ void particle_full(const Particles &P, const NbrList 
             const float sro = sqrtf(R_eff * ov);
             const float kn = (float)c.c_kn * sqrtf(R_eff);
             const float S_n = (float)c.c_Sn * sro;
-            const float eta_n = (float)fc.K_n_pp * sqrtf(S_n * m_eff);
+            const float eta_n = (float)K_n_pp * sqrtf(S_n * m_eff);
             const float kt = (float)c.c_kt * sro;
-            const float eta_t = (float)fc.K_t_pp * sqrtf(kt * m_eff);
+            const float eta_t = (float)K_t_pp * sqrtf(kt * m_eff);
             const float fn = kn * ov * sqrtf(ov);
             const float fn0 = fn * fnx - eta_n * (vdn * fnx);
             const float fn1 = fn * fny - eta_n * (vdn * fny);
@@ -345,7 +349,7 @@ __device__ __forceinline__ void particle_full(const Particles &P, const NbrList 
                 const float ft2 = -kt * (float)h2 - eta_t * vt2;
                 const float ft_magn = sqrtf(ft0 * ft0 + ft1 * ft1 + ft2 * ft2);
                 const float fn_magn = sqrtf(fn0 * fn0 + fn1 * fn1 + fn2 * fn2);
-                const float lim = (float)fc.mu_pp * fn_magn;
+                const float lim = (float)mu_pp * fn_magn;
                 const float fms = ft_magn > lim ? lim : ft_magn;
                 tf0 = -fms * ti0;
                 tf1 = -fms * ti1;
@@ -390,9 +394,9 @@ __device__ __forceinline__ void particle_full(const Particles &P, const NbrList 
         const double kn = c.c_kn * sqrt(R_eff);
         const double S_n = c.c_Sn * sqrt(R_eff * overlap);
         const double m_eff = 1. / (1. / mIi.x + 1. / P.mI[j].x);
-        const double eta_n = fc.K_n_pp * sqrt(S_n * m_eff);
+        const double eta_n = K_n_pp * sqrt(S_n * m_eff);
         const double kt = c.c_kt * sqrt(R_eff * overlap);
-        const double eta_t = fc.K_t_pp * sqrt(kt * m_eff);
+        const double eta_t = K_t_pp * sqrt(kt * m_eff);
         const double fn = kn * (overlap * sqrt(overlap));
         const double fn0 = fn * nx - eta_n * vn0;
         const double fn1 = fn * ny - eta_n * vn1;
@@ -423,7 +427,7 @@ __device__ __forceinline__ void particle_full(const Particles &P, const NbrList 
             const double ft_magn = sqrt(ft0 * ft0 + ft1 * ft1 + ft2 * ft2);
             const double fn_magn = sqrt(fn0 * fn0 + fn1 * fn1 + fn2 * fn2);
             double fms = ft_magn;
-            if (fms > fc.mu_pp * fn_magn) fms = fc.mu_pp * fn_magn;
+            if (fms > mu_pp * fn_magn) fms = mu_pp * fn_magn;
             tf0 = -fms * ti0;
             tf1 = -fms * ti1;
             tf2 = -fms * ti2;
@@ -461,16 +465,17 @@ __device__ __forceinline__ void particle_full(const Particles &P, const NbrList 
         }
     }
     // ---- particle-infinite wall (Force.hpp:475-673)
-    for (int w = 0; w < fc.nwall; ++w) {
+    for (int w = wall0; w < wall1; ++w) {
         const WallGeom g = walls[w];
+        const int lw = w - wall0;   // this particle's wall slot
         const double px = pi.x - g.x[0], py = pi.y - g.x[1], pz = pi.z - g.x[2];
         const double nx = g.n[0], ny = g.n[1], nz = g.n[2];
         const double tmp = px * nx + py * ny + pz * nz;
         const double overlap = pi.w - tmp;
-        const unsigned bit = 1u << w;
-        double *swx = P.sw + (long)w * cap + i;
-        double *swy = P.sw + (long)(P.mw + w) * cap + i;
-        double *swz = P.sw + (long)(2 * P.mw + w) * cap + i;
+        const unsigned bit = 1u << lw;
+        double *swx = P.sw + (long)lw * cap + i;
+        double *swy = P.sw + (long)(P.mw + lw) * cap + i;
+        double *swz = P.sw + (long)(2 * P.mw + lw) * cap + i;
         if (MIXED && overlap > 0.) {
             const float ov = (float)overlap;
             const double da_i = pi.w - 0.5 * overlap;
@@ -489,7 +494,7 @@ __device__ __forceinline__ void particle_full(const Particles &P, const NbrList 
             const float sro = sqrtf(R_eff * ov);
             const float kn = (float)c.c_kn * sqrtf(R_eff);
             const float S_n = (float)c.c_Sn * sro;
-            const float eta_n = (float)fc.K_n_pw * sqrtf(S_n * m_eff);
+            const float eta_n = (float)K_n_pw * sqrtf(S_n * m_eff);
             const float fn = kn * ov * sqrtf(ov);
             const float fn0 = fn * gx - eta_n * (vdn * gx);
             const float fn1 = fn * gy - eta_n * (vdn * gy);
@@ -511,7 +516,7 @@ __device__ __forceinline__ void particle_full(const Particles &P, const NbrList 
                 s1 += (dv1 - dvdn * ny) * fc.dt;
                 s2 += (dv2 - dvdn * nz) * fc.dt;
                 const float kt = (float)c.c_kt * sro;
-                const float eta_t = (float)fc.K_t_pw * sqrtf(kt * m_eff);
+                const float eta_t = (float)K_t_pw * sqrtf(kt * m_eff);
                 const float fx = -kt * (float)s0 - eta_t * vt0;
                 const float fy = -kt * (float)s1 - eta_t * vt1;
                 const float fz = -kt * (float)s2 - eta_t * vt2;
@@ -524,7 +529,7 @@ __device__ __forceinline__ void particle_full(const Particles &P, const NbrList 
                     ti2 = fz / ft_magn;
                 }
                 const float fn_magn = sqrtf(fn0 * fn0 + fn1 * fn1 + fn2 * fn2);
-                const float lim = (float)fc.mu_pw * fn_magn;
+                const float lim = (float)mu_pw * fn_magn;
                 const float fms = (ft_magn < lim) ? ft_magn : lim;
                 ft0 = fms * ti0 + eta_t * vt0;
                 ft1 = fms * ti1 + eta_t * vt1;
@@ -552,7 +557,7 @@ __device__ __forceinline__ void particle_full(const Particles &P, const NbrList 
             const double kn = c.c_kn * sqrt(R_eff);
             const double S_n = c.c_Sn * sqrt(R_eff * overlap);
             const double m_eff = 1. / (1. / mIi.x + 0.);
-            const double eta_n = fc.K_n_pw * sqrt(S_n * m_eff);
+            const double eta_n = K_n_pw * sqrt(S_n * m_eff);
             const double fn = kn * (overlap * sqrt(overlap));
             const double fn0 = fn * nx - eta_n * (vdn * nx);
             const double fn1 = fn * ny - eta_n * (vdn * ny);
@@ -574,7 +579,7 @@ __device__ __forceinline__ void particle_full(const Particles &P, const NbrList 
                 s1 += vt1 * fc.dt;
                 s2 += vt2 * fc.dt;
                 const double kt = c.c_kt * sqrt(R_eff * overlap);
-                const double eta_t = fc.K_t_pw * sqrt(kt * m_eff);
+                const double eta_t = K_t_pw * sqrt(kt * m_eff);
                 const double fx = -kt * s0 - eta_t * vt0;
                 const double fy = -kt * s1 - eta_t * vt1;
                 const double fz = -kt * s2 - eta_t * vt2;
@@ -587,7 +592,7 @@ __device__ __forceinline__ void particle_full(const Particles &P, const NbrList 
                     ti2 = fz / ft_magn;
                 }
                 const double fn_magn = sqrt(fn0 * fn0 + fn1 * fn1 + fn2 * fn2);
-                const double lim = fc.mu_pw * fn_magn;
+                const double lim = mu_pw * fn_magn;
                 const double fms = (ft_magn < lim) ? ft_magn : lim;  // std::min(lim, ft_magn)
                 ft0 = fms * ti0;
                 ft1 = fms * ti1;

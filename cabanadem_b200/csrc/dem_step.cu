@@ -49,13 +49,12 @@ __device__ __forceinline__ bool step_gate(const Ctl *ctl) {
 // neighbour reads them.  Every other particle is appended to L.defer for kernel 2.
 // Each thread reads the control word itself (no block barrier before the work).
 // ---------------------------------------------------------------------------------------
-#ifndef STREAM_MIN_BLOCKS
-#define STREAM_MIN_BLOCKS 10  // <= 48 registers: 10 blocks of 128 per SM (B200 sweep of block size
-                              // 64/128/256 and 4..16 blocks: 128 x 10 fastest on the 2M lattice)
-#endif
-__global__ void __launch_bounds__(kStreamBlock, STREAM_MIN_BLOCKS) k_stream(Particles P, NbrList L, Ctl *ctl,
-                                                                           ForceConsts fc,
-                                                                           const WallGeom *__restrict__ walls) {
+// Block size is a run-time choice (dem_solver_params.stream_block): 64 x 16, 128 x 10 or
+// 256 x 4 blocks per SM (register caps 64, 48, 64).  On the 2M lattice 128 x 10 was fastest in a
+// B200 sweep; the autotuner picks per workload.
+template <int BS, int MINB>
+__global__ void __launch_bounds__(BS, MINB) k_stream(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
+                                                     const WallGeom *__restrict__ walls) {
     if (!step_gate(ctl)) return;
     const int cur = ctl->cur, vcur = ctl->vcur;
     const bool last = ctl->steps_done + 1 >= ctl->target;
@@ -98,7 +97,10 @@ __global__ void __launch_bounds__(kStreamBlock, STREAM_MIN_BLOCKS) k_stream(Part
             const double sr = pi.w + pj.w;
             defer = !(r2ij >= sr * sr * 1.0000000001);
         }
-        for (int w = 0; w < fc.nwall && !defer; ++w) {
+        const int scene_i = P.scene ? P.scene[i] : 0;
+        const int wall0 = fc.wps ? scene_i * fc.wps : 0;
+        const int wall1 = fc.wps ? wall0 + fc.wps : fc.nwall;
+        for (int w = wall0; w < wall1 && !defer; ++w) {
             const WallGeom g = walls[w];
             const double tmp = (pi.x - g.x[0]) * g.n[0] + (pi.y - g.x[1]) * g.n[1] + (pi.z - g.x[2]) * g.n[2];
             defer = (pi.w - tmp) > 0.;
@@ -298,7 +300,10 @@ __global__ void __launch_bounds__(kBlock) k_energy_partials(Particles P, NbrList
                 e[2] += 0.5 * 0.4 * kn * ov * ov * sqrt(ov);  // half of each pair (full list)
             }
         }
-        for (int w = 0; w < fc.nwall; ++w) {
+        const int scene_i = P.scene ? P.scene[i] : 0;
+        const int wall0 = fc.wps ? scene_i * fc.wps : 0;
+        const int wall1 = fc.wps ? wall0 + fc.wps : fc.nwall;
+        for (int w = wall0; w < wall1; ++w) {
             const WallGeom g = walls[w];
             const double ov = pi.w - ((pi.x - g.x[0]) * g.n[0] + (pi.y - g.x[1]) * g.n[1] + (pi.z - g.x[2]) * g.n[2]);
             if (ov > 0.) {
@@ -362,7 +367,12 @@ void launch_step(const Particles &P, const NbrList &L, Ctl *ctl, const ForceCons
             ga = 32;
             last_n = P.n;
         }
-        k_stream<<<(P.n + kStreamBlock - 1) / kStreamBlock, kStreamBlock, 0, s>>>(P, L, ctl, fc, walls);
+        if (fc.stream_block == 64)
+            k_stream<64, 16><<<(P.n + 63) / 64, 64, 0, s>>>(P, L, ctl, fc, walls);
+        else if (fc.stream_block == 256)
+            k_stream<256, 4><<<(P.n + 255) / 256, 256, 0, s>>>(P, L, ctl, fc, walls);
+        else
+            k_stream<128, 10><<<(P.n + 127) / 128, 128, 0, s>>>(P, L, ctl, fc, walls);
         if (fc.mixed)
             launch_contact_mixed(P, L, ctl, fc, pp, pw, walls, gm, s);
         else

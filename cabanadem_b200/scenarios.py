@@ -171,6 +171,70 @@ def bonded_bar(nx=256, ny=64, nz=8, radius=0.5e-3, pull=0.05, dt=2e-8, nsteps=50
                              break_strain=break_strain))
 
 
+def batched_scenes(nscenes=1024, nmin=2, nmax=8192, radius=1e-3, seed=3, dt=1e-7, nsteps=20_000,
+                   quirks=REF_COMPAT, max_cnts=16):
+    """Independent scenes in one batch: scene k is a compact random cluster of n_k spheres
+    (n_k log-uniform in [2, 8192]) of r = 1 mm glass, fired at its own plane y = 0 at an angle
+    U[0, 90] degrees from the normal and a speed U[1, 5] m/s, with restitution U[0.3, 0.95]
+    and friction U[0.1, 0.5] (pp and pw alike).  All scenes share local coordinates; the
+    scene index keeps them apart.  dt = 1e-7 s."""
+    rng = np.random.default_rng(seed)
+    counts = np.floor(np.exp(rng.uniform(np.log(nmin), np.log(nmax), size=nscenes))).astype(int)
+    counts = np.clip(counts, nmin, nmax)
+    # lattice points of pitch 2.05 r sorted by distance from the origin: a scene takes the first n_k
+    pitch = 2.05 * radius
+    m = int(np.ceil((nmax * 6 / np.pi) ** (1 / 3))) + 2
+    g = np.arange(-m, m + 1)
+    lat = np.stack(np.meshgrid(g, g, g, indexing="ij"), axis=-1).reshape(-1, 3).astype(float) * pitch
+    lat = lat[np.argsort((lat ** 2).sum(axis=1), kind="stable")][:nmax]
+    n = int(counts.sum())
+    s = ParticleState.create(n, max_cnts=max_cnts, max_walls=1)
+    scene = np.repeat(np.arange(nscenes), counts).astype(np.int32)
+    params, walls = [], WallState.create(nscenes)
+    off = 0
+    for k in range(nscenes):
+        c = counts[k]
+        pts = lat[:c] + rng.uniform(-0.02, 0.02, size=(c, 3)) * radius
+        theta = np.deg2rad(rng.uniform(0.0, 90.0))
+        speed = rng.uniform(1.0, 5.0)
+        e, mu = rng.uniform(0.3, 0.95), rng.uniform(0.1, 0.5)
+        pts[:, 1] += -pts[:, 1].min() + radius * 1.02     # lowest sphere just above the plane
+        s.x[off:off + c] = pts
+        s.u[off:off + c] = (speed * np.sin(theta), -speed * np.cos(theta), 0.0)
+        params.append((e, e, mu, mu))
+        walls.x[k] = (0.0, 0.0, 0.0)
+        walls.normal[k] = (0.0, 1.0, 0.0)
+        off += c
+    _apply_glass(s, radius)
+    walls.E[:], walls.nu[:], walls.G[:] = GLASS["E"], GLASS["nu"], s.G[0]
+    sc = Scenario("batched_%d" % nscenes, s, walls, _force_params(0.8, 0.8, 0.3, 0.3, quirks), dt, nsteps,
+                  skin=0.1 * radius)
+    sc.extra = dict(scene=scene, scene_params=params, walls_per_scene=1, counts=counts)
+    return sc
+
+
+def scene_subset(sc, k):
+    """Scenario of scene k of a batched_scenes set on its own (its particles, wall and
+    restitution/friction), for checking the batch against separate runs."""
+    counts = sc.extra["counts"]
+    start = int(counts[:k].sum())
+    c = int(counts[k])
+    st = ParticleState.create(c, max_cnts=sc.state.max_cnts, max_walls=1)
+    for f, v in sc.state.arrays().items():
+        if f.startswith("tng_sw"):
+            getattr(st, f)[:] = v[start:start + c, :1]
+        else:
+            getattr(st, f)[...] = v[start:start + c]
+    w = WallState.create(1)
+    for f in ("x", "u", "omega", "normal"):
+        getattr(w, f)[0] = getattr(sc.walls, f)[k]
+    for f in ("E", "nu", "G"):
+        getattr(w, f)[0] = getattr(sc.walls, f)[k]
+    e_pp, e_pw, mu_pp, mu_pw = sc.extra["scene_params"][k]
+    return Scenario("scene_%d" % k, st, w, _force_params(e_pp, e_pw, mu_pp, mu_pw, sc.params["quirks"]), sc.dt,
+                    sc.nsteps, skin=sc.skin, gravity=sc.gravity)
+
+
 def bdem_two_particles():
     """examples/tst_01_BDEM_two_particles_tensile_3D.cpp:162-302: two bonded spheres
     pulled apart by +-1e3 N, particle 0's force zeroed after the bond pass."""

@@ -69,6 +69,7 @@ enum dem_field {
     DEM_F_TNG_SW_Z,
     DEM_F_FIX,          /* uint8  [n]  DEM_FIX_* flags (boundary-condition hook)      */
     DEM_F_EXT_FORCE,    /* double [n][3] external force added before the pair forces  */
+    DEM_F_SCENE,        /* int    [n]  scene index for batched independent scenes      */
     DEM_F_COUNT_
 };
 #define DEM_FIX_FORCE  0x1 /* zero F after the force pass (tst_01_BDEM:19-67)           */
@@ -102,6 +103,7 @@ typedef struct dem_solver_params {
     double gravity[3];     /* body acceleration, added after the pair forces                 */
     int max_neighbors;     /* initial neighbour-list capacity per particle (0 = 32)          */
     int steps_per_launch;  /* fused steps per captured graph (0 = 32)                        */
+    int stream_block;      /* streaming-kernel block size: 64, 128 or 256 (0 = 128)          */
 } dem_solver_params;
 
 typedef struct dem_run_stats {
@@ -153,6 +155,16 @@ int dem_solver_stats(dem_solver *s, dem_run_stats *out);
  * two CUDA events; *kernel_ms receives the mean duration of one fused step launch
  * (rebuilds excluded).  For roofline measurement; no reference counterpart. */
 int dem_solver_profile(dem_solver *s, int nsteps, double *kernel_ms);
+
+/* Batched independent scenes (no reference counterpart).  Each particle belongs to the scene
+ * given by DEM_F_SCENE; particles of different scenes never interact, whatever their
+ * coordinates (the neighbour grid is built per scene).  Scene k uses params[k] for its
+ * restitution and friction and owns walls [k*walls_per_scene, (k+1)*walls_per_scene) of the
+ * solver's wall set; walls_per_scene <= MaxNoWalls.  All scenes advance in the same launches. */
+typedef struct dem_scene_params {
+    double cor_pp, cor_pw, mu_pp, mu_pw;
+} dem_scene_params;
+int dem_solver_set_scenes(dem_solver *s, const dem_scene_params *params, int nscenes, int walls_per_scene);
 
 /* Reference-order phases, one launch each, for callers that drive the loop themselves:
  * Integrator::stage1/2/3 (src/CabanaDEM_Integrator.hpp:31-102), neighbors->build
@@ -223,7 +235,8 @@ int dem_bonded_run(dem_bonds *b, int nsteps);
  *                                 order, slot-major (partner k of particle i at idx[k*n + i])
  *   stream                        cudaStream_t (NULL: default stream); synchronised on return
  * Returns DEM_ERR_INVALID when n > DEM_NOALLOC_MAX_PARTICLES and DEM_ERR_NEIGHBOR_OVERFLOW when
- * a particle has more than max_neighbors partners (its list is cut at max_neighbors).
+ * a particle has more than max_neighbors partners (its list is cut at max_neighbors), and
+ * DEM_ERR_NAN when a position or radius is not finite (every list is then empty).
  * All calls share the scratch array and it keeps the last call's contents: calls that could
  * overlap on the GPU race and must be ordered by the caller.  The first call on a device looks
  * up the array's address (with that device current); make that call before any stream

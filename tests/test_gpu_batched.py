@@ -1,0 +1,78 @@
+"""Batched independent scenes: many clusters of uneven size fired at their own walls, all
+advanced by the same launches.  A scene in the batch must evolve exactly as it does alone (the
+neighbour grid is per scene, restitution/friction and walls come from the scene's table), and
+alone it must match the oracle; tuned launch settings must not change any result."""
+import os
+
+import numpy as np
+import pytest
+
+from cabanadem_b200 import api, autotune, scenarios as S
+from cabanadem_b200._lib import DEM_FP64, DEM_MIXED
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+STATE = ("x", "u", "omega", "force", "torque", "tng_count")
+
+
+def _scene_slice(st, start, c):
+    return {f: getattr(st, f)[start:start + c] for f in STATE}
+
+
+def test_batch_equals_scenes_run_alone_and_oracle():
+    sc = S.batched_scenes(nscenes=12, nmax=400, seed=21, nsteps=400)
+    s = api.from_scenario(sc)
+    s.run_steps(400)
+    got = s.particles.download()
+    counts = sc.extra["counts"]
+    starts = np.concatenate([[0], np.cumsum(counts)])
+    for k in range(len(counts)):
+        sub = S.scene_subset(sc, k)
+        alone = api.from_scenario(sub)
+        alone.run_steps(400)
+        a = alone.particles.download()
+        ref = sub.state.copy()
+        O.run(ref, sub.walls, sub.params, sub.dt, 400, skin=sub.skin, pow_mode=O.POW_SQRT)
+        mine = _scene_slice(got, starts[k], counts[k])
+        for f in STATE:
+            assert np.array_equal(mine[f], getattr(a, f)), (k, f)
+            assert np.array_equal(mine[f], getattr(ref, f)), (k, f, "oracle")
+    assert got.tng_count.sum() > 0 or np.abs(got.force).max() > 0
+
+
+def test_launch_settings_do_not_change_results(tmp_path):
+    sc = S.batched_scenes(nscenes=24, nmax=2000, seed=5, nsteps=150)
+    outs = []
+    for cfg in ({"stream_block": 64, "steps_per_launch": 16, "skin_factor": 0.5},
+                {"stream_block": 256, "steps_per_launch": 64, "skin_factor": 2.0},
+                dict(autotune.DEFAULTS)):
+        sc2 = S.batched_scenes(nscenes=24, nmax=2000, seed=5, nsteps=150)
+        kw = autotune.apply(sc2, cfg)
+        s = api.from_scenario(sc2, **kw)
+        s.run_steps(150)
+        outs.append(s.particles.download())
+    for o in outs[1:]:
+        for f in STATE:
+            assert np.array_equal(getattr(o, f), getattr(outs[0], f)), f
+
+
+def test_autotuner_picks_and_caches(tmp_path, monkeypatch):
+    monkeypatch.setenv("CABANADEM_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
+    sc = S.batched_scenes(nscenes=64, nmax=4096, seed=9, nsteps=100)
+    cfg = autotune.tune(sc, precision=DEM_MIXED, warmup=5, steps=40)
+    assert cfg["stream_block"] in (64, 128, 256)
+    assert os.path.exists(tmp_path / "tune.json")
+    assert autotune.tune(sc, precision=DEM_MIXED) == cfg    # served from the cache
+
+
+def test_full_batch_mixed_matches_fp64():
+    """The 1,024-scene batch (about 0.94M spheres): 50 steps mixed vs FP64."""
+    a = api.from_scenario(S.batched_scenes(nsteps=50), precision=DEM_FP64)
+    a.run_steps(50)
+    b = api.from_scenario(S.batched_scenes(nsteps=50), precision=DEM_MIXED)
+    b.run_steps(50)
+    fa, fb = a.particles.get("force"), b.particles.get("force")
+    assert np.all(np.isfinite(fb))
+    assert np.abs(fb - fa).max() <= 1e-5 * np.abs(fa).max()
+    assert np.array_equal(a.particles.get("tng_count"), b.particles.get("tng_count"))
