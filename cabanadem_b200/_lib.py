@@ -57,6 +57,15 @@ class RunStats(C.Structure):
                 ("launches", C.c_long)]
 
 
+class NnRows(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("index", C.c_void_p), ("width", C.c_int)]
+
+
+class NnMlp(C.Structure):
+    _fields_ = [("kin", C.c_int), ("nout", C.c_int), ("w1t", C.c_void_p), ("w1", C.c_void_p), ("b1", C.c_void_p),
+                ("w2t", C.c_void_p), ("w2", C.c_void_p), ("b2", C.c_void_p)]
+
+
 class DemError(RuntimeError):
     pass
 
@@ -100,6 +109,11 @@ _PROTOS = {
     "dem_bonds_broken": ([_VP, C.POINTER(C.c_long)], C.c_int),
     "dem_bonded_run": ([_VP, C.c_int], C.c_int),
     "dem_neighbor_list_noalloc": ([_VP, _VP, C.c_int, C.c_double, C.c_double, C.c_int, _VP, _VP, _VP], C.c_int),
+    "dem_nn_mlp_forward": ([_VP, C.POINTER(NnMlp), C.c_long, C.POINTER(NnRows), C.c_int, _VP, _VP, _VP, _VP],
+                           C.c_int),
+    "dem_nn_mlp_backward": ([_VP, C.POINTER(NnMlp), C.c_long, C.POINTER(NnRows), C.c_int, _VP, _VP, _VP, _VP, _VP,
+                             _VP, _VP, _VP], C.c_int),
+    "dem_nn_status": ([_VP, C.POINTER(C.c_int)], C.c_int),
 }
 NOALLOC_MAX_PARTICLES = 32768
 

@@ -24,6 +24,9 @@ struct dem_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     std::string err;
+    int *d_err = nullptr;           // error word of the tensor-core kernels
+    float *nn_part = nullptr;       // per-CTA weight-gradient partials
+    long nn_part_floats = 0;
 };
 
 struct dem_particles {
@@ -283,6 +286,8 @@ extern "C" int dem_ctx_create(int device, dem_ctx **out) {
 extern "C" int dem_ctx_destroy(dem_ctx *ctx) {
     if (!ctx) return DEM_ERR_INVALID;
     cudaStreamSynchronize(ctx->stream);
+    cudaFree(ctx->d_err);
+    cudaFree(ctx->nn_part);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return DEM_OK;
@@ -1288,4 +1293,72 @@ extern "C" int dem_bonded_run(dem_bonds *b, int nsteps) {
         if (c.steps_done >= c.target) return c.status & (DEM_ERR_BOND_OVERFLOW | DEM_ERR_NAN);
     }
     return fail(ctx, DEM_ERR_CUDA, "dem_bonded_run made no progress");
+}
+
+// ---- surrogate dense layers ---------------------------------------------------------
+namespace {
+int nn_prepare(dem_ctx *ctx, long part_floats) {
+    if (!ctx->d_err) {
+        CK(cudaMalloc(&ctx->d_err, sizeof(int)));
+        CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+    }
+    if (part_floats > ctx->nn_part_floats) {
+        CK(cudaStreamSynchronize(ctx->stream));
+        cudaFree(ctx->nn_part);
+        ctx->nn_part = nullptr;
+        ctx->nn_part_floats = 0;
+        CK(cudaMalloc(&ctx->nn_part, sizeof(float) * (size_t)part_floats));
+        ctx->nn_part_floats = part_floats;
+    }
+    return DEM_OK;
+}
+
+bool nn_args_ok(const dem_nn_mlp *m, long rows, const dem_nn_rows *src, int nsrc) {
+    if (!m || !src || nsrc < 1 || nsrc > 3 || rows < 0) return false;
+    int kin = 0;
+    for (int k = 0; k < nsrc; ++k) {
+        if (!src[k].data || src[k].width <= 0 || src[k].width % 8) return false;
+        kin += src[k].width;
+    }
+    return kin == m->kin && m->w1t && m->w2t && m->b1 && m->b2;
+}
+}  // namespace
+
+extern "C" int dem_nn_mlp_forward(dem_ctx *ctx, const dem_nn_mlp *m, long rows, const dem_nn_rows *src, int nsrc,
+                                  const void *resid, void *out, float *out_f32, void *h1) {
+    if (!ctx) return DEM_ERR_INVALID;
+    if (!nn_args_ok(m, rows, src, nsrc))
+        return fail(ctx, DEM_ERR_INVALID, "dem_nn_mlp_forward: bad layer description or sources");
+    int st = nn_prepare(ctx, 0);
+    if (st) return st;
+    st = nn_mlp_forward(*m, rows, src, nsrc, resid, out, out_f32, h1, ctx->d_err, ctx->stream);
+    if (st == DEM_ERR_UNSUPPORTED) return fail(ctx, st, "dem_nn_mlp_forward: unsupported (kin, nout)");
+    if (st) return cuda_check(ctx, cudaGetLastError(), "dem_nn_mlp_forward");
+    return DEM_OK;
+}
+
+extern "C" int dem_nn_mlp_backward(dem_ctx *ctx, const dem_nn_mlp *m, long rows, const dem_nn_rows *src, int nsrc,
+                                   const void *dy, const void *h1, void *dz1, float *dx, float *g_w1t, float *g_b1,
+                                   float *g_w2t, float *g_b2) {
+    if (!ctx) return DEM_ERR_INVALID;
+    if (!nn_args_ok(m, rows, src, nsrc) || !dy || !h1 || !dz1 || !g_w1t || !g_b1 || !g_w2t || !g_b2 ||
+        (dx && !m->w1) || !m->w2)
+        return fail(ctx, DEM_ERR_INVALID, "dem_nn_mlp_backward: bad arguments");
+    int st = nn_prepare(ctx, nn_wgrad_scratch(m->kin, m->nout));
+    if (st) return st;
+    st = nn_mlp_backward(*m, rows, src, nsrc, dy, h1, dz1, dx, g_w1t, g_b1, g_w2t, g_b2, ctx->nn_part, ctx->d_err,
+                         ctx->stream);
+    if (st == DEM_ERR_UNSUPPORTED) return fail(ctx, st, "dem_nn_mlp_backward: unsupported (kin, nout)");
+    if (st) return cuda_check(ctx, cudaGetLastError(), "dem_nn_mlp_backward");
+    return DEM_OK;
+}
+
+extern "C" int dem_nn_status(dem_ctx *ctx, int *status) {
+    if (!ctx || !status) return DEM_ERR_INVALID;
+    *status = 0;
+    if (!ctx->d_err) return DEM_OK;
+    CK(cudaMemcpyAsync(status, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return DEM_OK;
 }

@@ -19,6 +19,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "b200dem.h"
+
 namespace b200dem {
 
 constexpr int kMaxWalls = 24;
@@ -178,5 +180,13 @@ void launch_energy(const Particles &P, const NbrList &L, Ctl *ctl, const ForceCo
 // re-ordered by Morton cell key (state permuted, contact partners remapped).
 void launch_build(const Particles &P, Particles &alt, const NbrList &L, BuildBuffers &B, Ctl *ctl, double delta,
                   double skin, bool resort, bool check_run, cudaStream_t s);
+
+// dense layers of the surrogate (dem_nn.cu)
+int nn_mlp_forward(const dem_nn_mlp &m, long rows, const dem_nn_rows *src, int nsrc, const void *resid, void *out,
+                   float *out_f32, void *h1, int *err, cudaStream_t s);
+int nn_mlp_backward(const dem_nn_mlp &m, long rows, const dem_nn_rows *src, int nsrc, const void *dy, const void *h1,
+                    void *dz1, float *dx, float *g_w1t, float *g_b1, float *g_w2t, float *g_b2, float *part,
+                    int *err, cudaStream_t s);
+long nn_wgrad_scratch(int kin, int nout);
 
 }  // namespace b200dem

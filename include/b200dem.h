@@ -250,6 +250,42 @@ int dem_neighbor_list_noalloc(const double *x, const double *rad, int n, double 
  * contacts.  Fixed-order reduction, so repeated calls are bitwise identical. */
 int dem_energy(dem_solver *s, double out[4]);
 
+/* ---- Learned surrogate: dense layers on the tensor cores -----------------------------
+ * A two-layer perceptron over rows, y = W2 relu(W1 x + b1) + b2 (+ residual), hidden width
+ * 128, BF16 operands and FP32 accumulation (tcgen05 MMA, TMEM accumulators).  All pointers
+ * are device pointers; rows are row-major.  Shapes (kin, nout): (16,128), (128,128),
+ * (256,128), (384,128), (128,16).  Work is queued on the context's stream. */
+typedef struct {
+    const void *data;    /* bf16 [*][width] */
+    const int *index;    /* row r of the input takes row index[r] of data (null: row r) */
+    int width;           /* features taken from this source (multiple of 8) */
+} dem_nn_rows;
+
+typedef struct {
+    int kin, nout;
+    const void *w1t;     /* bf16 [128][kin]   W1 as out x in (forward) */
+    const void *w1;      /* bf16 [kin][128]   W1 as in x out (backward) */
+    const float *b1;     /* [128] */
+    const void *w2t;     /* bf16 [nout][128] */
+    const void *w2;      /* bf16 [128][nout] */
+    const float *b2;     /* [nout] */
+} dem_nn_mlp;
+
+/* Input = the concatenation of up to 3 gathered sources (widths sum to kin).  Outputs that
+ * are null are not written: out (bf16), out_f32, h1 (bf16 [rows][128] hidden activations,
+ * needed by the backward pass). */
+int dem_nn_mlp_forward(dem_ctx *ctx, const dem_nn_mlp *m, long rows, const dem_nn_rows *src, int nsrc,
+                       const void *resid, void *out, float *out_f32, void *h1);
+/* Backward of one forward call: dy (bf16 [rows][nout]) -> dz1 (bf16 [rows][128], written),
+ * dx (fp32 [rows][kin], written; null skips it) and weight/bias gradients ADDED to g_w1t
+ * [128][kin], g_b1 [128], g_w2t [nout][128], g_b2 [nout] (fixed-order sums: deterministic). */
+int dem_nn_mlp_backward(dem_ctx *ctx, const dem_nn_mlp *m, long rows, const dem_nn_rows *src, int nsrc,
+                        const void *dy, const void *h1, void *dz1, float *dx, float *g_w1t, float *g_b1,
+                        float *g_w2t, float *g_b2);
+/* Device error word of the context's tensor-core kernels (DEM_ERR_TIMEOUT when a bounded
+ * wait gave up); synchronises, returns it in *status and clears it. */
+int dem_nn_status(dem_ctx *ctx, int *status);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,115 @@
+"""Tensor-core dense layers (tcgen05 MMA, TMEM accumulators) against a plain PyTorch FP32
+reference of the same operation on the same BF16 operands.
+
+Forward: y = W2 relu(W1 x + b1) + b2 + residual with x gathered from up to three sources;
+the hidden activation is rounded to BF16 before the second product, as in the kernel.
+Backward: dZ = (dY W2) * [h > 0] (BF16), dX = dZ W1, dW1^T = dZ^T X, dW2^T = dY^T H and the
+bias sums.  The only differences allowed are FP32 summation order (and, for the forward
+output, a BF16 rounding of the hidden tile that can fall either way)."""
+import numpy as np
+import pytest
+import torch
+
+from cabanadem_b200 import api, nn
+
+pytestmark = pytest.mark.gpu
+
+
+def _sources(kin, rows, gen, dev):
+    """Input sources of a layer with `kin` features: edge-like rows gathered from node tables."""
+    nodes = max(rows // 3, 7)
+    bf = dict(device=dev, dtype=torch.bfloat16)
+    if kin == 384:
+        e = torch.randn(rows, 128, generator=gen).to(**bf)
+        h = torch.randn(nodes, 128, generator=gen).to(**bf)
+        ii = torch.randint(0, nodes, (rows,), generator=gen, dtype=torch.int32).to(dev)
+        jj = torch.randint(0, nodes, (rows,), generator=gen, dtype=torch.int32).to(dev)
+        return [(e, None), (h, ii), (h, jj)]
+    if kin == 256:
+        h = torch.randn(rows, 128, generator=gen).to(**bf)
+        a = torch.randn(rows, 128, generator=gen).to(**bf)
+        return [(h, None), (a, None)]
+    x = torch.randn(rows, kin, generator=gen).to(**bf)
+    return [(x, None)]
+
+
+def _gather(srcs):
+    return torch.cat([d.float() if i is None else d.float()[i.long()] for d, i in srcs], dim=1)
+
+
+@pytest.mark.parametrize("kin,nout", nn.SHAPES)
+@pytest.mark.parametrize("rows", [1000, 37, 148 * 128 + 200])
+def test_mlp_forward_backward_matches_torch_fp32(kin, nout, rows):
+    dev = torch.device("cuda:0")
+    ctx = api.Context(0)
+    gen = torch.Generator().manual_seed(kin * 7 + nout + rows)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr())
+    with torch.cuda.stream(stream):
+        m = nn.Mlp(kin, nout, dev, gen)
+        m.b1.copy_(torch.randn(128, generator=gen) * 0.1)
+        m.b2.copy_(torch.randn(nout, generator=gen) * 0.1)
+        srcs = _sources(kin, rows, gen, dev)
+        resid = torch.randn(rows, nout, generator=gen).to(dev, torch.bfloat16)
+        out = torch.empty(rows, nout, device=dev, dtype=torch.bfloat16)
+        out32 = torch.empty(rows, nout, device=dev, dtype=torch.float32)
+        h1 = torch.empty(rows, 128, device=dev, dtype=torch.bfloat16)
+        m.forward(ctx, rows, srcs, resid=resid, out=out, out_f32=out32, h1=h1)
+
+        x = _gather(srcs)
+        z = x @ m.w1t_bf.float().t() + m.b1
+        h_ref = torch.relu(z).to(torch.bfloat16).float()
+        y_ref = h_ref @ m.w2t_bf.float().t() + m.b2 + resid.float()
+        # the hidden tile: equal up to a BF16 rounding of values that sit on a rounding edge
+        dh = (h1.float() - h_ref).abs()
+        assert (dh > 0).float().mean().item() < 1e-3
+        assert dh.max().item() <= 1e-2 * max(h_ref.abs().max().item(), 1e-30)
+        # the output from the kernel's own hidden tile: FP32 summation order only
+        y_own = h1.float() @ m.w2t_bf.float().t() + m.b2 + resid.float()
+        scale = y_own.abs().max().item()
+        assert (out32 - y_own).abs().max().item() <= 1e-5 * scale
+        assert (out32 - y_ref).abs().max().item() <= 1e-2 * scale
+        assert (out.float() - out32).abs().max().item() <= 1e-2 * scale
+
+        dy = torch.randn(rows, nout, generator=gen).to(dev, torch.bfloat16)
+        dz1 = torch.empty(rows, 128, device=dev, dtype=torch.bfloat16)
+        dx = torch.empty(rows, kin, device=dev, dtype=torch.float32)
+        m.zero_grad()
+        m.backward(ctx, rows, srcs, dy, h1, dz1, dx=dx)
+
+        dz_ref = ((dy.float() @ m.w2t_bf.float()) * (h1.float() > 0)).to(torch.bfloat16).float()
+        ddz = (dz1.float() - dz_ref).abs()
+        assert ddz.max().item() <= 1e-2 * dz_ref.abs().max().item()
+        dzk = dz1.float()
+        dx_ref = dzk @ m.w1t_bf.float()
+        assert (dx - dx_ref).abs().max().item() <= 1e-5 * dx_ref.abs().max().item()
+        gw1t, gb1, gw2t, gb2 = m.grads
+        r_gw1t = dzk.t() @ x
+        r_gw2t = dy.float().t() @ h1.float()
+        for got, ref in ((gw1t, r_gw1t), (gb1, dzk.sum(0)), (gw2t, r_gw2t), (gb2, dy.float().sum(0))):
+            # sums over all rows: per-CTA partials added in block order vs torch's order
+            assert (got - ref).abs().max().item() <= 1e-4 * ref.abs().max().item() + 1e-6
+    assert nn.status(ctx) == 0
+    ctx.close()
+
+
+def test_backward_is_deterministic():
+    dev = torch.device("cuda:0")
+    ctx = api.Context(0)
+    gen = torch.Generator().manual_seed(3)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr())
+    rows = 148 * 128 * 3 + 5
+    with torch.cuda.stream(stream):
+        m = nn.Mlp(384, 128, dev, gen)
+        srcs = _sources(384, rows, gen, dev)
+        h1 = torch.empty(rows, 128, device=dev, dtype=torch.bfloat16)
+        m.forward(ctx, rows, srcs, h1=h1)
+        dy = torch.randn(rows, 128, generator=gen).to(dev, torch.bfloat16)
+        dz1 = torch.empty(rows, 128, device=dev, dtype=torch.bfloat16)
+        got = []
+        for _ in range(2):
+            m.zero_grad()
+            m.backward(ctx, rows, srcs, dy, h1, dz1)
+            got.append([g.cpu().numpy().copy() for g in m.grads])
+    for a, b in zip(*got):
+        assert np.array_equal(a, b)
+    ctx.close()
