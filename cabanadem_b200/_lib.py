@@ -66,6 +66,19 @@ class NnMlp(C.Structure):
                 ("w2t", C.c_void_p), ("w2", C.c_void_p), ("b2", C.c_void_p)]
 
 
+class SurrogateParams(C.Structure):
+    _fields_ = [("radius_graph", C.c_double), ("steps_per_stride", C.c_int), ("dt", C.c_double),
+                ("sigma_d", C.c_double), ("sigma_a", C.c_double), ("r_mean", C.c_double), ("r_std", C.c_double),
+                ("nwalls", C.c_int), ("wall_x", (C.c_double * 3) * 4), ("wall_n", (C.c_double * 3) * 4),
+                ("wall_clip", C.c_double), ("gravity", C.c_double * 3), ("max_overlap", C.c_double),
+                ("energy_tol", C.c_double), ("max_nodes", C.c_int), ("max_frames", C.c_int)]
+
+
+class RolloutStats(C.Structure):
+    _fields_ = [("strides_network", C.c_long), ("strides_dem", C.c_long), ("fallback_overlap", C.c_long),
+                ("fallback_energy", C.c_long), ("max_overlap_seen", C.c_double)]
+
+
 class DemError(RuntimeError):
     pass
 
@@ -114,6 +127,19 @@ _PROTOS = {
     "dem_nn_mlp_backward": ([_VP, C.POINTER(NnMlp), C.c_long, C.POINTER(NnRows), C.c_int, _VP, _VP, _VP, _VP, _VP,
                              _VP, _VP, _VP], C.c_int),
     "dem_nn_status": ([_VP, C.POINTER(C.c_int)], C.c_int),
+    "dem_particles_get_device": ([_VP, C.c_int, _VP, C.c_long], C.c_int),
+    "dem_surrogate_create": ([_VP, C.POINTER(SurrogateParams), C.POINTER(_VP)], C.c_int),
+    "dem_surrogate_destroy": ([_VP], C.c_int),
+    "dem_surrogate_num_params": ([_VP], C.c_long),
+    "dem_surrogate_get_params": ([_VP, _VP, C.c_long], C.c_int),
+    "dem_surrogate_set_params": ([_VP, _VP, C.c_long], C.c_int),
+    "dem_surrogate_init_params": ([_VP, C.c_ulonglong], C.c_int),
+    "dem_surrogate_loss_grad": ([_VP, C.c_int, _VP, _VP, _VP, _VP, _VP, C.c_int, C.c_double, C.c_ulonglong,
+                                 C.POINTER(C.c_double), _VP], C.c_int),
+    "dem_surrogate_train_step": ([_VP, C.c_int, _VP, _VP, _VP, _VP, _VP, C.c_int, C.c_double, C.c_ulonglong,
+                                  C.c_double, C.POINTER(C.c_double)], C.c_int),
+    "dem_surrogate_predict": ([_VP, C.c_int, _VP, _VP, _VP, _VP, C.c_int, _VP], C.c_int),
+    "dem_surrogate_rollout": ([_VP, _VP, C.c_int, C.c_int, C.POINTER(RolloutStats)], C.c_int),
 }
 NOALLOC_MAX_PARTICLES = 32768
 

@@ -106,6 +106,12 @@ class Particles:
         check(lib().dem_particles_get(self.h, F[field], a.ctypes.data, a.size), self.ctx.h, "get " + field)
         return a
 
+    def get_device(self, field: str, out):
+        """Copy a field in caller order into the device buffer `out` (a torch tensor of the
+        field's element count, e.g. float64 [n, 3] for "x"), queued on this context's stream."""
+        check(lib().dem_particles_get_device(self.h, F[field], C.c_void_p(out.data_ptr()), out.numel()), self.ctx.h,
+              "get_device " + field)
+
     def upload(self, s: ParticleState):
         for f in ("rad", "x", "u", "omega", "force", "torque", "m", "I", "rho", "E", "nu", "G",
                   "tng_idx", "tng_ss_x", "tng_ss_y", "tng_ss_z", "tng_count"):

@@ -497,7 +497,7 @@ extern "C" int dem_particles_set(dem_particles *p, int field, const void *host, 
     return DEM_OK;
 }
 
-extern "C" int dem_particles_get(dem_particles *p, int field, void *host, long count) {
+static int particles_get_impl(dem_particles *p, int field, void *host, long count, bool device) {
     if (!p || !host) return DEM_ERR_INVALID;
     dem_ctx *ctx = p->ctx;
     long need;
@@ -509,11 +509,17 @@ extern "C" int dem_particles_get(dem_particles *p, int field, void *host, long c
     Particles &P = p->P;
     if (field == DEM_F_RHO || field == DEM_F_E || field == DEM_F_NU || field == DEM_F_G) {
         const std::vector<double> &src = field == DEM_F_RHO ? p->rho : field == DEM_F_E ? p->E : field == DEM_F_NU ? p->nu : p->G;
-        std::memcpy(host, src.data(), sizeof(double) * n);
+        if (device) {
+            CK(cudaMemcpyAsync(host, src.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
+            CK(cudaStreamSynchronize(s));
+        } else {
+            std::memcpy(host, src.data(), sizeof(double) * n);
+        }
         return DEM_OK;
     }
     if (field == DEM_F_EXT_FORCE && !P.ext) {
-        std::memset(host, 0, sizeof(double) * 3 * n);
+        if (device) CK(cudaMemsetAsync(host, 0, sizeof(double) * 3 * n, s));
+        else std::memset(host, 0, sizeof(double) * 3 * n);
         return DEM_OK;
     }
     void *tmp = p->stage;
@@ -546,10 +552,23 @@ extern "C" int dem_particles_get(dem_particles *p, int field, void *host, long c
             break;
     }
     cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaMemcpyAsync(host, tmp, (size_t)need * es, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (device) {
+        // stream-ordered: the copy is complete for any later work on this context's stream
+        if (e == cudaSuccess) e = cudaMemcpyAsync(host, tmp, (size_t)need * es, cudaMemcpyDeviceToDevice, s);
+    } else {
+        if (e == cudaSuccess) e = cudaMemcpyAsync(host, tmp, (size_t)need * es, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    }
     CK(e);
     return DEM_OK;
+}
+
+extern "C" int dem_particles_get(dem_particles *p, int field, void *host, long count) {
+    return particles_get_impl(p, field, host, count, false);
+}
+
+extern "C" int dem_particles_get_device(dem_particles *p, int field, void *dev, long count) {
+    return particles_get_impl(p, field, dev, count, true);
 }
 
 // ---- walls --------------------------------------------------------------------------
@@ -1362,3 +1381,29 @@ extern "C" int dem_nn_status(dem_ctx *ctx, int *status) {
     CK(cudaStreamSynchronize(ctx->stream));
     return DEM_OK;
 }
+
+// ---- internal access for the surrogate (dem_surrogate.cu) ---------------------------
+namespace b200dem {
+int solver_view(dem_solver *s, SolverView *v) {
+    if (!s || !v) return DEM_ERR_INVALID;
+    v->P = s->p->P;
+    v->ctl = s->p->ctl;
+    v->stream = s->ctx->stream;
+    v->dt = s->sp.dt;
+    v->ctx = s->ctx;
+    return DEM_OK;
+}
+void solver_particles_changed(dem_solver *s) {
+    s->p->dirty = true;
+    s->built = false;
+}
+cudaStream_t ctx_stream(dem_ctx *ctx) { return ctx->stream; }
+int ctx_fail(dem_ctx *ctx, int code, const char *msg) { return fail(ctx, code, msg); }
+int ctx_cuda(dem_ctx *ctx, cudaError_t e, const char *what) { return cuda_check(ctx, e, what); }
+int ctx_nn_scratch(dem_ctx *ctx, long part_floats, int **err, float **part) {
+    const int st = nn_prepare(ctx, part_floats);
+    *err = ctx->d_err;
+    *part = ctx->nn_part;
+    return st;
+}
+}  // namespace b200dem

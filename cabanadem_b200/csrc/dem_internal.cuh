@@ -189,4 +189,19 @@ int nn_mlp_backward(const dem_nn_mlp &m, long rows, const dem_nn_rows *src, int 
                     int *err, cudaStream_t s);
 long nn_wgrad_scratch(int kin, int nout);
 
+// internal access to a solver's device state (dem_api.cu), used by the surrogate
+struct SolverView {
+    Particles P;
+    Ctl *ctl;
+    cudaStream_t stream;
+    double dt;
+    dem_ctx *ctx;
+};
+int solver_view(dem_solver *s, SolverView *v);
+void solver_particles_changed(dem_solver *s);
+cudaStream_t ctx_stream(dem_ctx *ctx);
+int ctx_fail(dem_ctx *ctx, int code, const char *msg);
+int ctx_cuda(dem_ctx *ctx, cudaError_t e, const char *what);
+int ctx_nn_scratch(dem_ctx *ctx, long part_floats, int **err, float **part);
+
 }  // namespace b200dem

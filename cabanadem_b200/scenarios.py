@@ -235,6 +235,57 @@ def scene_subset(sc, k):
                     sc.nsteps, skin=sc.skin, gravity=sc.gravity)
 
 
+# Quasi-2D granular dam break.  The stiffness is not fixed by the workload: E = 30 MPa (a
+# softened modulus, common DEM practice) keeps the static overlap at the foot of a 1 m column
+# near 2 % of r and allows dt = 4 us (about 25 steps per collision at 5 m/s).
+DAM = dict(rho=2600.0, E=3e7, nu=0.25, mu=0.4, cor=0.5, dt=4e-6)
+
+
+def dam_break(n=200_000, aspect=None, seed=11, rmin=0.9e-3, rmax=1.1e-3, nsteps=250_000, max_cnts=12,
+              quirks=REF_COMPAT, dt=DAM["dt"]):
+    """n disks (spheres with z = 0, in-plane motion only) with r ~ U[0.9, 1.1] mm on a jittered
+    hexagonal lattice of pitch 2.25 mm filling a column of width W and height aspect * W
+    (aspect ~ U[0.5, 4] unless given) against the left wall x = 0, on the floor y = 0, with
+    a right wall far downstream; released at rest under gravity -y.  mu = 0.4, e = 0.5
+    (pp and pw), E = 30 MPa, rho = 2600.  nsteps = 1 s at dt = 4 us."""
+    rng = np.random.default_rng(seed)
+    if aspect is None:
+        aspect = float(rng.uniform(0.5, 4.0))
+    pitch = 2.25e-3
+    rowh = pitch * math.sqrt(3.0) / 2.0
+    width = math.sqrt(n * pitch * rowh / aspect)
+    ncol = max(2, int(round(width / pitch)))
+    nrow = int(math.ceil(n / ncol))
+    k = np.arange(n)
+    row, col = k // ncol, k % ncol
+    x = (col + 0.5 * (row % 2)) * pitch + rmax + 0.1e-3
+    y = row * rowh + rmax + 0.1e-3
+    rad = rng.uniform(rmin, rmax, size=n)
+    room = 0.5 * pitch - rad
+    # |jitter| <= room / sqrt(2) per particle: lattice neighbours (all at distance pitch) keep a gap
+    x = x + rng.uniform(-0.5, 0.5, size=n) * room
+    y = y + rng.uniform(-0.5, 0.5, size=n) * room
+    st = ParticleState.create(n, max_cnts=max_cnts, max_walls=3)
+    st.x[:, 0], st.x[:, 1] = x, y
+    st.rad[:] = rad
+    st.rho[:] = DAM["rho"]
+    st.E[:], st.nu[:], st.G[:] = DAM["E"], DAM["nu"], DAM["E"] / (2.0 * (1.0 + DAM["nu"]))
+    st.m[:] = 4. / 3. * math.pi * rad ** 3 * DAM["rho"]
+    st.I[:] = 2. / 5. * st.m * rad * rad
+    col_w = (ncol + 0.5) * pitch + 2.0 * rmax
+    length = col_w * (2.0 + 3.0 * aspect)
+    w = WallState.create(3)
+    w.x[0], w.normal[0] = (0.0, 0.0, 0.0), (0.0, 1.0, 0.0)          # floor
+    w.x[1], w.normal[1] = (0.0, 0.0, 0.0), (1.0, 0.0, 0.0)          # back wall
+    w.x[2], w.normal[2] = (length, 0.0, 0.0), (-1.0, 0.0, 0.0)      # far wall
+    w.E[:], w.nu[:], w.G[:] = DAM["E"], DAM["nu"], DAM["E"] / (2.0 * (1.0 + DAM["nu"]))
+    sc = Scenario("dam_break_%d" % n, st, w, _force_params(DAM["cor"], DAM["cor"], DAM["mu"], DAM["mu"], quirks), dt,
+                  nsteps, skin=0.1 * 0.5 * (rmin + rmax), gravity=(0.0, -9.81, 0.0))
+    sc.extra = dict(aspect=aspect, column_width=col_w, column_height=nrow * rowh, length=length,
+                    r_mean=0.5 * (rmin + rmax), r_std=(rmax - rmin) / math.sqrt(12.0))
+    return sc
+
+
 def bdem_two_particles():
     """examples/tst_01_BDEM_two_particles_tensile_3D.cpp:162-302: two bonded spheres
     pulled apart by +-1e3 N, particle 0's force zeroed after the bond pass."""

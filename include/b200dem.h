@@ -134,6 +134,9 @@ int dem_particles_destroy(dem_particles *p);
  * count = number of elements in `host` (e.g. 3*n for DEM_F_X). */
 int dem_particles_set(dem_particles *p, int field, const void *host, long count);
 int dem_particles_get(dem_particles *p, int field, void *host, long count);
+/* As dem_particles_get into device memory `dev` (same layout and caller order), queued on
+ * the context's stream without a host synchronisation. */
+int dem_particles_get_device(dem_particles *p, int field, void *dev, long count);
 int dem_particles_size(dem_particles *p);
 
 /* ---- walls: Wall<Mem,3>(exec, n, out) (src/CabanaDEM_Wall.hpp:22-153) ------------- */
@@ -285,6 +288,70 @@ int dem_nn_mlp_backward(dem_ctx *ctx, const dem_nn_mlp *m, long rows, const dem_
 /* Device error word of the context's tensor-core kernels (DEM_ERR_TIMEOUT when a bounded
  * wait gave up); synchronises, returns it in *status and clears it. */
 int dem_nn_status(dem_ctx *ctx, int *status);
+
+/* ---- Learned surrogate: message-passing network over the contact graph -------------------
+ * Quasi-2D (x, y) particles.  One network stride replaces `steps_per_stride` DEM steps:
+ * from the positions at the last two strides it predicts the change of the per-stride
+ * displacement.  Graph: every pair closer than radius_graph (centre distance), per frame.
+ * Network: node and edge encoders (16 -> 128 -> 128), three rounds of edge update
+ * e += MLP[e, h_i, h_j] and node update h += MLP[h, sum_j e_ij], decoder 128 -> 128 -> 2;
+ * dense layers as in dem_nn_mlp_*; aggregation in a fixed order (deterministic).
+ * All position arrays are device pointers, double [n][3] in caller order (z ignored). */
+typedef struct dem_surrogate dem_surrogate;
+
+typedef struct {
+    double radius_graph;     /* edge cutoff (m) */
+    int steps_per_stride;    /* DEM steps per network stride (200) */
+    double dt;               /* DEM time step (s); a stride lasts steps_per_stride * dt */
+    double sigma_d;          /* scale of the per-stride displacement inputs (m) */
+    double sigma_a;          /* scale of the predicted displacement change (m) */
+    double r_mean, r_std;    /* radius normalisation */
+    int nwalls;              /* planar walls (<= 4): feature distances and projection */
+    double wall_x[4][3], wall_n[4][3];
+    double wall_clip;        /* wall distance features saturate at this distance (m) */
+    double gravity[3];       /* energy residual */
+    double max_overlap;      /* fallback: any overlap above this fraction of the smaller radius */
+    double energy_tol;       /* fallback: total energy rose by more than this fraction */
+    int max_nodes;           /* capacity (particles per call, all frames together) */
+    int max_frames;          /* capacity (independent frames per training batch) */
+} dem_surrogate_params;
+
+typedef struct {
+    long strides_network;    /* strides advanced by the network */
+    long strides_dem;        /* strides advanced by DEM (fallback) */
+    long fallback_overlap;   /* fallbacks caused by the overlap check */
+    long fallback_energy;    /* fallbacks caused by the energy check */
+    double max_overlap_seen; /* largest overlap fraction of an accepted network stride */
+} dem_rollout_stats;
+
+int dem_surrogate_create(dem_ctx *ctx, const dem_surrogate_params *prm, dem_surrogate **out);
+int dem_surrogate_destroy(dem_surrogate *sg);
+long dem_surrogate_num_params(dem_surrogate *sg);
+/* FP32 master parameters, flat: for each layer (node enc, edge enc, 3 x (edge upd, node upd),
+ * decoder) W1^T [128][kin], b1 [128], W2^T [nout][128], b2 [nout]. */
+int dem_surrogate_get_params(dem_surrogate *sg, float *host, long n);
+int dem_surrogate_set_params(dem_surrogate *sg, const float *host, long n);
+int dem_surrogate_init_params(dem_surrogate *sg, unsigned long long seed);
+/* Loss (mean squared error of the normalised displacement change) and its gradient for a
+ * batch of frames: node i belongs to frame[i] (null: one frame); pos_prev, pos_cur,
+ * pos_next: positions at strides k-1, k, k+1; Gaussian noise of std noise (m) is added to
+ * the input positions (seeded).  grads_host (flat, like the parameters) may be null. */
+int dem_surrogate_loss_grad(dem_surrogate *sg, int n, const double *pos_prev, const double *pos_cur,
+                            const double *pos_next, const double *rad, const int *frame, int nframes,
+                            double noise, unsigned long long seed, double *loss, float *grads_host);
+/* loss_grad followed by one Adam step (lr, beta1 0.9, beta2 0.999, eps 1e-8). */
+int dem_surrogate_train_step(dem_surrogate *sg, int n, const double *pos_prev, const double *pos_cur,
+                             const double *pos_next, const double *rad, const int *frame, int nframes,
+                             double noise, unsigned long long seed, double lr, double *loss);
+/* One network stride: pos_next = pos_cur + (pos_cur - pos_prev) + sigma_a * net(...). */
+int dem_surrogate_predict(dem_surrogate *sg, int n, const double *pos_prev, const double *pos_cur,
+                          const double *rad, const int *frame, int nframes, double *pos_next);
+/* Hybrid rollout of a solver's particles (2D: z untouched) for nstrides strides: each stride
+ * is a network stride unless its overlap or energy residual exceeds the thresholds, in
+ * which case that stride is run by dem_solver_run from the state before it.  use_network = 0
+ * runs every stride with DEM.  The solver's state is current on return. */
+int dem_surrogate_rollout(dem_surrogate *sg, dem_solver *s, int nstrides, int use_network,
+                          dem_rollout_stats *stats);
 
 #ifdef __cplusplus
 }
