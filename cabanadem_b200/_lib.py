@@ -71,7 +71,8 @@ class SurrogateParams(C.Structure):
                 ("sigma_d", C.c_double), ("sigma_a", C.c_double), ("r_mean", C.c_double), ("r_std", C.c_double),
                 ("nwalls", C.c_int), ("wall_x", (C.c_double * 3) * 4), ("wall_n", (C.c_double * 3) * 4),
                 ("wall_clip", C.c_double), ("gravity", C.c_double * 3), ("max_overlap", C.c_double),
-                ("energy_tol", C.c_double), ("max_nodes", C.c_int), ("max_frames", C.c_int)]
+                ("energy_tol", C.c_double), ("max_nodes", C.c_int), ("max_frames", C.c_int),
+                ("project_iters", C.c_int), ("project_allow", C.c_double)]
 
 
 class RolloutStats(C.Structure):

@@ -25,6 +25,7 @@ createSolverDEM / SolverDEM::run           :func:`createSolverDEM`, :meth:`Solve
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 
 import numpy as np
 
@@ -57,6 +58,11 @@ class Context:
         if st:
             raise DemError("dem_ctx_create failed (status %d): no usable CUDA device" % st)
         self.h = h
+        self._children = []   # weak references to objects created on this context, in order
+
+    def adopt(self, obj):
+        """Register an object created on this context; close() closes it first."""
+        self._children.append(weakref.ref(obj))
 
     def sync(self):
         check(lib().dem_ctx_sync(self.h), self.h, "dem_ctx_sync")
@@ -66,10 +72,19 @@ class Context:
         return int(lib().dem_ctx_stream(self.h) or 0)
 
     def close(self):
-        """Destroy the context; close every object created on it first."""
+        """Destroy the context after closing every object created on it (newest first)."""
         if self.h:
+            for r in reversed(self._children):
+                o = r()
+                if o is not None:
+                    o.close()
+            self._children = []
             lib().dem_ctx_destroy(self.h)
             self.h = None
+
+    @property
+    def alive(self) -> bool:
+        return bool(self.h)
 
 
 _default_ctx = None
@@ -90,6 +105,7 @@ class Particles:
         check(lib().dem_particles_create(self.ctx.h, self.n, self.max_cnts, self.max_walls, C.byref(h)),
               self.ctx.h, "dem_particles_create")
         self.h = h
+        self.ctx.adopt(self)
 
     # ---- field access
     def set(self, field: str, arr):
@@ -160,9 +176,9 @@ class Particles:
     def sliceTangentialDispSWz(self): return self.get("tng_sw_z")
 
     def close(self):
-        if self.h:
+        if self.h and self.ctx.alive:   # a closed context has closed this object already
             lib().dem_particles_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:
@@ -178,6 +194,7 @@ class Wall:
         h = C.c_void_p()
         check(lib().dem_walls_create(self.ctx.h, self.n, C.byref(h)), self.ctx.h, "dem_walls_create")
         self.h = h
+        self.ctx.adopt(self)
 
     def set(self, field, arr):
         a = np.ascontiguousarray(arr, dtype=np.float64)
@@ -188,9 +205,9 @@ class Wall:
             self.set(f, getattr(w, f))
 
     def close(self):
-        if self.h:
+        if self.h and self.ctx.alive:
             lib().dem_walls_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:
@@ -233,6 +250,7 @@ class SolverDEM:
         check(lib().dem_solver_create(particles.ctx.h, particles.h, wall.h if wall else None, C.byref(fp),
                                       C.byref(sp), C.byref(h)), particles.ctx.h, "dem_solver_create")
         self.h = h
+        particles.ctx.adopt(self)
         self.integrator = Integrator(self)
         self.last_status = 0
 
@@ -288,9 +306,9 @@ class SolverDEM:
         return np.array(out[:])
 
     def close(self):
-        if self.h:
+        if self.h and self.particles.ctx.alive:
             lib().dem_solver_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:
@@ -366,6 +384,7 @@ class Bonds:
         check(lib().dem_bonds_create(solver.h, self.max_bonds, C.byref(bp), C.byref(h)), solver.particles.ctx.h,
               "dem_bonds_create")
         self.h = h
+        solver.particles.ctx.adopt(self)
 
     def setupBonds(self, factor=3.0, search_cutoff=0.0):
         check(lib().dem_bonds_setup(self.h, float(factor), float(search_cutoff)), self.solver.particles.ctx.h,
@@ -395,9 +414,9 @@ class Bonds:
         return check(lib().dem_bonded_run(self.h, int(nsteps)), self.solver.particles.ctx.h, "dem_bonded_run")
 
     def close(self):
-        if self.h:
+        if self.h and self.solver.particles.ctx.alive:
             lib().dem_bonds_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:

@@ -1365,8 +1365,8 @@ extern "C" int dem_nn_mlp_backward(dem_ctx *ctx, const dem_nn_mlp *m, long rows,
         return fail(ctx, DEM_ERR_INVALID, "dem_nn_mlp_backward: bad arguments");
     int st = nn_prepare(ctx, nn_wgrad_scratch(m->kin, m->nout));
     if (st) return st;
-    st = nn_mlp_backward(*m, rows, src, nsrc, dy, h1, dz1, dx, g_w1t, g_b1, g_w2t, g_b2, ctx->nn_part, ctx->d_err,
-                         ctx->stream);
+    st = nn_mlp_backward(*m, rows, src, nsrc, dy, h1, dz1, dx, g_w1t, m->kin, g_b1, g_w2t, g_b2, ctx->nn_part,
+                         ctx->d_err, ctx->stream);
     if (st == DEM_ERR_UNSUPPORTED) return fail(ctx, st, "dem_nn_mlp_backward: unsupported (kin, nout)");
     if (st) return cuda_check(ctx, cudaGetLastError(), "dem_nn_mlp_backward");
     return DEM_OK;

@@ -185,9 +185,17 @@ void launch_build(const Particles &P, Particles &alt, const NbrList &L, BuildBuf
 int nn_mlp_forward(const dem_nn_mlp &m, long rows, const dem_nn_rows *src, int nsrc, const void *resid, void *out,
                    float *out_f32, void *h1, int *err, cudaStream_t s);
 int nn_mlp_backward(const dem_nn_mlp &m, long rows, const dem_nn_rows *src, int nsrc, const void *dy, const void *h1,
-                    void *dz1, float *dx, float *g_w1t, float *g_b1, float *g_w2t, float *g_b2, float *part,
-                    int *err, cudaStream_t s);
+                    void *dz1, float *dx, float *g_w1t, int ld_w1, float *g_b1, float *g_w2t, float *g_b2,
+                    float *part, int *err, cudaStream_t s);
 long nn_wgrad_scratch(int kin, int nout);
+// factorised edge layer of the surrogate (dem_nn.cu)
+int nn_linear_pq(long rows, const void *h, const void *w1ij_t, void *pq, int *err, cudaStream_t s);
+int nn_linear_pq_backward(long rows, const void *dpq, const void *w1ij, float *dh, int *err, cudaStream_t s);
+int nn_linear_pq_wgrad(long rows, const void *dpq, const void *h, float *g_w1t, int ld, int col0, float *part,
+                       int *err, cudaStream_t s);
+int nn_edge_forward(long rows, const void *e, const void *pq, const int *recv, const int *send, const void *w1e_t,
+                    const float *b1, const void *w2t, const float *b2, void *out, void *h1, int *err, cudaStream_t s);
+long nn_linear_wgrad_scratch();
 
 // internal access to a solver's device state (dem_api.cu), used by the surrogate
 struct SolverView {

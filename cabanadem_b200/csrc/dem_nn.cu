@@ -32,6 +32,7 @@ using bf16 = __nv_bfloat16;
 constexpr int kRows = 128;      // rows per tile (= MMA M)
 constexpr int kHidden = 128;    // hidden width
 constexpr int kThreads = 128;
+constexpr int kFwdThreads = 256;   // forward kernels: warps w and w + 4 split a TMEM lane quarter's columns
 
 struct RowSrc {
     const bf16 *p;
@@ -44,25 +45,28 @@ struct MlpW {
     const float *b1, *b2;
 };
 
-// 16-byte chunk `kc` (features 8kc..8kc+7) of input row `grow` of the concatenated sources.
-__device__ __forceinline__ uint4 src_chunk(const RowSrc *src, int nsrc, long grow, int kc) {
-    int f = kc * 8;
-    for (int s = 0; s < nsrc; ++s) {
-        const int w = src[s].width;
-        if (f < w) {
-            const long r = src[s].idx ? (long)src[s].idx[grow] : grow;
-            return *reinterpret_cast<const uint4 *>(src[s].p + r * w + f);
-        }
-        f -= w;
+// ---- asynchronous staging (cp.async: every chunk copy of a tile in flight at once) ----
+__device__ __forceinline__ void cp16(void *smem, const void *gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(tc::smem_u32(smem)), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Row indices of the tile's rows for the gathered sources: s_idx[s][row] (one round trip).
+__device__ __forceinline__ void load_row_index(int *s_idx, const RowSrc *src, int nsrc, long row0, long rows) {
+    const int t = threadIdx.x;
+    if (t < kRows) {
+        const long grow = row0 + t;
+        for (int s = 0; s < nsrc; ++s)
+            s_idx[s * kRows + t] = src[s].idx ? (grow < rows ? src[s].idx[grow] : 0) : (int)(grow < rows ? grow : 0);
     }
-    return make_uint4(0, 0, 0, 0);
 }
 
-// Stage rows [row0, row0 + kRows) (zero past `rows`) of the concatenated sources, C chunks
-// per row, into a row tile of 128 rows.  Eight consecutive threads take eight consecutive
-// rows of one chunk (bank-conflict-free 128-byte runs in shared memory).
+// Queue the copies of rows [row0, row0 + kRows) of the concatenated sources (C chunks of 8
+// features per row) into a row tile of 128 rows; rows past `rows` are zero-filled.  Eight
+// consecutive threads take eight consecutive rows of one chunk (conflict-free 128-byte runs
+// in shared memory).  s_idx must hold the tile's row indices (load_row_index + barrier).
 __device__ __forceinline__ void stage_gather(unsigned char *tile, const RowSrc *src, int nsrc, int C, long row0,
-                                             long rows) {
+                                             long rows, const int *s_idx) {
     const int G = C < 4 ? C : 4;
     for (int q = threadIdx.x; q < kRows * C; q += blockDim.x) {
         const int i = q & 7;
@@ -70,20 +74,52 @@ __device__ __forceinline__ void stage_gather(unsigned char *tile, const RowSrc *
         const int rest = (q >> 3) / G;
         const int row = (rest % (kRows / 8)) * 8 + i;
         const int kc = (rest / (kRows / 8)) * G + g;
-        const long grow = row0 + row;
-        const uint4 v = grow < rows ? src_chunk(src, nsrc, grow, kc) : make_uint4(0, 0, 0, 0);
-        *reinterpret_cast<uint4 *>(tile + tc::tile_off(kRows, row, kc)) = v;
+        unsigned char *dst = tile + tc::tile_off(kRows, row, kc);
+        if (row0 + row < rows) {
+            int f = kc * 8, s = 0;
+            while (s < nsrc - 1 && f >= src[s].width) {
+                f -= src[s].width;
+                ++s;
+            }
+            cp16(dst, src[s].p + (long)s_idx[s * kRows + row] * src[s].width + f);
+        } else {
+            *reinterpret_cast<uint4 *>(dst) = make_uint4(0, 0, 0, 0);
+        }
     }
 }
 
-// Stage a dense row-major block [R rows][F features] (row stride F) into a row tile of R rows.
+// Queue the copies of a dense row-major block [R rows][F features] (row stride F) into a row
+// tile of R rows; rows past `rows` are zero-filled.
 __device__ __forceinline__ void stage_dense(unsigned char *tile, const bf16 *g, int R, int F, long row0, long rows) {
     const int C = F / 8;
     for (int q = threadIdx.x; q < R * C; q += blockDim.x) {
         const int row = q % R, kc = q / R;
-        const long grow = row0 + row;
-        const uint4 v = grow < rows ? *reinterpret_cast<const uint4 *>(g + grow * F + kc * 8) : make_uint4(0, 0, 0, 0);
-        *reinterpret_cast<uint4 *>(tile + tc::tile_off(R, row, kc)) = v;
+        unsigned char *dst = tile + tc::tile_off(R, row, kc);
+        if (row0 + row < rows) cp16(dst, g + (row0 + row) * F + kc * 8);
+        else *reinterpret_cast<uint4 *>(dst) = make_uint4(0, 0, 0, 0);
+    }
+}
+
+// Completes this thread's queued copies and publishes the tiles to the tensor core.
+__device__ __forceinline__ void stage_done() {
+    cp_wait_all();
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+}
+
+// Row-major output tile in shared memory (128 rows x 256 bytes), 16-byte chunks XOR-swizzled
+// by the row so that thread t writing its row and 16 threads reading one row are both free of
+// bank conflicts; copy_out then writes whole 256-byte rows (coalesced).
+__device__ __forceinline__ void out_put(unsigned char *tile, int row, int chunk, uint4 v) {
+    *reinterpret_cast<uint4 *>(tile + row * 256 + ((chunk ^ (row & 15)) << 4)) = v;
+}
+__device__ __forceinline__ void copy_out(const unsigned char *tile, bf16 *g, long row0, long rows) {
+    for (int q = threadIdx.x; q < kRows * 16; q += blockDim.x) {
+        const int row = q >> 4, chunk = q & 15;
+        if (row0 + row < rows)
+            *reinterpret_cast<uint4 *>(g + (row0 + row) * kHidden + chunk * 8) =
+                *reinterpret_cast<const uint4 *>(tile + row * 256 + ((chunk ^ (row & 15)) << 4));
     }
 }
 
@@ -91,6 +127,25 @@ __device__ __forceinline__ void stage_dense(unsigned char *tile, const bf16 *g, 
 __device__ __forceinline__ void acc16(uint32_t tm, int col, float v[16]) {
     tc::tmem_ld16(tc::tmem_warp_addr(tm, col), v);
     tc::tmem_wait_ld();
+}
+
+// 32 accumulator columns [col, col + 32) of thread t's lane.
+__device__ __forceinline__ void acc32(uint32_t tm, int col, float v[32]) {
+    uint32_t r[32];
+    tc::tmem_ld32_nowait(tc::tmem_warp_addr(tm, col), r);
+    tc::tmem_wait_ld();
+#pragma unroll
+    for (int k = 0; k < 32; ++k) v[k] = __uint_as_float(r[k]);
+}
+
+// 64 accumulator columns [col, col + 64) of thread t's lane with one wait (two x32 loads).
+__device__ __forceinline__ void acc64(uint32_t tm, int col, float v[64]) {
+    uint32_t r[64];
+    tc::tmem_ld32_nowait(tc::tmem_warp_addr(tm, col), r);
+    tc::tmem_ld32_nowait(tc::tmem_warp_addr(tm, col + 32), r + 32);
+    tc::tmem_wait_ld();
+#pragma unroll
+    for (int k = 0; k < 64; ++k) v[k] = __uint_as_float(r[k]);
 }
 
 // Shared-memory prologue of every kernel: mbarrier, TMEM allocation (warp 0).
@@ -134,6 +189,7 @@ struct FwdArgs {
     int nsrc;
     MlpW w;
     const bf16 *resid;   // [rows][NOUT] or null
+    int resid_src0;      // the residual is source 0 of the input (read from the staged tile)
     bf16 *out;           // [rows][NOUT] or null
     float *out_f32;      // [rows][NOUT] or null
     bf16 *h1;            // [rows][128] or null
@@ -146,18 +202,30 @@ constexpr size_t fwd_smem() {
 }
 
 template <int KIN, int NOUT>
-__global__ void __launch_bounds__(kThreads, 1) k_mlp_fwd(FwdArgs a) {
-    extern __shared__ __align__(1024) unsigned char smem[];
+__global__ void __launch_bounds__(kFwdThreads, 1) k_mlp_fwd(FwdArgs a) {
+    extern __shared__ __align__(128) unsigned char smem[];
     constexpr int KA = KIN > kHidden ? KIN : kHidden;
     unsigned char *sW1 = smem;                                // W1^T: 128 rows x KIN
     unsigned char *sW2 = sW1 + (size_t)kHidden * KIN * 2;     // W2^T: NOUT rows x 128
     unsigned char *sA = sW2 + (size_t)NOUT * kHidden * 2;     // input tile, then hidden tile
     uint64_t *mbar = reinterpret_cast<uint64_t *>(sA + (size_t)kRows * KA * 2);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 1);
-    const int t = threadIdx.x;
+    __shared__ int s_idx[3 * kRows];
+    __shared__ float s_b1[kHidden], s_b2[kHidden];
+    const int tid = threadIdx.x;
+    const int t = tid & (kRows - 1);   // tile row (TMEM lane) of this thread
+    const int half = tid >> 7;         // column half [64 half, 64 half + 64) of the epilogues
+    // the hidden tile goes behind source 0 when the input is wide enough, so that a residual
+    // taken from source 0 is still in shared memory for the second epilogue
+    constexpr int HC = KIN >= 2 * kHidden ? kHidden / 8 : 0;   // first chunk of the hidden tile
+    const uint32_t aH = tc::smem_u32(sA) + (uint32_t)(HC * kRows * 16);
+    unsigned char *sOut = sA + (size_t)HC * kRows * 16;        // output tile (hidden tile is spent)
+    if (half == 0) s_b1[t] = a.w.b1[t];
+    else if (t < NOUT) s_b2[t] = a.w.b2[t];
 
     stage_dense(sW1, a.w.w1t, kHidden, KIN, 0, kHidden);
     stage_dense(sW2, a.w.w2t, NOUT, kHidden, 0, NOUT);
+    cp_wait_all();
     const uint32_t tm = tc_setup(mbar, tslot, 128);
     const uint32_t aW1 = tc::smem_u32(sW1), aW2 = tc::smem_u32(sW2), aA = tc::smem_u32(sA);
     constexpr uint32_t id1 = tc::idesc_bf16(kRows, kHidden, false, false);
@@ -168,11 +236,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fwd(FwdArgs a) {
     for (long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
         const long row0 = tile * kRows;
         const long grow = row0 + t;
-        stage_gather(sA, a.src, a.nsrc, KIN / 8, row0, a.rows);
-        tc::fence_async_smem();
-        tc::fence_before_sync();
+        load_row_index(s_idx, a.src, a.nsrc, row0, a.rows);
         __syncthreads();
-        if (t == 0) {
+        stage_gather(sA, a.src, a.nsrc, KIN / 8, row0, a.rows, s_idx);
+        stage_done();
+        if (tid == 0) {
             tc::fence_after_sync();
             for (int ks = 0; ks < KIN / 16; ++ks)
                 tc::mma_bf16(tm, tc::kmajor_desc(aA, kRows, ks), tc::kmajor_desc(aW1, kHidden, ks), id1, ks > 0);
@@ -181,44 +249,67 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fwd(FwdArgs a) {
         ok = mma_wait(mbar, phase);
         if (!ok) break;
         // hidden = relu(acc + b1) -> bf16 tile (A operand of GEMM2), optionally saved
-        for (int c = 0; c < kHidden / 16; ++c) {
-            float v[16];
-            acc16(tm, c * 16, v);
-            for (int k = 0; k < 16; ++k) v[k] = fmaxf(v[k] + a.w.b1[c * 16 + k], 0.f);
+        for (int c64 = half; c64 < kHidden / 64; c64 += 2) {
+          float w[64];
+          acc64(tm, c64 * 64, w);
+#pragma unroll
+          for (int cc = 0; cc < 4; ++cc) {
+            const int c = c64 * 4 + cc;
+            float *v = w + 16 * cc;
+            for (int k = 0; k < 16; ++k) v[k] = fmaxf(v[k] + s_b1[c * 16 + k], 0.f);
             const uint4 lo = tc::pack8(v), hi = tc::pack8(v + 8);
-            *reinterpret_cast<uint4 *>(sA + tc::tile_off(kRows, t, 2 * c)) = lo;
-            *reinterpret_cast<uint4 *>(sA + tc::tile_off(kRows, t, 2 * c + 1)) = hi;
+            *reinterpret_cast<uint4 *>(sA + tc::tile_off(kRows, t, HC + 2 * c)) = lo;
+            *reinterpret_cast<uint4 *>(sA + tc::tile_off(kRows, t, HC + 2 * c + 1)) = hi;
             if (a.h1 && grow < a.rows) {
                 uint4 *dst = reinterpret_cast<uint4 *>(a.h1 + grow * kHidden + c * 16);
                 dst[0] = lo;
                 dst[1] = hi;
             }
+          }
         }
         tc::fence_async_smem();
         tc::fence_before_sync();
         __syncthreads();
-        if (t == 0) {
+        if (tid == 0) {
             tc::fence_after_sync();
             for (int ks = 0; ks < kHidden / 16; ++ks)
-                tc::mma_bf16(tm, tc::kmajor_desc(aA, kRows, ks), tc::kmajor_desc(aW2, NOUT, ks), id2, ks > 0);
+                tc::mma_bf16(tm, tc::kmajor_desc(aH, kRows, ks), tc::kmajor_desc(aW2, NOUT, ks), id2, ks > 0);
             tc::mma_commit(mbar);
         }
         ok = mma_wait(mbar, phase);
         if (!ok) break;
-        for (int c = 0; c < NOUT / 16; ++c) {
-            float v[16];
-            acc16(tm, c * 16, v);
+        constexpr bool kStaged = NOUT == kHidden;   // bf16 rows written through the output tile
+        constexpr int CB = NOUT >= 64 ? 64 : NOUT;   // columns per TMEM wait
+        for (int c64 = half; c64 < NOUT / CB; c64 += 2) {
+          float w[64];
+          if (CB == 64) acc64(tm, c64 * 64, w);
+          else acc16(tm, 0, w);
+#pragma unroll
+          for (int cc = 0; cc < CB / 16; ++cc) {
+            const int c = c64 * (CB / 16) + cc;
+            float *v = w + 16 * cc;
             if (grow < a.rows) {
-                for (int k = 0; k < 16; ++k) v[k] += a.w.b2[c * 16 + k];
+                for (int k = 0; k < 16; ++k) v[k] += s_b2[c * 16 + k];
                 if (a.resid) {
                     float r[8];
-                    const uint4 *src = reinterpret_cast<const uint4 *>(a.resid + grow * NOUT + c * 16);
-                    tc::unpack8(src[0], r);
+                    uint4 r0, r1;
+                    if (HC > 0 && a.resid_src0) {   // source 0 is still staged in chunks [0, 16)
+                        r0 = *reinterpret_cast<const uint4 *>(sA + tc::tile_off(kRows, t, 2 * c));
+                        r1 = *reinterpret_cast<const uint4 *>(sA + tc::tile_off(kRows, t, 2 * c + 1));
+                    } else {
+                        const uint4 *src = reinterpret_cast<const uint4 *>(a.resid + grow * NOUT + c * 16);
+                        r0 = src[0];
+                        r1 = src[1];
+                    }
+                    tc::unpack8(r0, r);
                     for (int k = 0; k < 8; ++k) v[k] += r[k];
-                    tc::unpack8(src[1], r);
+                    tc::unpack8(r1, r);
                     for (int k = 0; k < 8; ++k) v[8 + k] += r[k];
                 }
-                if (a.out) {
+                if (a.out && kStaged) {
+                    out_put(sOut, t, 2 * c, tc::pack8(v));
+                    out_put(sOut, t, 2 * c + 1, tc::pack8(v + 8));
+                } else if (a.out) {
                     uint4 *dst = reinterpret_cast<uint4 *>(a.out + grow * NOUT + c * 16);
                     dst[0] = tc::pack8(v);
                     dst[1] = tc::pack8(v + 8);
@@ -228,9 +319,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fwd(FwdArgs a) {
                     for (int k = 0; k < 4; ++k) dst[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
                 }
             }
+          }
         }
         tc::fence_before_sync();
         __syncthreads();   // TMEM and the A tile are reused by the next tile
+        if (a.out && kStaged) {
+            copy_out(sOut, a.out, row0, a.rows);
+            __syncthreads();
+        }
     }
     tc_teardown(tm, 128, ok, a.err);
 }
@@ -250,23 +346,26 @@ struct BwdArgs {
 
 template <int KIN, int NOUT>
 constexpr size_t bwd_smem() {
-    return (size_t)kHidden * NOUT * 2 + (size_t)KIN * kHidden * 2 + (size_t)kRows * NOUT * 2 + (size_t)kRows * kHidden * 2 + 64;
+    return (size_t)kHidden * NOUT * 2 + (size_t)KIN * kHidden * 2 + (size_t)kRows * NOUT * 2 +
+           2 * (size_t)kRows * kHidden * 2 + 64;
 }
 
 template <int KIN, int NOUT>
 __global__ void __launch_bounds__(kThreads, 1) k_mlp_bwd(BwdArgs a) {
-    extern __shared__ __align__(1024) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     unsigned char *sW2 = smem;                                  // W2: 128 rows (in) x NOUT
     unsigned char *sW1 = sW2 + (size_t)kHidden * NOUT * 2;      // W1: KIN rows (in) x 128
     unsigned char *sY = sW1 + (size_t)KIN * kHidden * 2;        // dY tile: 128 x NOUT
     unsigned char *sZ = sY + (size_t)kRows * NOUT * 2;          // dZ tile: 128 x 128
-    uint64_t *mbar = reinterpret_cast<uint64_t *>(sZ + (size_t)kRows * kHidden * 2);
+    unsigned char *sH = sZ + (size_t)kRows * kHidden * 2;       // saved hidden tile: 128 x 128
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(sH + (size_t)kRows * kHidden * 2);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 1);
     const int t = threadIdx.x;
     const bool want_dx = a.dx != nullptr;
 
     stage_dense(sW2, a.w.w2, kHidden, NOUT, 0, kHidden);
     if (want_dx) stage_dense(sW1, a.w.w1, KIN, kHidden, 0, KIN);
+    cp_wait_all();
     const uint32_t tm = tc_setup(mbar, tslot, 512);
     const uint32_t aW1 = tc::smem_u32(sW1), aW2 = tc::smem_u32(sW2), aY = tc::smem_u32(sY), aZ = tc::smem_u32(sZ);
     constexpr uint32_t id1 = tc::idesc_bf16(kRows, kHidden, false, false);
@@ -279,9 +378,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_bwd(BwdArgs a) {
         const long row0 = tile * kRows;
         const long grow = row0 + t;
         stage_dense(sY, a.dy, kRows, NOUT, row0, a.rows);
-        tc::fence_async_smem();
-        tc::fence_before_sync();
-        __syncthreads();
+        stage_dense(sH, a.h1, kRows, kHidden, row0, a.rows);
+        stage_done();
         if (t == 0) {
             tc::fence_after_sync();
             for (int ks = 0; ks < NOUT / 16; ++ks)
@@ -294,10 +392,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_bwd(BwdArgs a) {
             float v[16], h[8];
             acc16(tm, c * 16, v);
             if (grow < a.rows) {
-                const uint4 *hs = reinterpret_cast<const uint4 *>(a.h1 + grow * kHidden + c * 16);
-                tc::unpack8(hs[0], h);
+                tc::unpack8(*reinterpret_cast<const uint4 *>(sH + tc::tile_off(kRows, t, 2 * c)), h);
                 for (int k = 0; k < 8; ++k) v[k] = h[k] > 0.f ? v[k] : 0.f;
-                tc::unpack8(hs[1], h);
+                tc::unpack8(*reinterpret_cast<const uint4 *>(sH + tc::tile_off(kRows, t, 2 * c + 1)), h);
                 for (int k = 0; k < 8; ++k) v[8 + k] = h[k] > 0.f ? v[8 + k] : 0.f;
             } else {
                 for (int k = 0; k < 16; ++k) v[k] = 0.f;
@@ -369,13 +466,14 @@ constexpr size_t wgrad_smem() {
 
 template <int KIN, int NOUT>
 __global__ void __launch_bounds__(kThreads, 1) k_mlp_wgrad(WgradArgs a) {
-    extern __shared__ __align__(1024) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     unsigned char *sZ = smem;                                   // dZ tile: 128 rows x 128
     unsigned char *sH = sZ + (size_t)kRows * kHidden * 2;       // H tile: 128 x 128
     unsigned char *sX = sH + (size_t)kRows * kHidden * 2;       // X tile: 128 x KIN
     unsigned char *sY = sX + (size_t)kRows * KIN * 2;           // dY tile: 128 x NOUT
     uint64_t *mbar = reinterpret_cast<uint64_t *>(sY + (size_t)kRows * NOUT * 2);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 1);
+    __shared__ int s_idx[3 * kRows];
     const int t = threadIdx.x;
     constexpr int TC = wgrad_tmem_cols<KIN, NOUT>();
     const uint32_t tm = tc_setup(mbar, tslot, TC);
@@ -390,13 +488,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_wgrad(WgradArgs a) {
     const long ntiles = (a.rows + kRows - 1) / kRows;
     for (long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
         const long row0 = tile * kRows;
+        load_row_index(s_idx, a.src, a.nsrc, row0, a.rows);
+        __syncthreads();
         stage_dense(sZ, a.dz1, kRows, kHidden, row0, a.rows);
         stage_dense(sH, a.h1, kRows, kHidden, row0, a.rows);
-        stage_gather(sX, a.src, a.nsrc, KIN / 8, row0, a.rows);
+        stage_gather(sX, a.src, a.nsrc, KIN / 8, row0, a.rows, s_idx);
         stage_dense(sY, a.dy, kRows, NOUT, row0, a.rows);
-        tc::fence_async_smem();
-        tc::fence_before_sync();
-        __syncthreads();
+        stage_done();
         if (t == 0) {
             tc::fence_after_sync();
             for (int j = 0; j < KIN / NX; ++j)   // dW1^T[:, j*NX .. ] += dZ^T X_j
@@ -444,7 +542,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_wgrad(WgradArgs a) {
 
 // Sum the per-CTA partials in block order and add them to the gradient buffers:
 // g_w1t [128][KIN], g_b1 [128], g_w2t [NOUT][128], g_b2 [NOUT].
-__global__ void k_wgrad_reduce(const float *part, int nblocks, int kin, int nout, float *g_w1t, float *g_b1,
+__global__ void k_wgrad_reduce(const float *part, int nblocks, int kin, int nout, float *g_w1t, int ld_w1, float *g_b1,
                                float *g_w2t, float *g_b2) {
     const int nw2 = nout == kHidden ? kHidden : nout;
     const int nc = kin + nw2 + 2;
@@ -452,7 +550,7 @@ __global__ void k_wgrad_reduce(const float *part, int nblocks, int kin, int nout
         const int r = e / nc, c = e % nc;
         float s = 0.f;
         for (int b = 0; b < nblocks; ++b) s += part[((long)b * kRows + r) * nc + c];
-        if (c < kin) g_w1t[r * kin + c] += s;
+        if (c < kin) g_w1t[(long)r * ld_w1 + c] += s;
         else if (c < kin + nw2) {
             const int cc = c - kin;
             if (nout == kHidden) g_w2t[r * kHidden + cc] += s;   // row r = output unit
@@ -465,16 +563,297 @@ __global__ void k_wgrad_reduce(const float *part, int nblocks, int kin, int nout
 // Dynamic shared memory is raised so that the CTAs one SM can hold never ask for more TMEM
 // columns than its 512 (an allocation that cannot be met would wait for another CTA).
 // 228 KB of shared memory per SM: > 114 KB leaves one CTA, > 76 KB two, > 57 KB three.
+// ------------------------------------------------------------------------------------
+// factorised edge layer:  z = W1e e + P[recv] + Q[send] + b1,  PQ = [W1i h | W1j h]
+// (W1 = [W1e | W1i | W1j] of the 384-wide edge-update perceptron), e' = e + W2 relu(z) + b2
+// ------------------------------------------------------------------------------------
+struct LinArgs {
+    long rows;
+    const bf16 *x;      // [rows][KIN]
+    const bf16 *wt;     // [NOUT][KIN] (out x in)
+    bf16 *out;          // [rows][NOUT]
+    float *acc_out;     // [rows][NOUT] FP32, added to (used instead of out when set)
+    int *err;
+};
+
+// out = x W^T (no bias), M = 128 rows per tile, N = NOUT (<= 256), K = KIN.
+template <int KIN, int NOUT>
+constexpr size_t lin_smem() { return (size_t)NOUT * KIN * 2 + (size_t)kRows * KIN * 2 + 64; }
+
+template <int KIN, int NOUT>
+__global__ void __launch_bounds__(kThreads, 1) k_linear(LinArgs a) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    unsigned char *sW = smem;                                  // NOUT rows x KIN
+    unsigned char *sA = sW + (size_t)NOUT * KIN * 2;           // 128 rows x KIN
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(sA + (size_t)kRows * KIN * 2);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 1);
+    const int t = threadIdx.x;
+    constexpr int TC = NOUT <= 128 ? 128 : 256;
+    stage_dense(sW, a.wt, NOUT, KIN, 0, NOUT);
+    cp_wait_all();
+    const uint32_t tm = tc_setup(mbar, tslot, TC);
+    const uint32_t aW = tc::smem_u32(sW), aA = tc::smem_u32(sA);
+    constexpr uint32_t id = tc::idesc_bf16(kRows, NOUT, false, false);
+    uint32_t phase = 0;
+    bool ok = true;
+    const long ntiles = (a.rows + kRows - 1) / kRows;
+    for (long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+        const long row0 = tile * kRows, grow = row0 + t;
+        stage_dense(sA, a.x, kRows, KIN, row0, a.rows);
+        stage_done();
+        if (t == 0) {
+            tc::fence_after_sync();
+            for (int ks = 0; ks < KIN / 16; ++ks)
+                tc::mma_bf16(tm, tc::kmajor_desc(aA, kRows, ks), tc::kmajor_desc(aW, NOUT, ks), id, ks > 0);
+            tc::mma_commit(mbar);
+        }
+        ok = mma_wait(mbar, phase);
+        if (!ok) break;
+        for (int c = 0; c < NOUT / 16; ++c) {
+            float v[16];
+            acc16(tm, c * 16, v);
+            if (grow < a.rows) {
+                if (a.acc_out) {
+                    float4 *d = reinterpret_cast<float4 *>(a.acc_out + grow * NOUT + c * 16);
+                    for (int k = 0; k < 4; ++k) {
+                        float4 o = d[k];
+                        o.x += v[4 * k];
+                        o.y += v[4 * k + 1];
+                        o.z += v[4 * k + 2];
+                        o.w += v[4 * k + 3];
+                        d[k] = o;
+                    }
+                } else {
+                    uint4 *d = reinterpret_cast<uint4 *>(a.out + grow * NOUT + c * 16);
+                    d[0] = tc::pack8(v);
+                    d[1] = tc::pack8(v + 8);
+                }
+            }
+        }
+        tc::fence_before_sync();
+        __syncthreads();
+    }
+    tc_teardown(tm, TC, ok, a.err);
+}
+
+struct EdgeArgs {
+    long rows;
+    const bf16 *e;       // [rows][128] input latent, also the residual
+    const bf16 *pq;      // [nodes][256]
+    const int *recv, *send;
+    const bf16 *w1e_t;   // [128][128]
+    const float *b1;
+    const bf16 *w2t;     // [128][128]
+    const float *b2;
+    bf16 *out;           // [rows][128]
+    bf16 *h1;            // [rows][128] or null
+    int *err;
+};
+
+constexpr size_t edge_smem() { return 3 * (size_t)kRows * kHidden * 2 + 64; }
+
+// Two CTAs of 256 threads per SM (96 KB of shared memory each), so that one CTA's tensor-core
+// and memory waits overlap the other's epilogues.  Thread (row t, half) prefetches the half
+// rows of P[recv] and Q[send] it needs into registers before the first product, reloads its
+// residual half row (an L2 hit) while the second product runs, and writes its output through
+// the spent tile so that whole 256-byte rows leave the SM.
+__global__ void __launch_bounds__(kFwdThreads, 2) k_edge_fwd(EdgeArgs a) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    constexpr size_t T = (size_t)kRows * kHidden * 2;
+    unsigned char *sW1 = smem;          // W1e^T 128 x 128
+    unsigned char *sW2 = sW1 + T;       // W2^T 128 x 128
+    unsigned char *sA = sW2 + T;        // e tile -> hidden tile -> output tile
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(sA + T);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 1);
+    __shared__ float s_b1[kHidden], s_b2[kHidden];
+    const int tid = threadIdx.x;
+    const int t = tid & (kRows - 1);   // tile row (TMEM lane)
+    const int half = tid >> 7;         // features [64 half, 64 half + 64)
+    if (half == 0) s_b1[t] = a.b1[t];
+    else s_b2[t] = a.b2[t];
+    stage_dense(sW1, a.w1e_t, kHidden, kHidden, 0, kHidden);
+    stage_dense(sW2, a.w2t, kHidden, kHidden, 0, kHidden);
+    cp_wait_all();
+    const uint32_t tm = tc_setup(mbar, tslot, 128);
+    const uint32_t aW1 = tc::smem_u32(sW1), aW2 = tc::smem_u32(sW2), aA = tc::smem_u32(sA);
+    constexpr uint32_t id = tc::idesc_bf16(kRows, kHidden, false, false);
+    uint32_t phase = 0;
+    bool ok = true;
+    const long ntiles = (a.rows + kRows - 1) / kRows;
+    for (long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+        const long row0 = tile * kRows, grow = row0 + t;
+        const bool live = grow < a.rows;
+        stage_dense(sA, a.e, kRows, kHidden, row0, a.rows);
+        uint4 p[8], q[8];
+        {
+            const long r = live ? a.recv[grow] : 0, c = live ? a.send[grow] : 0;
+            const uint4 *ps = reinterpret_cast<const uint4 *>(a.pq + r * 2 * kHidden + half * 64);
+            const uint4 *qs = reinterpret_cast<const uint4 *>(a.pq + c * 2 * kHidden + kHidden + half * 64);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                p[k] = ps[k];
+                q[k] = qs[k];
+            }
+        }
+        stage_done();
+        if (tid == 0) {
+            tc::fence_after_sync();
+            for (int ks = 0; ks < kHidden / 16; ++ks)
+                tc::mma_bf16(tm, tc::kmajor_desc(aA, kRows, ks), tc::kmajor_desc(aW1, kHidden, ks), id, ks > 0);
+            tc::mma_commit(mbar);
+        }
+        ok = mma_wait(mbar, phase);
+        if (!ok) break;
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {   // two batches of 32 columns keep the P/Q registers live
+            float w[32];
+            acc32(tm, half * 64 + b * 32, w);
+#pragma unroll
+            for (int c2 = 0; c2 < 2; ++c2) {
+                const int cc = 2 * b + c2;
+                const int c = half * 4 + cc;   // 16-feature group
+                float *v = w + 16 * c2, pf[8], qf[8];
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    tc::unpack8(p[2 * cc + h], pf);
+                    tc::unpack8(q[2 * cc + h], qf);
+                    for (int k = 0; k < 8; ++k)
+                        v[8 * h + k] = fmaxf(v[8 * h + k] + s_b1[c * 16 + 8 * h + k] + pf[k] + qf[k], 0.f);
+                }
+                const uint4 lo = tc::pack8(v), hi = tc::pack8(v + 8);
+                *reinterpret_cast<uint4 *>(sA + tc::tile_off(kRows, t, 2 * c)) = lo;
+                *reinterpret_cast<uint4 *>(sA + tc::tile_off(kRows, t, 2 * c + 1)) = hi;
+                if (a.h1 && live) {
+                    uint4 *dst = reinterpret_cast<uint4 *>(a.h1 + grow * kHidden + c * 16);
+                    dst[0] = lo;
+                    dst[1] = hi;
+                }
+            }
+        }
+        tc::fence_async_smem();
+        tc::fence_before_sync();
+        __syncthreads();
+        if (tid == 0) {
+            tc::fence_after_sync();
+            for (int ks = 0; ks < kHidden / 16; ++ks)
+                tc::mma_bf16(tm, tc::kmajor_desc(aA, kRows, ks), tc::kmajor_desc(aW2, kHidden, ks), id, ks > 0);
+            tc::mma_commit(mbar);
+        }
+        {   // residual half row while the second product runs
+            const uint4 *es = reinterpret_cast<const uint4 *>(a.e + (live ? grow : 0) * kHidden + half * 64);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) p[k] = es[k];
+        }
+        ok = mma_wait(mbar, phase);
+        if (!ok) break;
+        {
+            float w[64];
+            acc64(tm, half * 64, w);
+#pragma unroll
+            for (int cc = 0; cc < 4; ++cc) {
+                const int c = half * 4 + cc;
+                float *v = w + 16 * cc, r[8];
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    tc::unpack8(p[2 * cc + h], r);
+                    for (int k = 0; k < 8; ++k) v[8 * h + k] += s_b2[c * 16 + 8 * h + k] + r[k];
+                }
+                out_put(sA, t, 2 * c, tc::pack8(v));
+                out_put(sA, t, 2 * c + 1, tc::pack8(v + 8));
+            }
+        }
+        tc::fence_before_sync();
+        __syncthreads();
+        copy_out(sA, a.out, row0, a.rows);
+        __syncthreads();
+    }
+    tc_teardown(tm, 128, ok, a.err);
+}
+
+// dW^T [256][128] partials: D_half[o][k] = sum_rows A[row][128 half + o] B[row][k]
+struct LinWgradArgs {
+    long rows;
+    const bf16 *a;     // [rows][256]
+    const bf16 *b;     // [rows][128]
+    float *part;       // [gridDim.x][128][256]
+    int *err;
+};
+constexpr size_t linw_smem() { return (size_t)kRows * 256 * 2 + (size_t)kRows * kHidden * 2 + 64; }
+
+__global__ void __launch_bounds__(kThreads, 1) k_linear_wgrad(LinWgradArgs a) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    unsigned char *sA = smem;                              // 128 rows x 256
+    unsigned char *sB = sA + (size_t)kRows * 256 * 2;      // 128 rows x 128
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(sB + (size_t)kRows * kHidden * 2);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 1);
+    const int t = threadIdx.x;
+    const uint32_t tm = tc_setup(mbar, tslot, 256);
+    const uint32_t aA = tc::smem_u32(sA), aB = tc::smem_u32(sB);
+    constexpr uint32_t id = tc::idesc_bf16(kRows, kHidden, true, true);
+    uint32_t phase = 0;
+    bool ok = true, first = true;
+    const long ntiles = (a.rows + kRows - 1) / kRows;
+    for (long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+        const long row0 = tile * kRows;
+        stage_dense(sA, a.a, kRows, 256, row0, a.rows);
+        stage_dense(sB, a.b, kRows, kHidden, row0, a.rows);
+        stage_done();
+        if (t == 0) {
+            tc::fence_after_sync();
+            for (int h = 0; h < 2; ++h)
+                for (int ks = 0; ks < kRows / 16; ++ks)
+                    tc::mma_bf16(tm + h * kHidden, tc::mnmajor_desc(aA + (uint32_t)(h * 16 * kRows * 16), kRows, ks),
+                                 tc::mnmajor_desc(aB, kRows, ks), id, (!first || ks > 0) ? 1u : 0u);
+            tc::mma_commit(mbar);
+        }
+        ok = mma_wait(mbar, phase);
+        first = false;
+        tc::fence_before_sync();
+        __syncthreads();
+    }
+    float *dst = a.part + ((long)blockIdx.x * kRows + t) * 256;
+    if (ok && !first) {
+        tc::fence_after_sync();
+        for (int c = 0; c < 256 / 16; ++c) {
+            float v[16];
+            acc16(tm, c * 16, v);
+            for (int k = 0; k < 16; ++k) dst[c * 16 + k] = v[k];
+        }
+    } else {
+        for (int c = 0; c < 256; ++c) dst[c] = 0.f;
+    }
+    tc_teardown(tm, 256, ok, a.err);
+}
+
+// g[o * ld + col0 + c] += sum over blocks of part[b][o][c]   (o < 128, c < 256)
+__global__ void k_linw_reduce(const float *part, int nblocks, float *g, int ld, int col0) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < kRows * 256; e += gridDim.x * blockDim.x) {
+        const int o = e / 256, c = e % 256;
+        float s = 0.f;
+        for (int b = 0; b < nblocks; ++b) s += part[((long)b * kRows + o) * 256 + c];
+        g[(long)o * ld + col0 + c] += s;
+    }
+}
+
 template <typename K, typename A>
-int launch_tc(K kernel, size_t smem, int tmem_cols, long rows, A args, cudaStream_t s, int max_blocks = 148) {
+int launch_tc(K kernel, size_t smem, int tmem_cols, long rows, A args, cudaStream_t s, int max_blocks = 148,
+              int threads = kThreads) {
     if (rows <= 0) return DEM_OK;
     const size_t floor_bytes = tmem_cols >= 512 ? 116 * 1024 : (tmem_cols >= 256 ? 80 * 1024 : 0);
     if (smem < floor_bytes) smem = floor_bytes;
     if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return DEM_ERR_CUDA;
     const long ntiles = (rows + kRows - 1) / kRows;
+    if (max_blocks <= 0) {   // as many CTAs as the SMs hold (shared memory and TMEM), persistent
+        cudaFuncAttributes fa{};
+        if (cudaFuncGetAttributes(&fa, kernel) != cudaSuccess) return DEM_ERR_CUDA;
+        const size_t per = smem + fa.sharedSizeBytes + 1024;
+        int fit = (int)((228 * 1024) / per);
+        fit = fit < 512 / tmem_cols ? fit : 512 / tmem_cols;
+        max_blocks = 148 * (fit > 0 ? fit : 1);
+    }
     const int grid = (int)(ntiles < max_blocks ? ntiles : max_blocks);
-    kernel<<<grid, kThreads, smem, s>>>(args);
+    kernel<<<grid, threads, smem, s>>>(args);
     return cudaGetLastError() == cudaSuccess ? DEM_OK : DEM_ERR_CUDA;
 }
 
@@ -496,20 +875,22 @@ int nn_mlp_forward(const dem_nn_mlp &m, long rows, const dem_nn_rows *src, int n
     if (kin != m.kin) return DEM_ERR_INVALID;
     a.w = MlpW{(const bf16 *)m.w1t, (const bf16 *)m.w1, (const bf16 *)m.w2t, (const bf16 *)m.w2, m.b1, m.b2};
     a.resid = (const bf16 *)resid;
+    a.resid_src0 = (resid && resid == src[0].data && !src[0].index && src[0].width == m.nout) ? 1 : 0;
     a.out = (bf16 *)out;
     a.out_f32 = out_f32;
     a.h1 = (bf16 *)h1;
     a.err = err;
 #define X(KI, NO) \
-    if (m.kin == KI && m.nout == NO) return launch_tc(k_mlp_fwd<KI, NO>, fwd_smem<KI, NO>(), 128, rows, a, s);
+    if (m.kin == KI && m.nout == NO)                                                                        \
+        return launch_tc(k_mlp_fwd<KI, NO>, fwd_smem<KI, NO>(), 128, rows, a, s, 0, kFwdThreads);
     B200_NN_SHAPES(X)
 #undef X
     return DEM_ERR_UNSUPPORTED;
 }
 
 int nn_mlp_backward(const dem_nn_mlp &m, long rows, const dem_nn_rows *src, int nsrc, const void *dy, const void *h1,
-                    void *dz1, float *dx, float *g_w1t, float *g_b1, float *g_w2t, float *g_b2, float *part,
-                    int *err, cudaStream_t s) {
+                    void *dz1, float *dx, float *g_w1t, int ld_w1, float *g_b1, float *g_w2t, float *g_b2,
+                    float *part, int *err, cudaStream_t s) {
     BwdArgs b{};
     b.rows = rows;
     b.w = MlpW{(const bf16 *)m.w1t, (const bf16 *)m.w1, (const bf16 *)m.w2t, (const bf16 *)m.w2, m.b1, m.b2};
@@ -543,9 +924,42 @@ int nn_mlp_backward(const dem_nn_mlp &m, long rows, const dem_nn_rows *src, int 
     B200_NN_SHAPES(X)
 #undef X
     if (st != DEM_OK || rows <= 0) return st;
-    k_wgrad_reduce<<<64, 256, 0, s>>>(part, nblocks, m.kin, m.nout, g_w1t, g_b1, g_w2t, g_b2);
+    k_wgrad_reduce<<<64, 256, 0, s>>>(part, nblocks, m.kin, m.nout, g_w1t, ld_w1, g_b1, g_w2t, g_b2);
     return cudaGetLastError() == cudaSuccess ? DEM_OK : DEM_ERR_CUDA;
 }
+
+// PQ[rows][256] = h W1ij^T (W1ij^T: [256][128]).
+int nn_linear_pq(long rows, const void *h, const void *w1ij_t, void *pq, int *err, cudaStream_t s) {
+    LinArgs a{rows, (const bf16 *)h, (const bf16 *)w1ij_t, (bf16 *)pq, nullptr, err};
+    return launch_tc(k_linear<128, 256>, lin_smem<128, 256>(), 256, rows, a, s, 0);
+}
+
+// dh[rows][128] += dPQ W1ij (dPQ: [rows][256] bf16, W1ij: [128][256]).
+int nn_linear_pq_backward(long rows, const void *dpq, const void *w1ij, float *dh, int *err, cudaStream_t s) {
+    LinArgs a{rows, (const bf16 *)dpq, (const bf16 *)w1ij, nullptr, dh, err};
+    return launch_tc(k_linear<256, 128>, lin_smem<256, 128>(), 128, rows, a, s, 0);
+}
+
+// g_w1t[o][col0 + c] += sum_rows dPQ[row][c'] h[row][k] arranged as dW1ij^T (ld = row stride).
+int nn_linear_pq_wgrad(long rows, const void *dpq, const void *h, float *g_w1t, int ld, int col0, float *part,
+                       int *err, cudaStream_t s) {
+    if (rows <= 0) return DEM_OK;
+    LinWgradArgs a{rows, (const bf16 *)dpq, (const bf16 *)h, part, err};
+    const int st = launch_tc(k_linear_wgrad, linw_smem(), 256, rows, a, s);
+    if (st) return st;
+    const long ntiles = (rows + kRows - 1) / kRows;
+    k_linw_reduce<<<64, 256, 0, s>>>(part, (int)(ntiles < 148 ? ntiles : 148), g_w1t, ld, col0);
+    return cudaGetLastError() == cudaSuccess ? DEM_OK : DEM_ERR_CUDA;
+}
+
+int nn_edge_forward(long rows, const void *e, const void *pq, const int *recv, const int *send, const void *w1e_t,
+                    const float *b1, const void *w2t, const float *b2, void *out, void *h1, int *err, cudaStream_t s) {
+    EdgeArgs a{rows, (const bf16 *)e, (const bf16 *)pq, recv, send, (const bf16 *)w1e_t, b1, (const bf16 *)w2t, b2,
+               (bf16 *)out, (bf16 *)h1, err};
+    return launch_tc(k_edge_fwd, edge_smem(), 128, rows, a, s, 0, kFwdThreads);
+}
+
+long nn_linear_wgrad_scratch() { return 148L * kRows * 256; }
 
 // Scratch floats the per-CTA weight-gradient partials of one backward call need.
 long nn_wgrad_scratch(int kin, int nout) {

@@ -48,6 +48,7 @@ constexpr Shape kShape[kNL] = {{16, 128}, {16, 128}, {384, 128}, {256, 128}, {38
 constexpr int L_ENC_N = 0, L_ENC_E = 1, L_DEC = 8;
 inline int L_MSG(int l) { return 2 + 2 * l; }
 inline int L_UPD(int l) { return 3 + 2 * l; }
+inline bool is_msg(int l) { return l == 2 || l == 4 || l == 6; }
 
 struct FeatConst {
     double inv_rg, inv_sd, sigma_a, r_mean, inv_r_mean, inv_r_std, inv_clip;
@@ -238,31 +239,6 @@ __global__ void k_segsum(int n, const int *offs, const bf16 *ev, bf16 *agg) {
     }
 }
 
-// dh[i] += sum_e dx[e][c0:c0+128] + sum_e dx[rev[e]][c1:c1+128] over node i's edges (FP32).
-__global__ void k_node_from_edges(int n, const int *offs, const int *rev, const float *dx, int ld, int c0, int c1,
-                                  float *dh) {
-    const int lane = threadIdx.x & 31;
-    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += (gridDim.x * blockDim.x) >> 5) {
-        float4 s = *reinterpret_cast<const float4 *>(dh + (long)i * kH + 4 * lane);
-        for (int e = offs[i]; e < offs[i + 1]; ++e) {
-            const float4 a = *reinterpret_cast<const float4 *>(dx + (long)e * ld + c0 + 4 * lane);
-            s.x += a.x;
-            s.y += a.y;
-            s.z += a.z;
-            s.w += a.w;
-            const int r = rev[e];
-            if (r >= 0) {
-                const float4 b = *reinterpret_cast<const float4 *>(dx + (long)r * ld + c1 + 4 * lane);
-                s.x += b.x;
-                s.y += b.y;
-                s.z += b.z;
-                s.w += b.w;
-            }
-        }
-        *reinterpret_cast<float4 *>(dh + (long)i * kH + 4 * lane) = s;
-    }
-}
-
 // de[e] (=|+=) dn[recv[e]][c0:c0+128]
 __global__ void k_edge_from_node(int ne, const int *recv, const float *dn, int ld, int c0, float *de, int accumulate) {
     for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < (long)ne * (kH / 4); q += (long)gridDim.x * blockDim.x) {
@@ -368,6 +344,50 @@ __global__ void k_refresh(int kin, int nout, const float *w1t, const float *w2t,
     }
 }
 
+// Message layers: W1 = [W1e | W1i | W1j] (128 x 384) also as W1e^T [128][128], W1e [128][128],
+// W1ij^T [256][128] (row 128 h + o = W1t[o][128 + 128 h + k]) and W1ij [128][256].
+__global__ void k_refresh_msg(const float *w1t, bf16 *e_t, bf16 *e, bf16 *ij_t, bf16 *ij) {
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < kH * 384; q += gridDim.x * blockDim.x) {
+        const int o = q / 384, c = q % 384;
+        const bf16 x = __float2bfloat16_rn(w1t[q]);
+        if (c < kH) {
+            e_t[o * kH + c] = x;
+            e[c * kH + o] = x;
+        } else {
+            const int half = (c - kH) / kH, k = (c - kH) % kH;
+            const int row = half * kH + o;        // row of W1ij^T
+            ij_t[row * kH + k] = x;
+            ij[k * 2 * kH + row] = x;
+        }
+    }
+}
+
+// dPQ[i] = [sum over i's edges of dz1[e] | sum over edges sending from i of dz1[e]] (BF16 out).
+__global__ void k_dpq(int n, const int *offs, const int *rev, const bf16 *dz1, bf16 *dpq) {
+    const int lane = threadIdx.x & 31;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += (gridDim.x * blockDim.x) >> 5) {
+        float p[4] = {0.f, 0.f, 0.f, 0.f}, q[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int e = offs[i]; e < offs[i + 1]; ++e) {
+            const uint2 u = *reinterpret_cast<const uint2 *>(dz1 + (long)e * kH + 4 * lane);
+            const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&u.x));
+            const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&u.y));
+            p[0] += a.x; p[1] += a.y; p[2] += b.x; p[3] += b.y;
+            const int r = rev[e];
+            if (r >= 0) {
+                const uint2 w = *reinterpret_cast<const uint2 *>(dz1 + (long)r * kH + 4 * lane);
+                const float2 c = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&w.x));
+                const float2 d = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&w.y));
+                q[0] += c.x; q[1] += c.y; q[2] += d.x; q[3] += d.y;
+            }
+        }
+        bf16 *o = dpq + (long)i * 2 * kH;
+        *reinterpret_cast<__nv_bfloat162 *>(o + 4 * lane) = __floats2bfloat162_rn(p[0], p[1]);
+        *reinterpret_cast<__nv_bfloat162 *>(o + 4 * lane + 2) = __floats2bfloat162_rn(p[2], p[3]);
+        *reinterpret_cast<__nv_bfloat162 *>(o + kH + 4 * lane) = __floats2bfloat162_rn(q[0], q[1]);
+        *reinterpret_cast<__nv_bfloat162 *>(o + kH + 4 * lane + 2) = __floats2bfloat162_rn(q[2], q[3]);
+    }
+}
+
 // ---- stride update and checks ----
 __global__ void k_integrate(int n, const double4 *pk, const double2 *disp, const float *out, double sa, FeatConst fc,
                             const double *cur3, double *next3) {
@@ -386,6 +406,44 @@ __global__ void k_integrate(int n, const double4 *pk, const double2 *disp, const
         next3[3 * i + 1] = y;
         next3[3 * i + 2] = cur3[3 * i + 2];
     }
+}
+
+// One Jacobi sweep of contact projection on positions q (caller [n][3]) -> qo: every pair of
+// the graph overlapping by more than allow * min(r_i, r_j) is pushed apart along its normal,
+// each side by its mass share of the excess (times 0.5, for stability of the simultaneous
+// update); walls push a particle back to contact.
+__global__ void k_project(int n, const int *offs, const int *send, const double *q, const double *rad,
+                          const double *mass, FeatConst fc, double allow, double *qo) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double xi = q[3 * i], yi = q[3 * i + 1], ri = rad[i], mi = mass[i];
+        double dx_acc = 0.0, dy_acc = 0.0;
+        for (int e = offs[i]; e < offs[i + 1]; ++e) {
+            const int j = send[e];
+            const double dx = q[3 * j] - xi, dy = q[3 * j + 1] - yi;
+            const double d = sqrt(dx * dx + dy * dy);
+            const double excess = ri + rad[j] - d - allow * fmin(ri, rad[j]);
+            if (excess > 0.0 && d > 0.0) {
+                const double share = 0.5 * mass[j] / (mi + mass[j]);
+                dx_acc -= share * excess * dx / d;
+                dy_acc -= share * excess * dy / d;
+            }
+        }
+        double x = xi + dx_acc, y = yi + dy_acc;
+        for (int w = 0; w < fc.nwalls; ++w) {
+            const double dist = (x - fc.wx[w][0]) * fc.wn[w][0] + (y - fc.wx[w][1]) * fc.wn[w][1] - ri;
+            if (dist < 0.0) {
+                x -= dist * fc.wn[w][0];
+                y -= dist * fc.wn[w][1];
+            }
+        }
+        qo[3 * i] = x;
+        qo[3 * i + 1] = y;
+        qo[3 * i + 2] = q[3 * i + 2];
+    }
+}
+
+__global__ void k_rad3(int n, const double *rad, double *w) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) w[i] = rad[i] * rad[i] * rad[i];
 }
 
 // Largest overlap / smaller radius over the graph's pairs at positions q (caller [n][3]) and
@@ -515,10 +573,12 @@ struct dem_surrogate {
     bf16 *h1[kNL] = {};
     float *out = nullptr;
     bf16 *dout = nullptr, *dz1 = nullptr, *dyb = nullptr;
+    bf16 *pq = nullptr, *dpq = nullptr;   // [nodes][256] P | Q of a message layer and its gradient
     float *dxe = nullptr, *dxn = nullptr, *dh = nullptr, *de = nullptr;
     double *part = nullptr, *d_loss = nullptr;
     // rollout scratch (caller order)
-    double *x_prev = nullptr, *x_cur = nullptr, *x_next = nullptr, *rad = nullptr, *mass = nullptr;
+    double *x_prev = nullptr, *x_cur = nullptr, *x_next = nullptr, *x_tmp = nullptr, *rad = nullptr,
+           *mass = nullptr;
     int roll_n = 0;
     bool train_ready = false;
 };
@@ -530,6 +590,12 @@ int sg_fail(dem_surrogate *sg, int code, const char *msg) { return ctx_fail(sg->
     do {                                                                  \
         const cudaError_t _e = (call);                                    \
         if (_e != cudaSuccess) return ctx_cuda(sg->ctx, _e, #call);       \
+    } while (0)
+
+#define SG0(call)               \
+    do {                        \
+        const int _st = (call); \
+        if (_st) return _st;    \
     } while (0)
 
 dem_nn_mlp layer_desc(dem_surrogate *sg, int l) {
@@ -565,6 +631,10 @@ int refresh_bf16(dem_surrogate *sg) {
         bf16 *b = sg->wb + sg->boff[l];
         k_refresh<<<128, kTB, 0, s>>>(kin, nout, w, w + (long)kH * kin + kH, b, b + (long)kH * kin,
                                       b + 2L * kH * kin, b + 2L * kH * kin + (long)nout * kH);
+        if (is_msg(l)) {
+            bf16 *x = b + 2L * kH * kin + 2L * nout * kH;
+            k_refresh_msg<<<128, kTB, 0, s>>>(w, x, x + kH * kH, x + 2 * kH * kH, x + 4 * kH * kH);
+        }
     }
     SCK(cudaGetLastError());
     return DEM_OK;
@@ -608,6 +678,7 @@ int alloc_nodes(dem_surrogate *sg) {
     for (int k = 0; k < 4; ++k) SCK(dmalloc(&sg->h[k], (size_t)cap * kH));
     for (int k = 0; k < 3; ++k) SCK(dmalloc(&sg->agg[k], (size_t)cap * kH));
     SCK(dmalloc(&sg->out, (size_t)cap * kF));
+    SCK(dmalloc(&sg->pq, (size_t)cap * 2 * kH));
     SCK(dmalloc(&sg->part, 4 * (size_t)std::max(kLossBlocks, kChkBlocks)));
     SCK(dmalloc(&sg->d_loss, 8));
     Particles &P = sg->GP;
@@ -645,12 +716,13 @@ int ensure_edges(dem_surrogate *sg, long ne, bool training) {
         }
         SCK(dmalloc(&sg->dz1, (size_t)rows * kH));
         SCK(dmalloc(&sg->dyb, (size_t)rows * kH));
-        SCK(dmalloc(&sg->dxe, (size_t)cap * 384));
+        SCK(dmalloc(&sg->dxe, (size_t)cap * kH));
         SCK(dmalloc(&sg->de, (size_t)cap * kH));
         if (!sg->dxn) {
             SCK(dmalloc(&sg->dxn, (size_t)sg->cap * 256));
             SCK(dmalloc(&sg->dh, (size_t)sg->cap * kH));
             SCK(dmalloc(&sg->dout, (size_t)sg->cap * kF));
+            SCK(dmalloc(&sg->dpq, (size_t)sg->cap * 2 * kH));
         }
         sg->train_ready = true;
     }
@@ -718,9 +790,58 @@ int mlp_bwd(dem_surrogate *sg, int l, long rows, const dem_nn_rows *src, int nsr
     const dem_nn_mlp d = layer_desc(sg, l);
     float *gw1t, *gb1, *gw2t, *gb2;
     grad_ptrs(sg, l, &gw1t, &gb1, &gw2t, &gb2);
-    st = nn_mlp_backward(d, rows, src, nsrc, dy, sg->h1[l], sg->dz1, dx, gw1t, gb1, gw2t, gb2, part, err,
-                         ctx_stream(sg->ctx));
+    st = nn_mlp_backward(d, rows, src, nsrc, dy, sg->h1[l], sg->dz1, dx, gw1t, kShape[l].kin, gb1, gw2t, gb2, part,
+                         err, ctx_stream(sg->ctx));
     return st ? sg_fail(sg, st, "surrogate: dense layer backward") : DEM_OK;
+}
+
+// BF16 copies of a message layer: W1e^T, W1e, W1ij^T, W1ij.
+void msg_copies(dem_surrogate *sg, int l, const bf16 **e_t, const bf16 **e, const bf16 **ij_t, const bf16 **ij) {
+    const bf16 *x = sg->wb + sg->boff[l] + 2L * kH * 384 + 2L * kH * kH;
+    *e_t = x;
+    *e = x + kH * kH;
+    *ij_t = x + 2 * kH * kH;
+    *ij = x + 4 * kH * kH;
+}
+
+// e_out = e_in + Msg[e_in, h[recv], h[send]] through PQ = [W1i h | W1j h].
+int msg_fwd(dem_surrogate *sg, int l, int n, long ne, const bf16 *h, const bf16 *ein, bf16 *eout, bf16 *h1) {
+    int *err;
+    float *part;
+    SG0(ctx_nn_scratch(sg->ctx, 0, &err, &part));
+    const bf16 *e_t, *e, *ij_t, *ij;
+    msg_copies(sg, l, &e_t, &e, &ij_t, &ij);
+    const dem_nn_mlp d = layer_desc(sg, l);
+    cudaStream_t s = ctx_stream(sg->ctx);
+    int st = nn_linear_pq(n, h, ij_t, sg->pq, err, s);
+    if (!st) st = nn_edge_forward(ne, ein, sg->pq, sg->recv, sg->send, e_t, d.b1, d.w2t, d.b2, eout, h1, err, s);
+    return st ? sg_fail(sg, st, "surrogate: message layer forward") : DEM_OK;
+}
+
+// Backward of msg_fwd: dy (BF16 [ne][128]) -> dE_in (sg->dxe, FP32 [ne][128]), dh += dMsg/dh,
+// weight gradients added.
+int msg_bwd(dem_surrogate *sg, int l, int n, long ne, const bf16 *h, const bf16 *ein, const bf16 *dy, float *dh) {
+    int *err;
+    float *part;
+    const long need = std::max(nn_wgrad_scratch(128, 128), nn_linear_wgrad_scratch());
+    SG0(ctx_nn_scratch(sg->ctx, need, &err, &part));
+    const bf16 *e_t, *e, *ij_t, *ij;
+    msg_copies(sg, l, &e_t, &e, &ij_t, &ij);
+    const dem_nn_mlp full = layer_desc(sg, l);
+    dem_nn_mlp d = full;
+    d.kin = 128;
+    d.w1t = e_t;
+    d.w1 = e;
+    float *gw1t, *gb1, *gw2t, *gb2;
+    grad_ptrs(sg, l, &gw1t, &gb1, &gw2t, &gb2);
+    cudaStream_t s = ctx_stream(sg->ctx);
+    dem_nn_rows src{ein, nullptr, kH};
+    int st = nn_mlp_backward(d, ne, &src, 1, dy, sg->h1[l], sg->dz1, sg->dxe, gw1t, 384, gb1, gw2t, gb2, part, err, s);
+    if (st) return sg_fail(sg, st, "surrogate: message layer backward");
+    k_dpq<<<kGS, kTB, 0, s>>>(n, sg->offs, sg->rev, sg->dz1, sg->dpq);
+    st = nn_linear_pq_backward(n, sg->dpq, ij, dh, err, s);
+    if (!st) st = nn_linear_pq_wgrad(n, sg->dpq, h, gw1t, 384, kH, part, err, s);
+    return st ? sg_fail(sg, st, "surrogate: message layer backward") : DEM_OK;
 }
 
 #define SG(call)                \
@@ -746,8 +867,7 @@ int forward(dem_surrogate *sg, int n, long ne, bool training) {
         // inference keeps two edge latents (ping-pong); training keeps all four
         bf16 *ein = training ? sg->e[l] : sg->e[l & 1];
         bf16 *eout = training ? sg->e[l + 1] : sg->e[(l + 1) & 1];
-        dem_nn_rows ms[3] = {{ein, nullptr, kH}, {sg->h[l], sg->recv, kH}, {sg->h[l], sg->send, kH}};
-        SG(mlp_fwd(sg, L_MSG(l), ne, ms, 3, ein, eout, nullptr, H1(L_MSG(l))));
+        SG(msg_fwd(sg, L_MSG(l), n, ne, sg->h[l], ein, eout, H1(L_MSG(l))));
         k_segsum<<<kGS, kTB, 0, s>>>(n, sg->offs, eout, sg->agg[l]);
         dem_nn_rows us[2] = {{sg->h[l], nullptr, kH}, {sg->agg[l], nullptr, kH}};
         SG(mlp_fwd(sg, L_UPD(l), n, us, 2, sg->h[l], sg->h[l + 1], nullptr, H1(L_UPD(l))));
@@ -777,10 +897,8 @@ int backward(dem_surrogate *sg, int n, long ne) {
             k_edge_from_node<<<kGS, kTB, 0, s>>>((int)ne, sg->recv, sg->dxn, 256, 128, sg->de, 1);
             // e_{l+1} = e_l + Msg[e_l, h_l[recv], h_l[send]]
             k_f2bf<<<kGS, kTB, 0, s>>>(ne * kH, sg->de, sg->dyb);
-            dem_nn_rows ms[3] = {{sg->e[l], nullptr, kH}, {sg->h[l], sg->recv, kH}, {sg->h[l], sg->send, kH}};
-            SG(mlp_bwd(sg, L_MSG(l), ne, ms, 3, sg->dyb, sg->dxe));
-            k_add_cols<<<kGS, kTB, 0, s>>>(ne, sg->dxe, 384, 0, sg->de);      // de_l = de_{l+1} + dMsg/de_l
-            k_node_from_edges<<<kGS, kTB, 0, s>>>(n, sg->offs, sg->rev, sg->dxe, 384, 128, 256, sg->dh);
+            SG(msg_bwd(sg, L_MSG(l), n, ne, sg->h[l], sg->e[l], sg->dyb, sg->dh));   // dh += dMsg/dh_l
+            k_add_cols<<<kGS, kTB, 0, s>>>(ne, sg->dxe, kH, 0, sg->de);       // de_l = de_{l+1} + dMsg/de_l
         }
     }
     if (ne > 0) {
@@ -826,6 +944,19 @@ int loss_grad(dem_surrogate *sg, int n, const double *prev, const double *cur, c
     return DEM_OK;
 }
 
+// Contact projection of q in place (tmp: scratch of the same size), on the current graph.
+int project(dem_surrogate *sg, int n, double *q, double *tmp, const double *rad, const double *mass) {
+    cudaStream_t s = ctx_stream(sg->ctx);
+    const int it = sg->prm.project_iters;
+    for (int k = 0; k < it; ++k) {
+        k_project<<<kGS, kTB, 0, s>>>(n, sg->offs, sg->send, k % 2 == 0 ? q : tmp, rad, mass, sg->fc,
+                                      sg->prm.project_allow, k % 2 == 0 ? tmp : q);
+    }
+    if (it % 2 == 1) SCK(cudaMemcpyAsync(q, tmp, sizeof(double) * 3 * (size_t)n, cudaMemcpyDeviceToDevice, s));
+    SCK(cudaGetLastError());
+    return DEM_OK;
+}
+
 // One network stride from (sg->x_prev, sg->x_cur) into sg->x_next for the rollout.
 // now[0..3] / before[0..3]: largest overlap fraction, kinetic energy, potential energy and
 // total mass of the new state (velocity (next - cur)/T) and of the current one.
@@ -836,6 +967,7 @@ int net_stride(dem_surrogate *sg, int n, double T, double now[4], double before[
     SG(build_graph(sg, n, nullptr, 1, false, &ne));
     SG(forward(sg, n, ne, false));
     k_integrate<<<kGS, kTB, 0, s>>>(n, sg->packed, sg->disp, sg->out, sg->prm.sigma_a, sg->fc, sg->x_cur, sg->x_next);
+    SG(project(sg, n, sg->x_next, sg->x_tmp, sg->rad, sg->mass));
     const double gx = sg->prm.gravity[0], gy = sg->prm.gravity[1];
     k_check<<<kChkBlocks, kTB, 0, s>>>(n, sg->offs, sg->send, sg->x_next, sg->rad, sg->mass, sg->fc, 1.0 / T, gx, gy,
                                        sg->x_cur, sg->part);
@@ -862,7 +994,8 @@ extern "C" int dem_surrogate_create(dem_ctx *ctx, const dem_surrogate_params *pr
     *out = nullptr;
     if (!(prm->radius_graph > 0.0) || prm->steps_per_stride <= 0 || !(prm->dt > 0.0) || !(prm->sigma_d > 0.0) ||
         !(prm->sigma_a > 0.0) || !(prm->r_mean > 0.0) || !(prm->r_std > 0.0) || prm->nwalls < 0 ||
-        prm->nwalls > kSgWalls || prm->max_nodes <= 0 || !(prm->wall_clip > 0.0))
+        prm->nwalls > kSgWalls || prm->max_nodes <= 0 || !(prm->wall_clip > 0.0) || prm->project_iters < 0 ||
+        prm->project_iters > 64 || !(prm->project_allow >= 0.0))
         return ctx_fail(ctx, DEM_ERR_INVALID, "dem_surrogate_create: bad parameters");
     dem_surrogate *sg = new dem_surrogate();
     sg->ctx = ctx;
@@ -896,6 +1029,7 @@ extern "C" int dem_surrogate_create(dem_ctx *ctx, const dem_surrogate_params *pr
         const long kin = kShape[l].kin, nout = kShape[l].nout;
         o += kH * kin + kH + nout * kH + nout;
         b += 2 * (kH * kin) + 2 * (nout * kH);
+        if (is_msg(l)) b += 2L * kH * kH + 2L * 2 * kH * kH;   // W1e^T, W1e, W1ij^T, W1ij
     }
     sg->off[kNL] = o;
     sg->boff[kNL] = b;
@@ -930,8 +1064,8 @@ extern "C" int dem_surrogate_destroy(dem_surrogate *sg) {
     cudaStreamSynchronize(ctx_stream(sg->ctx));
     void *ptrs[] = {sg->w, sg->g, sg->m, sg->v, sg->wb, sg->ctl, sg->perm, sg->scene, sg->packed, sg->disp, sg->offs,
                     sg->bsum, sg->d_total, sg->recv, sg->send, sg->rev, sg->xn, sg->xe, sg->out, sg->dout, sg->dz1,
-                    sg->dyb, sg->dxe, sg->dxn, sg->dh, sg->de, sg->part, sg->d_loss, sg->x_prev, sg->x_cur,
-                    sg->x_next, sg->rad, sg->mass, sg->L.nn, sg->L.idx, sg->B.grid, sg->B.total, sg->B.key,
+                    sg->dyb, sg->dxe, sg->dxn, sg->dh, sg->de, sg->pq, sg->dpq, sg->part, sg->d_loss, sg->x_prev, sg->x_cur,
+                    sg->x_next, sg->x_tmp, sg->rad, sg->mass, sg->L.nn, sg->L.idx, sg->B.grid, sg->B.total, sg->B.key,
                     sg->B.cell_start, sg->B.cell_fill, sg->B.cell_items, sg->B.block_sums, sg->B.bbox};
     for (void *p : ptrs) cudaFree(p);
     for (int k = 0; k < 4; ++k) {
@@ -1021,6 +1155,17 @@ extern "C" int dem_surrogate_predict(dem_surrogate *sg, int n, const double *pos
     SG(forward(sg, n, ne, false));
     cudaStream_t s = ctx_stream(sg->ctx);
     k_integrate<<<kGS, kTB, 0, s>>>(n, sg->packed, sg->disp, sg->out, sg->prm.sigma_a, sg->fc, pos_cur, pos_next);
+    if (sg->prm.project_iters > 0) {
+        double *tmp = nullptr, *w = nullptr;
+        SCK(dmalloc(&tmp, 3 * (size_t)n));
+        SCK(dmalloc(&w, (size_t)n));
+        k_rad3<<<kGS, kTB, 0, s>>>(n, rad, w);   // mass weights of equal-density particles
+        const int st = project(sg, n, pos_next, tmp, rad, w);
+        SCK(cudaStreamSynchronize(s));
+        cudaFree(tmp);
+        cudaFree(w);
+        if (st) return st;
+    }
     SCK(cudaGetLastError());
     SCK(cudaStreamSynchronize(s));
     return DEM_OK;
@@ -1037,8 +1182,10 @@ extern "C" int dem_surrogate_rollout(dem_surrogate *sg, dem_solver *solver, int 
     cudaStream_t s = ctx_stream(sg->ctx);
     if (V.stream != s) return sg_fail(sg, DEM_ERR_INVALID, "dem_surrogate_rollout: solver and surrogate need one context");
     if (sg->roll_n < n) {
-        cudaFree(sg->x_prev); cudaFree(sg->x_cur); cudaFree(sg->x_next); cudaFree(sg->rad); cudaFree(sg->mass);
+        cudaFree(sg->x_prev); cudaFree(sg->x_cur); cudaFree(sg->x_next); cudaFree(sg->x_tmp); cudaFree(sg->rad);
+        cudaFree(sg->mass);
         SCK(dmalloc(&sg->x_prev, 3 * (size_t)n));
+        SCK(dmalloc(&sg->x_tmp, 3 * (size_t)n));
         SCK(dmalloc(&sg->x_cur, 3 * (size_t)n));
         SCK(dmalloc(&sg->x_next, 3 * (size_t)n));
         SCK(dmalloc(&sg->rad, n));

@@ -247,7 +247,8 @@ def dam_break(n=200_000, aspect=None, seed=11, rmin=0.9e-3, rmax=1.1e-3, nsteps=
     hexagonal lattice of pitch 2.25 mm filling a column of width W and height aspect * W
     (aspect ~ U[0.5, 4] unless given) against the left wall x = 0, on the floor y = 0, with
     a right wall far downstream; released at rest under gravity -y.  mu = 0.4, e = 0.5
-    (pp and pw), E = 30 MPa, rho = 2600.  nsteps = 1 s at dt = 4 us."""
+    (pp and pw), E = 30 MPa, rho = 2600.  nsteps = 1 s at dt = 4 us.  Verlet skin 0.4 r_mean:
+    the flow reaches a few m/s, and a thinner skin would rebuild the list every few steps."""
     rng = np.random.default_rng(seed)
     if aspect is None:
         aspect = float(rng.uniform(0.5, 4.0))
@@ -280,10 +281,40 @@ def dam_break(n=200_000, aspect=None, seed=11, rmin=0.9e-3, rmax=1.1e-3, nsteps=
     w.x[2], w.normal[2] = (length, 0.0, 0.0), (-1.0, 0.0, 0.0)      # far wall
     w.E[:], w.nu[:], w.G[:] = DAM["E"], DAM["nu"], DAM["E"] / (2.0 * (1.0 + DAM["nu"]))
     sc = Scenario("dam_break_%d" % n, st, w, _force_params(DAM["cor"], DAM["cor"], DAM["mu"], DAM["mu"], quirks), dt,
-                  nsteps, skin=0.1 * 0.5 * (rmin + rmax), gravity=(0.0, -9.81, 0.0))
+                  nsteps, skin=0.4 * 0.5 * (rmin + rmax), gravity=(0.0, -9.81, 0.0))
     sc.extra = dict(aspect=aspect, column_width=col_w, column_height=nrow * rowh, length=length,
                     r_mean=0.5 * (rmin + rmax), r_std=(rmax - rmin) / math.sqrt(12.0))
     return sc
+
+
+def combine_scenes(scenarios, name="batch"):
+    """Independent scenarios as one batch of scenes (same dt, gravity and walls per scene):
+    particles concatenated in order, scene k owns walls [k*W, (k+1)*W)."""
+    first = scenarios[0]
+    W = first.walls.n
+    mc = max(sc.state.max_cnts for sc in scenarios)
+    n = sum(sc.state.n for sc in scenarios)
+    st = ParticleState.create(n, max_cnts=mc, max_walls=W)
+    walls = WallState.create(W * len(scenarios))
+    scene = np.zeros(n, dtype=np.int32)
+    params, counts, off = [], [], 0
+    for k, sc in enumerate(scenarios):
+        if sc.walls.n != W or sc.dt != first.dt or tuple(sc.gravity) != tuple(first.gravity):
+            raise ValueError("scenes need the same wall count, dt and gravity")
+        c = sc.state.n
+        for f in ("x", "u", "omega", "m", "rho", "rad", "I", "E", "nu", "G"):
+            getattr(st, f)[off:off + c] = getattr(sc.state, f)
+        for f in ("x", "u", "omega", "normal", "E", "nu", "G"):
+            getattr(walls, f)[k * W:(k + 1) * W] = getattr(sc.walls, f)
+        scene[off:off + c] = k
+        p = sc.params
+        params.append((p["cor_pp"], p["cor_pw"], p["mu_pp"], p["mu_pw"]))
+        counts.append(c)
+        off += c
+    out = Scenario(name, st, walls, dict(first.params), first.dt, first.nsteps, delta=first.delta, skin=first.skin,
+                   gravity=first.gravity)
+    out.extra = dict(scene=scene, scene_params=params, walls_per_scene=W, counts=np.asarray(counts))
+    return out
 
 
 def bdem_two_particles():

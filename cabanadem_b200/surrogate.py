@@ -29,8 +29,11 @@ def _p(t):
 
 
 def params_for(sc, sigma_a, max_nodes, max_frames=8, radius_graph=3.0e-3, sigma_d=1.0e-3, wall_clip=5.0e-3,
-               max_overlap=0.05, energy_tol=0.05, steps_per_stride=STRIDE):
-    """Surrogate parameters for a dam_break scenario (walls, radii, gravity, dt from it)."""
+               max_overlap=0.05, energy_tol=0.05, steps_per_stride=STRIDE, nwalls=2, project_iters=6,
+               project_allow=0.01):
+    """Surrogate parameters for a dam_break scenario (radii, gravity, dt from it).  The network
+    sees the first `nwalls` walls (floor and back wall); the far wall of a dam break is placed
+    beyond the runout and left out, so one network serves columns of any length."""
     p = SurrogateParams()
     p.radius_graph = radius_graph
     p.steps_per_stride = steps_per_stride
@@ -39,7 +42,7 @@ def params_for(sc, sigma_a, max_nodes, max_frames=8, radius_graph=3.0e-3, sigma_
     p.sigma_a = sigma_a
     p.r_mean = sc.extra["r_mean"]
     p.r_std = sc.extra["r_std"]
-    nw = sc.walls.n
+    nw = min(sc.walls.n, nwalls)
     if nw > 4:
         raise ValueError("at most 4 walls")
     p.nwalls = nw
@@ -54,6 +57,8 @@ def params_for(sc, sigma_a, max_nodes, max_frames=8, radius_graph=3.0e-3, sigma_
     p.energy_tol = energy_tol
     p.max_nodes = int(max_nodes)
     p.max_frames = int(max_frames)
+    p.project_iters = int(project_iters)
+    p.project_allow = float(project_allow)
     return p
 
 
@@ -63,6 +68,7 @@ class Surrogate:
         h = C.c_void_p()
         check(lib().dem_surrogate_create(ctx.h, C.byref(prm), C.byref(h)), ctx.h, "dem_surrogate_create")
         self.h = h
+        ctx.adopt(self)
         self.stream = torch.cuda.ExternalStream(ctx.stream_ptr())
 
     @property
@@ -112,9 +118,15 @@ class Surrogate:
         return {k: getattr(s, k) for k, _ in s._fields_}
 
     def close(self):
-        if self.h:
+        if self.h and self.ctx.alive:
             lib().dem_surrogate_destroy(self.h)
-            self.h = None
+        self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # ---------------------------------------------------------------------------------------
@@ -207,3 +219,53 @@ def prm_dict(p: SurrogateParams) -> dict:
     return dict(radius_graph=p.radius_graph, sigma_d=p.sigma_d, sigma_a=p.sigma_a, r_mean=p.r_mean, r_std=p.r_std,
                 wall_clip=p.wall_clip,
                 walls=[(tuple(p.wall_x[w]), tuple(p.wall_n[w])) for w in range(p.nwalls)])
+
+
+def load(ctx: api.Context, path: str, sc, max_nodes=None, **kw) -> Surrogate:
+    """A surrogate for scenario `sc` with the weights and feature scales saved by
+    train_surrogate."""
+    import json
+    z = np.load(path)
+    meta = json.loads(str(z["meta"]))
+    prm = params_for(sc, sigma_a=meta["sigma_a"], max_nodes=max_nodes or sc.state.n, max_frames=1,
+                     radius_graph=meta["radius_graph"], sigma_d=meta["sigma_d"], wall_clip=meta["wall_clip"], **kw)
+    sg = Surrogate(ctx, prm)
+    sg.set_params(z["params"])
+    return sg
+
+
+def evaluate(sg: Surrogate, make_scenario, seconds: float, ctx: api.Context) -> dict:
+    """Full DEM rollout vs surrogate rollout (DEM fallback on) from the same initial state:
+    wall-clock of each, fallback statistics, runout front and deposit profile errors."""
+    sc = make_scenario()
+    strides = int(round(seconds / (STRIDE * sc.dt)))
+    a = api.from_scenario(sc, ctx=ctx)
+    ctx.sync()
+    t0 = time.perf_counter()
+    a.run_steps(strides * STRIDE)
+    ctx.sync()
+    t_dem = time.perf_counter() - t0
+    xa = a.particles.get("x")
+    a.close()
+    a.particles.close()
+    b = api.from_scenario(make_scenario(), ctx=ctx)
+    ctx.sync()
+    t0 = time.perf_counter()
+    st = sg.rollout(b, strides, use_network=True)
+    ctx.sync()
+    t_sur = time.perf_counter() - t0
+    xb = b.particles.get("x")
+    b.close()
+    b.particles.close()
+    x0 = sc.state.x
+    fa, fb, f0 = runout_front(xa), runout_front(xb), runout_front(x0)
+    length = sc.extra.get("length", float(max(xa[:, 0].max(), xb[:, 0].max())))
+    ha, hb = pile_profile(xa, sc.state.rad, length), pile_profile(xb, sc.state.rad, length)
+    n = sc.state.n
+    return dict(n=n, seconds=seconds, strides=strides, dem_wall_s=t_dem, surrogate_wall_s=t_sur,
+                speedup=t_dem / t_sur, dem_particle_steps_per_s=n * strides * STRIDE / t_dem,
+                surrogate_particle_steps_per_s=n * strides * STRIDE / t_sur,
+                front_dem=fa, front_surrogate=fb, front_initial=f0,
+                front_error=abs(fb - fa) / fa, runout_error=abs(fb - fa) / max(fa - f0, 1e-30),
+                profile_error=float(np.abs(ha - hb).mean() / max(ha.max(), 1e-30)),
+                max_height_dem=float(ha.max()), max_height_surrogate=float(hb.max()), **st)

@@ -314,6 +314,8 @@ typedef struct {
     double energy_tol;       /* fallback: total energy rose by more than this fraction */
     int max_nodes;           /* capacity (particles per call, all frames together) */
     int max_frames;          /* capacity (independent frames per training batch) */
+    int project_iters;       /* contact projection after a network stride: Jacobi sweeps (0: off) */
+    double project_allow;    /* overlap left by the projection, fraction of the smaller radius */
 } dem_surrogate_params;
 
 typedef struct {
@@ -343,7 +345,9 @@ int dem_surrogate_loss_grad(dem_surrogate *sg, int n, const double *pos_prev, co
 int dem_surrogate_train_step(dem_surrogate *sg, int n, const double *pos_prev, const double *pos_cur,
                              const double *pos_next, const double *rad, const int *frame, int nframes,
                              double noise, unsigned long long seed, double lr, double *loss);
-/* One network stride: pos_next = pos_cur + (pos_cur - pos_prev) + sigma_a * net(...). */
+/* One network stride: pos_next = pos_cur + (pos_cur - pos_prev) + sigma_a * net(...), then
+ * projected out of the walls and, with project_iters > 0, out of overlaps larger than
+ * project_allow (pairs of the graph, mass-weighted Jacobi sweeps). */
 int dem_surrogate_predict(dem_surrogate *sg, int n, const double *pos_prev, const double *pos_cur,
                           const double *rad, const int *frame, int nframes, double *pos_next);
 /* Hybrid rollout of a solver's particles (2D: z untouched) for nstrides strides: each stride

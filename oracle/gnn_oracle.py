@@ -133,6 +133,36 @@ class Net:
         dx = f(dz @ W["w1t"]) if want_dx else None
         return dx, g
 
+    def msg(self, l, e, h, recv, send):
+        """Edge update e + W2 relu(W1e e + P[recv] + Q[send] + b1) + b2 with P = W1i h, Q = W1j h
+        (W1 = [W1e | W1i | W1j]); P and Q are stored in BF16 on the GPU."""
+        W, q, f = self.W[l], self.q, self.f
+        w1 = W["w1t"]
+        P = q(f(h @ w1[:, H:2 * H].T))
+        Q = q(f(h @ w1[:, 2 * H:].T))
+        z = f(f(f(e @ w1[:, :H].T) + W["b1"]) + P[recv] + Q[send])
+        h1 = q(np.maximum(z, 0.0))
+        y = f(f(h1 @ W["w2t"].T) + f(W["b2"] + e))
+        return q(y), h1
+
+    def msg_back(self, l, e, h, h1, dy, recv, send, rev):
+        """-> dE (input latent), dh contribution, grads (BF16 dz, dP, dQ as on the GPU)."""
+        W, q, f = self.W[l], self.q, self.f
+        w1 = W["w1t"]
+        n = h.shape[0]
+        dz = q(f(dy @ W["w2t"]) * (h1 > 0))
+        dE = f(dz @ w1[:, :H])
+        dP = np.zeros((n, H))
+        np.add.at(dP, recv, dz)
+        dQ = np.zeros((n, H))
+        ok = rev >= 0
+        np.add.at(dQ, recv[ok], dz[rev[ok]])
+        dP, dQ = q(f(dP)), q(f(dQ))
+        dh = f(dP @ w1[:, H:2 * H] + dQ @ w1[:, 2 * H:])
+        gw1t = np.concatenate([dz.T @ e, dP.T @ h, dQ.T @ h], axis=1)
+        g = {"w1t": gw1t, "b1": dz.sum(0), "w2t": dy.T @ h1, "b2": dy.sum(0)}
+        return dE, dh, g
+
     def forward(self, xn, xe, recv, send, offs):
         q = self.q
         n = xn.shape[0]
@@ -141,8 +171,7 @@ class Net:
         c["h"][0], c["h1"][ENC_N] = self.mlp(ENC_N, c["xn"])
         c["e"][0], c["h1"][ENC_E] = self.mlp(ENC_E, c["xe"])
         for l in range(3):
-            xm = np.concatenate([c["e"][l], c["h"][l][recv], c["h"][l][send]], axis=1)
-            c["e"][l + 1], c["h1"][MSG(l)] = self.mlp(MSG(l), xm, resid=c["e"][l])
+            c["e"][l + 1], c["h1"][MSG(l)] = self.msg(MSG(l), c["e"][l], c["h"][l], recv, send)
             agg = np.zeros((n, H))
             np.add.at(agg, recv, c["e"][l + 1])
             c["agg"][l] = q(self.f(agg))
@@ -163,14 +192,10 @@ class Net:
             dxn, grads[UPD(l)] = self.mlp_back(UPD(l), xu, c["h1"][UPD(l)], q(dh), True)
             dh = f(dh + dxn[:, :H])
             de = f(de + dxn[recv, H:])
-            xm = np.concatenate([c["e"][l], c["h"][l][recv], c["h"][l][send]], axis=1)
-            dxe, grads[MSG(l)] = self.mlp_back(MSG(l), xm, c["h1"][MSG(l)], q(de), True)
-            de = f(de + dxe[:, :H])
-            acc = np.zeros((n, H))
-            np.add.at(acc, recv, dxe[:, H:2 * H])
-            ok = rev >= 0
-            np.add.at(acc, recv[ok], dxe[rev[ok], 2 * H:])
-            dh = f(dh + acc)
+            dE, dhm, grads[MSG(l)] = self.msg_back(MSG(l), c["e"][l], c["h"][l], c["h1"][MSG(l)], q(de), recv, send,
+                                                   rev)
+            dh = f(dh + dhm)
+            de = f(de + dE)
         _, grads[ENC_E] = self.mlp_back(ENC_E, c["xe"], c["h1"][ENC_E], q(de), False)
         _, grads[ENC_N] = self.mlp_back(ENC_N, c["xn"], c["h1"][ENC_N], q(dh), False)
         return grads

@@ -41,3 +41,40 @@ def test_no_gpu_means_loud_failure():
     from cabanadem_b200 import api
     with pytest.raises(_lib.DemError):
         api.Context(0)
+
+
+def test_closing_a_context_closes_its_objects_first():
+    """Objects created on a context are closed (newest first) when it closes, and closing one
+    afterwards does nothing: no destroy call can reach a freed context."""
+    from cabanadem_b200 import api
+
+    class Ctx(api.Context):
+        def __init__(self):   # no device needed: a context with a fake handle
+            self.h = object()
+            self._children = []
+
+    order = []
+
+    class Obj:
+        def __init__(self, ctx, name):
+            self.ctx, self.name, self.h = ctx, name, True
+            ctx.adopt(self)
+
+        def close(self):
+            if self.h and self.ctx.alive:
+                order.append(self.name)
+            self.h = None
+
+    import cabanadem_b200.api as A
+    ctx = Ctx()
+    a, b = Obj(ctx, "particles"), Obj(ctx, "solver")
+    real = A.lib
+    A.lib = lambda: type("L", (), {"dem_ctx_destroy": staticmethod(lambda h: None)})()
+    try:
+        ctx.close()
+    finally:
+        A.lib = real
+    assert order == ["solver", "particles"]
+    a.close()
+    b.close()
+    assert order == ["solver", "particles"] and not ctx.alive

@@ -40,6 +40,16 @@ def _gather(srcs):
 @pytest.mark.parametrize("kin,nout", nn.SHAPES)
 @pytest.mark.parametrize("rows", [1000, 37, 148 * 128 + 200])
 def test_mlp_forward_backward_matches_torch_fp32(kin, nout, rows):
+    _check_layer(kin, nout, rows, resid_src0=False)
+
+
+@pytest.mark.parametrize("kin", [256, 384])
+def test_residual_from_source0(kin):
+    """The message and update layers add their first input as residual (read from the staged tile)."""
+    _check_layer(kin, 128, 2000, resid_src0=True)
+
+
+def _check_layer(kin, nout, rows, resid_src0):
     dev = torch.device("cuda:0")
     ctx = api.Context(0)
     gen = torch.Generator().manual_seed(kin * 7 + nout + rows)
@@ -49,7 +59,7 @@ def test_mlp_forward_backward_matches_torch_fp32(kin, nout, rows):
         m.b1.copy_(torch.randn(128, generator=gen) * 0.1)
         m.b2.copy_(torch.randn(nout, generator=gen) * 0.1)
         srcs = _sources(kin, rows, gen, dev)
-        resid = torch.randn(rows, nout, generator=gen).to(dev, torch.bfloat16)
+        resid = srcs[0][0] if resid_src0 else torch.randn(rows, nout, generator=gen).to(dev, torch.bfloat16)
         out = torch.empty(rows, nout, device=dev, dtype=torch.bfloat16)
         out32 = torch.empty(rows, nout, device=dev, dtype=torch.float32)
         h1 = torch.empty(rows, 128, device=dev, dtype=torch.bfloat16)
