@@ -456,7 +456,7 @@ __global__ void k_check(int n, const int *offs, const int *send, const double *q
     double ov = 0.0, ek = 0.0, ep = 0.0, ms = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const double xi = q[3 * i], yi = q[3 * i + 1], ri = rad[i];
-        for (int e = offs[i]; e < offs[i + 1]; ++e) {
+        for (int e = offs ? offs[i] : 0; e < (offs ? offs[i + 1] : 0); ++e) {
             const int j = send[e];
             const double dx = q[3 * j] - xi, dy = q[3 * j + 1] - yi;
             const double gap = ri + rad[j] - sqrt(dx * dx + dy * dy);
@@ -1206,23 +1206,32 @@ extern "C" int dem_surrogate_rollout(dem_surrogate *sg, dem_solver *solver, int 
         return DEM_OK;
     };
     bool solver_stale = false;   // the surrogate's state is newer than the solver's
+    double e_floor = 0.0;        // lowest mechanical energy since the last DEM stride
+    bool have_floor = false;
     for (int k = 0; k < nstrides; ++k) {
         if (k == 0 || !use_network) {
             SG(dem_stride());
+            have_floor = false;
             continue;
         }
         double now[4], before[4];
         SG(net_stride(sg, n, T, now, before));
-        // energy residual: the mechanical energy of a dissipative granular flow may not rise by
-        // more than energy_tol x max(kinetic energy, total weight x mean radius)
+        // energy residual: the mechanical energy of a dissipative granular flow does not rise; a
+        // network stride may not lift it above the lowest value since the last DEM stride by
+        // more than energy_tol x (total weight x mean radius), so gains cannot accumulate
         const double g = std::sqrt(sg->prm.gravity[0] * sg->prm.gravity[0] + sg->prm.gravity[1] * sg->prm.gravity[1]);
-        const double escale = std::max(before[1], before[3] * g * sg->prm.r_mean);
-        const double rise = (now[1] + now[2]) - (before[1] + before[2]);
+        const double escale = now[3] * g * sg->prm.r_mean;
+        if (!have_floor) {
+            e_floor = before[1] + before[2];
+            have_floor = true;
+        }
+        const double e_new = now[1] + now[2];
         const bool bad_overlap = !(now[0] <= sg->prm.max_overlap);
-        const bool bad_energy = !(rise <= sg->prm.energy_tol * escale);
+        const bool bad_energy = !(e_new <= e_floor + sg->prm.energy_tol * escale);
         if (!bad_overlap && !bad_energy) {
             std::swap(sg->x_prev, sg->x_cur);   // prev <- cur
             std::swap(sg->x_cur, sg->x_next);   // cur <- next
+            e_floor = std::min(e_floor, e_new);
             st.strides_network += 1;
             st.max_overlap_seen = std::max(st.max_overlap_seen, now[0]);
             solver_stale = true;
@@ -1237,6 +1246,7 @@ extern "C" int dem_surrogate_rollout(dem_surrogate *sg, dem_solver *solver, int 
             solver_stale = false;
         }
         SG(dem_stride());
+        have_floor = false;   // the next network stride starts from this DEM state's energy
     }
     if (solver_stale) {
         k_to_solver<<<kGS, kTB, 0, s>>>(V.P, V.ctl, sg->x_cur, sg->x_prev, 1.0 / T);

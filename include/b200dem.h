@@ -311,7 +311,8 @@ typedef struct {
     double wall_clip;        /* wall distance features saturate at this distance (m) */
     double gravity[3];       /* energy residual */
     double max_overlap;      /* fallback: any overlap above this fraction of the smaller radius */
-    double energy_tol;       /* fallback: total energy rose by more than this fraction */
+    double energy_tol;       /* fallback: mechanical energy above its lowest value since the last
+                              * DEM stride by more than energy_tol x total weight x r_mean */
     int max_nodes;           /* capacity (particles per call, all frames together) */
     int max_frames;          /* capacity (independent frames per training batch) */
     int project_iters;       /* contact projection after a network stride: Jacobi sweeps (0: off) */
