@@ -8,6 +8,17 @@ Verlet skin 0.1 r_mean with rebuild when the displacement bound reaches skin/2
 
   python bench.py [--gpus N --steps K --warmup W] [--precision fp64|mixed]
   python bench.py --impl reference ...   # the reference algorithm on the host cores
+  python bench.py --workload random_box|batched|bonded|dam_break   # the other configurations
+
+The other workloads (one JSON line each, device-timed particle-steps/s):
+  random_box  4,096 r = 1 mm spheres in a 5 cm walled cube, dt 1e-7 (latency-bound size)
+  batched     1,024 independent scenes of log-uniform [2, 8192] spheres fired at their own
+              walls, one launch per step for all scenes, FP32 forces / FP64 state, launch
+              settings from the autotuner
+  bonded      256 x 64 x 8 bonded bar pulled at both ends, FP64
+  dam_break   200,000 quasi-2D disks: full DEM rollout vs the learned surrogate with DEM
+              fallback over the same simulated time (wall-clock of each, runout front and
+              deposit profile errors against DEM)
 
 Prints one JSON line (rank 0).  `value` is device-timed (CUDA events on the library's
 stream, inputs resident in HBM); `e2e` is the same metric through the C ABI with host
@@ -50,6 +61,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=50)
+    ap.add_argument("--workload", default="hcp", choices=["hcp", "random_box", "batched", "bonded", "dam_break"])
+    ap.add_argument("--seconds", type=float, default=0.25, help="dam_break: simulated time of both rollouts")
     return ap.parse_args()
 
 
@@ -184,10 +197,102 @@ def run_reference(args):
     return 0
 
 
+def _timed(ctx, fn):
+    """Device time (ms) of fn() on the library's stream, synchronised on both sides."""
+    import torch
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr())
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    fn()
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def run_other(args):
+    """The configurations other than the headline lattice (single GPU; N > 1 runs replicas)."""
+    ws, rank, local = dist_env()
+    import torch
+    torch.cuda.set_device(local)
+    from cabanadem_b200 import api, autotune, scenarios as S, surrogate as SG
+    from cabanadem_b200._lib import DEM_FP64, DEM_MIXED
+    ctx = api.Context(local)
+    clocks = ClockSampler(local)
+    line = {"metric": METRIC, "unit": METRIC, "n_gpus": ws, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "data": "synthetic"}
+    if args.workload in ("random_box", "batched", "bonded"):
+        if args.workload == "random_box":
+            sc = S.random_box(seed=1 + rank)
+            obj = api.from_scenario(sc, ctx=ctx)
+            n, steps, dtype = sc.state.n, args.steps, "f64"
+            desc = ("random_box_4096: 4096 r=1 mm glass spheres, non-overlapping, 5 cm cube, 6 walls, gravity, "
+                    "dt 1e-7 s, skin 0.1 r")
+            extra = {}
+        elif args.workload == "batched":
+            sc = S.batched_scenes(seed=3 + rank)
+            cfg = autotune.tune(sc, precision=DEM_MIXED, warmup=5, steps=40)
+            sc2 = S.batched_scenes(seed=3 + rank)
+            kw = autotune.apply(sc2, cfg)
+            obj = api.from_scenario(sc2, ctx=ctx, precision=DEM_MIXED, **kw)
+            n, steps, dtype = sc.state.n, args.steps, "f64 state / f32 force"
+            desc = ("batched_1024_scenes: %d spheres in 1024 independent scenes (log-uniform [2,8192] per scene), "
+                    "one plane per scene, e~U[0.3,0.95], mu~U[0.1,0.5], dt 1e-7 s, measured window %d steps"
+                    % (n, steps))
+            extra = {"autotuned": cfg}
+        else:
+            case = S.bonded_bar()
+            obj = api.bonded_from_case(case, ctx=ctx)
+            n, steps, dtype = case["state"].n, args.steps, "f64"
+            desc = ("bonded_bar_256x64x8: %d spheres r=0.5 mm, 6-neighbour bonds within 1.05 d, kn 1e7, kt 4e6, "
+                    "ends pulled at 0.05 m/s, break at 1 %% strain, dt 2e-8 s, measured window %d steps"
+                    % (n, steps))
+            extra = {}
+        obj.run_steps(max(3, args.warmup))
+        clocks.start()
+        ms = _timed(ctx, lambda: obj.run_steps(steps))
+        ck = clocks.stop()
+        if args.workload == "bonded":
+            extra["broken_bonds"] = obj.broken()
+        line.update({"value": ws * n * steps / (ms / 1e3), "steps": steps, "ms_per_step": ms / steps,
+                     "dtype": dtype, "config": {"workload": desc, "parallelism": "replicas" if ws > 1 else "single",
+                                                "l2": "state %s L2" % ("larger than" if n * 330 > 126e6 else
+                                                                       "smaller than (latency-bound size)"), **extra},
+                     "clocks": ck})
+    else:
+        n = 200_000
+        mk = lambda: S.dam_break(n=n, aspect=2.0, seed=101 + rank)
+        weights = os.path.join(ROOT, "cabanadem_b200", "data", "dam_break_surrogate.npz")
+        sg = SG.load(ctx, weights, mk())
+        clocks.start()
+        res = SG.evaluate(sg, mk, args.seconds, ctx)
+        ck = clocks.stop()
+        line.update({"value": ws * res["surrogate_particle_steps_per_s"], "steps": res["strides"] * SG.STRIDE,
+                     "ms_per_step": res["surrogate_wall_s"] * 1e3 / (res["strides"] * SG.STRIDE),
+                     "dtype": "bf16 network (fp32 accumulate) + f64 DEM fallback",
+                     "config": {"workload": "dam_break_200000: quasi-2D disks r~U[0.9,1.1] mm, column aspect 2, "
+                                            "mu 0.4, e 0.5, E 1 GPa, dt 1e-6 s, %.2f s simulated; learned surrogate "
+                                            "(200-step strides) vs plain FP64 DEM" % args.seconds},
+                     "dem_reference": {"value": res["dem_particle_steps_per_s"], "unit": METRIC,
+                                       "wall_s": res["dem_wall_s"]},
+                     "surrogate": {k: res[k] for k in ("speedup", "surrogate_wall_s", "front_error", "runout_error",
+                                                       "profile_error", "strides_network", "strides_dem",
+                                                       "fallback_overlap", "fallback_energy", "max_overlap_seen",
+                                                       "front_dem", "front_surrogate")},
+                     "clocks": ck})
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload != "hcp":
+        return run_other(args)
     ws, rank, local = dist_env()
     import torch
     if ws > 1:

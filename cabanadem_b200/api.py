@@ -425,9 +425,10 @@ class Bonds:
             pass
 
 
-def bonded_from_case(case: dict, ctx: Context | None = None, steps_per_launch=0):
+def bonded_from_case(case: dict, ctx: Context | None = None, steps_per_launch=0, precision=_lib.DEM_FP64):
     """Particles + SolverDEM + Bonds on the device for a scenarios.bonded_bar /
-    bdem_two_particles case (bonds set up)."""
+    bdem_two_particles case (bonds set up).  precision DEM_MIXED keeps the bond
+    force/moment history in FP32 (strain, geometry and integration stay FP64)."""
     st = case["state"]
     p = Particles(st.n, max(st.max_cnts, 1), 0, ctx=ctx)
     p.upload(st)
@@ -435,7 +436,8 @@ def bonded_from_case(case: dict, ctx: Context | None = None, steps_per_launch=0)
         p.set("ext_force", case["ext_force"])
     if case.get("fix_flags") is not None:
         p.set("fix", case["fix_flags"])
-    s = SolverDEM(p, None, Force(1.0, 1.0, 0.0, 0.0), case["dt"], skin=0.0, steps_per_launch=steps_per_launch)
+    s = SolverDEM(p, None, Force(1.0, 1.0, 0.0, 0.0), case["dt"], skin=0.0, steps_per_launch=steps_per_launch,
+                  precision=precision)
     bp = case["bparams"]
     b = Bonds(s, case["bonds"].max_bonds, quirks=bp["quirks"], beta=bp["beta"], radius_factor=bp["radius_factor"],
               kn=bp["kn"], kt=bp["kt"], break_strain=bp["break_strain"])

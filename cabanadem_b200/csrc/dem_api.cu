@@ -122,6 +122,13 @@ __global__ void k_scatter_d(const double *src, double *dst, int n, int ncomp, in
         dst[(long)k * cap + rank[c]] = src[t];
     }
 }
+__global__ void k_gather_f2d(const float *src, double *dst, int n, int ncomp, int cap, const int *rank) {
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < (long)n * ncomp; t += (long)gridDim.x * blockDim.x) {
+        const int c = (int)(t / ncomp), k = (int)(t % ncomp);
+        dst[t] = (double)src[(long)k * cap + rank[c]];
+    }
+}
+
 __global__ void k_gather_d(const double *src, double *dst, int n, int ncomp, int cap, const int *rank) {
     for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < (long)n * ncomp; t += (long)gridDim.x * blockDim.x) {
         const int c = (int)(t / ncomp), k = (int)(t % ncomp);
@@ -1161,7 +1168,11 @@ extern "C" int dem_bonds_create(dem_solver *s, int max_bonds, const dem_bond_par
     A(dalloc(&B.idx, (size_t)max_bonds * cap));
     A(dalloc(&B.init_len, (size_t)max_bonds * cap));
     A(dalloc(&B.count, cap));
-    A(dalloc(&B.hist, 9 * (size_t)max_bonds * cap));
+    const bool mixed = s->sp.precision == DEM_MIXED;   // FP32 bond force/moment history
+    B.hist = nullptr;
+    B.hist32 = nullptr;
+    if (mixed) A(dalloc(&B.hist32, 9 * (size_t)max_bonds * cap));
+    else A(dalloc(&B.hist, 9 * (size_t)max_bonds * cap));
     A(dalloc(&B.broken, (size_t)max_bonds * cap));
     A(dalloc(&B.E, cap));
     A(dalloc(&B.G, cap));
@@ -1174,7 +1185,8 @@ extern "C" int dem_bonds_create(dem_solver *s, int max_bonds, const dem_bond_par
     k_fill_i<<<kGS, kTB, 0, st>>>(B.idx, (long)max_bonds * cap, -1);
     cudaMemsetAsync(B.init_len, 0, sizeof(double) * max_bonds * (size_t)cap, st);
     cudaMemsetAsync(B.count, 0, sizeof(int) * cap, st);
-    cudaMemsetAsync(B.hist, 0, sizeof(double) * 9 * max_bonds * (size_t)cap, st);
+    if (B.hist) cudaMemsetAsync(B.hist, 0, sizeof(double) * 9 * max_bonds * (size_t)cap, st);
+    if (B.hist32) cudaMemsetAsync(B.hist32, 0, sizeof(float) * 9 * max_bonds * (size_t)cap, st);
     cudaMemsetAsync(B.broken, 0, (size_t)max_bonds * cap, st);
     b->bc.quirks = bp->quirks;
     b->bc.beta = bp->beta;
@@ -1193,7 +1205,7 @@ extern "C" int dem_bonds_destroy(dem_bonds *b) {
     cudaStreamSynchronize(b->s->ctx->stream);
     if (b->graph) cudaGraphExecDestroy(b->graph);
     Bonds &B = b->B;
-    cudaFree(B.idx); cudaFree(B.init_len); cudaFree(B.count); cudaFree(B.hist); cudaFree(B.broken);
+    cudaFree(B.idx); cudaFree(B.init_len); cudaFree(B.count); cudaFree(B.hist); cudaFree(B.hist32); cudaFree(B.broken);
     cudaFree(B.E); cudaFree(B.G); cudaFree(b->d_count);
     delete b;
     return DEM_OK;
@@ -1252,8 +1264,12 @@ extern "C" int dem_bonds_get(dem_bonds *b, int field, void *host, long count) {
         case DEM_B_COUNT: k_gather_i<<<kGS, kTB, 0, st>>>(B.count, (int *)tmp, n, 1, P.cap, P.rank, P.perm, 0); break;
         case DEM_B_BROKEN: k_gather_u8n<<<kGS, kTB, 0, st>>>(B.broken, (uint8_t *)tmp, n, mb, P.cap, P.rank); break;
         default:
-            k_gather_d<<<kGS, kTB, 0, st>>>(B.hist + (long)(field - DEM_B_FT_X) * mb * P.cap, (double *)tmp, n, mb,
-                                           P.cap, P.rank);
+            if (B.hist32)
+                k_gather_f2d<<<kGS, kTB, 0, st>>>(B.hist32 + (long)(field - DEM_B_FT_X) * mb * P.cap, (double *)tmp, n,
+                                                  mb, P.cap, P.rank);
+            else
+                k_gather_d<<<kGS, kTB, 0, st>>>(B.hist + (long)(field - DEM_B_FT_X) * mb * P.cap, (double *)tmp, n, mb,
+                                               P.cap, P.rank);
     }
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(host, tmp, (size_t)per * es, cudaMemcpyDeviceToHost, st);

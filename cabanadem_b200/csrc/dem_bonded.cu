@@ -50,7 +50,20 @@ __global__ void k_bond_setup(Particles P, NbrList L, Bonds B, Ctl *ctl, double f
     if (status) atomicOr(&ctl->status, status);
 }
 
+// R = double: the reference's FP64 arithmetic (bitwise parity with the oracle).  R = float
+// (mixed precision): strain, geometry and relative kinematics stay FP64 (rij - L0 and the
+// breakage test are exact), the bond force/moment history is stored and updated in FP32
+// (half the history traffic), per-particle sums and integration are FP64.
+template <typename R>
+__device__ __forceinline__ R *bond_hist(const Bonds &B);
+template <>
+__device__ __forceinline__ double *bond_hist<double>(const Bonds &B) { return B.hist; }
+template <>
+__device__ __forceinline__ float *bond_hist<float>(const Bonds &B) { return B.hist32; }
+
+template <typename R>
 __global__ void __launch_bounds__(kBondBlock) k_bond_step(Particles P, Bonds B, Ctl *ctl, ForceConsts fc, BondConsts bc) {
+    R *__restrict__ hist = bond_hist<R>(B);
     const CtlSnap cs_ = read_ctl(ctl, true);
     if (!cs_.go) return;
     const int cur = cs_.cur, nxt = cur ^ 1, vcur = ctl->vcur;
@@ -141,82 +154,81 @@ __global__ void __launch_bounds__(kBondBlock) k_bond_step(Particles P, Bonds B, 
             }
             // normal bond force (:205-222)
             const double overlap_n = rij - L0;
-            const double fn0 = -k_n_bond * overlap_n * n0;
-            const double fn1 = -k_n_bond * overlap_n * n1;
-            const double fn2 = -k_n_bond * overlap_n * n2;
-            double mX = (vn0 >= 0.0) ? 1.0 : -1.0;
-            double mY = (vn1 >= 0.0) ? 1.0 : -1.0;
-            double mZ = (vn2 >= 0.0) ? 1.0 : -1.0;
-            const double fd0 = fn0 + beta_bond * fabs(fn0) * mX;
-            const double fd1 = fn1 + beta_bond * fabs(fn1) * mY;
-            const double fd2 = fn2 + beta_bond * fabs(fn2) * mZ;
+            const R rn0 = (R)n0, rn1 = (R)n1, rn2 = (R)n2;
+            const R fn0 = -(R)k_n_bond * (R)overlap_n * rn0;
+            const R fn1 = -(R)k_n_bond * (R)overlap_n * rn1;
+            const R fn2 = -(R)k_n_bond * (R)overlap_n * rn2;
+            const R beta_b = (R)beta_bond;
+            R mX = (vn0 >= 0.0) ? (R)1 : (R)-1;
+            R mY = (vn1 >= 0.0) ? (R)1 : (R)-1;
+            R mZ = (vn2 >= 0.0) ? (R)1 : (R)-1;
+            const R fd0 = fn0 + beta_b * fabs(fn0) * mX;
+            const R fd1 = fn1 + beta_b * fabs(fn1) * mY;
+            const R fd2 = fn2 + beta_b * fabs(fn2) * mZ;
             // tangential bond force (:231-260)
-            double ft0 = B.hist[(0L * B.mb) * cap + hs], ft1 = B.hist[(1L * B.mb) * cap + hs],
-                   ft2 = B.hist[(2L * B.mb) * cap + hs];
-            const double fdp = ft0 * n0 + ft1 * n1 + ft2 * n2;
-            ft0 -= fdp * n0;
-            ft1 -= fdp * n1;
-            ft2 -= fdp * n2;
-            double tmp = k_t_bond * fc.dt;
-            ft0 += -vt0 * tmp;
-            ft1 += -vt1 * tmp;
-            ft2 += -vt2 * tmp;
-            mX = (vt0 >= 0.0) ? 1.0 : -1.0;
-            mY = (vt1 >= 0.0) ? 1.0 : -1.0;
-            mZ = (vt2 >= 0.0) ? 1.0 : -1.0;
-            const double ftd0 = ft0 - beta_bond * fabs(ft0) * mX;
-            const double ftd1 = ft1 - beta_bond * fabs(ft1) * mY;
-            const double ftd2 = ft2 - beta_bond * fabs(ft2) * mZ;
-            B.hist[(0L * B.mb) * cap + hs] = ftd0;
-            B.hist[(1L * B.mb) * cap + hs] = ftd1;
-            B.hist[(2L * B.mb) * cap + hs] = ftd2;
+            R ft0 = hist[(0L * B.mb) * cap + hs], ft1 = hist[(1L * B.mb) * cap + hs], ft2 = hist[(2L * B.mb) * cap + hs];
+            const R fdp = ft0 * rn0 + ft1 * rn1 + ft2 * rn2;
+            ft0 -= fdp * rn0;
+            ft1 -= fdp * rn1;
+            ft2 -= fdp * rn2;
+            R tmp = (R)k_t_bond * (R)fc.dt;
+            ft0 += -(R)vt0 * tmp;
+            ft1 += -(R)vt1 * tmp;
+            ft2 += -(R)vt2 * tmp;
+            mX = (vt0 >= 0.0) ? (R)1 : (R)-1;
+            mY = (vt1 >= 0.0) ? (R)1 : (R)-1;
+            mZ = (vt2 >= 0.0) ? (R)1 : (R)-1;
+            const R ftd0 = ft0 - beta_b * fabs(ft0) * mX;
+            const R ftd1 = ft1 - beta_b * fabs(ft1) * mY;
+            const R ftd2 = ft2 - beta_b * fabs(ft2) * mZ;
+            hist[(0L * B.mb) * cap + hs] = ftd0;
+            hist[(1L * B.mb) * cap + hs] = ftd1;
+            hist[(2L * B.mb) * cap + hs] = ftd2;
             // twisting moment (:267-291)
-            double tn0 = B.hist[(3L * B.mb) * cap + hs], tn1 = B.hist[(4L * B.mb) * cap + hs],
-                   tn2 = B.hist[(5L * B.mb) * cap + hs];
-            double tdp = tn0 * n0 + tn1 * n1 + tn2 * n2;
-            tn0 = tdp * n0;
-            tn1 = tdp * n1;
-            tn2 = tdp * n2;
-            tmp = k_tor_bond * fc.dt;
-            tn0 += -wn0 * tmp;
-            tn1 += -wn1 * tmp;
-            tn2 += -wn2 * tmp;
-            mX = (wn0 >= 0.0) ? 1.0 : -1.0;
-            mY = (wn1 >= 0.0) ? 1.0 : -1.0;
-            mZ = (wn2 >= 0.0) ? 1.0 : -1.0;
-            const double nd0 = tn0 - beta_bond * fabs(tn0) * mX;
-            const double nd1 = tn1 - beta_bond * fabs(tn1) * mY;
-            const double nd2 = tn2 - beta_bond * fabs(tn2) * mZ;
-            B.hist[(3L * B.mb) * cap + hs] = nd0;
-            B.hist[(4L * B.mb) * cap + hs] = nd1;
-            B.hist[(5L * B.mb) * cap + hs] = nd2;
+            R tn0 = hist[(3L * B.mb) * cap + hs], tn1 = hist[(4L * B.mb) * cap + hs], tn2 = hist[(5L * B.mb) * cap + hs];
+            R tdp = tn0 * rn0 + tn1 * rn1 + tn2 * rn2;
+            tn0 = tdp * rn0;
+            tn1 = tdp * rn1;
+            tn2 = tdp * rn2;
+            tmp = (R)k_tor_bond * (R)fc.dt;
+            tn0 += -(R)wn0 * tmp;
+            tn1 += -(R)wn1 * tmp;
+            tn2 += -(R)wn2 * tmp;
+            mX = (wn0 >= 0.0) ? (R)1 : (R)-1;
+            mY = (wn1 >= 0.0) ? (R)1 : (R)-1;
+            mZ = (wn2 >= 0.0) ? (R)1 : (R)-1;
+            const R nd0 = tn0 - beta_b * fabs(tn0) * mX;
+            const R nd1 = tn1 - beta_b * fabs(tn1) * mY;
+            const R nd2 = tn2 - beta_b * fabs(tn2) * mZ;
+            hist[(3L * B.mb) * cap + hs] = nd0;
+            hist[(4L * B.mb) * cap + hs] = nd1;
+            hist[(5L * B.mb) * cap + hs] = nd2;
             // bending moment (:298-322)
-            double tt0 = B.hist[(6L * B.mb) * cap + hs], tt1 = B.hist[(7L * B.mb) * cap + hs],
-                   tt2 = B.hist[(8L * B.mb) * cap + hs];
-            tdp = tt0 * n0 + tt1 * n1 + tt2 * n2;
-            tt0 -= tdp * n0;
-            tt1 -= tdp * n1;
-            tt2 -= tdp * n2;
-            tmp = k_ben_bond * fc.dt;
-            tt0 += -wt0 * tmp;
-            tt1 += -wt1 * tmp;
-            tt2 += -wt2 * tmp;
-            mX = (wt0 >= 0.0) ? 1.0 : -1.0;
-            mY = (wt1 >= 0.0) ? 1.0 : -1.0;
-            mZ = (wt2 >= 0.0) ? 1.0 : -1.0;
-            const double td0 = tt0 - beta_bond * fabs(tt0) * mX;
-            const double td1 = tt1 - beta_bond * fabs(tt1) * mY;
-            const double td2 = tt2 - beta_bond * fabs(tt2) * mZ;
-            B.hist[(6L * B.mb) * cap + hs] = td0;
-            B.hist[(7L * B.mb) * cap + hs] = td1;
-            B.hist[(8L * B.mb) * cap + hs] = td2;
+            R tt0 = hist[(6L * B.mb) * cap + hs], tt1 = hist[(7L * B.mb) * cap + hs], tt2 = hist[(8L * B.mb) * cap + hs];
+            tdp = tt0 * rn0 + tt1 * rn1 + tt2 * rn2;
+            tt0 -= tdp * rn0;
+            tt1 -= tdp * rn1;
+            tt2 -= tdp * rn2;
+            tmp = (R)k_ben_bond * (R)fc.dt;
+            tt0 += -(R)wt0 * tmp;
+            tt1 += -(R)wt1 * tmp;
+            tt2 += -(R)wt2 * tmp;
+            mX = (wt0 >= 0.0) ? (R)1 : (R)-1;
+            mY = (wt1 >= 0.0) ? (R)1 : (R)-1;
+            mZ = (wt2 >= 0.0) ? (R)1 : (R)-1;
+            const R td0 = tt0 - beta_b * fabs(tt0) * mX;
+            const R td1 = tt1 - beta_b * fabs(tt1) * mY;
+            const R td2 = tt2 - beta_b * fabs(tt2) * mZ;
+            hist[(6L * B.mb) * cap + hs] = td0;
+            hist[(7L * B.mb) * cap + hs] = td1;
+            hist[(8L * B.mb) * cap + hs] = td2;
             const double cri = rij * 1. / pi.w * 1. / (pi.w + pj.w);
-            F0 += fd0 + ftd0;
-            F1 += fd1 + ftd1;
-            F2 += fd2 + ftd2;
-            T0 += nd0 + td0 - cri * 0.0;
-            T1 += nd1 + td1 - cri * 0.0;
-            T2 += nd2 + td2 - cri * 0.0;
+            F0 += (double)(fd0 + ftd0);
+            F1 += (double)(fd1 + ftd1);
+            F2 += (double)(fd2 + ftd2);
+            T0 += (double)(nd0 + td0) - cri * 0.0;
+            T1 += (double)(nd1 + td1) - cri * 0.0;
+            T2 += (double)(nd2 + td2) - cri * 0.0;
         }
         if (fc.has_gravity) {
             F0 += mIi.x * fc.g[0];
@@ -283,7 +295,10 @@ void launch_bond_setup(const Particles &P, const NbrList &L, const Bonds &B, Ctl
 
 void launch_bond_step(const Particles &P, const Bonds &B, Ctl *ctl, const ForceConsts &fc, const BondConsts &bc,
                       cudaStream_t s) {
-    k_bond_step<<<(P.n + kBondBlock - 1) / kBondBlock, kBondBlock, 0, s>>>(P, B, ctl, fc, bc);
+    if (B.hist32)
+        k_bond_step<float><<<(P.n + kBondBlock - 1) / kBondBlock, kBondBlock, 0, s>>>(P, B, ctl, fc, bc);
+    else
+        k_bond_step<double><<<(P.n + kBondBlock - 1) / kBondBlock, kBondBlock, 0, s>>>(P, B, ctl, fc, bc);
 }
 
 void launch_bond_broken_count(const Bonds &B, int n, unsigned long long *out, cudaStream_t s) {

@@ -140,7 +140,8 @@ struct Bonds {
     int *idx;          // [mb][cap] partner (sorted index), -1 empty
     double *init_len;  // [mb][cap]
     int *count;        // [cap]
-    double *hist;      // [9][mb][cap]: ft x|y|z, mn x|y|z, mt x|y|z
+    double *hist;      // [9][mb][cap]: ft x|y|z, mn x|y|z, mt x|y|z (FP64 solvers)
+    float *hist32;     // the same in FP32 (mixed-precision solvers; hist is then unused)
     uint8_t *broken;   // [mb][cap]
     double *E, *G;     // [cap] per-particle moduli (sorted order)
 };
