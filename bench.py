@@ -73,6 +73,19 @@ def dist_env():
     return ws, rank, local
 
 
+def max_over_ranks(x: float) -> float:
+    """The largest value of x over all ranks (the job's time is its slowest rank's); x on a
+    single rank.  Works with the nccl (GPU tensor) and gloo (CPU tensor) backends."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def hbm_peak():
     try:
         with open(PEAKS_FILE) as f:
@@ -331,10 +344,7 @@ def main():
     ck = clocks.stop()
     ms = e0.elapsed_time(e1)
     stats1 = solver.stats()
-    if ws > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms)
     n = args.n
     value = ws * n * args.steps / (ms / 1e3)
 
@@ -370,10 +380,7 @@ def main():
     e2e_ms = a0.elapsed_time(a1)
     wall_ms = (time.perf_counter() - t0) * 1e3
     d2h = sum(v.nbytes for v in out.values())
-    if ws > 1:
-        t = torch.tensor([e2e_ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e2e_ms)
     e2e = {"value": ws * n * args.steps / (e2e_ms / 1e3), "unit": METRIC,
            "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
            "wall_ms": round(wall_ms, 2)}
