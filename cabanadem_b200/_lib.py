@@ -129,6 +129,8 @@ _PROTOS = {
                              _VP, _VP, _VP], C.c_int),
     "dem_nn_status": ([_VP, C.POINTER(C.c_int)], C.c_int),
     "dem_particles_get_device": ([_VP, C.c_int, _VP, C.c_long], C.c_int),
+    "dem_checkpoint_save": ([_VP, C.c_char_p], C.c_int),
+    "dem_checkpoint_load": ([_VP, C.c_char_p], C.c_int),
     "dem_surrogate_create": ([_VP, C.POINTER(SurrogateParams), C.POINTER(_VP)], C.c_int),
     "dem_surrogate_destroy": ([_VP], C.c_int),
     "dem_surrogate_num_params": ([_VP], C.c_long),

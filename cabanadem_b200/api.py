@@ -128,6 +128,14 @@ class Particles:
         check(lib().dem_particles_get_device(self.h, F[field], C.c_void_p(out.data_ptr()), out.numel()), self.ctx.h,
               "get_device " + field)
 
+    def save(self, path: str):
+        """Checkpoint every field (caller order) to `path` (dem_checkpoint_save)."""
+        check(lib().dem_checkpoint_save(self.h, str(path).encode()), self.ctx.h, "dem_checkpoint_save")
+
+    def load(self, path: str):
+        """Restore a checkpoint written by save() (same n, MaxCnts, MaxNoWalls)."""
+        check(lib().dem_checkpoint_load(self.h, str(path).encode()), self.ctx.h, "dem_checkpoint_load")
+
     def upload(self, s: ParticleState):
         for f in ("rad", "x", "u", "omega", "force", "torque", "m", "I", "rho", "E", "nu", "G",
                   "tng_idx", "tng_ss_x", "tng_ss_y", "tng_ss_z", "tng_count"):

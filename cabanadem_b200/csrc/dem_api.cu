@@ -1423,3 +1423,79 @@ int ctx_nn_scratch(dem_ctx *ctx, long part_floats, int **err, float **part) {
     return st;
 }
 }  // namespace b200dem
+
+// ---- checkpoint: every particle field in caller order ---------------------------------
+// File: "B200DEMC", u32 version 1, i32 n, MaxCnts, MaxNoWalls, i32 field count, then per
+// field i32 id, i64 bytes, data.  Fields that were never set (external force, scene) are
+// left out.
+extern "C" int dem_checkpoint_save(dem_particles *p, const char *path) {
+    if (!p || !path) return DEM_ERR_INVALID;
+    dem_ctx *ctx = p->ctx;
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return fail(ctx, DEM_ERR_INVALID, std::string("dem_checkpoint_save: cannot open ") + path);
+    std::vector<int> fields;
+    for (int fld = 0; fld < DEM_F_COUNT_; ++fld) {
+        if (fld == DEM_F_EXT_FORCE && !p->P.ext) continue;
+        if (fld == DEM_F_SCENE && !p->P.scene) continue;
+        fields.push_back(fld);
+    }
+    const uint32_t version = 1;
+    const int hdr[4] = {p->P.n, p->P.mc, p->P.mw, (int)fields.size()};
+    bool ok = std::fwrite("B200DEMC", 1, 8, f) == 8 && std::fwrite(&version, 4, 1, f) == 1 &&
+              std::fwrite(hdr, 4, 4, f) == 4;
+    std::vector<unsigned char> buf;
+    for (int fld : fields) {
+        if (!ok) break;
+        long count;
+        int es;
+        field_layout(p, fld, &count, &es);
+        buf.resize((size_t)count * es);
+        const int st = dem_particles_get(p, fld, buf.data(), count);
+        if (st) {
+            std::fclose(f);
+            return st;
+        }
+        const long long bytes = (long long)buf.size();
+        ok = std::fwrite(&fld, 4, 1, f) == 1 && std::fwrite(&bytes, 8, 1, f) == 1 &&
+             std::fwrite(buf.data(), 1, buf.size(), f) == buf.size();
+    }
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? DEM_OK : fail(ctx, DEM_ERR_INVALID, "dem_checkpoint_save: write failed");
+}
+
+extern "C" int dem_checkpoint_load(dem_particles *p, const char *path) {
+    if (!p || !path) return DEM_ERR_INVALID;
+    dem_ctx *ctx = p->ctx;
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return fail(ctx, DEM_ERR_INVALID, std::string("dem_checkpoint_load: cannot open ") + path);
+    char magic[8];
+    uint32_t version = 0;
+    int hdr[4];
+    auto bad = [&](const char *why) {
+        std::fclose(f);
+        return fail(ctx, DEM_ERR_INVALID, std::string("dem_checkpoint_load: ") + why);
+    };
+    if (std::fread(magic, 1, 8, f) != 8 || std::memcmp(magic, "B200DEMC", 8) != 0) return bad("not a checkpoint");
+    if (std::fread(&version, 4, 1, f) != 1 || version != 1) return bad("unknown version");
+    if (std::fread(hdr, 4, 4, f) != 4) return bad("truncated header");
+    if (hdr[0] != p->P.n || hdr[1] != p->P.mc || hdr[2] != p->P.mw)
+        return bad("particle count, MaxCnts or MaxNoWalls differ from the particles object");
+    std::vector<unsigned char> buf;
+    for (int k = 0; k < hdr[3]; ++k) {
+        int fld;
+        long long bytes;
+        if (std::fread(&fld, 4, 1, f) != 1 || std::fread(&bytes, 8, 1, f) != 1) return bad("truncated field header");
+        long count;
+        int es;
+        if (!field_layout(p, fld, &count, &es) || bytes != (long long)count * es) return bad("field size mismatch");
+        buf.resize((size_t)bytes);
+        if (std::fread(buf.data(), 1, buf.size(), f) != buf.size()) return bad("truncated field");
+        const int st = dem_particles_set(p, fld, buf.data(), count);
+        if (st) {
+            std::fclose(f);
+            return st;
+        }
+    }
+    std::fclose(f);
+    return DEM_OK;
+}

@@ -248,6 +248,12 @@ int dem_bonded_run(dem_bonds *b, int nsteps);
 int dem_neighbor_list_noalloc(const double *x, const double *rad, int n, double delta, double skin,
                               int max_neighbors, int *nn, int *idx, void *stream);
 
+/* Checkpoint of every particle field (caller order) to a file and back; the neighbour list
+ * is rebuilt after a load, so a restarted run continues bit for bit.  The particles object
+ * given to load must have the same n, MaxCnts and MaxNoWalls. */
+int dem_checkpoint_save(dem_particles *p, const char *path);
+int dem_checkpoint_load(dem_particles *p, const char *path);
+
 /* Energy totals (no reference counterpart): out[0] translational kinetic, out[1]
  * rotational kinetic, out[2] Hertz elastic energy of pp contacts, out[3] of wall
  * contacts.  Fixed-order reduction, so repeated calls are bitwise identical. */

@@ -186,3 +186,20 @@ def test_hcp_full_size_one_step_bitwise():
     ref, _ = _oracle(sc, 2)
     _, got = _gpu_run(sc, 2, False)
     _assert_bitwise(got, ref, fields=STATE_F + ("tng_count",), where="hcp")
+
+
+def test_checkpoint_restart_continues_bitwise(tmp_path):
+    """Save after 300 steps, load into fresh particles, continue 300 more: identical to the
+    uninterrupted run (the list is rebuilt, sums run in caller order)."""
+    sc = S.random_box(n=1024, seed=5)
+    a = api.from_scenario(sc)
+    a.run_steps(300)
+    path = tmp_path / "state.b200dem"
+    a.particles.save(path)
+    a.run_steps(300)
+    b = api.from_scenario(S.random_box(n=1024, seed=5))
+    b.particles.load(path)
+    b.run_steps(300)
+    sa, sb = a.particles.download(), b.particles.download()
+    for f in ("x", "u", "omega", "force", "torque", "tng_idx", "tng_count", "tng_ss_x", "tng_sw_y"):
+        assert np.array_equal(getattr(sa, f), getattr(sb, f)), f
