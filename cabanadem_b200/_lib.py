@@ -54,7 +54,7 @@ BFIELD = {name: k for k, name in enumerate(
 class RunStats(C.Structure):
     _fields_ = [("steps", C.c_long), ("rebuilds", C.c_long), ("max_neighbors", C.c_int),
                 ("neighbor_capacity", C.c_int), ("status", C.c_int), ("disp_bound", C.c_double),
-                ("launches", C.c_long)]
+                ("launches", C.c_long), ("graph_ms", C.c_double), ("graph_steps", C.c_long)]
 
 
 class NnRows(C.Structure):

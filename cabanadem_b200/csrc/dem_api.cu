@@ -76,6 +76,10 @@ struct dem_solver {
     long version = 0;   // bumps when anything baked into the graph changes
     long launches = 0;  // kernels launched (graph nodes counted per replay)
     long graph_nodes = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;   // around each step-graph replay
+    double graph_ms = 0.0;                      // device time of the replays
+    long graph_steps_run = 0;                   // steps those replays advanced
+    int graph_done_mark = 0;                    // steps_done before the current replay
 };
 
 struct dem_bonds {
@@ -175,18 +179,13 @@ __global__ void k_gather_pos(const double4 *pos, double *dst, int n, const int *
         }
     }
 }
-__global__ void k_scatter_mI(const double *src, double2 *mI, int n, const int *rank, int which) {
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
-        double2 &v = mI[rank[c]];
-        if (which) v.y = src[c];
-        else v.x = src[c];
-    }
+__global__ void k_scatter_mI(const double *src, double *mI, int n, int cap, const int *rank, int which) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+        mI[(long)which * cap + rank[c]] = src[c];
 }
-__global__ void k_gather_mI(const double2 *mI, double *dst, int n, const int *rank, int which) {
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
-        const double2 v = mI[rank[c]];
-        dst[c] = which ? v.y : v.x;
-    }
+__global__ void k_gather_mI(const double *mI, double *dst, int n, int cap, const int *rank, int which) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+        dst[c] = mI[(long)which * cap + rank[c]];
 }
 __global__ void k_scatter_u8(const uint8_t *src, uint8_t *dst, int n, const int *rank) {
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) dst[rank[c]] = src[c];
@@ -326,7 +325,7 @@ static cudaError_t alloc_particles(Particles &P, int n, int mc, int mw, bool pin
     }
     A(dalloc(&P.force, 3 * cap));
     A(dalloc(&P.torque, 3 * cap));
-    A(dalloc(&P.mI, cap));
+    A(dalloc(&P.mI, 2 * (size_t)cap));
     A(dalloc(&P.mat, cap));
     A(dalloc(&P.cstate, cap));
     A(dalloc(&P.tidx, (size_t)std::max(mc, 1) * cap));
@@ -387,7 +386,7 @@ extern "C" int dem_particles_create(dem_ctx *ctx, int n, int max_contacts, int m
     }
     cudaMemsetAsync(P.force, 0, sizeof(double) * 3 * cn, s);
     cudaMemsetAsync(P.torque, 0, sizeof(double) * 3 * cn, s);
-    cudaMemsetAsync(P.mI, 0, sizeof(double2) * cn, s);
+    cudaMemsetAsync(P.mI, 0, sizeof(double) * 2 * cn, s);
     cudaMemsetAsync(P.mat, 0, cn, s);
     cudaMemsetAsync(P.cstate, 0, sizeof(int) * cn, s);
     cudaMemsetAsync(P.th, 0, sizeof(double) * 3 * std::max(max_contacts, 1) * cn, s);
@@ -458,8 +457,8 @@ extern "C" int dem_particles_set(dem_particles *p, int field, const void *host, 
             }
             k_scatter_d<<<kGS, kTB, 0, s>>>((double *)tmp, P.ext, n, 3, P.cap, P.rank);
             break;
-        case DEM_F_M: k_scatter_mI<<<kGS, kTB, 0, s>>>((double *)tmp, P.mI, n, P.rank, 0); break;
-        case DEM_F_I: k_scatter_mI<<<kGS, kTB, 0, s>>>((double *)tmp, P.mI, n, P.rank, 1); break;
+        case DEM_F_M: k_scatter_mI<<<kGS, kTB, 0, s>>>((double *)tmp, P.mI, n, P.cap, P.rank, 0); break;
+        case DEM_F_I: k_scatter_mI<<<kGS, kTB, 0, s>>>((double *)tmp, P.mI, n, P.cap, P.rank, 1); break;
         case DEM_F_TNG_IDX: k_scatter_i<<<kGS, kTB, 0, s>>>((int *)tmp, P.tidx, n, P.mc, P.cap, P.rank, 1); break;
         case DEM_F_TNG_SS_X: case DEM_F_TNG_SS_Y: case DEM_F_TNG_SS_Z:
             k_scatter_d<<<kGS, kTB, 0, s>>>((double *)tmp, P.th + (long)(field - DEM_F_TNG_SS_X) * P.mc * P.cap, n, P.mc,
@@ -540,8 +539,8 @@ static int particles_get_impl(dem_particles *p, int field, void *host, long coun
         case DEM_F_FORCE: k_gather_d<<<kGS, kTB, 0, s>>>(P.force, (double *)tmp, n, 3, P.cap, P.rank); break;
         case DEM_F_TORQUE: k_gather_d<<<kGS, kTB, 0, s>>>(P.torque, (double *)tmp, n, 3, P.cap, P.rank); break;
         case DEM_F_EXT_FORCE: k_gather_d<<<kGS, kTB, 0, s>>>(P.ext, (double *)tmp, n, 3, P.cap, P.rank); break;
-        case DEM_F_M: k_gather_mI<<<kGS, kTB, 0, s>>>(P.mI, (double *)tmp, n, P.rank, 0); break;
-        case DEM_F_I: k_gather_mI<<<kGS, kTB, 0, s>>>(P.mI, (double *)tmp, n, P.rank, 1); break;
+        case DEM_F_M: k_gather_mI<<<kGS, kTB, 0, s>>>(P.mI, (double *)tmp, n, P.cap, P.rank, 0); break;
+        case DEM_F_I: k_gather_mI<<<kGS, kTB, 0, s>>>(P.mI, (double *)tmp, n, P.cap, P.rank, 1); break;
         case DEM_F_TNG_IDX: k_gather_i<<<kGS, kTB, 0, s>>>(P.tidx, (int *)tmp, n, P.mc, P.cap, P.rank, P.perm, 1); break;
         case DEM_F_TNG_SS_X: case DEM_F_TNG_SS_Y: case DEM_F_TNG_SS_Z:
             k_gather_d<<<kGS, kTB, 0, s>>>(P.th + (long)(field - DEM_F_TNG_SS_X) * P.mc * P.cap, (double *)tmp, n, P.mc,
@@ -890,6 +889,8 @@ extern "C" int dem_solver_destroy(dem_solver *s) {
     if (!s) return DEM_ERR_INVALID;
     cudaStreamSynchronize(s->ctx->stream);
     if (s->graph) cudaGraphExecDestroy(s->graph);
+    if (s->ev0) cudaEventDestroy(s->ev0);
+    if (s->ev1) cudaEventDestroy(s->ev1);
     cudaFree(s->d_pp); cudaFree(s->d_pw); cudaFree(s->d_walls); cudaFree(s->d_scenes);
     cudaFree(s->L.nn); cudaFree(s->L.idx); cudaFree(s->L.defer); cudaFree(s->L.defer_v); cudaFree(s->L.defer_w);
     BuildBuffers &B = s->B;
@@ -920,6 +921,7 @@ extern "C" int dem_solver_run(dem_solver *s, int nsteps) {
     k_run_begin<<<1, 32, 0, st>>>(s->p->ctl, nsteps, half_skin);
     launch_prologue(s->p->P, s->p->ctl, s->fc, st);
     s->launches += 2;
+    s->graph_done_mark = 0;
     CK(cudaGetLastError());
     const int chunk = s->sp.steps_per_launch;
     if (ref_mode(s)) {
@@ -955,15 +957,29 @@ extern "C" int dem_solver_run(dem_solver *s, int nsteps) {
             int e = build_now(s, true);
             if (e) return e;
         }
+        if (!s->ev0) {
+            CK(cudaEventCreate(&s->ev0));
+            CK(cudaEventCreate(&s->ev1));
+        }
         for (int guard = 0;; ++guard) {
             if (!s->graph || s->graph_version != s->version || s->graph_steps != chunk) {
                 int e = capture_graph(s, chunk);
                 if (e) return e;
             }
+            CK(cudaEventRecord(s->ev0, st));
             CK(cudaGraphLaunch(s->graph, st));
+            CK(cudaEventRecord(s->ev1, st));
             s->launches += s->graph_nodes;
+            const int done_before = s->graph_done_mark;
             Ctl c = read_ctl(s);
             CK(cudaGetLastError());
+            {
+                float ms = 0.f;
+                CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+                s->graph_ms += ms;
+                s->graph_steps_run += c.steps_done - done_before;
+                s->graph_done_mark = c.steps_done;
+            }
             if (c.steps_done >= c.target) break;
             if (!(c.disp < c.half_skin)) {
                 int e = build_now(s, true);
@@ -987,6 +1003,8 @@ extern "C" int dem_solver_stats(dem_solver *s, dem_run_stats *out) {
     out->status = c.status;
     out->disp_bound = c.disp;
     out->launches = s->launches;
+    out->graph_ms = s->graph_ms;
+    out->graph_steps = s->graph_steps_run;
     return DEM_OK;
 }
 

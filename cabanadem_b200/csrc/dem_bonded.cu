@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(kBondBlock) k_bond_step(Particles P, Bonds B, 
         const D4 pi = ld4(pc, i);
         double ui0 = vc[i], ui1 = vc[cap + i], ui2 = vc[2 * cap + i];
         double wi0 = wc[i], wi1 = wc[cap + i], wi2 = wc[2 * cap + i];
-        const double2 mIi = P.mI[i];
+        const double2 mIi = load_mI(P, i);
         double F0 = 0., F1 = 0., F2 = 0., T0 = 0., T1 = 0., T2 = 0.;
         if (fc.has_ext) {   // applyTensileForce (tst_01_BDEM:101-111) before the bond pass
             F0 += P.ext[i];

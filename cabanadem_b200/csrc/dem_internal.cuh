@@ -48,7 +48,7 @@ struct Particles {
     double *vel[2];
     double *omg[2];
     double *force, *torque;
-    double2 *mI;
+    double *mI;    // [2][cap]: mass m (row 0) and moment of inertia I (row 1)
     uint8_t *mat;
     int *cstate;
     int *tidx;
@@ -60,6 +60,11 @@ struct Particles {
     unsigned long long *vslots;   // kVmaxSlots x 32 words: per-step max |u|^2, spread over L2 lines
     int *scene;                   // [cap] scene of each particle, null when all share scene 0
 };
+
+// (m, I) of particle i: two rows of one array, so that a kernel needing only m reads 8 bytes.
+__host__ __device__ __forceinline__ double2 load_mI(const Particles &P, int i) {
+    return make_double2(P.mI[i], P.mI[(long)P.cap + i]);
+}
 
 constexpr int kVmaxSlots = 32;   // blocks fold their max into slot blockIdx % 32 (word 32 * slot)
 

@@ -355,6 +355,7 @@ __global__ void k_permute(Particles P, Particles A, const Ctl *ctl, const int *i
             if (P.ext) A.ext[d * cap + p] = P.ext[d * cap + q];
         }
         A.mI[p] = P.mI[q];
+        A.mI[cap + p] = P.mI[cap + q];
         A.mat[p] = P.mat[q];
         if (P.scene) A.scene[p] = P.scene[q];
         A.fix[p] = P.fix[q];
@@ -489,7 +490,7 @@ void launch_build(const Particles &P, Particles &alt, const NbrList &L, BuildBuf
         cudaMemcpyAsync(P.force, alt.force, 3 * cap * sizeof(double), cudaMemcpyDeviceToDevice, s);
         cudaMemcpyAsync(P.torque, alt.torque, 3 * cap * sizeof(double), cudaMemcpyDeviceToDevice, s);
         if (P.ext) cudaMemcpyAsync(P.ext, alt.ext, 3 * cap * sizeof(double), cudaMemcpyDeviceToDevice, s);
-        cudaMemcpyAsync(P.mI, alt.mI, cap * sizeof(double2), cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(P.mI, alt.mI, 2 * cap * sizeof(double), cudaMemcpyDeviceToDevice, s);
         cudaMemcpyAsync(P.mat, alt.mat, cap, cudaMemcpyDeviceToDevice, s);
         cudaMemcpyAsync(P.fix, alt.fix, cap, cudaMemcpyDeviceToDevice, s);
         cudaMemcpyAsync(P.cstate, alt.cstate, cap * sizeof(int), cudaMemcpyDeviceToDevice, s);

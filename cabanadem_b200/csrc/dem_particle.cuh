@@ -91,14 +91,16 @@ __device__ __forceinline__ void vmax_fold(unsigned long long *slots, double m) {
     if (m > 0.0) atomicMax(&slots[(blockIdx.x % kVmaxSlots) * 32], (unsigned long long)__double_as_longlong(m));
 }
 
-// Max over the slots, clearing them for the next step (called by one thread).
-__device__ __forceinline__ double vmax_collect(unsigned long long *slots) {
-    unsigned long long m = 0ull;
-    for (int s = 0; s < kVmaxSlots; ++s) {
-        const unsigned long long v = atomicExch(&slots[s * 32], 0ull);
-        m = v > m ? v : m;
+// Max over the slots, clearing them for the next step: one warp, lane s takes slot s
+// (kVmaxSlots == 32), one round trip.
+__device__ __forceinline__ double vmax_collect_warp(unsigned long long *slots) {
+    const int lane = threadIdx.x & 31;
+    unsigned long long v = atomicExch(&slots[lane * 32], 0ull);
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = w > v ? w : v;
     }
-    return __longlong_as_double((long long)m);
+    return __longlong_as_double((long long)v);
 }
 
 // Block max of |u|^2 folded into its slot, then the last block to finish advances the
@@ -122,19 +124,32 @@ __device__ __forceinline__ void finish_step(Ctl *ctl, unsigned long long *slots,
         am_last = (t == gridDim.x - 1);
     }
     __syncthreads();
-    if (am_last && threadIdx.x == 0) {
+    if (am_last && threadIdx.x < 32) {
         __threadfence();
-        const double v2 = vmax_collect(slots);
-        ctl->disp = ctl->disp + dt * sqrt(v2) * (1.0 + 1e-9);
-        ctl->ndefer = 0;
-        ctl->cur ^= 1;
-        if (flip_v) ctl->vcur ^= 1;
-        if (count_step) {
-            ctl->steps_done += 1;
-            ctl->total_steps += 1;
+        const double v2 = vmax_collect_warp(slots);
+        if (threadIdx.x == 0) {
+            ctl->disp = ctl->disp + dt * sqrt(v2) * (1.0 + 1e-9);
+            ctl->ndefer = 0;
+            ctl->cur ^= 1;
+            if (flip_v) ctl->vcur ^= 1;
+            if (count_step) {
+                ctl->steps_done += 1;
+                ctl->total_steps += 1;
+            }
+            __threadfence();
+            ctl->ticket = 0u;
         }
-        __threadfence();
-        ctl->ticket = 0u;
+    }
+}
+
+// Fold the warp's largest |u|^2 into a slot chosen by the global warp index (and OR its
+// status bits): no block barrier, one atomic per warp spread over the 32 slots.
+__device__ __forceinline__ void warp_vmax(Ctl *ctl, unsigned long long *slots, double vmax2, int status) {
+    for (int o = 16; o > 0; o >>= 1) vmax2 = fmax(vmax2, __shfl_xor_sync(0xffffffffu, vmax2, o));
+    if (status) atomicOr(&ctl->status, status);
+    if ((threadIdx.x & 31) == 0 && vmax2 > 0.0) {
+        const unsigned w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+        atomicMax(&slots[(w % kVmaxSlots) * 32], (unsigned long long)__double_as_longlong(vmax2));
     }
 }
 
@@ -177,10 +192,22 @@ __device__ __forceinline__ void particle_full(const Particles &P, const NbrList 
     const double4 *__restrict__ pc = P.pos[cur];
     const double *__restrict__ vc = P.vel[vcur];
     const double *__restrict__ wc = P.omg[vcur];
+    // Speculative partner prefetch, issued with the particle's own loads: the first two
+    // neighbour-list slots and the first two contact-history slots, then those partners'
+    // positions.  Slots past the list length or count hold stale values; an index outside
+    // [0, n) falls back to i, and a prefetched position is used only while its slot still
+    // holds the same partner, so the arithmetic is that of the plain loop.
+    int lpf0 = L.maxnb > 0 ? ld_early_i(L.idx + i) : i, lpf1 = L.maxnb > 1 ? ld_early_i(L.idx + cap + i) : i;
+    int tpf0 = P.mc > 0 ? ld_early_i(P.tidx + i) : i, tpf1 = P.mc > 1 ? ld_early_i(P.tidx + cap + i) : i;
+    lpf0 = (unsigned)lpf0 < (unsigned)P.n ? lpf0 : i;
+    lpf1 = (unsigned)lpf1 < (unsigned)P.n ? lpf1 : i;
+    tpf0 = (unsigned)tpf0 < (unsigned)P.n ? tpf0 : i;
+    tpf1 = (unsigned)tpf1 < (unsigned)P.n ? tpf1 : i;
+    const D4 lpp0 = ld4(pc, lpf0), lpp1 = ld4(pc, lpf1), tpp0 = ld4(pc, tpf0), tpp1 = ld4(pc, tpf1);
     const D4 pi = ld4(pc, i);
     double ui0 = vc[i], ui1 = vc[cap + i], ui2 = vc[2 * cap + i];
     double wi0 = wc[i], wi1 = wc[cap + i], wi2 = wc[2 * cap + i];
-    const double2 mIi = P.mI[i];
+    const double2 mIi = load_mI(P, i);
     const int mi = fc.nmat > 1 ? (int)P.mat[i] : 0;
     const int cs0 = P.cstate[i];
     int cnt = cs0 & 0xff;
@@ -203,7 +230,7 @@ __device__ __forceinline__ void particle_full(const Particles &P, const NbrList 
         while (count < total) {
             const int sidx = tidx[(long)k * cap];
             if (sidx == -1) break;
-            const D4 pj = ld4(pc, sidx);
+            const D4 pj = (k == 0 && sidx == tpf0) ? tpp0 : (k == 1 && sidx == tpf1) ? tpp1 : ld4(pc, sidx);
             const double px = pi.x - pj.x, py = pi.y - pj.y, pz = pi.z - pj.z;
             const double r2ij = px * px + py * py + pz * pz;
             const double rij = sqrt(r2ij);
@@ -238,7 +265,7 @@ __device__ __forceinline__ void particle_full(const Particles &P, const NbrList 
     const int *__restrict__ lidx = L.idx + i;
     for (int kk = 0; kk < nn; ++kk) {
         const int j = lidx[(long)kk * cap];
-        const D4 pj = ld4(pc, j);
+        const D4 pj = (kk == 0 && j == lpf0) ? lpp0 : (kk == 1 && j == lpf1) ? lpp1 : ld4(pc, j);
         const double px = pi.x - pj.x, py = pi.y - pj.y, pz = pi.z - pj.z;
         const double r2ij = px * px + py * py + pz * pz;
         const double sr = pi.w + pj.w;
@@ -313,7 +340,7 @@ __device__ __forceinline__ void particle_full(const Particles &P, const NbrList 
             const float vdn = (float)dvdn;
             const float vt0 = (float)(dv0 - dvdn * dnx), vt1 = (float)(dv1 - dvdn * dny), vt2 = (float)(dv2 - dvdn * dnz);
             const float R_eff = 1.f / (1.f / ri + 1.f / rj);
-            const float m_eff = 1.f / (1.f / (float)mIi.x + 1.f / (float)P.mI[j].x);
+            const float m_eff = 1.f / (1.f / (float)mIi.x + 1.f / (float)P.mI[j]);
             const float sro = sqrtf(R_eff * ov);
             const float kn = (float)c.c_kn * sqrtf(R_eff);
             const float S_n = (float)c.c_Sn * sro;
@@ -393,7 +420,7 @@ __device__ __forceinline__ void particle_full(const Particles &P, const NbrList 
         const double R_eff = 1. / (tmp_3 + tmp_4);
         const double kn = c.c_kn * sqrt(R_eff);
         const double S_n = c.c_Sn * sqrt(R_eff * overlap);
-        const double m_eff = 1. / (1. / mIi.x + 1. / P.mI[j].x);
+        const double m_eff = 1. / (1. / mIi.x + 1. / P.mI[j]);
         const double eta_n = K_n_pp * sqrt(S_n * m_eff);
         const double kt = c.c_kt * sqrt(R_eff * overlap);
         const double eta_t = K_t_pp * sqrt(kt * m_eff);

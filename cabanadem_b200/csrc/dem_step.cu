@@ -68,7 +68,7 @@ __global__ void __launch_bounds__(BS, MINB) k_stream(Particles P, NbrList L, Ctl
         const D4 pi = ld4_early(pc, i);
         const int cs = ld_early_i(P.cstate + i);
         const int nn = ld_early_i(L.nn + i);
-        const double m = ld_early(&P.mI[i].x);
+        const double m = ld_early(&P.mI[i]);
         double ui0 = ld_early(vc + i), ui1 = ld_early(vc + cap + i), ui2 = ld_early(vc + 2 * cap + i);
         // the first two list slots are read with the own state (in bounds for every i; the
         // value is only used below the list length), so that most warps need one more
@@ -155,7 +155,7 @@ __global__ void __launch_bounds__(BS, MINB) k_stream(Particles P, NbrList L, Ctl
             vc[2 * cap + i] = ui2;
         }
     }
-    block_vmax(ctl, P.vslots, vmax2, 0);
+    warp_vmax(ctl, P.vslots, vmax2, 0);
 }
 
 // Fused step, kernel 2 of 3: the full arithmetic for the deferred particles.  New u and
@@ -184,7 +184,7 @@ __global__ void __launch_bounds__(kBlock) k_contact(Particles P, NbrList L, Ctl 
 // step counter, deferred-list reset).  Each block copies ndefer before its ticket, so the
 // reset cannot cut another block's copy short.
 __global__ void __launch_bounds__(kApplyBlock) k_apply(Particles P, NbrList L, Ctl *ctl, ForceConsts fc) {
-    __shared__ int s_nd, s_go;
+    __shared__ int s_nd, s_go, s_last;
     if (threadIdx.x == 0) {
         s_go = step_gate(ctl);
         s_nd = ctl->ndefer;
@@ -203,9 +203,13 @@ __global__ void __launch_bounds__(kApplyBlock) k_apply(Particles P, NbrList L, C
     if (threadIdx.x == 0) {
         __threadfence();
         const unsigned tk = atomicAdd(&ctl->ticket, 1u);
-        if (tk == gridDim.x - 1) {
-            __threadfence();
-            const double v2 = vmax_collect(P.vslots);
+        s_last = (tk == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (s_last && threadIdx.x < 32) {   // every block has taken its ticket: the slots are quiescent
+        __threadfence();
+        const double v2 = vmax_collect_warp(P.vslots);
+        if (threadIdx.x == 0) {
             ctl->disp = ctl->disp + fc.dt * sqrt(v2) * (1.0 + 1e-9);
             ctl->ndefer = 0;
             ctl->cur ^= 1;
@@ -226,7 +230,7 @@ __global__ void __launch_bounds__(kBlock) k_prologue(Particles P, Ctl *ctl, Forc
     const int cap = P.cap;
     double vmax2 = 0.0;
     if (i < P.n) {
-        const double2 mIi = P.mI[i];
+        const double2 mIi = load_mI(P, i);
         const double m_inverse = 1. / mIi.x, I_inverse = 1. / mIi.y, h = fc.half_dt;
         double *vc = P.vel[vcur], *wc = P.omg[vcur];
         double u[3];
@@ -259,7 +263,7 @@ __global__ void k_stage(Particles P, Ctl *ctl, ForceConsts fc, int stage) {
         st4(P.pos[cur], i, p);
         return;
     }
-    const double2 mIi = P.mI[i];
+    const double2 mIi = load_mI(P, i);
     const double m_inverse = 1. / mIi.x, I_inverse = 1. / mIi.y, h = fc.half_dt;
     for (int d = 0; d < 3; ++d) {
         vc[d * cap + i] += h * P.force[d * cap + i] * m_inverse;
@@ -280,7 +284,7 @@ __global__ void __launch_bounds__(kBlock) k_energy_partials(Particles P, NbrList
     const int cap = P.cap;
     double e[4] = {0., 0., 0., 0.};
     if (i < P.n) {
-        const double2 mIi = P.mI[i];
+        const double2 mIi = load_mI(P, i);
         const double *vc = P.vel[vcur], *wc = P.omg[vcur];
         const double u0 = vc[i], u1 = vc[cap + i], u2 = vc[2 * cap + i];
         const double w0 = wc[i], w1 = wc[cap + i], w2 = wc[2 * cap + i];

@@ -518,7 +518,7 @@ __global__ void k_from_solver(Particles P, const Ctl *ctl, double *x3, double *r
         x3[3 * i + 1] = p.y;
         x3[3 * i + 2] = p.z;
         if (rad) rad[i] = p.w;
-        if (mass) mass[i] = P.mI[s].x;
+        if (mass) mass[i] = P.mI[s];
     }
 }
 // Positions, velocity = displacement / T (in plane), zero spin and no contact history.

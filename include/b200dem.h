@@ -114,6 +114,9 @@ typedef struct dem_run_stats {
     int status;            /* sticky DEM_ERR_* bits seen on the device     */
     double disp_bound;     /* displacement bound since the last build (m)  */
     long launches;         /* kernels launched by this solver (graph nodes counted per replay) */
+    double graph_ms;       /* device time of the step graphs replayed by dem_solver_run (CUDA
+                            * events around each replay; host gaps and rebuilds excluded)  */
+    long graph_steps;      /* fused steps those replays advanced                          */
 } dem_run_stats;
 
 /* ---- context ------------------------------------------------------------------- */
