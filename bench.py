@@ -290,7 +290,7 @@ def run_other(args):
                      "dem_reference": {"value": res["dem_particle_steps_per_s"], "unit": METRIC,
                                        "wall_s": res["dem_wall_s"]},
                      "surrogate": {k: res[k] for k in ("speedup", "surrogate_wall_s", "front_error", "runout_error",
-                                                       "profile_error", "strides_network", "strides_dem",
+                                                       "profile_error", "depth_error", "strides_network", "strides_dem",
                                                        "fallback_overlap", "fallback_energy", "max_overlap_seen",
                                                        "front_dem", "front_surrogate")},
                      "clocks": ck})

@@ -447,13 +447,14 @@ __global__ void k_rad3(int n, const double *rad, double *w) {
 }
 
 // Largest overlap / smaller radius over the graph's pairs at positions q (caller [n][3]) and
-// the walls; kinetic energy 0.5 m |q - p|^2 / T^2, potential -m g.q and the total mass.
-// Block partials, summed in block order.
+// the walls; kinetic energy 0.5 m |q - p|^2 / T^2, potential -m g.q, the total mass and the
+// largest specific energy 0.5 |v|^2 - g.q of one particle.  Block partials, summed in block
+// order.
 constexpr int kChkBlocks = 256;
 __global__ void k_check(int n, const int *offs, const int *send, const double *q, const double *rad, const double *mass,
                         FeatConst fc, double inv_T, double gx, double gy, const double *p, double *part) {
-    __shared__ double s_ov[kTB], s_ek[kTB], s_ep[kTB], s_m[kTB];
-    double ov = 0.0, ek = 0.0, ep = 0.0, ms = 0.0;
+    __shared__ double s_ov[kTB], s_ek[kTB], s_ep[kTB], s_m[kTB], s_es[kTB];
+    double ov = 0.0, ek = 0.0, ep = 0.0, ms = 0.0, es = -1e300;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const double xi = q[3 * i], yi = q[3 * i + 1], ri = rad[i];
         for (int e = offs ? offs[i] : 0; e < (offs ? offs[i + 1] : 0); ++e) {
@@ -470,11 +471,13 @@ __global__ void k_check(int n, const int *offs, const int *send, const double *q
         ek += 0.5 * mass[i] * (vx * vx + vy * vy);
         ep -= mass[i] * (gx * xi + gy * yi);
         ms += mass[i];
+        es = fmax(es, 0.5 * (vx * vx + vy * vy) - (gx * xi + gy * yi));
     }
     s_ov[threadIdx.x] = ov;
     s_ek[threadIdx.x] = ek;
     s_ep[threadIdx.x] = ep;
     s_m[threadIdx.x] = ms;
+    s_es[threadIdx.x] = es;
     __syncthreads();
     for (int o = kTB / 2; o > 0; o >>= 1) {
         if (threadIdx.x < o) {
@@ -482,29 +485,33 @@ __global__ void k_check(int n, const int *offs, const int *send, const double *q
             s_ek[threadIdx.x] += s_ek[threadIdx.x + o];
             s_ep[threadIdx.x] += s_ep[threadIdx.x + o];
             s_m[threadIdx.x] += s_m[threadIdx.x + o];
+            s_es[threadIdx.x] = fmax(s_es[threadIdx.x], s_es[threadIdx.x + o]);
         }
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        part[4 * blockIdx.x] = s_ov[0];
-        part[4 * blockIdx.x + 1] = s_ek[0];
-        part[4 * blockIdx.x + 2] = s_ep[0];
-        part[4 * blockIdx.x + 3] = s_m[0];
+        part[5 * blockIdx.x] = s_ov[0];
+        part[5 * blockIdx.x + 1] = s_ek[0];
+        part[5 * blockIdx.x + 2] = s_ep[0];
+        part[5 * blockIdx.x + 3] = s_m[0];
+        part[5 * blockIdx.x + 4] = s_es[0];
     }
 }
 __global__ void k_check_sum(int nb, const double *part, double *out) {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
-        double ov = 0.0, ek = 0.0, ep = 0.0, ms = 0.0;
+        double ov = 0.0, ek = 0.0, ep = 0.0, ms = 0.0, es = -1e300;
         for (int b = 0; b < nb; ++b) {
-            ov = fmax(ov, part[4 * b]);
-            ek += part[4 * b + 1];
-            ep += part[4 * b + 2];
-            ms += part[4 * b + 3];
+            ov = fmax(ov, part[5 * b]);
+            ek += part[5 * b + 1];
+            ep += part[5 * b + 2];
+            ms += part[5 * b + 3];
+            es = fmax(es, part[5 * b + 4]);
         }
         out[0] = ov;
         out[1] = ek;
         out[2] = ep;
         out[3] = ms;
+        out[4] = es;
     }
 }
 
@@ -679,8 +686,8 @@ int alloc_nodes(dem_surrogate *sg) {
     for (int k = 0; k < 3; ++k) SCK(dmalloc(&sg->agg[k], (size_t)cap * kH));
     SCK(dmalloc(&sg->out, (size_t)cap * kF));
     SCK(dmalloc(&sg->pq, (size_t)cap * 2 * kH));
-    SCK(dmalloc(&sg->part, 4 * (size_t)std::max(kLossBlocks, kChkBlocks)));
-    SCK(dmalloc(&sg->d_loss, 8));
+    SCK(dmalloc(&sg->part, 8 * (size_t)std::max(kLossBlocks, kChkBlocks)));
+    SCK(dmalloc(&sg->d_loss, 16));
     Particles &P = sg->GP;
     P = Particles{};
     P.n = 0;
@@ -958,9 +965,10 @@ int project(dem_surrogate *sg, int n, double *q, double *tmp, const double *rad,
 }
 
 // One network stride from (sg->x_prev, sg->x_cur) into sg->x_next for the rollout.
-// now[0..3] / before[0..3]: largest overlap fraction, kinetic energy, potential energy and
-// total mass of the new state (velocity (next - cur)/T) and of the current one.
-int net_stride(dem_surrogate *sg, int n, double T, double now[4], double before[4]) {
+// now[0..4] / before[0..4]: largest overlap fraction, kinetic energy, potential energy, total
+// mass and largest specific energy of the new state (velocity (next - cur)/T) and of the
+// current one.
+int net_stride(dem_surrogate *sg, int n, double T, double now[5], double before[5]) {
     cudaStream_t s = ctx_stream(sg->ctx);
     SG(prepare_inputs(sg, n, sg->x_prev, sg->x_cur, sg->rad, 0.0, 0));
     long ne = 0;
@@ -974,14 +982,14 @@ int net_stride(dem_surrogate *sg, int n, double T, double now[4], double before[
     k_check_sum<<<1, 32, 0, s>>>(kChkBlocks, sg->part, sg->d_loss);
     k_check<<<kChkBlocks, kTB, 0, s>>>(n, sg->offs, sg->send, sg->x_cur, sg->rad, sg->mass, sg->fc, 1.0 / T, gx, gy,
                                        sg->x_prev, sg->part);
-    k_check_sum<<<1, 32, 0, s>>>(kChkBlocks, sg->part, sg->d_loss + 4);
+    k_check_sum<<<1, 32, 0, s>>>(kChkBlocks, sg->part, sg->d_loss + 5);
     SCK(cudaGetLastError());
-    double v[8];
-    SCK(cudaMemcpyAsync(v, sg->d_loss, 8 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    double v[10];
+    SCK(cudaMemcpyAsync(v, sg->d_loss, 10 * sizeof(double), cudaMemcpyDeviceToHost, s));
     SCK(cudaStreamSynchronize(s));
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < 5; ++k) {
         now[k] = v[k];
-        before[k] = v[4 + k];
+        before[k] = v[5 + k];
     }
     return DEM_OK;
 }
@@ -1207,6 +1215,7 @@ extern "C" int dem_surrogate_rollout(dem_surrogate *sg, dem_solver *solver, int 
     };
     bool solver_stale = false;   // the surrogate's state is newer than the solver's
     double e_floor = 0.0;        // lowest mechanical energy since the last DEM stride
+    double s_floor = 0.0;        // lowest largest-specific-energy since the last DEM stride
     bool have_floor = false;
     for (int k = 0; k < nstrides; ++k) {
         if (k == 0 || !use_network) {
@@ -1214,24 +1223,30 @@ extern "C" int dem_surrogate_rollout(dem_surrogate *sg, dem_solver *solver, int 
             have_floor = false;
             continue;
         }
-        double now[4], before[4];
+        double now[5], before[5];
         SG(net_stride(sg, n, T, now, before));
         // energy residual: the mechanical energy of a dissipative granular flow does not rise; a
         // network stride may not lift it above the lowest value since the last DEM stride by
-        // more than energy_tol x (total weight x mean radius), so gains cannot accumulate
+        // more than energy_tol x (total weight x mean radius), so gains cannot accumulate.  The
+        // same per particle: the largest specific energy (0.5 |v|^2 + lift) may not rise above
+        // its lowest value since the last DEM stride by more than the lift of one diameter, so a
+        // few particles thrown by the network cannot hide inside the total.
         const double g = std::sqrt(sg->prm.gravity[0] * sg->prm.gravity[0] + sg->prm.gravity[1] * sg->prm.gravity[1]);
         const double escale = now[3] * g * sg->prm.r_mean;
         if (!have_floor) {
             e_floor = before[1] + before[2];
+            s_floor = before[4];
             have_floor = true;
         }
         const double e_new = now[1] + now[2];
         const bool bad_overlap = !(now[0] <= sg->prm.max_overlap);
-        const bool bad_energy = !(e_new <= e_floor + sg->prm.energy_tol * escale);
+        const bool bad_energy = !(e_new <= e_floor + sg->prm.energy_tol * escale) ||
+                                !(now[4] <= s_floor + 2.0 * g * sg->prm.r_mean);
         if (!bad_overlap && !bad_energy) {
             std::swap(sg->x_prev, sg->x_cur);   // prev <- cur
             std::swap(sg->x_cur, sg->x_next);   // cur <- next
             e_floor = std::min(e_floor, e_new);
+            s_floor = std::min(s_floor, now[4]);
             st.strides_network += 1;
             st.max_overlap_seen = std::max(st.max_overlap_seen, now[0]);
             solver_stale = true;

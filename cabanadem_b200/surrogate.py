@@ -205,6 +205,18 @@ def runout_front(x, q=0.999):
     return float(np.quantile(np.asarray(x)[:, 0], q))
 
 
+def depth_profile(x, rad, length, bins=400, packing=0.85):
+    """Deposit depth from mass: disk area in each of `bins` columns over [0, length] divided by
+    the column width and a packing fraction (insensitive to a few isolated particles)."""
+    x = np.asarray(x)
+    r = np.asarray(rad)
+    w = length / bins
+    idx = np.clip((x[:, 0] / length * bins).astype(int), 0, bins - 1)
+    a = np.zeros(bins)
+    np.add.at(a, idx, np.pi * r * r)
+    return a / (w * packing)
+
+
 def pile_profile(x, rad, length, bins=400):
     """Height of the deposit (max y + r) in `bins` columns over [0, length]."""
     x = np.asarray(x)
@@ -261,6 +273,7 @@ def evaluate(sg: Surrogate, make_scenario, seconds: float, ctx: api.Context) -> 
     fa, fb, f0 = runout_front(xa), runout_front(xb), runout_front(x0)
     length = sc.extra.get("length", float(max(xa[:, 0].max(), xb[:, 0].max())))
     ha, hb = pile_profile(xa, sc.state.rad, length), pile_profile(xb, sc.state.rad, length)
+    da, db = depth_profile(xa, sc.state.rad, length), depth_profile(xb, sc.state.rad, length)
     n = sc.state.n
     return dict(n=n, seconds=seconds, strides=strides, dem_wall_s=t_dem, surrogate_wall_s=t_sur,
                 speedup=t_dem / t_sur, dem_particle_steps_per_s=n * strides * STRIDE / t_dem,
@@ -268,4 +281,5 @@ def evaluate(sg: Surrogate, make_scenario, seconds: float, ctx: api.Context) -> 
                 front_dem=fa, front_surrogate=fb, front_initial=f0,
                 front_error=abs(fb - fa) / fa, runout_error=abs(fb - fa) / max(fa - f0, 1e-30),
                 profile_error=float(np.abs(ha - hb).mean() / max(ha.max(), 1e-30)),
+                depth_error=float(np.abs(da - db).mean() / max(da.max(), 1e-30)),
                 max_height_dem=float(ha.max()), max_height_surrogate=float(hb.max()), **st)

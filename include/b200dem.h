@@ -321,7 +321,9 @@ typedef struct {
     double gravity[3];       /* energy residual */
     double max_overlap;      /* fallback: any overlap above this fraction of the smaller radius */
     double energy_tol;       /* fallback: mechanical energy above its lowest value since the last
-                              * DEM stride by more than energy_tol x total weight x r_mean */
+                              * DEM stride by more than energy_tol x total weight x r_mean, or
+                              * the largest specific energy of one particle above its lowest
+                              * value by more than the lift of one diameter (2 g r_mean) */
     int max_nodes;           /* capacity (particles per call, all frames together) */
     int max_frames;          /* capacity (independent frames per training batch) */
     int project_iters;       /* contact projection after a network stride: Jacobi sweeps (0: off) */
