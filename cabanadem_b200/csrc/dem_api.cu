@@ -775,6 +775,19 @@ __global__ void k_clear_status(Ctl *ctl, int bits) {
 
 bool ref_mode(const dem_solver *s) { return s->sp.rebuild_every_step != 0; }
 
+// Pick the contact-kernel build for the next graph from the last step's deferred count: the
+// dense build (more resident blocks, wider apply grid) above 30 % of the particles, back to
+// the sparse one below 10 %.  Same arithmetic either way; a switch re-captures the graph.
+void adapt_density(dem_solver *s, const Ctl &c) {
+    const int n = s->p->P.n;
+    const double f = n > 0 ? (double)c.last_ndefer / n : 0.0;
+    const int want = s->fc.dense ? (f >= 0.10 ? 1 : 0) : (f > 0.30 ? 1 : 0);
+    if (want != s->fc.dense) {
+        s->fc.dense = want;
+        s->version++;
+    }
+}
+
 int check_walls(dem_solver *s) {
     if (s->walls_ok) return DEM_OK;
     return fail(s->ctx, DEM_ERR_INVALID,
@@ -937,6 +950,7 @@ extern "C" int dem_solver_run(dem_solver *s, int nsteps) {
                 CK(cudaGraphLaunch(s->graph, st));
                 s->launches += s->graph_nodes;
                 c = read_ctl(s);
+                adapt_density(s, c);
                 if (c.steps_done >= c.target || (c.status & DEM_ERR_NEIGHBOR_OVERFLOW) || c.steps_done == done_before)
                     break;
                 done_before = c.steps_done;
@@ -973,6 +987,7 @@ extern "C" int dem_solver_run(dem_solver *s, int nsteps) {
             const int done_before = s->graph_done_mark;
             Ctl c = read_ctl(s);
             CK(cudaGetLastError());
+            adapt_density(s, c);
             {
                 float ms = 0.f;
                 CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));

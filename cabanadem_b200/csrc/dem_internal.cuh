@@ -40,6 +40,7 @@ struct Ctl {
     int ndefer;               // particles handed from the streaming to the contact kernel
     long long total_steps;
     long long rebuilds;
+    int last_ndefer;          // deferred particles of the last completed fused step
 };
 
 struct Particles {
@@ -93,6 +94,8 @@ struct ForceConsts {
     int has_fix;
     int mixed;                 // 1: FP32 contact forces (dem_mixed.cu)
     int stream_block;          // k_stream block size: 64, 128 or 256
+    int dense;                 // 1: most particles are in contact -- contact kernels compiled for
+                               // more resident blocks, wider apply grid (same arithmetic)
     const struct SceneConst *scenes;   // per-scene damping/friction, null: the scalars above
     int wps;                   // walls per scene (> 0 with scenes): scene s owns [s*wps, s*wps+wps)
 };
@@ -176,7 +179,7 @@ void launch_contact_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const 
                           const PairConst *pw, const WallGeom *walls, int blocks, cudaStream_t s);
 void launch_force_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
                         const PairConst *pw, const WallGeom *walls, cudaStream_t s);
-const void *contact_mixed_kernel();
+const void *contact_mixed_kernel(int dense);
 void launch_energy(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
                    const PairConst *pw, const WallGeom *walls, double *partials, int nparts, double *out,
                    cudaStream_t s);

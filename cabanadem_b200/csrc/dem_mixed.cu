@@ -12,7 +12,8 @@ namespace b200dem {
 
 namespace {
 
-__global__ void __launch_bounds__(kBlock) k_contact_mixed(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
+template <int MINB>
+__global__ void __launch_bounds__(kBlock, MINB) k_contact_mixed(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
                                                           const PairConst *__restrict__ pp,
                                                           const PairConst *__restrict__ pw,
                                                           const WallGeom *__restrict__ walls) {
@@ -49,7 +50,10 @@ __global__ void __launch_bounds__(kBlock) k_force_mixed(Particles P, NbrList L, 
 
 void launch_contact_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
                           const PairConst *pw, const WallGeom *walls, int blocks, cudaStream_t s) {
-    k_contact_mixed<<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+    if (fc.dense)
+        k_contact_mixed<kContactMixedMinBlocksDense><<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+    else
+        k_contact_mixed<1><<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
 }
 
 void launch_force_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
@@ -57,6 +61,8 @@ void launch_force_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const Fo
     k_force_mixed<<<(P.n + kBlock - 1) / kBlock, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
 }
 
-const void *contact_mixed_kernel() { return (const void *)k_contact_mixed; }
+const void *contact_mixed_kernel(int dense) {
+    return dense ? (const void *)k_contact_mixed<kContactMixedMinBlocksDense> : (const void *)k_contact_mixed<1>;
+}
 
 }  // namespace b200dem

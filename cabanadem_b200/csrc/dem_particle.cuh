@@ -13,6 +13,12 @@ namespace b200dem {
 namespace {
 
 constexpr int kBlock = 128;
+// Resident blocks per SM the contact kernels are compiled for (a register cap).  A sparse step
+// defers few particles and prefers the uncapped kernel; when most particles are in contact the
+// kernel is latency-bound and more resident warps win (B200 sweep on a dense 200k flow: FP64
+// 177 -> 133 us per step at 5 blocks, mixed 120 -> 99 us at 4; the 2M lattice loses 1-3 %).
+constexpr int kContactMinBlocksDense = 5;
+constexpr int kContactMixedMinBlocksDense = 4;
 constexpr int kApplyBlock = 256;
 
 struct __align__(32) D4 {

@@ -160,7 +160,8 @@ __global__ void __launch_bounds__(BS, MINB) k_stream(Particles P, NbrList L, Ctl
 
 // Fused step, kernel 2 of 3: the full arithmetic for the deferred particles.  New u and
 // omega go to scratch slot t (their current values are still read by contact partners).
-__global__ void __launch_bounds__(kBlock) k_contact(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
+template <int MINB>
+__global__ void __launch_bounds__(kBlock, MINB) k_contact(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
                                                     const PairConst *__restrict__ pp, const PairConst *__restrict__ pw,
                                                     const WallGeom *__restrict__ walls) {
     if (!step_gate(ctl)) return;
@@ -211,6 +212,7 @@ __global__ void __launch_bounds__(kApplyBlock) k_apply(Particles P, NbrList L, C
         const double v2 = vmax_collect_warp(P.vslots);
         if (threadIdx.x == 0) {
             ctl->disp = ctl->disp + fc.dt * sqrt(v2) * (1.0 + 1e-9);
+            ctl->last_ndefer = nd;
             ctl->ndefer = 0;
             ctl->cur ^= 1;
             ctl->steps_done += 1;
@@ -361,14 +363,15 @@ static int persistent_blocks(const void *kernel, int block, int n) {
 void launch_step(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
                  const PairConst *pw, const WallGeom *walls, int mode, cudaStream_t s) {
     if (mode == MODE_FUSED) {
-        static int gc = 0, gm = 0, ga = 0, last_n = -1;
+        static int gc = 0, gm = 0, gcd = 0, gmd = 0, last_n = -1;
         if (last_n != P.n) {
-            // two contact blocks per SM: enough for dense packings, little fixed cost when
-            // only a few particles are deferred; the apply kernel copies 48 B per deferred
-            // particle and takes one ticket per block
-            gc = min(persistent_blocks((const void *)k_contact, kBlock, P.n), 2 * 148);
-            gm = min(persistent_blocks(contact_mixed_kernel(), kBlock, P.n), 2 * 148);
-            ga = 32;
+            // contact kernels: every block the SMs hold (a dense packing defers nearly every
+            // particle; blocks past the deferred count exit at once); the apply kernel copies
+            // 48 B per deferred particle and takes one ticket per block: one block per SM
+            gc = persistent_blocks((const void *)k_contact<1>, kBlock, P.n);
+            gm = persistent_blocks(contact_mixed_kernel(0), kBlock, P.n);
+            gcd = persistent_blocks((const void *)k_contact<kContactMinBlocksDense>, kBlock, P.n);
+            gmd = persistent_blocks(contact_mixed_kernel(1), kBlock, P.n);
             last_n = P.n;
         }
         if (fc.stream_block == 64)
@@ -378,10 +381,12 @@ void launch_step(const Particles &P, const NbrList &L, Ctl *ctl, const ForceCons
         else
             k_stream<128, 10><<<(P.n + 127) / 128, 128, 0, s>>>(P, L, ctl, fc, walls);
         if (fc.mixed)
-            launch_contact_mixed(P, L, ctl, fc, pp, pw, walls, gm, s);
+            launch_contact_mixed(P, L, ctl, fc, pp, pw, walls, fc.dense ? gmd : gm, s);
+        else if (fc.dense)
+            k_contact<kContactMinBlocksDense><<<gcd, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
         else
-            k_contact<<<gc, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
-        k_apply<<<ga, kApplyBlock, 0, s>>>(P, L, ctl, fc);
+            k_contact<1><<<gc, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+        k_apply<<<fc.dense ? 4 * 148 : 148, kApplyBlock, 0, s>>>(P, L, ctl, fc);
     } else if (fc.mixed) {
         launch_force_mixed(P, L, ctl, fc, pp, pw, walls, s);
     } else {
