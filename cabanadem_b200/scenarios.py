@@ -145,6 +145,47 @@ def tst03(inp: Inputs) -> Scenario:
                     output_frequency=int(inp["output_frequency"]))
 
 
+def tst04_points(length=1.0, height=1.0, spacing=0.1):
+    """Zigzag lattice of examples/tst_04_granular_dam_break_2d.cpp:14-52 (create_points): rows
+    and columns int(extent / spacing), odd rows shifted by half a spacing, points inside the
+    rectangle kept in row-major order."""
+    cols, rows = int(length / spacing), int(height / spacing)
+    pts = []
+    for i in range(rows):
+        off = 0.0 if i % 2 == 0 else spacing / 2.0
+        for j in range(cols):
+            x, y = j * spacing + off, i * spacing
+            if x <= length and y <= height:
+                pts.append((x, y))
+    return np.array(pts, dtype=np.float64).reshape(-1, 2)
+
+
+def tst04(inp: Inputs, box_walls: bool = False) -> Scenario:
+    """examples/tst_04_granular_dam_break_2d.cpp:120-267.  The reference sets a left wall, a
+    floor and a right wall (:189-222) and then overwrites all three in its wall functor
+    (:224-248): every wall at (0, -3 r, 0) with a zero normal, i.e. inert.  box_walls=True keeps
+    the three walls as first set.  Three wall-history slots per particle (the reference declares
+    one for its three walls)."""
+    r = float(inp["particle_radius"])
+    pts = tst04_points(1.0, 1.0, 2.0 * r)
+    s = ParticleState.create(len(pts), max_cnts=6, max_walls=3)
+    _material(s, inp)
+    s.x[:, 0], s.x[:, 1] = pts[:, 0], pts[:, 1]
+    w = WallState.create(3)
+    if box_walls:
+        w.x[:] = [(-2. * r, 0.5, 0.), (0.8, 0., 0.), (1.4, 0.5, 0.)]
+        w.normal[:] = [(1., 0., 0.), (0., 1., 0.), (-1., 0., 0.)]
+    else:
+        w.x[:] = (0., -3. * r, 0.)
+    w.E[:] = inp["wall_youngs_modulus"]
+    w.G[:] = inp["wall_shear_modulus"]
+    w.nu[:] = inp["wall_poissons_ratio"]
+    fp = _force_params(inp["coefficient_of_restitution_pp"], inp["coefficient_of_restitution_pw"],
+                       inp["friction_pp"], inp["friction_pw"])
+    return Scenario("tst04", s, w, fp, float(inp["timestep"]), inp["num_steps"] + 1, delta=3. * r,
+                    output_frequency=int(inp["output_frequency"]))
+
+
 def bonded_bar(nx=256, ny=64, nz=8, radius=0.5e-3, pull=0.05, dt=2e-8, nsteps=50_000, kn=1e7, kt=4e6,
                break_strain=0.01, max_bonds=8, bond_quirks=0x04):
     """Simple-cubic bar of nx*ny*nz spheres (r = 0.5 mm, pitch 1 mm), every pair within

@@ -23,6 +23,7 @@
 #include <cctype>
 #include <cmath>
 #include <cstdio>
+#include <filesystem>
 #include <fstream>
 #include <functional>
 #include <iostream>
@@ -224,6 +225,8 @@ class HostSlice {
         m_->dirty = true;
         return m_->data[static_cast<size_t>(i) * m_->ncomp + d];
     }
+    // read without marking the field for upload
+    T get(int i, int d = 0) const { return m_->data[static_cast<size_t>(i) * m_->ncomp + d]; }
     std::size_t size() const { return m_->data.size() / m_->ncomp; }
     const T *data() const { return m_->data.data(); }
 
@@ -246,6 +249,8 @@ class Particles {
               std::shared_ptr<Context> ctx = nullptr)
         : n_(static_cast<int>(n)), out_(output_folder), ctx_(ctx ? ctx : Context::get_default()) {
         ctx_->check(dem_particles_create(ctx_->handle(), n_, MaxCnts, MaxNoWalls, &h_), "dem_particles_create");
+        // Particles.hpp:53-61: the output folder is created if it does not exist
+        if (!out_.empty()) std::filesystem::create_directories(out_);
     }
     ~Particles() { dem_particles_destroy(h_); }
     Particles(const Particles &) = delete;
@@ -300,6 +305,84 @@ class Particles {
         for (auto &kv : mi_) kv.second->fresh = false;
     }
 
+    // output(step, time) (Particles.hpp:299-346): one snapshot per call, <folder>/particles_<step>.csv,
+    // one row per particle with the fields the reference writes to particles_<step>.h5 (its
+    // HDF5 writer; no HDF5 library here) minus the accelerations, which are not stored.
+    // Columns are named after the reference's slices with a component suffix.  No folder, no output.
+    void output(int output_step, double output_time) {
+        if (out_.empty()) return;
+        auto x = slicePosition();
+        auto u = sliceVelocity();
+        auto w = sliceOmega();
+        auto f = sliceForce();
+        auto m = sliceMass();
+        auto rho = sliceDensity();
+        auto r = sliceRadius();
+        auto tc = sliceTotalNoTangentialContacts();
+        const std::string path = out_ + "/particles_" + std::to_string(output_step) + ".csv";
+        std::FILE *fo = std::fopen(path.c_str(), "w");
+        if (!fo) throw Error("cannot write " + path);
+        std::fprintf(fo, "# time %.17g\n", output_time);
+        std::fprintf(fo, "id,positions_0,positions_1,positions_2,velocities_0,velocities_1,velocities_2,"
+                         "omega_0,omega_1,omega_2,forces_0,forces_1,forces_2,mass,density,radius,"
+                         "total_no_tangential_contacts\n");
+        for (int i = 0; i < n_; ++i)
+            std::fprintf(fo, "%d,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,"
+                             "%.17g,%.17g,%.17g,%d\n",
+                         i, x.get(i, 0), x.get(i, 1), x.get(i, 2), u.get(i, 0), u.get(i, 1), u.get(i, 2),
+                         w.get(i, 0), w.get(i, 1), w.get(i, 2), f.get(i, 0), f.get(i, 1), f.get(i, 2), m.get(i),
+                         rho.get(i), r.get(i), tc.get(i));
+        std::fclose(fo);
+    }
+    const std::string &output_folder() const { return out_; }
+
+    // resize(n) (Particles.hpp:273-297): the first min(n, size()) particles keep their values;
+    // added particles start zeroed with empty contact slots (tangential index -1).  The device
+    // set is re-created, so no solver may be attached: create solvers after the last resize.
+    // Slices taken before the call see the new size.  External forces and fix flags are reset.
+    void resize(std::size_t n) {
+        if (attached_ > 0) throw Error("Particles::resize: a solver is attached to this particle set");
+        const int nn = static_cast<int>(n);
+        const int dfields[][2] = {{DEM_F_X, 3},          {DEM_F_U, 3},          {DEM_F_OMEGA, 3},
+                                  {DEM_F_FORCE, 3},      {DEM_F_TORQUE, 3},     {DEM_F_M, 1},
+                                  {DEM_F_RHO, 1},        {DEM_F_RAD, 1},        {DEM_F_I, 1},
+                                  {DEM_F_E, 1},          {DEM_F_NU, 1},         {DEM_F_G, 1},
+                                  {DEM_F_TNG_SS_X, MaxCnts}, {DEM_F_TNG_SS_Y, MaxCnts}, {DEM_F_TNG_SS_Z, MaxCnts},
+                                  {DEM_F_TNG_SW_X, MaxNoWalls}, {DEM_F_TNG_SW_Y, MaxNoWalls},
+                                  {DEM_F_TNG_SW_Z, MaxNoWalls}};
+        for (const auto &f : dfields) slice_d(f[0], f[1]);   // current values (or pending edits)
+        slice_i(DEM_F_TNG_IDX, MaxCnts);
+        slice_i(DEM_F_TNG_COUNT, 1);
+        dem_particles *h = nullptr;
+        ctx_->check(dem_particles_create(ctx_->handle(), nn, MaxCnts, MaxNoWalls, &h), "dem_particles_create");
+        dem_particles_destroy(h_);
+        h_ = h;
+        n_ = nn;
+        for (auto &kv : md_) {
+            kv.second->data.resize(static_cast<size_t>(nn) * kv.second->ncomp, 0.0);
+            kv.second->dirty = kv.second->ncomp > 0;
+            kv.second->fresh = true;
+        }
+        for (auto &kv : mi_) {
+            kv.second->data.resize(static_cast<size_t>(nn) * kv.second->ncomp, kv.first == DEM_F_TNG_IDX ? -1 : 0);
+            kv.second->dirty = kv.second->ncomp > 0;
+            kv.second->fresh = true;
+        }
+        commit();
+    }
+
+    // External force added before the pair forces, [n][3], and DEM_FIX_* boundary flags, [n]
+    // (the hooks of the reference examples' applyTensileForce / applyBoundaryConditions).
+    void setExternalForce(const std::vector<double> &f) {
+        ctx_->check(dem_particles_set(h_, DEM_F_EXT_FORCE, f.data(), (long)f.size()), "dem_particles_set");
+    }
+    void setFixFlags(const std::vector<unsigned char> &flags) {
+        ctx_->check(dem_particles_set(h_, DEM_F_FIX, flags.data(), (long)flags.size()), "dem_particles_set");
+    }
+
+    // solvers hold the device handle: resize() is refused while one exists
+    void attach_solver(int d) { attached_ += d; }
+
     std::size_t size() const { return static_cast<std::size_t>(n_); }
     dem_particles *handle() { return h_; }
     Context &context() { return *ctx_; }
@@ -334,6 +417,7 @@ class Particles {
     }
 
     int n_;
+    int attached_ = 0;
     std::string out_;
     std::shared_ptr<Context> ctx_;
     dem_particles *h_ = nullptr;
@@ -422,8 +506,12 @@ class SolverDEM {
         particles_->context().check(dem_solver_create(particles_->context().handle(), particles_->handle(),
                                                       wall_ ? wall_->handle() : nullptr, &fp, &sp, &h_),
                                     "dem_solver_create");
+        particles_->attach_solver(1);
     }
-    ~SolverDEM() { dem_solver_destroy(h_); }
+    ~SolverDEM() {
+        dem_solver_destroy(h_);
+        particles_->attach_solver(-1);
+    }
 
     void set_output(std::function<void(int, double)> f) { out_ = std::move(f); }
 
@@ -450,6 +538,8 @@ class SolverDEM {
     void output(int step) {
         if (output_frequency > 0 && step % output_frequency == 0) {
             std::cout << "We are at " << step << " / " << num_steps << std::endl;
+            // Solver.hpp:100-107: particles->output(step / output_frequency, step * dt)
+            particles_->output(step / output_frequency, step * dt);
             if (out_) out_(step, step * dt);
         }
     }
@@ -493,11 +583,14 @@ class BondedDEM {
         const dem_force_params fp{1.0, 1.0, 0.0, 0.0, DEM_REF_COMPAT};
         ctx_->check(dem_solver_create(ctx_->handle(), particles->handle(), nullptr, &fp, &sp, &s_), "dem_solver_create");
         ctx_->check(dem_bonds_create(s_, MaxBonds, &bp, &b_), "dem_bonds_create");
+        particles->attach_solver(1);
         invalidate_ = [particles]() { particles->invalidate(); };
+        detach_ = [particles]() { particles->attach_solver(-1); };
     }
     ~BondedDEM() {
         dem_bonds_destroy(b_);
         dem_solver_destroy(s_);
+        detach_();
     }
     // setupBonds (BondedDEM_Particles.hpp:86-171): reference factor 3, search cutoff 4 rad(0)
     void setupBonds(double factor = 3.0, double search_cutoff = 0.0) {
@@ -518,7 +611,7 @@ class BondedDEM {
     std::shared_ptr<CabanaDEM::Context> ctx_;
     dem_solver *s_ = nullptr;
     dem_bonds *b_ = nullptr;
-    std::function<void()> invalidate_;
+    std::function<void()> invalidate_, detach_;
 };
 
 }  // namespace CabanaBondedDEM

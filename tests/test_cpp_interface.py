@@ -1,41 +1,216 @@
-"""The C++ interface (include/CabanaDEM_B200.hpp): the example driver builds against the
-header and library on the CPU; on the GPU it reproduces the head-on impact of the reference's
-first validation case bit for bit against the oracle."""
+"""The C++ interface (include/CabanaDEM_B200.hpp) and the example drivers on it.
+
+On the CPU every driver builds against the header and library, and the snapshot reader
+parses the drivers' output format.  On the GPU each driver runs with the reference's command
+line and input file; every snapshot it writes (particles_<k>.csv after each step divisible by
+output_frequency) is compared bit for bit with the oracle stepped the same way, and the
+observables the reference's automate.py reads from those files are checked: restitution
+out = in for example 03 (automate.py:315), the rebound spin peak for example 04 (:447), the
+contact slots of tst_03 (:531)."""
 import json
+import math
 import os
 import subprocess
 
 import numpy as np
 import pytest
 
+from cabanadem_b200 import snapshots
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-EXE = os.path.join(ROOT, "examples", "01_two_sphere_head_on")
+EXDIR = os.path.join(ROOT, "examples")
+EXE = os.path.join(EXDIR, "01_two_sphere_head_on")
+DRIVERS = ("01_two_sphere_head_on", "01ElasticNormalImpactOfTwoIdenticalParticles",
+           "02ElasticNormalImpactOfParticleWall", "03NormalParticleWallDifferentCOR",
+           "04ObliqueParticleWallDifferentAngles", "Tst01ParticleInsertion", "Tst03MultipleParticlesContacts",
+           "Tst04GranularDamBreak2d", "Tst01BDEMTwoParticlesTensile3D")
+K01 = "01_elastic_normal_impact_of_two_identical_particles"
+K02 = "02_elastic_normal_impact_of_particle_wall"
+K03 = "03_normal_particle_wall_different_cor"
+K04 = "04_oblique_particle_wall_different_angles"
+KT3 = "tst_03_multiple_particles_contacts"
+KT4 = "tst_04_granular_dam_break_2d"
 
 
 def _build():
     if not os.path.exists(os.path.join(ROOT, "cabanadem_b200", "libb200dem.so")):
         pytest.skip("library not built")
-    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "examples")], check=True)
+    subprocess.run(["make", "-s", "-C", EXDIR], check=True)
 
 
-def test_example_driver_builds():
+def _raw_inputs():
+    with open(os.path.join(ROOT, "tests", "golden", "example_inputs.json")) as f:
+        return json.load(f)
+
+
+def _run(tmp_path, exe, key, extra=()):
+    tmp_path.mkdir(parents=True, exist_ok=True)
+    inp = tmp_path / "in.json"
+    inp.write_text(json.dumps(_raw_inputs()[key]))
+    out = tmp_path / "out"
+    subprocess.run([os.path.join(EXDIR, exe), str(inp), str(out), *extra], check=True, capture_output=True)
+    return [snapshots.read(f) for f in snapshots.files(str(out))]
+
+
+def test_example_drivers_build():
     _build()
-    assert os.access(EXE, os.X_OK)
+    for d in DRIVERS:
+        assert os.access(os.path.join(EXDIR, d), os.X_OK), d
+
+
+def test_snapshot_reader(tmp_path):
+    (tmp_path / "particles_12.csv").write_text(
+        "# time 0.25\n"
+        "id,positions_0,positions_1,positions_2,velocities_0,velocities_1,velocities_2,omega_0,omega_1,omega_2,"
+        "forces_0,forces_1,forces_2,mass,density,radius,total_no_tangential_contacts\n"
+        "0,1,2,3,4,5,6,7,8,9,10,11,12,13,14,15,2\n"
+        "1,0.1,0.2,0.30000000000000004,0,0,0,0,0,0,0,0,0,1,1,1,0\n")
+    (tmp_path / "particles_3.csv").write_text((tmp_path / "particles_12.csv").read_text())
+    (tmp_path / "other.csv").write_text("x")
+    fs = snapshots.files(str(tmp_path))
+    assert [os.path.basename(f) for f in fs] == ["particles_3.csv", "particles_12.csv"]
+    s = snapshots.read(fs[1])
+    assert s["time"] == 0.25
+    assert s["positions"].shape == (2, 3) and s["positions"][1, 2] == 0.30000000000000004
+    assert s["forces"][0].tolist() == [10., 11., 12.]
+    assert s["total_no_tangential_contacts"].tolist() == [2, 0]
+    assert s["radius"].tolist() == [15., 1.]
+
+
+def _oracle_snapshots(sc):
+    """The oracle stepped as SolverDEM::run: steps 0..num_steps, a snapshot after every step
+    divisible by output_frequency (Solver.hpp:79-108)."""
+    from oracle import oracle as O
+    st, freq = sc.state.copy(), sc.output_frequency
+    last = sc.nsteps - 1
+    out, step = [], 0
+    while step <= last:
+        stop = min(last, -(-step // freq) * freq)
+        O.run(st, sc.walls, sc.params, sc.dt, stop - step + 1, delta=sc.delta, pow_mode=O.POW_SQRT)
+        if stop % freq == 0:
+            out.append((stop * sc.dt, st.copy()))
+        step = stop + 1
+    return out
+
+
+def _assert_snapshots(got, ref):
+    assert len(got) == len(ref)
+    for k, (g, (t, r)) in enumerate(zip(got, ref)):
+        assert g["time"] == t, k
+        for name, f in (("positions", "x"), ("velocities", "u"), ("omega", "omega"), ("forces", "force")):
+            assert np.array_equal(g[name], getattr(r, f)), (k, name, np.abs(g[name] - getattr(r, f)).max())
+        assert np.array_equal(g["total_no_tangential_contacts"], r.tng_count), k
+        assert np.array_equal(g["mass"], r.m) and np.array_equal(g["radius"], r.rad)
+
+
+def _cases():
+    from cabanadem_b200 import scenarios as S
+    return [
+        ("01", "01ElasticNormalImpactOfTwoIdenticalParticles", K01, (), lambda I: S.example01(I[K01])),
+        ("02", "02ElasticNormalImpactOfParticleWall", K02, (), lambda I: S.example02(I[K02])),
+        ("03_cor0.4", "03NormalParticleWallDifferentCOR", K03, ("--cor_pw=0.4",), lambda I: S.example03(I[K03], 0.4)),
+        ("04_30deg", "04ObliqueParticleWallDifferentAngles", K04, ("--angle=30",),
+         lambda I: S.example04(I[K04], 30.0)),
+        ("tst03", "Tst03MultipleParticlesContacts", KT3, (), lambda I: S.tst03(I[KT3])),
+        ("tst04", "Tst04GranularDamBreak2d", KT4, (), lambda I: S.tst04(I[KT4])),
+        ("tst04_box", "Tst04GranularDamBreak2d", KT4, ("--walls=box",), lambda I: S.tst04(I[KT4], box_walls=True)),
+    ]
+
+
+CASE_IDS = ["01", "02", "03_cor0.4", "04_30deg", "tst03", "tst04", "tst04_box"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", CASE_IDS)
+def test_driver_snapshots_match_oracle(tmp_path, example_inputs, case):
+    _build()
+    _, exe, key, extra, make = next(c for c in _cases() if c[0] == case)
+    got = _run(tmp_path, exe, key, extra)
+    sc = make(example_inputs)
+    _assert_snapshots(got, _oracle_snapshots(sc))
+    if case == "tst03":
+        counts = np.array([g["total_no_tangential_contacts"] for g in got])
+        assert counts[:, 0].max() == 2 and counts[-1].sum() == 0
+
+
+@pytest.mark.gpu
+def test_driver_03_restitution_out_equals_in(tmp_path, example_inputs):
+    """automate.py:303-343: the last snapshot's velocities[0][1] / velocity_p against cor_pw."""
+    _build()
+    v = float(example_inputs[K03]["velocity_p"])
+    for cor in (0.01, 0.2, 0.4, 0.6, 0.8, 1.0):
+        got = _run(tmp_path / ("c%g" % cor), "03NormalParticleWallDifferentCOR", K03, ("--cor_pw=%g" % cor,))
+        assert abs(got[-1]["velocities"][0, 1] / v - cor) < 0.02, cor
+
+
+@pytest.mark.gpu
+def test_driver_04_rebound_spin_peaks_near_30_degrees(tmp_path, example_inputs):
+    """automate.py:427-478 plots omega[0][2] of the last snapshot against the incident angle;
+    the oracle run of the same cases is pinned to the Lethe and experimental curves on the CPU."""
+    _build()
+    angles = [10., 20., 25., 30., 35., 40., 50.]
+    om = []
+    for a in angles:
+        got = _run(tmp_path / ("a%g" % a), "04ObliqueParticleWallDifferentAngles", K04, ("--angle=%g" % a,))
+        om.append(got[-1]["omega"][0, 2])
+    assert 25.0 <= angles[int(np.argmax(om))] <= 35.0
+
+
+@pytest.mark.gpu
+def test_particle_insertion_driver(tmp_path):
+    """tst_01_particle_insertion: snapshots of 1, 20, 20 (moved by 2 u) and 15 particles."""
+    _build()
+    raw = _raw_inputs()[K04]
+    got = _run(tmp_path, "Tst01ParticleInsertion", K04, ("--angle=30",))
+    r = raw["particle_radius"]["value"]
+    assert [g["positions"].shape[0] for g in got] == [1, 20, 20, 15]
+    assert [g["time"] for g in got] == [0.0, 0.1, 0.2, 0.3]
+    assert got[0]["positions"][0, 1] == r + r / 1000000.
+    a = 30. / 180. * math.pi
+    assert got[0]["velocities"][0, :2].tolist() == [3.9 * math.sin(a), -3.9 * math.cos(a)]
+    i = np.arange(20)
+    assert np.array_equal(got[1]["positions"][:, 1], 3 * i * r + r / 1000000.)
+    assert np.array_equal(got[2]["positions"][:, 1], 3 * i * r + r / 1000000. + 2.)
+    assert np.array_equal(got[3]["positions"][:, 1], 5 * np.arange(15) * r + r / 1000000.)
+    assert got[1]["mass"][0] > 0 and got[1]["mass"][1] == 0.0     # added particles start zeroed
+
+
+@pytest.mark.gpu
+def test_bdem_driver_matches_oracle(tmp_path):
+    """tst_01_BDEM: the driver's snapshots every 100 steps against the bonded oracle."""
+    _build()
+    from cabanadem_b200 import scenarios as S
+    from oracle import oracle as O
+    out = tmp_path / "bdem"
+    subprocess.run([os.path.join(EXDIR, "Tst01BDEMTwoParticlesTensile3D"), str(out)], check=True,
+                   capture_output=True)
+    got = [snapshots.read(f) for f in snapshots.files(str(out))]
+    case = S.bdem_two_particles()
+    st, b = case["state"].copy(), case["bonds"].copy()
+    O.setup_bonds(b, st, case["bond_factor"], case["search_cutoff"])
+    last = case["nsteps"] - 1
+    assert len(got) == last // 100 + 1
+    done = 0
+    for k, g in enumerate(got):
+        O.bonded_run(st, b, case["bparams"], case["dt"], k * 100 + 1 - done, ext_force=case["ext_force"],
+                     fix_flags=case["fix_flags"], pow_mode=O.POW_SQRT)
+        done = k * 100 + 1
+        for name, f in (("positions", "x"), ("velocities", "u"), ("omega", "omega"), ("forces", "force")):
+            assert np.array_equal(g[name], getattr(st, f)), (k, name)
 
 
 @pytest.mark.gpu
 def test_example_driver_matches_oracle(tmp_path, example_inputs):
+    """01_two_sphere_head_on records sphere 1's force at every step."""
     _build()
     from cabanadem_b200 import scenarios as S
     from oracle import oracle as O
-    raw = json.load(open(os.path.join(ROOT, "tests", "golden", "example_inputs.json")))
-    key = "01_elastic_normal_impact_of_two_identical_particles"
     inp = tmp_path / "in.json"
-    inp.write_text(json.dumps(raw[key]))
+    inp.write_text(json.dumps(_raw_inputs()[K01]))
     out = tmp_path / "out.csv"
     subprocess.run([EXE, str(inp), str(out)], check=True, capture_output=True)
     got = np.loadtxt(out, delimiter=",", skiprows=1)
-    sc = S.example01(example_inputs[key])
+    sc = S.example01(example_inputs[K01])
     st = sc.state
     ref = []
     for _ in range(sc.nsteps):
