@@ -643,6 +643,8 @@ double beta_of(double cor) {   // Force.hpp:206-210
     return tmp_1 / std::sqrt(tmp_2);
 }
 
+void pick_contact_kernel(dem_solver *s);
+
 int prepare(dem_solver *s) {
     dem_ctx *ctx = s->ctx;
     dem_particles *p = s->p;
@@ -728,6 +730,7 @@ int prepare(dem_solver *s) {
     fc.has_fix = p->any_fix ? 1 : 0;
     fc.mixed = s->sp.precision == DEM_MIXED ? 1 : 0;
     fc.stream_block = (s->sp.stream_block == 64 || s->sp.stream_block == 256) ? s->sp.stream_block : 128;
+    pick_contact_kernel(s);
     fc.scenes = s->nscenes > 0 ? s->d_scenes : nullptr;
     fc.wps = s->nscenes > 0 ? s->wps : 0;
     if (s->B.nscenes < p->nscenes) {   // per-scene grid descriptors and bounding boxes
@@ -775,6 +778,22 @@ __global__ void k_clear_status(Ctl *ctl, int bits) {
 
 bool ref_mode(const dem_solver *s) { return s->sp.rebuild_every_step != 0; }
 
+// Contact kernel of the next graph.  Few deferred particles (a sparse step): the cooperative
+// kernel, whose short dependent chains hide memory latency (B200, 2M-sphere lattice: 105 ->
+// 87 us per step late in the run at 8 lanes).  Most particles in contact (a dense step): the
+// per-thread build for more resident blocks, which issues fewer instructions per contact
+// (200k-disk dam break at t = 0.3 s: 131 us per step against 197 us at 8 lanes).
+// contact_lanes 1, 4 or 8 fixes the choice.
+void pick_contact_kernel(dem_solver *s) {
+    const int req = s->sp.contact_lanes;
+    if (req == 1 || s->p->P.mc > kCoopSlots)
+        s->fc.coop = 0;
+    else if (req == 4 || req == 8)
+        s->fc.coop = req;
+    else
+        s->fc.coop = s->fc.dense ? 0 : 8;
+}
+
 // Pick the contact-kernel build for the next graph from the last step's deferred count: the
 // dense build (more resident blocks, wider apply grid) above 30 % of the particles, back to
 // the sparse one below 10 %.  Same arithmetic either way; a switch re-captures the graph.
@@ -784,6 +803,7 @@ void adapt_density(dem_solver *s, const Ctl &c) {
     const int want = s->fc.dense ? (f >= 0.10 ? 1 : 0) : (f > 0.30 ? 1 : 0);
     if (want != s->fc.dense) {
         s->fc.dense = want;
+        pick_contact_kernel(s);
         s->version++;
     }
 }

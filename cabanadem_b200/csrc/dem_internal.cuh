@@ -67,6 +67,7 @@ __host__ __device__ __forceinline__ double2 load_mI(const Particles &P, int i) {
     return make_double2(P.mI[i], P.mI[(long)P.cap + i]);
 }
 
+constexpr int kCoopSlots = 32;   // largest MaxCnts the cooperative contact kernel stages in shared memory
 constexpr int kVmaxSlots = 32;   // blocks fold their max into slot blockIdx % 32 (word 32 * slot)
 
 struct PairConst {   // per (material a, material b) or (material a, wall w)
@@ -96,6 +97,8 @@ struct ForceConsts {
     int stream_block;          // k_stream block size: 64, 128 or 256
     int dense;                 // 1: most particles are in contact -- contact kernels compiled for
                                // more resident blocks, wider apply grid (same arithmetic)
+    int coop;                  // lanes per deferred particle in the contact kernel: 4 or 8
+                               // (cooperative, MaxCnts <= kCoopSlots), 0: one thread each
     const struct SceneConst *scenes;   // per-scene damping/friction, null: the scalars above
     int wps;                   // walls per scene (> 0 with scenes): scene s owns [s*wps, s*wps+wps)
 };
@@ -179,7 +182,7 @@ void launch_contact_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const 
                           const PairConst *pw, const WallGeom *walls, int blocks, cudaStream_t s);
 void launch_force_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
                         const PairConst *pw, const WallGeom *walls, cudaStream_t s);
-const void *contact_mixed_kernel(int dense);
+const void *contact_mixed_kernel(int dense, int coop);
 void launch_energy(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
                    const PairConst *pw, const WallGeom *walls, double *partials, int nparts, double *out,
                    cudaStream_t s);

@@ -7,6 +7,7 @@
 // stored in FP64, per-particle force sums and the velocity-Verlet update stay FP64.  The
 // streaming kernel (particles with no possible contact) is shared with the FP64 path.
 #include "dem_particle.cuh"
+#include "dem_contact_coop.cuh"
 
 namespace b200dem {
 
@@ -50,7 +51,11 @@ __global__ void __launch_bounds__(kBlock) k_force_mixed(Particles P, NbrList L, 
 
 void launch_contact_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
                           const PairConst *pw, const WallGeom *walls, int blocks, cudaStream_t s) {
-    if (fc.dense)
+    if (fc.coop == 8)
+        k_contact_coop<8, kCoopMinBlocks, true><<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+    else if (fc.coop == 4)
+        k_contact_coop<4, kCoopMinBlocks, true><<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+    else if (fc.dense)
         k_contact_mixed<kContactMixedMinBlocksDense><<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
     else
         k_contact_mixed<1><<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
@@ -61,7 +66,9 @@ void launch_force_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const Fo
     k_force_mixed<<<(P.n + kBlock - 1) / kBlock, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
 }
 
-const void *contact_mixed_kernel(int dense) {
+const void *contact_mixed_kernel(int dense, int coop) {
+    if (coop == 8) return (const void *)k_contact_coop<8, kCoopMinBlocks, true>;
+    if (coop == 4) return (const void *)k_contact_coop<4, kCoopMinBlocks, true>;
     return dense ? (const void *)k_contact_mixed<kContactMixedMinBlocksDense> : (const void *)k_contact_mixed<1>;
 }
 

@@ -19,6 +19,8 @@ constexpr int kBlock = 128;
 // 177 -> 133 us per step at 5 blocks, mixed 120 -> 99 us at 4; the 2M lattice loses 1-3 %).
 constexpr int kContactMinBlocksDense = 5;
 constexpr int kContactMixedMinBlocksDense = 4;
+// Resident blocks per SM of the cooperative contact kernel (register cap 128 at 128 threads).
+constexpr int kCoopMinBlocks = 4;
 constexpr int kApplyBlock = 256;
 
 struct __align__(32) D4 {
@@ -174,6 +176,342 @@ __device__ __forceinline__ void block_vmax(Ctl *ctl, unsigned long long *slots, 
 }
 
 
+// One particle-particle contact of i with partner j at overlap > 0 (Force.hpp:73-329): Hertz
+// normal force with damping, Mindlin tangential force with the Coulomb limit.  h is the
+// tangential history (in and out); cf receives the contribution to F (0..2) and tau (3..5) of i,
+// added by the caller in list order.  Shared by the per-thread and the cooperative contact
+// kernels, so both evaluate every expression identically.
+template <bool MIXED>
+__device__ __forceinline__ void pp_pair(const double *__restrict__ mrow, const double *__restrict__ vc,
+                                        const double *__restrict__ wc, const int cap, const unsigned q, const D4 &pi,
+                                        const D4 &pj, const int j, const double px, const double py, const double pz,
+                                        const double rij, const double overlap, const double ui0, const double ui1,
+                                        const double ui2, const double wi0, const double wi1, const double wi2,
+                                        const double m_i, const PairConst &c, const double K_n_pp,
+                                        const double K_t_pp, const double mu_pp, const double dt, double &h0,
+                                        double &h1, double &h2, double (&cf)[6]) {
+    if constexpr (MIXED) {
+        // Kinematics in FP64 (multiplies and adds only: the normal, the relative contact
+        // velocity and its normal/tangential split, where cancellation would cost FP32 its
+        // accuracy); force magnitudes -- square roots, divisions, x^1.5, Coulomb limit --
+        // in FP32; history accumulation and force sums in FP64.
+        const float ov = (float)overlap;
+        const double inv_r = 1.0 / rij;
+        const double dnx = px * inv_r, dny = py * inv_r, dnz = pz * inv_r;
+        const double da_i = pi.w - 0.5 * overlap, da_j = pj.w - 0.5 * overlap;
+        const double uj0 = vc[j];
+        const double uj1 = (q & DEM_Q1_VELJ_USES_UI) ? ui1 : vc[cap + j];
+        const double uj2 = (q & DEM_Q1_VELJ_USES_UI) ? ui2 : vc[2 * cap + j];
+        const double wj0 = wc[j], wj1 = wc[cap + j], wj2 = wc[2 * cap + j];
+        const double dv0 = (ui0 + (wi1 * dnz - wi2 * dny) * da_i) - (uj0 + (-wj1 * dnz + wj2 * dny) * da_j);
+        const double dv1 = (ui1 + (wi2 * dnx - wi0 * dnz) * da_i) - (uj1 + (-wj2 * dnx + wj0 * dnz) * da_j);
+        const double dv2 = (ui2 + (wi0 * dny - wi1 * dnx) * da_i) - (uj2 + (-wj0 * dny + wj1 * dnx) * da_j);
+        const double dvdn = dv0 * dnx + dv1 * dny + dv2 * dnz;
+        const float fnx = (float)dnx, fny = (float)dny, fnz = (float)dnz;
+        const float fa_i = (float)da_i;
+        const float ri = (float)pi.w, rj = (float)pj.w;
+        const float v0 = (float)dv0, v1 = (float)dv1, v2 = (float)dv2;
+        const float vdn = (float)dvdn;
+        const float vt0 = (float)(dv0 - dvdn * dnx), vt1 = (float)(dv1 - dvdn * dny), vt2 = (float)(dv2 - dvdn * dnz);
+        const float R_eff = 1.f / (1.f / ri + 1.f / rj);
+        const float m_eff = 1.f / (1.f / (float)m_i + 1.f / (float)mrow[j]);
+        const float sro = sqrtf(R_eff * ov);
+        const float kn = (float)c.c_kn * sqrtf(R_eff);
+        const float S_n = (float)c.c_Sn * sro;
+        const float eta_n = (float)K_n_pp * sqrtf(S_n * m_eff);
+        const float kt = (float)c.c_kt * sro;
+        const float eta_t = (float)K_t_pp * sqrtf(kt * m_eff);
+        const float fn = kn * ov * sqrtf(ov);
+        const float fn0 = fn * fnx - eta_n * (vdn * fnx);
+        const float fn1 = fn * fny - eta_n * (vdn * fny);
+        const float fn2 = fn * fnz - eta_n * (vdn * fnz);
+        float tf0 = 0.f, tf1 = 0.f, tf2 = 0.f;
+        const float vij_magn = sqrtf(v0 * v0 + v1 * v1 + v2 * v2);
+        if (vij_magn < 1e-12f) {
+            h0 = 0.;
+            h1 = 0.;
+            h2 = 0.;
+        } else {
+            const float ti_magn = sqrtf(vt0 * vt0 + vt1 * vt1 + vt2 * vt2);
+            float ti0 = 0.f, ti1 = 0.f, ti2 = 0.f;
+            if (ti_magn > 1e-12f) {
+                const float inv_t = 1.f / ti_magn;
+                ti0 = vt0 * inv_t;
+                ti1 = vt1 * inv_t;
+                ti2 = vt2 * inv_t;
+            }
+            const double dl0 = h0 + dv0 * dt, dl1 = h1 + dv1 * dt, dl2 = h2 + dv2 * dt;
+            const double dld = dl0 * (double)ti0 + dl1 * (double)ti1 + dl2 * (double)ti2;
+            h0 = dld * (double)ti0;
+            h1 = dld * (double)ti1;
+            h2 = dld * (double)ti2;
+            const float ft0 = -kt * (float)h0 - eta_t * vt0;
+            const float ft1 = -kt * (float)h1 - eta_t * vt1;
+            const float ft2 = -kt * (float)h2 - eta_t * vt2;
+            const float ft_magn = sqrtf(ft0 * ft0 + ft1 * ft1 + ft2 * ft2);
+            const float fn_magn = sqrtf(fn0 * fn0 + fn1 * fn1 + fn2 * fn2);
+            const float lim = (float)mu_pp * fn_magn;
+            const float fms = ft_magn > lim ? lim : ft_magn;
+            tf0 = -fms * ti0;
+            tf1 = -fms * ti1;
+            tf2 = -fms * ti2;
+            const float md0 = -tf0 / kt, md1 = -tf1 / kt, md2 = -tf2 / kt;
+            if (q & DEM_Q4_UNIT_HISTORY) {
+                const float lt = sqrtf(md0 * md0 + md1 * md1 + md2 * md2);
+                if (lt > 1e-12f) {
+                    h0 = (double)(md0 / lt);
+                    h1 = (double)(md1 / lt);
+                    h2 = (double)(md2 / lt);
+                } else {
+                    h0 = 0.;
+                    h1 = 0.;
+                    h2 = 0.;
+                }
+            } else {
+                h0 = (double)md0;
+                h1 = (double)md1;
+                h2 = (double)md2;
+            }
+        }
+        cf[0] = (double)(fn0 + tf0);
+        cf[1] = (double)(fn1 + tf1);
+        cf[2] = (double)(fn2 + tf2);
+        cf[3] = (double)((fny * tf2 - fnz * tf1) * fa_i);
+        cf[4] = (double)((fnz * tf0 - fnx * tf2) * fa_i);
+        cf[5] = (double)((fnx * tf1 - fny * tf0) * fa_i);
+    } else {
+        const double a_i = pi.w - overlap / 2.;
+        const double a_j = pj.w - overlap / 2.;
+        const double nx = px / rij, ny = py / rij, nz = pz / rij;
+        const double uj0 = vc[j];
+        const double uj1 = (q & DEM_Q1_VELJ_USES_UI) ? ui1 : vc[cap + j];
+        const double uj2 = (q & DEM_Q1_VELJ_USES_UI) ? ui2 : vc[2 * cap + j];
+        const double wj0 = wc[j], wj1 = wc[cap + j], wj2 = wc[2 * cap + j];
+        const double vi0 = ui0 + (wi1 * nz - wi2 * ny) * a_i;
+        const double vi1 = ui1 + (wi2 * nx - wi0 * nz) * a_i;
+        const double vi2 = ui2 + (wi0 * ny - wi1 * nx) * a_i;
+        const double vj0 = uj0 + (-wj1 * nz + wj2 * ny) * a_j;
+        const double vj1 = uj1 + (-wj2 * nx + wj0 * nz) * a_j;
+        const double vj2 = uj2 + (-wj0 * ny + wj1 * nx) * a_j;
+        const double v0 = vi0 - vj0, v1 = vi1 - vj1, v2 = vi2 - vj2;
+        const double vdn = v0 * nx + v1 * ny + v2 * nz;
+        const double vn0 = vdn * nx, vn1 = vdn * ny, vn2 = vdn * nz;
+        const double vt0 = v0 - vn0, vt1 = v1 - vn1, vt2 = v2 - vn2;
+        const double tmp_3 = 1. / pi.w;
+        const double tmp_4 = 1. / pj.w;
+        const double R_eff = 1. / (tmp_3 + tmp_4);
+        const double kn = c.c_kn * sqrt(R_eff);
+        const double S_n = c.c_Sn * sqrt(R_eff * overlap);
+        const double m_eff = 1. / (1. / m_i + 1. / mrow[j]);
+        const double eta_n = K_n_pp * sqrt(S_n * m_eff);
+        const double kt = c.c_kt * sqrt(R_eff * overlap);
+        const double eta_t = K_t_pp * sqrt(kt * m_eff);
+        const double fn = kn * (overlap * sqrt(overlap));
+        const double fn0 = fn * nx - eta_n * vn0;
+        const double fn1 = fn * ny - eta_n * vn1;
+        const double fn2 = fn * nz - eta_n * vn2;
+        double tf0 = 0., tf1 = 0., tf2 = 0.;
+        const double vij_magn = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+        if (vij_magn < 1e-12) {
+            h0 = 0.;
+            h1 = 0.;
+            h2 = 0.;
+        } else {
+            const double tx = v0 - nx * vdn, ty = v1 - ny * vdn, tz = v2 - nz * vdn;
+            const double ti_magn = sqrt(tx * tx + ty * ty + tz * tz);
+            double ti0 = 0., ti1 = 0., ti2 = 0.;
+            if (ti_magn > 1e-12) {
+                ti0 = tx / ti_magn;
+                ti1 = ty / ti_magn;
+                ti2 = tz / ti_magn;
+            }
+            const double dl0 = h0 + v0 * dt, dl1 = h1 + v1 * dt, dl2 = h2 + v2 * dt;
+            const double dld = (dl0 * ti0 + dl1 * ti1 + dl2 * ti2);
+            h0 = dld * ti0;
+            h1 = dld * ti1;
+            h2 = dld * ti2;
+            const double ft0 = -kt * h0 - eta_t * vt0;
+            const double ft1 = -kt * h1 - eta_t * vt1;
+            const double ft2 = -kt * h2 - eta_t * vt2;
+            const double ft_magn = sqrt(ft0 * ft0 + ft1 * ft1 + ft2 * ft2);
+            const double fn_magn = sqrt(fn0 * fn0 + fn1 * fn1 + fn2 * fn2);
+            double fms = ft_magn;
+            if (fms > mu_pp * fn_magn) fms = mu_pp * fn_magn;
+            tf0 = -fms * ti0;
+            tf1 = -fms * ti1;
+            tf2 = -fms * ti2;
+            const double md0 = -tf0 / kt, md1 = -tf1 / kt, md2 = -tf2 / kt;
+            if (q & DEM_Q4_UNIT_HISTORY) {
+                const double lt = sqrt(md0 * md0 + md1 * md1 + md2 * md2);
+                if (lt > 1e-12) {
+                    h0 = md0 / lt;
+                    h1 = md1 / lt;
+                    h2 = md2 / lt;
+                } else {
+                    h0 = 0.;
+                    h1 = 0.;
+                    h2 = 0.;
+                }
+            } else {
+                h0 = md0;
+                h1 = md1;
+                h2 = md2;
+            }
+        }
+        cf[0] = fn0 + tf0;
+        cf[1] = fn1 + tf1;
+        cf[2] = fn2 + tf2;
+        cf[3] = (ny * tf2 - nz * tf1) * a_i;
+        cf[4] = (nz * tf0 - nx * tf2) * a_i;
+        cf[5] = (nx * tf1 - ny * tf0) * a_i;
+    }
+}
+
+// One particle-wall contact at overlap > 0 (Force.hpp:475-673): forces of the infinite wall with
+// normal (nx, ny, nz) on i, the wall history (swx, swy, swz) read when has_hist and written;
+// cf as for pp_pair.
+template <bool MIXED>
+__device__ __forceinline__ void pw_wall(const unsigned q, const D4 &pi, const double nx, const double ny,
+                                        const double nz, const double overlap, const double ui0, const double ui1,
+                                        const double ui2, const double wi0, const double wi1, const double wi2,
+                                        const double m_i, const PairConst &c, const double K_n_pw,
+                                        const double K_t_pw, const double mu_pw, const double dt,
+                                        const bool has_hist, double *swx, double *swy, double *swz,
+                                        double (&cf)[6]) {
+    if constexpr (MIXED) {
+        const float ov = (float)overlap;
+        const double da_i = pi.w - 0.5 * overlap;
+        const double dv0 = ui0 + (wi1 * nz - wi2 * ny) * da_i;
+        const double dv1 = ui1 + (wi2 * nx - wi0 * nz) * da_i;
+        const double dv2 = ui2 + (wi0 * ny - wi1 * nx) * da_i;
+        const double dvdn = dv0 * nx + dv1 * ny + dv2 * nz;
+        const float fa_i = (float)da_i;
+        const float gx = (float)nx, gy = (float)ny, gz = (float)nz;
+        const float v0 = (float)dv0, v1 = (float)dv1, v2 = (float)dv2;
+        const float vdn = (float)dvdn;
+        const float vt0 = (float)(dv0 - dvdn * nx), vt1 = (float)(dv1 - dvdn * ny), vt2 = (float)(dv2 - dvdn * nz);
+        const float R_eff = (float)pi.w;
+        const float m_eff = (float)m_i;
+        const float sro = sqrtf(R_eff * ov);
+        const float kn = (float)c.c_kn * sqrtf(R_eff);
+        const float S_n = (float)c.c_Sn * sro;
+        const float eta_n = (float)K_n_pw * sqrtf(S_n * m_eff);
+        const float fn = kn * ov * sqrtf(ov);
+        const float fn0 = fn * gx - eta_n * (vdn * gx);
+        const float fn1 = fn * gy - eta_n * (vdn * gy);
+        const float fn2 = fn * gz - eta_n * (vdn * gz);
+        float ft0 = 0.f, ft1 = 0.f, ft2 = 0.f;
+        const float vij_magn = sqrtf(v0 * v0 + v1 * v1 + v2 * v2);
+        if (vij_magn < 1e-12f) {
+            *swx = 0.;
+            *swy = 0.;
+            *swz = 0.;
+        } else {
+            double s0 = 0., s1 = 0., s2 = 0.;
+            if (has_hist) {
+                s0 = *swx;
+                s1 = *swy;
+                s2 = *swz;
+            }
+            s0 += (dv0 - dvdn * nx) * dt;
+            s1 += (dv1 - dvdn * ny) * dt;
+            s2 += (dv2 - dvdn * nz) * dt;
+            const float kt = (float)c.c_kt * sro;
+            const float eta_t = (float)K_t_pw * sqrtf(kt * m_eff);
+            const float fx = -kt * (float)s0 - eta_t * vt0;
+            const float fy = -kt * (float)s1 - eta_t * vt1;
+            const float fz = -kt * (float)s2 - eta_t * vt2;
+            const float ft_magn = (q & DEM_Q5_WALL_FT_TYPO) ? sqrtf(fx * fx + fy * fy + fz * fy)
+                                                             : sqrtf(fx * fx + fy * fy + fz * fz);
+            float ti0 = 0.f, ti1 = 0.f, ti2 = 0.f;
+            if (ft_magn > 1e-12f) {
+                ti0 = fx / ft_magn;
+                ti1 = fy / ft_magn;
+                ti2 = fz / ft_magn;
+            }
+            const float fn_magn = sqrtf(fn0 * fn0 + fn1 * fn1 + fn2 * fn2);
+            const float lim = (float)mu_pw * fn_magn;
+            const float fms = (ft_magn < lim) ? ft_magn : lim;
+            ft0 = fms * ti0 + eta_t * vt0;
+            ft1 = fms * ti1 + eta_t * vt1;
+            ft2 = fms * ti2 + eta_t * vt2;
+            *swx = (double)(-ft0 / kt);
+            *swy = (double)(-ft1 / kt);
+            *swz = (double)(-ft2 / kt);
+        }
+        cf[0] = (double)(fn0 + ft0);
+        cf[1] = (double)(fn1 + ft1);
+        cf[2] = (double)(fn2 + ft2);
+        cf[3] = (double)((gy * ft2 - gz * ft1) * fa_i);
+        cf[4] = (double)((gz * ft0 - gx * ft2) * fa_i);
+        cf[5] = (double)((gx * ft1 - gy * ft0) * fa_i);
+    } else {
+        const double a_i = pi.w - overlap / 2.;
+        const double v0 = ui0 + (wi1 * nz - wi2 * ny) * a_i;
+        const double v1 = ui1 + (wi2 * nx - wi0 * nz) * a_i;
+        const double v2 = ui2 + (wi0 * ny - wi1 * nx) * a_i;
+        const double vdn = v0 * nx + v1 * ny + v2 * nz;
+        const double vt0 = v0 - vdn * nx, vt1 = v1 - vdn * ny, vt2 = v2 - vdn * nz;
+        const double R_eff = 1. / (1. / pi.w + 0.);
+        const double kn = c.c_kn * sqrt(R_eff);
+        const double S_n = c.c_Sn * sqrt(R_eff * overlap);
+        const double m_eff = 1. / (1. / m_i + 0.);
+        const double eta_n = K_n_pw * sqrt(S_n * m_eff);
+        const double fn = kn * (overlap * sqrt(overlap));
+        const double fn0 = fn * nx - eta_n * (vdn * nx);
+        const double fn1 = fn * ny - eta_n * (vdn * ny);
+        const double fn2 = fn * nz - eta_n * (vdn * nz);
+        double ft0 = 0., ft1 = 0., ft2 = 0.;
+        const double vij_magn = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+        if (vij_magn < 1e-12) {
+            *swx = 0.;
+            *swy = 0.;
+            *swz = 0.;
+        } else {
+            double s0 = 0., s1 = 0., s2 = 0.;
+            if (has_hist) {
+                s0 = *swx;
+                s1 = *swy;
+                s2 = *swz;
+            }
+            s0 += vt0 * dt;
+            s1 += vt1 * dt;
+            s2 += vt2 * dt;
+            const double kt = c.c_kt * sqrt(R_eff * overlap);
+            const double eta_t = K_t_pw * sqrt(kt * m_eff);
+            const double fx = -kt * s0 - eta_t * vt0;
+            const double fy = -kt * s1 - eta_t * vt1;
+            const double fz = -kt * s2 - eta_t * vt2;
+            const double ft_magn = (q & DEM_Q5_WALL_FT_TYPO) ? sqrt(fx * fx + fy * fy + fz * fy)
+                                                              : sqrt(fx * fx + fy * fy + fz * fz);
+            double ti0 = 0., ti1 = 0., ti2 = 0.;
+            if (ft_magn > 1e-12) {
+                ti0 = fx / ft_magn;
+                ti1 = fy / ft_magn;
+                ti2 = fz / ft_magn;
+            }
+            const double fn_magn = sqrt(fn0 * fn0 + fn1 * fn1 + fn2 * fn2);
+            const double lim = mu_pw * fn_magn;
+            const double fms = (ft_magn < lim) ? ft_magn : lim;  // std::min(lim, ft_magn)
+            ft0 = fms * ti0;
+            ft1 = fms * ti1;
+            ft2 = fms * ti2;
+            ft0 += eta_t * vt0;
+            ft1 += eta_t * vt1;
+            ft2 += eta_t * vt2;
+            *swx = -ft0 / kt;
+            *swy = -ft1 / kt;
+            *swz = -ft2 / kt;
+        }
+        cf[0] = fn0 + ft0;
+        cf[1] = fn1 + ft1;
+        cf[2] = fn2 + ft2;
+        cf[3] = (ny * ft2 - nz * ft1) * a_i;
+        cf[4] = (nz * ft0 - nx * ft2) * a_i;
+        cf[5] = (nx * ft1 - ny * ft0) * a_i;
+    }
+}
+
 // ---------------------------------------------------------------------------------------
 // Full per-particle step (contact compaction, pp and wall forces, hooks, integration).
 // MODE_FORCE_ONLY writes F and tau in place and leaves x, u, omega untouched (the
@@ -280,23 +618,6 @@ __device__ __forceinline__ void particle_full(const Particles &P, const NbrList 
         const double rij = sqrt(r2ij);
         const double overlap = sr - rij;
         if (!(overlap > 0.)) continue;
-        const double a_i = pi.w - overlap / 2.;
-        const double a_j = pj.w - overlap / 2.;
-        const double nx = px / rij, ny = py / rij, nz = pz / rij;
-        const double uj0 = vc[j];
-        const double uj1 = (q & DEM_Q1_VELJ_USES_UI) ? ui1 : vc[cap + j];
-        const double uj2 = (q & DEM_Q1_VELJ_USES_UI) ? ui2 : vc[2 * cap + j];
-        const double wj0 = wc[j], wj1 = wc[cap + j], wj2 = wc[2 * cap + j];
-        const double vi0 = ui0 + (wi1 * nz - wi2 * ny) * a_i;
-        const double vi1 = ui1 + (wi2 * nx - wi0 * nz) * a_i;
-        const double vi2 = ui2 + (wi0 * ny - wi1 * nx) * a_i;
-        const double vj0 = uj0 + (-wj1 * nz + wj2 * ny) * a_j;
-        const double vj1 = uj1 + (-wj2 * nx + wj0 * nz) * a_j;
-        const double vj2 = uj2 + (-wj0 * ny + wj1 * nx) * a_j;
-        const double v0 = vi0 - vj0, v1 = vi1 - vj1, v2 = vi2 - vj2;
-        const double vdn = v0 * nx + v1 * ny + v2 * nz;
-        const double vn0 = vdn * nx, vn1 = vdn * ny, vn2 = vdn * nz;
-        const double vt0 = v0 - vn0, vt1 = v1 - vn1, vt2 = v2 - vn2;
         // slot lookup / insert (Force.hpp:166-192)
         int found_at = -1;
         for (int s = 0; s < cnt; ++s)
@@ -322,179 +643,22 @@ __device__ __forceinline__ void particle_full(const Particles &P, const NbrList 
         }
         const int mj = fc.nmat > 1 ? (int)P.mat[j] : 0;
         const PairConst c = pp[mi * fc.nmat + mj];
-        if constexpr (MIXED) {
-            // Kinematics in FP64 (multiplies and adds only: the normal, the relative contact
-            // velocity and its normal/tangential split, where cancellation would cost FP32 its
-            // accuracy); force magnitudes -- square roots, divisions, x^1.5, Coulomb limit --
-            // in FP32; history accumulation and force sums in FP64.
-            const float ov = (float)overlap;
-            const double inv_r = 1.0 / rij;
-            const double dnx = px * inv_r, dny = py * inv_r, dnz = pz * inv_r;
-            const double da_i = pi.w - 0.5 * overlap, da_j = pj.w - 0.5 * overlap;
-            const double uj0 = vc[j];
-            const double uj1 = (q & DEM_Q1_VELJ_USES_UI) ? ui1 : vc[cap + j];
-            const double uj2 = (q & DEM_Q1_VELJ_USES_UI) ? ui2 : vc[2 * cap + j];
-            const double wj0 = wc[j], wj1 = wc[cap + j], wj2 = wc[2 * cap + j];
-            const double dv0 = (ui0 + (wi1 * dnz - wi2 * dny) * da_i) - (uj0 + (-wj1 * dnz + wj2 * dny) * da_j);
-            const double dv1 = (ui1 + (wi2 * dnx - wi0 * dnz) * da_i) - (uj1 + (-wj2 * dnx + wj0 * dnz) * da_j);
-            const double dv2 = (ui2 + (wi0 * dny - wi1 * dnx) * da_i) - (uj2 + (-wj0 * dny + wj1 * dnx) * da_j);
-            const double dvdn = dv0 * dnx + dv1 * dny + dv2 * dnz;
-            const float fnx = (float)dnx, fny = (float)dny, fnz = (float)dnz;
-            const float fa_i = (float)da_i;
-            const float ri = (float)pi.w, rj = (float)pj.w;
-            const float v0 = (float)dv0, v1 = (float)dv1, v2 = (float)dv2;
-            const float vdn = (float)dvdn;
-            const float vt0 = (float)(dv0 - dvdn * dnx), vt1 = (float)(dv1 - dvdn * dny), vt2 = (float)(dv2 - dvdn * dnz);
-            const float R_eff = 1.f / (1.f / ri + 1.f / rj);
-            const float m_eff = 1.f / (1.f / (float)mIi.x + 1.f / (float)P.mI[j]);
-            const float sro = sqrtf(R_eff * ov);
-            const float kn = (float)c.c_kn * sqrtf(R_eff);
-            const float S_n = (float)c.c_Sn * sro;
-            const float eta_n = (float)K_n_pp * sqrtf(S_n * m_eff);
-            const float kt = (float)c.c_kt * sro;
-            const float eta_t = (float)K_t_pp * sqrtf(kt * m_eff);
-            const float fn = kn * ov * sqrtf(ov);
-            const float fn0 = fn * fnx - eta_n * (vdn * fnx);
-            const float fn1 = fn * fny - eta_n * (vdn * fny);
-            const float fn2 = fn * fnz - eta_n * (vdn * fnz);
-            float tf0 = 0.f, tf1 = 0.f, tf2 = 0.f;
-            const float vij_magn = sqrtf(v0 * v0 + v1 * v1 + v2 * v2);
-            if (vij_magn < 1e-12f) {
-                h0 = 0.;
-                h1 = 0.;
-                h2 = 0.;
-            } else {
-                const float ti_magn = sqrtf(vt0 * vt0 + vt1 * vt1 + vt2 * vt2);
-                float ti0 = 0.f, ti1 = 0.f, ti2 = 0.f;
-                if (ti_magn > 1e-12f) {
-                    const float inv_t = 1.f / ti_magn;
-                    ti0 = vt0 * inv_t;
-                    ti1 = vt1 * inv_t;
-                    ti2 = vt2 * inv_t;
-                }
-                const double dl0 = h0 + dv0 * fc.dt, dl1 = h1 + dv1 * fc.dt, dl2 = h2 + dv2 * fc.dt;
-                const double dld = dl0 * (double)ti0 + dl1 * (double)ti1 + dl2 * (double)ti2;
-                h0 = dld * (double)ti0;
-                h1 = dld * (double)ti1;
-                h2 = dld * (double)ti2;
-                const float ft0 = -kt * (float)h0 - eta_t * vt0;
-                const float ft1 = -kt * (float)h1 - eta_t * vt1;
-                const float ft2 = -kt * (float)h2 - eta_t * vt2;
-                const float ft_magn = sqrtf(ft0 * ft0 + ft1 * ft1 + ft2 * ft2);
-                const float fn_magn = sqrtf(fn0 * fn0 + fn1 * fn1 + fn2 * fn2);
-                const float lim = (float)mu_pp * fn_magn;
-                const float fms = ft_magn > lim ? lim : ft_magn;
-                tf0 = -fms * ti0;
-                tf1 = -fms * ti1;
-                tf2 = -fms * ti2;
-                const float md0 = -tf0 / kt, md1 = -tf1 / kt, md2 = -tf2 / kt;
-                if (q & DEM_Q4_UNIT_HISTORY) {
-                    const float lt = sqrtf(md0 * md0 + md1 * md1 + md2 * md2);
-                    if (lt > 1e-12f) {
-                        h0 = (double)(md0 / lt);
-                        h1 = (double)(md1 / lt);
-                        h2 = (double)(md2 / lt);
-                    } else {
-                        h0 = 0.;
-                        h1 = 0.;
-                        h2 = 0.;
-                    }
-                } else {
-                    h0 = (double)md0;
-                    h1 = (double)md1;
-                    h2 = (double)md2;
-                }
-            }
-            if (found_at >= 0) {
-                const long a = (long)found_at * cap;
-                thx[a] = h0;
-                thy[a] = h1;
-                thz[a] = h2;
-            }
-            F0 += (double)(fn0 + tf0);
-            F1 += (double)(fn1 + tf1);
-            F2 += (double)(fn2 + tf2);
-            if (!(q & DEM_Q3_NO_PP_TORQUE)) {
-                T0 += (double)((fny * tf2 - fnz * tf1) * fa_i);
-                T1 += (double)((fnz * tf0 - fnx * tf2) * fa_i);
-                T2 += (double)((fnx * tf1 - fny * tf0) * fa_i);
-            }
-            continue;
-        }
-        const double tmp_3 = 1. / pi.w;
-        const double tmp_4 = 1. / pj.w;
-        const double R_eff = 1. / (tmp_3 + tmp_4);
-        const double kn = c.c_kn * sqrt(R_eff);
-        const double S_n = c.c_Sn * sqrt(R_eff * overlap);
-        const double m_eff = 1. / (1. / mIi.x + 1. / P.mI[j]);
-        const double eta_n = K_n_pp * sqrt(S_n * m_eff);
-        const double kt = c.c_kt * sqrt(R_eff * overlap);
-        const double eta_t = K_t_pp * sqrt(kt * m_eff);
-        const double fn = kn * (overlap * sqrt(overlap));
-        const double fn0 = fn * nx - eta_n * vn0;
-        const double fn1 = fn * ny - eta_n * vn1;
-        const double fn2 = fn * nz - eta_n * vn2;
-        double tf0 = 0., tf1 = 0., tf2 = 0.;
-        const double vij_magn = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
-        if (vij_magn < 1e-12) {
-            h0 = 0.;
-            h1 = 0.;
-            h2 = 0.;
-        } else {
-            const double tx = v0 - nx * vdn, ty = v1 - ny * vdn, tz = v2 - nz * vdn;
-            const double ti_magn = sqrt(tx * tx + ty * ty + tz * tz);
-            double ti0 = 0., ti1 = 0., ti2 = 0.;
-            if (ti_magn > 1e-12) {
-                ti0 = tx / ti_magn;
-                ti1 = ty / ti_magn;
-                ti2 = tz / ti_magn;
-            }
-            const double dl0 = h0 + v0 * fc.dt, dl1 = h1 + v1 * fc.dt, dl2 = h2 + v2 * fc.dt;
-            const double dld = (dl0 * ti0 + dl1 * ti1 + dl2 * ti2);
-            h0 = dld * ti0;
-            h1 = dld * ti1;
-            h2 = dld * ti2;
-            const double ft0 = -kt * h0 - eta_t * vt0;
-            const double ft1 = -kt * h1 - eta_t * vt1;
-            const double ft2 = -kt * h2 - eta_t * vt2;
-            const double ft_magn = sqrt(ft0 * ft0 + ft1 * ft1 + ft2 * ft2);
-            const double fn_magn = sqrt(fn0 * fn0 + fn1 * fn1 + fn2 * fn2);
-            double fms = ft_magn;
-            if (fms > mu_pp * fn_magn) fms = mu_pp * fn_magn;
-            tf0 = -fms * ti0;
-            tf1 = -fms * ti1;
-            tf2 = -fms * ti2;
-            const double md0 = -tf0 / kt, md1 = -tf1 / kt, md2 = -tf2 / kt;
-            if (q & DEM_Q4_UNIT_HISTORY) {
-                const double lt = sqrt(md0 * md0 + md1 * md1 + md2 * md2);
-                if (lt > 1e-12) {
-                    h0 = md0 / lt;
-                    h1 = md1 / lt;
-                    h2 = md2 / lt;
-                } else {
-                    h0 = 0.;
-                    h1 = 0.;
-                    h2 = 0.;
-                }
-            } else {
-                h0 = md0;
-                h1 = md1;
-                h2 = md2;
-            }
-        }
+        double cf[6];
+        pp_pair<MIXED>(P.mI, vc, wc, cap, q, pi, pj, j, px, py, pz, rij, overlap, ui0, ui1, ui2, wi0, wi1, wi2, mIi.x, c,
+                       K_n_pp, K_t_pp, mu_pp, fc.dt, h0, h1, h2, cf);
         if (found_at >= 0) {
             const long a = (long)found_at * cap;
             thx[a] = h0;
             thy[a] = h1;
             thz[a] = h2;
         }
-        F0 += fn0 + tf0;
-        F1 += fn1 + tf1;
-        F2 += fn2 + tf2;
+        F0 += cf[0];
+        F1 += cf[1];
+        F2 += cf[2];
         if (!(q & DEM_Q3_NO_PP_TORQUE)) {
-            T0 += (ny * tf2 - nz * tf1) * a_i;
-            T1 += (nz * tf0 - nx * tf2) * a_i;
-            T2 += (nx * tf1 - ny * tf0) * a_i;
+            T0 += cf[3];
+            T1 += cf[4];
+            T2 += cf[5];
         }
     }
     // ---- particle-infinite wall (Force.hpp:475-673)
@@ -509,141 +673,17 @@ __device__ __forceinline__ void particle_full(const Particles &P, const NbrList 
         double *swx = P.sw + (long)lw * cap + i;
         double *swy = P.sw + (long)(P.mw + lw) * cap + i;
         double *swz = P.sw + (long)(2 * P.mw + lw) * cap + i;
-        if (MIXED && overlap > 0.) {
-            const float ov = (float)overlap;
-            const double da_i = pi.w - 0.5 * overlap;
-            const double dv0 = ui0 + (wi1 * nz - wi2 * ny) * da_i;
-            const double dv1 = ui1 + (wi2 * nx - wi0 * nz) * da_i;
-            const double dv2 = ui2 + (wi0 * ny - wi1 * nx) * da_i;
-            const double dvdn = dv0 * nx + dv1 * ny + dv2 * nz;
-            const float fa_i = (float)da_i;
-            const float gx = (float)nx, gy = (float)ny, gz = (float)nz;
-            const float v0 = (float)dv0, v1 = (float)dv1, v2 = (float)dv2;
-            const float vdn = (float)dvdn;
-            const float vt0 = (float)(dv0 - dvdn * nx), vt1 = (float)(dv1 - dvdn * ny), vt2 = (float)(dv2 - dvdn * nz);
-            const PairConst c = pw[mi * fc.nwall + w];
-            const float R_eff = (float)pi.w;
-            const float m_eff = (float)mIi.x;
-            const float sro = sqrtf(R_eff * ov);
-            const float kn = (float)c.c_kn * sqrtf(R_eff);
-            const float S_n = (float)c.c_Sn * sro;
-            const float eta_n = (float)K_n_pw * sqrtf(S_n * m_eff);
-            const float fn = kn * ov * sqrtf(ov);
-            const float fn0 = fn * gx - eta_n * (vdn * gx);
-            const float fn1 = fn * gy - eta_n * (vdn * gy);
-            const float fn2 = fn * gz - eta_n * (vdn * gz);
-            float ft0 = 0.f, ft1 = 0.f, ft2 = 0.f;
-            const float vij_magn = sqrtf(v0 * v0 + v1 * v1 + v2 * v2);
-            if (vij_magn < 1e-12f) {
-                *swx = 0.;
-                *swy = 0.;
-                *swz = 0.;
-            } else {
-                double s0 = 0., s1 = 0., s2 = 0.;
-                if (wmask & bit) {
-                    s0 = *swx;
-                    s1 = *swy;
-                    s2 = *swz;
-                }
-                s0 += (dv0 - dvdn * nx) * fc.dt;
-                s1 += (dv1 - dvdn * ny) * fc.dt;
-                s2 += (dv2 - dvdn * nz) * fc.dt;
-                const float kt = (float)c.c_kt * sro;
-                const float eta_t = (float)K_t_pw * sqrtf(kt * m_eff);
-                const float fx = -kt * (float)s0 - eta_t * vt0;
-                const float fy = -kt * (float)s1 - eta_t * vt1;
-                const float fz = -kt * (float)s2 - eta_t * vt2;
-                const float ft_magn = (q & DEM_Q5_WALL_FT_TYPO) ? sqrtf(fx * fx + fy * fy + fz * fy)
-                                                                 : sqrtf(fx * fx + fy * fy + fz * fz);
-                float ti0 = 0.f, ti1 = 0.f, ti2 = 0.f;
-                if (ft_magn > 1e-12f) {
-                    ti0 = fx / ft_magn;
-                    ti1 = fy / ft_magn;
-                    ti2 = fz / ft_magn;
-                }
-                const float fn_magn = sqrtf(fn0 * fn0 + fn1 * fn1 + fn2 * fn2);
-                const float lim = (float)mu_pw * fn_magn;
-                const float fms = (ft_magn < lim) ? ft_magn : lim;
-                ft0 = fms * ti0 + eta_t * vt0;
-                ft1 = fms * ti1 + eta_t * vt1;
-                ft2 = fms * ti2 + eta_t * vt2;
-                *swx = (double)(-ft0 / kt);
-                *swy = (double)(-ft1 / kt);
-                *swz = (double)(-ft2 / kt);
-            }
+        if (overlap > 0.) {
+            double cf[6];
+            pw_wall<MIXED>(q, pi, nx, ny, nz, overlap, ui0, ui1, ui2, wi0, wi1, wi2, mIi.x, pw[mi * fc.nwall + w], K_n_pw,
+                           K_t_pw, mu_pw, fc.dt, (wmask & bit) != 0u, swx, swy, swz, cf);
             wmask |= bit;
-            F0 += (double)(fn0 + ft0);
-            F1 += (double)(fn1 + ft1);
-            F2 += (double)(fn2 + ft2);
-            T0 += (double)((gy * ft2 - gz * ft1) * fa_i);
-            T1 += (double)((gz * ft0 - gx * ft2) * fa_i);
-            T2 += (double)((gx * ft1 - gy * ft0) * fa_i);
-        } else if (overlap > 0.) {
-            const double a_i = pi.w - overlap / 2.;
-            const double v0 = ui0 + (wi1 * nz - wi2 * ny) * a_i;
-            const double v1 = ui1 + (wi2 * nx - wi0 * nz) * a_i;
-            const double v2 = ui2 + (wi0 * ny - wi1 * nx) * a_i;
-            const double vdn = v0 * nx + v1 * ny + v2 * nz;
-            const double vt0 = v0 - vdn * nx, vt1 = v1 - vdn * ny, vt2 = v2 - vdn * nz;
-            const PairConst c = pw[mi * fc.nwall + w];
-            const double R_eff = 1. / (1. / pi.w + 0.);
-            const double kn = c.c_kn * sqrt(R_eff);
-            const double S_n = c.c_Sn * sqrt(R_eff * overlap);
-            const double m_eff = 1. / (1. / mIi.x + 0.);
-            const double eta_n = K_n_pw * sqrt(S_n * m_eff);
-            const double fn = kn * (overlap * sqrt(overlap));
-            const double fn0 = fn * nx - eta_n * (vdn * nx);
-            const double fn1 = fn * ny - eta_n * (vdn * ny);
-            const double fn2 = fn * nz - eta_n * (vdn * nz);
-            double ft0 = 0., ft1 = 0., ft2 = 0.;
-            const double vij_magn = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
-            if (vij_magn < 1e-12) {
-                *swx = 0.;
-                *swy = 0.;
-                *swz = 0.;
-            } else {
-                double s0 = 0., s1 = 0., s2 = 0.;
-                if (wmask & bit) {
-                    s0 = *swx;
-                    s1 = *swy;
-                    s2 = *swz;
-                }
-                s0 += vt0 * fc.dt;
-                s1 += vt1 * fc.dt;
-                s2 += vt2 * fc.dt;
-                const double kt = c.c_kt * sqrt(R_eff * overlap);
-                const double eta_t = K_t_pw * sqrt(kt * m_eff);
-                const double fx = -kt * s0 - eta_t * vt0;
-                const double fy = -kt * s1 - eta_t * vt1;
-                const double fz = -kt * s2 - eta_t * vt2;
-                const double ft_magn = (q & DEM_Q5_WALL_FT_TYPO) ? sqrt(fx * fx + fy * fy + fz * fy)
-                                                                  : sqrt(fx * fx + fy * fy + fz * fz);
-                double ti0 = 0., ti1 = 0., ti2 = 0.;
-                if (ft_magn > 1e-12) {
-                    ti0 = fx / ft_magn;
-                    ti1 = fy / ft_magn;
-                    ti2 = fz / ft_magn;
-                }
-                const double fn_magn = sqrt(fn0 * fn0 + fn1 * fn1 + fn2 * fn2);
-                const double lim = mu_pw * fn_magn;
-                const double fms = (ft_magn < lim) ? ft_magn : lim;  // std::min(lim, ft_magn)
-                ft0 = fms * ti0;
-                ft1 = fms * ti1;
-                ft2 = fms * ti2;
-                ft0 += eta_t * vt0;
-                ft1 += eta_t * vt1;
-                ft2 += eta_t * vt2;
-                *swx = -ft0 / kt;
-                *swy = -ft1 / kt;
-                *swz = -ft2 / kt;
-            }
-            wmask |= bit;
-            F0 += fn0 + ft0;
-            F1 += fn1 + ft1;
-            F2 += fn2 + ft2;
-            T0 += (ny * ft2 - nz * ft1) * a_i;
-            T1 += (nz * ft0 - nx * ft2) * a_i;
-            T2 += (nx * ft1 - ny * ft0) * a_i;
+            F0 += cf[0];
+            F1 += cf[1];
+            F2 += cf[2];
+            T0 += cf[3];
+            T1 += cf[4];
+            T2 += cf[5];
         } else if (wmask & bit) {
             *swx = 0.;
             *swy = 0.;

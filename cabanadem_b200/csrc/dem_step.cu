@@ -16,6 +16,7 @@
 #include "b200dem.h"
 
 #include "dem_particle.cuh"
+#include "dem_contact_coop.cuh"
 
 namespace b200dem {
 
@@ -363,15 +364,20 @@ static int persistent_blocks(const void *kernel, int block, int n) {
 void launch_step(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
                  const PairConst *pw, const WallGeom *walls, int mode, cudaStream_t s) {
     if (mode == MODE_FUSED) {
-        static int gc = 0, gm = 0, gcd = 0, gmd = 0, last_n = -1;
+        static int gc = 0, gm = 0, gcd = 0, gmd = 0, gk4 = 0, gk8 = 0, gkm4 = 0, gkm8 = 0, last_n = -1;
         if (last_n != P.n) {
             // contact kernels: every block the SMs hold (a dense packing defers nearly every
             // particle; blocks past the deferred count exit at once); the apply kernel copies
             // 48 B per deferred particle and takes one ticket per block: one block per SM
             gc = persistent_blocks((const void *)k_contact<1>, kBlock, P.n);
-            gm = persistent_blocks(contact_mixed_kernel(0), kBlock, P.n);
+            gm = persistent_blocks(contact_mixed_kernel(0, 0), kBlock, P.n);
             gcd = persistent_blocks((const void *)k_contact<kContactMinBlocksDense>, kBlock, P.n);
-            gmd = persistent_blocks(contact_mixed_kernel(1), kBlock, P.n);
+            gmd = persistent_blocks(contact_mixed_kernel(1, 0), kBlock, P.n);
+            // cooperative kernels: a block serves kBlock / NL particles per pass
+            gk4 = persistent_blocks((const void *)k_contact_coop<4, kCoopMinBlocks, false>, kBlock, 4 * P.n);
+            gk8 = persistent_blocks((const void *)k_contact_coop<8, kCoopMinBlocks, false>, kBlock, 8 * P.n);
+            gkm4 = persistent_blocks(contact_mixed_kernel(0, 4), kBlock, 4 * P.n);
+            gkm8 = persistent_blocks(contact_mixed_kernel(0, 8), kBlock, 8 * P.n);
             last_n = P.n;
         }
         if (fc.stream_block == 64)
@@ -381,7 +387,12 @@ void launch_step(const Particles &P, const NbrList &L, Ctl *ctl, const ForceCons
         else
             k_stream<128, 10><<<(P.n + 127) / 128, 128, 0, s>>>(P, L, ctl, fc, walls);
         if (fc.mixed)
-            launch_contact_mixed(P, L, ctl, fc, pp, pw, walls, fc.dense ? gmd : gm, s);
+            launch_contact_mixed(P, L, ctl, fc, pp, pw, walls,
+                                 fc.coop == 8 ? gkm8 : fc.coop == 4 ? gkm4 : fc.dense ? gmd : gm, s);
+        else if (fc.coop == 8)
+            k_contact_coop<8, kCoopMinBlocks, false><<<gk8, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+        else if (fc.coop == 4)
+            k_contact_coop<4, kCoopMinBlocks, false><<<gk4, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
         else if (fc.dense)
             k_contact<kContactMinBlocksDense><<<gcd, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
         else

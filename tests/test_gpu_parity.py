@@ -101,6 +101,37 @@ def test_random_box_bitwise(quirks):
     assert st["rebuilds"] >= 1
 
 
+@pytest.mark.parametrize("lanes", [1, 4, 8], ids=["per_thread", "coop4", "coop8"])
+def test_contact_kernel_forms_bitwise(lanes):
+    """The per-thread contact kernel and the cooperative one (4 or 8 lanes per particle)
+    against the oracle on a compressed box: contacts form, break (slot compaction moves
+    histories between slots) and form again over 400 steps, against six walls."""
+    sc = S.random_box(n=4096, nsteps=400)
+    c = sc.state.x.mean(axis=0)
+    sc.state.x[:] = c + (sc.state.x - c) * 0.6
+    ref, _ = _oracle(sc, 400)
+    s = api.from_scenario(sc, contact_lanes=lanes)
+    s.run_steps(150)
+    mid = s.particles.download()
+    assert mid.tng_count.sum() > 1000
+    s.run_steps(250)
+    _assert_bitwise(s.particles.download(), ref, where="lanes%d" % lanes)
+
+
+@pytest.mark.parametrize("lanes", [1, 8], ids=["per_thread", "coop8"])
+def test_contact_overflow_all_kernels(lanes):
+    """Slot overflow (MaxCnts 2) through either contact kernel: status bit and state as the oracle."""
+    sc = S.random_box(n=512, max_cnts=2, nsteps=5)
+    c = sc.state.x.mean(axis=0)
+    sc.state.x[:] = c + (sc.state.x - c) * 0.3
+    ref, st = _oracle(sc, 5)
+    assert st & 0x1
+    s = api.from_scenario(sc, contact_lanes=lanes)
+    s.run_steps(5)
+    assert s.last_status & 0x004
+    _assert_bitwise(s.particles.download(), ref, where="overflow%d" % lanes)
+
+
 def test_unfused_phases_match_fused(example_inputs):
     sc = S.tst03(example_inputs["tst_03_multiple_particles_contacts"])
     steps = 400
