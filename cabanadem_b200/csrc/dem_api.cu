@@ -778,20 +778,26 @@ __global__ void k_clear_status(Ctl *ctl, int bits) {
 
 bool ref_mode(const dem_solver *s) { return s->sp.rebuild_every_step != 0; }
 
-// Contact kernel of the next graph.  Few deferred particles (a sparse step): the cooperative
-// kernel, whose short dependent chains hide memory latency (B200, 2M-sphere lattice: 105 ->
-// 87 us per step late in the run at 8 lanes).  Most particles in contact (a dense step): the
-// per-thread build for more resident blocks, which issues fewer instructions per contact
-// (200k-disk dam break at t = 0.3 s: 131 us per step against 197 us at 8 lanes).
-// contact_lanes 1, 4 or 8 fixes the choice.
+// Kernels of the next graph.  Few particles in contact (a sparse step): streaming kernel,
+// cooperative contact kernel, apply kernel; the cooperative kernel's short dependent chains
+// hide memory latency (B200, 2M-sphere lattice: 105 -> 87 us per step late in the run at 8
+// lanes).  Most particles in contact (a dense step): one per-thread kernel over every
+// particle, which issues fewer instructions per contact than the cooperative one (200k-disk
+// dam break at t = 0.3 s: 131 us per step against 197 us at 8 lanes) and needs neither the
+// streaming pass nor the apply pass.  contact_lanes 1, 4 or 8 keeps the three-kernel step
+// with that contact kernel.
 void pick_contact_kernel(dem_solver *s) {
     const int req = s->sp.contact_lanes;
-    if (req == 1 || s->p->P.mc > kCoopSlots)
+    const bool fits = s->p->P.mc <= kCoopSlots;
+    s->fc.all = 0;
+    if (req == 1) {
         s->fc.coop = 0;
-    else if (req == 4 || req == 8)
-        s->fc.coop = req;
-    else
-        s->fc.coop = s->fc.dense ? 0 : 8;
+    } else if (req == 4 || req == 8) {
+        s->fc.coop = fits ? req : 0;
+    } else {
+        s->fc.all = s->fc.dense;
+        s->fc.coop = (!s->fc.dense && fits) ? 8 : 0;
+    }
 }
 
 // Pick the contact-kernel build for the next graph from the last step's deferred count: the
@@ -860,7 +866,7 @@ int capture_graph(dem_solver *s, int steps) {
         launch_step(s->p->P, s->L, s->p->ctl, s->fc, s->d_pp, s->d_pw, s->d_walls, MODE_FUSED, ctx->stream);
     }
     CK(cudaStreamEndCapture(ctx->stream, &g));
-    s->graph_nodes = (long)steps * (kernels_per_step() + (ref_mode(s) ? build_kernel_count(false) : 0));
+    s->graph_nodes = (long)steps * (kernels_per_step(s->fc) + (ref_mode(s) ? build_kernel_count(false) : 0));
     cudaError_t e = cudaGraphInstantiate(&s->graph, g, 0);
     cudaGraphDestroy(g);
     CK(e);
@@ -1100,7 +1106,7 @@ extern "C" int dem_solver_profile(dem_solver *s, int nsteps, double *kernel_ms) 
         CK(cudaEventRecord(e0, st));
         launch_step(s->p->P, s->L, s->p->ctl, s->fc, s->d_pp, s->d_pw, s->d_walls, MODE_FUSED, st);
         CK(cudaEventRecord(e1, st));
-        s->launches += kernels_per_step();
+        s->launches += kernels_per_step(s->fc);
         CK(cudaEventSynchronize(e1));
         const Ctl c = read_ctl(s);
         float ms = 0.f;

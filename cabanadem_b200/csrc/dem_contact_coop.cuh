@@ -301,9 +301,9 @@ __device__ __forceinline__ void particle_coop(const Particles &P, const NbrList 
     const int cs1 = cnt | (int)(wmask << 8);
     if (cs1 != cs0) P.cstate[i] = cs1;
     if (fc.has_gravity) {
-        F0 += mIi.x * fc.g[0];
-        F1 += mIi.x * fc.g[1];
-        F2 += mIi.x * fc.g[2];
+        F0 = dadd(F0, dmul(mIi.x, fc.g[0]));
+        F1 = dadd(F1, dmul(mIi.x, fc.g[1]));
+        F2 = dadd(F2, dmul(mIi.x, fc.g[2]));
     }
     if (fc.has_fix) {
         const int f = P.fix[i];
@@ -313,12 +313,12 @@ __device__ __forceinline__ void particle_coop(const Particles &P, const NbrList 
     const double m_inverse = 1. / mIi.x;
     const double I_inverse = 1. / mIi.y;
     const double h = fc.half_dt;
-    ui0 += h * F0 * m_inverse;
-    ui1 += h * F1 * m_inverse;
-    ui2 += h * F2 * m_inverse;
-    wi0 += h * T0 * I_inverse;
-    wi1 += h * T1 * I_inverse;
-    wi2 += h * T2 * I_inverse;
+    ui0 = dadd(ui0, dmul(dmul(h, F0), m_inverse));
+    ui1 = dadd(ui1, dmul(dmul(h, F1), m_inverse));
+    ui2 = dadd(ui2, dmul(dmul(h, F2), m_inverse));
+    wi0 = dadd(wi0, dmul(dmul(h, T0), I_inverse));
+    wi1 = dadd(wi1, dmul(dmul(h, T1), I_inverse));
+    wi2 = dadd(wi2, dmul(dmul(h, T2), I_inverse));
     D4 pn = pi;
     if (last) {
         P.force[i] = F0;
@@ -328,16 +328,16 @@ __device__ __forceinline__ void particle_coop(const Particles &P, const NbrList 
         P.torque[cap + i] = T1;
         P.torque[2 * cap + i] = T2;
     } else {
-        ui0 += h * F0 * m_inverse;
-        ui1 += h * F1 * m_inverse;
-        ui2 += h * F2 * m_inverse;
-        wi0 += h * T0 * I_inverse;
-        wi1 += h * T1 * I_inverse;
-        wi2 += h * T2 * I_inverse;
-        pn.x += fc.dt * ui0;
-        pn.y += fc.dt * ui1;
-        pn.z += fc.dt * ui2;
-        vmax2 = ui0 * ui0 + ui1 * ui1 + ui2 * ui2;
+        ui0 = dadd(ui0, dmul(dmul(h, F0), m_inverse));
+        ui1 = dadd(ui1, dmul(dmul(h, F1), m_inverse));
+        ui2 = dadd(ui2, dmul(dmul(h, F2), m_inverse));
+        wi0 = dadd(wi0, dmul(dmul(h, T0), I_inverse));
+        wi1 = dadd(wi1, dmul(dmul(h, T1), I_inverse));
+        wi2 = dadd(wi2, dmul(dmul(h, T2), I_inverse));
+        pn.x = dadd(pn.x, dmul(fc.dt, ui0));
+        pn.y = dadd(pn.y, dmul(fc.dt, ui1));
+        pn.z = dadd(pn.z, dmul(fc.dt, ui2));
+        vmax2 = dadd(dadd(dmul(ui0, ui0), dmul(ui1, ui1)), dmul(ui2, ui2));
     }
     st4(P.pos[nxt], i, pn);
     double *vn = L.defer_v, *wn = L.defer_w;

@@ -99,6 +99,8 @@ struct ForceConsts {
                                // more resident blocks, wider apply grid (same arithmetic)
     int coop;                  // lanes per deferred particle in the contact kernel: 4 or 8
                                // (cooperative, MaxCnts <= kCoopSlots), 0: one thread each
+    int all;                   // 1: one kernel steps every particle (dense flows), no streaming
+                               // or apply kernel; velocities ping-pong between their buffers
     const struct SceneConst *scenes;   // per-scene damping/friction, null: the scalars above
     int wps;                   // walls per scene (> 0 with scenes): scene s owns [s*wps, s*wps+wps)
 };
@@ -169,15 +171,19 @@ void launch_bond_step(const Particles &P, const Bonds &B, Ctl *ctl, const ForceC
 void launch_bond_broken_count(const Bonds &B, int n, unsigned long long *out, cudaStream_t s);
 
 // ---- launchers (dem_step.cu) ------------------------------------------------------
-// MODE_FUSED launches the streaming kernel and the contact kernel (kernels_per_step());
-// MODE_FORCE_ONLY one force-only kernel.
-enum StepMode { MODE_FUSED = 0, MODE_FORCE_ONLY = 1 };
-int kernels_per_step();
+// MODE_FUSED launches the fused step (kernels_per_step(fc) kernels); MODE_FORCE_ONLY one
+// force-only kernel.  MODE_FUSED_DIRECT is the per-particle body of the one-kernel dense step.
+enum StepMode { MODE_FUSED = 0, MODE_FORCE_ONLY = 1, MODE_FUSED_DIRECT = 2 };
+int kernels_per_step(const ForceConsts &fc);
 void launch_prologue(const Particles &P, Ctl *ctl, const ForceConsts &fc, cudaStream_t s);
 void launch_step(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
                  const PairConst *pw, const WallGeom *walls, int mode, cudaStream_t s);
 void launch_stage(const Particles &P, Ctl *ctl, const ForceConsts &fc, int stage, cudaStream_t s);
 // dem_mixed.cu
+void launch_contact_mixed_all(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc,
+                              const PairConst *pp, const PairConst *pw, const WallGeom *walls, int blocks,
+                              cudaStream_t s);
+const void *contact_mixed_all_kernel();
 void launch_contact_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
                           const PairConst *pw, const WallGeom *walls, int blocks, cudaStream_t s);
 void launch_force_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,

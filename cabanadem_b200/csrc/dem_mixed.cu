@@ -34,6 +34,28 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contact_mixed(Particles P, Nbr
     block_vmax(ctl, P.vslots, vmax2, status);
 }
 
+// One-kernel dense step in mixed precision (see k_contact_all in dem_step.cu).
+template <int MINB>
+__global__ void __launch_bounds__(kBlock, MINB) k_contact_mixed_all(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
+                                                              const PairConst *__restrict__ pp,
+                                                              const PairConst *__restrict__ pw,
+                                                              const WallGeom *__restrict__ walls) {
+    const CtlSnap c = read_ctl(ctl, true);
+    if (!c.go) return;
+    const int vcur = ctl->vcur;
+    double vmax2 = 0.0;
+    int status = 0, active = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += gridDim.x * blockDim.x) {
+        double v2 = 0.0;
+        int a = 0;
+        particle_full<MODE_FUSED_DIRECT, true>(P, L, fc, pp, pw, walls, c.cur, c.cur ^ 1, vcur, c.last, i, i, v2,
+                                               status, &a);
+        vmax2 = fmax(vmax2, v2);
+        active += a;
+    }
+    finish_step_counted(ctl, P.vslots, vmax2, fc.dt, status, active);
+}
+
 __global__ void __launch_bounds__(kBlock) k_force_mixed(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
                                                         const PairConst *__restrict__ pp,
                                                         const PairConst *__restrict__ pw,
@@ -60,6 +82,14 @@ void launch_contact_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const 
     else
         k_contact_mixed<1><<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
 }
+
+void launch_contact_mixed_all(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc,
+                              const PairConst *pp, const PairConst *pw, const WallGeom *walls, int blocks,
+                              cudaStream_t s) {
+    k_contact_mixed_all<kContactMixedMinBlocksDense><<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+}
+
+const void *contact_mixed_all_kernel() { return (const void *)k_contact_mixed_all<kContactMixedMinBlocksDense>; }
 
 void launch_force_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
                         const PairConst *pw, const WallGeom *walls, cudaStream_t s) {

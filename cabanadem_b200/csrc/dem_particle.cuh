@@ -61,6 +61,13 @@ __device__ __forceinline__ D4 ld4_early(const double4 *p, int i) {
     return r;
 }
 
+// Round-to-nearest add and multiply that the compiler never contracts into an FMA: the
+// gravity hook and the velocity-Verlet updates of a particle give the same bits in the FP64
+// translation unit (built without contraction) and in the mixed one (built with it), so a
+// particle's step does not depend on which kernel form stepped it.
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+
 // L2 prefetch of a contiguous range with the TMA bulk-prefetch instruction (no registers,
 // no completion to wait for).  The range is clipped to 16-byte granules inside [p, p+bytes).
 __device__ __forceinline__ void prefetch_l2(const void *p, long bytes) {
@@ -144,6 +151,55 @@ __device__ __forceinline__ void finish_step(Ctl *ctl, unsigned long long *slots,
                 ctl->steps_done += 1;
                 ctl->total_steps += 1;
             }
+            __threadfence();
+            ctl->ticket = 0u;
+        }
+    }
+}
+
+// finish_step for the one-kernel dense step: also counts the particles in contact (`active`
+// per thread; one atomic per block, added before the block's ticket) and leaves the count in last_ndefer,
+// where the host reads the step's density.  Flips the position and velocity buffers.
+__device__ __forceinline__ void finish_step_counted(Ctl *ctl, unsigned long long *slots, double vmax2, double dt,
+                                                    int status, int active) {
+    __shared__ int cnt_s[32];
+    __shared__ double red[32];
+    __shared__ bool am_last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int c = active;   // particles in contact among this thread's
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    for (int o = 16; o > 0; o >>= 1) vmax2 = fmax(vmax2, __shfl_xor_sync(0xffffffffu, vmax2, o));
+    if (status) atomicOr(&ctl->status, status);
+    if (lane == 0) {
+        cnt_s[warp] = c;
+        red[warp] = vmax2;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int t = 0;
+        double m = red[0];
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            t += cnt_s[w];
+            m = fmax(m, red[w]);
+        }
+        if (t) atomicAdd(&ctl->ndefer, t);
+        vmax_fold(slots, m);
+        __threadfence();
+        const unsigned tk = atomicAdd(&ctl->ticket, 1u);
+        am_last = (tk == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (am_last && threadIdx.x < 32) {
+        __threadfence();
+        const double v2 = vmax_collect_warp(slots);
+        if (threadIdx.x == 0) {
+            ctl->disp = ctl->disp + dt * sqrt(v2) * (1.0 + 1e-9);
+            ctl->last_ndefer = atomicAdd(&ctl->ndefer, 0);
+            ctl->ndefer = 0;
+            ctl->cur ^= 1;
+            ctl->vcur ^= 1;
+            ctl->steps_done += 1;
+            ctl->total_steps += 1;
             __threadfence();
             ctl->ticket = 0u;
         }
@@ -522,7 +578,7 @@ __device__ __forceinline__ void particle_full(const Particles &P, const NbrList 
                                               const PairConst *__restrict__ pp, const PairConst *__restrict__ pw,
                                               const WallGeom *__restrict__ walls, const int cur, const int nxt,
                                               const int vcur, const int last, const int i, const int slot,
-                                              double &vmax2, int &status) {
+                                              double &vmax2, int &status, int *active = nullptr) {
     const int cap = P.cap;
     const unsigned q = fc.quirks;
     // batched scenes: this particle's scene supplies damping, friction and its walls
@@ -693,11 +749,12 @@ __device__ __forceinline__ void particle_full(const Particles &P, const NbrList 
     }
     const int cs1 = cnt | (int)(wmask << 8);
     if (cs1 != cs0) P.cstate[i] = cs1;
+    if (active) *active = (cs0 | cs1) != 0;
     // ---- hooks after the pair forces
     if (fc.has_gravity) {
-        F0 += mIi.x * fc.g[0];
-        F1 += mIi.x * fc.g[1];
-        F2 += mIi.x * fc.g[2];
+        F0 = dadd(F0, dmul(mIi.x, fc.g[0]));
+        F1 = dadd(F1, dmul(mIi.x, fc.g[1]));
+        F2 = dadd(F2, dmul(mIi.x, fc.g[2]));
     }
     if (fc.has_fix) {
         const int f = P.fix[i];
@@ -716,12 +773,12 @@ __device__ __forceinline__ void particle_full(const Particles &P, const NbrList 
         const double I_inverse = 1. / mIi.y;
         const double h = fc.half_dt;
         // stage3 of this step
-        ui0 += h * F0 * m_inverse;
-        ui1 += h * F1 * m_inverse;
-        ui2 += h * F2 * m_inverse;
-        wi0 += h * T0 * I_inverse;
-        wi1 += h * T1 * I_inverse;
-        wi2 += h * T2 * I_inverse;
+        ui0 = dadd(ui0, dmul(dmul(h, F0), m_inverse));
+        ui1 = dadd(ui1, dmul(dmul(h, F1), m_inverse));
+        ui2 = dadd(ui2, dmul(dmul(h, F2), m_inverse));
+        wi0 = dadd(wi0, dmul(dmul(h, T0), I_inverse));
+        wi1 = dadd(wi1, dmul(dmul(h, T1), I_inverse));
+        wi2 = dadd(wi2, dmul(dmul(h, T2), I_inverse));
         D4 pn = pi;
         if (last) {
             P.force[i] = F0;
@@ -732,21 +789,24 @@ __device__ __forceinline__ void particle_full(const Particles &P, const NbrList 
             P.torque[2 * cap + i] = T2;
         } else {
             // stage1 + stage2 of the next step
-            ui0 += h * F0 * m_inverse;
-            ui1 += h * F1 * m_inverse;
-            ui2 += h * F2 * m_inverse;
-            wi0 += h * T0 * I_inverse;
-            wi1 += h * T1 * I_inverse;
-            wi2 += h * T2 * I_inverse;
-            pn.x += fc.dt * ui0;
-            pn.y += fc.dt * ui1;
-            pn.z += fc.dt * ui2;
-            vmax2 = ui0 * ui0 + ui1 * ui1 + ui2 * ui2;
+            ui0 = dadd(ui0, dmul(dmul(h, F0), m_inverse));
+            ui1 = dadd(ui1, dmul(dmul(h, F1), m_inverse));
+            ui2 = dadd(ui2, dmul(dmul(h, F2), m_inverse));
+            wi0 = dadd(wi0, dmul(dmul(h, T0), I_inverse));
+            wi1 = dadd(wi1, dmul(dmul(h, T1), I_inverse));
+            wi2 = dadd(wi2, dmul(dmul(h, T2), I_inverse));
+            pn.x = dadd(pn.x, dmul(fc.dt, ui0));
+            pn.y = dadd(pn.y, dmul(fc.dt, ui1));
+            pn.z = dadd(pn.z, dmul(fc.dt, ui2));
+            vmax2 = dadd(dadd(dmul(ui0, ui0), dmul(ui1, ui1)), dmul(ui2, ui2));
         }
         // positions go to the next buffer; u and omega to this particle's scratch slot,
         // committed by the apply kernel once no thread reads the current values any more
+        // (MODE_FUSED), or straight to the other velocity buffer when one kernel steps every
+        // particle (MODE_FUSED_DIRECT, slot = i)
         st4(P.pos[nxt], i, pn);
-        double *vn = L.defer_v, *wn = L.defer_w;
+        double *vn = MODE == MODE_FUSED_DIRECT ? P.vel[vcur ^ 1] : L.defer_v;
+        double *wn = MODE == MODE_FUSED_DIRECT ? P.omg[vcur ^ 1] : L.defer_w;
         vn[slot] = ui0;
         vn[cap + slot] = ui1;
         vn[2 * cap + slot] = ui2;

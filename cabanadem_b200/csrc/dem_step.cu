@@ -181,6 +181,30 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contact(Particles P, NbrList L
     block_vmax(ctl, P.vslots, vmax2, status);
 }
 
+// One-kernel step for dense flows (most particles in contact): every particle takes the
+// full arithmetic, positions and velocities go to the other buffers, and the last block
+// finalises the step.  Same results as the three-kernel step.
+template <int MINB>
+__global__ void __launch_bounds__(kBlock, MINB) k_contact_all(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
+                                                        const PairConst *__restrict__ pp,
+                                                        const PairConst *__restrict__ pw,
+                                                        const WallGeom *__restrict__ walls) {
+    const CtlSnap c = read_ctl(ctl, true);
+    if (!c.go) return;
+    const int vcur = ctl->vcur;
+    double vmax2 = 0.0;
+    int status = 0, active = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += gridDim.x * blockDim.x) {
+        double v2 = 0.0;
+        int a = 0;
+        particle_full<MODE_FUSED_DIRECT, false>(P, L, fc, pp, pw, walls, c.cur, c.cur ^ 1, vcur, c.last, i, i, v2,
+                                                status, &a);
+        vmax2 = fmax(vmax2, v2);
+        active += a;
+    }
+    finish_step_counted(ctl, P.vslots, vmax2, fc.dt, status, active);
+}
+
 // Fused step, kernel 3 of 3: commit the deferred particles' u and omega, then the last
 // block to take a ticket finalises the step (displacement bound, position-buffer flip,
 // step counter, deferred-list reset).  Each block copies ndefer before its ticket, so the
@@ -344,7 +368,7 @@ void launch_prologue(const Particles &P, Ctl *ctl, const ForceConsts &fc, cudaSt
     k_prologue<<<nblocks(P.n), kBlock, 0, s>>>(P, ctl, fc);
 }
 
-int kernels_per_step() { return 3; }
+int kernels_per_step(const ForceConsts &fc) { return fc.all ? 1 : 3; }
 
 static int persistent_blocks(const void *kernel, int block, int n) {
     static int sms = 0;
@@ -363,7 +387,18 @@ static int persistent_blocks(const void *kernel, int block, int n) {
 
 void launch_step(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
                  const PairConst *pw, const WallGeom *walls, int mode, cudaStream_t s) {
-    if (mode == MODE_FUSED) {
+    if (mode == MODE_FUSED && fc.all) {
+        static int ga = 0, gma = 0, last_na = -1;
+        if (last_na != P.n) {
+            ga = persistent_blocks((const void *)k_contact_all<kContactMinBlocksDense>, kBlock, P.n);
+            gma = persistent_blocks(contact_mixed_all_kernel(), kBlock, P.n);
+            last_na = P.n;
+        }
+        if (fc.mixed)
+            launch_contact_mixed_all(P, L, ctl, fc, pp, pw, walls, gma, s);
+        else
+            k_contact_all<kContactMinBlocksDense><<<ga, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+    } else if (mode == MODE_FUSED) {
         static int gc = 0, gm = 0, gcd = 0, gmd = 0, gk4 = 0, gk8 = 0, gkm4 = 0, gkm8 = 0, last_n = -1;
         if (last_n != P.n) {
             // contact kernels: every block the SMs hold (a dense packing defers nearly every

@@ -101,11 +101,12 @@ def test_random_box_bitwise(quirks):
     assert st["rebuilds"] >= 1
 
 
-@pytest.mark.parametrize("lanes", [1, 4, 8], ids=["per_thread", "coop4", "coop8"])
+@pytest.mark.parametrize("lanes", [0, 1, 4, 8], ids=["auto", "per_thread", "coop4", "coop8"])
 def test_contact_kernel_forms_bitwise(lanes):
-    """The per-thread contact kernel and the cooperative one (4 or 8 lanes per particle)
-    against the oracle on a compressed box: contacts form, break (slot compaction moves
-    histories between slots) and form again over 400 steps, against six walls."""
+    """The step's kernel forms against the oracle on a compressed box: contacts form, break
+    (slot compaction moves histories between slots) and form again over 400 steps, against
+    six walls.  Three-kernel step with the per-thread or the cooperative (4 or 8 lanes)
+    contact kernel; auto: dense, so after the first graph one kernel steps every particle."""
     sc = S.random_box(n=4096, nsteps=400)
     c = sc.state.x.mean(axis=0)
     sc.state.x[:] = c + (sc.state.x - c) * 0.6
@@ -116,6 +117,12 @@ def test_contact_kernel_forms_bitwise(lanes):
     assert mid.tng_count.sum() > 1000
     s.run_steps(250)
     _assert_bitwise(s.particles.download(), ref, where="lanes%d" % lanes)
+    if lanes == 0:
+        # the same trajectory (so the same rebuilds) with three kernels a step launches more
+        t = api.from_scenario(sc, contact_lanes=1)
+        t.run_steps(400)
+        assert s.stats()["rebuilds"] == t.stats()["rebuilds"]
+        assert s.stats()["launches"] < t.stats()["launches"] - 400
 
 
 @pytest.mark.parametrize("lanes", [1, 8], ids=["per_thread", "coop8"])
