@@ -116,9 +116,18 @@ class Particles:
             raise DemError("set(%s): expected shape %s, got %s" % (field, exp, a.shape))
         check(lib().dem_particles_set(self.h, F[field], a.ctypes.data, a.size), self.ctx.h, "set " + field)
 
-    def get(self, field: str):
+    def get(self, field: str, out=None):
+        """Host copy of a field in caller order; `out` (a C-contiguous array of the field's
+        dtype and size, e.g. in pinned memory) receives it instead of a new array."""
         dt = _F_DTYPE.get(field, np.float64)
-        a = np.empty(_shape(field, self.n, self.max_cnts, self.max_walls), dtype=dt)
+        shape = _shape(field, self.n, self.max_cnts, self.max_walls)
+        if out is None:
+            a = np.empty(shape, dtype=dt)
+        else:
+            a = out
+            if a.dtype != dt or a.size != int(np.prod(shape)) or not a.flags["C_CONTIGUOUS"]:
+                raise DemError("get(%s): out must be C-contiguous %s of %d elements" % (field, np.dtype(dt).name,
+                                                                                         int(np.prod(shape))))
         check(lib().dem_particles_get(self.h, F[field], a.ctypes.data, a.size), self.ctx.h, "get " + field)
         return a
 

@@ -654,8 +654,15 @@ int prepare(dem_solver *s) {
         std::map<std::tuple<double, double, double>, int> ids;
         p->mats.clear();
         p->mat.assign(n, 0);
+        int last = -1;   // neighbours in caller order usually share a material: test it first
         for (int i = 0; i < n; ++i) {
-            auto key = std::make_tuple(p->E[i], p->nu[i], p->G[i]);
+            const double E = p->E[i], nu = p->nu[i], G = p->G[i];
+            if (last >= 0 && std::get<0>(p->mats[last]) == E && std::get<1>(p->mats[last]) == nu &&
+                std::get<2>(p->mats[last]) == G) {
+                p->mat[i] = (uint8_t)last;
+                continue;
+            }
+            auto key = std::make_tuple(E, nu, G);
             auto it = ids.find(key);
             if (it == ids.end()) {
                 if ((int)p->mats.size() >= kMaxMat)
@@ -663,14 +670,14 @@ int prepare(dem_solver *s) {
                 it = ids.emplace(key, (int)p->mats.size()).first;
                 p->mats.push_back(key);
             }
-            p->mat[i] = (uint8_t)it->second;
+            last = it->second;
+            p->mat[i] = (uint8_t)last;
         }
-        uint8_t *tmp = nullptr;
-        CK(cudaMalloc(&tmp, n));
+        // through the staging buffer (cap * 24 bytes or more) of the particle set
+        uint8_t *tmp = (uint8_t *)p->stage;
         CK(cudaMemcpyAsync(tmp, p->mat.data(), n, cudaMemcpyHostToDevice, st));
         k_scatter_u8<<<kGS, kTB, 0, st>>>(tmp, p->P.mat, n, p->P.rank);
         CK(cudaStreamSynchronize(st));
-        cudaFree(tmp);
         p->mat_dirty = false;
         s->built = false;
     }
@@ -822,7 +829,7 @@ int check_walls(dem_solver *s) {
 }
 
 // kernels issued by one launch_build (see dem_nbr.cu)
-long build_kernel_count(bool resort) { return 13 + (resort ? 4 : 0); }
+long build_kernel_count(bool resort) { return 13 + (resort ? 6 : 0); }
 
 // Build with overflow handling (host-driven; re-sorts into Morton order).
 int build_with(dem_solver *s, bool resort, double delta, double skin);
@@ -907,6 +914,7 @@ extern "C" int dem_solver_create(dem_ctx *ctx, dem_particles *p, dem_walls *w, c
     A(dalloc(&B.bbox, 8));
     A(dalloc(&B.src, n));
     A(dalloc(&B.dst, n));
+    A(dalloc(&B.part_sums, (size_t)n / kPartBlock + 2));
     s->nparts = (p->P.n + 127) / 128;
     A(dalloc(&s->d_epart, 4 * (size_t)s->nparts));
     A(dalloc(&s->d_eout, 4));
@@ -935,6 +943,7 @@ extern "C" int dem_solver_destroy(dem_solver *s) {
     BuildBuffers &B = s->B;
     cudaFree(B.grid); cudaFree(B.total); cudaFree(B.key); cudaFree(B.cell_start); cudaFree(B.cell_fill); cudaFree(B.cell_items);
     cudaFree(B.block_sums); cudaFree(B.bbox); cudaFree(B.src); cudaFree(B.dst);
+    cudaFree(B.part_sums);
     cudaFree(s->d_epart); cudaFree(s->d_eout);
     delete s;
     return DEM_OK;

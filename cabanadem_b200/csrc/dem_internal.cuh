@@ -41,6 +41,8 @@ struct Ctl {
     long long total_steps;
     long long rebuilds;
     int last_ndefer;          // deferred particles of the last completed fused step
+    int nlone;                // particles [0, nlone) had no listed neighbour at the last build
+                              // (placed first by the re-sort; 0 when the build did not re-sort)
 };
 
 struct Particles {
@@ -141,7 +143,10 @@ struct BuildBuffers {
     int cell_cap;
     unsigned long long *bbox; // 8 ordered-int words per scene: lo[3], hi[3], rmax
     int *src, *dst;           // permutation at re-sort
+    int *part_sums;           // [cap / kPartBlock + 2] per-block counts of the re-sort's partition
 };
+
+constexpr int kPartBlock = 256;   // block size of the re-sort's partition kernels
 
 // Bond slots (bonded DEM), slot-major like the contact history.
 constexpr unsigned BQ10_INDEX_BY_J = 0x01u;   // history(i, partner id), BondedDEM_Force.hpp:207, :231-322

@@ -372,10 +372,6 @@ __global__ void k_permute(Particles P, Particles A, const Ctl *ctl, const int *i
     }
 }
 
-__global__ void k_identity(int n, int *items) {
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) items[p] = p;
-}
-
 __global__ void k_flip(Ctl *ctl) {
     if (threadIdx.x == 0) {
         ctl->cur ^= 1;
@@ -451,8 +447,109 @@ __global__ void __launch_bounds__(128) k_list(Particles P, NbrList L, Ctl *ctl, 
     }
 }
 
+// Re-sort partition, pass 1: for cell slot s (cell order of the old storage), flag[s] = 1 when
+// its particle has no neighbour within the list cutoff (the predicate of k_list), so that its
+// list will be empty; per-block counts of flagged slots into sums.
+__global__ void __launch_bounds__(kPartBlock) k_part_flag(Particles P, const Ctl *ctl, const Grid *g, const int *start,
+                                                          const int *items, double delta, double skin, int *flag,
+                                                          int *sums) {
+    const int cur = ctl->cur, n = P.n;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    int lone = 0;
+    if (s < n && !(ctl->status & DEM_ERR_NAN)) {
+        const int q = items[s];
+        const Grid G = g[scene_of(P, q)];
+        const double4 *pc = P.pos[cur];
+        const D4 pi = ld4(pc, q);
+        int c[3];
+        cell_of(G, pi, c);
+        lone = 1;
+        for (int dz = -1; dz <= 1 && lone; ++dz) {
+            const int z = c[2] + dz;
+            if (z < 0 || z >= G.dims[2]) continue;
+            for (int dy = -1; dy <= 1 && lone; ++dy) {
+                const int y = c[1] + dy;
+                if (y < 0 || y >= G.dims[1]) continue;
+                for (int dx = -1; dx <= 1 && lone; ++dx) {
+                    const int x = c[0] + dx;
+                    if (x < 0 || x >= G.dims[0]) continue;
+                    const int key = cell_key(G, x, y, z);
+                    const int e = start[key + 1];
+                    for (int t = start[key]; t < e; ++t) {
+                        const int j = items[t];
+                        if (j == q) continue;
+                        const D4 pj = ld4(pc, j);
+                        const double px = pi.x - pj.x, py = pi.y - pj.y, pz = pi.z - pj.z;
+                        const double r2 = px * px + py * py + pz * pz;
+                        const double cut = delta > 0.0 ? delta : pi.w + pj.w + skin;
+                        if (r2 <= cut * cut) {
+                            lone = 0;
+                            break;
+                        }
+                    }
+                }
+            }
+        }
+    }
+    if (s < n) flag[s] = lone;
+    __shared__ int cnt;
+    if (threadIdx.x == 0) cnt = 0;
+    __syncthreads();
+    const int w = __popc(__ballot_sync(0xffffffffu, lone != 0));
+    if ((threadIdx.x & 31) == 0 && w) atomicAdd(&cnt, w);
+    __syncthreads();
+    if (threadIdx.x == 0) sums[blockIdx.x] = cnt;
+}
+
+// Pass 2, one block: exclusive scan of the per-block counts (block order), total into nlone.
+__global__ void __launch_bounds__(1024) k_part_scan(int *sums, int nb, Ctl *ctl) {
+    __shared__ int part[1024];
+    const int per = (nb + 1023) / 1024;
+    const int b0 = threadIdx.x * per, b1 = min(b0 + per, nb);
+    int t = 0;
+    for (int b = b0; b < b1; ++b) t += sums[b];
+    part[threadIdx.x] = t;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {   // inclusive scan of the thread totals
+        const int v = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    int run = threadIdx.x > 0 ? part[threadIdx.x - 1] : 0;
+    for (int b = b0; b < b1; ++b) {
+        const int v = sums[b];
+        sums[b] = run;
+        run += v;
+    }
+    if (threadIdx.x == 1023) ctl->nlone = part[1023];
+}
+
+// Pass 3: stable partition of the cell order, flagged slots first.  New position of slot s:
+// newitems[pos] = old index, and items[s] = pos (the cell table of the permuted storage).
+__global__ void __launch_bounds__(kPartBlock) k_part_place(int n, const int *flag, const int *sums, const Ctl *ctl,
+                                                           int *items, int *newitems) {
+    __shared__ int woff[kPartBlock / 32];
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int f = s < n ? flag[s] : 0;
+    const unsigned b = __ballot_sync(0xffffffffu, f != 0);
+    if (lane == 0) woff[warp] = __popc(b);
+    __syncthreads();
+    int before = 0;   // flagged slots of this block before this warp
+    for (int w = 0; w < warp; ++w) before += woff[w];
+    if (s >= n) return;
+    const int lone_before = sums[blockIdx.x] + before + __popc(b & ((1u << lane) - 1u));
+    const int pos = f ? lone_before : ctl->nlone + (s - lone_before);
+    newitems[pos] = items[s];
+    items[s] = pos;
+}
+
 __global__ void k_build_begin(Ctl *ctl) {
-    if (threadIdx.x == 0) ctl->max_nbr = 0;
+    if (threadIdx.x == 0) {
+        ctl->max_nbr = 0;
+        ctl->nlone = 0;
+    }
 }
 
 __global__ void k_build_end(Ctl *ctl) {
@@ -484,8 +581,15 @@ void launch_build(const Particles &P, Particles &alt, const NbrList &L, BuildBuf
     k_fill<<<gs, kB, 0, s>>>(n, B.key, B.cell_start, B.cell_items);
     k_cell_sort<<<gs, kB, 0, s>>>(B.cell_fill, B.cell_items, P.perm, B.total, ctl);
     if (resort) {
-        k_make_dst<<<gs, kB, 0, s>>>(n, B.cell_items, B.dst);
-        k_permute<<<gs, kB, 0, s>>>(P, alt, ctl, B.cell_items, B.dst);
+        // new order: the cell order, split stably into particles with no listed neighbour
+        // (first) and the rest, so that the streaming kernel's leading warps load no list
+        const int nb = (n + kPartBlock - 1) / kPartBlock;
+        k_part_flag<<<nb, kPartBlock, 0, s>>>(P, ctl, B.grid, B.cell_fill, B.cell_items, delta, skin, B.src,
+                                              B.part_sums);
+        k_part_scan<<<1, 1024, 0, s>>>(B.part_sums, nb, ctl);
+        k_part_place<<<nb, kPartBlock, 0, s>>>(n, B.src, B.part_sums, ctl, B.cell_items, B.key);
+        k_make_dst<<<gs, kB, 0, s>>>(n, B.key, B.dst);
+        k_permute<<<gs, kB, 0, s>>>(P, alt, ctl, B.key, B.dst);
         const size_t cap = (size_t)P.cap;
         cudaMemcpyAsync(P.force, alt.force, 3 * cap * sizeof(double), cudaMemcpyDeviceToDevice, s);
         cudaMemcpyAsync(P.torque, alt.torque, 3 * cap * sizeof(double), cudaMemcpyDeviceToDevice, s);
@@ -501,7 +605,6 @@ void launch_build(const Particles &P, Particles &alt, const NbrList &L, BuildBuf
         cudaMemcpyAsync(P.perm, alt.perm, cap * sizeof(int), cudaMemcpyDeviceToDevice, s);
         if (P.scene) cudaMemcpyAsync(P.scene, alt.scene, cap * sizeof(int), cudaMemcpyDeviceToDevice, s);
         k_flip<<<1, 32, 0, s>>>(ctl);
-        k_identity<<<gs, kB, 0, s>>>(n, B.cell_items);
     }
     k_list<<<(n + 127) / 128, 128, 0, s>>>(P, L, ctl, B.grid, B.cell_fill, B.cell_items, delta, skin);
     k_build_end<<<1, 32, 0, s>>>(ctl);

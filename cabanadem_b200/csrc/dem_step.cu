@@ -57,7 +57,7 @@ template <int BS, int MINB>
 __global__ void __launch_bounds__(BS, MINB) k_stream(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
                                                      const WallGeom *__restrict__ walls) {
     if (!step_gate(ctl)) return;
-    const int cur = ctl->cur, vcur = ctl->vcur;
+    const int cur = ctl->cur, vcur = ctl->vcur, nlone = ctl->nlone;
     const bool last = ctl->steps_done + 1 >= ctl->target;
     const int nxt = cur ^ 1, cap = P.cap;
     const double4 *__restrict__ pc = P.pos[cur];
@@ -68,14 +68,17 @@ __global__ void __launch_bounds__(BS, MINB) k_stream(Particles P, NbrList L, Ctl
         // all own-state loads first (one memory round trip per particle)
         const D4 pi = ld4_early(pc, i);
         const int cs = ld_early_i(P.cstate + i);
-        const int nn = ld_early_i(L.nn + i);
+        // the re-sort placed particles without listed neighbours first: their lists stay empty
+        // until the next build, so neither the list nor a partner is read (one round trip)
+        const bool lone = i < nlone;
+        const int nn = lone ? 0 : ld_early_i(L.nn + i);
         const double m = ld_early(&P.mI[i]);
         double ui0 = ld_early(vc + i), ui1 = ld_early(vc + cap + i), ui2 = ld_early(vc + 2 * cap + i);
         // the first two list slots are read with the own state (in bounds for every i; the
         // value is only used below the list length), so that most warps need one more
         // round trip (the partners' positions) instead of two per neighbour
-        const int j0 = L.maxnb > 0 ? ld_early_i(L.idx + i) : 0;
-        const int j1 = L.maxnb > 1 ? ld_early_i(L.idx + cap + i) : 0;
+        const int j0 = (!lone && L.maxnb > 0) ? ld_early_i(L.idx + i) : 0;
+        const int j1 = (!lone && L.maxnb > 1) ? ld_early_i(L.idx + cap + i) : 0;
         bool defer = cs != 0;
         if (!defer && nn > 0) {
             const D4 pa = ld4(pc, j0);

@@ -104,9 +104,11 @@ typedef struct dem_solver_params {
     int max_neighbors;     /* initial neighbour-list capacity per particle (0 = 32)          */
     int steps_per_launch;  /* fused steps per captured graph (0 = 32)                        */
     int stream_block;      /* streaming-kernel block size: 64, 128 or 256 (0 = 128)          */
-    int contact_lanes;     /* lanes per particle in the contact kernel: 1 (one thread each), 4
-                            * or 8 (cooperative, MaxCnts <= 32); 0 = automatic: 8 while few
-                            * particles are in contact, 1 while most are.  Same results.      */
+    int contact_lanes;     /* 0 = automatic: while few particles are in contact, a streaming,
+                            * a cooperative contact (8 lanes per particle, MaxCnts <= 32) and
+                            * an apply kernel per step; while most are, one kernel over every
+                            * particle.  1, 4 or 8: always the three-kernel step, its contact
+                            * kernel with that many lanes per particle.  Same results.        */
 } dem_solver_params;
 
 typedef struct dem_run_stats {

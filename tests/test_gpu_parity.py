@@ -215,6 +215,8 @@ def test_set_get_roundtrip_after_resort():
     u = np.random.default_rng(5).normal(size=x.shape)
     p.set("u", u)
     assert np.array_equal(p.get("u"), u)
+    buf = np.empty_like(u)
+    assert p.get("u", out=buf) is buf and np.array_equal(buf, u)
     assert np.array_equal(p.get("rad"), sc.state.rad)
 
 
