@@ -120,10 +120,19 @@ class ClockSampler:
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        # nvidia-smi takes a while to start: the timed region begins once it samples, so that
+        # even a sub-second timed region is covered
+        t0 = time.time()
+        while time.time() - t0 < 10.0 and self.proc.poll() is None:
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.01)
+        self.skip = sum(1 for _ in open(self.path))   # samples taken before the timed region
 
     def stop(self):
         if not self.proc:
@@ -136,7 +145,9 @@ class ClockSampler:
         self.f.close()
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
+        for k, line in enumerate(open(self.path)):
+            if k < getattr(self, "skip", 0):
+                continue
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue

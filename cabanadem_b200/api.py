@@ -34,7 +34,7 @@ from ._lib import DemError, F, W, check, lib
 from .inputs import Inputs
 from .state import ParticleState, WallState
 
-REF_COMPAT = 0x1F
+REF_COMPAT = 0x3F
 
 _F_DTYPE = {"tng_idx": np.int32, "tng_count": np.int32, "fix": np.uint8, "scene": np.int32}
 
@@ -281,6 +281,15 @@ class SolverDEM:
         st = lib().dem_solver_run(self.h, int(nsteps))
         self.last_status = st
         return check(st, self.particles.ctx.h, "dem_solver_run", allow=allow)
+
+    def wall_positions(self):
+        """Current positions [nw, 3] of the solver's walls: walls with a velocity move by
+        dt * u each step when the force's DEM_Q6_WALL_STATIC bit is clear."""
+        nw = self.wall.n if self.wall is not None else 0
+        out = np.zeros((nw, 3))
+        check(lib().dem_solver_wall_positions(self.h, out.ctypes.data, out.size), self.particles.ctx.h,
+              "dem_solver_wall_positions")
+        return out
 
     def stats(self):
         s = _lib.RunStats()

@@ -62,6 +62,8 @@ struct dem_solver {
     ForceConsts fc{};
     PairConst *d_pp = nullptr, *d_pw = nullptr;
     WallGeom *d_walls = nullptr;
+    std::vector<double> wall_pos;   // wall positions at the last preparation ([nw][3])
+    bool walls_move = false;        // some wall has a velocity and Q6 is clear
     SceneConst *d_scenes = nullptr;
     int nscenes = 0, wps = 0;
     bool walls_ok = true;
@@ -701,11 +703,28 @@ int prepare(dem_solver *s) {
             pw[(size_t)a * nw + w] = pair_const(std::get<0>(A), std::get<1>(A), std::get<2>(A), s->w->E[w], s->w->nu[w],
                                                 s->w->G[w]);
     }
+    // moving walls keep their current (device) positions across a re-preparation
+    if (s->d_walls && s->walls_move && (int)s->wall_pos.size() == 3 * nw) {
+        std::vector<WallGeom> now(nw);
+        CK(cudaMemcpyAsync(now.data(), s->d_walls, nw * sizeof(WallGeom), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        for (int w = 0; w < nw; ++w)
+            for (int d = 0; d < 3; ++d) s->wall_pos[3 * w + d] = now[w].x[d];
+    } else {
+        if (s->w)
+            s->wall_pos = s->w->x;
+        else
+            s->wall_pos.clear();
+    }
+    const bool wall_static = (s->fp.quirks & DEM_Q6_WALL_STATIC) != 0;
+    bool moving = false;
     std::vector<WallGeom> wg(std::max(nw, 1));
     for (int w = 0; w < nw; ++w)
         for (int d = 0; d < 3; ++d) {
-            wg[w].x[d] = s->w->x[3 * w + d];
+            wg[w].x[d] = s->wall_pos[3 * w + d];
             wg[w].n[d] = s->w->normal[3 * w + d];
+            wg[w].u[d] = wall_static ? 0.0 : s->w->u[3 * w + d];
+            moving = moving || wg[w].u[d] != 0.0;
         }
     cudaFree(s->d_pp);
     cudaFree(s->d_pw);
@@ -718,6 +737,8 @@ int prepare(dem_solver *s) {
     CK(cudaMemcpyAsync(s->d_walls, wg.data(), wg.size() * sizeof(WallGeom), cudaMemcpyHostToDevice, st));
     ForceConsts &fc = s->fc;
     fc = ForceConsts{};
+    s->walls_move = moving;
+    fc.mwalls = moving ? s->d_walls : nullptr;
     const unsigned q = s->fp.quirks;
     const double bpp = beta_of(s->fp.cor_pp), bpw = beta_of(s->fp.cor_pw);
     fc.K_n_pp = -2. * std::sqrt(5. / 6.) * bpp;             // Force.hpp:215
@@ -1041,6 +1062,24 @@ extern "C" int dem_solver_run(dem_solver *s, int nsteps) {
     Ctl c = read_ctl(s);
     CK(cudaGetLastError());
     return c.status & (DEM_ERR_CONTACT_OVERFLOW | DEM_ERR_NAN);
+}
+
+extern "C" int dem_solver_wall_positions(dem_solver *s, double *host, long count) {
+    if (!s || !host) return DEM_ERR_INVALID;
+    const int nw = s->w ? s->w->n : 0;
+    if (count != 3L * nw) return fail(s->ctx, DEM_ERR_INVALID, "dem_solver_wall_positions: count != 3 * walls");
+    if (nw == 0) return DEM_OK;
+    if (!s->d_walls) {
+        std::copy(s->w->x.begin(), s->w->x.end(), host);
+        return DEM_OK;
+    }
+    std::vector<WallGeom> now(nw);
+    dem_ctx *ctx = s->ctx;
+    CK(cudaMemcpyAsync(now.data(), s->d_walls, nw * sizeof(WallGeom), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int w = 0; w < nw; ++w)
+        for (int d = 0; d < 3; ++d) host[3 * w + d] = now[w].x[d];
+    return DEM_OK;
 }
 
 extern "C" int dem_solver_stats(dem_solver *s, dem_run_stats *out) {

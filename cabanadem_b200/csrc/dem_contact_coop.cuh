@@ -262,8 +262,9 @@ __device__ __forceinline__ void particle_coop(const Particles &P, const NbrList 
             double *swy = P.sw + (long)(P.mw + lw) * cap + ii;
             double *swz = P.sw + (long)(2 * P.mw + lw) * cap + ii;
             if (overlap > 0.) {
-                pw_wall<MIXED>(q, pi, nx, ny, nz, overlap, ui0, ui1, ui2, wi0, wi1, wi2, mIi.x, pw[mi * fc.nwall + w],
-                               K_n_pw, K_t_pw, mu_pw, fc.dt, (wmask0 & bit) != 0u, swx, swy, swz, cf);
+                pw_wall<MIXED>(q, pi, nx, ny, nz, overlap, ui0, ui1, ui2, wi0, wi1, wi2, g.u[0], g.u[1], g.u[2],
+                               mIi.x, pw[mi * fc.nwall + w], K_n_pw, K_t_pw, mu_pw, fc.dt, (wmask0 & bit) != 0u, swx,
+                               swy, swz, cf);
                 con = true;
             } else if (wmask0 & bit) {
                 *swx = 0.;

@@ -82,6 +82,7 @@ struct PairConst {   // per (material a, material b) or (material a, wall w)
 struct WallGeom {
     double x[3];
     double n[3];
+    double u[3];   // velocity (zero under DEM_Q6_WALL_STATIC): relative velocity of the contact
 };
 
 struct ForceConsts {
@@ -101,6 +102,8 @@ struct ForceConsts {
                                // more resident blocks, wider apply grid (same arithmetic)
     int coop;                  // lanes per deferred particle in the contact kernel: 4 or 8
                                // (cooperative, MaxCnts <= kCoopSlots), 0: one thread each
+    struct WallGeom *mwalls;   // the device walls when some wall moves (Q6 clear, nonzero
+                               // velocity): each step's finaliser advances x += dt u; else null
     int all;                   // 1: one kernel steps every particle (dense flows), no streaming
                                // or apply kernel; velocities ping-pong between their buffers
     const struct SceneConst *scenes;   // per-scene damping/friction, null: the scalars above

@@ -53,7 +53,7 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contact_mixed_all(Particles P,
         vmax2 = fmax(vmax2, v2);
         active += a;
     }
-    finish_step_counted(ctl, P.vslots, vmax2, fc.dt, status, active);
+    finish_step_counted(ctl, P.vslots, vmax2, fc.dt, status, active, c.last ? nullptr : fc.mwalls, fc.nwall);
 }
 
 __global__ void __launch_bounds__(kBlock) k_force_mixed(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,

@@ -118,11 +118,20 @@ __device__ __forceinline__ double vmax_collect_warp(unsigned long long *slots) {
     return __longlong_as_double((long long)v);
 }
 
+// Kinematic walls: x_w += dt u_w (the walls' stage2), by one full warp of the block that
+// finalises a step, after every particle of the step has used the current positions.
+__device__ __forceinline__ void advance_walls(WallGeom *walls, int nwall, double dt) {
+    if (!walls) return;
+    for (int w = threadIdx.x & 31; w < nwall; w += 32)
+        for (int d = 0; d < 3; ++d) walls[w].x[d] = dadd(walls[w].x[d], dmul(dt, walls[w].u[d]));
+}
+
 // Block max of |u|^2 folded into its slot, then the last block to finish advances the
 // control word: disp += dt*|u|max (conservative displacement bound), flips the position
 // buffer (and the velocity buffer when the kernel wrote the other one).
 __device__ __forceinline__ void finish_step(Ctl *ctl, unsigned long long *slots, double vmax2, double dt, int status,
-                                            bool count_step, bool flip_v = false) {
+                                            bool count_step, bool flip_v = false, WallGeom *mwalls = nullptr,
+                                            int nwall = 0) {
     __shared__ double red[32];
     __shared__ bool am_last;
     for (int o = 16; o > 0; o >>= 1) vmax2 = fmax(vmax2, __shfl_xor_sync(0xffffffffu, vmax2, o));
@@ -142,6 +151,7 @@ __device__ __forceinline__ void finish_step(Ctl *ctl, unsigned long long *slots,
     if (am_last && threadIdx.x < 32) {
         __threadfence();
         const double v2 = vmax_collect_warp(slots);
+        advance_walls(mwalls, nwall, dt);
         if (threadIdx.x == 0) {
             ctl->disp = ctl->disp + dt * sqrt(v2) * (1.0 + 1e-9);
             ctl->ndefer = 0;
@@ -161,7 +171,7 @@ __device__ __forceinline__ void finish_step(Ctl *ctl, unsigned long long *slots,
 // per thread; one atomic per block, added before the block's ticket) and leaves the count in last_ndefer,
 // where the host reads the step's density.  Flips the position and velocity buffers.
 __device__ __forceinline__ void finish_step_counted(Ctl *ctl, unsigned long long *slots, double vmax2, double dt,
-                                                    int status, int active) {
+                                                    int status, int active, WallGeom *mwalls, int nwall) {
     __shared__ int cnt_s[32];
     __shared__ double red[32];
     __shared__ bool am_last;
@@ -192,6 +202,7 @@ __device__ __forceinline__ void finish_step_counted(Ctl *ctl, unsigned long long
     if (am_last && threadIdx.x < 32) {
         __threadfence();
         const double v2 = vmax_collect_warp(slots);
+        advance_walls(mwalls, nwall, dt);   // null on the last step of a run (no next drift)
         if (threadIdx.x == 0) {
             ctl->disp = ctl->disp + dt * sqrt(v2) * (1.0 + 1e-9);
             ctl->last_ndefer = atomicAdd(&ctl->ndefer, 0);
@@ -430,6 +441,7 @@ template <bool MIXED>
 __device__ __forceinline__ void pw_wall(const unsigned q, const D4 &pi, const double nx, const double ny,
                                         const double nz, const double overlap, const double ui0, const double ui1,
                                         const double ui2, const double wi0, const double wi1, const double wi2,
+                                        const double uw0, const double uw1, const double uw2,
                                         const double m_i, const PairConst &c, const double K_n_pw,
                                         const double K_t_pw, const double mu_pw, const double dt,
                                         const bool has_hist, double *swx, double *swy, double *swz,
@@ -437,9 +449,9 @@ __device__ __forceinline__ void pw_wall(const unsigned q, const D4 &pi, const do
     if constexpr (MIXED) {
         const float ov = (float)overlap;
         const double da_i = pi.w - 0.5 * overlap;
-        const double dv0 = ui0 + (wi1 * nz - wi2 * ny) * da_i;
-        const double dv1 = ui1 + (wi2 * nx - wi0 * nz) * da_i;
-        const double dv2 = ui2 + (wi0 * ny - wi1 * nx) * da_i;
+        const double dv0 = ui0 + (wi1 * nz - wi2 * ny) * da_i - uw0;
+        const double dv1 = ui1 + (wi2 * nx - wi0 * nz) * da_i - uw1;
+        const double dv2 = ui2 + (wi0 * ny - wi1 * nx) * da_i - uw2;
         const double dvdn = dv0 * nx + dv1 * ny + dv2 * nz;
         const float fa_i = (float)da_i;
         const float gx = (float)nx, gy = (float)ny, gz = (float)nz;
@@ -503,9 +515,10 @@ __device__ __forceinline__ void pw_wall(const unsigned q, const D4 &pi, const do
         cf[5] = (double)((gx * ft1 - gy * ft0) * fa_i);
     } else {
         const double a_i = pi.w - overlap / 2.;
-        const double v0 = ui0 + (wi1 * nz - wi2 * ny) * a_i;
-        const double v1 = ui1 + (wi2 * nx - wi0 * nz) * a_i;
-        const double v2 = ui2 + (wi0 * ny - wi1 * nx) * a_i;
+        // contact-point velocity minus the wall's (vel_i - vel_j, Force.hpp:529-533)
+        const double v0 = ui0 + (wi1 * nz - wi2 * ny) * a_i - uw0;
+        const double v1 = ui1 + (wi2 * nx - wi0 * nz) * a_i - uw1;
+        const double v2 = ui2 + (wi0 * ny - wi1 * nx) * a_i - uw2;
         const double vdn = v0 * nx + v1 * ny + v2 * nz;
         const double vt0 = v0 - vdn * nx, vt1 = v1 - vdn * ny, vt2 = v2 - vdn * nz;
         const double R_eff = 1. / (1. / pi.w + 0.);
@@ -731,8 +744,8 @@ __device__ __forceinline__ void particle_full(const Particles &P, const NbrList 
         double *swz = P.sw + (long)(2 * P.mw + lw) * cap + i;
         if (overlap > 0.) {
             double cf[6];
-            pw_wall<MIXED>(q, pi, nx, ny, nz, overlap, ui0, ui1, ui2, wi0, wi1, wi2, mIi.x, pw[mi * fc.nwall + w], K_n_pw,
-                           K_t_pw, mu_pw, fc.dt, (wmask & bit) != 0u, swx, swy, swz, cf);
+            pw_wall<MIXED>(q, pi, nx, ny, nz, overlap, ui0, ui1, ui2, wi0, wi1, wi2, g.u[0], g.u[1], g.u[2], mIi.x,
+                           pw[mi * fc.nwall + w], K_n_pw, K_t_pw, mu_pw, fc.dt, (wmask & bit) != 0u, swx, swy, swz, cf);
             wmask |= bit;
             F0 += cf[0];
             F1 += cf[1];

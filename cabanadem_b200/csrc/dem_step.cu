@@ -205,7 +205,7 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contact_all(Particles P, NbrLi
         vmax2 = fmax(vmax2, v2);
         active += a;
     }
-    finish_step_counted(ctl, P.vslots, vmax2, fc.dt, status, active);
+    finish_step_counted(ctl, P.vslots, vmax2, fc.dt, status, active, c.last ? nullptr : fc.mwalls, fc.nwall);
 }
 
 // Fused step, kernel 3 of 3: commit the deferred particles' u and omega, then the last
@@ -238,6 +238,8 @@ __global__ void __launch_bounds__(kApplyBlock) k_apply(Particles P, NbrList L, C
     if (s_last && threadIdx.x < 32) {   // every block has taken its ticket: the slots are quiescent
         __threadfence();
         const double v2 = vmax_collect_warp(P.vslots);
+        // the walls drift with the particles' stage2 of the next step (none after a run's last step)
+        if (ctl->steps_done + 1 < ctl->target) advance_walls(fc.mwalls, fc.nwall, fc.dt);
         if (threadIdx.x == 0) {
             ctl->disp = ctl->disp + fc.dt * sqrt(v2) * (1.0 + 1e-9);
             ctl->last_ndefer = nd;
@@ -276,12 +278,13 @@ __global__ void __launch_bounds__(kBlock) k_prologue(Particles P, Ctl *ctl, Forc
         vmax2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
         st4(P.pos[nxt], i, p);
     }
-    finish_step(ctl, P.vslots, vmax2, fc.dt, 0, false);
+    finish_step(ctl, P.vslots, vmax2, fc.dt, 0, false, false, fc.mwalls, fc.nwall);
 }
 
 // Unfused Integrator stages, in place on the current buffer.
 __global__ void k_stage(Particles P, Ctl *ctl, ForceConsts fc, int stage) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (stage == 2 && i < 32) advance_walls(fc.mwalls, fc.nwall, fc.dt);   // block 0's first warp
     if (i >= P.n) return;
     const int cur = ctl->cur, vcur = ctl->vcur, cap = P.cap;
     double *vc = P.vel[vcur], *wc = P.omg[vcur];

@@ -27,7 +27,8 @@ Q2_ETA_T_ZERO = 0x02
 Q3_NO_PP_TORQUE = 0x04
 Q4_UNIT_HISTORY = 0x08
 Q5_WALL_FT_TYPO = 0x10
-REF_COMPAT = 0x1F
+Q6_WALL_STATIC = 0x20
+REF_COMPAT = 0x3F
 
 
 @dataclass
@@ -445,6 +446,17 @@ def random_box(n=4096, radius=1e-3, side=0.05, seed=1, vmax=0.1, max_cnts=16, qu
     w = _box_walls((0.0, 0.0, 0.0), (side, side, side), GLASS["E"], GLASS["nu"], s.G[0])
     return Scenario("random_box_4096", s, w, _force_params(0.8, 0.8, 0.3, 0.3, quirks), dt, nsteps,
                     skin=0.1 * radius, gravity=(0.0, 0.0, -9.81))
+
+
+def piston_box(n=4096, speed=2.0, seed=1, nsteps=400, quirks=REF_COMPAT & ~Q6_WALL_STATIC):
+    """random_box with its +x wall (wall 1) moved to touch the outermost sphere and driven
+    inwards at `speed` m/s: a kinematic wall (DEM_Q6_WALL_STATIC clear; the reference's walls
+    never move, src/CabanaDEM_Force.hpp:529)."""
+    sc = random_box(n=n, seed=seed, quirks=quirks, nsteps=nsteps)
+    sc.walls.x[1, 0] = float((sc.state.x[:, 0] + sc.state.rad).max())
+    sc.walls.u[1, 0] = -float(speed)
+    sc.name = "piston_box_%d" % n
+    return sc
 
 
 def hcp_box(n=2_000_000, rmin=0.8e-3, rmax=1.2e-3, seed=2, vmax=0.1, max_cnts=16, quirks=REF_COMPAT,

@@ -544,6 +544,14 @@ class SolverDEM {
         }
     }
     dem_solver *handle() { return h_; }
+    // current wall positions [nw][3]: a wall with a velocity moves by dt * u each step when the
+    // force's DEM_Q6_WALL_STATIC bit is clear (the reference's walls never move)
+    std::vector<double> wallPositions() {
+        std::vector<double> x(wall_ ? 3 * wall_->size() : 0);
+        particles_->context().check(dem_solver_wall_positions(h_, x.data(), (long)x.size()),
+                                    "dem_solver_wall_positions");
+        return x;
+    }
 
     int num_steps = 0;
     int output_frequency = 0;

@@ -43,7 +43,11 @@ extern "C" {
 #define DEM_Q3_NO_PP_TORQUE  0x04u /* src/CabanaDEM_Force.hpp:324-326                    */
 #define DEM_Q4_UNIT_HISTORY  0x08u /* src/CabanaDEM_Force.hpp:310-319                    */
 #define DEM_Q5_WALL_FT_TYPO  0x10u /* src/CabanaDEM_Force.hpp:624                        */
-#define DEM_REF_COMPAT       0x1Fu
+#define DEM_Q6_WALL_STATIC   0x20u /* src/CabanaDEM_Force.hpp:529: wall velocity ignored;
+                                    * clear: walls move with their velocity (x += dt u each
+                                    * step, with the particles' drift) and the wall contact uses
+                                    * the relative velocity                                  */
+#define DEM_REF_COMPAT       0x3Fu
 
 /* ---- particle fields for dem_particles_set/get (Particles.hpp:99-271) ------------ */
 enum dem_field {
@@ -162,6 +166,10 @@ int dem_solver_destroy(dem_solver *s);
  * displacement bound exceeds skin/2 (or every step when rebuild_every_step). */
 int dem_solver_run(dem_solver *s, int nsteps);
 int dem_solver_stats(dem_solver *s, dem_run_stats *out);
+/* Current wall positions [nw][3] (moving walls advance by dt * u each step when
+ * DEM_Q6_WALL_STATIC is clear; no reference counterpart: the reference's walls never move,
+ * src/CabanaDEM_Force.hpp:529). */
+int dem_solver_wall_positions(dem_solver *s, double *host, long count);
 /* Same steps as dem_solver_run, but each fused step kernel is launched on its own between
  * two CUDA events; *kernel_ms receives the mean duration of one fused step launch
  * (rebuilds excluded).  For roofline measurement; no reference counterpart. */

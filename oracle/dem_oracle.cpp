@@ -154,6 +154,12 @@ extern "C" void orc_stage2(orc_particles *p, double dt) {
         for (int d = 0; d < 3; ++d) p->x[3 * i + d] += dt * p->u[3 * i + d];
 }
 
+extern "C" void orc_stage2_walls(const orc_walls *w, double dt) {
+    if (!w || !w->u) return;
+    for (int j = 0; j < w->n; ++j)
+        for (int d = 0; d < 3; ++d) w->x[3 * j + d] += dt * w->u[3 * j + d];
+}
+
 extern "C" void orc_stage3(orc_particles *p, double dt) { orc_stage1(p, dt); }
 
 // src/CabanaDEM_Force.hpp:40-47
@@ -383,7 +389,7 @@ extern "C" int orc_force_pp(orc_particles *p, const orc_nlist *nl, const orc_for
 
 // ---------------------------------------------------------------------------------
 // src/CabanaDEM_Force.hpp:448-678: particle against each infinite plane, in wall order.
-// Wall velocity is not used (:529).
+// Wall velocity is not used (:529, Q6); with Q6 clear vel_j is the wall's velocity.
 // ---------------------------------------------------------------------------------
 extern "C" void orc_force_wall(orc_particles *p, const orc_walls *w, const orc_force_params *fp, double dt) {
     const int mw = p->max_walls;
@@ -409,6 +415,8 @@ extern "C" void orc_force_wall(orc_particles *p, const orc_walls *w, const orc_f
             vel_i[1] = u[3 * i + 1] + (omega[3 * i + 2] * nij_x - omega[3 * i + 0] * nij_z) * a_i;
             vel_i[2] = u[3 * i + 2] + (omega[3 * i + 0] * nij_y - omega[3 * i + 1] * nij_x) * a_i;
             double vel_j[3] = {0., 0., 0.};
+            if (!(q & ORC_Q6_WALL_STATIC) && w->u)
+                for (int d = 0; d < 3; ++d) vel_j[d] = w->u[3 * j + d];
             double vel_ij[3] = {vel_i[0] - vel_j[0], vel_i[1] - vel_j[1], vel_i[2] - vel_j[2]};
             double vij_dot_nij = vel_ij[0] * nij_x + vel_ij[1] * nij_y + vel_ij[2] * nij_z;
             double vn_x = vij_dot_nij * nij_x;
@@ -523,6 +531,7 @@ extern "C" int orc_step(orc_particles *p, const orc_walls *w, const orc_force_pa
                         orc_nlist *nl, double dt, double delta, double skin) {
     orc_stage1(p, dt);
     orc_stage2(p, dt);
+    if (w && w->n > 0 && !(fp->quirks & ORC_Q6_WALL_STATIC)) orc_stage2_walls(w, dt);
     orc_nlist_build(nl, p, delta, skin);
     orc_zero_force(p);
     orc_apply_ext_force(p, h);

@@ -33,7 +33,8 @@ extern "C" {
 #define ORC_Q3_NO_PP_TORQUE   0x04u /* Force.hpp:324-326: pp contact adds no torque      */
 #define ORC_Q4_UNIT_HISTORY   0x08u /* Force.hpp:310-319: history stored normalised      */
 #define ORC_Q5_WALL_FT_TYPO   0x10u /* Force.hpp:624: ft_z*ft_y in |ft|                   */
-#define ORC_REF_COMPAT        0x1Fu
+#define ORC_Q6_WALL_STATIC    0x20u /* Force.hpp:529: vel_j = 0, walls never move          */
+#define ORC_REF_COMPAT        0x3Fu
 
 /* pow handling: 0 = libm pow() exactly as the reference; 1 = x*sqrt(x) and sqrt(x)
  * for pow(x,1.5) and pow(x,0.5) (the device kernels' arithmetic). */
@@ -62,9 +63,10 @@ typedef struct orc_particles {
 
 typedef struct orc_walls {
     int n;
-    double *x;        /* [n*3] point on the plane */
+    double *x;        /* [n*3] point on the plane (advanced in place by moving walls) */
     double *normal;   /* [n*3] unit normal        */
     double *E, *nu, *G;
+    double *u;        /* [n*3] velocity, or NULL: used only with ORC_Q6_WALL_STATIC clear */
 } orc_walls;
 
 typedef struct orc_force_params {
@@ -94,6 +96,8 @@ void orc_nlist_copy(const orc_nlist *nl, int *offsets /*n+1*/, int *idx /*total*
 
 void orc_stage1(orc_particles *p, double dt);
 void orc_stage2(orc_particles *p, double dt);
+/* Kinematic walls (no reference counterpart): x_w += dt * u_w, with the particles' drift. */
+void orc_stage2_walls(const orc_walls *w, double dt);
 void orc_stage3(orc_particles *p, double dt);
 void orc_zero_force(orc_particles *p);
 void orc_update_tangential_contacts(orc_particles *p);

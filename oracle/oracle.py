@@ -20,7 +20,8 @@ Q2_ETA_T_ZERO = 0x02
 Q3_NO_PP_TORQUE = 0x04
 Q4_UNIT_HISTORY = 0x08
 Q5_WALL_FT_TYPO = 0x10
-REF_COMPAT = 0x1F
+Q6_WALL_STATIC = 0x20
+REF_COMPAT = 0x3F
 POW_LIBM = 0
 POW_SQRT = 1
 BQ10_INDEX_BY_J = 0x01
@@ -41,7 +42,7 @@ class _Particles(C.Structure):
 
 
 class _Walls(C.Structure):
-    _fields_ = [("n", C.c_int), ("x", _dp), ("normal", _dp), ("E", _dp), ("nu", _dp), ("G", _dp)]
+    _fields_ = [("n", C.c_int), ("x", _dp), ("normal", _dp), ("E", _dp), ("nu", _dp), ("G", _dp), ("u", _dp)]
 
 
 class _ForceParams(C.Structure):
@@ -129,6 +130,7 @@ def _walls(w):
     c.n = w.n
     c.x, c.normal = _ptr(w.x, _dp), _ptr(w.normal, _dp)
     c.E, c.nu, c.G = _ptr(w.E, _dp), _ptr(w.nu, _dp), _ptr(w.G, _dp)
+    c.u = _ptr(w.u, _dp)   # velocity: used with Q6 clear; x is then advanced in place
     return c
 
 

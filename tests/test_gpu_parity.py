@@ -125,6 +125,28 @@ def test_contact_kernel_forms_bitwise(lanes):
         assert s.stats()["launches"] < t.stats()["launches"] - 400
 
 
+@pytest.mark.parametrize("lanes", [0, 1, 8], ids=["auto", "per_thread", "coop8"])
+def test_moving_wall_bitwise(lanes):
+    """A kinematic piston (DEM_Q6_WALL_STATIC clear) driven into a compressed box at 5 m/s,
+    400 steps in three runs (each run's last step must not move the walls, its next run's
+    first drift must): particles and wall positions bit-identical to the oracle."""
+    sc = S.piston_box(n=4096, speed=5.0, nsteps=400)
+    c = sc.state.x.mean(axis=0)
+    sc.state.x[:] = c + (sc.state.x - c) * 0.8
+    sc.walls.x[1, 0] = float((sc.state.x[:, 0] + sc.state.rad).max())   # touching the compressed box
+    ref = sc.state.copy()
+    w = sc.walls.copy()
+    O.run(ref, w, sc.params, sc.dt, 400, skin=sc.skin, gravity=sc.gravity, pow_mode=O.POW_SQRT)
+    s = api.from_scenario(sc, contact_lanes=lanes)
+    for n in (150, 101, 149):
+        s.run_steps(n)
+    _assert_bitwise(s.particles.download(), ref, where="piston%d" % lanes)
+    assert np.array_equal(s.wall_positions(), w.x)
+    assert w.x[1, 0] < sc.walls.x[1, 0]
+    # particles in sliding contact with the piston (history tangential to its normal, -x)
+    assert ((ref.tng_sw_y[:, 1] != 0) | (ref.tng_sw_z[:, 1] != 0)).any()
+
+
 @pytest.mark.parametrize("lanes", [1, 8], ids=["per_thread", "coop8"])
 def test_contact_overflow_all_kernels(lanes):
     """Slot overflow (MaxCnts 2) through either contact kernel: status bit and state as the oracle."""
