@@ -107,6 +107,8 @@ _PROTOS = {
     "dem_solver_run": ([_VP, C.c_int], C.c_int),
     "dem_solver_stats": ([_VP, C.POINTER(RunStats)], C.c_int),
     "dem_solver_wall_positions": ([_VP, _VP, C.c_long], C.c_int),
+    "dem_solver_set_mesh": ([_VP, _VP, C.c_int, C.c_double, C.c_double, C.c_double, _VP, C.c_int], C.c_int),
+    "dem_solver_mesh_translation": ([_VP, _VP], C.c_int),
     "dem_solver_profile": ([_VP, C.c_int, C.POINTER(C.c_double)], C.c_int),
     "dem_ctx_stream": ([_VP], C.c_void_p),
     "dem_stage1": ([_VP], C.c_int),

@@ -282,6 +282,22 @@ class SolverDEM:
         self.last_status = st
         return check(st, self.particles.ctx.h, "dem_solver_run", allow=allow)
 
+    def set_mesh(self, tri, E, nu, G, velocity=None, max_contacts=8):
+        """Triangle-mesh wall: tri [nt, 3, 3] vertex coordinates, one material, optional
+        translation velocity (applied when the force's DEM_Q6_WALL_STATIC bit is clear)
+        (dem_solver_set_mesh)."""
+        t = np.ascontiguousarray(tri, dtype=np.float64).reshape(-1, 9)
+        v = None if velocity is None else np.ascontiguousarray(velocity, dtype=np.float64)
+        check(lib().dem_solver_set_mesh(self.h, t.ctypes.data if t.size else None, t.shape[0], float(E), float(nu),
+                                        float(G), v.ctypes.data if v is not None else None, int(max_contacts)),
+              self.particles.ctx.h, "dem_solver_set_mesh")
+
+    def mesh_translation(self):
+        out = np.zeros(3)
+        check(lib().dem_solver_mesh_translation(self.h, out.ctypes.data), self.particles.ctx.h,
+              "dem_solver_mesh_translation")
+        return out
+
     def wall_positions(self):
         """Current positions [nw, 3] of the solver's walls: walls with a velocity move by
         dt * u each step when the force's DEM_Q6_WALL_STATIC bit is clear."""
@@ -395,6 +411,9 @@ def from_scenario(sc, ctx: Context | None = None, rebuild_every_step=False, prec
     if sc.extra.get("scene") is not None:
         p.set("scene", sc.extra["scene"])
         s.set_scenes(sc.extra["scene_params"], sc.extra["walls_per_scene"])
+    m = sc.extra.get("mesh")
+    if m is not None:
+        s.set_mesh(m.tri, m.E, m.nu, m.G, velocity=m.u, max_contacts=m.max_contacts)
     return s
 
 

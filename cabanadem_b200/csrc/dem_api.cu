@@ -64,6 +64,13 @@ struct dem_solver {
     WallGeom *d_walls = nullptr;
     std::vector<double> wall_pos;   // wall positions at the last preparation ([nw][3])
     bool walls_move = false;        // some wall has a velocity and Q6 is clear
+    // triangle-mesh wall (dem_solver_set_mesh): host copy of its definition, device arrays
+    int mesh_nt = 0;
+    double mesh_mat[3] = {0., 0., 0.};   // E, nu, G
+    double mesh_u[3] = {0., 0., 0.};
+    MeshDev mesh{};                 // device arrays (tri, D, tid, th, cnt, cand, ncand); pm set by prepare
+    MeshDev mesh_alt{};             // tid, th, cnt of the re-sort
+    PairConst *d_mesh_pm = nullptr;
     SceneConst *d_scenes = nullptr;
     int nscenes = 0, wps = 0;
     bool walls_ok = true;
@@ -735,10 +742,33 @@ int prepare(dem_solver *s) {
     CK(cudaMemcpyAsync(s->d_pp, pp.data(), pp.size() * sizeof(PairConst), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(s->d_pw, pw.data(), pw.size() * sizeof(PairConst), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(s->d_walls, wg.data(), wg.size() * sizeof(WallGeom), cudaMemcpyHostToDevice, st));
+    // mesh: particle materials against the mesh's, in the plane walls' expression order
+    cudaFree(s->d_mesh_pm);
+    s->d_mesh_pm = nullptr;
+    if (s->mesh_nt > 0) {
+        std::vector<PairConst> pm(std::max(nm, 1));
+        for (int a = 0; a < nm; ++a) {
+            const auto &A = p->mats[a];
+            pm[a] = pair_const(std::get<0>(A), std::get<1>(A), std::get<2>(A), s->mesh_mat[0], s->mesh_mat[1],
+                               s->mesh_mat[2]);
+        }
+        CK(dalloc(&s->d_mesh_pm, pm.size()));
+        CK(cudaMemcpyAsync(s->d_mesh_pm, pm.data(), pm.size() * sizeof(PairConst), cudaMemcpyHostToDevice, st));
+    }
     ForceConsts &fc = s->fc;
     fc = ForceConsts{};
     s->walls_move = moving;
     fc.mwalls = moving ? s->d_walls : nullptr;
+    if (s->mesh_nt > 0) {
+        fc.mesh = s->mesh;
+        fc.mesh.pm = s->d_mesh_pm;
+        bool mv = false;
+        for (int d = 0; d < 3; ++d) {
+            fc.mesh.u[d] = wall_static ? 0.0 : s->mesh_u[d];
+            mv = mv || fc.mesh.u[d] != 0.0;
+        }
+        fc.mesh_moving = mv ? 1 : 0;
+    }
     const unsigned q = s->fp.quirks;
     const double bpp = beta_of(s->fp.cor_pp), bpw = beta_of(s->fp.cor_pw);
     fc.K_n_pp = -2. * std::sqrt(5. / 6.) * bpp;             // Force.hpp:215
@@ -862,10 +892,25 @@ int build_with(dem_solver *s, bool resort, double delta, double skin) {
     for (int attempt = 0; attempt < 8; ++attempt) {
         launch_build(s->p->P, s->p->alt, s->L, s->B, s->p->ctl, delta, skin, resort, false, ctx->stream);
         s->launches += build_kernel_count(resort);
+        if (resort && s->mesh_nt > 0) {   // tracked triangle contacts follow the re-sort (B.key: new <- old)
+            const size_t cap = (size_t)s->p->P.cap;
+            const MeshDev &M = s->mesh, &A = s->mesh_alt;
+            launch_permute_mesh(M, A, s->p->P.n, s->p->P.cap, s->B.key, ctx->stream);
+            s->launches += 1;
+            CK(cudaMemcpyAsync(M.tid, A.tid, (size_t)M.mt * cap * sizeof(int), cudaMemcpyDeviceToDevice, ctx->stream));
+            CK(cudaMemcpyAsync(M.th, A.th, 3 * (size_t)M.mt * cap * sizeof(double), cudaMemcpyDeviceToDevice,
+                               ctx->stream));
+            CK(cudaMemcpyAsync(M.cnt, A.cnt, cap, cudaMemcpyDeviceToDevice, ctx->stream));
+        }
         CK(cudaGetLastError());
         Ctl c = read_ctl(s);
         CK(cudaGetLastError());
         if (!(c.status & DEM_ERR_NEIGHBOR_OVERFLOW)) {
+            if (s->mesh_nt > 0) {
+                launch_mesh_candidates(s->p->P, s->fc.mesh, s->p->ctl, delta, skin, ctx->stream);
+                s->launches += 1;
+                CK(cudaGetLastError());
+            }
             s->built = true;
             s->p->dirty = false;
             return DEM_OK;
@@ -889,12 +934,15 @@ int capture_graph(dem_solver *s, int steps) {
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < steps; ++k) {
-        if (ref_mode(s))
+        if (ref_mode(s)) {
             launch_build(s->p->P, s->p->alt, s->L, s->B, s->p->ctl, s->sp.delta, s->sp.skin, false, true, ctx->stream);
+            if (s->mesh_nt > 0) launch_mesh_candidates(s->p->P, s->fc.mesh, s->p->ctl, s->sp.delta, s->sp.skin, ctx->stream);
+        }
         launch_step(s->p->P, s->L, s->p->ctl, s->fc, s->d_pp, s->d_pw, s->d_walls, MODE_FUSED, ctx->stream);
     }
     CK(cudaStreamEndCapture(ctx->stream, &g));
-    s->graph_nodes = (long)steps * (kernels_per_step(s->fc) + (ref_mode(s) ? build_kernel_count(false) : 0));
+    s->graph_nodes = (long)steps * (kernels_per_step(s->fc) +
+                                    (ref_mode(s) ? build_kernel_count(false) + (s->mesh_nt > 0 ? 1 : 0) : 0));
     cudaError_t e = cudaGraphInstantiate(&s->graph, g, 0);
     cudaGraphDestroy(g);
     CK(e);
@@ -953,6 +1001,24 @@ extern "C" int dem_solver_create(dem_ctx *ctx, dem_particles *p, dem_walls *w, c
     return DEM_OK;
 }
 
+static void free_mesh(dem_solver *s) {
+    cudaFree(const_cast<double *>(s->mesh.tri));
+    cudaFree(s->mesh.D);
+    cudaFree(s->mesh.tid);
+    cudaFree(s->mesh.th);
+    cudaFree(s->mesh.cnt);
+    cudaFree(s->mesh.cand);
+    cudaFree(s->mesh.ncand);
+    cudaFree(s->mesh_alt.tid);
+    cudaFree(s->mesh_alt.th);
+    cudaFree(s->mesh_alt.cnt);
+    cudaFree(s->d_mesh_pm);
+    s->mesh = MeshDev{};
+    s->mesh_alt = MeshDev{};
+    s->d_mesh_pm = nullptr;
+    s->mesh_nt = 0;
+}
+
 extern "C" int dem_solver_destroy(dem_solver *s) {
     if (!s) return DEM_ERR_INVALID;
     cudaStreamSynchronize(s->ctx->stream);
@@ -966,7 +1032,74 @@ extern "C" int dem_solver_destroy(dem_solver *s) {
     cudaFree(B.block_sums); cudaFree(B.bbox); cudaFree(B.src); cudaFree(B.dst);
     cudaFree(B.part_sums);
     cudaFree(s->d_epart); cudaFree(s->d_eout);
+    free_mesh(s);
     delete s;
+    return DEM_OK;
+}
+
+extern "C" int dem_solver_set_mesh(dem_solver *s, const double *tri, int nt, double E, double nu, double G,
+                                   const double *velocity, int max_contacts) {
+    if (!s) return DEM_ERR_INVALID;
+    dem_ctx *ctx = s->ctx;
+    if (nt < 0 || nt > kMeshMaxTri || (nt > 0 && !tri))
+        return fail(ctx, DEM_ERR_INVALID, "dem_solver_set_mesh: 0 <= triangles <= 4096");
+    if (nt > 0 && (max_contacts < 1 || max_contacts > kMeshMaxContacts))
+        return fail(ctx, DEM_ERR_INVALID, "dem_solver_set_mesh: 1 <= max_contacts <= 16");
+    if (nt > 0 && !(E > 0. && G > 0.)) return fail(ctx, DEM_ERR_INVALID, "dem_solver_set_mesh: E, G > 0");
+    if (nt > 0 && (s->nscenes > 0 || s->p->has_bonds))
+        return fail(ctx, DEM_ERR_UNSUPPORTED, "dem_solver_set_mesh: not with batched scenes or bonds");
+    CK(cudaStreamSynchronize(ctx->stream));
+    free_mesh(s);
+    if (nt > 0) {
+        const size_t cap = (size_t)s->p->P.cap;
+        MeshDev &M = s->mesh;
+        double *dtri = nullptr;
+        cudaError_t e = cudaSuccess;
+        auto A = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
+        A(dalloc(&dtri, 9 * (size_t)nt));
+        A(dalloc(&M.D, 3));
+        A(dalloc(&M.tid, (size_t)max_contacts * cap));
+        A(dalloc(&M.th, 3 * (size_t)max_contacts * cap));
+        A(dalloc(&M.cnt, cap));
+        A(dalloc(&M.cand, (size_t)kMeshCand * cap));
+        A(dalloc(&M.ncand, cap));
+        A(dalloc(&s->mesh_alt.tid, (size_t)max_contacts * cap));
+        A(dalloc(&s->mesh_alt.th, 3 * (size_t)max_contacts * cap));
+        A(dalloc(&s->mesh_alt.cnt, cap));
+        M.tri = dtri;
+        if (e != cudaSuccess) {
+            free_mesh(s);
+            return cuda_check(ctx, e, "dem_solver_set_mesh");
+        }
+        cudaStream_t st = ctx->stream;
+        CK(cudaMemcpyAsync(dtri, tri, 9 * (size_t)nt * sizeof(double), cudaMemcpyHostToDevice, st));
+        CK(cudaMemsetAsync(M.D, 0, 3 * sizeof(double), st));
+        CK(cudaMemsetAsync(M.tid, 0xff, (size_t)max_contacts * cap * sizeof(int), st));   // -1
+        CK(cudaMemsetAsync(M.th, 0, 3 * (size_t)max_contacts * cap * sizeof(double), st));
+        CK(cudaMemsetAsync(M.cnt, 0, cap, st));
+        CK(cudaMemsetAsync(M.ncand, 0, cap, st));
+        M.nt = nt;
+        M.mt = max_contacts;
+        s->mesh_alt.nt = nt;
+        s->mesh_alt.mt = max_contacts;
+        s->mesh_nt = nt;
+        s->mesh_mat[0] = E;
+        s->mesh_mat[1] = nu;
+        s->mesh_mat[2] = G;
+        for (int d = 0; d < 3; ++d) s->mesh_u[d] = velocity ? velocity[d] : 0.0;
+        CK(cudaStreamSynchronize(st));
+    }
+    s->built = false;
+    return prepare(s);
+}
+
+extern "C" int dem_solver_mesh_translation(dem_solver *s, double *host3) {
+    if (!s || !host3) return DEM_ERR_INVALID;
+    host3[0] = host3[1] = host3[2] = 0.0;
+    if (s->mesh_nt == 0) return DEM_OK;
+    dem_ctx *ctx = s->ctx;
+    CK(cudaMemcpyAsync(host3, s->mesh.D, 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
     return DEM_OK;
 }
 

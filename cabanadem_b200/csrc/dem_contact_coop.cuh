@@ -31,7 +31,7 @@ __device__ __forceinline__ int nth_high_bit(unsigned b, int r) {
 // Warp-collective: all 32 lanes call it; the groups of lanes [g NL, g NL + NL) each take one
 // particle i (i < 0: no particle, the group still takes part in the warp's shuffles).  t is
 // the particle's deferred slot.  s_tidx / s_h are the group's shared slots.
-template <int NL, bool MIXED>
+template <int NL, bool MIXED, bool MESH = false>
 __device__ __forceinline__ void particle_coop(const Particles &P, const NbrList &L, const ForceConsts &fc,
                                               const PairConst *__restrict__ pp, const PairConst *__restrict__ pw,
                                               const WallGeom *__restrict__ walls, const int cur, const int nxt,
@@ -296,7 +296,17 @@ __device__ __forceinline__ void particle_coop(const Particles &P, const NbrList 
     }
     if (!act || gl != 0) return;
 
-    // ---- the group's first lane: contact state, hooks, integration (as particle_full)
+    // ---- the group's first lane: mesh contacts, contact state, hooks, integration (as particle_full)
+    if constexpr (MESH) {
+        double FT[6] = {F0, F1, F2, T0, T1, T2};
+        mesh_pass<MIXED>(P, fc, i, pi, ui0, ui1, ui2, wi0, wi1, wi2, mIi.x, mi, K_n_pw, K_t_pw, mu_pw, FT, &status);
+        F0 = FT[0];
+        F1 = FT[1];
+        F2 = FT[2];
+        T0 = FT[3];
+        T1 = FT[4];
+        T2 = FT[5];
+    }
     const unsigned wrange = nwall >= 32 ? FULL : ((1u << nwall) - 1u);
     const unsigned wmask = (wmask0 & ~wrange) | wset;
     const int cs1 = cnt | (int)(wmask << 8);
@@ -353,7 +363,7 @@ __device__ __forceinline__ void particle_coop(const Particles &P, const NbrList 
 // Fused step, kernel 2 of 3 in its cooperative form: NL lanes per deferred particle, warps
 // striding over the deferred list in groups of 32 / NL.  No block barrier: a warp past the
 // list leaves at once, and the velocity bound is folded per warp.
-template <int NL, int MINB, bool MIXED>
+template <int NL, int MINB, bool MIXED, bool MESH = false>
 __global__ void __launch_bounds__(kBlock, MINB) k_contact_coop(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
                                                                const PairConst *__restrict__ pp,
                                                                const PairConst *__restrict__ pw,
@@ -378,7 +388,7 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contact_coop(Particles P, NbrL
         const int t = base + grp;
         const int i = t < nd ? L.defer[t] : -1;
         double v2 = 0.0;
-        particle_coop<NL, MIXED>(P, L, fc, pp, pw, walls, cur, cur ^ 1, vcur, last, i, t, s_tidx[sg], s_h[sg], v2,
+        particle_coop<NL, MIXED, MESH>(P, L, fc, pp, pw, walls, cur, cur ^ 1, vcur, last, i, t, s_tidx[sg], s_h[sg], v2,
                                  status);
         vmax2 = fmax(vmax2, v2);
     }

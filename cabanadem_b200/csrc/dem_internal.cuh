@@ -85,6 +85,24 @@ struct WallGeom {
     double u[3];   // velocity (zero under DEM_Q6_WALL_STATIC): relative velocity of the contact
 };
 
+// Triangle-mesh wall on the device (one per solver).  Candidates: every triangle within the
+// list cutoff of a particle at the last neighbour build, ascending id.
+constexpr int kMeshCand = 32;      // candidate triangles per particle
+constexpr int kMeshMaxTri = 4096;  // triangles per mesh (candidates are found by brute force)
+constexpr int kMeshMaxContacts = 16;   // tracked triangle contacts per particle (upper bound)
+struct MeshDev {
+    int nt, mt;                    // triangles; tracked triangle contacts per particle
+    const double *tri;             // [nt][9]: a, b, c at zero translation
+    double *D;                     // [3] translation (advanced by the step finaliser when moving)
+    double u[3];                   // velocity (zero for a static mesh)
+    const struct PairConst *pm;    // [nmat] particle material against the mesh
+    int *tid;                      // [mt][cap] triangle of each tracked contact
+    double *th;                    // [3][mt][cap] tangential history
+    unsigned char *cnt;            // [cap] tracked contacts
+    int *cand;                     // [kMeshCand][cap]
+    unsigned char *ncand;          // [cap]
+};
+
 struct ForceConsts {
     double K_n_pp, K_t_pp;     // eta = K * sqrt(S * m_eff)       (Force.hpp:215, :224)
     double K_n_pw, K_t_pw;     //                                  (Force.hpp:580, :618)
@@ -102,6 +120,8 @@ struct ForceConsts {
                                // more resident blocks, wider apply grid (same arithmetic)
     int coop;                  // lanes per deferred particle in the contact kernel: 4 or 8
                                // (cooperative, MaxCnts <= kCoopSlots), 0: one thread each
+    MeshDev mesh;              // triangle-mesh wall (nt == 0: none)
+    int mesh_moving;           // the mesh translates each step (Q6 clear, nonzero velocity)
     struct WallGeom *mwalls;   // the device walls when some wall moves (Q6 clear, nonzero
                                // velocity): each step's finaliser advances x += dt u; else null
     int all;                   // 1: one kernel steps every particle (dense flows), no streaming
@@ -183,20 +203,22 @@ void launch_bond_broken_count(const Bonds &B, int n, unsigned long long *out, cu
 // force-only kernel.  MODE_FUSED_DIRECT is the per-particle body of the one-kernel dense step.
 enum StepMode { MODE_FUSED = 0, MODE_FORCE_ONLY = 1, MODE_FUSED_DIRECT = 2 };
 int kernels_per_step(const ForceConsts &fc);
+void launch_mesh_candidates(const Particles &P, const MeshDev &M, Ctl *ctl, double delta, double skin, cudaStream_t s);
+void launch_permute_mesh(const MeshDev &M, const MeshDev &A, int n, int cap, const int *items, cudaStream_t s);
 void launch_prologue(const Particles &P, Ctl *ctl, const ForceConsts &fc, cudaStream_t s);
 void launch_step(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
                  const PairConst *pw, const WallGeom *walls, int mode, cudaStream_t s);
 void launch_stage(const Particles &P, Ctl *ctl, const ForceConsts &fc, int stage, cudaStream_t s);
 // dem_mixed.cu
 void launch_contact_mixed_all(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc,
-                              const PairConst *pp, const PairConst *pw, const WallGeom *walls, int blocks,
+                              const PairConst *pp, const PairConst *pw, const WallGeom *walls, int blocks, bool mesh,
                               cudaStream_t s);
-const void *contact_mixed_all_kernel();
+const void *contact_mixed_all_kernel(bool mesh);
 void launch_contact_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
-                          const PairConst *pw, const WallGeom *walls, int blocks, cudaStream_t s);
+                          const PairConst *pw, const WallGeom *walls, bool mesh, int blocks, cudaStream_t s);
 void launch_force_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
-                        const PairConst *pw, const WallGeom *walls, cudaStream_t s);
-const void *contact_mixed_kernel(int dense, int coop);
+                        const PairConst *pw, const WallGeom *walls, bool mesh, cudaStream_t s);
+const void *contact_mixed_kernel(int dense, int coop, bool mesh);
 void launch_energy(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
                    const PairConst *pw, const WallGeom *walls, double *partials, int nparts, double *out,
                    cudaStream_t s);

@@ -13,7 +13,7 @@ namespace b200dem {
 
 namespace {
 
-template <int MINB>
+template <int MINB, bool MESH = false>
 __global__ void __launch_bounds__(kBlock, MINB) k_contact_mixed(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
                                                           const PairConst *__restrict__ pp,
                                                           const PairConst *__restrict__ pw,
@@ -28,14 +28,15 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contact_mixed(Particles P, Nbr
     int status = 0;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nd; t += gridDim.x * blockDim.x) {
         double v2 = 0.0;
-        particle_full<MODE_FUSED, true>(P, L, fc, pp, pw, walls, cur, cur ^ 1, vcur, last, L.defer[t], t, v2, status);
+        particle_full<MODE_FUSED, true, MESH>(P, L, fc, pp, pw, walls, cur, cur ^ 1, vcur, last, L.defer[t], t, v2,
+                                              status);
         vmax2 = fmax(vmax2, v2);
     }
     block_vmax(ctl, P.vslots, vmax2, status);
 }
 
 // One-kernel dense step in mixed precision (see k_contact_all in dem_step.cu).
-template <int MINB>
+template <int MINB, bool MESH = false>
 __global__ void __launch_bounds__(kBlock, MINB) k_contact_mixed_all(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
                                                               const PairConst *__restrict__ pp,
                                                               const PairConst *__restrict__ pw,
@@ -48,14 +49,15 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contact_mixed_all(Particles P,
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += gridDim.x * blockDim.x) {
         double v2 = 0.0;
         int a = 0;
-        particle_full<MODE_FUSED_DIRECT, true>(P, L, fc, pp, pw, walls, c.cur, c.cur ^ 1, vcur, c.last, i, i, v2,
+        particle_full<MODE_FUSED_DIRECT, true, MESH>(P, L, fc, pp, pw, walls, c.cur, c.cur ^ 1, vcur, c.last, i, i, v2,
                                                status, &a);
         vmax2 = fmax(vmax2, v2);
         active += a;
     }
-    finish_step_counted(ctl, P.vslots, vmax2, fc.dt, status, active, c.last ? nullptr : fc.mwalls, fc.nwall);
+    finish_step_counted(ctl, P.vslots, vmax2, fc.dt, status, active, fc, !c.last);
 }
 
+template <bool MESH>
 __global__ void __launch_bounds__(kBlock) k_force_mixed(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
                                                         const PairConst *__restrict__ pp,
                                                         const PairConst *__restrict__ pw,
@@ -65,41 +67,66 @@ __global__ void __launch_bounds__(kBlock) k_force_mixed(Particles P, NbrList L, 
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double vmax2 = 0.0;
     int status = 0;
-    if (i < P.n) particle_full<MODE_FORCE_ONLY, true>(P, L, fc, pp, pw, walls, cur, cur ^ 1, vcur, 1, i, 0, vmax2, status);
+    if (i < P.n)
+        particle_full<MODE_FORCE_ONLY, true, MESH>(P, L, fc, pp, pw, walls, cur, cur ^ 1, vcur, 1, i, 0, vmax2, status);
     if (status) atomicOr(&ctl->status, status);
 }
 
 }  // namespace
 
-void launch_contact_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
-                          const PairConst *pw, const WallGeom *walls, int blocks, cudaStream_t s) {
+template <bool MESH>
+static void contact_mixed_t(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
+                            const PairConst *pw, const WallGeom *walls, int blocks, cudaStream_t s) {
     if (fc.coop == 8)
-        k_contact_coop<8, kCoopMinBlocks, true><<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+        k_contact_coop<8, kCoopMinBlocks, true, MESH><<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
     else if (fc.coop == 4)
-        k_contact_coop<4, kCoopMinBlocks, true><<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+        k_contact_coop<4, kCoopMinBlocks, true, MESH><<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
     else if (fc.dense)
-        k_contact_mixed<kContactMixedMinBlocksDense><<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+        k_contact_mixed<kContactMixedMinBlocksDense, MESH><<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
     else
-        k_contact_mixed<1><<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+        k_contact_mixed<1, MESH><<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+}
+
+void launch_contact_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
+                          const PairConst *pw, const WallGeom *walls, bool mesh, int blocks, cudaStream_t s) {
+    if (mesh)
+        contact_mixed_t<true>(P, L, ctl, fc, pp, pw, walls, blocks, s);
+    else
+        contact_mixed_t<false>(P, L, ctl, fc, pp, pw, walls, blocks, s);
 }
 
 void launch_contact_mixed_all(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc,
-                              const PairConst *pp, const PairConst *pw, const WallGeom *walls, int blocks,
+                              const PairConst *pp, const PairConst *pw, const WallGeom *walls, int blocks, bool mesh,
                               cudaStream_t s) {
-    k_contact_mixed_all<kContactMixedMinBlocksDense><<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+    if (mesh)
+        k_contact_mixed_all<kContactMixedMinBlocksDense, true><<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+    else
+        k_contact_mixed_all<kContactMixedMinBlocksDense, false><<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
 }
 
-const void *contact_mixed_all_kernel() { return (const void *)k_contact_mixed_all<kContactMixedMinBlocksDense>; }
+const void *contact_mixed_all_kernel(bool mesh) {
+    return mesh ? (const void *)k_contact_mixed_all<kContactMixedMinBlocksDense, true>
+                : (const void *)k_contact_mixed_all<kContactMixedMinBlocksDense, false>;
+}
 
 void launch_force_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
-                        const PairConst *pw, const WallGeom *walls, cudaStream_t s) {
-    k_force_mixed<<<(P.n + kBlock - 1) / kBlock, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+                        const PairConst *pw, const WallGeom *walls, bool mesh, cudaStream_t s) {
+    if (mesh)
+        k_force_mixed<true><<<(P.n + kBlock - 1) / kBlock, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+    else
+        k_force_mixed<false><<<(P.n + kBlock - 1) / kBlock, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
 }
 
-const void *contact_mixed_kernel(int dense, int coop) {
-    if (coop == 8) return (const void *)k_contact_coop<8, kCoopMinBlocks, true>;
-    if (coop == 4) return (const void *)k_contact_coop<4, kCoopMinBlocks, true>;
-    return dense ? (const void *)k_contact_mixed<kContactMixedMinBlocksDense> : (const void *)k_contact_mixed<1>;
+template <bool MESH>
+static const void *contact_mixed_kernel_t(int dense, int coop) {
+    if (coop == 8) return (const void *)k_contact_coop<8, kCoopMinBlocks, true, MESH>;
+    if (coop == 4) return (const void *)k_contact_coop<4, kCoopMinBlocks, true, MESH>;
+    return dense ? (const void *)k_contact_mixed<kContactMixedMinBlocksDense, MESH>
+                 : (const void *)k_contact_mixed<1, MESH>;
+}
+
+const void *contact_mixed_kernel(int dense, int coop, bool mesh) {
+    return mesh ? contact_mixed_kernel_t<true>(dense, coop) : contact_mixed_kernel_t<false>(dense, coop);
 }
 
 }  // namespace b200dem

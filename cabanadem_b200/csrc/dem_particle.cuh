@@ -118,20 +118,29 @@ __device__ __forceinline__ double vmax_collect_warp(unsigned long long *slots) {
     return __longlong_as_double((long long)v);
 }
 
-// Kinematic walls: x_w += dt u_w (the walls' stage2), by one full warp of the block that
-// finalises a step, after every particle of the step has used the current positions.
-__device__ __forceinline__ void advance_walls(WallGeom *walls, int nwall, double dt) {
-    if (!walls) return;
-    for (int w = threadIdx.x & 31; w < nwall; w += 32)
-        for (int d = 0; d < 3; ++d) walls[w].x[d] = dadd(walls[w].x[d], dmul(dt, walls[w].u[d]));
+// Kinematic walls and mesh: x_w += dt u_w and D += dt u (their stage2), by one full warp of the
+// block that finalises a step, after every particle of the step has used the current positions.
+__device__ __forceinline__ void advance_kinematics(const ForceConsts &fc) {
+    if (fc.mwalls)
+        for (int w = threadIdx.x & 31; w < fc.nwall; w += 32)
+            for (int d = 0; d < 3; ++d) fc.mwalls[w].x[d] = dadd(fc.mwalls[w].x[d], dmul(fc.dt, fc.mwalls[w].u[d]));
+    if (fc.mesh_moving && (threadIdx.x & 31) == 0)
+        for (int d = 0; d < 3; ++d) fc.mesh.D[d] = dadd(fc.mesh.D[d], dmul(fc.dt, fc.mesh.u[d]));
+}
+
+// |u|^2 of the moving mesh (0 otherwise): its motion enters the displacement bound, since the
+// mesh candidates of a particle are fixed between neighbour builds.
+__device__ __forceinline__ double mesh_speed2(const ForceConsts &fc) {
+    if (!fc.mesh_moving) return 0.0;
+    return dadd(dadd(dmul(fc.mesh.u[0], fc.mesh.u[0]), dmul(fc.mesh.u[1], fc.mesh.u[1])),
+                dmul(fc.mesh.u[2], fc.mesh.u[2]));
 }
 
 // Block max of |u|^2 folded into its slot, then the last block to finish advances the
 // control word: disp += dt*|u|max (conservative displacement bound), flips the position
 // buffer (and the velocity buffer when the kernel wrote the other one).
 __device__ __forceinline__ void finish_step(Ctl *ctl, unsigned long long *slots, double vmax2, double dt, int status,
-                                            bool count_step, bool flip_v = false, WallGeom *mwalls = nullptr,
-                                            int nwall = 0) {
+                                            bool count_step, bool flip_v = false, const ForceConsts *kin = nullptr) {
     __shared__ double red[32];
     __shared__ bool am_last;
     for (int o = 16; o > 0; o >>= 1) vmax2 = fmax(vmax2, __shfl_xor_sync(0xffffffffu, vmax2, o));
@@ -150,8 +159,11 @@ __device__ __forceinline__ void finish_step(Ctl *ctl, unsigned long long *slots,
     __syncthreads();
     if (am_last && threadIdx.x < 32) {
         __threadfence();
-        const double v2 = vmax_collect_warp(slots);
-        advance_walls(mwalls, nwall, dt);
+        double v2 = vmax_collect_warp(slots);
+        if (kin) {
+            advance_kinematics(*kin);
+            v2 = fmax(v2, mesh_speed2(*kin));
+        }
         if (threadIdx.x == 0) {
             ctl->disp = ctl->disp + dt * sqrt(v2) * (1.0 + 1e-9);
             ctl->ndefer = 0;
@@ -171,7 +183,7 @@ __device__ __forceinline__ void finish_step(Ctl *ctl, unsigned long long *slots,
 // per thread; one atomic per block, added before the block's ticket) and leaves the count in last_ndefer,
 // where the host reads the step's density.  Flips the position and velocity buffers.
 __device__ __forceinline__ void finish_step_counted(Ctl *ctl, unsigned long long *slots, double vmax2, double dt,
-                                                    int status, int active, WallGeom *mwalls, int nwall) {
+                                                    int status, int active, const ForceConsts &fc, bool advance) {
     __shared__ int cnt_s[32];
     __shared__ double red[32];
     __shared__ bool am_last;
@@ -201,8 +213,8 @@ __device__ __forceinline__ void finish_step_counted(Ctl *ctl, unsigned long long
     __syncthreads();
     if (am_last && threadIdx.x < 32) {
         __threadfence();
-        const double v2 = vmax_collect_warp(slots);
-        advance_walls(mwalls, nwall, dt);   // null on the last step of a run (no next drift)
+        const double v2 = fmax(vmax_collect_warp(slots), mesh_speed2(fc));
+        if (advance) advance_kinematics(fc);   // not on the last step of a run (no next drift)
         if (threadIdx.x == 0) {
             ctl->disp = ctl->disp + dt * sqrt(v2) * (1.0 + 1e-9);
             ctl->last_ndefer = atomicAdd(&ctl->ndefer, 0);
@@ -582,11 +594,214 @@ __device__ __forceinline__ void pw_wall(const unsigned q, const D4 &pi, const do
 }
 
 // ---------------------------------------------------------------------------------------
+// Triangle-mesh wall (no reference counterpart).  Closest point of triangle (a, b, c) to p:
+// the Voronoi-region method of Ericson, Real-Time Collision Detection (2005), sec. 5.1.5;
+// feature 0 face interior, 1 edge, 2 vertex.
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ void tri_closest(const double p[3], const double a[3], const double b[3], const double c[3],
+                                            double out[3], int &feature) {
+    double ab[3], ac[3], ap[3];
+    for (int d = 0; d < 3; ++d) {
+        ab[d] = b[d] - a[d];
+        ac[d] = c[d] - a[d];
+        ap[d] = p[d] - a[d];
+    }
+    const double d1 = ab[0] * ap[0] + ab[1] * ap[1] + ab[2] * ap[2];
+    const double d2 = ac[0] * ap[0] + ac[1] * ap[1] + ac[2] * ap[2];
+    if (d1 <= 0. && d2 <= 0.) {
+        for (int d = 0; d < 3; ++d) out[d] = a[d];
+        feature = 2;
+        return;
+    }
+    double bp[3];
+    for (int d = 0; d < 3; ++d) bp[d] = p[d] - b[d];
+    const double d3 = ab[0] * bp[0] + ab[1] * bp[1] + ab[2] * bp[2];
+    const double d4 = ac[0] * bp[0] + ac[1] * bp[1] + ac[2] * bp[2];
+    if (d3 >= 0. && d4 <= d3) {
+        for (int d = 0; d < 3; ++d) out[d] = b[d];
+        feature = 2;
+        return;
+    }
+    const double vc = d1 * d4 - d3 * d2;
+    if (vc <= 0. && d1 >= 0. && d3 <= 0.) {
+        const double v = d1 / (d1 - d3);
+        for (int d = 0; d < 3; ++d) out[d] = a[d] + v * ab[d];
+        feature = 1;
+        return;
+    }
+    double cp[3];
+    for (int d = 0; d < 3; ++d) cp[d] = p[d] - c[d];
+    const double d5 = ab[0] * cp[0] + ab[1] * cp[1] + ab[2] * cp[2];
+    const double d6 = ac[0] * cp[0] + ac[1] * cp[1] + ac[2] * cp[2];
+    if (d6 >= 0. && d5 <= d6) {
+        for (int d = 0; d < 3; ++d) out[d] = c[d];
+        feature = 2;
+        return;
+    }
+    const double vb = d5 * d2 - d1 * d6;
+    if (vb <= 0. && d2 >= 0. && d6 <= 0.) {
+        const double w = d2 / (d2 - d6);
+        for (int d = 0; d < 3; ++d) out[d] = a[d] + w * ac[d];
+        feature = 1;
+        return;
+    }
+    const double va = d3 * d6 - d5 * d4;
+    if (va <= 0. && (d4 - d3) >= 0. && (d5 - d6) >= 0.) {
+        const double w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+        for (int d = 0; d < 3; ++d) out[d] = b[d] + w * (c[d] - b[d]);
+        feature = 1;
+        return;
+    }
+    const double denom = 1. / (va + vb + vc);
+    const double v = vb * denom, w = vc * denom;
+    for (int d = 0; d < 3; ++d) out[d] = a[d] + ab[d] * v + ac[d] * w;
+    feature = 0;
+}
+
+__device__ __forceinline__ void mesh_vertices(const MeshDev &M, int t, const double D[3], double a[3], double b[3],
+                                              double c[3]) {
+    const double *v = M.tri + 9L * t;
+    for (int d = 0; d < 3; ++d) {
+        a[d] = v[d] + D[d];
+        b[d] = v[3 + d] + D[d];
+        c[d] = v[6 + d] + D[d];
+    }
+}
+
+// Contacts of particle i with the mesh, over its candidates in triangle order: contacts at
+// 0 < d < r (d = distance to the closest point); face contacts kept, an edge or vertex
+// contact dropped when its point coincides (1e-9 r) with a kept contact's or lies on a
+// triangle with a face contact; tracked slots: the still-live slots in their order, then the
+// new contacts with zero history; each kept contact acts as a plane through its point with
+// normal (x - c)/d (pw_wall), added in triangle order.  Returns the tracked count.  Not
+// inlined: particles away from the mesh never enter it.
+template <bool MIXED>
+__device__ __noinline__ int mesh_pass(const Particles &P, const ForceConsts &fc, const int i, const D4 pi,
+                                      const double ui0, const double ui1, const double ui2, const double wi0,
+                                      const double wi1, const double wi2, const double m_i, const int mi,
+                                      const double K_n_pw, const double K_t_pw, const double mu_pw, double *FT,
+                                      int *status) {
+    const MeshDev &M = fc.mesh;
+    const int cap = P.cap, mt = M.mt;
+    const int nc = M.ncand[i], cnt0 = M.cnt[i];
+    if (nc == 0 && cnt0 == 0) return 0;
+    const double r = pi.w;
+    const double x[3] = {pi.x, pi.y, pi.z};
+    const double D[3] = {M.D[0], M.D[1], M.D[2]};
+    int ht[kMeshCand], hf[kMeshCand];
+    double hc[kMeshCand][3], hd[kMeshCand], ho[kMeshCand];
+    bool keep[kMeshCand];
+    int nh = 0;
+    for (int k = 0; k < nc; ++k) {
+        const int t = M.cand[(long)k * cap + i];
+        double a[3], b[3], c[3], q[3];
+        int f;
+        mesh_vertices(M, t, D, a, b, c);
+        tri_closest(x, a, b, c, q, f);
+        const double dx = x[0] - q[0], dy = x[1] - q[1], dz = x[2] - q[2];
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        if (!(d2 < r * r) || !(d2 > 0.)) continue;
+        const double d = sqrt(d2);
+        const double overlap = r - d;
+        if (!(overlap > 0.)) continue;
+        ht[nh] = t;
+        hf[nh] = f;
+        hc[nh][0] = q[0];
+        hc[nh][1] = q[1];
+        hc[nh][2] = q[2];
+        hd[nh] = d;
+        ho[nh] = overlap;
+        ++nh;
+    }
+    const double eps = 1e-9 * r, eps2 = eps * eps;
+    for (int h = 0; h < nh; ++h) keep[h] = hf[h] == 0;
+    for (int h = 0; h < nh; ++h) {
+        if (hf[h] == 0) continue;
+        bool drop = false;
+        for (int k = 0; k < nh && !drop; ++k) {
+            if (k == h || !keep[k]) continue;
+            const double ex = hc[h][0] - hc[k][0], ey = hc[h][1] - hc[k][1], ez = hc[h][2] - hc[k][2];
+            if (ex * ex + ey * ey + ez * ez <= eps2) drop = true;
+            if (!drop && hf[k] == 0) {
+                double a[3], b[3], c[3], q[3];
+                int f;
+                mesh_vertices(M, ht[k], D, a, b, c);
+                tri_closest(hc[h], a, b, c, q, f);
+                const double fx = hc[h][0] - q[0], fy = hc[h][1] - q[1], fz = hc[h][2] - q[2];
+                if (fx * fx + fy * fy + fz * fz <= eps2) drop = true;
+            }
+        }
+        keep[h] = !drop;
+    }
+    // tracked slots: live slots in order, then new contacts in triangle order
+    int *tid = M.tid + i;
+    double *thx = M.th + i, *thy = M.th + (long)mt * cap + i, *thz = M.th + 2L * mt * cap + i;
+    int ntid[kMeshMaxContacts];
+    double n0[kMeshMaxContacts], n1[kMeshMaxContacts], n2[kMeshMaxContacts];
+    int cnt1 = 0;
+    for (int s2 = 0; s2 < cnt0; ++s2) {
+        const int t = tid[(long)s2 * cap];
+        bool live = false;
+        for (int h = 0; h < nh; ++h)
+            if (keep[h] && ht[h] == t) live = true;
+        if (live) {
+            ntid[cnt1] = t;
+            n0[cnt1] = thx[(long)s2 * cap];
+            n1[cnt1] = thy[(long)s2 * cap];
+            n2[cnt1] = thz[(long)s2 * cap];
+            ++cnt1;
+        }
+    }
+    const int kept_old = cnt1;
+    for (int h = 0; h < nh; ++h) {
+        if (!keep[h]) continue;
+        bool found = false;
+        for (int s2 = 0; s2 < cnt1; ++s2)
+            if (ntid[s2] == ht[h]) found = true;
+        if (found) continue;
+        if (cnt1 < mt) {
+            ntid[cnt1] = ht[h];
+            n0[cnt1] = n1[cnt1] = n2[cnt1] = 0.;
+            ++cnt1;
+        } else {
+            *status |= DEM_ERR_CONTACT_OVERFLOW;
+        }
+    }
+    for (int s2 = 0; s2 < mt; ++s2) {
+        const long a = (long)s2 * cap;
+        tid[a] = s2 < cnt1 ? ntid[s2] : -1;
+        thx[a] = s2 < cnt1 ? n0[s2] : 0.;
+        thy[a] = s2 < cnt1 ? n1[s2] : 0.;
+        thz[a] = s2 < cnt1 ? n2[s2] : 0.;
+    }
+    M.cnt[i] = (unsigned char)cnt1;
+    // forces, in triangle order
+    const PairConst c = M.pm[mi];
+    for (int h = 0; h < nh; ++h) {
+        if (!keep[h]) continue;
+        int slot = -1;
+        for (int s2 = 0; s2 < cnt1; ++s2)
+            if (ntid[s2] == ht[h]) slot = s2;
+        double dummy[3] = {0., 0., 0.};
+        double *sx = slot >= 0 ? thx + (long)slot * cap : dummy, *sy = slot >= 0 ? thy + (long)slot * cap : dummy + 1,
+               *sz = slot >= 0 ? thz + (long)slot * cap : dummy + 2;
+        const double d = hd[h];
+        const double nx = (x[0] - hc[h][0]) / d, ny = (x[1] - hc[h][1]) / d, nz = (x[2] - hc[h][2]) / d;
+        double cf[6];
+        pw_wall<MIXED>(fc.quirks, pi, nx, ny, nz, ho[h], ui0, ui1, ui2, wi0, wi1, wi2, M.u[0], M.u[1], M.u[2], m_i, c,
+                       K_n_pw, K_t_pw, mu_pw, fc.dt, slot >= 0 && slot < kept_old, sx, sy, sz, cf);
+        for (int k = 0; k < 6; ++k) FT[k] += cf[k];
+    }
+    return cnt1;
+}
+
+// ---------------------------------------------------------------------------------------
 // Full per-particle step (contact compaction, pp and wall forces, hooks, integration).
 // MODE_FORCE_ONLY writes F and tau in place and leaves x, u, omega untouched (the
 // unfused reference-order path); MODE_FUSED integrates into the next buffer.
 // ---------------------------------------------------------------------------------------
-template <int MODE, bool MIXED>
+// MESH: the solver has a triangle mesh (a separate build, so that meshless steps carry no call).
+template <int MODE, bool MIXED, bool MESH = false>
 __device__ __forceinline__ void particle_full(const Particles &P, const NbrList &L, const ForceConsts &fc,
                                               const PairConst *__restrict__ pp, const PairConst *__restrict__ pw,
                                               const WallGeom *__restrict__ walls, const int cur, const int nxt,
@@ -760,9 +975,21 @@ __device__ __forceinline__ void particle_full(const Particles &P, const NbrList 
             wmask &= ~bit;
         }
     }
+    int mcnt = 0;
+    if constexpr (MESH) {
+        double FT[6] = {F0, F1, F2, T0, T1, T2};
+        mcnt = mesh_pass<MIXED>(P, fc, i, pi, ui0, ui1, ui2, wi0, wi1, wi2, mIi.x, mi, K_n_pw, K_t_pw, mu_pw, FT,
+                                &status);
+        F0 = FT[0];
+        F1 = FT[1];
+        F2 = FT[2];
+        T0 = FT[3];
+        T1 = FT[4];
+        T2 = FT[5];
+    }
     const int cs1 = cnt | (int)(wmask << 8);
     if (cs1 != cs0) P.cstate[i] = cs1;
-    if (active) *active = (cs0 | cs1) != 0;
+    if (active) *active = (cs0 | cs1) != 0 || mcnt != 0;
     // ---- hooks after the pair forces
     if (fc.has_gravity) {
         F0 = dadd(F0, dmul(mIi.x, fc.g[0]));

@@ -21,6 +21,7 @@
 namespace b200dem {
 
 // Unfused force pass (MODE_FORCE_ONLY): F and tau written in place.
+template <bool MESH>
 __global__ void __launch_bounds__(kBlock) k_force(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
                                                   const PairConst *__restrict__ pp, const PairConst *__restrict__ pw,
                                                   const WallGeom *__restrict__ walls) {
@@ -30,7 +31,8 @@ __global__ void __launch_bounds__(kBlock) k_force(Particles P, NbrList L, Ctl *c
     double vmax2 = 0.0;
     int status = 0;
     if (i < P.n)
-        particle_full<MODE_FORCE_ONLY, false>(P, L, fc, pp, pw, walls, cur, cur ^ 1, vcur, 1, i, 0, vmax2, status);
+        particle_full<MODE_FORCE_ONLY, false, MESH>(P, L, fc, pp, pw, walls, cur, cur ^ 1, vcur, 1, i, 0, vmax2,
+                                                    status);
     if (status) atomicOr(&ctl->status, status);
 }
 
@@ -101,6 +103,8 @@ __global__ void __launch_bounds__(BS, MINB) k_stream(Particles P, NbrList L, Ctl
             const double sr = pi.w + pj.w;
             defer = !(r2ij >= sr * sr * 1.0000000001);
         }
+        // a particle near the mesh (candidates) or with a tracked triangle contact takes the full step
+        if (!defer && fc.mesh.nt) defer = (fc.mesh.ncand[i] | fc.mesh.cnt[i]) != 0;
         const int scene_i = P.scene ? P.scene[i] : 0;
         const int wall0 = fc.wps ? scene_i * fc.wps : 0;
         const int wall1 = fc.wps ? wall0 + fc.wps : fc.nwall;
@@ -164,7 +168,7 @@ __global__ void __launch_bounds__(BS, MINB) k_stream(Particles P, NbrList L, Ctl
 
 // Fused step, kernel 2 of 3: the full arithmetic for the deferred particles.  New u and
 // omega go to scratch slot t (their current values are still read by contact partners).
-template <int MINB>
+template <int MINB, bool MESH = false>
 __global__ void __launch_bounds__(kBlock, MINB) k_contact(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
                                                     const PairConst *__restrict__ pp, const PairConst *__restrict__ pw,
                                                     const WallGeom *__restrict__ walls) {
@@ -177,7 +181,7 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contact(Particles P, NbrList L
     int status = 0;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nd; t += gridDim.x * blockDim.x) {
         double v2 = 0.0;
-        particle_full<MODE_FUSED, false>(P, L, fc, pp, pw, walls, cur, cur ^ 1, vcur, last, L.defer[t], t, v2,
+        particle_full<MODE_FUSED, false, MESH>(P, L, fc, pp, pw, walls, cur, cur ^ 1, vcur, last, L.defer[t], t, v2,
                                          status);
         vmax2 = fmax(vmax2, v2);
     }
@@ -187,7 +191,7 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contact(Particles P, NbrList L
 // One-kernel step for dense flows (most particles in contact): every particle takes the
 // full arithmetic, positions and velocities go to the other buffers, and the last block
 // finalises the step.  Same results as the three-kernel step.
-template <int MINB>
+template <int MINB, bool MESH = false>
 __global__ void __launch_bounds__(kBlock, MINB) k_contact_all(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
                                                         const PairConst *__restrict__ pp,
                                                         const PairConst *__restrict__ pw,
@@ -200,12 +204,12 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contact_all(Particles P, NbrLi
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += gridDim.x * blockDim.x) {
         double v2 = 0.0;
         int a = 0;
-        particle_full<MODE_FUSED_DIRECT, false>(P, L, fc, pp, pw, walls, c.cur, c.cur ^ 1, vcur, c.last, i, i, v2,
+        particle_full<MODE_FUSED_DIRECT, false, MESH>(P, L, fc, pp, pw, walls, c.cur, c.cur ^ 1, vcur, c.last, i, i, v2,
                                                 status, &a);
         vmax2 = fmax(vmax2, v2);
         active += a;
     }
-    finish_step_counted(ctl, P.vslots, vmax2, fc.dt, status, active, c.last ? nullptr : fc.mwalls, fc.nwall);
+    finish_step_counted(ctl, P.vslots, vmax2, fc.dt, status, active, fc, !c.last);
 }
 
 // Fused step, kernel 3 of 3: commit the deferred particles' u and omega, then the last
@@ -237,9 +241,9 @@ __global__ void __launch_bounds__(kApplyBlock) k_apply(Particles P, NbrList L, C
     __syncthreads();
     if (s_last && threadIdx.x < 32) {   // every block has taken its ticket: the slots are quiescent
         __threadfence();
-        const double v2 = vmax_collect_warp(P.vslots);
-        // the walls drift with the particles' stage2 of the next step (none after a run's last step)
-        if (ctl->steps_done + 1 < ctl->target) advance_walls(fc.mwalls, fc.nwall, fc.dt);
+        const double v2 = fmax(vmax_collect_warp(P.vslots), mesh_speed2(fc));
+        // walls and mesh drift with the particles' stage2 of the next step (none after a run's last step)
+        if (ctl->steps_done + 1 < ctl->target) advance_kinematics(fc);
         if (threadIdx.x == 0) {
             ctl->disp = ctl->disp + fc.dt * sqrt(v2) * (1.0 + 1e-9);
             ctl->last_ndefer = nd;
@@ -278,13 +282,13 @@ __global__ void __launch_bounds__(kBlock) k_prologue(Particles P, Ctl *ctl, Forc
         vmax2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
         st4(P.pos[nxt], i, p);
     }
-    finish_step(ctl, P.vslots, vmax2, fc.dt, 0, false, false, fc.mwalls, fc.nwall);
+    finish_step(ctl, P.vslots, vmax2, fc.dt, 0, false, false, &fc);
 }
 
 // Unfused Integrator stages, in place on the current buffer.
 __global__ void k_stage(Particles P, Ctl *ctl, ForceConsts fc, int stage) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (stage == 2 && i < 32) advance_walls(fc.mwalls, fc.nwall, fc.dt);   // block 0's first warp
+    if (stage == 2 && i < 32) advance_kinematics(fc);   // block 0's first warp
     if (i >= P.n) return;
     const int cur = ctl->cur, vcur = ctl->vcur, cap = P.cap;
     double *vc = P.vel[vcur], *wc = P.omg[vcur];
@@ -367,8 +371,59 @@ __global__ void k_energy_final(const double *partials, int nparts, double *out) 
     }
 }
 
+// Mesh candidates of each particle at a neighbour build: every triangle whose closest point lies
+// within the list cutoff (delta, or r_i + skin), ascending id, by brute force over the mesh.
+// More than kMeshCand candidates: DEM_ERR_MESH_OVERFLOW (the extra triangles are not seen).
+__global__ void __launch_bounds__(kBlock) k_mesh_cand(Particles P, MeshDev M, Ctl *ctl, double delta, double skin) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n) return;
+    if (ctl->status & DEM_ERR_NAN) {
+        M.ncand[i] = 0;
+        return;
+    }
+    const D4 pi = ld4(P.pos[ctl->cur], i);
+    const double x[3] = {pi.x, pi.y, pi.z};
+    const double D[3] = {M.D[0], M.D[1], M.D[2]};
+    const double reach = delta > 0.0 ? delta : pi.w + skin;
+    int k = 0;
+    bool over = false;
+    for (int t = 0; t < M.nt; ++t) {
+        double a[3], b[3], c[3], q[3];
+        int f;
+        mesh_vertices(M, t, D, a, b, c);
+        tri_closest(x, a, b, c, q, f);
+        const double dx = x[0] - q[0], dy = x[1] - q[1], dz = x[2] - q[2];
+        if (dx * dx + dy * dy + dz * dz <= reach * reach) {
+            if (k < kMeshCand)
+                M.cand[(long)k++ * P.cap + i] = t;
+            else
+                over = true;
+        }
+    }
+    M.ncand[i] = (unsigned char)k;
+    if (over) atomicOr(&ctl->status, DEM_ERR_MESH_OVERFLOW);
+}
+
+// Re-sort: the tracked triangle contacts move with their particles (new p <- old items[p]).
+__global__ void k_permute_mesh(MeshDev M, MeshDev A, int n, int cap, const int *items) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const int q = items[p];
+        A.cnt[p] = M.cnt[q];
+        for (int s2 = 0; s2 < M.mt; ++s2) A.tid[(long)s2 * cap + p] = M.tid[(long)s2 * cap + q];
+        for (long k = 0; k < 3L * M.mt; ++k) A.th[k * cap + p] = M.th[k * cap + q];
+    }
+}
+
 // ---------------------------------------------------------------------------------------
 static inline int nblocks(int n) { return (n + kBlock - 1) / kBlock; }
+
+void launch_mesh_candidates(const Particles &P, const MeshDev &M, Ctl *ctl, double delta, double skin, cudaStream_t s) {
+    k_mesh_cand<<<nblocks(P.n), kBlock, 0, s>>>(P, M, ctl, delta, skin);
+}
+
+void launch_permute_mesh(const MeshDev &M, const MeshDev &A, int n, int cap, const int *items, cudaStream_t s) {
+    k_permute_mesh<<<148 * 4, 256, 0, s>>>(M, A, n, cap, items);
+}
 
 void launch_prologue(const Particles &P, Ctl *ctl, const ForceConsts &fc, cudaStream_t s) {
     k_prologue<<<nblocks(P.n), kBlock, 0, s>>>(P, ctl, fc);
@@ -391,34 +446,35 @@ static int persistent_blocks(const void *kernel, int block, int n) {
     return need < sms * per ? (need > 0 ? need : 1) : sms * per;
 }
 
-void launch_step(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
+template <bool MESH>
+static void launch_step_t(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
                  const PairConst *pw, const WallGeom *walls, int mode, cudaStream_t s) {
     if (mode == MODE_FUSED && fc.all) {
         static int ga = 0, gma = 0, last_na = -1;
         if (last_na != P.n) {
-            ga = persistent_blocks((const void *)k_contact_all<kContactMinBlocksDense>, kBlock, P.n);
-            gma = persistent_blocks(contact_mixed_all_kernel(), kBlock, P.n);
+            ga = persistent_blocks((const void *)k_contact_all<kContactMinBlocksDense, MESH>, kBlock, P.n);
+            gma = persistent_blocks(contact_mixed_all_kernel(MESH), kBlock, P.n);
             last_na = P.n;
         }
         if (fc.mixed)
-            launch_contact_mixed_all(P, L, ctl, fc, pp, pw, walls, gma, s);
+            launch_contact_mixed_all(P, L, ctl, fc, pp, pw, walls, gma, MESH, s);
         else
-            k_contact_all<kContactMinBlocksDense><<<ga, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+            k_contact_all<kContactMinBlocksDense, MESH><<<ga, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
     } else if (mode == MODE_FUSED) {
         static int gc = 0, gm = 0, gcd = 0, gmd = 0, gk4 = 0, gk8 = 0, gkm4 = 0, gkm8 = 0, last_n = -1;
         if (last_n != P.n) {
             // contact kernels: every block the SMs hold (a dense packing defers nearly every
             // particle; blocks past the deferred count exit at once); the apply kernel copies
             // 48 B per deferred particle and takes one ticket per block: one block per SM
-            gc = persistent_blocks((const void *)k_contact<1>, kBlock, P.n);
-            gm = persistent_blocks(contact_mixed_kernel(0, 0), kBlock, P.n);
-            gcd = persistent_blocks((const void *)k_contact<kContactMinBlocksDense>, kBlock, P.n);
-            gmd = persistent_blocks(contact_mixed_kernel(1, 0), kBlock, P.n);
+            gc = persistent_blocks((const void *)k_contact<1, MESH>, kBlock, P.n);
+            gm = persistent_blocks(contact_mixed_kernel(0, 0, MESH), kBlock, P.n);
+            gcd = persistent_blocks((const void *)k_contact<kContactMinBlocksDense, MESH>, kBlock, P.n);
+            gmd = persistent_blocks(contact_mixed_kernel(1, 0, MESH), kBlock, P.n);
             // cooperative kernels: a block serves kBlock / NL particles per pass
-            gk4 = persistent_blocks((const void *)k_contact_coop<4, kCoopMinBlocks, false>, kBlock, 4 * P.n);
-            gk8 = persistent_blocks((const void *)k_contact_coop<8, kCoopMinBlocks, false>, kBlock, 8 * P.n);
-            gkm4 = persistent_blocks(contact_mixed_kernel(0, 4), kBlock, 4 * P.n);
-            gkm8 = persistent_blocks(contact_mixed_kernel(0, 8), kBlock, 8 * P.n);
+            gk4 = persistent_blocks((const void *)k_contact_coop<4, kCoopMinBlocks, false, MESH>, kBlock, 4 * P.n);
+            gk8 = persistent_blocks((const void *)k_contact_coop<8, kCoopMinBlocks, false, MESH>, kBlock, 8 * P.n);
+            gkm4 = persistent_blocks(contact_mixed_kernel(0, 4, MESH), kBlock, 4 * P.n);
+            gkm8 = persistent_blocks(contact_mixed_kernel(0, 8, MESH), kBlock, 8 * P.n);
             last_n = P.n;
         }
         if (fc.stream_block == 64)
@@ -428,22 +484,30 @@ void launch_step(const Particles &P, const NbrList &L, Ctl *ctl, const ForceCons
         else
             k_stream<128, 10><<<(P.n + 127) / 128, 128, 0, s>>>(P, L, ctl, fc, walls);
         if (fc.mixed)
-            launch_contact_mixed(P, L, ctl, fc, pp, pw, walls,
+            launch_contact_mixed(P, L, ctl, fc, pp, pw, walls, MESH,
                                  fc.coop == 8 ? gkm8 : fc.coop == 4 ? gkm4 : fc.dense ? gmd : gm, s);
         else if (fc.coop == 8)
-            k_contact_coop<8, kCoopMinBlocks, false><<<gk8, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+            k_contact_coop<8, kCoopMinBlocks, false, MESH><<<gk8, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
         else if (fc.coop == 4)
-            k_contact_coop<4, kCoopMinBlocks, false><<<gk4, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+            k_contact_coop<4, kCoopMinBlocks, false, MESH><<<gk4, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
         else if (fc.dense)
-            k_contact<kContactMinBlocksDense><<<gcd, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+            k_contact<kContactMinBlocksDense, MESH><<<gcd, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
         else
-            k_contact<1><<<gc, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+            k_contact<1, MESH><<<gc, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
         k_apply<<<fc.dense ? 4 * 148 : 148, kApplyBlock, 0, s>>>(P, L, ctl, fc);
     } else if (fc.mixed) {
-        launch_force_mixed(P, L, ctl, fc, pp, pw, walls, s);
+        launch_force_mixed(P, L, ctl, fc, pp, pw, walls, MESH, s);
     } else {
-        k_force<<<nblocks(P.n), kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+        k_force<MESH><<<nblocks(P.n), kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
     }
+}
+
+void launch_step(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
+                 const PairConst *pw, const WallGeom *walls, int mode, cudaStream_t s) {
+    if (fc.mesh.nt)
+        launch_step_t<true>(P, L, ctl, fc, pp, pw, walls, mode, s);
+    else
+        launch_step_t<false>(P, L, ctl, fc, pp, pw, walls, mode, s);
 }
 
 void launch_stage(const Particles &P, Ctl *ctl, const ForceConsts &fc, int stage, cudaStream_t s) {

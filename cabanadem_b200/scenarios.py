@@ -459,6 +459,61 @@ def piston_box(n=4096, speed=2.0, seed=1, nsteps=400, quirks=REF_COMPAT & ~Q6_WA
     return sc
 
 
+def mesh_hopper(n=2048, radius=1e-3, seed=4, nsteps=2000, speed=0.0, quirks=REF_COMPAT, max_contacts=8,
+                drop_speed=2.0, band=0.01):
+    """Spheres falling into a V-shaped trough made of triangles (no reference counterpart):
+    two planes sloping at 35 degrees towards the line x = 0.025 m, y = 0, each made of 6
+    rectangular panels split along a diagonal, closed by two vertical end plates (plane walls
+    at z = 0 and z = 0.05).  The spheres start within `band` m above touching the trough,
+    moving down at drop_speed.  Glass, e = 0.8, mu = 0.3, gravity -y, dt 1e-7, skin 0.1 r.
+    speed > 0 drives the whole trough upwards (Q6 cleared)."""
+    from .state import MeshState
+    rng = np.random.default_rng(seed)
+    L, depth = 0.05, 0.05
+    tan = math.tan(math.radians(35.0))
+    s = ParticleState.create(n, max_cnts=16, max_walls=2)
+    pts, cell, grid, k, tries = np.zeros((n, 3)), 2.0 * radius, {}, 0, 0
+    while k < n:   # non-overlapping, above the trough
+        tries += 1
+        if tries > 200 * n:
+            raise ValueError("mesh_hopper: %d spheres do not fit in the release layer" % n)
+        p = rng.uniform((2 * radius, 0.0, 2 * radius), (L - 2 * radius, band, depth - 2 * radius))
+        p[1] += abs(p[0] - L / 2) * tan + 1.25 * radius / math.cos(math.radians(35.0))
+        c = tuple((p // cell).astype(int))
+        if all(np.sum((pts[q] - p) ** 2) >= (2.0 * radius) ** 2
+               for dx in (-1, 0, 1) for dy in (-1, 0, 1) for dz in (-1, 0, 1)
+               for q in grid.get((c[0] + dx, c[1] + dy, c[2] + dz), ())):
+            pts[k] = p
+            grid.setdefault(c, []).append(k)
+            k += 1
+    s.x[:] = pts
+    s.u[:, 1] = -float(drop_speed)
+    _apply_glass(s, radius)
+    tri = []
+    for side in (-1.0, 1.0):
+        xs = np.linspace(L / 2, L / 2 + side * (L / 2 + 4 * radius), 7)
+        zs = np.linspace(0.0, depth, 2)
+        for a in range(6):
+            for b in range(1):
+                p00 = (xs[a], abs(xs[a] - L / 2) * tan, zs[b])
+                p10 = (xs[a + 1], abs(xs[a + 1] - L / 2) * tan, zs[b])
+                p01 = (xs[a], abs(xs[a] - L / 2) * tan, zs[b + 1])
+                p11 = (xs[a + 1], abs(xs[a + 1] - L / 2) * tan, zs[b + 1])
+                tri += [(p00, p10, p11), (p00, p11, p01)]
+    mesh = MeshState.create(np.array(tri), n, GLASS["E"], GLASS["nu"], s.G[0], u=(0.0, speed, 0.0),
+                            max_contacts=max_contacts)
+    w = WallState.create(2)
+    w.x[1, 2] = depth
+    w.normal[0, 2], w.normal[1, 2] = 1.0, -1.0
+    w.E[:], w.nu[:], w.G[:] = GLASS["E"], GLASS["nu"], s.G[0]
+    if speed:
+        quirks = quirks & ~Q6_WALL_STATIC
+    sc = Scenario("mesh_hopper_%d" % n, s, w, _force_params(0.8, 0.8, 0.3, 0.3, quirks), 1e-7, nsteps,
+                  skin=0.1 * radius, gravity=(0.0, -9.81, 0.0))
+    sc.extra["mesh"] = mesh
+    return sc
+
+
 def hcp_box(n=2_000_000, rmin=0.8e-3, rmax=1.2e-3, seed=2, vmax=0.1, max_cnts=16, quirks=REF_COMPAT,
             dt=5e-8, nsteps=2000, jitter=0.05):
     """Polydisperse spheres (r ~ U[0.8, 1.2] mm) on a hexagonal-close-packed lattice of

@@ -111,6 +111,46 @@ class WallState:
         return w
 
 
+@dataclass
+class MeshState:
+    """A triangle-mesh wall: vertices [nt, 3, 3] at translation D, one material, translation
+    velocity u (the mesh moves only when the force's Q6 bit is clear), and the per-particle
+    tracked triangle contacts (triangle id, tangential history, count) for n particles."""
+    tri: np.ndarray = field(repr=False, default=None)
+    E: float = 0.0
+    nu: float = 0.0
+    G: float = 0.0
+    u: np.ndarray = field(repr=False, default=None)
+    D: np.ndarray = field(repr=False, default=None)
+    max_contacts: int = 8
+    tid: np.ndarray = field(repr=False, default=None)
+    th_x: np.ndarray = field(repr=False, default=None)
+    th_y: np.ndarray = field(repr=False, default=None)
+    th_z: np.ndarray = field(repr=False, default=None)
+    cnt: np.ndarray = field(repr=False, default=None)
+
+    @classmethod
+    def create(cls, tri, n: int, E: float, nu: float, G: float, u=(0.0, 0.0, 0.0), max_contacts: int = 8):
+        m = cls(tri=np.ascontiguousarray(tri, dtype=np.float64).reshape(-1, 3, 3), E=float(E), nu=float(nu),
+                G=float(G), u=np.array(u, dtype=np.float64), D=np.zeros(3), max_contacts=int(max_contacts))
+        m.tid = np.full((n, m.max_contacts), -1, dtype=np.int32)
+        for f in ("th_x", "th_y", "th_z"):
+            setattr(m, f, np.zeros((n, m.max_contacts)))
+        m.cnt = np.zeros(n, dtype=np.int32)
+        return m
+
+    @property
+    def nt(self) -> int:
+        return self.tri.shape[0]
+
+    def copy(self) -> "MeshState":
+        m = MeshState(tri=self.tri.copy(), E=self.E, nu=self.nu, G=self.G, u=self.u.copy(), D=self.D.copy(),
+                      max_contacts=self.max_contacts)
+        for f in ("tid", "th_x", "th_y", "th_z", "cnt"):
+            setattr(m, f, getattr(self, f).copy())
+        return m
+
+
 BOND_HIST = ("fn_x", "fn_y", "fn_z", "ft_x", "ft_y", "ft_z", "mn_x", "mn_y", "mn_z", "mt_x", "mt_y", "mt_z")
 
 

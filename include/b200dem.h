@@ -36,6 +36,7 @@ extern "C" {
 #define DEM_ERR_BOND_OVERFLOW     0x040 /* more than MaxBonds bonds                       */
 #define DEM_ERR_NOMEM             0x080 /* device allocation failed                       */
 #define DEM_ERR_UNSUPPORTED       0x100 /* option not supported                           */
+#define DEM_ERR_MESH_OVERFLOW     0x200 /* more than 32 mesh triangles near one particle  */
 
 /* ---- reference behaviours (bit set = reproduce the reference) ------------------ */
 #define DEM_Q1_VELJ_USES_UI  0x01u /* src/CabanaDEM_Force.hpp:133-137                    */
@@ -170,6 +171,22 @@ int dem_solver_stats(dem_solver *s, dem_run_stats *out);
  * DEM_Q6_WALL_STATIC is clear; no reference counterpart: the reference's walls never move,
  * src/CabanaDEM_Force.hpp:529). */
 int dem_solver_wall_positions(dem_solver *s, double *host, long count);
+/* Triangle-mesh wall (no reference counterpart: the reference has a Python intersection
+ * prototype only, examples/python/particle_single_trangle_intersection_test.py).
+ * tri [nt][3][3]: vertex coordinates (nt <= 4096, 0 removes the mesh); one material (E, nu,
+ * G) with the plane walls' force parameters (cor_pw, mu_pw); velocity [3] or NULL: the mesh
+ * translates by dt * velocity each step when DEM_Q6_WALL_STATIC is clear.  A contact acts as
+ * a plane through the triangle's closest point (normal from that point to the particle
+ * centre); an edge or vertex shared with a triangle already in contact, or lying on a
+ * triangle the particle touches by its face, makes no second contact.  Each particle tracks
+ * up to max_contacts (<= 16) triangle contacts (more: DEM_ERR_CONTACT_OVERFLOW, the extra
+ * contacts act without history); candidates are the triangles within the list cutoff at
+ * each neighbour build (more than 32: DEM_ERR_MESH_OVERFLOW).  Not with batched scenes or
+ * bonds.  The contacts are summed after the plane walls, in triangle order. */
+int dem_solver_set_mesh(dem_solver *s, const double *tri, int nt, double E, double nu, double G,
+                        const double *velocity, int max_contacts);
+/* The mesh's current translation [3] (zero for a static mesh). */
+int dem_solver_mesh_translation(dem_solver *s, double *host3);
 /* Same steps as dem_solver_run, but each fused step kernel is launched on its own between
  * two CUDA events; *kernel_ms receives the mean duration of one fused step launch
  * (rebuilds excluded).  For roofline measurement; no reference counterpart. */

@@ -21,6 +21,98 @@ namespace {
 inline double pow15(double x, int mode) { return mode == ORC_POW_SQRT ? x * std::sqrt(x) : std::pow(x, 1.5); }
 inline double pow05(double x, int mode) { return mode == ORC_POW_SQRT ? std::sqrt(x) : std::pow(x, 0.5); }
 
+// The contact law of src/CabanaDEM_Force.hpp:561-664 between particle i and a plane through
+// its contact point: unit normal (nij_x, nij_y, nij_z) towards the particle, overlap > 0, the
+// wall's material and velocity (vel_j; zero for the reference's static walls, :529), and the
+// contact's tangential history (swx, swy, swz), read and written.  Adds to F and tau of i.
+void plane_contact(orc_particles *p, int i, double nij_x, double nij_y, double nij_z, double overlap, double E_w,
+                   double nu_w, double G_w, const double vel_j[3], double *swx, double *swy, double *swz,
+                   const orc_force_params *fp, double dt) {
+    const unsigned q = fp->quirks;
+    const int pm = fp->pow_mode;
+    const double cor_pw = fp->cor_pw, friction_pw = fp->mu_pw;
+    const double *u = p->u, *omega = p->omega, *rad = p->rad, *m = p->m;
+    double a_i = rad[i] - overlap / 2.;
+    double vel_i[3];
+    vel_i[0] = u[3 * i + 0] + (omega[3 * i + 1] * nij_z - omega[3 * i + 2] * nij_y) * a_i;
+    vel_i[1] = u[3 * i + 1] + (omega[3 * i + 2] * nij_x - omega[3 * i + 0] * nij_z) * a_i;
+    vel_i[2] = u[3 * i + 2] + (omega[3 * i + 0] * nij_y - omega[3 * i + 1] * nij_x) * a_i;
+    double vel_ij[3] = {vel_i[0] - vel_j[0], vel_i[1] - vel_j[1], vel_i[2] - vel_j[2]};
+    double vij_dot_nij = vel_ij[0] * nij_x + vel_ij[1] * nij_y + vel_ij[2] * nij_z;
+    double vn_x = vij_dot_nij * nij_x;
+    double vn_y = vij_dot_nij * nij_y;
+    double vn_z = vij_dot_nij * nij_z;
+    double vt_x = vel_ij[0] - vn_x;
+    double vt_y = vel_ij[1] - vn_y;
+    double vt_z = vel_ij[2] - vn_z;
+    double tmp_1 = (1. - (p->nu[i] * p->nu[i])) / p->E[i];
+    double tmp_2 = (1. - (nu_w * nu_w)) / E_w;
+    double E_eff = 1. / (tmp_1 + tmp_2);
+    double tmp_3 = 1. / rad[i];
+    double tmp_4 = 0.;
+    double R_eff = 1. / (tmp_3 + tmp_4);
+    double kn = 4. / 3. * E_eff * std::sqrt(R_eff);
+    tmp_1 = std::log(cor_pw);
+    tmp_2 = tmp_1 * tmp_1 + M_PI * M_PI;
+    double beta = tmp_1 / std::sqrt(tmp_2);
+    double S_n = 2. * E_eff * std::sqrt(R_eff * overlap);
+    tmp_1 = 1. / m[i];
+    tmp_2 = 0.;
+    double m_eff = 1. / (tmp_1 + tmp_2);
+    double eta_n = -2. * std::sqrt(5. / 6.) * beta * std::sqrt(S_n * m_eff);
+    double fn = kn * pow15(overlap, pm);
+    double fn_x = fn * nij_x - eta_n * vn_x;
+    double fn_y = fn * nij_y - eta_n * vn_y;
+    double fn_z = fn * nij_z - eta_n * vn_z;
+    double ft_x = 0., ft_y = 0., ft_z = 0.;
+    double vij_magn = std::sqrt(vel_ij[0] * vel_ij[0] + vel_ij[1] * vel_ij[1] + vel_ij[2] * vel_ij[2]);
+    if (vij_magn < 1e-12) {
+        *swx = 0.;
+        *swy = 0.;
+        *swz = 0.;
+    } else {
+        *swx += vt_x * dt;
+        *swy += vt_y * dt;
+        *swz += vt_z * dt;
+        tmp_1 = (2. - p->nu[i]) / p->G[i];
+        tmp_2 = (2. - nu_w) / G_w;
+        double G_eff = 1. / (tmp_1 + tmp_2);
+        double kt = 8. * G_eff * std::sqrt(R_eff * overlap);
+        double S_t = kt;
+        double eta_t = (q & ORC_Q2_ETA_T_ZERO) ? -2 * std::sqrt((double)(5 / 6)) * beta * std::sqrt(S_t * m_eff)
+                                               : -2. * std::sqrt(5. / 6.) * beta * std::sqrt(S_t * m_eff);
+        double ft_x_star = -kt * *swx - eta_t * vt_x;
+        double ft_y_star = -kt * *swy - eta_t * vt_y;
+        double ft_z_star = -kt * *swz - eta_t * vt_z;
+        double ft_magn = (q & ORC_Q5_WALL_FT_TYPO)
+                             ? std::sqrt(ft_x_star * ft_x_star + ft_y_star * ft_y_star + ft_z_star * ft_y_star)
+                             : std::sqrt(ft_x_star * ft_x_star + ft_y_star * ft_y_star + ft_z_star * ft_z_star);
+        double ti_x = 0., ti_y = 0., ti_z = 0.;
+        if (ft_magn > 1e-12) {
+            ti_x = ft_x_star / ft_magn;
+            ti_y = ft_y_star / ft_magn;
+            ti_z = ft_z_star / ft_magn;
+        }
+        double fn_magn = std::sqrt(fn_x * fn_x + fn_y * fn_y + fn_z * fn_z);
+        double ft_magn_star = std::min(friction_pw * fn_magn, ft_magn);
+        ft_x = ft_magn_star * ti_x;
+        ft_y = ft_magn_star * ti_y;
+        ft_z = ft_magn_star * ti_z;
+        ft_x += eta_t * vt_x;
+        ft_y += eta_t * vt_y;
+        ft_z += eta_t * vt_z;
+        *swx = -ft_x / kt;
+        *swy = -ft_y / kt;
+        *swz = -ft_z / kt;
+    }
+    p->force[3 * i + 0] += fn_x + ft_x;
+    p->force[3 * i + 1] += fn_y + ft_y;
+    p->force[3 * i + 2] += fn_z + ft_z;
+    p->torque[3 * i + 0] += (nij_y * ft_z - nij_z * ft_y) * a_i;
+    p->torque[3 * i + 1] += (nij_z * ft_x - nij_x * ft_z) * a_i;
+    p->torque[3 * i + 2] += (nij_x * ft_y - nij_y * ft_x) * a_i;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------------
@@ -394,11 +486,9 @@ extern "C" int orc_force_pp(orc_particles *p, const orc_nlist *nl, const orc_for
 extern "C" void orc_force_wall(orc_particles *p, const orc_walls *w, const orc_force_params *fp, double dt) {
     const int mw = p->max_walls;
     const unsigned q = fp->quirks;
-    const int pm = fp->pow_mode;
-    const double cor_pw = fp->cor_pw, friction_pw = fp->mu_pw;
 #pragma omp parallel for schedule(static)
     for (int i = 0; i < p->n; ++i) {
-        const double *x = p->x, *u = p->u, *omega = p->omega, *rad = p->rad, *m = p->m;
+        const double *x = p->x, *rad = p->rad;
         for (int j = 0; j < w->n; ++j) {
             double *swx = p->tng_sw_x + (long)i * mw + j, *swy = p->tng_sw_y + (long)i * mw + j,
                    *swz = p->tng_sw_z + (long)i * mw + j;
@@ -409,89 +499,12 @@ extern "C" void orc_force_wall(orc_particles *p, const orc_walls *w, const orc_f
             double nij_z = w->normal[3 * j + 2];
             double tmp = pos_ij[0] * nij_x + pos_ij[1] * nij_y + pos_ij[2] * nij_z;
             double overlap = rad[i] - tmp;
-            double a_i = rad[i] - overlap / 2.;
-            double vel_i[3];
-            vel_i[0] = u[3 * i + 0] + (omega[3 * i + 1] * nij_z - omega[3 * i + 2] * nij_y) * a_i;
-            vel_i[1] = u[3 * i + 1] + (omega[3 * i + 2] * nij_x - omega[3 * i + 0] * nij_z) * a_i;
-            vel_i[2] = u[3 * i + 2] + (omega[3 * i + 0] * nij_y - omega[3 * i + 1] * nij_x) * a_i;
-            double vel_j[3] = {0., 0., 0.};
-            if (!(q & ORC_Q6_WALL_STATIC) && w->u)
-                for (int d = 0; d < 3; ++d) vel_j[d] = w->u[3 * j + d];
-            double vel_ij[3] = {vel_i[0] - vel_j[0], vel_i[1] - vel_j[1], vel_i[2] - vel_j[2]};
-            double vij_dot_nij = vel_ij[0] * nij_x + vel_ij[1] * nij_y + vel_ij[2] * nij_z;
-            double vn_x = vij_dot_nij * nij_x;
-            double vn_y = vij_dot_nij * nij_y;
-            double vn_z = vij_dot_nij * nij_z;
-            double vt_x = vel_ij[0] - vn_x;
-            double vt_y = vel_ij[1] - vn_y;
-            double vt_z = vel_ij[2] - vn_z;
             if (overlap > 0.) {
-                double tmp_1 = (1. - (p->nu[i] * p->nu[i])) / p->E[i];
-                double tmp_2 = (1. - (w->nu[j] * w->nu[j])) / w->E[j];
-                double E_eff = 1. / (tmp_1 + tmp_2);
-                double tmp_3 = 1. / rad[i];
-                double tmp_4 = 0.;
-                double R_eff = 1. / (tmp_3 + tmp_4);
-                double kn = 4. / 3. * E_eff * std::sqrt(R_eff);
-                tmp_1 = std::log(cor_pw);
-                tmp_2 = tmp_1 * tmp_1 + M_PI * M_PI;
-                double beta = tmp_1 / std::sqrt(tmp_2);
-                double S_n = 2. * E_eff * std::sqrt(R_eff * overlap);
-                tmp_1 = 1. / m[i];
-                tmp_2 = 0.;
-                double m_eff = 1. / (tmp_1 + tmp_2);
-                double eta_n = -2. * std::sqrt(5. / 6.) * beta * std::sqrt(S_n * m_eff);
-                double fn = kn * pow15(overlap, pm);
-                double fn_x = fn * nij_x - eta_n * vn_x;
-                double fn_y = fn * nij_y - eta_n * vn_y;
-                double fn_z = fn * nij_z - eta_n * vn_z;
-                double ft_x = 0., ft_y = 0., ft_z = 0.;
-                double vij_magn = std::sqrt(vel_ij[0] * vel_ij[0] + vel_ij[1] * vel_ij[1] + vel_ij[2] * vel_ij[2]);
-                if (vij_magn < 1e-12) {
-                    *swx = 0.;
-                    *swy = 0.;
-                    *swz = 0.;
-                } else {
-                    *swx += vt_x * dt;
-                    *swy += vt_y * dt;
-                    *swz += vt_z * dt;
-                    tmp_1 = (2. - p->nu[i]) / p->G[i];
-                    tmp_2 = (2. - w->nu[j]) / w->G[j];
-                    double G_eff = 1. / (tmp_1 + tmp_2);
-                    double kt = 8. * G_eff * std::sqrt(R_eff * overlap);
-                    double S_t = kt;
-                    double eta_t = (q & ORC_Q2_ETA_T_ZERO) ? -2 * std::sqrt((double)(5 / 6)) * beta * std::sqrt(S_t * m_eff)
-                                                           : -2. * std::sqrt(5. / 6.) * beta * std::sqrt(S_t * m_eff);
-                    double ft_x_star = -kt * *swx - eta_t * vt_x;
-                    double ft_y_star = -kt * *swy - eta_t * vt_y;
-                    double ft_z_star = -kt * *swz - eta_t * vt_z;
-                    double ft_magn = (q & ORC_Q5_WALL_FT_TYPO)
-                                         ? std::sqrt(ft_x_star * ft_x_star + ft_y_star * ft_y_star + ft_z_star * ft_y_star)
-                                         : std::sqrt(ft_x_star * ft_x_star + ft_y_star * ft_y_star + ft_z_star * ft_z_star);
-                    double ti_x = 0., ti_y = 0., ti_z = 0.;
-                    if (ft_magn > 1e-12) {
-                        ti_x = ft_x_star / ft_magn;
-                        ti_y = ft_y_star / ft_magn;
-                        ti_z = ft_z_star / ft_magn;
-                    }
-                    double fn_magn = std::sqrt(fn_x * fn_x + fn_y * fn_y + fn_z * fn_z);
-                    double ft_magn_star = std::min(friction_pw * fn_magn, ft_magn);
-                    ft_x = ft_magn_star * ti_x;
-                    ft_y = ft_magn_star * ti_y;
-                    ft_z = ft_magn_star * ti_z;
-                    ft_x += eta_t * vt_x;
-                    ft_y += eta_t * vt_y;
-                    ft_z += eta_t * vt_z;
-                    *swx = -ft_x / kt;
-                    *swy = -ft_y / kt;
-                    *swz = -ft_z / kt;
-                }
-                p->force[3 * i + 0] += fn_x + ft_x;
-                p->force[3 * i + 1] += fn_y + ft_y;
-                p->force[3 * i + 2] += fn_z + ft_z;
-                p->torque[3 * i + 0] += (nij_y * ft_z - nij_z * ft_y) * a_i;
-                p->torque[3 * i + 1] += (nij_z * ft_x - nij_x * ft_z) * a_i;
-                p->torque[3 * i + 2] += (nij_x * ft_y - nij_y * ft_x) * a_i;
+                double vel_j[3] = {0., 0., 0.};
+                if (!(q & ORC_Q6_WALL_STATIC) && w->u)
+                    for (int d = 0; d < 3; ++d) vel_j[d] = w->u[3 * j + d];
+                plane_contact(p, i, nij_x, nij_y, nij_z, overlap, w->E[j], w->nu[j], w->G[j], vel_j, swx, swy, swz, fp,
+                              dt);
             } else {
                 *swx = 0.;
                 *swy = 0.;
@@ -499,6 +512,200 @@ extern "C" void orc_force_wall(orc_particles *p, const orc_walls *w, const orc_f
             }
         }
     }
+}
+
+// ---------------------------------------------------------------------------------
+// Triangle-mesh wall (no reference counterpart).  Closest point of a triangle to a point:
+// the Voronoi-region method of Ericson, Real-Time Collision Detection (2005), sec. 5.1.5.
+// feature: 0 face interior, 1 edge, 2 vertex.
+// ---------------------------------------------------------------------------------
+static void tri_closest(const double p[3], const double a[3], const double b[3], const double c[3], double out[3],
+                        int *feature) {
+    double ab[3], ac[3], ap[3];
+    for (int d = 0; d < 3; ++d) {
+        ab[d] = b[d] - a[d];
+        ac[d] = c[d] - a[d];
+        ap[d] = p[d] - a[d];
+    }
+    const double d1 = ab[0] * ap[0] + ab[1] * ap[1] + ab[2] * ap[2];
+    const double d2 = ac[0] * ap[0] + ac[1] * ap[1] + ac[2] * ap[2];
+    if (d1 <= 0. && d2 <= 0.) {
+        for (int d = 0; d < 3; ++d) out[d] = a[d];
+        *feature = 2;
+        return;
+    }
+    double bp[3];
+    for (int d = 0; d < 3; ++d) bp[d] = p[d] - b[d];
+    const double d3 = ab[0] * bp[0] + ab[1] * bp[1] + ab[2] * bp[2];
+    const double d4 = ac[0] * bp[0] + ac[1] * bp[1] + ac[2] * bp[2];
+    if (d3 >= 0. && d4 <= d3) {
+        for (int d = 0; d < 3; ++d) out[d] = b[d];
+        *feature = 2;
+        return;
+    }
+    const double vc = d1 * d4 - d3 * d2;
+    if (vc <= 0. && d1 >= 0. && d3 <= 0.) {
+        const double v = d1 / (d1 - d3);
+        for (int d = 0; d < 3; ++d) out[d] = a[d] + v * ab[d];
+        *feature = 1;
+        return;
+    }
+    double cp[3];
+    for (int d = 0; d < 3; ++d) cp[d] = p[d] - c[d];
+    const double d5 = ab[0] * cp[0] + ab[1] * cp[1] + ab[2] * cp[2];
+    const double d6 = ac[0] * cp[0] + ac[1] * cp[1] + ac[2] * cp[2];
+    if (d6 >= 0. && d5 <= d6) {
+        for (int d = 0; d < 3; ++d) out[d] = c[d];
+        *feature = 2;
+        return;
+    }
+    const double vb = d5 * d2 - d1 * d6;
+    if (vb <= 0. && d2 >= 0. && d6 <= 0.) {
+        const double w = d2 / (d2 - d6);
+        for (int d = 0; d < 3; ++d) out[d] = a[d] + w * ac[d];
+        *feature = 1;
+        return;
+    }
+    const double va = d3 * d6 - d5 * d4;
+    if (va <= 0. && (d4 - d3) >= 0. && (d5 - d6) >= 0.) {
+        const double w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+        for (int d = 0; d < 3; ++d) out[d] = b[d] + w * (c[d] - b[d]);
+        *feature = 1;
+        return;
+    }
+    const double denom = 1. / (va + vb + vc);
+    const double v = vb * denom, w = vc * denom;
+    for (int d = 0; d < 3; ++d) out[d] = a[d] + ab[d] * v + ac[d] * w;
+    *feature = 0;
+}
+
+static void mesh_vertices(const orc_mesh *m, int t, double a[3], double b[3], double c[3]) {
+    for (int d = 0; d < 3; ++d) {
+        a[d] = m->tri[9 * t + d] + m->D[d];
+        b[d] = m->tri[9 * t + 3 + d] + m->D[d];
+        c[d] = m->tri[9 * t + 6 + d] + m->D[d];
+    }
+}
+
+// Contacts of particle i with the mesh, in triangle order:
+//  1. every triangle whose closest point lies closer than r_i (0 < d) is a candidate contact;
+//  2. face contacts are kept; an edge or vertex contact is dropped when its point lies on a
+//     kept contact's point (a shared edge or vertex seen from two triangles) or on a triangle
+//     that has a face contact (the particle rests on that face; the edge belongs to it);
+//     tolerance 1e-9 r_i;
+//  3. tracked slots: the slots whose triangle is still in contact keep their order and
+//     history, then the new contacts in triangle order with zero history; slots past
+//     max_contacts are not tracked (overflow status);
+//  4. each kept contact acts as a plane through its point, normal (x - c)/d, overlap r - d,
+//     the mesh's material and velocity (plane_contact), added in triangle order.
+extern "C" int orc_force_mesh(orc_particles *p, orc_mesh *m, const orc_force_params *fp, double dt) {
+    if (!m || m->nt <= 0) return 0;
+    const int mc = m->max_contacts;
+    const bool moving = !(fp->quirks & ORC_Q6_WALL_STATIC);
+    int status = 0;
+#pragma omp parallel for schedule(static) reduction(| : status)
+    for (int i = 0; i < p->n; ++i) {
+        const double r = p->rad[i];
+        const double x[3] = {p->x[3 * i], p->x[3 * i + 1], p->x[3 * i + 2]};
+        struct Hit {
+            int t, feature;
+            double c[3], d, overlap;
+        };
+        std::vector<Hit> hits;
+        for (int t = 0; t < m->nt; ++t) {
+            double a[3], b[3], c[3], q[3];
+            int f;
+            mesh_vertices(m, t, a, b, c);
+            tri_closest(x, a, b, c, q, &f);
+            const double dx = x[0] - q[0], dy = x[1] - q[1], dz = x[2] - q[2];
+            const double d2 = dx * dx + dy * dy + dz * dz;
+            if (!(d2 < r * r) || !(d2 > 0.)) continue;
+            const double d = std::sqrt(d2);
+            const double overlap = r - d;
+            if (!(overlap > 0.)) continue;
+            hits.push_back({t, f, {q[0], q[1], q[2]}, d, overlap});
+        }
+        const double eps = 1e-9 * r, eps2 = eps * eps;
+        std::vector<char> keep(hits.size(), 0);
+        for (size_t h = 0; h < hits.size(); ++h) keep[h] = hits[h].feature == 0;
+        for (size_t h = 0; h < hits.size(); ++h) {
+            if (hits[h].feature == 0) continue;
+            bool drop = false;
+            for (size_t k = 0; k < hits.size() && !drop; ++k) {
+                if (k == h || !keep[k]) continue;
+                const double ex = hits[h].c[0] - hits[k].c[0], ey = hits[h].c[1] - hits[k].c[1],
+                             ez = hits[h].c[2] - hits[k].c[2];
+                if (ex * ex + ey * ey + ez * ez <= eps2) drop = true;
+                if (!drop && hits[k].feature == 0) {
+                    double a[3], b[3], c[3], q[3];
+                    int f;
+                    mesh_vertices(m, hits[k].t, a, b, c);
+                    tri_closest(hits[h].c, a, b, c, q, &f);
+                    const double fx = hits[h].c[0] - q[0], fy = hits[h].c[1] - q[1], fz = hits[h].c[2] - q[2];
+                    if (fx * fx + fy * fy + fz * fz <= eps2) drop = true;
+                }
+            }
+            keep[h] = !drop;
+        }
+        // tracked slots
+        int *tid = m->tid + (long)i * mc;
+        double *thx = m->th_x + (long)i * mc, *thy = m->th_y + (long)i * mc, *thz = m->th_z + (long)i * mc;
+        const int cnt0 = m->cnt[i];
+        std::vector<int> ntid;
+        std::vector<double> nhx, nhy, nhz;
+        std::vector<char> had;
+        for (int s2 = 0; s2 < cnt0; ++s2) {
+            bool live = false;
+            for (size_t h = 0; h < hits.size(); ++h)
+                if (keep[h] && hits[h].t == tid[s2]) live = true;
+            if (live) {
+                ntid.push_back(tid[s2]);
+                nhx.push_back(thx[s2]);
+                nhy.push_back(thy[s2]);
+                nhz.push_back(thz[s2]);
+                had.push_back(1);
+            }
+        }
+        for (size_t h = 0; h < hits.size(); ++h) {
+            if (!keep[h]) continue;
+            bool found = false;
+            for (size_t s2 = 0; s2 < ntid.size(); ++s2)
+                if (ntid[s2] == hits[h].t) found = true;
+            if (found) continue;
+            if ((int)ntid.size() < mc) {
+                ntid.push_back(hits[h].t);
+                nhx.push_back(0.);
+                nhy.push_back(0.);
+                nhz.push_back(0.);
+                had.push_back(0);
+            } else {
+                status |= ORC_ERR_CONTACT_OVERFLOW;
+            }
+        }
+        const int cnt1 = (int)ntid.size();
+        for (int s2 = 0; s2 < mc; ++s2) {
+            tid[s2] = s2 < cnt1 ? ntid[s2] : -1;
+            thx[s2] = s2 < cnt1 ? nhx[s2] : 0.;
+            thy[s2] = s2 < cnt1 ? nhy[s2] : 0.;
+            thz[s2] = s2 < cnt1 ? nhz[s2] : 0.;
+        }
+        m->cnt[i] = cnt1;
+        // forces, in triangle order
+        const double vel_j[3] = {moving ? m->u[0] : 0., moving ? m->u[1] : 0., moving ? m->u[2] : 0.};
+        for (size_t h = 0; h < hits.size(); ++h) {
+            if (!keep[h]) continue;
+            int slot = -1;
+            for (int s2 = 0; s2 < cnt1; ++s2)
+                if (tid[s2] == hits[h].t) slot = s2;
+            double dummy[3] = {0., 0., 0.};
+            double *sx = slot >= 0 ? thx + slot : dummy, *sy = slot >= 0 ? thy + slot : dummy + 1,
+                   *sz = slot >= 0 ? thz + slot : dummy + 2;
+            const double d = hits[h].d;
+            const double nx = (x[0] - hits[h].c[0]) / d, ny = (x[1] - hits[h].c[1]) / d, nz = (x[2] - hits[h].c[2]) / d;
+            plane_contact(p, i, nx, ny, nz, hits[h].overlap, m->E, m->nu, m->G, vel_j, sx, sy, sz, fp, dt);
+        }
+    }
+    return status;
 }
 
 // Hook before the interaction forces: external force (tst_01_BDEM:70-117 adds it
@@ -532,12 +739,15 @@ extern "C" int orc_step(orc_particles *p, const orc_walls *w, const orc_force_pa
     orc_stage1(p, dt);
     orc_stage2(p, dt);
     if (w && w->n > 0 && !(fp->quirks & ORC_Q6_WALL_STATIC)) orc_stage2_walls(w, dt);
+    if (h && h->mesh && !(fp->quirks & ORC_Q6_WALL_STATIC))
+        for (int d = 0; d < 3; ++d) h->mesh->D[d] += dt * h->mesh->u[d];
     orc_nlist_build(nl, p, delta, skin);
     orc_zero_force(p);
     orc_apply_ext_force(p, h);
     orc_update_tangential_contacts(p);
     int st = orc_force_pp(p, nl, fp, dt);
     if (w && w->n > 0) orc_force_wall(p, w, fp, dt);
+    if (h && h->mesh) st |= orc_force_mesh(p, h->mesh, fp, dt);
     orc_apply_post_hooks(p, h);
     orc_stage3(p, dt);
     return st;

@@ -75,6 +75,21 @@ typedef struct orc_force_params {
     int pow_mode;
 } orc_force_params;
 
+/* Triangle-mesh wall (no reference counterpart; the reference has a Python intersection
+ * prototype only).  Vertices [nt][3][3] at translation D (advanced by dt * u in stage2 when
+ * ORC_Q6_WALL_STATIC is clear).  Per particle: up to max_contacts tracked triangle contacts. */
+typedef struct orc_mesh {
+    int nt;
+    const double *tri;               /* [nt*9]: a, b, c                                  */
+    double E, nu, G;
+    double u[3];                     /* translation velocity                             */
+    double D[3];                     /* accumulated translation (advanced in place)      */
+    int max_contacts;
+    int *tid;                        /* [n*max_contacts] triangle of each tracked slot   */
+    double *th_x, *th_y, *th_z;      /* [n*max_contacts] tangential history              */
+    int *cnt;                        /* [n] tracked triangle contacts                    */
+} orc_mesh;
+
 /* Hooks applied in the position of tst_01_BDEM's applyTensileForce /
  * applyBoundaryConditions: ext_force (may be NULL) is added before the interaction
  * forces, gravity * m after them, then fix flags zero F and/or tau. */
@@ -82,6 +97,7 @@ typedef struct orc_hooks {
     double gravity[3];
     const double *ext_force;          /* [n*3] or NULL */
     const unsigned char *fix_flags;   /* [n] or NULL   */
+    orc_mesh *mesh;                   /* triangle-mesh wall or NULL (after the plane walls) */
 } orc_hooks;
 
 typedef struct orc_nlist orc_nlist;
@@ -104,6 +120,9 @@ void orc_update_tangential_contacts(orc_particles *p);
 int  orc_force_pp(orc_particles *p, const orc_nlist *nl, const orc_force_params *fp, double dt);
 void orc_force_wall(orc_particles *p, const orc_walls *w, const orc_force_params *fp, double dt);
 void orc_apply_ext_force(orc_particles *p, const orc_hooks *h);
+/* Contacts with the mesh, after the plane walls; returns ORC_ERR_CONTACT_OVERFLOW when a
+ * particle has more than max_contacts triangle contacts (the rest are not tracked). */
+int  orc_force_mesh(orc_particles *p, orc_mesh *m, const orc_force_params *fp, double dt);
 void orc_apply_post_hooks(orc_particles *p, const orc_hooks *h);
 
 /* One reference time step (Solver.hpp:81-94) with the neighbour list rebuilt from the

@@ -50,8 +50,14 @@ class _ForceParams(C.Structure):
                 ("quirks", C.c_uint), ("pow_mode", C.c_int)]
 
 
+class _Mesh(C.Structure):
+    _fields_ = [("nt", C.c_int), ("tri", _dp), ("E", C.c_double), ("nu", C.c_double), ("G", C.c_double),
+                ("u", C.c_double * 3), ("D", C.c_double * 3), ("max_contacts", C.c_int), ("tid", _ip),
+                ("th_x", _dp), ("th_y", _dp), ("th_z", _dp), ("cnt", _ip)]
+
+
 class _Hooks(C.Structure):
-    _fields_ = [("gravity", C.c_double * 3), ("ext_force", _dp), ("fix_flags", _up)]
+    _fields_ = [("gravity", C.c_double * 3), ("ext_force", _dp), ("fix_flags", _up), ("mesh", C.POINTER(_Mesh))]
 
 
 class _Bonds(C.Structure):
@@ -140,22 +146,45 @@ def _fp(params, pow_mode):
 
 
 class _HookHolder:
-    def __init__(self, gravity=(0.0, 0.0, 0.0), ext_force=None, fix_flags=None):
+    def __init__(self, gravity=(0.0, 0.0, 0.0), ext_force=None, fix_flags=None, mesh=None):
         self.h = _Hooks()
         self.h.gravity = (C.c_double * 3)(*gravity)
         self._ext = None if ext_force is None else np.ascontiguousarray(ext_force, dtype=np.float64)
         self._fix = None if fix_flags is None else np.ascontiguousarray(fix_flags, dtype=np.uint8)
         self.h.ext_force = _ptr(self._ext, _dp) if self._ext is not None else None
         self.h.fix_flags = _ptr(self._fix, _up) if self._fix is not None else None
+        self.mesh = mesh
+        if mesh is not None:
+            self._m = _Mesh()
+            self._tri = np.ascontiguousarray(mesh.tri, dtype=np.float64)
+            self._m.nt = mesh.nt
+            self._m.tri = _ptr(self._tri, _dp)
+            self._m.E, self._m.nu, self._m.G = mesh.E, mesh.nu, mesh.G
+            self._m.u = (C.c_double * 3)(*mesh.u)
+            self._m.D = (C.c_double * 3)(*mesh.D)
+            self._m.max_contacts = mesh.max_contacts
+            self._m.tid = _ptr(mesh.tid, _ip)
+            self._m.th_x, self._m.th_y, self._m.th_z = _ptr(mesh.th_x, _dp), _ptr(mesh.th_y, _dp), _ptr(mesh.th_z, _dp)
+            self._m.cnt = _ptr(mesh.cnt, _ip)
+            self.h.mesh = C.pointer(self._m)
+
+    def done(self):
+        """Copy the mesh translation back into the MeshState (the arrays are shared)."""
+        if self.mesh is not None:
+            self.mesh.D[:] = list(self._m.D)
 
 
 def run(state, walls, params, dt, nsteps, delta=0.0, skin=0.0, gravity=(0.0, 0.0, 0.0), ext_force=None,
-        fix_flags=None, pow_mode=POW_LIBM):
+        fix_flags=None, pow_mode=POW_LIBM, mesh=None):
     """Advance `state` in place by nsteps reference steps (Solver.hpp:81-94).
-    Neighbour cutoff is `delta` when > 0, else rad_i + rad_j + skin; rebuilt every step."""
+    Neighbour cutoff is `delta` when > 0, else rad_i + rad_j + skin; rebuilt every step.
+    `mesh` (a MeshState) adds a triangle-mesh wall after the plane walls; its contact
+    history and translation are updated in place."""
     p, w, fp = _particles(state), _walls(walls), _fp(params, pow_mode)
-    h = _HookHolder(gravity, ext_force, fix_flags)
-    return lib().orc_run(C.byref(p), C.byref(w), C.byref(fp), C.byref(h.h), dt, int(nsteps), float(delta), float(skin))
+    h = _HookHolder(gravity, ext_force, fix_flags, mesh)
+    st = lib().orc_run(C.byref(p), C.byref(w), C.byref(fp), C.byref(h.h), dt, int(nsteps), float(delta), float(skin))
+    h.done()
+    return st
 
 
 def neighbor_list(state, delta=0.0, skin=0.0):
