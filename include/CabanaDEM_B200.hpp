@@ -544,6 +544,19 @@ class SolverDEM {
         }
     }
     dem_solver *handle() { return h_; }
+    // triangle-mesh wall (dem_solver_set_mesh): tri = nt * 9 vertex coordinates, one material,
+    // optional translation velocity (used when the force's DEM_Q6_WALL_STATIC bit is clear)
+    void setMesh(const std::vector<double> &tri, double E, double nu, double G,
+                 std::array<double, 3> velocity = {0.0, 0.0, 0.0}, int max_contacts = 8) {
+        particles_->context().check(dem_solver_set_mesh(h_, tri.empty() ? nullptr : tri.data(), (int)(tri.size() / 9), E,
+                                                        nu, G, velocity.data(), max_contacts),
+                                    "dem_solver_set_mesh");
+    }
+    std::array<double, 3> meshTranslation() {
+        std::array<double, 3> d{};
+        particles_->context().check(dem_solver_mesh_translation(h_, d.data()), "dem_solver_mesh_translation");
+        return d;
+    }
     // current wall positions [nw][3]: a wall with a velocity moves by dt * u each step when the
     // force's DEM_Q6_WALL_STATIC bit is clear (the reference's walls never move)
     std::vector<double> wallPositions() {
