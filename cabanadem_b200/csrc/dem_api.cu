@@ -983,7 +983,7 @@ extern "C" int dem_solver_create(dem_ctx *ctx, dem_particles *p, dem_walls *w, c
     A(dalloc(&B.bbox, 8));
     A(dalloc(&B.src, n));
     A(dalloc(&B.dst, n));
-    A(dalloc(&B.part_sums, (size_t)n / kPartBlock + 2));
+    A(dalloc(&B.part_sums, 2 * ((size_t)n / kPartBlock + 2)));
     s->nparts = (p->P.n + 127) / 128;
     A(dalloc(&s->d_epart, 4 * (size_t)s->nparts));
     A(dalloc(&s->d_eout, 4));

@@ -43,6 +43,8 @@ struct Ctl {
     int last_ndefer;          // deferred particles of the last completed fused step
     int nlone;                // particles [0, nlone) had no listed neighbour at the last build
                               // (placed first by the re-sort; 0 when the build did not re-sort)
+    int nclear;               // particles [nlone, nlone + nclear): every listed neighbour's gap
+                              // exceeded skin/2 at the last build (placed second)
 };
 
 struct Particles {
@@ -166,7 +168,7 @@ struct BuildBuffers {
     int cell_cap;
     unsigned long long *bbox; // 8 ordered-int words per scene: lo[3], hi[3], rmax
     int *src, *dst;           // permutation at re-sort
-    int *part_sums;           // [cap / kPartBlock + 2] per-block counts of the re-sort's partition
+    int *part_sums;           // [2][cap / kPartBlock + 2] per-block counts of the re-sort's partition
 };
 
 constexpr int kPartBlock = 256;   // block size of the re-sort's partition kernels

@@ -447,30 +447,33 @@ __global__ void __launch_bounds__(128) k_list(Particles P, NbrList L, Ctl *ctl, 
     }
 }
 
-// Re-sort partition, pass 1: for cell slot s (cell order of the old storage), flag[s] = 1 when
-// its particle has no neighbour within the list cutoff (the predicate of k_list), so that its
-// list will be empty; per-block counts of flagged slots into sums.
+// Re-sort partition, pass 1: class of cell slot s (cell order of the old storage): 0 when its
+// particle has no neighbour within the list cutoff (the predicate of k_list: its list will be
+// empty), 1 when, in the Verlet-skin mode, every listed neighbour's gap |x_i - x_j| - r_i - r_j
+// exceeds skin/2 (no contact possible while twice the displacement bound stays below skin/2),
+// else 2.  Per-block counts of classes 0 and 1 into sums[0][b], sums[1][b].
 __global__ void __launch_bounds__(kPartBlock) k_part_flag(Particles P, const Ctl *ctl, const Grid *g, const int *start,
-                                                          const int *items, double delta, double skin, int *flag,
-                                                          int *sums) {
+                                                          const int *items, double delta, double skin, int *cls,
+                                                          int *sums, int nb) {
     const int cur = ctl->cur, n = P.n;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    int lone = 0;
+    int c_s = 2;
     if (s < n && !(ctl->status & DEM_ERR_NAN)) {
         const int q = items[s];
         const Grid G = g[scene_of(P, q)];
         const double4 *pc = P.pos[cur];
         const D4 pi = ld4(pc, q);
+        const bool skin_mode = !(delta > 0.0) && skin > 0.0;
         int c[3];
         cell_of(G, pi, c);
-        lone = 1;
-        for (int dz = -1; dz <= 1 && lone; ++dz) {
+        bool any = false, near = false;
+        for (int dz = -1; dz <= 1 && !near; ++dz) {
             const int z = c[2] + dz;
             if (z < 0 || z >= G.dims[2]) continue;
-            for (int dy = -1; dy <= 1 && lone; ++dy) {
+            for (int dy = -1; dy <= 1 && !near; ++dy) {
                 const int y = c[1] + dy;
                 if (y < 0 || y >= G.dims[1]) continue;
-                for (int dx = -1; dx <= 1 && lone; ++dx) {
+                for (int dx = -1; dx <= 1 && !near; ++dx) {
                     const int x = c[0] + dx;
                     if (x < 0 || x >= G.dims[0]) continue;
                     const int key = cell_key(G, x, y, z);
@@ -483,64 +486,92 @@ __global__ void __launch_bounds__(kPartBlock) k_part_flag(Particles P, const Ctl
                         const double r2 = px * px + py * py + pz * pz;
                         const double cut = delta > 0.0 ? delta : pi.w + pj.w + skin;
                         if (r2 <= cut * cut) {
-                            lone = 0;
-                            break;
+                            any = true;
+                            if (!skin_mode || !(sqrt(r2) - (pi.w + pj.w) > 0.5 * skin)) {
+                                near = true;
+                                break;
+                            }
                         }
                     }
                 }
             }
         }
+        c_s = !any ? 0 : (near ? 2 : 1);
     }
-    if (s < n) flag[s] = lone;
-    __shared__ int cnt;
-    if (threadIdx.x == 0) cnt = 0;
+    if (s < n) cls[s] = c_s;
+    __shared__ int cnt[2];
+    if (threadIdx.x < 2) cnt[threadIdx.x] = 0;
     __syncthreads();
-    const int w = __popc(__ballot_sync(0xffffffffu, lone != 0));
-    if ((threadIdx.x & 31) == 0 && w) atomicAdd(&cnt, w);
+    const int w0 = __popc(__ballot_sync(0xffffffffu, s < n && c_s == 0));
+    const int w1 = __popc(__ballot_sync(0xffffffffu, s < n && c_s == 1));
+    if ((threadIdx.x & 31) == 0) {
+        if (w0) atomicAdd(&cnt[0], w0);
+        if (w1) atomicAdd(&cnt[1], w1);
+    }
     __syncthreads();
-    if (threadIdx.x == 0) sums[blockIdx.x] = cnt;
+    if (threadIdx.x < 2) sums[threadIdx.x * (nb + 1) + blockIdx.x] = cnt[threadIdx.x];
 }
 
-// Pass 2, one block: exclusive scan of the per-block counts (block order), total into nlone.
+// Pass 2, one block: exclusive scans of both per-block counts (block order); totals into
+// nlone and nclear.
 __global__ void __launch_bounds__(1024) k_part_scan(int *sums, int nb, Ctl *ctl) {
     __shared__ int part[1024];
-    const int per = (nb + 1023) / 1024;
-    const int b0 = threadIdx.x * per, b1 = min(b0 + per, nb);
-    int t = 0;
-    for (int b = b0; b < b1; ++b) t += sums[b];
-    part[threadIdx.x] = t;
-    __syncthreads();
-    for (int o = 1; o < 1024; o <<= 1) {   // inclusive scan of the thread totals
-        const int v = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+    for (int k = 0; k < 2; ++k) {
+        int *sk = sums + k * (nb + 1);
+        const int per = (nb + 1023) / 1024;
+        const int b0 = threadIdx.x * per, b1 = min(b0 + per, nb);
+        int t = 0;
+        for (int b = b0; b < b1; ++b) t += sk[b];
+        part[threadIdx.x] = t;
         __syncthreads();
-        part[threadIdx.x] += v;
+        for (int o = 1; o < 1024; o <<= 1) {   // inclusive scan of the thread totals
+            const int v = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+            __syncthreads();
+            part[threadIdx.x] += v;
+            __syncthreads();
+        }
+        int run = threadIdx.x > 0 ? part[threadIdx.x - 1] : 0;
+        for (int b = b0; b < b1; ++b) {
+            const int v = sk[b];
+            sk[b] = run;
+            run += v;
+        }
+        if (threadIdx.x == 1023) {
+            if (k == 0)
+                ctl->nlone = part[1023];
+            else
+                ctl->nclear = part[1023];
+        }
         __syncthreads();
     }
-    int run = threadIdx.x > 0 ? part[threadIdx.x - 1] : 0;
-    for (int b = b0; b < b1; ++b) {
-        const int v = sums[b];
-        sums[b] = run;
-        run += v;
-    }
-    if (threadIdx.x == 1023) ctl->nlone = part[1023];
 }
 
-// Pass 3: stable partition of the cell order, flagged slots first.  New position of slot s:
-// newitems[pos] = old index, and items[s] = pos (the cell table of the permuted storage).
-__global__ void __launch_bounds__(kPartBlock) k_part_place(int n, const int *flag, const int *sums, const Ctl *ctl,
-                                                           int *items, int *newitems) {
-    __shared__ int woff[kPartBlock / 32];
+// Pass 3: stable partition of the cell order by class (0, then 1, then 2).  New position of
+// slot s: newitems[pos] = old index, and items[s] = pos (the cell table of the permuted storage).
+__global__ void __launch_bounds__(kPartBlock) k_part_place(int n, const int *cls, const int *sums, int nb,
+                                                           const Ctl *ctl, int *items, int *newitems) {
+    __shared__ int woff[2][kPartBlock / 32];
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int f = s < n ? flag[s] : 0;
-    const unsigned b = __ballot_sync(0xffffffffu, f != 0);
-    if (lane == 0) woff[warp] = __popc(b);
+    const int c = s < n ? cls[s] : 2;
+    const unsigned b0 = __ballot_sync(0xffffffffu, s < n && c == 0);
+    const unsigned b1 = __ballot_sync(0xffffffffu, s < n && c == 1);
+    if (lane == 0) {
+        woff[0][warp] = __popc(b0);
+        woff[1][warp] = __popc(b1);
+    }
     __syncthreads();
-    int before = 0;   // flagged slots of this block before this warp
-    for (int w = 0; w < warp; ++w) before += woff[w];
+    int before0 = 0, before1 = 0;   // slots of class 0 / 1 of this block before this warp
+    for (int w = 0; w < warp; ++w) {
+        before0 += woff[0][w];
+        before1 += woff[1][w];
+    }
     if (s >= n) return;
-    const int lone_before = sums[blockIdx.x] + before + __popc(b & ((1u << lane) - 1u));
-    const int pos = f ? lone_before : ctl->nlone + (s - lone_before);
+    const unsigned below = (1u << lane) - 1u;
+    const int r0 = sums[blockIdx.x] + before0 + __popc(b0 & below);              // class-0 slots before s
+    const int r1 = sums[(nb + 1) + blockIdx.x] + before1 + __popc(b1 & below);   // class-1 slots before s
+    const int nl = ctl->nlone, nc = ctl->nclear;
+    const int pos = c == 0 ? r0 : c == 1 ? nl + r1 : nl + nc + (s - r0 - r1);
     newitems[pos] = items[s];
     items[s] = pos;
 }
@@ -549,6 +580,7 @@ __global__ void k_build_begin(Ctl *ctl) {
     if (threadIdx.x == 0) {
         ctl->max_nbr = 0;
         ctl->nlone = 0;
+        ctl->nclear = 0;
     }
 }
 
@@ -581,13 +613,14 @@ void launch_build(const Particles &P, Particles &alt, const NbrList &L, BuildBuf
     k_fill<<<gs, kB, 0, s>>>(n, B.key, B.cell_start, B.cell_items);
     k_cell_sort<<<gs, kB, 0, s>>>(B.cell_fill, B.cell_items, P.perm, B.total, ctl);
     if (resort) {
-        // new order: the cell order, split stably into particles with no listed neighbour
-        // (first) and the rest, so that the streaming kernel's leading warps load no list
+        // new order: the cell order, split stably into particles with no listed neighbour,
+        // particles whose listed neighbours all keep a gap above skin/2, and the rest, so that
+        // the streaming kernel's leading warps load no list and the next ones no partner
         const int nb = (n + kPartBlock - 1) / kPartBlock;
         k_part_flag<<<nb, kPartBlock, 0, s>>>(P, ctl, B.grid, B.cell_fill, B.cell_items, delta, skin, B.src,
-                                              B.part_sums);
+                                              B.part_sums, nb);
         k_part_scan<<<1, 1024, 0, s>>>(B.part_sums, nb, ctl);
-        k_part_place<<<nb, kPartBlock, 0, s>>>(n, B.src, B.part_sums, ctl, B.cell_items, B.key);
+        k_part_place<<<nb, kPartBlock, 0, s>>>(n, B.src, B.part_sums, nb, ctl, B.cell_items, B.key);
         k_make_dst<<<gs, kB, 0, s>>>(n, B.key, B.dst);
         k_permute<<<gs, kB, 0, s>>>(P, alt, ctl, B.key, B.dst);
         const size_t cap = (size_t)P.cap;

@@ -60,6 +60,9 @@ __global__ void __launch_bounds__(BS, MINB) k_stream(Particles P, NbrList L, Ctl
                                                      const WallGeom *__restrict__ walls) {
     if (!step_gate(ctl)) return;
     const int cur = ctl->cur, vcur = ctl->vcur, nlone = ctl->nlone;
+    // particles [nlone, nclear_end) had every listed neighbour at a gap above skin/2: while
+    // twice the displacement bound stays below skin/2 none of them can touch
+    const int nclear_end = (2.0 * ctl->disp < ctl->half_skin) ? nlone + ctl->nclear : nlone;
     const bool last = ctl->steps_done + 1 >= ctl->target;
     const int nxt = cur ^ 1, cap = P.cap;
     const double4 *__restrict__ pc = P.pos[cur];
@@ -82,7 +85,7 @@ __global__ void __launch_bounds__(BS, MINB) k_stream(Particles P, NbrList L, Ctl
         const int j0 = (!lone && L.maxnb > 0) ? ld_early_i(L.idx + i) : 0;
         const int j1 = (!lone && L.maxnb > 1) ? ld_early_i(L.idx + cap + i) : 0;
         bool defer = cs != 0;
-        if (!defer && nn > 0) {
+        if (!defer && nn > 0 && i >= nclear_end) {
             const D4 pa = ld4(pc, j0);
             D4 pb = pa;
             if (nn > 1) pb = ld4(pc, j1);
@@ -95,7 +98,7 @@ __global__ void __launch_bounds__(BS, MINB) k_stream(Particles P, NbrList L, Ctl
                 defer = defer || !(bx * bx + by * by + bz * bz >= sb * sb * 1.0000000001);
             }
         }
-        for (int kk = 2; kk < nn && !defer; ++kk) {
+        for (int kk = 2; kk < nn && !defer && i >= nclear_end; ++kk) {
             const int j = L.idx[(long)kk * cap + i];
             const D4 pj = ld4(pc, j);
             const double px = pi.x - pj.x, py = pi.y - pj.y, pz = pi.z - pj.z;
