@@ -836,7 +836,9 @@ __global__ void k_clear_status(Ctl *ctl, int bits) {
 
 bool ref_mode(const dem_solver *s) { return s->sp.rebuild_every_step != 0; }
 
-// Kernels of the next graph.  Few particles in contact (a sparse step): streaming kernel,
+// Kernels of the next graph.  Up to kOneKernelMaxN particles: always the one-kernel step (the
+// three-kernel step is launch-bound there; B200, 4,096 spheres in a walled box: 16.8 -> 10.6 us
+// per step).  Larger, few particles in contact (a sparse step): streaming kernel,
 // cooperative contact kernel, apply kernel; the cooperative kernel's short dependent chains
 // hide memory latency (B200, 2M-sphere lattice: 105 -> 87 us per step late in the run at 8
 // lanes).  Most particles in contact (a dense step): one per-thread kernel over every
@@ -853,8 +855,10 @@ void pick_contact_kernel(dem_solver *s) {
     } else if (req == 4 || req == 8) {
         s->fc.coop = fits ? req : 0;
     } else {
-        s->fc.all = s->fc.dense;
-        s->fc.coop = (!s->fc.dense && fits) ? 8 : 0;
+        // small systems are launch-bound: one kernel per step whatever the density
+        const bool one = s->fc.dense || s->p->P.n <= kOneKernelMaxN;
+        s->fc.all = one ? 1 : 0;
+        s->fc.coop = (!one && fits) ? 8 : 0;
     }
 }
 

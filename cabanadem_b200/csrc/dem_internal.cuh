@@ -72,6 +72,7 @@ __host__ __device__ __forceinline__ double2 load_mI(const Particles &P, int i) {
 }
 
 constexpr int kCoopSlots = 32;   // largest MaxCnts the cooperative contact kernel stages in shared memory
+constexpr int kOneKernelMaxN = 65536;   // particle count up to which the step is always one kernel
 constexpr int kVmaxSlots = 32;   // blocks fold their max into slot blockIdx % 32 (word 32 * slot)
 
 struct PairConst {   // per (material a, material b) or (material a, wall w)

@@ -44,3 +44,28 @@ def test_mesh_removed_is_plain_dem():
     got = s.particles.download()
     for f in ("x", "u", "omega"):
         assert np.array_equal(getattr(got, f), getattr(ref, f)), f
+
+
+def test_set_mesh_rejects_bad_arguments():
+    """More than 4,096 triangles, max_contacts outside 1..16 or a non-positive modulus are
+    refused with DEM_ERR_INVALID and leave the solver as it was: the next steps are the plain
+    DEM's, bit for bit."""
+    from cabanadem_b200._lib import DemError
+    sc = S.mesh_hopper(n=384, nsteps=200, band=0.002, drop_speed=4.0)
+    tri = np.asarray(sc.extra["mesh"].tri).reshape(-1, 3, 3)
+    s = api.from_scenario(sc)
+    s.set_mesh(np.zeros((0, 3, 3)), 1.0, 0.25, 1.0)
+    for args, kw, what in ((np.zeros((4097, 3, 3)), {}, "triangles"),
+                           (tri, {"max_contacts": 0}, "max_contacts"),
+                           (tri, {"max_contacts": 17}, "max_contacts"),
+                           (tri, {"E": 0.0}, "E, G")):
+        p = {"E": 1e9, "nu": 0.25, "G": 4e8, **kw}
+        mc = p.pop("max_contacts", 8)
+        with pytest.raises(DemError, match=what):
+            s.set_mesh(args, p["E"], p["nu"], p["G"], max_contacts=mc)
+    s.run_steps(200)
+    ref = sc.state.copy()
+    O.run(ref, sc.walls.copy(), sc.params, sc.dt, 200, skin=sc.skin, gravity=sc.gravity, pow_mode=O.POW_SQRT)
+    got = s.particles.download()
+    for f in ("x", "u", "omega"):
+        assert np.array_equal(getattr(got, f), getattr(ref, f)), f
