@@ -1,0 +1,152 @@
+"""Slab decomposition (cabanadem_b200/slabs.py) on CPU gloo ranks, the oracle stepping each
+rank's local set: a gas of soft spheres in a walled box, decomposed over 1, 2 and 3 slabs
+along x, is bit-identical to the undecomposed oracle run (positions, velocities, forces,
+torques, contact counts, live tangential history with partners as global ids, wall history).
+The run has particles that change slabs and contacts across slab faces, so both the
+migration and the ghost exchange are exercised.  A halo too thin for the step's drift makes
+every rank raise together instead of leaving one waiting."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+RADIUS, SIDE, STEPS, DT = 1e-3, 0.02, 600, 2e-6
+HALO = 2.0 * RADIUS + 1e-4
+LO = -1e-3      # slab faces off the lattice planes, within reach of the moving spheres
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _gas(seed=5):
+    """8 x 8 x 8 spheres of r = 1 mm on a 2.5 mm lattice with 0.1 mm jitter, velocities
+    U[-1, 1] m/s, E = 5 MPa (contacts last about 130 steps of 2 us), six walls, gravity."""
+    import sys
+    sys.path.insert(0, ROOT)
+    from cabanadem_b200.scenarios import _box_walls, _force_params
+    from cabanadem_b200.state import ParticleState
+    rng = np.random.default_rng(seed)
+    g = (np.arange(8) + 0.5) * 2.5e-3
+    pos = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    pos += rng.uniform(-1e-4, 1e-4, size=pos.shape)
+    s = ParticleState.create(len(pos), max_cnts=12, max_walls=6)
+    s.x[:] = pos
+    s.u[:] = rng.uniform(-1.0, 1.0, size=pos.shape)
+    s.rad[:] = RADIUS
+    s.rho[:] = 2500.0
+    s.set_sphere_mass()
+    s.E[:], s.nu[:] = 5e6, 0.3
+    s.G[:] = s.E / (2.0 * (1.0 + s.nu))
+    w = _box_walls((0.0, 0.0, 0.0), (SIDE, SIDE, SIDE), 5e6, 0.3, float(s.G[0]))
+    return s, w, _force_params(0.7, 0.7, 0.3, 0.3)
+
+
+def _oracle_step(walls, params):
+    from oracle import oracle as O
+
+    def step(st):
+        status = O.run(st, walls, params, DT, 1, skin=0.1 * RADIUS, gravity=(0.0, 0.0, -9.81), pow_mode=O.POW_SQRT)
+        assert status == 0
+    return step
+
+
+def _rank(rank, world, port, out, halo):
+    import sys
+    sys.path.insert(0, ROOT)
+    import torch.distributed as dist
+    from cabanadem_b200._lib import DemError
+    from cabanadem_b200.slabs import SlabDecomposition
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        s, w, prm = _gas()
+        dec = SlabDecomposition(0, LO, SIDE, halo, s.max_cnts, 6)
+        dec.scatter(s)
+        step = _oracle_step(w.copy(), prm)
+        cross, ghosts = 0, 0
+        try:
+            for _ in range(STEPS):
+                dec.step(step)
+                gid = dec.rows[:, 0].astype(np.int64)
+                a, k = dec.cols["tng_idx"]
+                part = dec.rows[:, a:a + k]
+                cross += int(np.sum((part >= 0) & ~np.isin(part, gid)))
+                ghosts = max(ghosts, dec.ghosts)
+        except DemError as e:
+            out[rank] = ("error", str(e))
+            return
+        g = dec.gather()
+        out[rank] = ("ok", dec.migrated, cross, ghosts, g)
+    finally:
+        dist.destroy_process_group()
+
+
+def _spawn(world, halo=HALO):
+    ctx = mp.get_context("spawn")
+    mgr = ctx.Manager()
+    out = mgr.dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank, args=(r, world, port, out, halo)) for r in range(world)]
+    # one OpenMP thread per rank, set before the children start: the runtime reads it when
+    # it is first loaded, which happens while the child imports torch
+    old = os.environ.get("OMP_NUM_THREADS")
+    os.environ["OMP_NUM_THREADS"] = "1"
+    try:
+        for p in procs:
+            p.start()
+    finally:
+        if old is None:
+            del os.environ["OMP_NUM_THREADS"]
+        else:
+            os.environ["OMP_NUM_THREADS"] = old
+    for p in procs:
+        p.join(300)
+    for p in procs:
+        if p.exitcode is None:
+            p.kill()
+        assert p.exitcode == 0
+    return dict(out)
+
+
+def _reference():
+    from oracle import oracle as O
+    s, w, prm = _gas()
+    st = O.run(s, w, prm, DT, STEPS, skin=0.1 * RADIUS, gravity=(0.0, 0.0, -9.81), pow_mode=O.POW_SQRT)
+    assert st == 0
+    return s
+
+
+@pytest.mark.parametrize("world", [1, 2, 3])
+def test_slab_decomposition_is_bitwise_single_domain(world):
+    out = _spawn(world)
+    assert all(out[r][0] == "ok" for r in range(world)), out
+    got = out[0][4]
+    ref = _reference()
+    for f in ("x", "u", "omega", "force", "torque", "tng_count"):
+        assert np.array_equal(getattr(got, f), getattr(ref, f)), f
+    live = np.arange(ref.max_cnts)[None, :] < ref.tng_count[:, None]
+    assert live.sum() > 100                       # a contact-rich run
+    for f in ("tng_idx", "tng_ss_x", "tng_ss_y", "tng_ss_z"):
+        assert np.array_equal(getattr(got, f)[live], getattr(ref, f)[live]), f
+    for f in ("tng_sw_x", "tng_sw_y", "tng_sw_z"):
+        assert np.array_equal(getattr(got, f), getattr(ref, f)), f
+    if world > 1:
+        assert sum(out[r][1] for r in range(world)) > 0      # particles changed slabs
+        assert sum(out[r][2] for r in range(world)) > 0      # contacts across a slab face
+        assert all(out[r][3] > 0 for r in range(world))      # every rank held ghosts
+
+
+def test_thin_halo_fails_on_every_rank():
+    """halo = 2 r exactly leaves no room for the drift: the first step's check fails and both
+    ranks raise (no rank is left waiting in an exchange)."""
+    out = _spawn(2, halo=2.0 * RADIUS)
+    assert [out[r][0] for r in range(2)] == ["error", "error"], out
+    assert any("moved more than" in out[r][1] for r in range(2))
