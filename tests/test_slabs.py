@@ -1,7 +1,8 @@
 """Slab decomposition (cabanadem_b200/slabs.py) on CPU gloo ranks, the oracle stepping each
 rank's local set: a gas of soft spheres in a walled box, decomposed over 1, 2 and 3 slabs
-along x, is bit-identical to the undecomposed oracle run (positions, velocities, forces,
-torques, contact counts, live tangential history with partners as global ids, wall history).
+along x (and over 2 slabs with a kinematic piston wall), is bit-identical to the
+undecomposed oracle run (positions, velocities, forces, torques, contact counts, live
+tangential history with partners as global ids, wall history).
 The run has particles that change slabs and contacts across slab faces, so both the
 migration and the ghost exchange are exercised.  A halo too thin for the step's drift makes
 every rank raise together instead of leaving one waiting."""
@@ -26,12 +27,13 @@ def _free_port():
     return p
 
 
-def _gas(seed=5):
+def _gas(seed=5, piston=0.0):
     """8 x 8 x 8 spheres of r = 1 mm on a 2.5 mm lattice with 0.1 mm jitter, velocities
-    U[-1, 1] m/s, E = 5 MPa (contacts last about 130 steps of 2 us), six walls, gravity."""
+    U[-1, 1] m/s, E = 5 MPa (contacts last about 130 steps of 2 us), six walls, gravity.
+    piston > 0: the +x wall moves inwards at that speed (DEM_Q6_WALL_STATIC clear)."""
     import sys
     sys.path.insert(0, ROOT)
-    from cabanadem_b200.scenarios import _box_walls, _force_params
+    from cabanadem_b200.scenarios import Q6_WALL_STATIC, REF_COMPAT, _box_walls, _force_params
     from cabanadem_b200.state import ParticleState
     rng = np.random.default_rng(seed)
     g = (np.arange(8) + 0.5) * 2.5e-3
@@ -46,6 +48,9 @@ def _gas(seed=5):
     s.E[:], s.nu[:] = 5e6, 0.3
     s.G[:] = s.E / (2.0 * (1.0 + s.nu))
     w = _box_walls((0.0, 0.0, 0.0), (SIDE, SIDE, SIDE), 5e6, 0.3, float(s.G[0]))
+    if piston:
+        w.u[1, 0] = -piston
+        return s, w, _force_params(0.7, 0.7, 0.3, 0.3, REF_COMPAT & ~Q6_WALL_STATIC)
     return s, w, _force_params(0.7, 0.7, 0.3, 0.3)
 
 
@@ -58,7 +63,7 @@ def _oracle_step(walls, params):
     return step
 
 
-def _rank(rank, world, port, out, halo):
+def _rank(rank, world, port, out, halo, piston):
     import sys
     sys.path.insert(0, ROOT)
     import torch.distributed as dist
@@ -67,7 +72,7 @@ def _rank(rank, world, port, out, halo):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
-        s, w, prm = _gas()
+        s, w, prm = _gas(piston=piston)
         dec = SlabDecomposition(0, LO, SIDE, halo, s.max_cnts, 6)
         dec.scatter(s)
         step = _oracle_step(w.copy(), prm)
@@ -89,12 +94,12 @@ def _rank(rank, world, port, out, halo):
         dist.destroy_process_group()
 
 
-def _spawn(world, halo=HALO):
+def _spawn(world, halo=HALO, piston=0.0):
     ctx = mp.get_context("spawn")
     mgr = ctx.Manager()
     out = mgr.dict()
     port = _free_port()
-    procs = [ctx.Process(target=_rank, args=(r, world, port, out, halo)) for r in range(world)]
+    procs = [ctx.Process(target=_rank, args=(r, world, port, out, halo, piston)) for r in range(world)]
     # one OpenMP thread per rank, set before the children start: the runtime reads it when
     # it is first loaded, which happens while the child imports torch
     old = os.environ.get("OMP_NUM_THREADS")
@@ -116,20 +121,21 @@ def _spawn(world, halo=HALO):
     return dict(out)
 
 
-def _reference():
+def _reference(piston=0.0):
     from oracle import oracle as O
-    s, w, prm = _gas()
+    s, w, prm = _gas(piston=piston)
     st = O.run(s, w, prm, DT, STEPS, skin=0.1 * RADIUS, gravity=(0.0, 0.0, -9.81), pow_mode=O.POW_SQRT)
     assert st == 0
     return s
 
 
-@pytest.mark.parametrize("world", [1, 2, 3])
-def test_slab_decomposition_is_bitwise_single_domain(world):
-    out = _spawn(world)
+@pytest.mark.parametrize("world,piston", [(1, 0.0), (2, 0.0), (3, 0.0), (2, 0.5)],
+                         ids=["1", "2", "3", "2_piston"])
+def test_slab_decomposition_is_bitwise_single_domain(world, piston):
+    out = _spawn(world, piston=piston)
     assert all(out[r][0] == "ok" for r in range(world)), out
     got = out[0][4]
-    ref = _reference()
+    ref = _reference(piston)
     for f in ("x", "u", "omega", "force", "torque", "tng_count"):
         assert np.array_equal(getattr(got, f), getattr(ref, f)), f
     live = np.arange(ref.max_cnts)[None, :] < ref.tng_count[:, None]
@@ -138,6 +144,8 @@ def test_slab_decomposition_is_bitwise_single_domain(world):
         assert np.array_equal(getattr(got, f)[live], getattr(ref, f)[live]), f
     for f in ("tng_sw_x", "tng_sw_y", "tng_sw_z"):
         assert np.array_equal(getattr(got, f), getattr(ref, f)), f
+    if piston:
+        assert not np.array_equal(got.u, _reference(0.0).u)  # the moving wall changed the run
     if world > 1:
         assert sum(out[r][1] for r in range(world)) > 0      # particles changed slabs
         assert sum(out[r][2] for r in range(world)) > 0      # contacts across a slab face
