@@ -254,8 +254,9 @@ class DeviceStep:
     advance inside the solver)."""
 
     def __init__(self, walls: WallState | None, params: dict, dt: float, skin: float = 0.0, delta: float = 0.0,
-                 gravity=(0.0, 0.0, 0.0), ctx=None):
-        from . import api
+                 gravity=(0.0, 0.0, 0.0), ctx=None, api=None):
+        if api is None:      # the device library's Python API (a stand-in with the same calls in tests)
+            from . import api
         self.api = api
         self.walls = walls.copy() if walls is not None and walls.n > 0 else None
         self.force = api.Force(params["cor_pp"], params["cor_pw"], params["mu_pp"], params["mu_pw"],

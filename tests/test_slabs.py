@@ -63,7 +63,68 @@ def _oracle_step(walls, params):
     return step
 
 
-def _rank(rank, world, port, out, halo, piston):
+class _HostApi:
+    """Stand-in for cabanadem_b200.api with the calls DeviceStep makes and the same host-side
+    semantics (upload of the first MaxNoWalls wall-history columns, download into a state with
+    max(MaxNoWalls, 1) columns, solver-owned wall positions), the oracle taking the step: it
+    checks DeviceStep's glue on the CPU."""
+    REF_COMPAT = 0x3F
+
+    @staticmethod
+    def default_context():
+        return None
+
+    class Force:
+        def __init__(self, cor_pp, cor_pw, mu_pp, mu_pw, quirks):
+            self.params = dict(cor_pp=cor_pp, cor_pw=cor_pw, mu_pp=mu_pp, mu_pw=mu_pw, quirks=quirks)
+
+    class Particles:
+        def __init__(self, n, max_cnts, max_walls, ctx=None):
+            from cabanadem_b200.state import ParticleState
+            self.mw = max_walls
+            self.st = ParticleState.create(n, max_cnts, max(max_walls, 1))
+
+        def upload(self, s):
+            for k, v in s.arrays().items():
+                if k.startswith("tng_sw_"):
+                    getattr(self.st, k)[:, : self.mw] = v[:, : self.mw]
+                else:
+                    getattr(self.st, k)[...] = v
+
+        def download(self):
+            return self.st.copy()
+
+        def close(self):
+            self.st = None
+
+    class Wall:
+        def __init__(self, n, ctx=None):
+            self.w = None
+
+        def upload(self, w):
+            self.w = w.copy()
+
+        def close(self):
+            self.w = None
+
+    class SolverDEM:
+        def __init__(self, p, w, force, dt, delta=0.0, skin=0.0, gravity=(0.0, 0.0, 0.0)):
+            self.p, self.w, self.f = p, w, force
+            self.dt, self.delta, self.skin, self.g = dt, delta, skin, gravity
+
+        def run_steps(self, n):
+            from oracle import oracle as O
+            assert O.run(self.p.st, self.w.w, self.f.params, self.dt, n, delta=self.delta, skin=self.skin,
+                         gravity=self.g, pow_mode=O.POW_SQRT) == 0
+
+        def wall_positions(self):
+            return self.w.w.x.copy()
+
+        def close(self):
+            pass
+
+
+def _rank(rank, world, port, out, halo, piston, glue=False):
     import sys
     sys.path.insert(0, ROOT)
     import torch.distributed as dist
@@ -75,7 +136,11 @@ def _rank(rank, world, port, out, halo, piston):
         s, w, prm = _gas(piston=piston)
         dec = SlabDecomposition(0, LO, SIDE, halo, s.max_cnts, 6)
         dec.scatter(s)
-        step = _oracle_step(w.copy(), prm)
+        if glue:
+            from cabanadem_b200.slabs import DeviceStep
+            step = DeviceStep(w, prm, DT, skin=0.1 * RADIUS, gravity=(0.0, 0.0, -9.81), api=_HostApi)
+        else:
+            step = _oracle_step(w.copy(), prm)
         cross, ghosts = 0, 0
         try:
             for _ in range(STEPS):
@@ -94,12 +159,12 @@ def _rank(rank, world, port, out, halo, piston):
         dist.destroy_process_group()
 
 
-def _spawn(world, halo=HALO, piston=0.0):
+def _spawn(world, halo=HALO, piston=0.0, glue=False):
     ctx = mp.get_context("spawn")
     mgr = ctx.Manager()
     out = mgr.dict()
     port = _free_port()
-    procs = [ctx.Process(target=_rank, args=(r, world, port, out, halo, piston)) for r in range(world)]
+    procs = [ctx.Process(target=_rank, args=(r, world, port, out, halo, piston, glue)) for r in range(world)]
     # one OpenMP thread per rank, set before the children start: the runtime reads it when
     # it is first loaded, which happens while the child imports torch
     old = os.environ.get("OMP_NUM_THREADS")
@@ -158,3 +223,13 @@ def test_thin_halo_fails_on_every_rank():
     out = _spawn(2, halo=2.0 * RADIUS)
     assert [out[r][0] for r in range(2)] == ["error", "error"], out
     assert any("moved more than" in out[r][1] for r in range(2))
+
+
+def test_device_step_glue_with_host_stand_in():
+    """DeviceStep's upload / step / download / wall-carry logic, the device calls replaced by
+    the host stand-in: 2 slabs with the piston wall stay bit-identical to the oracle run."""
+    out = _spawn(2, piston=0.5, glue=True)
+    assert all(out[r][0] == "ok" for r in range(2)), out
+    got, ref = out[0][4], _reference(0.5)
+    for f in ("x", "u", "omega", "force", "torque", "tng_count", "tng_sw_y", "tng_sw_z"):
+        assert np.array_equal(getattr(got, f), getattr(ref, f)), f
