@@ -235,6 +235,75 @@ class HostSlice {
 };
 
 // ---------------------------------------------------------------------------------------
+// XDMF snapshot.  The reference's writer (Cabana's HDF5 particle output, called at
+// Particles.hpp:306-326) stores one dataset per slice label in particles_<k>.h5 with the
+// step's time; viewers open it through an XDMF index.  No HDF5 library is in this image, so
+// here the heavy data is one raw little-endian file, particles_<k>.bin (the datasets one after
+// another), and particles_<k>.xmf indexes it (XDMF 2: a Polyvertex grid with its Time, the
+// positions as XYZ geometry, one node attribute per other dataset, Format="Binary" data items
+// with byte offsets), which XDMF readers such as ParaView and VisIt open.
+// ---------------------------------------------------------------------------------------
+struct XdmfField {
+    std::string name;   // dataset name (the reference's slice label)
+    const void *data;   // [n][ncomp] row-major
+    int ncomp;          // 1 (Scalar attribute) or 3 (Vector; the positions are the Geometry)
+    bool is_int;        // int32 instead of float64
+};
+
+// <folder>/particles_<step>.xmf and .bin; fields[0] holds the positions.
+inline void writeXdmfSnapshot(const std::string &folder, int step, double time, int n,
+                              const std::vector<XdmfField> &fields) {
+    const unsigned short probe = 1;
+    if (*reinterpret_cast<const unsigned char *>(&probe) != 1) throw Error("writeXdmfSnapshot: big-endian host");
+    if (fields.empty() || fields[0].ncomp != 3 || fields[0].is_int)
+        throw Error("writeXdmfSnapshot: fields[0] must be the positions, [n][3] float64");
+    for (const auto &f : fields)
+        if (f.ncomp != 1 && f.ncomp != 3) throw Error("writeXdmfSnapshot: " + f.name + ": 1 or 3 components");
+    const std::string stem = "particles_" + std::to_string(step);
+    const std::string bin = folder + "/" + stem + ".bin", xmf = folder + "/" + stem + ".xmf";
+    std::vector<long> seek;
+    {
+        std::FILE *fb = std::fopen(bin.c_str(), "wb");
+        if (!fb) throw Error("cannot write " + bin);
+        long at = 0;
+        for (const auto &f : fields) {
+            const size_t bytes = static_cast<size_t>(n) * f.ncomp * (f.is_int ? 4 : 8);
+            seek.push_back(at);
+            if (bytes && std::fwrite(f.data, 1, bytes, fb) != bytes) {
+                std::fclose(fb);
+                throw Error("short write to " + bin);
+            }
+            at += static_cast<long>(bytes);
+        }
+        if (std::fclose(fb) != 0) throw Error("cannot close " + bin);
+    }
+    std::FILE *fx = std::fopen(xmf.c_str(), "w");
+    if (!fx) throw Error("cannot write " + xmf);
+    auto item = [&](size_t k) {
+        const XdmfField &f = fields[k];
+        std::fprintf(fx,
+                     "        <DataItem Dimensions=\"%d%s\" NumberType=\"%s\" Precision=\"%d\" Format=\"Binary\" "
+                     "Endian=\"Little\" Seek=\"%ld\">%s.bin</DataItem>\n",
+                     n, f.ncomp == 3 ? " 3" : "", f.is_int ? "Int" : "Float", f.is_int ? 4 : 8, seek[k], stem.c_str());
+    };
+    std::fprintf(fx, "<?xml version=\"1.0\" ?>\n<!DOCTYPE Xdmf SYSTEM \"Xdmf.dtd\" []>\n<Xdmf Version=\"2.0\">\n");
+    std::fprintf(fx, "  <Domain>\n    <Grid Name=\"particles\" GridType=\"Uniform\">\n");
+    std::fprintf(fx, "      <Time Value=\"%.17g\"/>\n", time);
+    std::fprintf(fx, "      <Topology TopologyType=\"Polyvertex\" NumberOfElements=\"%d\" NodesPerElement=\"1\"/>\n", n);
+    std::fprintf(fx, "      <Geometry GeometryType=\"XYZ\">\n");
+    item(0);
+    std::fprintf(fx, "      </Geometry>\n");
+    for (size_t k = 1; k < fields.size(); ++k) {
+        std::fprintf(fx, "      <Attribute Name=\"%s\" AttributeType=\"%s\" Center=\"Node\">\n", fields[k].name.c_str(),
+                     fields[k].ncomp == 3 ? "Vector" : "Scalar");
+        item(k);
+        std::fprintf(fx, "      </Attribute>\n");
+    }
+    std::fprintf(fx, "    </Grid>\n  </Domain>\n</Xdmf>\n");
+    if (std::fclose(fx) != 0) throw Error("cannot close " + xmf);
+}
+
+// ---------------------------------------------------------------------------------------
 // Particles<MemorySpace, Dim, MaxCnts, MaxNoWalls> (Particles.hpp:22-71)
 // ---------------------------------------------------------------------------------------
 template <class MemorySpace, int Dimension, int MaxCnts, int MaxNoWalls>
@@ -305,12 +374,37 @@ class Particles {
         for (auto &kv : mi_) kv.second->fresh = false;
     }
 
+    // Snapshot format of output(): "csv" (the default), "xdmf" or "both".
+    void setOutputFormat(const std::string &format) {
+        if (format != "csv" && format != "xdmf" && format != "both")
+            throw Error("setOutputFormat: csv, xdmf or both");
+        format_ = format;
+    }
+
     // output(step, time) (Particles.hpp:299-346): one snapshot per call, <folder>/particles_<step>.csv,
     // one row per particle with the fields the reference writes to particles_<step>.h5 (its
     // HDF5 writer; no HDF5 library here) minus the accelerations, which are not stored.
-    // Columns are named after the reference's slices with a component suffix.  No folder, no output.
+    // Columns are named after the reference's slices with a component suffix.  With the
+    // "xdmf" format the same datasets go to particles_<step>.xmf / .bin (writeXdmfSnapshot).
+    // No folder, no output.
     void output(int output_step, double output_time) {
         if (out_.empty()) return;
+        if (format_ != "csv") {
+            auto x = slicePosition();
+            auto u = sliceVelocity();
+            auto w = sliceOmega();
+            auto f = sliceForce();
+            auto m = sliceMass();
+            auto rho = sliceDensity();
+            auto r = sliceRadius();
+            auto tc = sliceTotalNoTangentialContacts();
+            writeXdmfSnapshot(out_, output_step, output_time, n_,
+                              {{"positions", x.data(), 3, false}, {"velocities", u.data(), 3, false},
+                               {"omega", w.data(), 3, false}, {"forces", f.data(), 3, false},
+                               {"mass", m.data(), 1, false}, {"density", rho.data(), 1, false},
+                               {"radius", r.data(), 1, false}, {"total_no_tangential_contacts", tc.data(), 1, true}});
+            if (format_ == "xdmf") return;
+        }
         auto x = slicePosition();
         auto u = sliceVelocity();
         auto w = sliceOmega();
@@ -419,6 +513,7 @@ class Particles {
     int n_;
     int attached_ = 0;
     std::string out_;
+    std::string format_ = "csv";
     std::shared_ptr<Context> ctx_;
     dem_particles *h_ = nullptr;
     std::map<int, std::shared_ptr<Mirror<double>>> md_;

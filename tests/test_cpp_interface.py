@@ -1,7 +1,7 @@
 """The C++ interface (include/CabanaDEM_B200.hpp) and the example drivers on it.
 
-On the CPU every driver builds against the header and library, and the snapshot reader
-parses the drivers' output format.  On the GPU each driver runs with the reference's command
+On the CPU every driver builds against the header and library, the snapshot reader parses
+the drivers' output format, and the header's XDMF writer round-trips through the reader.  On the GPU each driver runs with the reference's command
 line and input file; every snapshot it writes (particles_<k>.csv after each step divisible by
 output_frequency) is compared bit for bit with the oracle stepped the same way, and the
 observables the reference's automate.py reads from those files are checked: restitution
@@ -75,6 +75,65 @@ def test_snapshot_reader(tmp_path):
     assert s["forces"][0].tolist() == [10., 11., 12.]
     assert s["total_no_tangential_contacts"].tolist() == [2, 0]
     assert s["radius"].tolist() == [15., 1.]
+
+
+_XDMF_PROG = r"""
+#include "CabanaDEM_B200.hpp"
+#include <cstdlib>
+int main(int argc, char **argv) {
+    const int n = 5;
+    std::vector<double> x(3 * n), u(3 * n), w(3 * n), f(3 * n), m(n), rho(n), r(n);
+    std::vector<int> tc(n);
+    for (int i = 0; i < n; ++i) {
+        for (int d = 0; d < 3; ++d) {
+            x[3 * i + d] = 0.1 * i + d + 1.0 / 3.0;
+            u[3 * i + d] = -2.5 * i + d;
+            w[3 * i + d] = 1e-300 * (i + 1) * (d + 1);
+            f[3 * i + d] = 1e9 / (i + d + 1);
+        }
+        m[i] = 0.5 + i; rho[i] = 2500.0; r[i] = 1e-3 * (i + 1); tc[i] = i % 3;
+    }
+    CabanaDEM::writeXdmfSnapshot(argv[1], std::atoi(argv[2]), 0.1 + 0.2, n,
+        {{"positions", x.data(), 3, false}, {"velocities", u.data(), 3, false}, {"omega", w.data(), 3, false},
+         {"forces", f.data(), 3, false}, {"mass", m.data(), 1, false}, {"density", rho.data(), 1, false},
+         {"radius", r.data(), 1, false}, {"total_no_tangential_contacts", tc.data(), 1, true}});
+    return 0;
+}
+"""
+
+
+def test_xdmf_snapshot_round_trip(tmp_path):
+    """writeXdmfSnapshot (the C++ interface's XDMF output) read back by snapshots.read_xdmf:
+    every dataset bit for bit, the time, the Polyvertex topology and the grid's layout."""
+    import xml.etree.ElementTree as ET
+    src = tmp_path / "xdmf.cpp"
+    src.write_text(_XDMF_PROG)
+    exe = tmp_path / "xdmf"
+    subprocess.run(["g++", "-O1", "-std=c++17", "-I" + os.path.join(ROOT, "include"), str(src), "-o", str(exe)],
+                   check=True)
+    for step in (7, 12):
+        subprocess.run([str(exe), str(tmp_path), str(step)], check=True)
+    fs = snapshots.files(str(tmp_path), ".xmf")
+    assert [os.path.basename(f) for f in fs] == ["particles_7.xmf", "particles_12.xmf"]
+    s = snapshots.read_xdmf(fs[1])
+    n, i = 5, np.arange(5)[:, None]
+    d = np.arange(3)[None, :]
+    assert s["time"] == 0.1 + 0.2
+    assert np.array_equal(s["positions"], 0.1 * i + d + 1.0 / 3.0)
+    assert np.array_equal(s["velocities"], -2.5 * i + d)
+    assert np.array_equal(s["omega"], 1e-300 * (i + 1) * (d + 1))
+    assert np.array_equal(s["forces"], 1e9 / (i + d + 1))
+    assert np.array_equal(s["mass"], 0.5 + np.arange(n)) and np.array_equal(s["density"], np.full(n, 2500.0))
+    assert np.array_equal(s["radius"], 1e-3 * (np.arange(n) + 1))
+    assert s["total_no_tangential_contacts"].dtype == np.int32
+    assert s["total_no_tangential_contacts"].tolist() == [0, 1, 2, 0, 1]
+    grid = ET.parse(fs[1]).getroot().find("Domain/Grid")
+    topo = grid.find("Topology")
+    assert topo.get("TopologyType") == "Polyvertex" and topo.get("NumberOfElements") == "5"
+    assert grid.find("Geometry").get("GeometryType") == "XYZ"
+    kinds = {a.get("Name"): a.get("AttributeType") for a in grid.findall("Attribute")}
+    assert kinds["velocities"] == "Vector" and kinds["mass"] == "Scalar"
+    assert os.path.getsize(tmp_path / "particles_12.bin") == n * (4 * 3 * 8 + 3 * 8 + 4)
 
 
 def _oracle_snapshots(sc):
