@@ -10,6 +10,12 @@
 //   CabanaDEM::Force<Exec>(cor_pp,cor_pw,mu_pp,mu_pw) same (+ optional quirk bits)
 //   CabanaDEM::createSolverDEM<Mem>(...)->run()     same: num_steps + 1 steps
 //     (Solver.hpp:66-138)
+//   CabanaDEM::Integrator<Exec>(dt).stage1/2/3(p)   Integrator<Solver>(solver).stage1/2/3(p)
+//     (Integrator.hpp:15-102)
+//   computeForceParticleParticleInfiniteWall(        computeForceParticleParticleInfiniteWall(solver)
+//     force, p, wall, neigh, tag, dt) (Force.hpp:700-710)   and solver->buildNeighbors()
+//   Particles::output -> particles_<k>.h5            particles_<k>.csv, or .xmf + .bin
+//                                                    (setOutputFormat("xdmf"))
 //   CabanaBondedDEM::ParticlesBondedDEM<Mem,3,MaxBonds>::setupBonds (BondedDEM_Particles.hpp:86)
 //                                                    BondedDEM<Mem,3,MaxBonds> (setupBonds, run)
 //
@@ -638,6 +644,16 @@ class SolverDEM {
             if (out_) out_(step, step * dt);
         }
     }
+    // The reference loop's phases, one launch each, for callers that drive the loop themselves
+    // (Solver.hpp:81-94): integrator->stage1 / stage2 (Integrator.hpp:31-74), neighbors->build,
+    // computeForceParticleParticleInfiniteWall (Force.hpp:700-710), stage3 (:77-102).  Host
+    // edits made through slices are uploaded first; slices read the new state afterwards.
+    void stage1() { phase(dem_stage1, "dem_stage1"); }
+    void stage2() { phase(dem_stage2, "dem_stage2"); }
+    void buildNeighbors() { phase(dem_build_neighbors, "dem_build_neighbors"); }
+    void computeForce() { phase(dem_compute_force, "dem_compute_force", DEM_ERR_CONTACT_OVERFLOW); }
+    void stage3() { phase(dem_stage3, "dem_stage3"); }
+
     dem_solver *handle() { return h_; }
     // triangle-mesh wall (dem_solver_set_mesh): tri = nt * 9 vertex coordinates, one material,
     // optional translation velocity (used when the force's DEM_Q6_WALL_STATIC bit is clear)
@@ -666,12 +682,42 @@ class SolverDEM {
     double dt = 0.0;
 
   private:
+    void phase(int (*f)(dem_solver *), const char *what, int allow = 0) {
+        particles_->commit();
+        particles_->context().check(f(h_), what, allow);
+        particles_->invalidate();
+    }
+
     std::shared_ptr<ParticleType> particles_;
     std::shared_ptr<WallType> wall_;
     std::shared_ptr<ForceModel> force_;
     dem_solver *h_ = nullptr;
     std::function<void(int, double)> out_;
 };
+
+// Integrator<ExecutionSpace> (Integrator.hpp:15-102) on a solver's particles: the reference
+// constructs it from dt; here the solver holds dt and the device state, so it wraps the solver.
+template <class SolverType>
+class Integrator {
+  public:
+    explicit Integrator(std::shared_ptr<SolverType> solver) : s_(std::move(solver)) {}
+    template <class ParticleType>
+    void stage1(ParticleType &) { s_->stage1(); }
+    template <class ParticleType>
+    void stage2(ParticleType &) { s_->stage2(); }
+    template <class ParticleType>
+    void stage3(ParticleType &) { s_->stage3(); }
+
+  private:
+    std::shared_ptr<SolverType> s_;
+};
+
+// computeForceParticleParticleInfiniteWall (Force.hpp:700-710): zero F and tau, compact the
+// tangential contacts, particle-particle force, wall force, on the solver's particles and walls
+template <class SolverType>
+void computeForceParticleParticleInfiniteWall(SolverType &solver) {
+    solver.computeForce();
+}
 
 // createSolverDEM<MemorySpace>(inputs, particles, wall, force, delta) (Solver.hpp:127-138)
 template <class MemorySpace, class InputsType, class ParticleType, class WallType, class ForceModel>

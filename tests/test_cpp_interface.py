@@ -136,6 +136,49 @@ def test_xdmf_snapshot_round_trip(tmp_path):
     assert os.path.getsize(tmp_path / "particles_12.bin") == n * (4 * 3 * 8 + 3 * 8 + 4)
 
 
+_PHASE_PROG = r"""
+#include "CabanaDEM_B200.hpp"
+struct mem {};
+struct exe {};
+// the reference loop (Solver.hpp:81-94) written with the phase-level calls
+template <class S, class P>
+void loop(std::shared_ptr<S> solver, P &particles, int nsteps) {
+    CabanaDEM::Integrator<S> integrator(solver);
+    for (int step = 0; step < nsteps; ++step) {
+        integrator.stage1(particles);
+        integrator.stage2(particles);
+        solver->buildNeighbors();
+        CabanaDEM::computeForceParticleParticleInfiniteWall(*solver);
+        integrator.stage3(particles);
+    }
+}
+int main(int argc, char **argv) {
+    CabanaDEM::Inputs inputs(argv[1]);
+    auto force = std::make_shared<CabanaDEM::Force<exe>>(0.8, 0.8, 0.3, 0.3);
+    auto particles = std::make_shared<CabanaDEM::Particles<mem, 3, 6, 1>>(exe(), 2, argv[2]);
+    particles->setOutputFormat("both");
+    std::shared_ptr<CabanaDEM::Wall<mem, 3>> wall;
+    auto solver = CabanaDEM::createSolverDEM<mem>(inputs, particles, wall, force, 3e-3);
+    loop(solver, *particles, 3);
+    particles->output(0, 0.0);
+    return 0;
+}
+"""
+
+
+def test_phase_level_interface_builds(tmp_path):
+    """The reference loop written with Integrator<Solver>, buildNeighbors and
+    computeForceParticleParticleInfiniteWall builds and links against the library (it runs
+    only with a GPU)."""
+    _build()
+    src = tmp_path / "phases.cpp"
+    src.write_text(_PHASE_PROG)
+    lib = os.path.join(ROOT, "cabanadem_b200")
+    subprocess.run(["g++", "-O1", "-std=c++17", "-I" + os.path.join(ROOT, "include"), str(src), "-o",
+                    str(tmp_path / "phases"), "-L" + lib, "-lb200dem", "-Wl,-rpath," + lib], check=True)
+    assert os.access(tmp_path / "phases", os.X_OK)
+
+
 def _oracle_snapshots(sc):
     """The oracle stepped as SolverDEM::run: steps 0..num_steps, a snapshot after every step
     divisible by output_frequency (Solver.hpp:79-108)."""
