@@ -1,0 +1,122 @@
+"""Analytic known-answer checks of the oracle's physics, independent of the reference's data
+files.  An elastic head-on impact (e = 1, mu = 0) gives back the kinetic energy it started
+with and swaps the velocities.  A damped one separates at e times the approach speed (the
+damping law of src/CabanaDEM_Force.hpp:206-215).  Colliding clusters with friction and damping
+keep their total momentum: with every reference quirk cleared, each pair's forces are equal and
+opposite.  A bond at its rest length exerts no force.  The device FP64 path is bit-identical to
+the oracle, so these hold for it too."""
+import numpy as np
+import pytest
+
+from cabanadem_b200.scenarios import _force_params
+from cabanadem_b200.state import BondState, ParticleState
+from oracle import oracle as O
+
+R, RHO, E, NU = 0.01, 2600.0, 70e9, 0.25
+
+
+def _pair(v=0.5, gap=1e-5):
+    """Two glass spheres of r = 1 cm closing head-on along x at +-v."""
+    s = ParticleState.create(2, max_cnts=6, max_walls=1)
+    s.x[0, 0], s.x[1, 0] = -R - gap / 2, R + gap / 2
+    s.u[0, 0], s.u[1, 0] = v, -v
+    s.rad[:], s.rho[:], s.E[:], s.nu[:] = R, RHO, E, NU
+    s.G[:] = E / (2.0 * (1.0 + NU))
+    s.set_sphere_mass()
+    return s
+
+
+def _run(s, cor, mu, nsteps, quirks=None, dt=1e-6):
+    prm = _force_params(cor, cor, mu, mu) if quirks is None else _force_params(cor, cor, mu, mu, quirks)
+    assert O.run(s, None, prm, dt, nsteps, skin=0.1 * R, pow_mode=O.POW_SQRT) == 0
+    return s
+
+
+def test_elastic_head_on_impact_conserves_energy():
+    """The kinetic energy after an e = 1 impact equals the energy before, up to velocity
+    Verlet's error, which shrinks at least 3x each time dt halves (6e-5 at 1 us, 9e-7 at 0.25 us
+    for this 240 us contact)."""
+    err = []
+    for dt in (1e-6, 5e-7, 2.5e-7):
+        s = _pair()
+        ke0 = O.kinetic_energy(s)
+        _run(s, 1.0, 0.0, int(round(600e-6 / dt)), dt=dt)
+        assert s.tng_count.sum() == 0 and s.x[1, 0] - s.x[0, 0] > 2 * R   # separated
+        err.append(abs(O.kinetic_energy(s) - ke0) / ke0)
+        assert abs(s.u[0, 0] + 0.5) <= 1e-4 and abs(s.u[1, 0] - 0.5) <= 1e-4     # velocities swapped
+    assert err[0] / err[1] >= 3.0 and err[1] / err[2] >= 3.0, err
+    assert err[2] < 2e-6, err
+
+
+@pytest.mark.parametrize("cor", [0.3, 0.5, 0.8])
+def test_damped_head_on_impact_separates_at_e_times_approach(cor):
+    s = _pair()
+    _run(s, cor, 0.0, 800)
+    assert s.x[1, 0] - s.x[0, 0] > 2 * R
+    assert abs((s.u[1, 0] - s.u[0, 0]) / 1.0 - cor) <= 0.02 * cor
+
+
+def test_cluster_collision_conserves_momentum():
+    """Two jittered 3x3x3 clusters meet off-centre (oblique contacts, friction 0.4, e = 0.7,
+    rotation): total momentum is unchanged to round-off."""
+    rng = np.random.default_rng(7)
+    g = np.arange(3) * 2.05 * R
+    block = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    pos = np.vstack([block, block + [5.7 * R, 1.0 * R, 1.0 * R]])      # closest centres 2.12 R apart
+    pos += rng.uniform(-0.02 * R, 0.02 * R, size=pos.shape)
+    n = len(pos)
+    s = ParticleState.create(n, max_cnts=12, max_walls=1)
+    s.x[:] = pos
+    s.u[:27, 0], s.u[27:, 0] = 0.8, -0.8
+    s.u[:] += rng.uniform(-0.05, 0.05, size=(n, 3))
+    s.rad[:] = R * rng.uniform(0.95, 1.0, size=n)
+    s.rho[:], s.E[:], s.nu[:] = RHO, E, NU
+    s.G[:] = E / (2.0 * (1.0 + NU))
+    s.set_sphere_mass()
+    p0 = (s.m[:, None] * s.u).sum(0)
+    scale = (s.m[:, None] * np.abs(s.u)).sum()
+    contacts = 0
+    for _ in range(160):
+        _run(s, 0.7, 0.4, 25, quirks=0)
+        contacts = max(contacts, int(s.tng_count.sum()))
+    assert contacts >= 10                                        # the clusters collided
+    assert np.abs(s.omega).max() > 0                             # oblique contacts spun them
+    p1 = (s.m[:, None] * s.u).sum(0)
+    assert np.abs(p1 - p0).max() <= 1e-12 * scale, np.abs(p1 - p0).max() / scale
+
+
+def _bonded_pair():
+    s = ParticleState.create(2, max_cnts=1, max_walls=1)
+    s.x[1, 0] = 1.0
+    s.rad[:], s.rho[:], s.E[:], s.G[:], s.nu[:] = 0.5, 2000.0, 1e4, 1e3, 0.25
+    s.set_sphere_mass()
+    b = BondState.create(2, 4)
+    O.setup_bonds(b, s, 3.0, 2.0)
+    assert b.count.tolist() == [1, 1] and b.idx[:, 0].tolist() == [1, 0]
+    return s, b
+
+
+def test_bond_at_rest_length_exerts_no_force():
+    """Two bonded spheres at rest (setupBonds sets the rest length to the current distance),
+    the reference's bond law with its history indexed by bond slot (DEM_BQ10 clear): zero force
+    and torque, and no motion, however many steps."""
+    s, b = _bonded_pair()
+    x0 = s.x.copy()
+    prm = dict(quirks=O.BOND_REF_COMPAT & ~0x01, beta=0.1, radius_factor=1.0)
+    assert O.bonded_run(s, b, prm, 1e-4, 1000, pow_mode=O.POW_SQRT) == 0
+    assert np.array_equal(s.x, x0)
+    assert not s.force.any() and not s.torque.any() and not s.u.any() and not s.omega.any()
+
+
+def test_reference_bond_indexing_pulls_a_bond_at_rest():
+    """src/CabanaBondedDEM_Force.hpp:207 reads the rest length as bond_init_len(i, j), with the
+    partner's id j in place of the bond's slot.  Particle 0's bond (partner 1) is in slot 0,
+    so it reads slot 1, an empty rest length of 0, and is pulled towards particle 1 by
+    k_n * rij.  Particle 1's partner 0 is its slot 0, so it reads its own rest length and feels
+    nothing.  The oracle reproduces this with DEM_BQ10 set."""
+    s, b = _bonded_pair()
+    assert O.bonded_run(s, b, dict(quirks=O.BOND_REF_COMPAT, beta=0.1, radius_factor=1.0), 1e-4, 1,
+                        pow_mode=O.POW_SQRT) == 0
+    r = 0.5
+    k_n = 1e4 * np.pi * r ** 2 / (2 * r)               # E A / (r_i + r_j), BondedDEM_Force.hpp:194
+    assert s.force[0, 0] > 0.9 * k_n and s.force[1, 0] == 0.0
