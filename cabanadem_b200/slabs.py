@@ -21,7 +21,10 @@ further than that margin allows.  Slabs are at least `halo` wide, so ghosts come
 neighbouring slabs only.
 
 Exchanges are point-to-point (`batch_isend_irecv`: counts, then rows) between neighbouring
-ranks only.  They are float64 tensors on `device`: the CPU for gloo, the rank's GPU for NCCL.
+ranks only.  They are float64 tensors on `device`: the CPU for gloo, the rank's GPU for NCCL
+(set it with torch.cuda.set_device first).  Every step starts with an all-reduce on all
+ranks, so the group's first collective involves every rank, as NCCL requires before
+point-to-point batches.
 A particle's row carries its global id, every per-particle field of the reference's Particles
 (src/CabanaDEM_Particles.hpp:349-370) and its history with partners as global ids.
 
