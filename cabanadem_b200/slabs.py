@@ -209,7 +209,8 @@ class SlabDecomposition:
         self._agree(err)
         x0 = st.x[owned, self.axis].copy()
         try:
-            step_fn(st)
+            if owned.any():      # a rank with an empty slab (or ghosts only) has nothing to step
+                step_fn(st)
         except DemError as e:
             err = "slab step: " + str(e)
         if not err and self.world > 1 and st.n:

@@ -80,7 +80,10 @@ class _HostApi:
 
     class Particles:
         def __init__(self, n, max_cnts, max_walls, ctx=None):
+            from cabanadem_b200._lib import DemError
             from cabanadem_b200.state import ParticleState
+            if n <= 0:       # dem_particles_create: n > 0
+                raise DemError("dem_particles_create: n > 0")
             self.mw = max_walls
             self.st = ParticleState.create(n, max_cnts, max(max_walls, 1))
 
@@ -124,7 +127,7 @@ class _HostApi:
             pass
 
 
-def _rank(rank, world, port, out, halo, piston, glue=False):
+def _rank(rank, world, port, out, halo, piston, glue=False, hi=SIDE):
     import sys
     sys.path.insert(0, ROOT)
     import torch.distributed as dist
@@ -134,7 +137,7 @@ def _rank(rank, world, port, out, halo, piston, glue=False):
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         s, w, prm = _gas(piston=piston)
-        dec = SlabDecomposition(0, LO, SIDE, halo, s.max_cnts, 6)
+        dec = SlabDecomposition(0, LO, hi, halo, s.max_cnts, 6)
         dec.scatter(s)
         if glue:
             from cabanadem_b200.slabs import DeviceStep
@@ -159,12 +162,12 @@ def _rank(rank, world, port, out, halo, piston, glue=False):
         dist.destroy_process_group()
 
 
-def _spawn(world, halo=HALO, piston=0.0, glue=False):
+def _spawn(world, halo=HALO, piston=0.0, glue=False, hi=SIDE):
     ctx = mp.get_context("spawn")
     mgr = ctx.Manager()
     out = mgr.dict()
     port = _free_port()
-    procs = [ctx.Process(target=_rank, args=(r, world, port, out, halo, piston, glue)) for r in range(world)]
+    procs = [ctx.Process(target=_rank, args=(r, world, port, out, halo, piston, glue, hi)) for r in range(world)]
     # one OpenMP thread per rank, set before the children start: the runtime reads it when
     # it is first loaded, which happens while the child imports torch
     old = os.environ.get("OMP_NUM_THREADS")
@@ -225,11 +228,23 @@ def test_thin_halo_fails_on_every_rank():
     assert any("moved more than" in out[r][1] for r in range(2))
 
 
-def test_device_step_glue_with_host_stand_in():
+@pytest.mark.parametrize("world,hi", [(2, SIDE), (3, 2 * SIDE + 1e-3)], ids=["2", "3_empty_slab"])
+def test_device_step_glue_with_host_stand_in(world, hi):
     """DeviceStep's upload / step / download / wall-carry logic, the device calls replaced by
-    the host stand-in: 2 slabs with the piston wall stay bit-identical to the oracle run."""
-    out = _spawn(2, piston=0.5, glue=True)
-    assert all(out[r][0] == "ok" for r in range(2)), out
+    the host stand-in: slabs with the piston wall stay bit-identical to the oracle run (with
+    3 ranks the third slab is empty and never creates a particle set)."""
+    out = _spawn(world, piston=0.5, glue=True, hi=hi)
+    assert all(out[r][0] == "ok" for r in range(world)), out
     got, ref = out[0][4], _reference(0.5)
     for f in ("x", "u", "omega", "force", "torque", "tng_count", "tng_sw_y", "tng_sw_z"):
+        assert np.array_equal(getattr(got, f), getattr(ref, f)), f
+
+
+def test_empty_slab():
+    """Slabs over [-1 mm, 41 mm] with 3 ranks: the third slab (27-41 mm) holds no particle
+    and skips its steps; the result is still the single-domain run's."""
+    out = _spawn(3, hi=2 * SIDE + 1e-3)
+    assert all(out[r][0] == "ok" for r in range(3)), out
+    got, ref = out[0][4], _reference()
+    for f in ("x", "u", "omega", "force", "torque", "tng_count"):
         assert np.array_equal(getattr(got, f), getattr(ref, f)), f
