@@ -214,7 +214,10 @@ def run_reference(args):
             "warmup": args.warmup, "impl": "reference", "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "hcp_box_%d: %d polydisperse spheres r~U[0.8,1.2] mm, jittered HCP, 6 walls, "
-                                   "gravity, dt 5e-8 s" % (n, n)},
+                                   "gravity, dt 5e-8 s, skin 0.1 r_mean" % (n, n),
+                       "precision": "fp64", "parallelism": "single",
+                       "algorithm": "the reference's CPU path: neighbour list rebuilt every step with cutoff "
+                                    "3 r_max (the skin is not used)"},
             "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
