@@ -1,15 +1,19 @@
 """Analytic known-answer checks of the oracle's physics, independent of the reference's data
 files.  An elastic head-on impact (e = 1, mu = 0) gives back the kinetic energy it started
 with and swaps the velocities.  A damped one separates at e times the approach speed (the
-damping law of src/CabanaDEM_Force.hpp:206-215).  Colliding clusters with friction and damping
+damping law of src/CabanaDEM_Force.hpp:206-215).  A sphere resting on a floor settles at
+the Hertz static overlap, and one sliding without spin ends up rolling at 5/7 of its initial
+speed (the wall's Mindlin spring and Coulomb limit, Force.hpp:448-678); with the tangential
+damping switched on (DEM_Q2 clear) the reference's wall law speeds a sliding sphere up
+instead.  Colliding clusters with friction and damping
 keep their total momentum: with every reference quirk cleared, each pair's forces are equal and
 opposite.  A bond at its rest length exerts no force.  The device FP64 path is bit-identical to
 the oracle, so these hold for it too."""
 import numpy as np
 import pytest
 
-from cabanadem_b200.scenarios import _force_params
-from cabanadem_b200.state import BondState, ParticleState
+from cabanadem_b200.scenarios import Q2_ETA_T_ZERO, _force_params
+from cabanadem_b200.state import BondState, ParticleState, WallState
 from oracle import oracle as O
 
 R, RHO, E, NU = 0.01, 2600.0, 70e9, 0.25
@@ -54,6 +58,69 @@ def test_damped_head_on_impact_separates_at_e_times_approach(cor):
     _run(s, cor, 0.0, 800)
     assert s.x[1, 0] - s.x[0, 0] > 2 * R
     assert abs((s.u[1, 0] - s.u[0, 0]) / 1.0 - cor) <= 0.02 * cor
+
+
+def _floor():
+    w = WallState.create(1)
+    w.normal[0, 2] = 1.0
+    w.E[:], w.nu[:], w.G[:] = E, NU, E / (2.0 * (1.0 + NU))
+    return w
+
+
+def _ball(z, vx=0.0):
+    s = ParticleState.create(1, max_cnts=6, max_walls=1)
+    s.x[0, 2], s.u[0, 0] = z, vx
+    s.rad[:], s.rho[:], s.E[:], s.nu[:] = R, RHO, E, NU
+    s.G[:] = E / (2.0 * (1.0 + NU))
+    s.set_sphere_mass()
+    return s
+
+
+def _hertz_rest_overlap(m, g=9.81):
+    """m g = 4/3 E* sqrt(R) delta^1.5 with 1/E* = (1 - nu_i^2)/E_i + (1 - nu_w^2)/E_w."""
+    e_star = 1.0 / (2.0 * (1.0 - NU * NU) / E)
+    return (m * g / (4.0 / 3.0 * e_star * np.sqrt(R))) ** (2.0 / 3.0)
+
+
+def test_sphere_on_floor_settles_at_hertz_overlap():
+    s = _ball(R)                                   # touching the floor, at rest
+    d_eq = _hertz_rest_overlap(s.m[0])
+    prm = _force_params(0.5, 0.5, 0.3, 0.3)
+    assert O.run(s, _floor(), prm, 1e-6, 20000, skin=0.1 * R, gravity=(0.0, 0.0, -9.81), pow_mode=O.POW_SQRT) == 0
+    assert abs((R - s.x[0, 2]) / d_eq - 1.0) < 1e-3, (R - s.x[0, 2]) / d_eq
+    assert abs(s.u[0, 2]) < 1e-6
+
+
+def test_sliding_sphere_rolls_at_five_sevenths():
+    """Launched along the floor at 1 m/s without spin (friction 0.5; every quirk clear but
+    DEM_Q2, see the next test): it slides, friction spins it up, and it rolls on at 5/7 m/s.
+    The reference's contact-point velocity is u + a (omega x n) with n from the contact
+    towards the centre, and its torque a (n x f_t) (src/CabanaDEM_Force.hpp:520-527, :661-663;
+    the pair law likewise, :114-139): its omega is the physical angular velocity negated,
+    consistently, so rolling reads v = -omega_y R."""
+    s0 = _ball(R)
+    s = _ball(R - _hertz_rest_overlap(s0.m[0]), vx=1.0)
+    prm = _force_params(0.5, 0.5, 0.5, 0.5, Q2_ETA_T_ZERO)
+    assert O.run(s, _floor(), prm, 1e-6, 100000, skin=0.1 * R, gravity=(0.0, 0.0, -9.81), pow_mode=O.POW_SQRT) == 0
+    v, w = s.u[0, 0], s.omega[0, 1]
+    assert abs(v / (5.0 / 7.0) - 1.0) < 0.01, v
+    assert abs(v + w * R) < 0.01 * v, (v, w * R)
+
+
+def test_wall_friction_with_tangential_damping_adds_energy():
+    """src/CabanaDEM_Force.hpp:640-643 adds eta_t v_t to the wall's tangential force after the
+    Coulomb limit ("Add damping to the limited force").  The reference's eta_t is zero
+    (sqrt(5/6) in integer arithmetic, :618, DEM_Q2), so the line has no effect there.  With
+    DEM_Q2 clear, eta_t > 0 and the term pushes along the sliding direction: the sliding
+    sphere of the previous test speeds up, 1 -> 54 m/s in 300 steps, instead of slowing
+    down at mu g.  The pair law applies its limited force as is (:297-301)."""
+    s0 = _ball(R)
+    grow, keep = (_ball(R - _hertz_rest_overlap(s0.m[0]), vx=1.0) for _ in range(2))
+    for s, q in ((grow, 0), (keep, Q2_ETA_T_ZERO)):
+        assert O.run(s, _floor(), _force_params(0.5, 0.5, 0.5, 0.5, q), 1e-6, 300, skin=0.1 * R,
+                     gravity=(0.0, 0.0, -9.81), pow_mode=O.POW_SQRT) == 0
+    assert grow.u[0, 0] > 10.0
+    assert abs(keep.u[0, 0] - (1.0 - 0.5 * 9.81 * 300e-6)) < 1e-3
 
 
 def test_cluster_collision_conserves_momentum():
