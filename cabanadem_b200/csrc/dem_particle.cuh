@@ -518,6 +518,11 @@ __device__ __forceinline__ void pw_wall(const unsigned q, const D4 &pi, const do
             *swx = (double)(-ft0 / kt);
             *swy = (double)(-ft1 / kt);
             *swz = (double)(-ft2 / kt);
+            if (!(q & DEM_Q2_ETA_T_ZERO)) {   // as the FP64 branch: the limited force acts
+                ft0 = __fmul_rn(fms, ti0);
+                ft1 = __fmul_rn(fms, ti1);
+                ft2 = __fmul_rn(fms, ti2);
+            }
         }
         cf[0] = (double)(fn0 + ft0);
         cf[1] = (double)(fn1 + ft1);
@@ -583,6 +588,14 @@ __device__ __forceinline__ void pw_wall(const unsigned q, const D4 &pi, const do
             *swx = -ft0 / kt;
             *swy = -ft1 / kt;
             *swz = -ft2 / kt;
+            if (!(q & DEM_Q2_ETA_T_ZERO)) {
+                // with eta_t live (Q2 clear) the limited force is what acts; the damping is
+                // added back (Force.hpp:640-643) only to reset the spring above.  The reference
+                // applies the sum, which pushes a sliding contact along its sliding direction.
+                ft0 = fms * ti0;
+                ft1 = fms * ti1;
+                ft2 = fms * ti2;
+            }
         }
         cf[0] = fn0 + ft0;
         cf[1] = fn1 + ft1;

@@ -41,10 +41,10 @@ extern "C" {
 /* ---- reference behaviours (bit set = reproduce the reference) ------------------ */
 #define DEM_Q1_VELJ_USES_UI  0x01u /* src/CabanaDEM_Force.hpp:133-137                    */
 #define DEM_Q2_ETA_T_ZERO    0x02u /* src/CabanaDEM_Force.hpp:224, :618.  Clear: eta_t > 0,
-                                    * which also brings in the wall law's re-added damping
-                                    * after the Coulomb limit (:640-643), a push along the
-                                    * sliding direction: a sliding wall contact gains energy.
-                                    * Keep it set for wall friction.                         */
+                                    * and the wall law applies its Coulomb-limited force (the
+                                    * reference adds eta_t v_t back to it, :640-643, harmless
+                                    * only with its eta_t = 0); the damping then only resets
+                                    * the spring, as the reference's reset does.            */
 #define DEM_Q3_NO_PP_TORQUE  0x04u /* src/CabanaDEM_Force.hpp:324-326                    */
 #define DEM_Q4_UNIT_HISTORY  0x08u /* src/CabanaDEM_Force.hpp:310-319                    */
 #define DEM_Q5_WALL_FT_TYPO  0x10u /* src/CabanaDEM_Force.hpp:624                        */

@@ -104,6 +104,14 @@ void plane_contact(orc_particles *p, int i, double nij_x, double nij_y, double n
         *swx = -ft_x / kt;
         *swy = -ft_y / kt;
         *swz = -ft_z / kt;
+        if (!(q & ORC_Q2_ETA_T_ZERO)) {
+            // with eta_t live (Q2 clear) the limited force is what acts; the damping is added
+            // back (:640-643) only to reset the spring above.  The reference applies the sum,
+            // which pushes a sliding contact along its sliding direction (eta_t = 0 there).
+            ft_x = ft_magn_star * ti_x;
+            ft_y = ft_magn_star * ti_y;
+            ft_z = ft_magn_star * ti_z;
+        }
     }
     p->force[3 * i + 0] += fn_x + ft_x;
     p->force[3 * i + 1] += fn_y + ft_y;

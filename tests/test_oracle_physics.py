@@ -3,9 +3,8 @@ files.  An elastic head-on impact (e = 1, mu = 0) gives back the kinetic energy 
 with and swaps the velocities.  A damped one separates at e times the approach speed (the
 damping law of src/CabanaDEM_Force.hpp:206-215).  A sphere resting on a floor settles at
 the Hertz static overlap, and one sliding without spin ends up rolling at 5/7 of its initial
-speed (the wall's Mindlin spring and Coulomb limit, Force.hpp:448-678); with the tangential
-damping switched on (DEM_Q2 clear) the reference's wall law speeds a sliding sphere up
-instead.  Colliding clusters with friction and damping
+speed (the wall's Mindlin spring and Coulomb limit, Force.hpp:448-678), with the tangential
+damping off (the reference) or on (DEM_Q2 clear).  Colliding clusters with friction and damping
 keep their total momentum: with every reference quirk cleared, each pair's forces are equal and
 opposite.  A bond at its rest length exerts no force.  The device FP64 path is bit-identical to
 the oracle, so these hold for it too."""
@@ -91,36 +90,35 @@ def test_sphere_on_floor_settles_at_hertz_overlap():
     assert abs(s.u[0, 2]) < 1e-6
 
 
-def test_sliding_sphere_rolls_at_five_sevenths():
-    """Launched along the floor at 1 m/s without spin (friction 0.5; every quirk clear but
-    DEM_Q2, see the next test): it slides, friction spins it up, and it rolls on at 5/7 m/s.
+@pytest.mark.parametrize("quirks", [0, Q2_ETA_T_ZERO], ids=["all_clear", "Q2_set"])
+def test_sliding_sphere_rolls_at_five_sevenths(quirks):
+    """Launched along the floor at 1 m/s without spin (friction 0.5, tangential damping on or
+    off): it slides, friction spins it up, and it rolls on at 5/7 m/s.
     The reference's contact-point velocity is u + a (omega x n) with n from the contact
     towards the centre, and its torque a (n x f_t) (src/CabanaDEM_Force.hpp:520-527, :661-663;
     the pair law likewise, :114-139): its omega is the physical angular velocity negated,
     consistently, so rolling reads v = -omega_y R."""
     s0 = _ball(R)
     s = _ball(R - _hertz_rest_overlap(s0.m[0]), vx=1.0)
-    prm = _force_params(0.5, 0.5, 0.5, 0.5, Q2_ETA_T_ZERO)
+    prm = _force_params(0.5, 0.5, 0.5, 0.5, quirks)
     assert O.run(s, _floor(), prm, 1e-6, 100000, skin=0.1 * R, gravity=(0.0, 0.0, -9.81), pow_mode=O.POW_SQRT) == 0
     v, w = s.u[0, 0], s.omega[0, 1]
     assert abs(v / (5.0 / 7.0) - 1.0) < 0.01, v
     assert abs(v + w * R) < 0.01 * v, (v, w * R)
 
 
-def test_wall_friction_with_tangential_damping_adds_energy():
-    """src/CabanaDEM_Force.hpp:640-643 adds eta_t v_t to the wall's tangential force after the
-    Coulomb limit ("Add damping to the limited force").  The reference's eta_t is zero
-    (sqrt(5/6) in integer arithmetic, :618, DEM_Q2), so the line has no effect there.  With
-    DEM_Q2 clear, eta_t > 0 and the term pushes along the sliding direction: the sliding
-    sphere of the previous test speeds up, 1 -> 54 m/s in 300 steps, instead of slowing
-    down at mu g.  The pair law applies its limited force as is (:297-301)."""
-    s0 = _ball(R)
-    grow, keep = (_ball(R - _hertz_rest_overlap(s0.m[0]), vx=1.0) for _ in range(2))
-    for s, q in ((grow, 0), (keep, Q2_ETA_T_ZERO)):
-        assert O.run(s, _floor(), _force_params(0.5, 0.5, 0.5, 0.5, q), 1e-6, 300, skin=0.1 * R,
-                     gravity=(0.0, 0.0, -9.81), pow_mode=O.POW_SQRT) == 0
-    assert grow.u[0, 0] > 10.0
-    assert abs(keep.u[0, 0] - (1.0 - 0.5 * 9.81 * 300e-6)) < 1e-3
+@pytest.mark.parametrize("quirks", [0, Q2_ETA_T_ZERO], ids=["all_clear", "Q2_set"])
+def test_sliding_sphere_slows_at_mu_g(quirks):
+    """A sphere sliding along the floor decelerates at mu g (plus the small rolling-resistance
+    share of the spin-up), with the tangential damping off (DEM_Q2 set, the reference) and on
+    (DEM_Q2 clear).  The reference adds eta_t v_t back to the limited wall force
+    (src/CabanaDEM_Force.hpp:640-643); with its eta_t = 0 that changes nothing, but with
+    eta_t > 0 it would push along the sliding direction (1 -> 54 m/s in 300 steps).  With
+    DEM_Q2 clear the limited force acts and the damping only resets the spring."""
+    s = _ball(R - _hertz_rest_overlap(_ball(R).m[0]), vx=1.0)
+    assert O.run(s, _floor(), _force_params(0.5, 0.5, 0.5, 0.5, quirks), 1e-6, 300, skin=0.1 * R,
+                 gravity=(0.0, 0.0, -9.81), pow_mode=O.POW_SQRT) == 0
+    assert abs(s.u[0, 0] - (1.0 - 0.5 * 9.81 * 300e-6)) < 1e-3, s.u[0, 0]
 
 
 def test_cluster_collision_conserves_momentum():
