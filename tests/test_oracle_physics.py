@@ -38,12 +38,12 @@ def _run(s, cor, mu, nsteps, quirks=None, dt=1e-6):
 def test_elastic_head_on_impact_conserves_energy():
     """The kinetic energy after an e = 1 impact equals the energy before, up to velocity
     Verlet's error, which shrinks at least 3x each time dt halves (6e-5 at 1 us, 9e-7 at 0.25 us
-    for this 240 us contact)."""
+    for this contact of about 60 us)."""
     err = []
     for dt in (1e-6, 5e-7, 2.5e-7):
         s = _pair()
         ke0 = O.kinetic_energy(s)
-        _run(s, 1.0, 0.0, int(round(600e-6 / dt)), dt=dt)
+        _run(s, 1.0, 0.0, int(round(600e-6 / dt)), dt=dt)     # closes, touches, separates
         assert s.tng_count.sum() == 0 and s.x[1, 0] - s.x[0, 0] > 2 * R   # separated
         err.append(abs(O.kinetic_energy(s) - ke0) / ke0)
         assert abs(s.u[0, 0] + 0.5) <= 1e-4 and abs(s.u[1, 0] - 0.5) <= 1e-4     # velocities swapped
@@ -119,6 +119,25 @@ def test_sliding_sphere_slows_at_mu_g(quirks):
     assert O.run(s, _floor(), _force_params(0.5, 0.5, 0.5, 0.5, quirks), 1e-6, 300, skin=0.1 * R,
                  gravity=(0.0, 0.0, -9.81), pow_mode=O.POW_SQRT) == 0
     assert abs(s.u[0, 0] - (1.0 - 0.5 * 9.81 * 300e-6)) < 1e-3, s.u[0, 0]
+
+
+def test_sliding_pair_contact_is_at_the_coulomb_limit():
+    """Two spheres closing at 0.5 m/s while grazing at 2 m/s (e = 1, friction 0.3, every quirk
+    clear but DEM_Q2): the contact slides throughout, and at every step of it the tangential
+    force is mu times the normal force in the contact frame (the limit of
+    src/CabanaDEM_Force.hpp:290-301).  With damping (e < 1) the normal force turns tensile near
+    the end of the contact, so the friction impulse then exceeds mu times the normal impulse."""
+    s = _pair(v=0.25)
+    s.u[0, 1], s.u[1, 1] = 1.0, -1.0
+    ratio = []
+    for _ in range(300):
+        _run(s, 1.0, 0.3, 1, quirks=Q2_ETA_T_ZERO)
+        if s.tng_count[0]:
+            n = (s.x[0] - s.x[1]) / np.linalg.norm(s.x[0] - s.x[1])
+            fn = s.force[0] @ n
+            ratio.append(np.linalg.norm(s.force[0] - fn * n) / fn)
+    assert len(ratio) >= 50 and s.tng_count[0] == 0
+    assert np.abs(np.array(ratio) - 0.3).max() < 1e-12
 
 
 def test_cluster_collision_conserves_momentum():
