@@ -265,3 +265,29 @@ def test_checkpoint_restart_continues_bitwise(tmp_path):
     sa, sb = a.particles.download(), b.particles.download()
     for f in ("x", "u", "omega", "force", "torque", "tng_idx", "tng_count", "tng_ss_x", "tng_sw_y"):
         assert np.array_equal(getattr(sa, f), getattr(sb, f)), f
+
+
+@pytest.mark.parametrize("quirks", [0, S.REF_COMPAT], ids=["all_clear", "ref"])
+def test_sliding_sphere_on_floor(quirks):
+    """A glass sphere launched along a floor at 1 m/s without spin: wall friction through the
+    sliding phase into rolling, with the tangential damping on (every quirk clear: the wall law
+    applies its Coulomb-limited force) and off (the reference), bit for bit with the oracle."""
+    from cabanadem_b200.state import ParticleState, WallState
+    r, rho, E, nu = 0.01, 2600.0, 70e9, 0.25
+    s = ParticleState.create(1, max_cnts=6, max_walls=1)
+    s.rad[:], s.rho[:], s.E[:], s.nu[:] = r, rho, E, nu
+    s.G[:] = E / (2.0 * (1.0 + nu))
+    s.set_sphere_mass()
+    s.x[0, 2] = r - (s.m[0] * 9.81 / (4.0 / 3.0 * E / (2.0 * (1.0 - nu * nu)) * np.sqrt(r))) ** (2.0 / 3.0)
+    s.u[0, 0] = 1.0
+    w = WallState.create(1)
+    w.normal[0, 2] = 1.0
+    w.E[:], w.nu[:], w.G[:] = E, nu, s.G[0]
+    sc = S.Scenario("sliding_sphere", s, w, S._force_params(0.5, 0.5, 0.5, 0.5, quirks), 1e-6, 3000,
+                    skin=0.1 * r, gravity=(0.0, 0.0, -9.81))
+    ref = s.copy()
+    assert O.run(ref, w.copy(), sc.params, sc.dt, 3000, skin=sc.skin, gravity=sc.gravity, pow_mode=O.POW_SQRT) == 0
+    g = api.from_scenario(sc)
+    g.run_steps(3000)
+    _assert_bitwise(g.particles.download(), ref, where="sliding%d" % quirks)
+    assert ref.u[0, 0] < 1.0 - 0.5 * 9.81 * 2e-3        # slowing down by friction
