@@ -31,6 +31,7 @@ a bounded sample of the same workload.
 from __future__ import annotations
 
 import argparse
+import atexit
 import json
 import os
 import statistics
@@ -111,20 +112,21 @@ class ClockSampler:
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device):
+    def __init__(self, device, cmd=None):
         self.device = device
         self.proc = None
         self.path = os.path.join("/tmp", "bench_clocks_%d_%d.csv" % (os.getpid(), device))
+        self.cmd = cmd or ["nvidia-smi", "-i", str(device), "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                           "-lms", "20"]
 
     def start(self):
         try:
             self.f = open(self.path, "w")
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
-                                          "--format=csv,noheader,nounits", "-lms", "20"],
-                                         stdout=self.f, stderr=subprocess.DEVNULL)
+            self.proc = subprocess.Popen(self.cmd, stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
             return
+        atexit.register(self._end)   # a timed region that raises leaves no sampler behind
         # nvidia-smi takes a while to start: the timed region begins once it samples, so that
         # even a sub-second timed region is covered
         t0 = time.time()
@@ -133,6 +135,17 @@ class ClockSampler:
                 break
             time.sleep(0.01)
         self.skip = sum(1 for _ in open(self.path))   # samples taken before the timed region
+
+    def _end(self):
+        if self.proc and self.proc.poll() is None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if os.path.exists(self.path):
+            self.f.close()
+            os.unlink(self.path)
 
     def stop(self):
         if not self.proc:
