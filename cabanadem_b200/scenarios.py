@@ -417,8 +417,11 @@ def random_box(n=4096, radius=1e-3, side=0.05, seed=1, vmax=0.1, max_cnts=16, qu
     pos = np.zeros((n, 3))
     cell = 2.0 * radius
     grid = {}
-    k = 0
+    k = tries = 0
     while k < n:
+        tries += 1
+        if tries > 200 * n:
+            raise ValueError("random_box: cannot place %d spheres of r = %g in a cube of side %g" % (n, radius, side))
         p = rng.uniform(radius, side - radius, size=3)
         c = tuple((p // cell).astype(int))
         ok = True
