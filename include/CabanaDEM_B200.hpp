@@ -29,6 +29,7 @@
 #include <cctype>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <filesystem>
 #include <fstream>
 #include <functional>
@@ -326,6 +327,8 @@ class Particles {
         ctx_->check(dem_particles_create(ctx_->handle(), n_, MaxCnts, MaxNoWalls, &h_), "dem_particles_create");
         // Particles.hpp:53-61: the output folder is created if it does not exist
         if (!out_.empty()) std::filesystem::create_directories(out_);
+        // snapshot format for programs that do not call setOutputFormat (the example drivers)
+        if (const char *fmt = std::getenv("CABANADEM_OUTPUT_FORMAT")) setOutputFormat(fmt);
     }
     ~Particles() { dem_particles_destroy(h_); }
     Particles(const Particles &) = delete;
@@ -380,7 +383,8 @@ class Particles {
         for (auto &kv : mi_) kv.second->fresh = false;
     }
 
-    // Snapshot format of output(): "csv" (the default), "xdmf" or "both".
+    // Snapshot format of output(): "csv" (the default), "xdmf" or "both".  The environment
+    // variable CABANADEM_OUTPUT_FORMAT sets it for every particle set a program creates.
     void setOutputFormat(const std::string &format) {
         if (format != "csv" && format != "xdmf" && format != "both")
             throw Error("setOutputFormat: csv, xdmf or both");
