@@ -1,5 +1,6 @@
-"""Particle snapshots written by the C++ interface's Particles::output (particles_<k>.csv, or
-particles_<k>.xmf with its particles_<k>.bin).
+"""Particle snapshots as the C++ interface's Particles::output writes them (particles_<k>.csv,
+or particles_<k>.xmf with its particles_<k>.bin): readers, and writers of the same files for
+Python callers (a ParticleState, e.g. from api.Particles.download()).
 
 The reference writes particles_<k>.h5 through Cabana's HDF5 writer with one dataset per
 slice label and a Time attribute (src/CabanaDEM_Particles.hpp:299-326); no HDF5 library is
@@ -77,3 +78,54 @@ def read_xdmf(path: str) -> dict:
     if missing:
         raise ValueError("%s: missing datasets %s" % (path, missing))
     return out
+
+
+# dataset name (the reference's slice label) -> ParticleState field
+_FIELDS = (("positions", "x"), ("velocities", "u"), ("omega", "omega"), ("forces", "force"), ("mass", "m"),
+           ("density", "rho"), ("radius", "rad"), ("total_no_tangential_contacts", "tng_count"))
+
+
+def write_csv(folder: str, step: int, time: float, state) -> str:
+    """particles_<step>.csv of a ParticleState, byte for byte as Particles::output writes it
+    (every double with 17 significant digits, so read() gives back the same bits)."""
+    path = os.path.join(folder, "particles_%d.csv" % step)
+    cols = [getattr(state, f) for _, f in _FIELDS]
+    with open(path, "w") as fh:
+        fh.write("# time %.17g\n" % time)
+        fh.write("id," + ",".join("%s_%d" % (n, d) for n in _VEC for d in range(3)) + "," + ",".join(_SCALAR) + "\n")
+        for i in range(state.n):
+            vals = [("%.17g" % v) for c in cols[:4] for v in c[i]] + [("%.17g" % c[i]) for c in cols[4:7]]
+            fh.write("%d,%s,%d\n" % (i, ",".join(vals), int(cols[7][i])))
+    return path
+
+
+def write_xdmf(folder: str, step: int, time: float, state) -> str:
+    """particles_<step>.xmf and .bin of a ParticleState, byte for byte as the C++ interface's
+    writeXdmfSnapshot writes them; returns the .xmf path."""
+    stem = "particles_%d" % step
+    n, seek, at = state.n, [], 0
+    with open(os.path.join(folder, stem + ".bin"), "wb") as fb:
+        for name, f in _FIELDS:
+            a = np.ascontiguousarray(getattr(state, f), dtype="<i4" if name == _SCALAR[-1] else "<f8")
+            seek.append(at)
+            fb.write(a.tobytes())
+            at += a.nbytes
+    lines = ['<?xml version="1.0" ?>', '<!DOCTYPE Xdmf SYSTEM "Xdmf.dtd" []>', '<Xdmf Version="2.0">',
+             '  <Domain>', '    <Grid Name="particles" GridType="Uniform">', '      <Time Value="%.17g"/>' % time,
+             '      <Topology TopologyType="Polyvertex" NumberOfElements="%d" NodesPerElement="1"/>' % n]
+
+    def item(k, name):
+        vec, is_int = name in _VEC, name == _SCALAR[-1]
+        return ('        <DataItem Dimensions="%d%s" NumberType="%s" Precision="%d" Format="Binary" Endian="Little" '
+                'Seek="%d">%s.bin</DataItem>' % (n, " 3" if vec else "", "Int" if is_int else "Float",
+                                                 4 if is_int else 8, seek[k], stem))
+    lines += ['      <Geometry GeometryType="XYZ">', item(0, "positions"), '      </Geometry>']
+    for k, (name, _) in enumerate(_FIELDS[1:], start=1):
+        lines += ['      <Attribute Name="%s" AttributeType="%s" Center="Node">' % (name, "Vector" if name in _VEC
+                                                                                       else "Scalar"),
+                  item(k, name), '      </Attribute>']
+    lines += ['    </Grid>', '  </Domain>', '</Xdmf>']
+    path = os.path.join(folder, stem + ".xmf")
+    with open(path, "w") as fh:
+        fh.write("\n".join(lines) + "\n")
+    return path

@@ -136,6 +136,38 @@ def test_xdmf_snapshot_round_trip(tmp_path):
     assert os.path.getsize(tmp_path / "particles_12.bin") == n * (4 * 3 * 8 + 3 * 8 + 4)
 
 
+def test_python_writers_match_the_cpp_interface(tmp_path):
+    """snapshots.write_xdmf writes the same bytes as the C++ writeXdmfSnapshot for the same
+    data; snapshots.write_csv round-trips through read() bit for bit."""
+    from cabanadem_b200.state import ParticleState
+    src = tmp_path / "xdmf.cpp"
+    src.write_text(_XDMF_PROG)
+    exe = tmp_path / "xdmf"
+    subprocess.run(["g++", "-O1", "-std=c++17", "-I" + os.path.join(ROOT, "include"), str(src), "-o", str(exe)],
+                   check=True)
+    (tmp_path / "cpp").mkdir()
+    (tmp_path / "py").mkdir()
+    subprocess.run([str(exe), str(tmp_path / "cpp"), "5"], check=True)
+    n = 5
+    st = ParticleState.create(n, max_cnts=1, max_walls=1)
+    for i in range(n):
+        for d in range(3):
+            st.x[i, d] = 0.1 * i + d + 1.0 / 3.0
+            st.u[i, d] = -2.5 * i + d
+            st.omega[i, d] = 1e-300 * (i + 1) * (d + 1)
+            st.force[i, d] = 1e9 / (i + d + 1)
+        st.m[i], st.rho[i], st.rad[i], st.tng_count[i] = 0.5 + i, 2500.0, 1e-3 * (i + 1), i % 3
+    snapshots.write_xdmf(str(tmp_path / "py"), 5, 0.1 + 0.2, st)
+    for ext in (".xmf", ".bin"):
+        assert (tmp_path / "py" / ("particles_5" + ext)).read_bytes() == \
+            (tmp_path / "cpp" / ("particles_5" + ext)).read_bytes(), ext
+    got = snapshots.read(snapshots.write_csv(str(tmp_path / "py"), 5, 0.1 + 0.2, st))
+    assert got["time"] == 0.1 + 0.2
+    for name, f in (("positions", "x"), ("velocities", "u"), ("omega", "omega"), ("forces", "force"),
+                    ("mass", "m"), ("density", "rho"), ("radius", "rad"), ("total_no_tangential_contacts", "tng_count")):
+        assert np.array_equal(got[name], getattr(st, f)), name
+
+
 _PHASE_PROG = r"""
 #include "CabanaDEM_B200.hpp"
 struct mem {};
