@@ -226,6 +226,27 @@ class SlabDecomposition:
             self.step(step_fn)
 
     # ---- results
+    def kinetic_energy(self) -> float:
+        """Total translational + rotational kinetic energy of the scene (collective: every rank
+        calls it and gets the same value), summed per rank over its own particles in global-id
+        order, then over the ranks in rank order.  The rank sums are gathered rather than
+        all-reduced so that every rank adds them in the same order."""
+        gid = self._col(self.rows, "gid")[:, 0]
+        rows = self.rows[np.argsort(gid, kind="stable")]
+        u, w = self._col(rows, "u"), self._col(rows, "omega")
+        m, inertia = self._col(rows, "m")[:, 0], self._col(rows, "I")[:, 0]
+        e = 0.0
+        for k in range(len(rows)):
+            e += 0.5 * m[k] * (u[k, 0] * u[k, 0] + u[k, 1] * u[k, 1] + u[k, 2] * u[k, 2]) + \
+                0.5 * inertia[k] * (w[k, 0] * w[k, 0] + w[k, 1] * w[k, 1] + w[k, 2] * w[k, 2])
+        mine = torch.tensor([e], dtype=torch.float64, device=self.device)
+        parts = [torch.zeros(1, dtype=torch.float64, device=self.device) for _ in range(self.world)]
+        dist.all_gather(parts, mine, group=self.group)
+        total = 0.0
+        for p in parts:
+            total += float(p.item())
+        return total
+
     def gather(self) -> ParticleState | None:
         """The global state on rank 0 (particles in global-id order, history partners as global
         ids), None on the other ranks."""

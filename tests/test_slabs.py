@@ -156,8 +156,9 @@ def _rank(rank, world, port, out, halo, piston, glue=False, hi=SIDE):
         except DemError as e:
             out[rank] = ("error", str(e))
             return
+        ke = dec.kinetic_energy()
         g = dec.gather()
-        out[rank] = ("ok", dec.migrated, cross, ghosts, g)
+        out[rank] = ("ok", dec.migrated, cross, ghosts, g, ke)
     finally:
         dist.destroy_process_group()
 
@@ -206,6 +207,10 @@ def test_slab_decomposition_is_bitwise_single_domain(world, piston):
     ref = _reference(piston)
     for f in ("x", "u", "omega", "force", "torque", "tng_count"):
         assert np.array_equal(getattr(got, f), getattr(ref, f)), f
+    from oracle import oracle as O
+    ke = O.kinetic_energy(ref)
+    assert len({out[r][5] for r in range(world)}) == 1                  # every rank has the same total
+    assert abs(out[0][5] - ke) <= 1e-12 * ke
     live = np.arange(ref.max_cnts)[None, :] < ref.tng_count[:, None]
     assert live.sum() > 100                       # a contact-rich run
     for f in ("tng_idx", "tng_ss_x", "tng_ss_y", "tng_ss_z"):
