@@ -140,6 +140,51 @@ def test_sliding_pair_contact_is_at_the_coulomb_limit():
     assert np.abs(np.array(ratio) - 0.3).max() < 1e-12
 
 
+def _elastic_energy(s, w):
+    """Hertz elastic energy 2/5 k_n delta^(5/2) of every particle-particle and particle-wall
+    overlap (k_n = 4/3 E* sqrt(R*), Force.hpp:196-203 and :561-568)."""
+    e = 0.0
+    for i in range(s.n):
+        for j in range(i + 1, s.n):
+            d = s.rad[i] + s.rad[j] - np.linalg.norm(s.x[i] - s.x[j])
+            if d > 0:
+                es = 1.0 / ((1 - s.nu[i] ** 2) / s.E[i] + (1 - s.nu[j] ** 2) / s.E[j])
+                rs = 1.0 / (1.0 / s.rad[i] + 1.0 / s.rad[j])
+                e += 0.4 * (4.0 / 3.0 * es * np.sqrt(rs)) * d ** 2.5
+        for k in range(w.n):
+            d = s.rad[i] - (s.x[i] - w.x[k]) @ w.normal[k]
+            if d > 0:
+                es = 1.0 / ((1 - s.nu[i] ** 2) / s.E[i] + (1 - w.nu[k] ** 2) / w.E[k])
+                e += 0.4 * (4.0 / 3.0 * es * np.sqrt(s.rad[i])) * d ** 2.5
+    return e
+
+
+def test_elastic_gas_conserves_energy_with_the_reference_bits():
+    """60 spheres bouncing in a walled box for 25 ms with the reference's bits (e = 1, mu = 0):
+    kinetic plus Hertz elastic energy stays constant to velocity Verlet's error (1e-5) through
+    their collisions with each other and the walls."""
+    from cabanadem_b200.scenarios import _box_walls
+    rng = np.random.default_rng(3)
+    g = (np.arange(4) + 0.5) * 2.6 * R
+    pos = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)[:60]
+    s = ParticleState.create(60, max_cnts=12, max_walls=6)
+    s.x[:] = pos + rng.uniform(-0.1 * R, 0.1 * R, size=pos.shape)
+    s.u[:] = rng.uniform(-1.0, 1.0, size=pos.shape)
+    s.rad[:], s.rho[:], s.E[:], s.nu[:] = R, RHO, E, NU
+    s.G[:] = E / (2.0 * (1.0 + NU))
+    s.set_sphere_mass()
+    w = _box_walls((0.0, 0.0, 0.0), (10.4 * R,) * 3, E, NU, float(s.G[0]))
+    e0 = O.kinetic_energy(s) + _elastic_energy(s, w)
+    in_contact = 0
+    for _ in range(200):                      # 25 ms
+        assert O.run(s, w, _force_params(1.0, 1.0, 0.0, 0.0), 2.5e-7, 500, skin=0.1 * R, pow_mode=O.POW_SQRT) == 0
+        ke = O.kinetic_energy(s)
+        e = ke + _elastic_energy(s, w)
+        in_contact += int(ke < (1.0 - 1e-4) * e)          # energy stored in some contact
+        assert abs(e - e0) <= 1e-5 * e0, (e - e0) / e0
+    assert in_contact >= 5
+
+
 def test_cluster_collision_conserves_momentum():
     """Two jittered 3x3x3 clusters meet off-centre (oblique contacts, friction 0.4, e = 0.7,
     rotation): total momentum is unchanged to round-off."""
