@@ -185,6 +185,30 @@ def test_elastic_gas_conserves_energy_with_the_reference_bits():
     assert in_contact >= 5
 
 
+@pytest.mark.parametrize("quirks,stands", [(0x3F, False), (0x3F & ~0x04, True)], ids=["reference", "Q3_clear"])
+def test_three_sphere_pyramid(quirks, stands):
+    """Two spheres on a floor with a third on top (friction 0.5, statically stable in physics:
+    it needs mu > tan 15 deg).  With the pair contact's torque (DEM_Q3 clear) it settles and
+    stands.  The reference's pair contacts add no torque (src/CabanaDEM_Force.hpp:324-326): the
+    floor's friction turns the base spheres and nothing at the top contact resists it, so
+    they roll apart."""
+    d_eq = _hertz_rest_overlap(_ball(R).m[0])
+    s = ParticleState.create(3, max_cnts=6, max_walls=1)
+    s.x[0] = [-R + 0.5e-6, 0.0, R - d_eq]
+    s.x[1] = [R - 0.5e-6, 0.0, R - d_eq]
+    s.x[2] = [0.0, 0.0, R - d_eq + np.sqrt(3.0) * R]
+    s.rad[:], s.rho[:], s.E[:], s.nu[:] = R, RHO, E, NU
+    s.G[:] = E / (2.0 * (1.0 + NU))
+    s.set_sphere_mass()
+    assert O.run(s, _floor(), _force_params(0.5, 0.5, 0.5, 0.5, quirks), 1e-6, 20000, skin=0.1 * R,
+                 gravity=(0.0, 0.0, -9.81), pow_mode=O.POW_SQRT) == 0
+    spread = s.x[1, 0] - s.x[0, 0] - 2.0 * R
+    if stands:
+        assert spread < 5e-5 and np.abs(s.u).max() < 1e-4, (spread, np.abs(s.u).max())
+    else:
+        assert spread > 2e-4 and np.abs(s.u).max() > 5e-3, (spread, np.abs(s.u).max())
+
+
 def test_cluster_collision_conserves_momentum():
     """Two jittered 3x3x3 clusters meet off-centre (oblique contacts, friction 0.4, e = 0.7,
     rotation): total momentum is unchanged to round-off."""
