@@ -77,12 +77,15 @@ def tune(sc, precision=0, warmup=20, steps=200, use_cache=True, ctx=None):
     best = dict(DEFAULTS)
     best_t = time_config(sc, best, precision, warmup, steps, ctx)
     trials = [(dict(best), best_t)]
+    tried = {tuple(sorted(best.items()))}
     for name in ("stream_block", "steps_per_launch", "skin_factor"):
         for v in CANDIDATES[name]:
-            if v == best[name]:
-                continue
             cfg = dict(best)
             cfg[name] = v
+            key_cfg = tuple(sorted(cfg.items()))
+            if key_cfg in tried:      # the current best, or timed before the best moved
+                continue
+            tried.add(key_cfg)
             t = time_config(sc, cfg, precision, warmup, steps, ctx)
             trials.append((cfg, t))
             if t < best_t:
