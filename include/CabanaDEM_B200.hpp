@@ -158,15 +158,77 @@ class JsonValue {
         }
         return v;
     }
+    // a JSON string at s[i] ('"' ... '"'), escapes decoded (\uXXXX as UTF-8, surrogate pairs
+    // joined); i ends past the closing quote
     static std::string string(const std::string &s, size_t &i) {
-        if (s[i] != '"') throw Error("json: expected string");
+        if (i >= s.size() || s[i] != '"') throw Error("json: expected string");
         std::string out;
-        for (++i; i < s.size() && s[i] != '"'; ++i) {
-            if (s[i] == '\\' && i + 1 < s.size()) ++i;
-            out += s[i];
+        for (++i;; ++i) {
+            if (i >= s.size()) throw Error("json: unterminated string");
+            const char c = s[i];
+            if (c == '"') break;
+            if (c != '\\') {
+                out += c;
+                continue;
+            }
+            if (++i >= s.size()) throw Error("json: unterminated string");
+            switch (s[i]) {
+                case '"': out += '"'; break;
+                case '\\': out += '\\'; break;
+                case '/': out += '/'; break;
+                case 'b': out += '\b'; break;
+                case 'f': out += '\f'; break;
+                case 'n': out += '\n'; break;
+                case 'r': out += '\r'; break;
+                case 't': out += '\t'; break;
+                case 'u': {
+                    unsigned cp = hex4(s, i + 1);
+                    i += 4;
+                    if (cp >= 0xD800 && cp < 0xDC00 && i + 6 < s.size() && s[i + 1] == '\\' && s[i + 2] == 'u') {
+                        const unsigned lo = hex4(s, i + 3);
+                        if (lo >= 0xDC00 && lo < 0xE000) {
+                            cp = 0x10000 + ((cp - 0xD800) << 10) + (lo - 0xDC00);
+                            i += 6;
+                        }
+                    }
+                    utf8(out, cp);
+                    break;
+                }
+                default: throw Error("json: bad escape");
+            }
         }
         ++i;
         return out;
+    }
+    static unsigned hex4(const std::string &s, size_t at) {
+        if (at + 4 > s.size()) throw Error("json: short \\u escape");
+        unsigned v = 0;
+        for (size_t k = at; k < at + 4; ++k) {
+            const char c = s[k];
+            v <<= 4;
+            if (c >= '0' && c <= '9') v |= unsigned(c - '0');
+            else if (c >= 'a' && c <= 'f') v |= unsigned(c - 'a' + 10);
+            else if (c >= 'A' && c <= 'F') v |= unsigned(c - 'A' + 10);
+            else throw Error("json: bad \\u escape");
+        }
+        return v;
+    }
+    static void utf8(std::string &out, unsigned cp) {
+        if (cp < 0x80) {
+            out += char(cp);
+        } else if (cp < 0x800) {
+            out += char(0xC0 | (cp >> 6));
+            out += char(0x80 | (cp & 0x3F));
+        } else if (cp < 0x10000) {
+            out += char(0xE0 | (cp >> 12));
+            out += char(0x80 | ((cp >> 6) & 0x3F));
+            out += char(0x80 | (cp & 0x3F));
+        } else {
+            out += char(0xF0 | (cp >> 18));
+            out += char(0x80 | ((cp >> 12) & 0x3F));
+            out += char(0x80 | ((cp >> 6) & 0x3F));
+            out += char(0x80 | (cp & 0x3F));
+        }
     }
 };
 

@@ -168,6 +168,72 @@ def test_python_writers_match_the_cpp_interface(tmp_path):
         assert np.array_equal(got[name], getattr(st, f)), name
 
 
+_JSON_PROG = r"""
+#include "CabanaDEM_B200.hpp"
+#include <cstdio>
+static void dump(const CabanaDEM::JsonValue &v, const std::string &path) {
+    using K = CabanaDEM::JsonValue;
+    switch (v.kind) {
+        case K::Object: for (const auto &kv : v.obj) dump(kv.second, path + "/" + kv.first); break;
+        case K::Array: for (size_t k = 0; k < v.arr.size(); ++k) dump(v.arr[k], path + "/" + std::to_string(k)); break;
+        case K::Number: std::printf("%s N %.17g\n", path.c_str(), v.num); break;
+        case K::String: std::printf("%s S ", path.c_str()); for (unsigned char c : v.str) std::printf("%02x", c);
+                        std::printf("\n"); break;
+        case K::Bool: std::printf("%s B %d\n", path.c_str(), int(v.num)); break;
+        case K::Null: std::printf("%s Z\n", path.c_str()); break;
+    }
+}
+int main(int argc, char **argv) {
+    std::ifstream f(argv[1]);
+    std::stringstream ss;
+    ss << f.rdbuf();
+    dump(CabanaDEM::JsonValue::parse(ss.str()), "");
+    CabanaDEM::Inputs in(argv[1]);
+    std::printf("num_steps %d\n", int(in["num_steps"]));
+    return 0;
+}
+"""
+
+
+def _flatten(v, path=""):
+    if isinstance(v, dict):
+        return [x for k in sorted(v) for x in _flatten(v[k], path + "/" + k)]
+    if isinstance(v, list):
+        return [x for k, e in enumerate(v) for x in _flatten(e, path + "/" + str(k))]
+    if isinstance(v, bool):
+        return ["%s B %d" % (path, v)]
+    if v is None:
+        return ["%s Z" % path]
+    if isinstance(v, str):
+        return ["%s S %s" % (path, v.encode("utf-8").hex())]
+    return ["%s N %s" % (path, "%.17g" % float(v))]
+
+
+def test_json_reader_matches_python(tmp_path):
+    """The C++ interface's JSON reader (Inputs; the reference uses nlohmann::json,
+    Input.hpp:58-62) gives every value of the seven example inputs and of a file with escapes,
+    exponents, nesting and literals as Python's json does; num_steps = int(final_time /
+    timestep) truncates as Input.hpp:50-54 (0.3 / 0.1 -> 2)."""
+    src = tmp_path / "json.cpp"
+    src.write_text(_JSON_PROG)
+    exe = tmp_path / "json"
+    subprocess.run(["g++", "-O1", "-std=c++17", "-I" + os.path.join(ROOT, "include"), str(src), "-o", str(exe)],
+                   check=True)
+    tricky = ('{ "final_time": {"value": 0.3}, "timestep" :{"value":1e-1},\n'
+              ' "a": {"value": -1.5E-3, "units": "m\\/s\\u00b2 \\"x\\" \\ud83d\\ude00\\n\\t\\\\"},\n'
+              ' "arr": [1, 2.5, [true, false, null], {}, "\\u0041"], "big": 12345678901234567890}')
+    cases = dict(_raw_inputs())
+    cases["tricky"] = None
+    for name, raw in cases.items():
+        f = tmp_path / ("%s.json" % name)
+        f.write_text(tricky if raw is None else json.dumps(raw, indent=2))
+        data = json.loads(f.read_text())
+        out = subprocess.run([str(exe), str(f)], check=True, capture_output=True, text=True).stdout.splitlines()
+        assert out[:-1] == _flatten(data), name
+        assert out[-1] == "num_steps %d" % int(float(data["final_time"]["value"]) / float(data["timestep"]["value"]))
+    assert out[-1] == "num_steps 2"
+
+
 _PHASE_PROG = r"""
 #include "CabanaDEM_B200.hpp"
 struct mem {};
