@@ -304,6 +304,29 @@ class HostSlice {
 };
 
 // ---------------------------------------------------------------------------------------
+// CSV snapshot: <folder>/particles_<step>.csv, a "# time <t>" line, a header of the reference's
+// slice labels with a component suffix and one row per particle, every double with 17
+// significant digits (so it reads back bit for bit).  Vectors are [n][3] row-major.
+// ---------------------------------------------------------------------------------------
+inline void writeCsvSnapshot(const std::string &folder, int step, double time, int n, const double *x,
+                             const double *u, const double *w, const double *f, const double *m,
+                             const double *rho, const double *r, const int *tc) {
+    const std::string path = folder + "/particles_" + std::to_string(step) + ".csv";
+    std::FILE *fo = std::fopen(path.c_str(), "w");
+    if (!fo) throw Error("cannot write " + path);
+    std::fprintf(fo, "# time %.17g\n", time);
+    std::fprintf(fo, "id,positions_0,positions_1,positions_2,velocities_0,velocities_1,velocities_2,"
+                     "omega_0,omega_1,omega_2,forces_0,forces_1,forces_2,mass,density,radius,"
+                     "total_no_tangential_contacts\n");
+    for (int i = 0; i < n; ++i)
+        std::fprintf(fo, "%d,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,"
+                         "%.17g,%.17g,%.17g,%d\n",
+                     i, x[3 * i], x[3 * i + 1], x[3 * i + 2], u[3 * i], u[3 * i + 1], u[3 * i + 2], w[3 * i],
+                     w[3 * i + 1], w[3 * i + 2], f[3 * i], f[3 * i + 1], f[3 * i + 2], m[i], rho[i], r[i], tc[i]);
+    std::fclose(fo);
+}
+
+// ---------------------------------------------------------------------------------------
 // XDMF snapshot.  The reference's writer (Cabana's HDF5 particle output, called at
 // Particles.hpp:306-326) stores one dataset per slice label in particles_<k>.h5 with the
 // step's time; viewers open it through an XDMF index.  No HDF5 library is in this image, so
@@ -485,20 +508,8 @@ class Particles {
         auto rho = sliceDensity();
         auto r = sliceRadius();
         auto tc = sliceTotalNoTangentialContacts();
-        const std::string path = out_ + "/particles_" + std::to_string(output_step) + ".csv";
-        std::FILE *fo = std::fopen(path.c_str(), "w");
-        if (!fo) throw Error("cannot write " + path);
-        std::fprintf(fo, "# time %.17g\n", output_time);
-        std::fprintf(fo, "id,positions_0,positions_1,positions_2,velocities_0,velocities_1,velocities_2,"
-                         "omega_0,omega_1,omega_2,forces_0,forces_1,forces_2,mass,density,radius,"
-                         "total_no_tangential_contacts\n");
-        for (int i = 0; i < n_; ++i)
-            std::fprintf(fo, "%d,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,"
-                             "%.17g,%.17g,%.17g,%d\n",
-                         i, x.get(i, 0), x.get(i, 1), x.get(i, 2), u.get(i, 0), u.get(i, 1), u.get(i, 2),
-                         w.get(i, 0), w.get(i, 1), w.get(i, 2), f.get(i, 0), f.get(i, 1), f.get(i, 2), m.get(i),
-                         rho.get(i), r.get(i), tc.get(i));
-        std::fclose(fo);
+        writeCsvSnapshot(out_, output_step, output_time, n_, x.data(), u.data(), w.data(), f.data(), m.data(),
+                         rho.data(), r.data(), tc.data());
     }
     const std::string &output_folder() const { return out_; }
 

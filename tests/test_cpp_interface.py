@@ -97,6 +97,8 @@ int main(int argc, char **argv) {
         {{"positions", x.data(), 3, false}, {"velocities", u.data(), 3, false}, {"omega", w.data(), 3, false},
          {"forces", f.data(), 3, false}, {"mass", m.data(), 1, false}, {"density", rho.data(), 1, false},
          {"radius", r.data(), 1, false}, {"total_no_tangential_contacts", tc.data(), 1, true}});
+    CabanaDEM::writeCsvSnapshot(argv[1], std::atoi(argv[2]), 0.1 + 0.2, n, x.data(), u.data(), w.data(), f.data(),
+                                m.data(), rho.data(), r.data(), tc.data());
     return 0;
 }
 """
@@ -137,8 +139,9 @@ def test_xdmf_snapshot_round_trip(tmp_path):
 
 
 def test_python_writers_match_the_cpp_interface(tmp_path):
-    """snapshots.write_xdmf writes the same bytes as the C++ writeXdmfSnapshot for the same
-    data; snapshots.write_csv round-trips through read() bit for bit."""
+    """snapshots.write_xdmf and write_csv write the same bytes as the C++ interface's
+    writeXdmfSnapshot and writeCsvSnapshot (what Particles::output calls) for the same data, and
+    the CSV reads back bit for bit."""
     from cabanadem_b200.state import ParticleState
     src = tmp_path / "xdmf.cpp"
     src.write_text(_XDMF_PROG)
@@ -161,7 +164,9 @@ def test_python_writers_match_the_cpp_interface(tmp_path):
     for ext in (".xmf", ".bin"):
         assert (tmp_path / "py" / ("particles_5" + ext)).read_bytes() == \
             (tmp_path / "cpp" / ("particles_5" + ext)).read_bytes(), ext
-    got = snapshots.read(snapshots.write_csv(str(tmp_path / "py"), 5, 0.1 + 0.2, st))
+    csv = snapshots.write_csv(str(tmp_path / "py"), 5, 0.1 + 0.2, st)
+    assert open(csv, "rb").read() == (tmp_path / "cpp" / "particles_5.csv").read_bytes()
+    got = snapshots.read(csv)
     assert got["time"] == 0.1 + 0.2
     for name, f in (("positions", "x"), ("velocities", "u"), ("omega", "omega"), ("forces", "force"),
                     ("mass", "m"), ("density", "rho"), ("radius", "rad"), ("total_no_tangential_contacts", "tng_count")):
