@@ -209,6 +209,37 @@ def test_three_sphere_pyramid(quirks, stands):
         assert spread > 2e-4 and np.abs(s.u).max() > 5e-3, (spread, np.abs(s.u).max())
 
 
+@pytest.mark.parametrize("uz", [-0.6, 0.6], ids=["opposite_signs", "same_signs"])
+def test_reference_wall_friction_depends_on_direction(uz):
+    """src/CabanaDEM_Force.hpp:624 takes |f_t| as sqrt(f_x^2 + f_y^2 + f_z f_y) (DEM_Q5).  A
+    sphere pressed on a wall with normal +x and sliding with (v_y, v_z) = (0.3, -0.6) has
+    f_z f_y < -f_y^2: the square root is NaN, `ft_magn > 1e-12` is false, the direction stays
+    zero and no friction acts at all (the velocity is unchanged; nothing becomes NaN).  Sliding
+    with (0.3, 0.6) the wrong magnitude is sqrt(3) f_y instead of sqrt(5) f_y, the direction
+    vector is sqrt(5/3) long, and friction acts 1.29 times too strongly.  With the bit clear it
+    slows the sphere at mu g in both directions."""
+    from cabanadem_b200.scenarios import Q5_WALL_FT_TYPO, REF_COMPAT
+    w = WallState.create(1)
+    w.normal[0, 0] = 1.0
+    w.E[:], w.nu[:], w.G[:] = E, NU, E / (2.0 * (1.0 + NU))
+    got = {}
+    for q in (REF_COMPAT, REF_COMPAT & ~Q5_WALL_FT_TYPO):
+        s = _ball(R)
+        s.x[0] = [R - _hertz_rest_overlap(s.m[0]), 0.0, 0.0]
+        s.u[0] = [0.0, 0.3, uz]
+        assert O.run(s, w, _force_params(0.5, 0.5, 0.5, 0.5, q), 1e-6, 200, skin=0.1 * R,
+                     gravity=(-9.81, 0.0, 0.0), pow_mode=O.POW_SQRT) == 0
+        assert np.isfinite(s.u).all() and np.isfinite(s.force).all()
+        got[q] = np.hypot(s.u[0, 1], s.u[0, 2])
+    v0, slowed = np.hypot(0.3, uz), np.hypot(0.3, uz) - 0.5 * 9.81 * 200e-6
+    assert abs(got[REF_COMPAT & ~Q5_WALL_FT_TYPO] - slowed) < 2e-5
+    if uz < 0:
+        assert abs(got[REF_COMPAT] - v0) < 1e-12
+    else:
+        ratio = (v0 - got[REF_COMPAT]) / (v0 - got[REF_COMPAT & ~Q5_WALL_FT_TYPO])
+        assert abs(ratio - np.sqrt(5.0 / 3.0)) < 0.01, ratio
+
+
 def test_cluster_collision_conserves_momentum():
     """Two jittered 3x3x3 clusters meet off-centre (oblique contacts, friction 0.4, e = 0.7,
     rotation): total momentum is unchanged to round-off."""
