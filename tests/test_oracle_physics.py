@@ -240,6 +240,26 @@ def test_reference_wall_friction_depends_on_direction(uz):
         assert abs(ratio - np.sqrt(5.0 / 3.0)) < 0.01, ratio
 
 
+def test_reference_pair_friction_ignores_sliding_across_y_and_z():
+    """src/CabanaDEM_Force.hpp:133-137 builds the partner's contact velocity in y and z from
+    particle i's own velocity (DEM_Q1).  For two spheres colliding along x while sliding past
+    each other along y, the relative sliding velocity is then lost, and friction takes almost
+    nothing off the sliding speed.  The 0.002 m/s that does go comes from the contact normal
+    tilting as they pass.  With the bit clear the sliding speed drops by mu times the normal
+    speed change, as in the Coulomb test above."""
+    from cabanadem_b200.scenarios import Q1_VELJ_USES_UI, REF_COMPAT
+    drop = {}
+    for q in (REF_COMPAT, REF_COMPAT & ~Q1_VELJ_USES_UI):
+        s = _pair(v=0.25)
+        s.u[0, 1], s.u[1, 1] = 1.0, -1.0
+        _run(s, 1.0, 0.3, 300, quirks=q)
+        # sliding speed lost by sphere 0, normal speed change of sphere 1 (-0.25 -> about +0.24)
+        drop[q] = (1.0 - s.u[0, 1], s.u[1, 0] + 0.25)
+    (ref_t, _), (fix_t, fix_n) = drop[REF_COMPAT], drop[REF_COMPAT & ~Q1_VELJ_USES_UI]
+    assert ref_t < 0.01 and ref_t < 0.1 * fix_t
+    assert abs(fix_t / fix_n - 0.3) < 0.03
+
+
 def test_cluster_collision_conserves_momentum():
     """Two jittered 3x3x3 clusters meet off-centre (oblique contacts, friction 0.4, e = 0.7,
     rotation): total momentum is unchanged to round-off."""
