@@ -25,6 +25,7 @@ createSolverDEM / SolverDEM::run           :func:`createSolverDEM`, :meth:`Solve
 from __future__ import annotations
 
 import ctypes as C
+import os
 import weakref
 
 import numpy as np
@@ -98,7 +99,11 @@ def default_context():
 
 
 class Particles:
-    def __init__(self, n: int, max_cnts: int = 6, max_walls: int = 1, ctx: Context | None = None):
+    output_folder = ""      # Particles(exec, n, output_folder) of the reference; "" writes nothing
+    output_format = None    # "csv", "xdmf" or "both"; None: $CABANADEM_OUTPUT_FORMAT, else "csv"
+
+    def __init__(self, n: int, max_cnts: int = 6, max_walls: int = 1, ctx: Context | None = None,
+                 output_folder: str = ""):
         self.ctx = ctx or default_context()
         self.n, self.max_cnts, self.max_walls = int(n), int(max_cnts), int(max_walls)
         h = C.c_void_p()
@@ -106,6 +111,47 @@ class Particles:
               self.ctx.h, "dem_particles_create")
         self.h = h
         self.ctx.adopt(self)
+        if output_folder:      # Particles.hpp:53-61: created if it does not exist
+            os.makedirs(output_folder, exist_ok=True)
+            self.output_folder = str(output_folder)
+
+    # ---- output and resize (Particles.hpp:273-346)
+    def setOutputFormat(self, fmt: str):
+        if fmt not in ("csv", "xdmf", "both"):
+            raise DemError("setOutputFormat: csv, xdmf or both")
+        self.output_format = fmt
+
+    def output(self, output_step: int, output_time: float):
+        """One snapshot of the current state in the output folder (Particles.hpp:299-346):
+        particles_<step>.csv and/or particles_<step>.xmf + .bin, as the C++ interface writes them."""
+        if not self.output_folder:
+            return
+        from . import snapshots
+        fmt = self.output_format or os.environ.get("CABANADEM_OUTPUT_FORMAT", "csv")
+        if fmt not in ("csv", "xdmf", "both"):
+            raise DemError("output format: csv, xdmf or both, got %r" % fmt)
+        st = self.download()
+        if fmt != "xdmf":
+            snapshots.write_csv(self.output_folder, int(output_step), float(output_time), st)
+        if fmt != "csv":
+            snapshots.write_xdmf(self.output_folder, int(output_step), float(output_time), st)
+
+    def resize(self, n: int):
+        """Particles::resize(n) (Particles.hpp:273-297): the first min(n, size) particles keep
+        their values, added ones start zeroed with empty contact slots.  The device set is
+        re-created, so no solver may use it (create solvers after the last resize); external
+        forces and fix flags are reset."""
+        for r in self.ctx._children:
+            o = r()
+            if o is not None and o is not self and getattr(o, "particles", None) is self and getattr(o, "h", None):
+                raise DemError("Particles.resize: a solver is attached to this particle set")
+        st = self.download().resized(int(n))
+        h = C.c_void_p()
+        check(lib().dem_particles_create(self.ctx.h, int(n), self.max_cnts, self.max_walls, C.byref(h)),
+              self.ctx.h, "dem_particles_create")
+        lib().dem_particles_destroy(self.h)
+        self.h, self.n = h, int(n)
+        self.upload(st)
 
     # ---- field access
     def set(self, field: str, arr):

@@ -67,6 +67,16 @@ class ParticleState:
             setattr(s, k, np.ascontiguousarray(v).copy())
         return s
 
+    def resized(self, n: int) -> "ParticleState":
+        """A copy with n particles (Particles::resize, src/CabanaDEM_Particles.hpp:273-297): the
+        first min(n, self.n) keep their values; added particles are zeroed, with empty contact
+        slots (tangential index -1)."""
+        out = ParticleState.create(n, self.max_cnts, self.tng_sw_x.shape[1])
+        k = min(n, self.n)
+        for name, a in self.arrays().items():
+            getattr(out, name)[:k] = a[:k]
+        return out
+
     def set_sphere_mass(self):
         """m = 4/3 pi r^3 rho and I = 2/5 m r^2, in the reference examples' order (e.g.
         examples/01_elastic_normal_impact_of_two_identical_particles.cpp:106-107)."""

@@ -80,3 +80,17 @@ def test_bonded_bar():
     left, right = st.x[:, 0] == st.x[:, 0].min(), st.x[:, 0] == st.x[:, 0].max()
     assert np.all(st.u[left, 0] == -0.05) and np.all(st.u[right, 0] == 0.05)
     assert np.all(case["fix_flags"][left | right] == 3)
+
+
+def test_state_resized():
+    """ParticleState.resized (the host half of Particles.resize, Particles.hpp:273-297): the
+    first particles keep every field, added ones are zeroed with empty contact slots."""
+    st = S.random_box(n=50).state
+    st.tng_idx[:5, 0], st.tng_count[:5] = 7, 1
+    grow, shrink = st.resized(80), st.resized(20)
+    for name, a in st.arrays().items():
+        assert np.array_equal(getattr(grow, name)[:50], a), name
+        assert np.array_equal(getattr(shrink, name), a[:20]), name
+    assert not grow.x[50:].any() and not grow.m[50:].any() and not grow.tng_count[50:].any()
+    assert np.all(grow.tng_idx[50:] == -1)
+    assert grow.n == 80 and shrink.n == 20 and grow.tng_sw_x.shape == (80, st.tng_sw_x.shape[1])
