@@ -15,6 +15,7 @@ ERR = {
     0x001: "DEM_ERR_INVALID", 0x002: "DEM_ERR_CUDA", 0x004: "DEM_ERR_CONTACT_OVERFLOW",
     0x008: "DEM_ERR_NEIGHBOR_OVERFLOW", 0x010: "DEM_ERR_NAN", 0x020: "DEM_ERR_TIMEOUT",
     0x040: "DEM_ERR_BOND_OVERFLOW", 0x080: "DEM_ERR_NOMEM", 0x100: "DEM_ERR_UNSUPPORTED",
+    0x200: "DEM_ERR_MESH_OVERFLOW",
 }
 DEM_ERR_CONTACT_OVERFLOW = 0x004
 DEM_ERR_TIMEOUT = 0x020
