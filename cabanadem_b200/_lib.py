@@ -149,6 +149,7 @@ _PROTOS = {
     "dem_surrogate_rollout": ([_VP, _VP, C.c_int, C.c_int, C.POINTER(RolloutStats)], C.c_int),
 }
 NOALLOC_MAX_PARTICLES = 32768
+NOALLOC_MAX_NEIGHBORS = 128
 
 
 def exported_symbols():

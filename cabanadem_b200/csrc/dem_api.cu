@@ -1724,22 +1724,27 @@ extern "C" int dem_checkpoint_load(dem_particles *p, const char *path) {
     if (std::fread(hdr, 4, 4, f) != 4) return bad("truncated header");
     if (hdr[0] != p->P.n || hdr[1] != p->P.mc || hdr[2] != p->P.mw)
         return bad("particle count, MaxCnts or MaxNoWalls differ from the particles object");
-    std::vector<unsigned char> buf;
-    for (int k = 0; k < hdr[3]; ++k) {
+    if (hdr[3] < 0 || hdr[3] > DEM_F_COUNT_) return bad("bad field count");
+    // read and check every field first, then apply them all: a truncated or mismatched file
+    // leaves the particles object as it was
+    struct Field {
         int fld;
-        long long bytes;
-        if (std::fread(&fld, 4, 1, f) != 1 || std::fread(&bytes, 8, 1, f) != 1) return bad("truncated field header");
         long count;
+        std::vector<unsigned char> data;
+    };
+    std::vector<Field> fields((size_t)hdr[3]);
+    for (Field &F : fields) {
+        long long bytes;
+        if (std::fread(&F.fld, 4, 1, f) != 1 || std::fread(&bytes, 8, 1, f) != 1) return bad("truncated field header");
         int es;
-        if (!field_layout(p, fld, &count, &es) || bytes != (long long)count * es) return bad("field size mismatch");
-        buf.resize((size_t)bytes);
-        if (std::fread(buf.data(), 1, buf.size(), f) != buf.size()) return bad("truncated field");
-        const int st = dem_particles_set(p, fld, buf.data(), count);
-        if (st) {
-            std::fclose(f);
-            return st;
-        }
+        if (!field_layout(p, F.fld, &F.count, &es) || bytes != (long long)F.count * es) return bad("field size mismatch");
+        F.data.resize((size_t)bytes);
+        if (std::fread(F.data.data(), 1, F.data.size(), f) != F.data.size()) return bad("truncated field");
     }
     std::fclose(f);
+    for (const Field &F : fields) {
+        const int st = dem_particles_set(p, F.fld, F.data.data(), F.count);
+        if (st) return st;
+    }
     return DEM_OK;
 }

@@ -431,7 +431,9 @@ __global__ void __launch_bounds__(128) k_list(Particles P, NbrList L, Ctl *ctl, 
                 }
             }
         }
-        const int keep = count < L.maxnb ? count : L.maxnb;
+        // at most kMaxCand candidates were kept, whatever the list capacity
+        const int lim = L.maxnb < kMaxCand ? L.maxnb : kMaxCand;
+        const int keep = count < lim ? count : lim;
         for (int k = 0; k < keep; ++k) L.idx[(long)k * cap + i] = cand[k];
         L.nn[i] = keep;
     }
@@ -443,7 +445,7 @@ __global__ void __launch_bounds__(128) k_list(Particles P, NbrList L, Ctl *ctl, 
     __syncthreads();
     if (threadIdx.x == 0) {
         atomicMax(&ctl->max_nbr, smax);
-        if (smax > L.maxnb) atomicOr(&ctl->status, DEM_ERR_NEIGHBOR_OVERFLOW);
+        if (smax > L.maxnb || smax > kMaxCand) atomicOr(&ctl->status, DEM_ERR_NEIGHBOR_OVERFLOW);
     }
 }
 

@@ -10,7 +10,9 @@
 // the caller passes inputs and outputs, and the scratch comes from the fixed array below.
 //
 // Limits and sharing rules:
-//  - at most DEM_NOALLOC_MAX_PARTICLES particles per call; larger inputs are rejected;
+//  - at most DEM_NOALLOC_MAX_PARTICLES particles per call and at most
+//    DEM_NOALLOC_MAX_NEIGHBORS list entries per particle (the list build keeps that many
+//    candidates per particle); larger values are rejected with DEM_ERR_INVALID;
 //  - every GPU that loads this library holds the array (about 2.4 MB) until the process
 //    exits, whether or not the function is called;
 //  - all calls on a device share the one array, which keeps the last call's contents; the
@@ -19,7 +21,9 @@
 //    issued;
 //  - the first call on a device looks up the array's device address with
 //    cudaGetSymbolAddress (with that device current) and caches it; make that first call
-//    before any stream capture begins.
+//    before any stream capture begins.  The cache is per process and is not refreshed: after
+//    a cudaDeviceReset on that device the cached address is stale, so a process that resets
+//    a device must not call this function on it again.
 #include <cstring>
 #include <mutex>
 
@@ -79,7 +83,7 @@ __global__ void k_pack(const double *x, const double *rad, int n, double4 *pos, 
 extern "C" int dem_neighbor_list_noalloc(const double *x, const double *rad, int n, double delta, double skin,
                                          int max_neighbors, int *nn, int *idx, void *stream) {
     if (!x || !rad || !nn || !idx || n <= 0 || max_neighbors <= 0) return DEM_ERR_INVALID;
-    if (n > DEM_NOALLOC_MAX_PARTICLES) return DEM_ERR_INVALID;
+    if (n > DEM_NOALLOC_MAX_PARTICLES || max_neighbors > DEM_NOALLOC_MAX_NEIGHBORS) return DEM_ERR_INVALID;
     if (!(delta > 0.0) && !(skin >= 0.0)) return DEM_ERR_INVALID;
     void *base = nullptr;
     int st = scratch_address(&base);

@@ -274,20 +274,25 @@ int dem_bonded_run(dem_bonds *b, int nsteps);
  *   nn[n], idx[max_neighbors][n]  device outputs: list length, partner indices in ascending
  *                                 order, slot-major (partner k of particle i at idx[k*n + i])
  *   stream                        cudaStream_t (NULL: default stream); synchronised on return
- * Returns DEM_ERR_INVALID when n > DEM_NOALLOC_MAX_PARTICLES and DEM_ERR_NEIGHBOR_OVERFLOW when
- * a particle has more than max_neighbors partners (its list is cut at max_neighbors), and
- * DEM_ERR_NAN when a position or radius is not finite (every list is then empty).
+ * Returns DEM_ERR_INVALID when n > DEM_NOALLOC_MAX_PARTICLES or max_neighbors >
+ * DEM_NOALLOC_MAX_NEIGHBORS, DEM_ERR_NEIGHBOR_OVERFLOW when a particle has more than
+ * max_neighbors partners (its list is cut at max_neighbors), and DEM_ERR_NAN when a position
+ * or radius is not finite (every list is then empty).
  * All calls share the scratch array and it keeps the last call's contents: calls that could
  * overlap on the GPU race and must be ordered by the caller.  The first call on a device looks
- * up the array's address (with that device current); make that call before any stream
- * capture. */
+ * up the array's address (with that device current) and keeps it for the life of the
+ * process; make that call before any stream capture, and do not call this function again on
+ * a device after a cudaDeviceReset of it (the kept address is then stale). */
 #define DEM_NOALLOC_MAX_PARTICLES 32768
+#define DEM_NOALLOC_MAX_NEIGHBORS 128
 int dem_neighbor_list_noalloc(const double *x, const double *rad, int n, double delta, double skin,
                               int max_neighbors, int *nn, int *idx, void *stream);
 
 /* Checkpoint of every particle field (caller order) to a file and back; the neighbour list
  * is rebuilt after a load, so a restarted run continues bit for bit.  The particles object
- * given to load must have the same n, MaxCnts and MaxNoWalls. */
+ * given to load must have the same n, MaxCnts and MaxNoWalls.  Load reads and checks the
+ * whole file before it changes anything: on DEM_ERR_INVALID (unreadable, truncated or
+ * mismatched file) the particles keep their previous state. */
 int dem_checkpoint_save(dem_particles *p, const char *path);
 int dem_checkpoint_load(dem_particles *p, const char *path);
 

@@ -96,7 +96,9 @@ def test_constants_and_struct_layouts_match_the_header(tmp_path):
     hdr_path = os.path.join(ROOT, "include", "b200dem.h")
     consts = {"DEM_F_" + k.upper(): v for k, v in _lib.F.items()}
     consts.update({"DEM_W_" + k.upper(): v for k, v in _lib.W.items()})
-    consts.update({"DEM_FP64": _lib.DEM_FP64, "DEM_MIXED": _lib.DEM_MIXED, "DEM_REF_COMPAT": S.REF_COMPAT})
+    consts.update({"DEM_FP64": _lib.DEM_FP64, "DEM_MIXED": _lib.DEM_MIXED, "DEM_REF_COMPAT": S.REF_COMPAT,
+                   "DEM_NOALLOC_MAX_PARTICLES": _lib.NOALLOC_MAX_PARTICLES,
+                   "DEM_NOALLOC_MAX_NEIGHBORS": _lib.NOALLOC_MAX_NEIGHBORS})
     consts.update({"DEM_" + k: getattr(S, k) for k in dir(S) if re.fullmatch(r"Q\d_[A-Z_]+", k)})
     errs = re.findall(r"#define\s+(DEM_ERR_[A-Z_]+)\s", open(hdr_path).read())
     consts.update({name: code for code, name in _lib.ERR.items()})

@@ -267,6 +267,25 @@ def test_checkpoint_restart_continues_bitwise(tmp_path):
         assert np.array_equal(getattr(sa, f), getattr(sb, f)), f
 
 
+def test_checkpoint_load_of_a_truncated_file_changes_nothing(tmp_path):
+    """A checkpoint cut short in its last field is refused with DEM_ERR_INVALID, and the
+    particles keep every field they had before the call."""
+    sc = S.random_box(n=512, seed=6)
+    a = api.from_scenario(sc)
+    a.run_steps(200)
+    path = tmp_path / "state.b200dem"
+    a.particles.save(path)
+    data = path.read_bytes()
+    path.write_bytes(data[:-16])
+    b = api.from_scenario(S.random_box(n=512, seed=6))
+    before = b.particles.download()
+    with pytest.raises(api.DemError):
+        b.particles.load(path)
+    after = b.particles.download()
+    for f in ("x", "u", "omega", "rad", "tng_idx", "tng_count", "tng_ss_x", "tng_sw_y"):
+        assert np.array_equal(getattr(before, f), getattr(after, f)), f
+
+
 @pytest.mark.parametrize("quirks", [0, S.REF_COMPAT], ids=["all_clear", "ref"])
 def test_sliding_sphere_on_floor(quirks):
     """A glass sphere launched along a floor at 1 m/s without spin: wall friction through the
