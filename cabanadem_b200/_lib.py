@@ -116,6 +116,7 @@ _PROTOS = {
     "dem_stage2": ([_VP], C.c_int),
     "dem_stage3": ([_VP], C.c_int),
     "dem_build_neighbors": ([_VP], C.c_int),
+    "dem_solver_rebuild": ([_VP], C.c_int),
     "dem_compute_force": ([_VP], C.c_int),
     "dem_neighbors_get": ([_VP, _VP, _VP, C.POINTER(C.c_long)], C.c_int),
     "dem_energy": ([_VP, C.POINTER(C.c_double)], C.c_int),
@@ -133,6 +134,7 @@ _PROTOS = {
                              _VP, _VP, _VP], C.c_int),
     "dem_nn_status": ([_VP, C.POINTER(C.c_int)], C.c_int),
     "dem_particles_get_device": ([_VP, C.c_int, _VP, C.c_long], C.c_int),
+    "dem_particles_clear_contacts": ([_VP], C.c_int),
     "dem_checkpoint_save": ([_VP, C.c_char_p], C.c_int),
     "dem_checkpoint_load": ([_VP, C.c_char_p], C.c_int),
     "dem_surrogate_create": ([_VP, C.POINTER(SurrogateParams), C.POINTER(_VP)], C.c_int),

@@ -191,6 +191,11 @@ class Particles:
         """Restore a checkpoint written by save() (same n, MaxCnts, MaxNoWalls)."""
         check(lib().dem_checkpoint_load(self.h, str(path).encode()), self.ctx.h, "dem_checkpoint_load")
 
+    def clear_contacts(self):
+        """Contact counts 0, slot partners -1, slot and wall history 0, on the device
+        (dem_particles_clear_contacts): a fresh start without uploading zero history."""
+        check(lib().dem_particles_clear_contacts(self.h), self.ctx.h, "dem_particles_clear_contacts")
+
     def upload(self, s: ParticleState):
         for f in ("rad", "x", "u", "omega", "force", "torque", "m", "I", "rho", "E", "nu", "G",
                   "tng_idx", "tng_ss_x", "tng_ss_y", "tng_ss_z", "tng_count"):
@@ -375,6 +380,11 @@ class SolverDEM:
 
     def build_neighbors(self):
         check(lib().dem_build_neighbors(self.h), self.particles.ctx.h, "dem_build_neighbors")
+
+    def rebuild(self):
+        """The time loop's rebuild, now: Morton re-sort, new list, displacement bound reset
+        (dem_solver_rebuild)."""
+        check(lib().dem_solver_rebuild(self.h), self.particles.ctx.h, "dem_solver_rebuild")
 
     def compute_force(self):
         return check(lib().dem_compute_force(self.h), self.particles.ctx.h, "dem_compute_force",

@@ -512,6 +512,27 @@ extern "C" int dem_particles_set(dem_particles *p, int field, const void *host, 
     return DEM_OK;
 }
 
+__global__ void k_clear_slots(Particles P) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += gridDim.x * blockDim.x)
+        for (int k = 0; k < P.mc; ++k) P.tidx[(long)k * P.cap + i] = -1;
+}
+
+extern "C" int dem_particles_clear_contacts(dem_particles *p) {
+    if (!p) return DEM_ERR_INVALID;
+    dem_ctx *ctx = p->ctx;
+    cudaStream_t s = ctx->stream;
+    Particles &P = p->P;
+    const size_t cn = (size_t)P.cap;
+    CK(cudaMemsetAsync(P.cstate, 0, sizeof(int) * cn, s));
+    CK(cudaMemsetAsync(P.th, 0, sizeof(double) * 3 * std::max(P.mc, 1) * cn, s));
+    CK(cudaMemsetAsync(P.sw, 0, sizeof(double) * 3 * std::max(P.mw, 1) * cn, s));
+    k_clear_slots<<<kGS, kTB, 0, s>>>(P);
+    CK(cudaGetLastError());
+    p->dirty = true;
+    k_invalidate<<<1, 32, 0, s>>>(p->ctl);
+    return DEM_OK;
+}
+
 static int particles_get_impl(dem_particles *p, int field, void *host, long count, bool device) {
     if (!p || !host) return DEM_ERR_INVALID;
     dem_ctx *ctx = p->ctx;
@@ -1345,6 +1366,14 @@ extern "C" int dem_build_neighbors(dem_solver *s) {
     int st = build_now(s, false);
     if (st) return st;
     return DEM_OK;
+}
+extern "C" int dem_solver_rebuild(dem_solver *s) {
+    if (!s) return DEM_ERR_INVALID;
+    if (s->p->mat_dirty || (s->p->P.ext != nullptr) != (s->fc.has_ext != 0)) {
+        int st = prepare(s);
+        if (st) return st;
+    }
+    return build_now(s, true);
 }
 extern "C" int dem_compute_force(dem_solver *s) {
     if (!s) return DEM_ERR_INVALID;

@@ -154,6 +154,12 @@ int dem_particles_get(dem_particles *p, int field, void *host, long count);
 /* As dem_particles_get into device memory `dev` (same layout and caller order), queued on
  * the context's stream without a host synchronisation. */
 int dem_particles_get_device(dem_particles *p, int field, void *dev, long count);
+/* Forget every contact: the tangential contact counts become 0, slot partners -1, slot and
+ * wall history 0 -- the values the reference's examples give every particle in their set-up
+ * functors (examples/01_elastic_normal_impact_of_two_identical_particles.cpp:125-130).
+ * Device-side, no host copy: a caller starting a new run from fresh positions and
+ * velocities sets those fields and calls this instead of uploading zero history arrays. */
+int dem_particles_clear_contacts(dem_particles *p);
 int dem_particles_size(dem_particles *p);
 
 /* ---- walls: Wall<Mem,3>(exec, n, out) (src/CabanaDEM_Wall.hpp:22-153) ------------- */
@@ -214,6 +220,13 @@ int dem_stage1(dem_solver *s);
 int dem_stage2(dem_solver *s);
 int dem_stage3(dem_solver *s);
 int dem_build_neighbors(dem_solver *s);
+/* The rebuild dem_solver_run performs when the displacement bound reaches skin/2, done now:
+ * storage re-sorted along the Morton curve (contact partners remapped), list rebuilt,
+ * displacement bound reset.  Results of later steps are unchanged bit for bit (sums run in
+ * caller order); for callers that want a rebuild at a point of their choice, e.g. after
+ * moving particles themselves.  No reference counterpart beyond neighbors->build
+ * (src/CabanaDEM_Solver.hpp:87-88), which this extends with the re-sort. */
+int dem_solver_rebuild(dem_solver *s);
 int dem_compute_force(dem_solver *s);
 
 /* Neighbour list of the last build in caller order, CSR: offsets[n+1], idx[total]

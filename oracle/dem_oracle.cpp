@@ -779,6 +779,40 @@ extern "C" double orc_kinetic_energy(const orc_particles *p) {
     return e;
 }
 
+// Hertz elastic energy (no reference counterpart: the reference has no reductions).  The
+// normal law fn = kn * overlap^1.5 with kn = 4/3 E_eff sqrt(R_eff) (Force.hpp:196-203 for a
+// pair, :561-566 for a wall) is the derivative of kn * 2/5 * overlap^2.5, summed over every
+// overlapping pair (each pair once, by brute force over all j > i, independent of any
+// neighbour list) and over every particle-wall overlap.  out[0]: pairs, out[1]: walls.
+extern "C" void orc_elastic_energy(const orc_particles *p, const orc_walls *w, double *out) {
+    double epp = 0.0, epw = 0.0;
+    for (int i = 0; i < p->n; ++i) {
+        const double *xi = p->x + 3 * i;
+        for (int j = i + 1; j < p->n; ++j) {
+            const double *xj = p->x + 3 * j;
+            const double dx = xi[0] - xj[0], dy = xi[1] - xj[1], dz = xi[2] - xj[2];
+            const double overlap = p->rad[i] + p->rad[j] - std::sqrt(dx * dx + dy * dy + dz * dz);
+            if (overlap <= 0.) continue;
+            const double E_eff = 1. / ((1. - p->nu[i] * p->nu[i]) / p->E[i] + (1. - p->nu[j] * p->nu[j]) / p->E[j]);
+            const double R_eff = 1. / (1. / p->rad[i] + 1. / p->rad[j]);
+            const double kn = 4. / 3. * E_eff * std::sqrt(R_eff);
+            epp += 0.4 * kn * overlap * overlap * std::sqrt(overlap);
+        }
+        if (!w) continue;
+        for (int k = 0; k < w->n; ++k) {
+            const double *wx = w->x + 3 * k, *wn = w->normal + 3 * k;
+            const double d = (xi[0] - wx[0]) * wn[0] + (xi[1] - wx[1]) * wn[1] + (xi[2] - wx[2]) * wn[2];
+            const double overlap = p->rad[i] - d;
+            if (overlap <= 0.) continue;
+            const double E_eff = 1. / ((1. - p->nu[i] * p->nu[i]) / p->E[i] + (1. - w->nu[k] * w->nu[k]) / w->E[k]);
+            const double kn = 4. / 3. * E_eff * std::sqrt(p->rad[i]);
+            epw += 0.4 * kn * overlap * overlap * std::sqrt(overlap);
+        }
+    }
+    out[0] = epp;
+    out[1] = epw;
+}
+
 // ---------------------------------------------------------------------------------
 // Bonded DEM.
 // ---------------------------------------------------------------------------------

@@ -135,6 +135,9 @@ int orc_run(orc_particles *p, const orc_walls *w, const orc_force_params *fp,
 
 /* Kinetic (translational + rotational) energy, sequential sum over i. */
 double orc_kinetic_energy(const orc_particles *p);
+/* Hertz elastic energy 2/5 kn overlap^2.5 of every overlapping pair (each pair once, all
+ * pairs by brute force) in out[0] and of every particle-wall overlap in out[1]. */
+void orc_elastic_energy(const orc_particles *p, const orc_walls *w, double *out);
 
 /* ---------------- bonded DEM (CabanaBondedDEM_*) ---------------- */
 typedef struct orc_bonds {

@@ -102,6 +102,8 @@ def lib():
         L.orc_update_tangential_contacts.argtypes = [C.POINTER(_Particles)]
         L.orc_kinetic_energy.restype = C.c_double
         L.orc_kinetic_energy.argtypes = [C.POINTER(_Particles)]
+        L.orc_elastic_energy.restype = None
+        L.orc_elastic_energy.argtypes = [C.POINTER(_Particles), C.POINTER(_Walls), C.POINTER(C.c_double)]
         L.orc_setup_bonds.argtypes = [C.POINTER(_Bonds), C.POINTER(_Particles), C.c_double, C.c_double]
         L.orc_bonded_force.argtypes = [C.POINTER(_Particles), C.POINTER(_Bonds), C.POINTER(_BondParams), C.c_double]
         L.orc_bonded_step.argtypes = [C.POINTER(_Particles), C.POINTER(_Bonds), C.POINTER(_BondParams),
@@ -205,6 +207,15 @@ def neighbor_list(state, delta=0.0, skin=0.0):
 def kinetic_energy(state):
     p = _particles(state)
     return lib().orc_kinetic_energy(C.byref(p))
+
+
+def elastic_energy(state, walls):
+    """Hertz elastic energy (pairs, walls) of a state: 2/5 kn overlap^2.5 per overlap."""
+    p = _particles(state)
+    w = _walls(walls)
+    out = (C.c_double * 2)()
+    lib().orc_elastic_energy(C.byref(p), C.byref(w), out)
+    return float(out[0]), float(out[1])
 
 
 def _bonds(b):

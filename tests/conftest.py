@@ -9,7 +9,9 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-REFERENCE = "/root/reference"
+# Where the reference repository is mounted (read-only; its golden data are read in place).
+# Set CABANADEM_REFERENCE to another checkout; tests that need it skip when it is absent.
+REFERENCE = os.environ.get("CABANADEM_REFERENCE", "/root/reference")
 
 
 def pytest_configure(config):

@@ -180,6 +180,8 @@ def test_elastic_gas_conserves_energy_with_the_reference_bits():
         assert O.run(s, w, _force_params(1.0, 1.0, 0.0, 0.0), 2.5e-7, 500, skin=0.1 * R, pow_mode=O.POW_SQRT) == 0
         ke = O.kinetic_energy(s)
         e = ke + _elastic_energy(s, w)
+        ep, ew = O.elastic_energy(s, w)                    # the oracle's C restatement agrees
+        assert abs(ep + ew - (e - ke)) <= 1e-12 * e0
         in_contact += int(ke < (1.0 - 1e-4) * e)          # energy stored in some contact
         assert abs(e - e0) <= 1e-5 * e0, (e - e0) / e0
     assert in_contact >= 5
