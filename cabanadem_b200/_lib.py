@@ -117,6 +117,7 @@ _PROTOS = {
     "dem_stage3": ([_VP], C.c_int),
     "dem_build_neighbors": ([_VP], C.c_int),
     "dem_solver_rebuild": ([_VP], C.c_int),
+    "dem_solver_set_timestep": ([_VP, C.c_double], C.c_int),
     "dem_compute_force": ([_VP], C.c_int),
     "dem_neighbors_get": ([_VP, _VP, _VP, C.POINTER(C.c_long)], C.c_int),
     "dem_energy": ([_VP, C.POINTER(C.c_double)], C.c_int),
@@ -127,6 +128,11 @@ _PROTOS = {
     "dem_bonds_get": ([_VP, C.c_int, _VP, C.c_long], C.c_int),
     "dem_bonds_broken": ([_VP, C.POINTER(C.c_long)], C.c_int),
     "dem_bonded_run": ([_VP, C.c_int], C.c_int),
+    "dem_bonds_set": ([_VP, C.c_int, _VP, C.c_long], C.c_int),
+    "dem_bonded_reset": ([_VP], C.c_int),
+    "dem_apply_external_force": ([_VP], C.c_int),
+    "dem_bonded_force": ([_VP, C.c_double], C.c_int),
+    "dem_apply_boundary_conditions": ([_VP], C.c_int),
     "dem_neighbor_list_noalloc": ([_VP, _VP, C.c_int, C.c_double, C.c_double, C.c_int, _VP, _VP, _VP], C.c_int),
     "dem_nn_mlp_forward": ([_VP, C.POINTER(NnMlp), C.c_long, C.POINTER(NnRows), C.c_int, _VP, _VP, _VP, _VP],
                            C.c_int),

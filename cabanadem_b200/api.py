@@ -507,6 +507,32 @@ class Bonds:
               "dem_bonds_get " + field)
         return a
 
+    def set(self, field, arr):
+        """Upload a bond slice (dem_bonds_set): idx in caller indices (-1 empty), count,
+        init_len, the history fields (ft_*, mn_*, mt_*) or broken, shaped as get() returns."""
+        dt = {"count": np.int32, "idx": np.int32, "broken": np.uint8}.get(field, np.float64)
+        a = np.ascontiguousarray(arr, dtype=dt)
+        check(lib().dem_bonds_set(self.h, _lib.BFIELD[field], a.ctypes.data, a.size), self.solver.particles.ctx.h,
+              "dem_bonds_set " + field)
+
+    # ---- the bonded loop phase by phase (tst_01_BDEM:295-306)
+    def resetForcesAndTorques(self):
+        """CabanaBondedDEM::resetForcesAndTorques (src/CabanaBondedDEM_Force.hpp:16-50): F = tau = 0."""
+        check(lib().dem_bonded_reset(self.h), self.solver.particles.ctx.h, "dem_bonded_reset")
+
+    def applyExternalForce(self):
+        """F += the external force (the example's applyTensileForce, tst_01_BDEM:70-117)."""
+        check(lib().dem_apply_external_force(self.solver.h), self.solver.particles.ctx.h, "dem_apply_external_force")
+
+    def computeBondedForce(self, dt: float):
+        """CabanaBondedDEM::computeBondedForce(particles, dt) (src/CabanaBondedDEM_Force.hpp:53-348)."""
+        return check(lib().dem_bonded_force(self.h, float(dt)), self.solver.particles.ctx.h, "dem_bonded_force")
+
+    def applyBoundaryConditions(self):
+        """Gravity, then the fix flags (the example's applyBoundaryConditions, tst_01_BDEM:19-67)."""
+        check(lib().dem_apply_boundary_conditions(self.solver.h), self.solver.particles.ctx.h,
+              "dem_apply_boundary_conditions")
+
     def broken(self) -> int:
         """Broken bond ends (each bond of a symmetric pair is counted at both particles)."""
         c = C.c_long(0)

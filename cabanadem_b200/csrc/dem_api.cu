@@ -208,6 +208,18 @@ __global__ void k_gather_u8n(const uint8_t *src, uint8_t *dst, int n, int ncomp,
         dst[t] = src[(long)k * cap + rank[c]];
     }
 }
+__global__ void k_scatter_u8n(const uint8_t *src, uint8_t *dst, int n, int ncomp, int cap, const int *rank) {
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < (long)n * ncomp; t += (long)gridDim.x * blockDim.x) {
+        const int c = (int)(t / ncomp), k = (int)(t % ncomp);
+        dst[(long)k * cap + rank[c]] = src[t];
+    }
+}
+__global__ void k_scatter_d2f(const double *src, float *dst, int n, int ncomp, int cap, const int *rank) {
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < (long)n * ncomp; t += (long)gridDim.x * blockDim.x) {
+        const int c = (int)(t / ncomp), k = (int)(t % ncomp);
+        dst[(long)k * cap + rank[c]] = (float)src[t];
+    }
+}
 __global__ void k_fill_i(int *a, long count, int v) {
     for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < count; t += (long)gridDim.x * blockDim.x) a[t] = v;
 }
@@ -1367,6 +1379,15 @@ extern "C" int dem_build_neighbors(dem_solver *s) {
     if (st) return st;
     return DEM_OK;
 }
+extern "C" int dem_solver_set_timestep(dem_solver *s, double dt) {
+    if (!s || !(dt > 0.0)) return DEM_ERR_INVALID;
+    if (dt == s->sp.dt) return DEM_OK;
+    s->sp.dt = dt;
+    s->fc.dt = dt;
+    s->fc.half_dt = 0.5 * dt;   // Integrator.hpp:25
+    s->version++;               // captured graphs hold the old step constants
+    return DEM_OK;
+}
 extern "C" int dem_solver_rebuild(dem_solver *s) {
     if (!s) return DEM_ERR_INVALID;
     if (s->p->mat_dirty || (s->p->P.ext != nullptr) != (s->fc.has_ext != 0)) {
@@ -1549,6 +1570,98 @@ extern "C" int dem_bonds_get(dem_bonds *b, int field, void *host, long count) {
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     cudaFree(tmp);
     CK(e);
+    return DEM_OK;
+}
+
+extern "C" int dem_bonds_set(dem_bonds *b, int field, const void *host, long count) {
+    if (!b || !host) return DEM_ERR_INVALID;
+    dem_solver *s = b->s;
+    dem_ctx *ctx = s->ctx;
+    const Particles &P = s->p->P;
+    const Bonds &B = b->B;
+    const int n = P.n, mb = B.mb;
+    const long per = (field == DEM_B_COUNT) ? n : (long)n * mb;
+    const int es = (field == DEM_B_IDX || field == DEM_B_COUNT) ? 4 : (field == DEM_B_BROKEN ? 1 : 8);
+    if (field < DEM_B_IDX || field > DEM_B_BROKEN || count != per)
+        return fail(ctx, DEM_ERR_INVALID, "dem_bonds_set: unknown field or wrong element count");
+    if (field == DEM_B_IDX || field == DEM_B_COUNT) {
+        const int *v = static_cast<const int *>(host);
+        for (long t = 0; t < per; ++t) {
+            const bool ok = field == DEM_B_IDX ? (v[t] >= -1 && v[t] < n) : (v[t] >= 0 && v[t] <= mb);
+            if (!ok) return fail(ctx, DEM_ERR_INVALID, "dem_bonds_set: bond partner or count out of range");
+        }
+    }
+    cudaStream_t st = ctx->stream;
+    void *tmp = s->p->stage;
+    if ((size_t)per * es > s->p->stage_bytes) return fail(ctx, DEM_ERR_INVALID, "dem_bonds_set: field too large");
+    CK(cudaMemcpyAsync(tmp, host, (size_t)per * es, cudaMemcpyHostToDevice, st));
+    switch (field) {
+        case DEM_B_IDX: k_scatter_i<<<kGS, kTB, 0, st>>>((const int *)tmp, B.idx, n, mb, P.cap, P.rank, 1); break;
+        case DEM_B_INIT_LEN: k_scatter_d<<<kGS, kTB, 0, st>>>((const double *)tmp, B.init_len, n, mb, P.cap, P.rank); break;
+        case DEM_B_COUNT: k_scatter_i<<<kGS, kTB, 0, st>>>((const int *)tmp, B.count, n, 1, P.cap, P.rank, 0); break;
+        case DEM_B_BROKEN: k_scatter_u8n<<<kGS, kTB, 0, st>>>((const uint8_t *)tmp, B.broken, n, mb, P.cap, P.rank); break;
+        default:
+            if (B.hist32)
+                k_scatter_d2f<<<kGS, kTB, 0, st>>>((const double *)tmp, B.hist32 + (long)(field - DEM_B_FT_X) * mb * P.cap,
+                                                   n, mb, P.cap, P.rank);
+            else
+                k_scatter_d<<<kGS, kTB, 0, st>>>((const double *)tmp, B.hist + (long)(field - DEM_B_FT_X) * mb * P.cap, n,
+                                                 mb, P.cap, P.rank);
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(st));   // the staging buffer is reused by the next upload
+    if (field == DEM_B_IDX || field == DEM_B_COUNT) {
+        // bonds given by the caller define the particle order from now on, as setupBonds does
+        s->p->has_bonds = true;
+        b->set_up = true;
+    }
+    return DEM_OK;
+}
+
+extern "C" int dem_bonded_reset(dem_bonds *b) {
+    if (!b) return DEM_ERR_INVALID;
+    dem_ctx *ctx = b->s->ctx;
+    const Particles &P = b->s->p->P;
+    cudaStream_t st = b->s->ctx->stream;
+    CK(cudaMemsetAsync(P.force, 0, sizeof(double) * 3 * (size_t)P.cap, st));
+    CK(cudaMemsetAsync(P.torque, 0, sizeof(double) * 3 * (size_t)P.cap, st));
+    return DEM_OK;
+}
+
+extern "C" int dem_apply_external_force(dem_solver *s) {
+    if (!s) return DEM_ERR_INVALID;
+    dem_ctx *ctx = s->ctx;
+    launch_add_ext_force(s->p->P, s->ctx->stream);
+    CK(cudaGetLastError());
+    return DEM_OK;
+}
+
+extern "C" int dem_bonded_force(dem_bonds *b, double dt) {
+    if (!b || !(dt > 0.0)) return DEM_ERR_INVALID;
+    dem_solver *s = b->s;
+    dem_ctx *ctx = s->ctx;
+    if (!b->set_up) return fail(ctx, DEM_ERR_INVALID, "dem_bonded_force: call dem_bonds_setup first");
+    if (s->p->mat_dirty) {
+        int st = prepare(s);
+        if (st) return st;
+    }
+    launch_bond_force(s->p->P, b->B, s->p->ctl, b->bc, dt, ctx->stream);
+    CK(cudaGetLastError());
+    int status = 0;
+    CK(cudaMemcpyAsync(&status, &s->p->ctl->status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return status & (DEM_ERR_BOND_OVERFLOW | DEM_ERR_NAN);
+}
+
+extern "C" int dem_apply_boundary_conditions(dem_solver *s) {
+    if (!s) return DEM_ERR_INVALID;
+    if (s->p->mat_dirty || (s->p->P.ext != nullptr) != (s->fc.has_ext != 0)) {
+        int st = prepare(s);
+        if (st) return st;
+    }
+    dem_ctx *ctx = s->ctx;
+    launch_post_hooks(s->p->P, s->fc, ctx->stream);
+    CK(cudaGetLastError());
     return DEM_OK;
 }
 

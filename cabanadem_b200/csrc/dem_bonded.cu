@@ -7,6 +7,8 @@
 //   k_bond_step    one bonded step in the order of tst_01_BDEM:295-306: force reset, external
 //                  force, computeBondedForce (src/CabanaBondedDEM_Force.hpp:86-341), boundary
 //                  hook, stage3, then stage1 + stage2 of the next step (ping-pong buffers)
+//   k_bond_force   computeBondedForce alone, for callers that drive the bonded loop phase by
+//                  phase (with k_add_ext_force and k_post_hooks for the example's hooks)
 //
 // Bond slots are slot-major per particle: partner (sorted index), rest length, and the 9 live
 // history components (tangential force, normal and tangential moments; the reference's
@@ -316,6 +318,78 @@ __global__ void __launch_bounds__(kBondBlock) k_bond_step(Particles P, Bonds B, 
     finish_step(ctl, P.vslots, vmax2, fc.dt, status, true, true);
 }
 
+// computeBondedForce as a phase of its own (src/CabanaBondedDEM_Force.hpp:53-348): for every
+// particle, F and tau += the bond terms in slot order, starting from the F and tau the earlier
+// phases left (resetForcesAndTorques, then the caller's hooks).  Same per-bond arithmetic as
+// the fused step (bond_term), so a loop of phases equals the fused step bit for bit.
+template <typename R>
+__global__ void __launch_bounds__(kBondBlock) k_bond_force(Particles P, Bonds B, Ctl *ctl, BondConsts bc, double dt) {
+    R *__restrict__ hist = bond_hist<R>(B);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n) return;
+    const int cur = ctl->cur, vcur = ctl->vcur, cap = P.cap;
+    const double4 *__restrict__ pc = P.pos[cur];
+    const double *__restrict__ vc = P.vel[vcur];
+    const double *__restrict__ wc = P.omg[vcur];
+    const D4 pi = ld4(pc, i);
+    const double ui0 = vc[i], ui1 = vc[cap + i], ui2 = vc[2 * cap + i];
+    const double wi0 = wc[i], wi1 = wc[cap + i], wi2 = wc[2 * cap + i];
+    double F0 = P.force[i], F1 = P.force[cap + i], F2 = P.force[2 * cap + i];
+    double T0 = P.torque[i], T1 = P.torque[cap + i], T2 = P.torque[2 * cap + i];
+    const double Ei = B.E[i], Gi = B.G[i];
+    int status = 0;
+    const int no_bonds_i = B.count[i];
+    for (int k = 0; k < no_bonds_i; k++) {
+        double cf[6];
+        if (!bond_term<R>(P, B, bc, hist, pc, vc, wc, cap, i, k, pi, ui0, ui1, ui2, wi0, wi1, wi2, Ei, Gi, dt, status,
+                          cf))
+            continue;
+        F0 += cf[0];
+        F1 += cf[1];
+        F2 += cf[2];
+        T0 += cf[3];
+        T1 += cf[4];
+        T2 += cf[5];
+    }
+    P.force[i] = F0;
+    P.force[cap + i] = F1;
+    P.force[2 * cap + i] = F2;
+    P.torque[i] = T0;
+    P.torque[cap + i] = T1;
+    P.torque[2 * cap + i] = T2;
+    if (status) atomicOr(&ctl->status, status);
+}
+
+// The hook in the position of tst_01_BDEM's applyTensileForce (:101-111): F += the external
+// force (DEM_F_EXT_FORCE).
+__global__ void k_add_ext_force(Particles P) {
+    const int cap = P.cap;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += gridDim.x * blockDim.x) {
+        P.force[i] += P.ext[i];
+        P.force[cap + i] += P.ext[cap + i];
+        P.force[2 * cap + i] += P.ext[2 * cap + i];
+    }
+}
+
+// The hooks in the position of tst_01_BDEM's applyBoundaryConditions (:19-67): gravity (m g
+// added), then the DEM_FIX_* flags zero F and/or tau -- the order of the fused step.
+__global__ void k_post_hooks(Particles P, ForceConsts fc) {
+    const int cap = P.cap;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += gridDim.x * blockDim.x) {
+        if (fc.has_gravity) {
+            const double m = load_mI(P, i).x;
+            P.force[i] += m * fc.g[0];
+            P.force[cap + i] += m * fc.g[1];
+            P.force[2 * cap + i] += m * fc.g[2];
+        }
+        if (fc.has_fix) {
+            const int f = P.fix[i];
+            if (f & DEM_FIX_FORCE) P.force[i] = P.force[cap + i] = P.force[2 * cap + i] = 0.;
+            if (f & DEM_FIX_TORQUE) P.torque[i] = P.torque[cap + i] = P.torque[2 * cap + i] = 0.;
+        }
+    }
+}
+
 __global__ void k_bond_broken_count(Bonds B, int n, unsigned long long *out) {
     unsigned long long c = 0;
     for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < (long)B.mb * B.cap; t += (long)gridDim.x * blockDim.x)
@@ -336,6 +410,21 @@ void launch_bond_step(const Particles &P, const Bonds &B, Ctl *ctl, const ForceC
         k_bond_step<float><<<(P.n + kBondBlock - 1) / kBondBlock, kBondBlock, 0, s>>>(P, B, ctl, fc, bc);
     else
         k_bond_step<double><<<(P.n + kBondBlock - 1) / kBondBlock, kBondBlock, 0, s>>>(P, B, ctl, fc, bc);
+}
+
+void launch_bond_force(const Particles &P, const Bonds &B, Ctl *ctl, const BondConsts &bc, double dt, cudaStream_t s) {
+    if (B.hist32)
+        k_bond_force<float><<<(P.n + kBondBlock - 1) / kBondBlock, kBondBlock, 0, s>>>(P, B, ctl, bc, dt);
+    else
+        k_bond_force<double><<<(P.n + kBondBlock - 1) / kBondBlock, kBondBlock, 0, s>>>(P, B, ctl, bc, dt);
+}
+
+void launch_add_ext_force(const Particles &P, cudaStream_t s) {
+    if (P.ext) k_add_ext_force<<<(P.n + 255) / 256, 256, 0, s>>>(P);
+}
+
+void launch_post_hooks(const Particles &P, const ForceConsts &fc, cudaStream_t s) {
+    if (fc.has_gravity || fc.has_fix) k_post_hooks<<<(P.n + 255) / 256, 256, 0, s>>>(P, fc);
 }
 
 void launch_bond_broken_count(const Bonds &B, int n, unsigned long long *out, cudaStream_t s) {

@@ -200,6 +200,9 @@ void launch_bond_setup(const Particles &P, const NbrList &L, const Bonds &B, Ctl
 void launch_bond_step(const Particles &P, const Bonds &B, Ctl *ctl, const ForceConsts &fc, const BondConsts &bc,
                       cudaStream_t s);
 void launch_bond_broken_count(const Bonds &B, int n, unsigned long long *out, cudaStream_t s);
+void launch_bond_force(const Particles &P, const Bonds &B, Ctl *ctl, const BondConsts &bc, double dt, cudaStream_t s);
+void launch_add_ext_force(const Particles &P, cudaStream_t s);
+void launch_post_hooks(const Particles &P, const ForceConsts &fc, cudaStream_t s);
 
 // ---- launchers (dem_step.cu) ------------------------------------------------------
 // MODE_FUSED launches the fused step (kernels_per_step(fc) kernels); MODE_FORCE_ONLY one

@@ -16,8 +16,12 @@
 //     force, p, wall, neigh, tag, dt) (Force.hpp:700-710)   and solver->buildNeighbors()
 //   Particles::output -> particles_<k>.h5            particles_<k>.csv, or .xmf + .bin
 //                                                    (setOutputFormat("xdmf"))
-//   CabanaBondedDEM::ParticlesBondedDEM<Mem,3,MaxBonds>::setupBonds (BondedDEM_Particles.hpp:86)
-//                                                    BondedDEM<Mem,3,MaxBonds> (setupBonds, run)
+//   CabanaBondedDEM::ParticlesBondedDEM<Mem,3,MaxBonds> same template: particle and bond slices,
+//     (BondedDEM_Particles.hpp:29-293)              setupBonds<Exec>(), update_mesh_limits, output
+//   CabanaBondedDEM::resetForcesAndTorques<Exec>(p), same, one device phase each (the reference's
+//     computeBondedForce<Exec>(p, dt),               loop, tst_01_BDEM:295-306, ports unchanged);
+//     BondedDEMIntegrator<Exec>(dt).stage1/2/3(p)    ParticlesBondedDEM::run_steps fuses the loop
+//     (BondedDEM_Force.hpp:16-348, BondedDEM_Integrator.hpp:15-102)
 //
 // Slices: slicePosition() etc. return a HostSlice, a shared host copy of one field taken at
 // the call; writing through it marks the field dirty, and updateParticles(exec, functor)
@@ -438,6 +442,17 @@ class Particles {
     HostSlice<double> sliceTangentialDispSWy() { return slice_d(DEM_F_TNG_SW_Y, MaxNoWalls); }
     HostSlice<double> sliceTangentialDispSWz() { return slice_d(DEM_F_TNG_SW_Z, MaxNoWalls); }
     HostSlice<int> sliceTangentialDispIdx() { return slice_i(DEM_F_TNG_IDX, MaxCnts); }
+    // the reference's accelerations (Particles.hpp:117-124) are written by its examples' set-up
+    // functors and read by nothing on the path: a host-only [n][3] array here
+    HostSlice<double> sliceAcceleration() {
+        if (!au_) {
+            au_ = std::make_shared<Mirror<double>>();
+            au_->ncomp = 3;
+            au_->data.assign(static_cast<size_t>(n_) * 3, 0.0);
+            au_->fresh = true;
+        }
+        return HostSlice<double>(au_);
+    }
     HostSlice<int> sliceTotalNoTangentialContacts() { return slice_i(DEM_F_TNG_COUNT, 1); }
 
     // updateParticles(exec, functor) (Particles.hpp:91-97): functor(pid) on the host for every
@@ -545,6 +560,7 @@ class Particles {
             kv.second->dirty = kv.second->ncomp > 0;
             kv.second->fresh = true;
         }
+        if (au_) au_->data.resize(static_cast<size_t>(nn) * 3, 0.0);
         commit();
     }
 
@@ -601,6 +617,7 @@ class Particles {
     dem_particles *h_ = nullptr;
     std::map<int, std::shared_ptr<Mirror<double>>> md_;
     std::map<int, std::shared_ptr<Mirror<int>>> mi_;
+    std::shared_ptr<Mirror<double>> au_;
 };
 
 // ---------------------------------------------------------------------------------------
@@ -808,49 +825,246 @@ auto createSolverDEM(const InputsType &inputs, std::shared_ptr<ParticleType> par
 
 namespace CabanaBondedDEM {
 
-// Bond slots and the bonded loop on a particle set (ParticlesBondedDEM, BondedDEM_Particles.hpp:29-293;
-// computeBondedForce, BondedDEM_Force.hpp:53-348; loop of tst_01_BDEM:295-306).
+using CabanaDEM::Context;
+using CabanaDEM::Error;
+using CabanaDEM::HostSlice;
+using CabanaDEM::Mirror;
+
+// ParticlesBondedDEM<MemorySpace, Dim, MaxBonds> (BondedDEM_Particles.hpp:29-293): the particle
+// fields of CabanaDEM::Particles plus the bond slots.  Bond slices are host mirrors of the
+// device slots, like the particle slices: written through, they are uploaded before the next
+// device phase; read after a phase, they are downloaded fresh.  The device solver and bond
+// storage are created by setupBonds(); bond slices written before it are replaced by the
+// bonds it finds (the reference's examples write their initial zeros and -1 there).
+// sliceBondFn*() are host-only: the reference never writes its bond_fn_* arrays
+// (BondedDEM_Force.hpp:69-71 takes them, no line stores to them).
 template <class MemorySpace, int Dimension, int MaxBonds>
-class BondedDEM {
+class ParticlesBondedDEM : public CabanaDEM::Particles<MemorySpace, Dimension, 1, 0> {
+    using Base = CabanaDEM::Particles<MemorySpace, Dimension, 1, 0>;
+
   public:
-    template <class ParticleType>
-    BondedDEM(std::shared_ptr<ParticleType> particles, double dt, const dem_bond_params &bp)
-        : ctx_(particles->context_ptr()) {
-        particles->commit();
-        dem_solver_params sp{};
-        sp.dt = dt;
-        const dem_force_params fp{1.0, 1.0, 0.0, 0.0, DEM_REF_COMPAT};
-        ctx_->check(dem_solver_create(ctx_->handle(), particles->handle(), nullptr, &fp, &sp, &s_), "dem_solver_create");
-        ctx_->check(dem_bonds_create(s_, MaxBonds, &bp, &b_), "dem_bonds_create");
-        particles->attach_solver(1);
-        invalidate_ = [particles]() { particles->invalidate(); };
-        detach_ = [particles]() { particles->attach_solver(-1); };
+    using memory_space = MemorySpace;
+    using execution_space = typename MemorySpace::execution_space;
+    double delta = 0.0;
+
+    // ParticlesBondedDEM(exec, n) (:49-58); output_folder and bond_params are additions: the
+    // folder of output() and the bond model (default: the reference's, every DEM_BQ* bit set,
+    // sign-damping 0.1, bond radius = the smaller particle radius)
+    template <class ExecSpace>
+    ParticlesBondedDEM(const ExecSpace &e, std::size_t n, const std::string &output_folder = "",
+                       const dem_bond_params *bond_params = nullptr, std::shared_ptr<Context> ctx = nullptr)
+        : Base(e, n, output_folder, ctx) {
+        if (bond_params) bp_ = *bond_params;
+        else {
+            bp_ = dem_bond_params{};
+            bp_.quirks = DEM_BOND_REF_COMPAT;
+            bp_.beta = 0.1;
+            bp_.radius_factor = 1.0;
+        }
+        for (int f : {DEM_B_IDX, DEM_B_COUNT}) {
+            auto m = std::make_shared<Mirror<int>>();
+            m->ncomp = f == DEM_B_IDX ? MaxBonds : 1;
+            m->data.assign(n * static_cast<size_t>(m->ncomp), f == DEM_B_IDX ? -1 : 0);
+            m->fresh = true;
+            bi_[f] = m;
+        }
+        for (int f = DEM_B_INIT_LEN; f <= DEM_B_MT_Z; ++f) {
+            if (f == DEM_B_COUNT) continue;
+            auto m = std::make_shared<Mirror<double>>();
+            m->ncomp = MaxBonds;
+            m->data.assign(n * static_cast<size_t>(MaxBonds), 0.0);
+            m->fresh = true;
+            bd_[f] = m;
+        }
+        for (auto &m : fn_) {
+            m = std::make_shared<Mirror<double>>();
+            m->ncomp = MaxBonds;
+            m->data.assign(n * static_cast<size_t>(MaxBonds), 0.0);
+            m->fresh = true;
+        }
     }
-    ~BondedDEM() {
-        dem_bonds_destroy(b_);
-        dem_solver_destroy(s_);
-        detach_();
+    ~ParticlesBondedDEM() {
+        if (b_) dem_bonds_destroy(b_);
+        if (s_) {
+            dem_solver_destroy(s_);
+            this->attach_solver(-1);
+        }
     }
-    // setupBonds (BondedDEM_Particles.hpp:86-171): reference factor 3, search cutoff 4 rad(0)
+
+    void update_mesh_limits(const std::array<double, 3> &lo, const std::array<double, 3> &hi) {
+        this->mesh_lo = lo;   // kept for source compatibility: the device grid follows the
+        this->mesh_hi = hi;   // particles' bounding box
+    }
+
+    // updateParticles(exec, functor) (:60-64): functor(pid) on the host for every particle,
+    // then every particle and bond slice written through is uploaded
+    template <class ExecSpace, class Functor>
+    void updateParticles(const ExecSpace &, const Functor &f) {
+        for (int pid = 0; pid < static_cast<int>(this->size()); ++pid) f(pid);
+        commit();
+    }
+
+    HostSlice<double> sliceBondFnX() { return HostSlice<double>(fn_[0]); }
+    HostSlice<double> sliceBondFnY() { return HostSlice<double>(fn_[1]); }
+    HostSlice<double> sliceBondFnZ() { return HostSlice<double>(fn_[2]); }
+    HostSlice<double> sliceBondFtX() { return bslice_d(DEM_B_FT_X); }
+    HostSlice<double> sliceBondFtY() { return bslice_d(DEM_B_FT_Y); }
+    HostSlice<double> sliceBondFtZ() { return bslice_d(DEM_B_FT_Z); }
+    HostSlice<double> sliceBondMnX() { return bslice_d(DEM_B_MN_X); }
+    HostSlice<double> sliceBondMnY() { return bslice_d(DEM_B_MN_Y); }
+    HostSlice<double> sliceBondMnZ() { return bslice_d(DEM_B_MN_Z); }
+    HostSlice<double> sliceBondMtX() { return bslice_d(DEM_B_MT_X); }
+    HostSlice<double> sliceBondMtY() { return bslice_d(DEM_B_MT_Y); }
+    HostSlice<double> sliceBondMtZ() { return bslice_d(DEM_B_MT_Z); }
+    HostSlice<double> sliceBondInitLen() { return bslice_d(DEM_B_INIT_LEN); }
+    HostSlice<int> sliceBondIdx() { return bslice_i(DEM_B_IDX); }
+    HostSlice<int> sliceTotalNoBonds() { return bslice_i(DEM_B_COUNT); }
+
+    // setupBonds<ExecSpace>() (:86-171): bond every j with rij < 3 rad(i) among the particles
+    // within 4 rad(0), as the reference hard-codes (:130, :152-154); the arguments allow others
+    template <class ExecSpace>
     void setupBonds(double factor = 3.0, double search_cutoff = 0.0) {
-        ctx_->check(dem_bonds_setup(b_, factor, search_cutoff), "dem_bonds_setup");
+        this->commit();
+        if (!s_) create_device();
+        if (!(search_cutoff > 0.0)) search_cutoff = 4.0 * this->sliceRadius().get(0);
+        this->context().check(dem_bonds_setup(b_, factor, search_cutoff), "dem_bonds_setup");
+        for (auto &kv : bi_) kv.second->dirty = kv.second->fresh = false;
+        for (auto &kv : bd_) kv.second->dirty = kv.second->fresh = false;
+        this->invalidate();
     }
-    void run_steps(int n) {
-        ctx_->check(dem_bonded_run(b_, n), "dem_bonded_run");
-        invalidate_();
+
+    // host edits -> device, for every particle and bond slice written since the last phase
+    void commit() {
+        Base::commit();
+        if (!b_) return;
+        for (auto &kv : bi_)
+            if (kv.second->dirty) {
+                this->context().check(dem_bonds_set(b_, kv.first, kv.second->data.data(), (long)kv.second->data.size()),
+                                      "dem_bonds_set");
+                kv.second->dirty = false;
+            }
+        for (auto &kv : bd_)
+            if (kv.second->dirty) {
+                this->context().check(dem_bonds_set(b_, kv.first, kv.second->data.data(), (long)kv.second->data.size()),
+                                      "dem_bonds_set");
+                kv.second->dirty = false;
+            }
+    }
+    // device -> mirrors on their next read
+    void invalidate() {
+        Base::invalidate();
+        for (auto &kv : bi_) kv.second->fresh = false;
+        for (auto &kv : bd_) kv.second->fresh = false;
+    }
+
+    // One device phase: slice edits uploaded first, slices stale afterwards.
+    template <class F>
+    int phase(F &&f, const char *what, int allow = 0) {
+        if (!s_) throw Error(std::string(what) + ": call setupBonds first");
+        commit();
+        const int st = f();
+        invalidate();
+        this->context().check(st, what, allow);
+        return st;
+    }
+    // The hooks of the reference example, on the device: F += the external force set with
+    // setExternalForce (applyTensileForce, tst_01_BDEM:70-117), and gravity then the fix
+    // flags set with setFixFlags (applyBoundaryConditions, :19-67).
+    void addExternalForce() {
+        phase([&] { return dem_apply_external_force(s_); }, "dem_apply_external_force");
+    }
+    void applyFixFlags() {
+        phase([&] { return dem_apply_boundary_conditions(s_); }, "dem_apply_boundary_conditions");
+    }
+    // The whole bonded loop fused on the device, n steps of dt (dem_bonded_run).
+    void run_steps(int n, double dt) {
+        set_timestep(dt);
+        phase([&] { return dem_bonded_run(b_, n); }, "dem_bonded_run");
     }
     long broken() {
         long c = 0;
-        ctx_->check(dem_bonds_broken(b_, &c), "dem_bonds_broken");
+        this->context().check(dem_bonds_broken(b_, &c), "dem_bonds_broken");
         return c;
     }
-    dem_bonds *handle() { return b_; }
+    void set_timestep(double dt) {
+        if (!s_) throw Error("set_timestep: call setupBonds first");
+        if (dt != dt_) {
+            this->context().check(dem_solver_set_timestep(s_, dt), "dem_solver_set_timestep");
+            dt_ = dt;
+        }
+    }
+    dem_solver *solver_handle() { return s_; }
+    dem_bonds *bonds_handle() { return b_; }
 
   private:
-    std::shared_ptr<CabanaDEM::Context> ctx_;
+    void create_device() {
+        dem_solver_params sp{};
+        sp.dt = dt_;
+        const dem_force_params fp{1.0, 1.0, 0.0, 0.0, DEM_REF_COMPAT};
+        this->context().check(dem_solver_create(this->context().handle(), this->handle(), nullptr, &fp, &sp, &s_),
+                              "dem_solver_create");
+        this->attach_solver(1);
+        this->context().check(dem_bonds_create(s_, MaxBonds, &bp_, &b_), "dem_bonds_create");
+    }
+    HostSlice<double> bslice_d(int field) {
+        auto &m = bd_[field];
+        if (b_ && !m->fresh && !m->dirty) {
+            this->context().check(dem_bonds_get(b_, field, m->data.data(), (long)m->data.size()), "dem_bonds_get");
+            m->fresh = true;
+        }
+        return HostSlice<double>(m);
+    }
+    HostSlice<int> bslice_i(int field) {
+        auto &m = bi_[field];
+        if (b_ && !m->fresh && !m->dirty) {
+            this->context().check(dem_bonds_get(b_, field, m->data.data(), (long)m->data.size()), "dem_bonds_get");
+            m->fresh = true;
+        }
+        return HostSlice<int>(m);
+    }
+
+    dem_bond_params bp_{};
     dem_solver *s_ = nullptr;
     dem_bonds *b_ = nullptr;
-    std::function<void()> invalidate_, detach_;
+    double dt_ = 1e-4;   // replaced by the integrator's or run_steps' dt
+    std::map<int, std::shared_ptr<Mirror<int>>> bi_;
+    std::map<int, std::shared_ptr<Mirror<double>>> bd_;
+    std::array<std::shared_ptr<Mirror<double>>, 3> fn_;
+};
+
+// resetForcesAndTorques<ExecutionSpace>(particles) (BondedDEM_Force.hpp:16-50): F = tau = 0.
+template <class ExecutionSpace, class ParticleType>
+void resetForcesAndTorques(ParticleType &particles) {
+    particles.phase([&] { return dem_bonded_reset(particles.bonds_handle()); }, "dem_bonded_reset");
+}
+
+// computeBondedForce<ExecutionSpace>(particles, dt) (BondedDEM_Force.hpp:53-348): F and tau +=
+// every bond's force and moment, in slot order, on top of what the phases before it left.
+template <class ExecutionSpace, class ParticleType>
+void computeBondedForce(ParticleType &particles, double dt) {
+    particles.phase([&] { return dem_bonded_force(particles.bonds_handle(), dt); }, "dem_bonded_force");
+}
+
+// BondedDEMIntegrator<ExecutionSpace>(dt) (BondedDEM_Integrator.hpp:15-102): velocity-Verlet
+// half-kicks and drift of a ParticlesBondedDEM, with the integrator's dt.
+template <class ExecutionSpace>
+class BondedDEMIntegrator {
+  public:
+    explicit BondedDEMIntegrator(double dt) : _dt(dt), _half_dt(0.5 * dt) {}
+    template <class ParticlesType>
+    void stage1(ParticlesType &p) { stage(p, dem_stage1, "dem_stage1"); }
+    template <class ParticlesType>
+    void stage2(ParticlesType &p) { stage(p, dem_stage2, "dem_stage2"); }
+    template <class ParticlesType>
+    void stage3(ParticlesType &p) { stage(p, dem_stage3, "dem_stage3"); }
+
+  private:
+    template <class ParticlesType>
+    void stage(ParticlesType &p, int (*f)(dem_solver *), const char *what) {
+        p.set_timestep(_dt);
+        p.phase([&] { return f(p.solver_handle()); }, what);
+    }
+    double _dt, _half_dt;
 };
 
 }  // namespace CabanaBondedDEM

@@ -177,6 +177,11 @@ int dem_solver_destroy(dem_solver *s);
  * displacement bound exceeds skin/2 (or every step when rebuild_every_step). */
 int dem_solver_run(dem_solver *s, int nsteps);
 int dem_solver_stats(dem_solver *s, dem_run_stats *out);
+/* Change the time step of later steps and phases: the dt an Integrator / BondedDEMIntegrator
+ * is constructed with (src/CabanaDEM_Integrator.hpp:22-27,
+ * src/CabanaBondedDEM_Integrator.hpp:22-27), for callers whose integrator and solver are
+ * set up apart. */
+int dem_solver_set_timestep(dem_solver *s, double dt);
 /* Current wall positions [nw][3] (moving walls advance by dt * u each step when
  * DEM_Q6_WALL_STATIC is clear; no reference counterpart: the reference's walls never move,
  * src/CabanaDEM_Force.hpp:529). */
@@ -273,6 +278,32 @@ int dem_bonds_broken(dem_bonds *b, long *count);
  * force (DEM_F_EXT_FORCE), computeBondedForce, boundary hook (DEM_F_FIX), stage3 -- fused
  * into one kernel per step, graph-captured. */
 int dem_bonded_run(dem_bonds *b, int nsteps);
+/* Upload of a bond slice (the reference's slices are writable views,
+ * src/CabanaBondedDEM_Particles.hpp:187-201): DEM_B_IDX in caller indices (-1 empty),
+ * DEM_B_COUNT, DEM_B_INIT_LEN, the history fields and DEM_B_BROKEN, in the layout of
+ * dem_bonds_get.  Bonds set this way fix the particle order as dem_bonds_setup does. */
+int dem_bonds_set(dem_bonds *b, int field, const void *host, long count);
+
+/* The bonded loop phase by phase, for callers that drive it themselves (the reference's
+ * loop, tst_01_BDEM:295-306):
+ *   stage1, stage2            BondedDEMIntegrator::stage1/2 (src/CabanaBondedDEM_Integrator.hpp:
+ *                             31-74): dem_stage1 / dem_stage2 on the solver the bonds belong to
+ *                             (the same arithmetic as Integrator::stage1/2)
+ *   dem_bonded_reset          resetForcesAndTorques (src/CabanaBondedDEM_Force.hpp:16-50): F = tau = 0
+ *   dem_apply_external_force  F += DEM_F_EXT_FORCE, in the position of the example's
+ *                             applyTensileForce (tst_01_BDEM:70-117); no-op without it
+ *   dem_bonded_force          computeBondedForce(particles, dt) (src/CabanaBondedDEM_Force.hpp:
+ *                             53-348): F and tau += every bond's force and moment in slot order,
+ *                             bond history updated, bonds past the breakage strain broken;
+ *                             returns DEM_ERR_BOND_OVERFLOW as dem_bonded_run does
+ *   dem_apply_boundary_conditions  gravity (m g), then the DEM_F_FIX flags zero F and/or tau, in
+ *                             the position of the example's applyBoundaryConditions (tst_01_BDEM:19-67)
+ *   stage3                    BondedDEMIntegrator::stage3 (:77-102): dem_stage3
+ * The phases in this order give the fused dem_bonded_run's results bit for bit. */
+int dem_bonded_reset(dem_bonds *b);
+int dem_apply_external_force(dem_solver *s);
+int dem_bonded_force(dem_bonds *b, double dt);
+int dem_apply_boundary_conditions(dem_solver *s);
 
 /* ---- neighbour list without allocation ---------------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device memory at the

@@ -381,13 +381,17 @@ def test_particle_insertion_driver(tmp_path):
 
 
 @pytest.mark.gpu
-def test_bdem_driver_matches_oracle(tmp_path):
-    """tst_01_BDEM: the driver's snapshots every 100 steps against the bonded oracle."""
+@pytest.mark.parametrize("mode", [[], ["--hooks=device"], ["--fused"]], ids=["reference_loop", "device_hooks", "fused"])
+def test_bdem_driver_matches_oracle(tmp_path, mode):
+    """tst_01_BDEM written as the reference's loop (BondedDEMIntegrator stages,
+    resetForcesAndTorques, the example's hooks through the force slice, computeBondedForce):
+    the driver's snapshots every 100 steps against the bonded oracle, bit for bit; the same
+    with the hooks on the device, and with the loop fused."""
     _build()
     from cabanadem_b200 import scenarios as S
     from oracle import oracle as O
     out = tmp_path / "bdem"
-    subprocess.run([os.path.join(EXDIR, "Tst01BDEMTwoParticlesTensile3D"), str(out)], check=True,
+    subprocess.run([os.path.join(EXDIR, "Tst01BDEMTwoParticlesTensile3D"), str(out)] + mode, check=True,
                    capture_output=True)
     got = [snapshots.read(f) for f in snapshots.files(str(out))]
     case = S.bdem_two_particles()

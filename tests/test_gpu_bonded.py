@@ -90,3 +90,70 @@ def test_bonded_mixed_precision_against_fp64():
     assert np.array_equal(br64, br32)
     assert np.abs(c32 - c64).max() <= 1e-4 * np.abs(c64).max()
     assert np.abs(x32 - x64).max() <= 1e-8   # m, against r = 0.5 mm
+
+
+def _phase_loop(bonds, dt, nsteps):
+    """The reference's bonded loop phase by phase (tst_01_BDEM:295-306), through the C ABI."""
+    it = bonds.solver.integrator
+    for _ in range(nsteps):
+        it.stage1()
+        it.stage2()
+        bonds.resetForcesAndTorques()
+        bonds.applyExternalForce()
+        bonds.computeBondedForce(dt)
+        bonds.applyBoundaryConditions()
+        it.stage3()
+
+
+def test_bonded_phases_equal_the_oracle_and_the_fused_loop():
+    """dem_bonded_reset, dem_apply_external_force, dem_bonded_force, dem_apply_boundary_conditions
+    and the stages, called one by one on the breaking bar (pulled ends, breakage): every field
+    and the bond slots bit-identical to the oracle and to the fused dem_bonded_run."""
+    case = S.bonded_bar(nx=32, ny=8, nz=4, pull=5.0, nsteps=600)
+    st, b, status = _oracle(case, 600)
+    assert int(b.broken.sum()) > 0
+    phased = api.bonded_from_case(case)
+    _phase_loop(phased, case["dt"], 600)
+    _compare(phased, st, b, "phases")
+    fused = api.bonded_from_case(case)
+    fused.run_steps(600)
+    _compare(fused, st, b, "fused")
+
+
+def test_bonded_phases_two_particle_reference_case():
+    case = S.bdem_two_particles()
+    st, b, status = _oracle(case, 1500)
+    bonds = api.bonded_from_case(case)
+    _phase_loop(bonds, case["dt"], 1500)
+    _compare(bonds, st, b, "tst01 phases")
+
+
+def test_bond_slices_upload_round_trip():
+    """dem_bonds_set: every bond slice written back unchanged reads back bit for bit, a
+    modified history acts in the next phase as in the oracle given the same history, and a
+    partner index out of range is refused."""
+    case = S.bonded_bar(nx=16, ny=4, nz=4, pull=5.0, nsteps=200)
+    bonds = api.bonded_from_case(case)
+    bonds.run_steps(100)
+    before = {k: bonds.get(k) for k in ("idx", "count", "init_len", "broken") + HIST}
+    for k, v in before.items():
+        bonds.set(k, v)
+    for k, v in before.items():
+        assert np.array_equal(bonds.get(k), v), k
+    # scale the tangential bond force history, then one more phase loop step on both sides
+    st = bonds.solver.particles.download()
+    ob = case["bonds"].copy()
+    ob.idx[:], ob.count[:], ob.init_len[:], ob.broken[:] = before["idx"], before["count"], before["init_len"], before["broken"]
+    for k in HIST:
+        ob.hist[k][:] = before[k] * (1.5 if k.startswith("ft") else 1.0)
+    bonds.set("ft_x", ob.hist["ft_x"])
+    bonds.set("ft_y", ob.hist["ft_y"])
+    bonds.set("ft_z", ob.hist["ft_z"])
+    O.bonded_run(st, ob, case["bparams"], case["dt"], 1, ext_force=case["ext_force"], fix_flags=case["fix_flags"],
+                 pow_mode=O.POW_SQRT)
+    _phase_loop(bonds, case["dt"], 1)
+    _compare(bonds, st, ob, "after set")
+    bad = before["idx"].copy()
+    bad[0, 0] = case["state"].n
+    with pytest.raises(api.DemError):
+        bonds.set("idx", bad)
