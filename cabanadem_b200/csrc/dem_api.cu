@@ -1774,6 +1774,13 @@ extern "C" int dem_nn_mlp_backward(dem_ctx *ctx, const dem_nn_mlp *m, long rows,
     return DEM_OK;
 }
 
+extern "C" int dem_nn_debug_waits(dem_ctx *ctx, int poll_limit, int drop_mma) {
+    if (!ctx || poll_limit < 0) return DEM_ERR_INVALID;
+    const int st = nn_debug_waits(poll_limit, drop_mma, ctx->stream);
+    if (st) return fail(ctx, st, "dem_nn_debug_waits: cannot set the wait bounds");
+    return DEM_OK;
+}
+
 extern "C" int dem_nn_status(dem_ctx *ctx, int *status) {
     if (!ctx || !status) return DEM_ERR_INVALID;
     *status = 0;

@@ -242,6 +242,7 @@ int nn_mlp_backward(const dem_nn_mlp &m, long rows, const dem_nn_rows *src, int 
                     void *dz1, float *dx, float *g_w1t, int ld_w1, float *g_b1, float *g_w2t, float *g_b2,
                     float *part, int *err, cudaStream_t s);
 long nn_wgrad_scratch(int kin, int nout);
+int nn_debug_waits(int poll_limit, int drop_mma, cudaStream_t s);
 // factorised edge layer of the surrogate (dem_nn.cu)
 int nn_linear_pq(long rows, const void *h, const void *w1ij_t, void *pq, int *err, cudaStream_t s);
 int nn_linear_pq_backward(long rows, const void *dpq, const void *w1ij, float *dh, int *err, cudaStream_t s);

@@ -161,7 +161,32 @@ __device__ __forceinline__ uint32_t tc_setup(uint64_t *mbar, uint32_t *tslot, in
     return *tslot;
 }
 
-__device__ __forceinline__ void tc_teardown(uint32_t tm, int ncols, bool ok, int *err) {
+// Bounded waits of the tensor-core kernels: polls of mbarrier.try_wait per wait, and a
+// diagnostic switch under which the kernels issue no MMA and no commit (so every wait runs
+// out with nothing in flight).  Process-wide per device; set by dem_nn_debug_waits.
+__device__ int g_tc_wait_limit = 1 << 22;
+__device__ int g_tc_drop_mma = 0;
+
+// The elected thread's MMA issue and commit, skipped under the diagnostic switch.
+__device__ __forceinline__ void mma_issue(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+    if (!g_tc_drop_mma) tc::mma_bf16(tmem_d, adesc, bdesc, idesc, accumulate);
+}
+__device__ __forceinline__ void mma_commit_issue(uint64_t *mbar) {
+    if (!g_tc_drop_mma) tc::mma_commit(mbar);
+}
+
+// End of every kernel: free the block's TMEM.  When a wait gave up (ok false), the MMA batch
+// of that wait may still be running and writing TMEM: the block first waits once more, with
+// the same bound, for that batch's commit (parity `phase ^ 1`: mma_wait flipped it), so TMEM
+// is freed after the batch completes.  If that wait gives up too, TMEM is freed anyway and the
+// error word carries DEM_ERR_TIMEOUT; the host learns of it from dem_nn_status.
+__device__ __forceinline__ void tc_teardown(uint32_t tm, int ncols, bool ok, int *err, uint64_t *mbar,
+                                            uint32_t phase) {
+    if (!ok) {
+        if (threadIdx.x == 0) (void)tc::mbar_wait(mbar, phase ^ 1u, g_tc_wait_limit);
+        __syncthreads();
+    }
     tc::fence_before_sync();
     __syncthreads();
     if (threadIdx.x < 32) {
@@ -173,7 +198,7 @@ __device__ __forceinline__ void tc_teardown(uint32_t tm, int ncols, bool ok, int
 
 // All threads wait for the MMA batch committed last; uniform result across the block.
 __device__ __forceinline__ bool mma_wait(uint64_t *mbar, uint32_t &phase) {
-    const bool ok = tc::mbar_wait(mbar, phase);
+    const bool ok = tc::mbar_wait(mbar, phase, g_tc_wait_limit);
     phase ^= 1u;
     const bool all = __syncthreads_and(ok) != 0;
     tc::fence_after_sync();
@@ -243,8 +268,8 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_mlp_fwd(FwdArgs a) {
         if (tid == 0) {
             tc::fence_after_sync();
             for (int ks = 0; ks < KIN / 16; ++ks)
-                tc::mma_bf16(tm, tc::kmajor_desc(aA, kRows, ks), tc::kmajor_desc(aW1, kHidden, ks), id1, ks > 0);
-            tc::mma_commit(mbar);
+                mma_issue(tm, tc::kmajor_desc(aA, kRows, ks), tc::kmajor_desc(aW1, kHidden, ks), id1, ks > 0);
+            mma_commit_issue(mbar);
         }
         ok = mma_wait(mbar, phase);
         if (!ok) break;
@@ -273,8 +298,8 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_mlp_fwd(FwdArgs a) {
         if (tid == 0) {
             tc::fence_after_sync();
             for (int ks = 0; ks < kHidden / 16; ++ks)
-                tc::mma_bf16(tm, tc::kmajor_desc(aH, kRows, ks), tc::kmajor_desc(aW2, NOUT, ks), id2, ks > 0);
-            tc::mma_commit(mbar);
+                mma_issue(tm, tc::kmajor_desc(aH, kRows, ks), tc::kmajor_desc(aW2, NOUT, ks), id2, ks > 0);
+            mma_commit_issue(mbar);
         }
         ok = mma_wait(mbar, phase);
         if (!ok) break;
@@ -328,7 +353,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_mlp_fwd(FwdArgs a) {
             __syncthreads();
         }
     }
-    tc_teardown(tm, 128, ok, a.err);
+    tc_teardown(tm, 128, ok, a.err, mbar, phase);
 }
 
 // ------------------------------------------------------------------------------------
@@ -383,8 +408,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_bwd(BwdArgs a) {
         if (t == 0) {
             tc::fence_after_sync();
             for (int ks = 0; ks < NOUT / 16; ++ks)
-                tc::mma_bf16(tm, tc::kmajor_desc(aY, kRows, ks), tc::kmajor_desc(aW2, kHidden, ks), id1, ks > 0);
-            tc::mma_commit(mbar);
+                mma_issue(tm, tc::kmajor_desc(aY, kRows, ks), tc::kmajor_desc(aW2, kHidden, ks), id1, ks > 0);
+            mma_commit_issue(mbar);
         }
         ok = mma_wait(mbar, phase);
         if (!ok) break;
@@ -416,9 +441,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_bwd(BwdArgs a) {
                 tc::fence_after_sync();
                 for (int j = 0; j < KIN / NX; ++j)   // N chunk j: input features [j*NX, j*NX + NX)
                     for (int ks = 0; ks < kHidden / 16; ++ks)
-                        tc::mma_bf16(tm + kHidden + j * NX, tc::kmajor_desc(aZ, kRows, ks),
+                        mma_issue(tm + kHidden + j * NX, tc::kmajor_desc(aZ, kRows, ks),
                                      tc::kmajor_desc(aW1 + (uint32_t)(j * NX * 16), KIN, ks), idx, ks > 0);
-                tc::mma_commit(mbar);
+                mma_commit_issue(mbar);
             }
             ok = mma_wait(mbar, phase);
             if (!ok) break;
@@ -434,7 +459,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_bwd(BwdArgs a) {
         tc::fence_before_sync();
         __syncthreads();
     }
-    tc_teardown(tm, 512, ok, a.err);
+    tc_teardown(tm, 512, ok, a.err, mbar, phase);
 }
 
 // ------------------------------------------------------------------------------------
@@ -499,18 +524,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_wgrad(WgradArgs a) {
             tc::fence_after_sync();
             for (int j = 0; j < KIN / NX; ++j)   // dW1^T[:, j*NX .. ] += dZ^T X_j
                 for (int ks = 0; ks < kRows / 16; ++ks)
-                    tc::mma_bf16(tm + j * NX, tc::mnmajor_desc(aZ, kRows, ks),
+                    mma_issue(tm + j * NX, tc::mnmajor_desc(aZ, kRows, ks),
                                  tc::mnmajor_desc(aX + (uint32_t)(j * (NX / 8) * kRows * 16), kRows, ks), idx,
                                  (!first || ks > 0) ? 1u : 0u);
             for (int ks = 0; ks < kRows / 16; ++ks) {
                 if (NOUT == kHidden)   // dW2^T += dY^T H
-                    tc::mma_bf16(tm + KIN, tc::mnmajor_desc(aY, kRows, ks), tc::mnmajor_desc(aH, kRows, ks), id2,
+                    mma_issue(tm + KIN, tc::mnmajor_desc(aY, kRows, ks), tc::mnmajor_desc(aH, kRows, ks), id2,
                                  (!first || ks > 0) ? 1u : 0u);
                 else                   // dW2 += H^T dY (M = 128 hidden, N = NOUT)
-                    tc::mma_bf16(tm + KIN, tc::mnmajor_desc(aH, kRows, ks), tc::mnmajor_desc(aY, kRows, ks), id2,
+                    mma_issue(tm + KIN, tc::mnmajor_desc(aH, kRows, ks), tc::mnmajor_desc(aY, kRows, ks), id2,
                                  (!first || ks > 0) ? 1u : 0u);
             }
-            tc::mma_commit(mbar);
+            mma_commit_issue(mbar);
         }
         // bias sums from the staged tiles while the tensor core runs (fixed row order)
         for (int r = 0; r < kRows; ++r) {
@@ -537,7 +562,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_wgrad(WgradArgs a) {
     }
     dst[NC - 2] = db1;
     dst[NC - 1] = t < NOUT ? db2 : 0.f;
-    tc_teardown(tm, TC, ok, a.err);
+    tc_teardown(tm, TC, ok, a.err, mbar, phase);
 }
 
 // Sum the per-CTA partials in block order and add them to the gradient buffers:
@@ -604,8 +629,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_linear(LinArgs a) {
         if (t == 0) {
             tc::fence_after_sync();
             for (int ks = 0; ks < KIN / 16; ++ks)
-                tc::mma_bf16(tm, tc::kmajor_desc(aA, kRows, ks), tc::kmajor_desc(aW, NOUT, ks), id, ks > 0);
-            tc::mma_commit(mbar);
+                mma_issue(tm, tc::kmajor_desc(aA, kRows, ks), tc::kmajor_desc(aW, NOUT, ks), id, ks > 0);
+            mma_commit_issue(mbar);
         }
         ok = mma_wait(mbar, phase);
         if (!ok) break;
@@ -633,7 +658,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_linear(LinArgs a) {
         tc::fence_before_sync();
         __syncthreads();
     }
-    tc_teardown(tm, TC, ok, a.err);
+    tc_teardown(tm, TC, ok, a.err, mbar, phase);
 }
 
 struct EdgeArgs {
@@ -699,8 +724,8 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_edge_fwd(EdgeArgs a) {
         if (tid == 0) {
             tc::fence_after_sync();
             for (int ks = 0; ks < kHidden / 16; ++ks)
-                tc::mma_bf16(tm, tc::kmajor_desc(aA, kRows, ks), tc::kmajor_desc(aW1, kHidden, ks), id, ks > 0);
-            tc::mma_commit(mbar);
+                mma_issue(tm, tc::kmajor_desc(aA, kRows, ks), tc::kmajor_desc(aW1, kHidden, ks), id, ks > 0);
+            mma_commit_issue(mbar);
         }
         ok = mma_wait(mbar, phase);
         if (!ok) break;
@@ -736,8 +761,8 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_edge_fwd(EdgeArgs a) {
         if (tid == 0) {
             tc::fence_after_sync();
             for (int ks = 0; ks < kHidden / 16; ++ks)
-                tc::mma_bf16(tm, tc::kmajor_desc(aA, kRows, ks), tc::kmajor_desc(aW2, kHidden, ks), id, ks > 0);
-            tc::mma_commit(mbar);
+                mma_issue(tm, tc::kmajor_desc(aA, kRows, ks), tc::kmajor_desc(aW2, kHidden, ks), id, ks > 0);
+            mma_commit_issue(mbar);
         }
         {   // residual half row while the second product runs
             const uint4 *es = reinterpret_cast<const uint4 *>(a.e + (live ? grow : 0) * kHidden + half * 64);
@@ -767,7 +792,7 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_edge_fwd(EdgeArgs a) {
         copy_out(sA, a.out, row0, a.rows);
         __syncthreads();
     }
-    tc_teardown(tm, 128, ok, a.err);
+    tc_teardown(tm, 128, ok, a.err, mbar, phase);
 }
 
 // dW^T [256][128] partials: D_half[o][k] = sum_rows A[row][128 half + o] B[row][k]
@@ -802,9 +827,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_linear_wgrad(LinWgradArgs a) {
             tc::fence_after_sync();
             for (int h = 0; h < 2; ++h)
                 for (int ks = 0; ks < kRows / 16; ++ks)
-                    tc::mma_bf16(tm + h * kHidden, tc::mnmajor_desc(aA + (uint32_t)(h * 16 * kRows * 16), kRows, ks),
+                    mma_issue(tm + h * kHidden, tc::mnmajor_desc(aA + (uint32_t)(h * 16 * kRows * 16), kRows, ks),
                                  tc::mnmajor_desc(aB, kRows, ks), id, (!first || ks > 0) ? 1u : 0u);
-            tc::mma_commit(mbar);
+            mma_commit_issue(mbar);
         }
         ok = mma_wait(mbar, phase);
         first = false;
@@ -822,7 +847,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_linear_wgrad(LinWgradArgs a) {
     } else {
         for (int c = 0; c < 256; ++c) dst[c] = 0.f;
     }
-    tc_teardown(tm, 256, ok, a.err);
+    tc_teardown(tm, 256, ok, a.err, mbar, phase);
 }
 
 // g[o * ld + col0 + c] += sum over blocks of part[b][o][c]   (o < 128, c < 256)
@@ -962,6 +987,16 @@ int nn_edge_forward(long rows, const void *e, const void *pq, const int *recv, c
 long nn_linear_wgrad_scratch() { return 148L * kRows * 256; }
 
 // Scratch floats the per-CTA weight-gradient partials of one backward call need.
+int nn_debug_waits(int poll_limit, int drop_mma, cudaStream_t s) {
+    const int lim = poll_limit > 0 ? poll_limit : (1 << 22);
+    const int drop = drop_mma ? 1 : 0;
+    if (cudaMemcpyToSymbolAsync(g_tc_wait_limit, &lim, sizeof(int), 0, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyToSymbolAsync(g_tc_drop_mma, &drop, sizeof(int), 0, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return DEM_ERR_CUDA;
+    return DEM_OK;
+}
+
 long nn_wgrad_scratch(int kin, int nout) {
     const int nw2 = nout == kHidden ? kHidden : nout;
     return 148L * kRows * (kin + nw2 + 2);

@@ -380,6 +380,15 @@ int dem_nn_mlp_backward(dem_ctx *ctx, const dem_nn_mlp *m, long rows, const dem_
 /* Device error word of the context's tensor-core kernels (DEM_ERR_TIMEOUT when a bounded
  * wait gave up); synchronises, returns it in *status and clears it. */
 int dem_nn_status(dem_ctx *ctx, int *status);
+/* Bounds of the tensor-core kernels' waits, for testing that a wait which runs out is
+ * reported and leaves the context usable (no reference counterpart).  poll_limit: polls of
+ * the MMA-completion barrier per wait (0 = the default, about 4 million, seconds of waiting);
+ * drop_mma != 0: the kernels issue no MMA and no commit, so every wait runs out with nothing
+ * in flight (their outputs are then not written).  A block whose wait ran out waits once more,
+ * with the same bound, for the MMA batch it was waiting on before it frees its tensor memory,
+ * and sets DEM_ERR_TIMEOUT in the word dem_nn_status returns.  The setting is per device and
+ * process-wide; it takes effect for kernels queued after the call. */
+int dem_nn_debug_waits(dem_ctx *ctx, int poll_limit, int drop_mma);
 
 /* ---- Learned surrogate: message-passing network over the contact graph -------------------
  * Quasi-2D (x, y) particles.  One network stride replaces `steps_per_stride` DEM steps:

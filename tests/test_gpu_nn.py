@@ -123,3 +123,36 @@ def test_backward_is_deterministic():
     for a, b in zip(*got):
         assert np.array_equal(a, b)
     ctx.close()
+
+
+def test_wait_that_runs_out_is_reported_and_the_next_call_succeeds():
+    """A bounded wait that runs out: with dem_nn_debug_waits(drop_mma=1) the kernels issue no
+    MMA and no commit, so each block's wait on the completion barrier gives up after the poll
+    limit (nothing is in flight, nothing faults).  The call reports DEM_ERR_TIMEOUT through
+    dem_nn_status, and with the default bounds restored the same layer runs and matches the
+    FP32 reference: the context stayed usable and no tensor memory was left allocated."""
+    from cabanadem_b200 import _lib
+    dev = torch.device("cuda:0")
+    ctx = api.Context(0)
+    gen = torch.Generator().manual_seed(11)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr())
+    rows = 148 * 128 + 77
+    L = _lib.lib()
+    with torch.cuda.stream(stream):
+        m = nn.Mlp(128, 128, dev, gen)
+        srcs = _sources(128, rows, gen, dev)
+        out32 = torch.full((rows, 128), 7.0, device=dev, dtype=torch.float32)
+        assert L.dem_nn_debug_waits(ctx.h, 1000, 1) == 0
+        try:
+            m.forward(ctx, rows, srcs, out_f32=out32)
+            assert nn.status(ctx) == 0x020           # DEM_ERR_TIMEOUT
+            assert bool((out32 == 7.0).all())        # no block got past its first wait
+        finally:
+            assert L.dem_nn_debug_waits(ctx.h, 0, 0) == 0
+        m.forward(ctx, rows, srcs, out_f32=out32)
+        assert nn.status(ctx) == 0
+        x = _gather(srcs)
+        h = torch.relu(x @ m.w1t_bf.float().t() + m.b1).to(torch.bfloat16).float()
+        ref = h @ m.w2t_bf.float().t() + m.b2
+        assert (out32 - ref).abs().max().item() <= 1e-2 * ref.abs().max().item()
+    ctx.close()
