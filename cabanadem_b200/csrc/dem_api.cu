@@ -86,6 +86,7 @@ struct dem_solver {
     long launches = 0;  // kernels launched (graph nodes counted per replay)
     long graph_nodes = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;   // around each step-graph replay
+    AuxStream aux;                              // second branch of the split streaming pass
     double graph_ms = 0.0;                      // device time of the replays
     long graph_steps_run = 0;                   // steps those replays advanced
     int graph_done_mark = 0;                    // steps_done before the current replay
@@ -821,6 +822,7 @@ int prepare(dem_solver *s) {
     fc.has_fix = p->any_fix ? 1 : 0;
     fc.mixed = s->sp.precision == DEM_MIXED ? 1 : 0;
     fc.stream_block = (s->sp.stream_block == 64 || s->sp.stream_block == 256) ? s->sp.stream_block : 128;
+    fc.split = (s->sp.stream_split >= 1 && s->sp.stream_split <= 3) ? s->sp.stream_split : 3;
     pick_contact_kernel(s);
     fc.scenes = s->nscenes > 0 ? s->d_scenes : nullptr;
     fc.wps = s->nscenes > 0 ? s->wps : 0;
@@ -917,7 +919,7 @@ int check_walls(dem_solver *s) {
 }
 
 // kernels issued by one launch_build (see dem_nbr.cu)
-long build_kernel_count(bool resort) { return 13 + (resort ? 6 : 0); }
+long build_kernel_count(bool resort) { return 13 + (resort ? 7 : 0); }
 
 // Build with overflow handling (host-driven; re-sorts into Morton order).
 int build_with(dem_solver *s, bool resort, double delta, double skin);
@@ -975,7 +977,7 @@ int capture_graph(dem_solver *s, int steps) {
             launch_build(s->p->P, s->p->alt, s->L, s->B, s->p->ctl, s->sp.delta, s->sp.skin, false, true, ctx->stream);
             if (s->mesh_nt > 0) launch_mesh_candidates(s->p->P, s->fc.mesh, s->p->ctl, s->sp.delta, s->sp.skin, ctx->stream);
         }
-        launch_step(s->p->P, s->L, s->p->ctl, s->fc, s->d_pp, s->d_pw, s->d_walls, MODE_FUSED, ctx->stream);
+        launch_step(s->p->P, s->L, s->p->ctl, s->fc, s->d_pp, s->d_pw, s->d_walls, MODE_FUSED, ctx->stream, s->aux);
     }
     CK(cudaStreamEndCapture(ctx->stream, &g));
     s->graph_nodes = (long)steps * (kernels_per_step(s->fc) +
@@ -1024,6 +1026,9 @@ extern "C" int dem_solver_create(dem_ctx *ctx, dem_particles *p, dem_walls *w, c
     s->nparts = (p->P.n + 127) / 128;
     A(dalloc(&s->d_epart, 4 * (size_t)s->nparts));
     A(dalloc(&s->d_eout, 4));
+    A(cudaStreamCreateWithFlags(&s->aux.stream, cudaStreamNonBlocking));
+    A(cudaEventCreateWithFlags(&s->aux.fork, cudaEventDisableTiming));
+    A(cudaEventCreateWithFlags(&s->aux.join, cudaEventDisableTiming));
     if (e != cudaSuccess) {
         dem_solver_destroy(s);
         return cuda_check(ctx, e, "dem_solver_create");
@@ -1062,6 +1067,12 @@ extern "C" int dem_solver_destroy(dem_solver *s) {
     if (s->graph) cudaGraphExecDestroy(s->graph);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
+    if (s->aux.stream) {
+        cudaStreamSynchronize(s->aux.stream);
+        cudaStreamDestroy(s->aux.stream);
+    }
+    if (s->aux.fork) cudaEventDestroy(s->aux.fork);
+    if (s->aux.join) cudaEventDestroy(s->aux.join);
     cudaFree(s->d_pp); cudaFree(s->d_pw); cudaFree(s->d_walls); cudaFree(s->d_scenes);
     cudaFree(s->L.nn); cudaFree(s->L.idx); cudaFree(s->L.defer); cudaFree(s->L.defer_v); cudaFree(s->L.defer_w);
     BuildBuffers &B = s->B;
@@ -1322,7 +1333,7 @@ extern "C" int dem_solver_profile(dem_solver *s, int nsteps, double *kernel_ms) 
     int done = 0;
     for (int guard = 0; guard < 4 * (nsteps + 4); ++guard) {
         CK(cudaEventRecord(e0, st));
-        launch_step(s->p->P, s->L, s->p->ctl, s->fc, s->d_pp, s->d_pw, s->d_walls, MODE_FUSED, st);
+        launch_step(s->p->P, s->L, s->p->ctl, s->fc, s->d_pp, s->d_pw, s->d_walls, MODE_FUSED, st, s->aux);
         CK(cudaEventRecord(e1, st));
         s->launches += kernels_per_step(s->fc);
         CK(cudaEventSynchronize(e1));

@@ -119,6 +119,9 @@ struct ForceConsts {
     int has_fix;
     int mixed;                 // 1: FP32 contact forces (dem_mixed.cu)
     int stream_block;          // k_stream block size: 64, 128 or 256
+    int split;                 // streaming pass: 1 one kernel over every particle (k_stream);
+                               // 2 the lone particles and the rest in two persistent kernels
+                               // (k_stream_lone, k_stream_rest); 3 the same as concurrent branches
     int dense;                 // 1: most particles are in contact -- contact kernels compiled for
                                // more resident blocks, wider apply grid (same arithmetic)
     int coop;                  // lanes per deferred particle in the contact kernel: 4 or 8
@@ -212,8 +215,14 @@ int kernels_per_step(const ForceConsts &fc);
 void launch_mesh_candidates(const Particles &P, const MeshDev &M, Ctl *ctl, double delta, double skin, cudaStream_t s);
 void launch_permute_mesh(const MeshDev &M, const MeshDev &A, int n, int cap, const int *items, cudaStream_t s);
 void launch_prologue(const Particles &P, Ctl *ctl, const ForceConsts &fc, cudaStream_t s);
+// Second stream and fork/join events for steps whose streaming pass runs as two concurrent
+// graph branches (ForceConsts::split == 3); a null stream runs the branches in sequence.
+struct AuxStream {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+};
 void launch_step(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
-                 const PairConst *pw, const WallGeom *walls, int mode, cudaStream_t s);
+                 const PairConst *pw, const WallGeom *walls, int mode, cudaStream_t s, const AuxStream &aux = AuxStream());
 void launch_stage(const Particles &P, Ctl *ctl, const ForceConsts &fc, int stage, cudaStream_t s);
 // dem_mixed.cu
 void launch_contact_mixed_all(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc,

@@ -359,16 +359,51 @@ __global__ void k_permute(Particles P, Particles A, const Ctl *ctl, const int *i
         A.mat[p] = P.mat[q];
         if (P.scene) A.scene[p] = P.scene[q];
         A.fix[p] = P.fix[q];
-        A.cstate[p] = P.cstate[q];
-        for (int k = 0; k < P.mc; ++k) {
+        const int cs = P.cstate[q];
+        A.cstate[p] = cs;
+        // live history only: the tracked slots below the contact count and the walls whose
+        // history bit is set (every other slot holds -1 / 0, see k_hist_back)
+        const int cnt = cs & 0xff;
+        const unsigned wm = (unsigned)cs >> 8;
+        for (int k = 0; k < cnt; ++k) {
             const int t = P.tidx[(long)k * cap + q];
             A.tidx[(long)k * cap + p] = (t >= 0 && t < n) ? dst[t] : t;
+            for (int d = 0; d < 3; ++d) A.th[((long)d * P.mc + k) * cap + p] = P.th[((long)d * P.mc + k) * cap + q];
         }
-        for (long k = 0; k < 3L * P.mc; ++k) A.th[k * cap + p] = P.th[k * cap + q];
-        for (long k = 0; k < 3L * P.mw; ++k) A.sw[k * cap + p] = P.sw[k * cap + q];
+        for (int w = 0; w < P.mw; ++w)
+            if ((wm >> w) & 1u)
+                for (int d = 0; d < 3; ++d) A.sw[((long)d * P.mw + w) * cap + p] = P.sw[((long)d * P.mw + w) * cap + q];
         const int orig = P.perm[q];
         A.perm[p] = orig;
         P.rank[orig] = p;
+    }
+}
+
+// Re-sort, history back into place: slot p takes the live slots k_permute gathered for its new
+// particle, and the slots its previous particle used beyond them are reset (partner -1,
+// history 0), so that every slot past a particle's contact count, and every wall slot whose
+// history bit is clear, keeps holding -1 / 0 as the contact kernels leave them.  Reads the
+// old contact word at p (P.cstate, before it is replaced by the gathered one).
+__global__ void k_hist_back(Particles P, Particles A) {
+    const int n = P.n, cap = P.cap;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const int nc = A.cstate[p], oc = P.cstate[p];
+        const int ncnt = nc & 0xff, ocnt = oc & 0xff;
+        for (int k = 0; k < ncnt; ++k) {
+            P.tidx[(long)k * cap + p] = A.tidx[(long)k * cap + p];
+            for (int d = 0; d < 3; ++d) P.th[((long)d * P.mc + k) * cap + p] = A.th[((long)d * P.mc + k) * cap + p];
+        }
+        for (int k = ncnt; k < ocnt; ++k) {
+            P.tidx[(long)k * cap + p] = -1;
+            for (int d = 0; d < 3; ++d) P.th[((long)d * P.mc + k) * cap + p] = 0.;
+        }
+        const unsigned nm = (unsigned)nc >> 8, om = (unsigned)oc >> 8;
+        for (int w = 0; w < P.mw; ++w) {
+            if ((nm >> w) & 1u)
+                for (int d = 0; d < 3; ++d) P.sw[((long)d * P.mw + w) * cap + p] = A.sw[((long)d * P.mw + w) * cap + p];
+            else if ((om >> w) & 1u)
+                for (int d = 0; d < 3; ++d) P.sw[((long)d * P.mw + w) * cap + p] = 0.;
+        }
     }
 }
 
@@ -632,11 +667,8 @@ void launch_build(const Particles &P, Particles &alt, const NbrList &L, BuildBuf
         cudaMemcpyAsync(P.mI, alt.mI, 2 * cap * sizeof(double), cudaMemcpyDeviceToDevice, s);
         cudaMemcpyAsync(P.mat, alt.mat, cap, cudaMemcpyDeviceToDevice, s);
         cudaMemcpyAsync(P.fix, alt.fix, cap, cudaMemcpyDeviceToDevice, s);
+        k_hist_back<<<gs, kB, 0, s>>>(P, alt);   // before the contact words are replaced
         cudaMemcpyAsync(P.cstate, alt.cstate, cap * sizeof(int), cudaMemcpyDeviceToDevice, s);
-        cudaMemcpyAsync(P.tidx, alt.tidx, (size_t)P.mc * cap * sizeof(int), cudaMemcpyDeviceToDevice, s);
-        cudaMemcpyAsync(P.th, alt.th, 3 * (size_t)P.mc * cap * sizeof(double), cudaMemcpyDeviceToDevice, s);
-        if (P.mw > 0)
-            cudaMemcpyAsync(P.sw, alt.sw, 3 * (size_t)P.mw * cap * sizeof(double), cudaMemcpyDeviceToDevice, s);
         cudaMemcpyAsync(P.perm, alt.perm, cap * sizeof(int), cudaMemcpyDeviceToDevice, s);
         if (P.scene) cudaMemcpyAsync(P.scene, alt.scene, cap * sizeof(int), cudaMemcpyDeviceToDevice, s);
         k_flip<<<1, 32, 0, s>>>(ctl);

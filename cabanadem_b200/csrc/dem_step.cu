@@ -52,119 +52,209 @@ __device__ __forceinline__ bool step_gate(const Ctl *ctl) {
 // neighbour reads them.  Every other particle is appended to L.defer for kernel 2.
 // Each thread reads the control word itself (no block barrier before the work).
 // ---------------------------------------------------------------------------------------
+
+// Per-step values of the control word every streaming thread needs.
+struct StreamCtl {
+    int cur, vcur, nlone, nclear_end, n;
+    bool last;
+};
+__device__ __forceinline__ StreamCtl stream_ctl(const Ctl *ctl, int n) {
+    StreamCtl c;
+    c.cur = ctl->cur;
+    c.vcur = ctl->vcur;
+    c.nlone = ctl->nlone;
+    // particles [nlone, nclear_end) had every listed neighbour at a gap above skin/2: while
+    // twice the displacement bound stays below skin/2 none of them can touch
+    c.nclear_end = (2.0 * ctl->disp < ctl->half_skin) ? c.nlone + ctl->nclear : c.nlone;
+    c.last = ctl->steps_done + 1 >= ctl->target;
+    c.n = n;
+    return c;
+}
+
+// Appends the deferred lanes of a converged warp to L.defer (one atomic per warp).
+__device__ __forceinline__ void defer_append(Ctl *ctl, const NbrList &L, bool defer, int i) {
+    const unsigned dmask = __ballot_sync(0xffffffffu, defer);
+    if (defer) {
+        const int lane = threadIdx.x & 31;
+        const int leader = __ffs(dmask) - 1;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(&ctl->ndefer, __popc(dmask));
+        base = __shfl_sync(dmask, base, leader);
+        L.defer[base + __popc(dmask & ((1u << lane) - 1u))] = i;
+    }
+}
+
+// The step of particle i without pair force and torque: F = ext (added to zero), the
+// post-force hooks, stage3 of this step and stage1 + stage2 of the next (u in place, x to the
+// next buffer), or F and tau stored after the run's last step.
+__device__ __forceinline__ void stream_free_step(const Particles &P, const ForceConsts &fc, const StreamCtl &c,
+                                                 double *vc, int i, const D4 &pi, double m, double ui0, double ui1,
+                                                 double ui2, double &vmax2) {
+    const int cap = P.cap;
+    double F0 = 0., F1 = 0., F2 = 0.;
+    if (fc.has_ext) {
+        F0 += P.ext[i];
+        F1 += P.ext[cap + i];
+        F2 += P.ext[2 * cap + i];
+    }
+    if (fc.has_gravity) {
+        F0 += m * fc.g[0];
+        F1 += m * fc.g[1];
+        F2 += m * fc.g[2];
+    }
+    if (fc.has_fix && (P.fix[i] & DEM_FIX_FORCE)) F0 = F1 = F2 = 0.;
+    const double m_inverse = 1. / m;
+    const double h = fc.half_dt;
+    ui0 += h * F0 * m_inverse;
+    ui1 += h * F1 * m_inverse;
+    ui2 += h * F2 * m_inverse;
+    D4 pn = pi;
+    if (c.last) {
+        P.force[i] = F0;
+        P.force[cap + i] = F1;
+        P.force[2 * cap + i] = F2;
+        P.torque[i] = 0.;
+        P.torque[cap + i] = 0.;
+        P.torque[2 * cap + i] = 0.;
+    } else {
+        ui0 += h * F0 * m_inverse;
+        ui1 += h * F1 * m_inverse;
+        ui2 += h * F2 * m_inverse;
+        pn.x += fc.dt * ui0;
+        pn.y += fc.dt * ui1;
+        pn.z += fc.dt * ui2;
+        vmax2 = fmax(vmax2, ui0 * ui0 + ui1 * ui1 + ui2 * ui2);
+    }
+    st4(P.pos[c.cur ^ 1], i, pn);
+    vc[i] = ui0;
+    vc[cap + i] = ui1;
+    vc[2 * cap + i] = ui2;
+}
+
+// A particle whose only contact candidates are the walls (and the mesh): defer when it has
+// tracked contacts, mesh candidates or a wall overlap.
+__device__ __forceinline__ bool wall_defer(const Particles &P, const ForceConsts &fc,
+                                           const WallGeom *__restrict__ walls, int i, const D4 &pi, bool defer) {
+    // a particle near the mesh (candidates) or with a tracked triangle contact takes the full step
+    if (!defer && fc.mesh.nt) defer = (fc.mesh.ncand[i] | fc.mesh.cnt[i]) != 0;
+    const int scene_i = P.scene ? P.scene[i] : 0;
+    const int wall0 = fc.wps ? scene_i * fc.wps : 0;
+    const int wall1 = fc.wps ? wall0 + fc.wps : fc.nwall;
+    for (int w = wall0; w < wall1 && !defer; ++w) {
+        const WallGeom &g = walls[w];   // point and normal only (the velocity is not needed here)
+        const double tmp = (pi.x - __ldg(&g.x[0])) * __ldg(&g.n[0]) + (pi.y - __ldg(&g.x[1])) * __ldg(&g.n[1]) +
+                           (pi.z - __ldg(&g.x[2])) * __ldg(&g.n[2]);
+        defer = (pi.w - tmp) > 0.;
+    }
+    return defer;
+}
+
+// Streaming body for one particle i (any class); returns whether it is deferred.
+__device__ __forceinline__ bool stream_particle(const Particles &P, const NbrList &L, const ForceConsts &fc,
+                                                const WallGeom *__restrict__ walls, const StreamCtl &c, int i,
+                                                double &vmax2) {
+    const int cap = P.cap;
+    const double4 *__restrict__ pc = P.pos[c.cur];
+    double *vc = P.vel[c.vcur];
+    // all own-state loads first (one memory round trip per particle)
+    const D4 pi = ld4_early(pc, i);
+    const int cs = ld_early_i(P.cstate + i);
+    // the re-sort placed particles without listed neighbours first: their lists stay empty
+    // until the next build, so neither the list nor a partner is read (one round trip)
+    const bool lone = i < c.nlone;
+    const int nn = lone ? 0 : ld_early_i(L.nn + i);
+    const double m = ld_early(&P.mI[i]);
+    const double ui0 = ld_early(vc + i), ui1 = ld_early(vc + cap + i), ui2 = ld_early(vc + 2 * cap + i);
+    // the first two list slots are read with the own state (in bounds for every i; the
+    // value is only used below the list length), so that most warps need one more
+    // round trip (the partners' positions) instead of two per neighbour
+    const int j0 = (!lone && L.maxnb > 0) ? ld_early_i(L.idx + i) : 0;
+    const int j1 = (!lone && L.maxnb > 1) ? ld_early_i(L.idx + cap + i) : 0;
+    bool defer = cs != 0;
+    if (!defer && nn > 0 && i >= c.nclear_end) {
+        const D4 pa = ld4(pc, j0);
+        D4 pb = pa;
+        if (nn > 1) pb = ld4(pc, j1);
+        const double ax = pi.x - pa.x, ay = pi.y - pa.y, az = pi.z - pa.z;
+        const double sa = pi.w + pa.w;
+        defer = !(ax * ax + ay * ay + az * az >= sa * sa * 1.0000000001);
+        if (nn > 1) {
+            const double bx = pi.x - pb.x, by = pi.y - pb.y, bz = pi.z - pb.z;
+            const double sb = pi.w + pb.w;
+            defer = defer || !(bx * bx + by * by + bz * bz >= sb * sb * 1.0000000001);
+        }
+    }
+    for (int kk = 2; kk < nn && !defer && i >= c.nclear_end; ++kk) {
+        const int j = L.idx[(long)kk * cap + i];
+        const D4 pj = ld4(pc, j);
+        const double px = pi.x - pj.x, py = pi.y - pj.y, pz = pi.z - pj.z;
+        const double r2ij = px * px + py * py + pz * pz;
+        const double sr = pi.w + pj.w;
+        defer = !(r2ij >= sr * sr * 1.0000000001);
+    }
+    defer = wall_defer(P, fc, walls, i, pi, defer);
+    if (!defer) stream_free_step(P, fc, c, vc, i, pi, m, ui0, ui1, ui2, vmax2);
+    return defer;
+}
+
 // Block size is a run-time choice (dem_solver_params.stream_block): 64 x 16, 128 x 10 or
 // 256 x 4 blocks per SM (register caps 64, 48, 64).  On the 2M lattice 128 x 10 was fastest in a
-// B200 sweep; the autotuner picks per workload.
+// B200 sweep; the autotuner picks per workload.  One thread per particle, every particle.
 template <int BS, int MINB>
 __global__ void __launch_bounds__(BS, MINB) k_stream(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
                                                      const WallGeom *__restrict__ walls) {
     if (!step_gate(ctl)) return;
-    const int cur = ctl->cur, vcur = ctl->vcur, nlone = ctl->nlone;
-    // particles [nlone, nclear_end) had every listed neighbour at a gap above skin/2: while
-    // twice the displacement bound stays below skin/2 none of them can touch
-    const int nclear_end = (2.0 * ctl->disp < ctl->half_skin) ? nlone + ctl->nclear : nlone;
-    const bool last = ctl->steps_done + 1 >= ctl->target;
-    const int nxt = cur ^ 1, cap = P.cap;
-    const double4 *__restrict__ pc = P.pos[cur];
-    double *vc = P.vel[vcur];
+    const StreamCtl c = stream_ctl(ctl, P.n);
     double vmax2 = 0.0;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < P.n) {
-        // all own-state loads first (one memory round trip per particle)
-        const D4 pi = ld4_early(pc, i);
-        const int cs = ld_early_i(P.cstate + i);
-        // the re-sort placed particles without listed neighbours first: their lists stay empty
-        // until the next build, so neither the list nor a partner is read (one round trip)
-        const bool lone = i < nlone;
-        const int nn = lone ? 0 : ld_early_i(L.nn + i);
-        const double m = ld_early(&P.mI[i]);
-        double ui0 = ld_early(vc + i), ui1 = ld_early(vc + cap + i), ui2 = ld_early(vc + 2 * cap + i);
-        // the first two list slots are read with the own state (in bounds for every i; the
-        // value is only used below the list length), so that most warps need one more
-        // round trip (the partners' positions) instead of two per neighbour
-        const int j0 = (!lone && L.maxnb > 0) ? ld_early_i(L.idx + i) : 0;
-        const int j1 = (!lone && L.maxnb > 1) ? ld_early_i(L.idx + cap + i) : 0;
-        bool defer = cs != 0;
-        if (!defer && nn > 0 && i >= nclear_end) {
-            const D4 pa = ld4(pc, j0);
-            D4 pb = pa;
-            if (nn > 1) pb = ld4(pc, j1);
-            const double ax = pi.x - pa.x, ay = pi.y - pa.y, az = pi.z - pa.z;
-            const double sa = pi.w + pa.w;
-            defer = !(ax * ax + ay * ay + az * az >= sa * sa * 1.0000000001);
-            if (nn > 1) {
-                const double bx = pi.x - pb.x, by = pi.y - pb.y, bz = pi.z - pb.z;
-                const double sb = pi.w + pb.w;
-                defer = defer || !(bx * bx + by * by + bz * bz >= sb * sb * 1.0000000001);
-            }
+    bool defer = false;
+    if (i < P.n) defer = stream_particle(P, L, fc, walls, c, i, vmax2);
+    defer_append(ctl, L, defer, i);
+    warp_vmax(ctl, P.vslots, vmax2, 0);
+}
+
+// Split streaming pass, part 1: the particles [0, nlone) the last re-sort placed first (no
+// listed neighbour until the next build).  Persistent grid-stride loop over that range; per
+// particle only the own state is read (position, radius, contact word, mass, velocity), so
+// the kernel is compiled for the full 64 warps per SM.
+template <int BS>
+__global__ void __launch_bounds__(BS, 1536 / BS) k_stream_lone(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
+                                                               const WallGeom *__restrict__ walls) {
+    if (!step_gate(ctl)) return;
+    const StreamCtl c = stream_ctl(ctl, P.n);
+    const int cap = P.cap;
+    const double4 *__restrict__ pc = P.pos[c.cur];
+    double *vc = P.vel[c.vcur];
+    double vmax2 = 0.0;
+    for (int base = blockIdx.x * BS; base < c.nlone; base += gridDim.x * BS) {   // block-uniform
+        const int i = base + threadIdx.x;
+        bool defer = false;
+        if (i < c.nlone) {
+            const D4 pi = ld4_early(pc, i);
+            const int cs = ld_early_i(P.cstate + i);
+            const double m = ld_early(&P.mI[i]);
+            const double ui0 = ld_early(vc + i), ui1 = ld_early(vc + cap + i), ui2 = ld_early(vc + 2 * cap + i);
+            defer = wall_defer(P, fc, walls, i, pi, cs != 0);
+            if (!defer) stream_free_step(P, fc, c, vc, i, pi, m, ui0, ui1, ui2, vmax2);
         }
-        for (int kk = 2; kk < nn && !defer && i >= nclear_end; ++kk) {
-            const int j = L.idx[(long)kk * cap + i];
-            const D4 pj = ld4(pc, j);
-            const double px = pi.x - pj.x, py = pi.y - pj.y, pz = pi.z - pj.z;
-            const double r2ij = px * px + py * py + pz * pz;
-            const double sr = pi.w + pj.w;
-            defer = !(r2ij >= sr * sr * 1.0000000001);
-        }
-        // a particle near the mesh (candidates) or with a tracked triangle contact takes the full step
-        if (!defer && fc.mesh.nt) defer = (fc.mesh.ncand[i] | fc.mesh.cnt[i]) != 0;
-        const int scene_i = P.scene ? P.scene[i] : 0;
-        const int wall0 = fc.wps ? scene_i * fc.wps : 0;
-        const int wall1 = fc.wps ? wall0 + fc.wps : fc.nwall;
-        for (int w = wall0; w < wall1 && !defer; ++w) {
-            const WallGeom g = walls[w];
-            const double tmp = (pi.x - g.x[0]) * g.n[0] + (pi.y - g.x[1]) * g.n[1] + (pi.z - g.x[2]) * g.n[2];
-            defer = (pi.w - tmp) > 0.;
-        }
-        const unsigned dmask = __ballot_sync(__activemask(), defer);
-        if (defer) {
-            const int lane = threadIdx.x & 31;
-            const int leader = __ffs(dmask) - 1;
-            int base = 0;
-            if (lane == leader) base = atomicAdd(&ctl->ndefer, __popc(dmask));
-            base = __shfl_sync(dmask, base, leader);
-            L.defer[base + __popc(dmask & ((1u << lane) - 1u))] = i;
-        } else {
-            // no pair force: F = ext (added to zero), then the post-force hooks; tau = 0
-            double F0 = 0., F1 = 0., F2 = 0.;
-            if (fc.has_ext) {
-                F0 += P.ext[i];
-                F1 += P.ext[cap + i];
-                F2 += P.ext[2 * cap + i];
-            }
-            if (fc.has_gravity) {
-                F0 += m * fc.g[0];
-                F1 += m * fc.g[1];
-                F2 += m * fc.g[2];
-            }
-            if (fc.has_fix && (P.fix[i] & DEM_FIX_FORCE)) F0 = F1 = F2 = 0.;
-            const double m_inverse = 1. / m;
-            const double h = fc.half_dt;
-            ui0 += h * F0 * m_inverse;
-            ui1 += h * F1 * m_inverse;
-            ui2 += h * F2 * m_inverse;
-            D4 pn = pi;
-            if (last) {
-                P.force[i] = F0;
-                P.force[cap + i] = F1;
-                P.force[2 * cap + i] = F2;
-                P.torque[i] = 0.;
-                P.torque[cap + i] = 0.;
-                P.torque[2 * cap + i] = 0.;
-            } else {
-                ui0 += h * F0 * m_inverse;
-                ui1 += h * F1 * m_inverse;
-                ui2 += h * F2 * m_inverse;
-                pn.x += fc.dt * ui0;
-                pn.y += fc.dt * ui1;
-                pn.z += fc.dt * ui2;
-                vmax2 = ui0 * ui0 + ui1 * ui1 + ui2 * ui2;
-            }
-            st4(P.pos[nxt], i, pn);
-            vc[i] = ui0;
-            vc[cap + i] = ui1;
-            vc[2 * cap + i] = ui2;
-        }
+        defer_append(ctl, L, defer, i);
+    }
+    warp_vmax(ctl, P.vslots, vmax2, 0);
+}
+
+// Split streaming pass, part 2: the particles [nlone, n), persistent grid-stride loop, the
+// body of k_stream.
+template <int BS, int MINB>
+__global__ void __launch_bounds__(BS, MINB) k_stream_rest(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
+                                                          const WallGeom *__restrict__ walls) {
+    if (!step_gate(ctl)) return;
+    const StreamCtl c = stream_ctl(ctl, P.n);
+    double vmax2 = 0.0;
+    for (int base = c.nlone + blockIdx.x * BS; base < P.n; base += gridDim.x * BS) {   // block-uniform
+        const int i = base + threadIdx.x;
+        bool defer = false;
+        if (i < P.n) defer = stream_particle(P, L, fc, walls, c, i, vmax2);
+        defer_append(ctl, L, defer, i);
     }
     warp_vmax(ctl, P.vslots, vmax2, 0);
 }
@@ -432,7 +522,7 @@ void launch_prologue(const Particles &P, Ctl *ctl, const ForceConsts &fc, cudaSt
     k_prologue<<<nblocks(P.n), kBlock, 0, s>>>(P, ctl, fc);
 }
 
-int kernels_per_step(const ForceConsts &fc) { return fc.all ? 1 : 3; }
+int kernels_per_step(const ForceConsts &fc) { return fc.all ? 1 : (fc.split >= 2 ? 4 : 3); }
 
 static int persistent_blocks(const void *kernel, int block, int n) {
     static int sms = 0;
@@ -451,7 +541,7 @@ static int persistent_blocks(const void *kernel, int block, int n) {
 
 template <bool MESH>
 static void launch_step_t(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
-                 const PairConst *pw, const WallGeom *walls, int mode, cudaStream_t s) {
+                 const PairConst *pw, const WallGeom *walls, int mode, cudaStream_t s, const AuxStream &aux) {
     if (mode == MODE_FUSED && fc.all) {
         static int ga = 0, gma = 0, last_na = -1;
         if (last_na != P.n) {
@@ -480,7 +570,30 @@ static void launch_step_t(const Particles &P, const NbrList &L, Ctl *ctl, const 
             gkm8 = persistent_blocks(contact_mixed_kernel(0, 8, MESH), kBlock, 8 * P.n);
             last_n = P.n;
         }
-        if (fc.stream_block == 64)
+        if (fc.split >= 2) {
+            // lone particles and the rest in two persistent kernels; with the concurrent form
+            // (split 3, an aux stream given) as two graph branches whose grids share the SMs
+            static int sms = 0;
+            if (!sms) {
+                int dev = 0;
+                cudaGetDevice(&dev);
+                cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+                if (sms <= 0) sms = 148;
+            }
+            const bool conc = fc.split == 3 && aux.stream;
+            const int glone = sms * (conc ? 7 : 12), grest = sms * (conc ? 5 : 9);
+            if (conc) {
+                cudaEventRecord(aux.fork, s);
+                cudaStreamWaitEvent(aux.stream, aux.fork, 0);
+                k_stream_rest<128, 9><<<grest, 128, 0, aux.stream>>>(P, L, ctl, fc, walls);
+                k_stream_lone<128><<<glone, 128, 0, s>>>(P, L, ctl, fc, walls);
+                cudaEventRecord(aux.join, aux.stream);
+                cudaStreamWaitEvent(s, aux.join, 0);
+            } else {
+                k_stream_lone<128><<<glone, 128, 0, s>>>(P, L, ctl, fc, walls);
+                k_stream_rest<128, 9><<<grest, 128, 0, s>>>(P, L, ctl, fc, walls);
+            }
+        } else if (fc.stream_block == 64)
             k_stream<64, 16><<<(P.n + 63) / 64, 64, 0, s>>>(P, L, ctl, fc, walls);
         else if (fc.stream_block == 256)
             k_stream<256, 4><<<(P.n + 255) / 256, 256, 0, s>>>(P, L, ctl, fc, walls);
@@ -506,11 +619,11 @@ static void launch_step_t(const Particles &P, const NbrList &L, Ctl *ctl, const 
 }
 
 void launch_step(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
-                 const PairConst *pw, const WallGeom *walls, int mode, cudaStream_t s) {
+                 const PairConst *pw, const WallGeom *walls, int mode, cudaStream_t s, const AuxStream &aux) {
     if (fc.mesh.nt)
-        launch_step_t<true>(P, L, ctl, fc, pp, pw, walls, mode, s);
+        launch_step_t<true>(P, L, ctl, fc, pp, pw, walls, mode, s, aux);
     else
-        launch_step_t<false>(P, L, ctl, fc, pp, pw, walls, mode, s);
+        launch_step_t<false>(P, L, ctl, fc, pp, pw, walls, mode, s, aux);
 }
 
 void launch_stage(const Particles &P, Ctl *ctl, const ForceConsts &fc, int stage, cudaStream_t s) {

@@ -118,6 +118,10 @@ typedef struct dem_solver_params {
                             * an apply kernel per step; while most are, one kernel over every
                             * particle.  1, 4 or 8: always the three-kernel step, its contact
                             * kernel with that many lanes per particle.  Same results.        */
+    int stream_split;      /* streaming pass of the three-kernel step: 0 = automatic (3), 1 one
+                            * kernel over every particle, 2 the particles without listed
+                            * neighbours and the rest in two kernels, 3 the same two kernels as
+                            * concurrent branches.  Same results.                              */
 } dem_solver_params;
 
 typedef struct dem_run_stats {
