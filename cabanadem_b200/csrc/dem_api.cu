@@ -13,6 +13,7 @@
 #include <map>
 #include <string>
 #include <tuple>
+#include <limits>
 #include <vector>
 
 #include "b200dem.h"
@@ -87,6 +88,7 @@ struct dem_solver {
     long graph_nodes = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;   // around each step-graph replay
     AuxStream aux;                              // second branch of the split streaming pass
+    bool loop = false;                          // steps in a graph while-loop (steps_per_launch 0)
     double graph_ms = 0.0;                      // device time of the replays
     long graph_steps_run = 0;                   // steps those replays advanced
     int graph_done_mark = 0;                    // steps_done before the current replay
@@ -257,7 +259,27 @@ __global__ void k_run_begin(Ctl *ctl, int target, double half_skin) {
         ctl->half_skin = half_skin;
         ctl->ticket = 0u;
         ctl->vmax2 = 0ull;
+        ctl->npairs = 0;
     }
+}
+// Step loop of a graph replay (a conditional while node): the loop counter is reset by the
+// replay's first node, and after every step one thread decides whether the body runs again --
+// while steps remain, the list is still valid, no list overflowed and the density regime the
+// kernels were chosen for still holds.  At most target + 1 iterations per replay, so the loop
+// ends even if some step made no progress.
+__global__ void k_loop_begin(Ctl *ctl) {
+    if (threadIdx.x == 0) ctl->loop_iter = 0;
+}
+__global__ void k_loop_ctl(Ctl *ctl, cudaGraphConditionalHandle h, int n, int dense) {
+    if (threadIdx.x != 0) return;
+    const int it = ++ctl->loop_iter;
+    bool go = it <= ctl->target && ctl->steps_done < ctl->target && ctl->disp < ctl->half_skin &&
+              !(ctl->status & DEM_ERR_NEIGHBOR_OVERFLOW);
+    if (go && n > 0) {   // the thresholds of adapt_density: leave the loop to switch kernel forms
+        const double f = (double)ctl->last_ndefer / n;
+        go = dense ? f >= 0.10 : !(f > 0.30);
+    }
+    cudaGraphSetConditional(h, go ? 1u : 0u);
 }
 __global__ void k_invalidate(Ctl *ctl) {
     if (threadIdx.x == 0) ctl->disp = 1e300;
@@ -822,7 +844,9 @@ int prepare(dem_solver *s) {
     fc.has_fix = p->any_fix ? 1 : 0;
     fc.mixed = s->sp.precision == DEM_MIXED ? 1 : 0;
     fc.stream_block = (s->sp.stream_block == 64 || s->sp.stream_block == 256) ? s->sp.stream_block : 128;
-    fc.split = (s->sp.stream_split >= 1 && s->sp.stream_split <= 3) ? s->sp.stream_split : 3;
+    // one streaming kernel unless asked: on the 2M lattice (B200) the split forms ran the step in
+    // 76.5 us (two kernels) and 78.4 us (two branches) against 67.6 us
+    fc.split = (s->sp.stream_split >= 1 && s->sp.stream_split <= 3) ? s->sp.stream_split : 1;
     pick_contact_kernel(s);
     fc.scenes = s->nscenes > 0 ? s->d_scenes : nullptr;
     fc.wps = s->nscenes > 0 ? s->wps : 0;
@@ -839,6 +863,27 @@ int prepare(dem_solver *s) {
     return DEM_OK;
 }
 
+void free_pairs(dem_solver *s) {
+    cudaFree(s->L.pitem);
+    cudaFree(s->L.pterm);
+    cudaFree(s->L.prec);
+    s->L.pitem = nullptr;
+    s->L.pterm = nullptr;
+    s->L.prec = nullptr;
+}
+
+// Work-item buffers of the pair-parallel dense step: one item per list entry at most, so
+// maxnb * cap items (16 B each, and 48 B of force/torque terms).
+int ensure_pairs(dem_solver *s) {
+    if (s->L.pitem) return DEM_OK;
+    dem_ctx *ctx = s->ctx;
+    const size_t items = (size_t)s->L.maxnb * s->p->P.cap;
+    CK(dalloc(&s->L.pitem, items));
+    CK(dalloc(&s->L.pterm, 3 * items));
+    CK(dalloc(&s->L.prec, (size_t)s->p->P.cap));
+    return DEM_OK;
+}
+
 int alloc_lists(dem_solver *s, int maxnb) {
     dem_ctx *ctx = s->ctx;
     cudaFree(s->L.nn);
@@ -846,6 +891,8 @@ int alloc_lists(dem_solver *s, int maxnb) {
     cudaFree(s->L.defer);
     cudaFree(s->L.defer_v);
     cudaFree(s->L.defer_w);
+    const bool pairs = s->L.pitem != nullptr;
+    free_pairs(s);
     s->L.maxnb = maxnb;
     CK(dalloc(&s->L.nn, s->p->P.cap));
     CK(dalloc(&s->L.idx, (size_t)maxnb * s->p->P.cap));
@@ -853,6 +900,10 @@ int alloc_lists(dem_solver *s, int maxnb) {
     CK(dalloc(&s->L.defer_v, 3 * (size_t)s->p->P.cap));
     CK(dalloc(&s->L.defer_w, 3 * (size_t)s->p->P.cap));
     CK(cudaMemsetAsync(s->L.nn, 0, sizeof(int) * s->p->P.cap, ctx->stream));
+    if (pairs) {
+        const int st = ensure_pairs(s);
+        if (st) return st;
+    }
     s->version++;
     s->built = false;
     return DEM_OK;
@@ -894,6 +945,10 @@ void pick_contact_kernel(dem_solver *s) {
         const bool one = s->fc.dense || s->p->P.n <= kOneKernelMaxN;
         s->fc.all = one ? 1 : 0;
         s->fc.coop = (!one && fits) ? 8 : 0;
+        // a dense step of a larger system: the pair-parallel form, unless the caller asked for
+        // the one-kernel form (dense_form 1); dense_form 2 uses it at every size and density
+        const int df = s->sp.dense_form;
+        if ((one && df == 0 && s->p->P.n > kOneKernelMaxN) || df == 2) s->fc.all = 2;
     }
 }
 
@@ -966,6 +1021,10 @@ int build_with(dem_solver *s, bool resort, double delta, double skin) {
 
 int capture_graph(dem_solver *s, int steps) {
     dem_ctx *ctx = s->ctx;
+    if (s->fc.all == 2) {
+        const int st = ensure_pairs(s);
+        if (st) return st;
+    }
     if (s->graph) {
         cudaGraphExecDestroy(s->graph);
         s->graph = nullptr;
@@ -990,6 +1049,59 @@ int capture_graph(dem_solver *s, int steps) {
     return DEM_OK;
 }
 
+// The step loop as one graph: a node resetting the loop counter, then a while node whose body
+// is one step (with the neighbour build first in the rebuild-every-step mode) and k_loop_ctl.
+int capture_loop_graph(dem_solver *s) {
+    dem_ctx *ctx = s->ctx;
+    cudaStream_t st = ctx->stream;
+    if (s->fc.all == 2) {
+        const int e = ensure_pairs(s);
+        if (e) return e;
+    }
+    if (s->graph) {
+        cudaGraphExecDestroy(s->graph);
+        s->graph = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    CK(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle h;
+    cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+    if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        k_loop_begin<<<1, 32, 0, st>>>(s->p->ctl);
+        e = cudaStreamEndCapture(st, &g);
+    }
+    cudaGraphNode_t begin = nullptr;
+    size_t nnodes = 1;
+    if (e == cudaSuccess) e = cudaGraphGetNodes(g, &begin, &nnodes);
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cnode = nullptr;
+    if (e == cudaSuccess) e = cudaGraphAddNode(&cnode, g, &begin, 1, &cp);
+    cudaGraph_t body = e == cudaSuccess ? cp.conditional.phGraph_out[0] : nullptr;
+    if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        if (ref_mode(s)) {
+            launch_build(s->p->P, s->p->alt, s->L, s->B, s->p->ctl, s->sp.delta, s->sp.skin, false, true, st);
+            if (s->mesh_nt > 0) launch_mesh_candidates(s->p->P, s->fc.mesh, s->p->ctl, s->sp.delta, s->sp.skin, st);
+        }
+        launch_step(s->p->P, s->L, s->p->ctl, s->fc, s->d_pp, s->d_pw, s->d_walls, MODE_FUSED, st, s->aux);
+        k_loop_ctl<<<1, 32, 0, st>>>(s->p->ctl, h, s->p->P.n, s->fc.dense);
+        e = cudaStreamEndCapture(st, &body);
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&s->graph, g, 0);
+    cudaGraphDestroy(g);
+    CK(e);
+    s->graph_nodes = kernels_per_step(s->fc) + 1 +
+                     (ref_mode(s) ? build_kernel_count(false) + (s->mesh_nt > 0 ? 1 : 0) : 0);   // per iteration
+    s->graph_steps = -1;
+    s->graph_version = s->version;
+    return DEM_OK;
+}
+
 }  // namespace
 
 extern "C" int dem_solver_create(dem_ctx *ctx, dem_particles *p, dem_walls *w, const dem_force_params *fp,
@@ -1005,6 +1117,7 @@ extern "C" int dem_solver_create(dem_ctx *ctx, dem_particles *p, dem_walls *w, c
     s->w = w;
     s->fp = *fp;
     s->sp = *sp;
+    s->loop = s->sp.steps_per_launch <= 0;
     if (s->sp.steps_per_launch <= 0) s->sp.steps_per_launch = 32;
     const int n = p->P.cap;
     BuildBuffers &B = s->B;
@@ -1075,6 +1188,7 @@ extern "C" int dem_solver_destroy(dem_solver *s) {
     if (s->aux.join) cudaEventDestroy(s->aux.join);
     cudaFree(s->d_pp); cudaFree(s->d_pw); cudaFree(s->d_walls); cudaFree(s->d_scenes);
     cudaFree(s->L.nn); cudaFree(s->L.idx); cudaFree(s->L.defer); cudaFree(s->L.defer_v); cudaFree(s->L.defer_w);
+    free_pairs(s);
     BuildBuffers &B = s->B;
     cudaFree(B.grid); cudaFree(B.total); cudaFree(B.key); cudaFree(B.cell_start); cudaFree(B.cell_fill); cudaFree(B.cell_items);
     cudaFree(B.block_sums); cudaFree(B.bbox); cudaFree(B.src); cudaFree(B.dst);
@@ -1174,23 +1288,35 @@ extern "C" int dem_solver_run(dem_solver *s, int nsteps) {
     s->graph_done_mark = 0;
     CK(cudaGetLastError());
     const int chunk = s->sp.steps_per_launch;
+    // the graph of the next replay: the step loop (while node), or `chunk` gated steps
+    auto ensure_graph = [&]() -> int {
+        if (s->loop) {
+            if (!s->graph || s->graph_version != s->version || s->graph_steps != -1) return capture_loop_graph(s);
+        } else if (!s->graph || s->graph_version != s->version || s->graph_steps != chunk) {
+            return capture_graph(s, chunk);
+        }
+        return DEM_OK;
+    };
+    // kernels one replay launched: per iteration of the loop graph, per captured step otherwise
+    auto count_launches = [&](const Ctl &c) { s->launches += s->loop ? 1 + (long)c.loop_iter * s->graph_nodes : s->graph_nodes; };
     if (ref_mode(s)) {
         // rebuild before every force pass, inside the graph (no re-sort)
         for (;;) {
-            if (!s->graph || s->graph_version != s->version || s->graph_steps != chunk) {
-                int e = capture_graph(s, chunk);
+            {
+                int e = ensure_graph();
                 if (e) return e;
             }
             Ctl c{};
             int done_before = -1;
             for (;;) {
                 CK(cudaGraphLaunch(s->graph, st));
-                s->launches += s->graph_nodes;
                 c = read_ctl(s);
+                count_launches(c);
                 adapt_density(s, c);
                 if (c.steps_done >= c.target || (c.status & DEM_ERR_NEIGHBOR_OVERFLOW) || c.steps_done == done_before)
                     break;
                 done_before = c.steps_done;
+                if (s->loop && s->graph_version != s->version) break;   // kernel form switched: recapture
             }
             if (c.status & DEM_ERR_NEIGHBOR_OVERFLOW) {
                 const int want = std::min(std::max(2 * s->L.maxnb, c.max_nbr + 8), 128);
@@ -1201,6 +1327,8 @@ extern "C" int dem_solver_run(dem_solver *s, int nsteps) {
                 continue;
             }
             if (c.steps_done >= c.target) break;
+            // the loop graph left to switch kernel forms (a switch needs a step, so this progresses)
+            if (s->loop && s->graph_version != s->version) continue;
             return fail(ctx, DEM_ERR_CUDA, "solver made no progress");
         }
     } else {
@@ -1213,17 +1341,17 @@ extern "C" int dem_solver_run(dem_solver *s, int nsteps) {
             CK(cudaEventCreate(&s->ev1));
         }
         for (int guard = 0;; ++guard) {
-            if (!s->graph || s->graph_version != s->version || s->graph_steps != chunk) {
-                int e = capture_graph(s, chunk);
+            {
+                int e = ensure_graph();
                 if (e) return e;
             }
             CK(cudaEventRecord(s->ev0, st));
             CK(cudaGraphLaunch(s->graph, st));
             CK(cudaEventRecord(s->ev1, st));
-            s->launches += s->graph_nodes;
             const int done_before = s->graph_done_mark;
             Ctl c = read_ctl(s);
             CK(cudaGetLastError());
+            count_launches(c);
             adapt_density(s, c);
             {
                 float ms = 0.f;
@@ -1603,9 +1731,15 @@ extern "C" int dem_bonds_set(dem_bonds *b, int field, const void *host, long cou
         }
     }
     cudaStream_t st = ctx->stream;
-    void *tmp = s->p->stage;
-    if ((size_t)per * es > s->p->stage_bytes) return fail(ctx, DEM_ERR_INVALID, "dem_bonds_set: field too large");
-    CK(cudaMemcpyAsync(tmp, host, (size_t)per * es, cudaMemcpyHostToDevice, st));
+    void *tmp = nullptr;
+    CK(cudaMalloc(&tmp, (size_t)per * es));
+    {
+        const cudaError_t e = cudaMemcpyAsync(tmp, host, (size_t)per * es, cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) {
+            cudaFree(tmp);
+            return cuda_check(ctx, e, "dem_bonds_set");
+        }
+    }
     switch (field) {
         case DEM_B_IDX: k_scatter_i<<<kGS, kTB, 0, st>>>((const int *)tmp, B.idx, n, mb, P.cap, P.rank, 1); break;
         case DEM_B_INIT_LEN: k_scatter_d<<<kGS, kTB, 0, st>>>((const double *)tmp, B.init_len, n, mb, P.cap, P.rank); break;
@@ -1619,8 +1753,10 @@ extern "C" int dem_bonds_set(dem_bonds *b, int field, const void *host, long cou
                 k_scatter_d<<<kGS, kTB, 0, st>>>((const double *)tmp, B.hist + (long)(field - DEM_B_FT_X) * mb * P.cap, n,
                                                  mb, P.cap, P.rank);
     }
-    CK(cudaGetLastError());
-    CK(cudaStreamSynchronize(st));   // the staging buffer is reused by the next upload
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(tmp);
+    CK(e);
     if (field == DEM_B_IDX || field == DEM_B_COUNT) {
         // bonds given by the caller define the particle order from now on, as setupBonds does
         s->p->has_bonds = true;
@@ -1698,7 +1834,9 @@ extern "C" int dem_bonded_run(dem_bonds *b, int nsteps) {
         if (st) return st;
     }
     cudaStream_t st = ctx->stream;
-    k_run_begin<<<1, 32, 0, st>>>(s->p->ctl, nsteps, 1e300);
+    // the bonded step reads no neighbour list: no displacement bound may stop it (an upload
+    // marks the list stale with a bound of 1e300)
+    k_run_begin<<<1, 32, 0, st>>>(s->p->ctl, nsteps, std::numeric_limits<double>::infinity());
     launch_prologue(s->p->P, s->p->ctl, s->fc, st);
     s->launches += 2;
     CK(cudaGetLastError());

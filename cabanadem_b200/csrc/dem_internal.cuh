@@ -45,6 +45,8 @@ struct Ctl {
                               // (placed first by the re-sort; 0 when the build did not re-sort)
     int nclear;               // particles [nlone, nlone + nclear): every listed neighbour's gap
                               // exceeded skin/2 at the last build (placed second)
+    int npairs;               // contact work items of the current step (pair-parallel dense step)
+    int loop_iter;            // iterations of the step loop in the current graph replay
 };
 
 struct Particles {
@@ -131,7 +133,8 @@ struct ForceConsts {
     struct WallGeom *mwalls;   // the device walls when some wall moves (Q6 clear, nonzero
                                // velocity): each step's finaliser advances x += dt u; else null
     int all;                   // 1: one kernel steps every particle (dense flows), no streaming
-                               // or apply kernel; velocities ping-pong between their buffers
+                               // or apply kernel; velocities ping-pong between their buffers;
+                               // 2: the same step as three pair-parallel kernels (dem_pairs.cuh)
     const struct SceneConst *scenes;   // per-scene damping/friction, null: the scalars above
     int wps;                   // walls per scene (> 0 with scenes): scene s owns [s*wps, s*wps+wps)
 };
@@ -148,6 +151,10 @@ struct NbrList {
     int maxnb;
     int *defer;  // [cap] particles deferred to the contact kernel in the current step
     double *defer_v, *defer_w;  // [3][cap] new u, omega of deferred particle t (slot t)
+    // pair-parallel dense step (dem_pairs.cuh), allocated when that form is first used:
+    int4 *pitem;     // [maxnb * cap] contact work items (i, j, history slot or -1, -)
+    double2 *pterm;  // [3][maxnb * cap]: per item F (3) and tau (3) of particle i
+    int4 *prec;      // [cap] first item, item count, contact word at the step's start
 };
 
 struct Grid {                 // one per scene, computed on the device at every build
@@ -223,6 +230,9 @@ struct AuxStream {
 };
 void launch_step(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
                  const PairConst *pw, const WallGeom *walls, int mode, cudaStream_t s, const AuxStream &aux = AuxStream());
+// the pair-parallel dense step in mixed precision (dem_mixed.cu)
+void launch_pairs_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
+                        const PairConst *pw, const WallGeom *walls, bool mesh, cudaStream_t s);
 void launch_stage(const Particles &P, Ctl *ctl, const ForceConsts &fc, int stage, cudaStream_t s);
 // dem_mixed.cu
 void launch_contact_mixed_all(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc,

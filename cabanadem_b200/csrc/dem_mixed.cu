@@ -8,6 +8,7 @@
 // streaming kernel (particles with no possible contact) is shared with the FP64 path.
 #include "dem_particle.cuh"
 #include "dem_contact_coop.cuh"
+#include "dem_pairs.cuh"
 
 namespace b200dem {
 
@@ -123,6 +124,41 @@ static const void *contact_mixed_kernel_t(int dense, int coop) {
     if (coop == 4) return (const void *)k_contact_coop<4, kCoopMinBlocks, true, MESH>;
     return dense ? (const void *)k_contact_mixed<kContactMixedMinBlocksDense, MESH>
                  : (const void *)k_contact_mixed<1, MESH>;
+}
+
+// Every block the SMs hold of a kernel (a persistent grid), at most enough for `work` threads.
+static int fill_blocks(const void *kernel, int block, long work) {
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, block, 0);
+    if (per <= 0) per = 1;
+    const long need = (work + block - 1) / block;
+    return (int)(need < (long)sms * per ? (need > 0 ? need : 1) : (long)sms * per);
+}
+
+template <bool MESH>
+static void pairs_mixed_t(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
+                          const PairConst *pw, const WallGeom *walls, cudaStream_t s) {
+    static int g1 = 0, g2 = 0, g3 = 0, last_n = -1;
+    if (last_n != P.n) {
+        g1 = fill_blocks((const void *)k_pairs_find<true>, kPairsBlock, P.n);
+        g2 = fill_blocks((const void *)k_pairs_eval<true>, kPairsBlock, 8L * P.n);
+        g3 = fill_blocks((const void *)k_pairs_sum<true, MESH>, kPairsBlock, P.n);
+        last_n = P.n;
+    }
+    k_pairs_find<true><<<g1, kPairsBlock, 0, s>>>(P, L, ctl, fc);
+    k_pairs_eval<true><<<g2, kPairsBlock, 0, s>>>(P, L, ctl, fc, pp);
+    k_pairs_sum<true, MESH><<<g3, kPairsBlock, 0, s>>>(P, L, ctl, fc, pw, walls);
+}
+
+void launch_pairs_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
+                        const PairConst *pw, const WallGeom *walls, bool mesh, cudaStream_t s) {
+    if (mesh)
+        pairs_mixed_t<true>(P, L, ctl, fc, pp, pw, walls, s);
+    else
+        pairs_mixed_t<false>(P, L, ctl, fc, pp, pw, walls, s);
 }
 
 const void *contact_mixed_kernel(int dense, int coop, bool mesh) {

@@ -219,6 +219,7 @@ __device__ __forceinline__ void finish_step_counted(Ctl *ctl, unsigned long long
             ctl->disp = ctl->disp + dt * sqrt(v2) * (1.0 + 1e-9);
             ctl->last_ndefer = atomicAdd(&ctl->ndefer, 0);
             ctl->ndefer = 0;
+            ctl->npairs = 0;
             ctl->cur ^= 1;
             ctl->vcur ^= 1;
             ctl->steps_done += 1;

@@ -17,6 +17,7 @@
 
 #include "dem_particle.cuh"
 #include "dem_contact_coop.cuh"
+#include "dem_pairs.cuh"
 
 namespace b200dem {
 
@@ -522,7 +523,10 @@ void launch_prologue(const Particles &P, Ctl *ctl, const ForceConsts &fc, cudaSt
     k_prologue<<<nblocks(P.n), kBlock, 0, s>>>(P, ctl, fc);
 }
 
-int kernels_per_step(const ForceConsts &fc) { return fc.all ? 1 : (fc.split >= 2 ? 4 : 3); }
+int kernels_per_step(const ForceConsts &fc) {
+    if (fc.all) return fc.all == 2 ? 3 : 1;
+    return fc.split >= 2 ? 4 : 3;
+}
 
 static int persistent_blocks(const void *kernel, int block, int n) {
     static int sms = 0;
@@ -542,7 +546,22 @@ static int persistent_blocks(const void *kernel, int block, int n) {
 template <bool MESH>
 static void launch_step_t(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
                  const PairConst *pw, const WallGeom *walls, int mode, cudaStream_t s, const AuxStream &aux) {
-    if (mode == MODE_FUSED && fc.all) {
+    if (mode == MODE_FUSED && fc.all == 2) {
+        if (fc.mixed) {
+            launch_pairs_mixed(P, L, ctl, fc, pp, pw, walls, MESH, s);
+        } else {
+            static int g1 = 0, g2 = 0, g3 = 0, last_np = -1;
+            if (last_np != P.n) {
+                g1 = persistent_blocks((const void *)k_pairs_find<false>, kPairsBlock, P.n);
+                g2 = persistent_blocks((const void *)k_pairs_eval<false>, kPairsBlock, 8 * P.n);
+                g3 = persistent_blocks((const void *)k_pairs_sum<false, MESH>, kPairsBlock, P.n);
+                last_np = P.n;
+            }
+            k_pairs_find<false><<<g1, kPairsBlock, 0, s>>>(P, L, ctl, fc);
+            k_pairs_eval<false><<<g2, kPairsBlock, 0, s>>>(P, L, ctl, fc, pp);
+            k_pairs_sum<false, MESH><<<g3, kPairsBlock, 0, s>>>(P, L, ctl, fc, pw, walls);
+        }
+    } else if (mode == MODE_FUSED && fc.all) {
         static int ga = 0, gma = 0, last_na = -1;
         if (last_na != P.n) {
             ga = persistent_blocks((const void *)k_contact_all<kContactMinBlocksDense, MESH>, kBlock, P.n);

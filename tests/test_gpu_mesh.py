@@ -14,7 +14,7 @@ STATE_F = ("x", "u", "omega", "force", "torque", "tng_count")
 
 
 @pytest.mark.parametrize("speed", [0.0, 0.5], ids=["static", "moving"])
-@pytest.mark.parametrize("lanes", [0, 1, 8], ids=["auto", "per_thread", "coop8"])
+@pytest.mark.parametrize("lanes", [0, 1, 8, "pairs"], ids=["auto", "per_thread", "coop8", "pairs"])
 def test_mesh_hopper_bitwise(lanes, speed):
     sc = S.mesh_hopper(n=384, nsteps=4000, band=0.002, drop_speed=4.0, speed=speed)
     ref, m = sc.state.copy(), sc.extra["mesh"].copy()
@@ -22,7 +22,10 @@ def test_mesh_hopper_bitwise(lanes, speed):
                mesh=m)
     assert st == 0
     assert (ref.u[:, 1] > 0).sum() > 50        # bounced off the trough
-    s = api.from_scenario(sc, contact_lanes=lanes)
+    if lanes == "pairs":
+        s = api.from_scenario(sc, dense_form=2)
+    else:
+        s = api.from_scenario(sc, contact_lanes=lanes)
     for n in (1500, 1001, 1499):
         s.run_steps(n)
     got = s.particles.download()

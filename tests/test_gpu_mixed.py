@@ -112,15 +112,16 @@ def test_mixed_energy_drift_elastic(example_inputs):
 
 
 def test_mixed_contact_kernels_agree():
-    """Mixed precision through the per-thread and the cooperative contact kernel and the
-    one-kernel dense step: the same per-contact function and summation order, so the same
-    state after 300 dense steps."""
+    """Mixed precision through the per-thread and the cooperative contact kernel, the
+    one-kernel dense step and the pair-parallel dense step: the same per-contact function and
+    summation order, so the same state after 300 dense steps."""
     sc = S.random_box(n=4096, nsteps=300)
     c = sc.state.x.mean(axis=0)
     sc.state.x[:] = c + (sc.state.x - c) * 0.6
     got = []
-    for lanes in (1, 8, 0):      # 0: the one-kernel dense step once the box is found dense
-        s = api.from_scenario(sc, precision=DEM_MIXED, contact_lanes=lanes)
+    # 0: the one-kernel dense step once the box is found dense; (0, 2): the pair-parallel form
+    for lanes, form in ((1, 0), (8, 0), (0, 0), (0, 2)):
+        s = api.from_scenario(sc, precision=DEM_MIXED, contact_lanes=lanes, dense_form=form)
         s.run_steps(300)
         got.append(s.particles.download())
     for other in got[1:]:

@@ -125,6 +125,36 @@ def test_contact_kernel_forms_bitwise(lanes):
         assert s.stats()["launches"] < t.stats()["launches"] - 400
 
 
+@pytest.mark.parametrize("packing", [1.0, 0.6], ids=["gas", "compressed"])
+def test_pair_parallel_dense_step_bitwise(packing):
+    """The pair-parallel step (contact search per particle, pair law per contact, sums per
+    particle) forced at every density (dense_form 2): bit-identical to the oracle, slots and
+    wall history included, over 1,200 steps of the compressed box (contacts form, break and
+    move between slots; rebuilds) and of the C1 gas."""
+    sc = S.random_box(n=4096, nsteps=1200)
+    c = sc.state.x.mean(axis=0)
+    sc.state.x[:] = c + (sc.state.x - c) * packing
+    ref, _ = _oracle(sc, 1200)
+    s = api.from_scenario(sc, dense_form=2)
+    for n in (500, 700):
+        s.run_steps(n)
+    _assert_bitwise(s.particles.download(), ref, where="pairs")
+    assert s.stats()["rebuilds"] >= 1
+
+
+def test_pair_parallel_contact_overflow():
+    """Slot overflow (MaxCnts 2) through the pair-parallel step: status bit and state as the oracle."""
+    sc = S.random_box(n=512, max_cnts=2, nsteps=5)
+    c = sc.state.x.mean(axis=0)
+    sc.state.x[:] = c + (sc.state.x - c) * 0.3
+    ref, st = _oracle(sc, 5)
+    assert st & 0x1
+    s = api.from_scenario(sc, dense_form=2)
+    s.run_steps(5)
+    assert s.last_status & 0x004
+    _assert_bitwise(s.particles.download(), ref, where="pairs overflow")
+
+
 @pytest.mark.parametrize("split", [1, 2, 3], ids=["one_kernel", "two_kernels", "two_branches"])
 @pytest.mark.parametrize("packing", [1.0, 0.7], ids=["gas", "compressed"])
 def test_streaming_pass_forms_bitwise(split, packing):
@@ -191,6 +221,25 @@ def test_unfused_phases_match_fused(example_inputs):
         api.computeForceParticleParticleInfiniteWall(s)
         s.integrator.stage3()
     _assert_bitwise(s.particles.download(), fused, where="unfused")
+
+
+@pytest.mark.parametrize("chunk", [1, 16, 64])
+def test_chunked_graphs_equal_the_loop_graph(chunk):
+    """The step loop as a graph while-loop (steps_per_launch 0, the default) against graphs of
+    a fixed number of gated steps: the same trajectory bit for bit, through rebuilds and the
+    switch between the sparse and the dense kernel forms, and the oracle's."""
+    sc = S.random_box(n=4096, nsteps=500)
+    c = sc.state.x.mean(axis=0)
+    sc.state.x[:] = c + (sc.state.x - c) * 0.75
+    ref, _ = _oracle(sc, 500)
+    a = api.from_scenario(sc, contact_lanes=0)
+    b = api.from_scenario(sc, contact_lanes=0, steps_per_launch=chunk)
+    for n in (123, 377):
+        a.run_steps(n)
+        b.run_steps(n)
+    _assert_bitwise(a.particles.download(), ref, where="loop")
+    _assert_bitwise(b.particles.download(), ref, where="chunk%d" % chunk)
+    assert a.stats()["steps"] == b.stats()["steps"] == 500
 
 
 def test_split_runs_equal_one_run():
