@@ -74,6 +74,9 @@ def parse():
     ap.add_argument("--save", default="", help="dense: checkpoint the state after --dense-advance steps")
     ap.add_argument("--load", default="", help="dense: start from a checkpoint instead of advancing")
     ap.add_argument("--contact-lanes", type=int, default=0, help="dense: contact kernel form (0 automatic)")
+    ap.add_argument("--dense-form", type=int, default=0, help="dense: 1 one kernel, 2 pair-parallel (0 automatic)")
+    ap.add_argument("--steps-per-launch", type=int, default=0,
+                    help="0: the step loop as a graph while-loop; else steps per captured graph (for profilers)")
     ap.add_argument("--seconds", type=float, default=0.25, help="dam_break: simulated time of both rollouts")
     ap.add_argument("--sub-steps", type=int, default=1000,
                     help="steps timed in each sub-measurement (mixed, dense); at least --steps")
@@ -285,7 +288,8 @@ def run_other(args):
         from cabanadem_b200._lib import DEM_FP64 as _F64
         prec = DEM_MIXED if args.precision == "mixed" else _F64
         sc = S.dam_break(n=200_000, aspect=2.0, seed=101)
-        s = api.from_scenario(sc, ctx=ctx, precision=prec, contact_lanes=args.contact_lanes)
+        s = api.from_scenario(sc, ctx=ctx, precision=prec, contact_lanes=args.contact_lanes, dense_form=args.dense_form,
+                              steps_per_launch=args.steps_per_launch)
         desc = "dam_break_200000 (dense flow)"
         if args.load:
             s.particles.load(args.load)
@@ -296,7 +300,8 @@ def run_other(args):
         if args.save:
             s.particles.save(args.save)
         line.update({"steps": args.steps, "dtype": "f64" if prec == _F64 else "f64 state / f32 force",
-                     "config": {"workload": desc, "contact_lanes": args.contact_lanes}})
+                     "config": {"workload": desc, "contact_lanes": args.contact_lanes, "dense_form": args.dense_form,
+                                "steps_per_launch": args.steps_per_launch}})
         if args.steps > 0:
             s.run_steps(min(args.steps, 64))      # graph capture, kernel-form choice, build
             clocks.start()
@@ -341,15 +346,14 @@ def run_other(args):
             extra = {}
         elif args.workload == "batched":
             sc = S.batched_scenes(seed=3 + rank)
-            cfg = autotune.tune(sc, precision=DEM_MIXED, warmup=5, steps=40)
-            sc2 = S.batched_scenes(seed=3 + rank)
-            kw = autotune.apply(sc2, cfg)
-            obj = api.from_scenario(sc2, ctx=ctx, precision=DEM_MIXED, **kw)
+            obj = api.BatchRunner(sc, precision=DEM_MIXED, tune=True, device=local)
             n, steps, dtype = sc.state.n, args.steps, "f64 state / f32 force"
             desc = ("batched_1024_scenes: %d spheres in 1024 independent scenes (log-uniform [2,8192] per scene), "
-                    "one plane per scene, e~U[0.3,0.95], mu~U[0.1,0.5], dt 1e-7 s, measured window %d steps"
-                    % (n, steps))
-            extra = {"autotuned": cfg}
+                    "one plane per scene, e~U[0.3,0.95], mu~U[0.1,0.5], dt 1e-7 s, measured window %d steps; "
+                    "scenes grouped by size bucket, each bucket a graph-looped solver with its own tuned "
+                    "settings on its own stream, the buckets concurrent; wall-clock timing" % (n, steps))
+            extra = {"autotuned": {str(p["bucket"]): dict(p["config"], particles=p["scenario"].state.n,
+                                                          scenes=len(p["scenes"])) for p in obj.parts}}
         else:
             case = S.bonded_bar()
             obj = api.bonded_from_case(case, ctx=ctx)
@@ -360,10 +364,20 @@ def run_other(args):
             extra = {}
         obj.run_steps(max(3, args.warmup))
         clocks.start()
-        ms = _timed(ctx, lambda: obj.run_steps(steps))
+        if args.workload == "batched":
+            # several contexts: the run returns once every bucket's device work is done
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            obj.run_steps(steps)
+            torch.cuda.synchronize()
+            ms = (time.perf_counter() - t0) * 1e3
+        else:
+            ms = _timed(ctx, lambda: obj.run_steps(steps))
         ck = clocks.stop()
         if args.workload == "bonded":
             extra["broken_bonds"] = obj.broken()
+        if args.workload == "batched":
+            obj.close()
         line.update({"value": ws * n * steps / (ms / 1e3), "steps": steps, "ms_per_step": ms / steps,
                      "dtype": dtype, "config": {"workload": desc, "parallelism": "replicas" if ws > 1 else "single",
                                                 "l2": "state %s L2" % ("larger than" if n * 330 > 126e6 else

@@ -477,6 +477,65 @@ def from_scenario(sc, ctx: Context | None = None, rebuild_every_step=False, prec
     return s
 
 
+class BatchRunner:
+    """Independent scenes of a batched set (scenarios.batched_scenes) grouped by scene size
+    (scenarios.split_scenes): each size bucket is one solver, with the launch settings tuned for
+    that bucket (autotune.tune on the bucket's scenes, or `configs[bucket]`), on a context of its
+    own, so on a CUDA stream of its own.  run_steps advances every bucket at once: one host
+    thread per bucket, each a graph-looped run of its solver, the buckets' kernels running
+    concurrently on the GPU.  Scenes never interact, so every scene evolves as it does alone."""
+
+    def __init__(self, sc, precision=_lib.DEM_FP64, configs=None, tune=False, device=0, tune_steps=40):
+        from . import autotune, scenarios as S
+        self.n = sc.state.n
+        self.parts = []
+        for b, sub, ids in S.split_scenes(sc):
+            cfg = (configs or {}).get(b)
+            if cfg is None and tune:
+                cfg = autotune.tune(sub, precision=precision, warmup=5, steps=tune_steps)
+            cfg = dict(autotune.DEFAULTS, **(cfg or {}))
+            kw = autotune.apply(sub, cfg)
+            ctx = Context(device)
+            self.parts.append(dict(bucket=b, scenario=sub, scenes=ids, ctx=ctx, config=cfg,
+                                   solver=from_scenario(sub, ctx=ctx, precision=precision, **kw)))
+
+    def run_steps(self, nsteps: int):
+        import threading
+        errors = []
+
+        def work(s):
+            try:
+                s.run_steps(nsteps)
+            except Exception as e:   # re-raised on the calling thread
+                errors.append(e)
+        threads = [threading.Thread(target=work, args=(p["solver"],)) for p in self.parts]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        if errors:
+            raise errors[0]
+
+    def download(self) -> ParticleState:
+        """The whole batch's state in the original particle order."""
+        parts = [(p["scenario"].extra["rows"], p["solver"].particles.download()) for p in self.parts]
+        first = parts[0][1]
+        out = ParticleState.create(self.n, max_cnts=first.max_cnts, max_walls=first.max_walls)
+        for rows, st in parts:
+            for f, v in st.arrays().items():
+                getattr(out, f)[rows] = v
+        return out
+
+    def stats(self):
+        return [dict(bucket=p["bucket"], config=p["config"], **p["solver"].stats()) for p in self.parts]
+
+    def close(self):
+        for p in self.parts:
+            p["solver"].close()
+            p["ctx"].close()
+        self.parts = []
+
+
 class Bonds:
     """ParticlesBondedDEM's bond slots (src/CabanaBondedDEM_Particles.hpp:29-293) on a solver's
     particles, with setupBonds (:86-171) and the bonded loop (tst_01_BDEM:295-306)."""

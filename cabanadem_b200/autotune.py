@@ -1,16 +1,23 @@
 """Autotuner for the launch configuration of a workload.
 
-Three settings change speed but not results (the neighbour list is always a superset of the
-overlapping pairs and is summed in caller-index order, whatever its cutoff or the re-sort):
+The settings change speed but not results (every kernel form sums the same terms in the same
+order, and the neighbour list is always a superset of the overlapping pairs summed in
+caller-index order, whatever its cutoff or the re-sort):
 
-* ``stream_block``      block size of the streaming kernel (64, 128, 256)
-* ``steps_per_launch``  fused steps per captured CUDA graph (host round trip per graph)
+* ``contact_lanes``     threads per particle of the contact kernel: 0 automatic (one thread per
+                        particle in dense steps, 8 in sparse ones), 1, 4 or 8 (the three-kernel
+                        step with that cooperative width)
+* ``dense_form``        dense steps as one kernel (1) or as the pair-parallel three kernels (2)
+* ``stream_block``      block size (tile) of the streaming kernel (64, 128, 256)
+* ``steps_per_launch``  0: the step loop as a graph while-loop; else fused steps per captured graph
 * ``skin``              Verlet skin, i.e. the rebuild cadence
 
 ``tune`` times short runs of the caller's workload for each candidate, one setting at a time
-(coordinate search from the defaults), and caches the winner per size bucket
-(log2 of the particle count, precision, batched or not) in a JSON file
-(``$CABANADEM_B200_TUNE_CACHE``, default ``~/.cache/cabanadem_b200/autotune.json``).
+(coordinate search from the defaults), and caches the winner per size bucket (log2 of the
+particle count, precision, batched or single, and for a batch the scene-size bucket of its
+scenes) in a JSON file (``$CABANADEM_B200_TUNE_CACHE``, default
+``~/.cache/cabanadem_b200/autotune.json``).  Batches are tuned per scene-size bucket through
+``scenarios.split_scenes`` and run by ``api.BatchRunner``.
 """
 from __future__ import annotations
 
@@ -21,8 +28,10 @@ import time
 
 from . import api
 
-DEFAULTS = dict(stream_block=128, steps_per_launch=32, skin_factor=1.0)
-CANDIDATES = dict(stream_block=(64, 128, 256), steps_per_launch=(16, 32, 64), skin_factor=(0.5, 1.0, 2.0))
+DEFAULTS = dict(contact_lanes=0, dense_form=0, stream_block=128, steps_per_launch=0, skin_factor=1.0)
+CANDIDATES = dict(contact_lanes=(0, 1, 4, 8), dense_form=(1, 2), stream_block=(64, 128, 256),
+                  steps_per_launch=(0, 32), skin_factor=(0.5, 1.0, 2.0))
+ORDER = ("contact_lanes", "dense_form", "stream_block", "steps_per_launch", "skin_factor")
 
 
 def cache_path():
@@ -32,7 +41,12 @@ def cache_path():
 
 def bucket(sc, precision):
     batched = sc.extra.get("scene") is not None
-    return "n2^%d|p%d|%s" % (int(math.log2(max(sc.state.n, 1))), int(precision), "batched" if batched else "single")
+    key = "n2^%d|p%d|%s" % (int(math.log2(max(sc.state.n, 1))), int(precision), "batched" if batched else "single")
+    if batched and sc.extra.get("counts") is not None:
+        from .scenarios import scene_bucket_of
+        sb = {scene_bucket_of(int(c)) for c in sc.extra["counts"]}
+        key += "|scenes%s" % (str(sb.pop()) if len(sb) == 1 else "mixed")
+    return key
 
 
 def _load():
@@ -55,8 +69,7 @@ def time_config(sc, cfg, precision, warmup, steps, ctx=None):
     base_skin = sc.skin
     sc.skin = base_skin * cfg["skin_factor"]
     try:
-        s = api.from_scenario(sc, ctx=ctx, precision=precision, stream_block=cfg["stream_block"],
-                              steps_per_launch=cfg["steps_per_launch"])
+        s = api.from_scenario(sc, ctx=ctx, precision=precision, **_solver_kwargs(cfg))
         s.run_steps(warmup)
         t0 = time.perf_counter()
         s.run_steps(steps)      # returns after the device finished (status read-back)
@@ -69,7 +82,7 @@ def time_config(sc, cfg, precision, warmup, steps, ctx=None):
 
 
 def tune(sc, precision=0, warmup=20, steps=200, use_cache=True, ctx=None):
-    """Best {stream_block, steps_per_launch, skin_factor} for this workload's bucket."""
+    """Best setting of every knob of CANDIDATES for this workload's bucket."""
     key = bucket(sc, precision)
     table = _load() if use_cache else {}
     if use_cache and key in table:
@@ -78,7 +91,7 @@ def tune(sc, precision=0, warmup=20, steps=200, use_cache=True, ctx=None):
     best_t = time_config(sc, best, precision, warmup, steps, ctx)
     trials = [(dict(best), best_t)]
     tried = {tuple(sorted(best.items()))}
-    for name in ("stream_block", "steps_per_launch", "skin_factor"):
+    for name in ORDER:
         for v in CANDIDATES[name]:
             cfg = dict(best)
             cfg[name] = v
@@ -96,7 +109,14 @@ def tune(sc, precision=0, warmup=20, steps=200, use_cache=True, ctx=None):
     return dict(best)
 
 
+def _solver_kwargs(cfg):
+    full = dict(DEFAULTS)
+    full.update(cfg)
+    return dict(stream_block=full["stream_block"], steps_per_launch=full["steps_per_launch"],
+                contact_lanes=full["contact_lanes"], dense_form=full["dense_form"])
+
+
 def apply(sc, cfg):
     """Scenario settings for a tuned configuration (skin) and from_scenario keyword arguments."""
-    sc.skin = sc.skin * cfg["skin_factor"]
-    return dict(stream_block=cfg["stream_block"], steps_per_launch=cfg["steps_per_launch"])
+    sc.skin = sc.skin * dict(DEFAULTS, **cfg)["skin_factor"]
+    return _solver_kwargs(cfg)

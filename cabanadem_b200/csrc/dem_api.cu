@@ -266,7 +266,8 @@ __global__ void k_run_begin(Ctl *ctl, int target, double half_skin) {
 // replay's first node, and after every step one thread decides whether the body runs again --
 // while steps remain, the list is still valid, no list overflowed and the density regime the
 // kernels were chosen for still holds.  At most target + 1 iterations per replay, so the loop
-// ends even if some step made no progress.
+// ends even if some step made no progress.  An iteration runs several steps (kLoopUnroll);
+// those past a stop condition are gated no-ops.
 __global__ void k_loop_begin(Ctl *ctl) {
     if (threadIdx.x == 0) ctl->loop_iter = 0;
 }
@@ -274,7 +275,7 @@ __global__ void k_loop_ctl(Ctl *ctl, cudaGraphConditionalHandle h, int n, int de
     if (threadIdx.x != 0) return;
     const int it = ++ctl->loop_iter;
     bool go = it <= ctl->target && ctl->steps_done < ctl->target && ctl->disp < ctl->half_skin &&
-              !(ctl->status & DEM_ERR_NEIGHBOR_OVERFLOW);
+              !(ctl->status & DEM_ERR_NEIGHBOR_OVERFLOW);   // (at least one step per iteration)
     if (go && n > 0) {   // the thresholds of adapt_density: leave the loop to switch kernel forms
         const double f = (double)ctl->last_ndefer / n;
         go = dense ? f >= 0.10 : !(f > 0.30);
@@ -1049,8 +1050,14 @@ int capture_graph(dem_solver *s, int steps) {
     return DEM_OK;
 }
 
+// Steps per iteration of the graph while-loop: each iteration pays for the conditional and the
+// control kernel (about 5 us on a B200 with one step per iteration); steps past the target in
+// the last iteration are gated no-ops.
+constexpr int kLoopUnroll = 8;
+
 // The step loop as one graph: a node resetting the loop counter, then a while node whose body
-// is one step (with the neighbour build first in the rebuild-every-step mode) and k_loop_ctl.
+// is kLoopUnroll steps (each with the neighbour build first in the rebuild-every-step mode) and
+// k_loop_ctl.
 int capture_loop_graph(dem_solver *s) {
     dem_ctx *ctx = s->ctx;
     cudaStream_t st = ctx->stream;
@@ -1084,19 +1091,22 @@ int capture_loop_graph(dem_solver *s) {
     cudaGraph_t body = e == cudaSuccess ? cp.conditional.phGraph_out[0] : nullptr;
     if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-        if (ref_mode(s)) {
-            launch_build(s->p->P, s->p->alt, s->L, s->B, s->p->ctl, s->sp.delta, s->sp.skin, false, true, st);
-            if (s->mesh_nt > 0) launch_mesh_candidates(s->p->P, s->fc.mesh, s->p->ctl, s->sp.delta, s->sp.skin, st);
+        for (int k = 0; k < kLoopUnroll; ++k) {
+            if (ref_mode(s)) {
+                launch_build(s->p->P, s->p->alt, s->L, s->B, s->p->ctl, s->sp.delta, s->sp.skin, false, true, st);
+                if (s->mesh_nt > 0) launch_mesh_candidates(s->p->P, s->fc.mesh, s->p->ctl, s->sp.delta, s->sp.skin, st);
+            }
+            launch_step(s->p->P, s->L, s->p->ctl, s->fc, s->d_pp, s->d_pw, s->d_walls, MODE_FUSED, st, s->aux);
         }
-        launch_step(s->p->P, s->L, s->p->ctl, s->fc, s->d_pp, s->d_pw, s->d_walls, MODE_FUSED, st, s->aux);
         k_loop_ctl<<<1, 32, 0, st>>>(s->p->ctl, h, s->p->P.n, s->fc.dense);
         e = cudaStreamEndCapture(st, &body);
     }
     if (e == cudaSuccess) e = cudaGraphInstantiate(&s->graph, g, 0);
     cudaGraphDestroy(g);
     CK(e);
-    s->graph_nodes = kernels_per_step(s->fc) + 1 +
-                     (ref_mode(s) ? build_kernel_count(false) + (s->mesh_nt > 0 ? 1 : 0) : 0);   // per iteration
+    s->graph_nodes = kLoopUnroll * (kernels_per_step(s->fc) +
+                                    (ref_mode(s) ? build_kernel_count(false) + (s->mesh_nt > 0 ? 1 : 0) : 0)) +
+                     1;   // per iteration
     s->graph_steps = -1;
     s->graph_version = s->version;
     return DEM_OK;

@@ -277,6 +277,45 @@ def scene_subset(sc, k):
                     sc.nsteps, skin=sc.skin, gravity=sc.gravity)
 
 
+SCENE_BUCKETS = (64, 1024)   # scene-size bucket edges of the batched workload
+
+
+def scene_bucket_of(count, edges=SCENE_BUCKETS):
+    """Index of the size bucket of a scene with `count` particles: [2, 64), [64, 1024), [1024, ...)."""
+    return int(np.searchsorted(np.asarray(edges), count, side="right"))
+
+
+def split_scenes(sc, edges=SCENE_BUCKETS):
+    """The scenes of a batched_scenes set grouped by size bucket: a list of (bucket, scenario,
+    scene ids) with one batched scenario per non-empty bucket, its scenes renumbered 0..k-1 in
+    their original order and keeping their particles, wall, restitution and friction.  A scene
+    evolves the same in any batch (scenes never interact), so each bucket can run with launch
+    settings of its own."""
+    counts = np.asarray(sc.extra["counts"])
+    starts = np.concatenate([[0], np.cumsum(counts)])
+    buckets = np.array([scene_bucket_of(c, edges) for c in counts])
+    out = []
+    for b in range(len(edges) + 1):
+        ids = np.nonzero(buckets == b)[0]
+        if len(ids) == 0:
+            continue
+        rows = np.concatenate([np.arange(starts[k], starts[k + 1]) for k in ids])
+        n = len(rows)
+        st = ParticleState.create(n, max_cnts=sc.state.max_cnts, max_walls=sc.state.max_walls)
+        for f, v in sc.state.arrays().items():
+            getattr(st, f)[...] = v[rows]
+        w = WallState.create(len(ids))
+        for f in ("x", "u", "omega", "normal", "E", "nu", "G"):
+            getattr(w, f)[...] = getattr(sc.walls, f)[ids]
+        sub = Scenario("%s_bucket%d" % (sc.name, b), st, w, dict(sc.params), sc.dt, sc.nsteps, skin=sc.skin,
+                       gravity=sc.gravity)
+        sub.extra = dict(scene=np.repeat(np.arange(len(ids)), counts[ids]).astype(np.int32),
+                         scene_params=[sc.extra["scene_params"][k] for k in ids], walls_per_scene=1,
+                         counts=counts[ids], rows=rows)
+        out.append((b, sub, ids))
+    return out
+
+
 # Quasi-2D granular dam break.  The stiffness is not fixed by the workload: E = 1 GPa keeps the
 # largest Hertz overlap of a 4 m/s collision near 3.4 % of r (below the surrogate's 5 % check;
 # E = 30 MPa would reach 14 %) and the static overlap at the foot of a 1 m column near 0.2 %,

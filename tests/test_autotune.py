@@ -9,9 +9,15 @@ from cabanadem_b200 import autotune, scenarios as S
 
 
 def _cost(cfg):
-    # separable, minimum at stream_block 256, steps_per_launch 64, skin_factor 0.5
-    return ({64: 3.0, 128: 2.0, 256: 1.0}[cfg["stream_block"]] + {16: 3.0, 32: 2.0, 64: 1.0}[cfg["steps_per_launch"]]
+    # separable, minimum at contact_lanes 4, dense_form 2, stream_block 256, steps_per_launch 32,
+    # skin_factor 0.5
+    return ({0: 4.0, 1: 3.0, 4: 1.0, 8: 2.0}[cfg["contact_lanes"]] + {0: 3.0, 1: 2.0, 2: 1.0}[cfg["dense_form"]]
+            + {64: 3.0, 128: 2.0, 256: 1.0}[cfg["stream_block"]] + {0: 2.0, 32: 1.0}[cfg["steps_per_launch"]]
             + {0.5: 1.0, 1.0: 2.0, 2.0: 3.0}[cfg["skin_factor"]])
+
+
+BEST = dict(contact_lanes=4, dense_form=2, stream_block=256, steps_per_launch=32, skin_factor=0.5)
+NTRIALS = 1 + 3 + 2 + 2 + 1 + 2     # defaults + every other candidate of each knob
 
 
 def test_coordinate_search_and_cache(tmp_path, monkeypatch):
@@ -24,20 +30,43 @@ def test_coordinate_search_and_cache(tmp_path, monkeypatch):
     monkeypatch.setattr(autotune, "time_config", fake)
     sc = S.random_box(n=300)
     cfg = autotune.tune(sc, precision=0)
-    assert cfg == dict(stream_block=256, steps_per_launch=64, skin_factor=0.5)
-    assert calls[0] == autotune.DEFAULTS and len(calls) == 7          # defaults + 2 per knob
+    assert cfg == BEST
+    assert calls[0] == autotune.DEFAULTS and len(calls) == NTRIALS
     table = json.loads((tmp_path / "tune.json").read_text())
     key = autotune.bucket(sc, 0)
-    assert key == "n2^8|p0|single" and table[key]["config"] == cfg and table[key]["s_per_step"] == 3.0
+    assert key == "n2^8|p0|single" and table[key]["config"] == cfg and table[key]["s_per_step"] == 5.0
     calls.clear()
     assert autotune.tune(S.random_box(n=400), precision=0) == cfg and calls == []   # same bucket: cached
     autotune.tune(sc, precision=1)
-    assert len(calls) == 7                                            # another precision: tuned anew
+    assert len(calls) == NTRIALS                                      # another precision: tuned anew
     sc_skin = sc.skin
     kw = autotune.apply(sc, cfg)
-    assert kw == dict(stream_block=256, steps_per_launch=64) and sc.skin == sc_skin * 0.5
+    assert kw == dict(stream_block=256, steps_per_launch=32, contact_lanes=4, dense_form=2)
+    assert sc.skin == sc_skin * 0.5
 
 
 def test_batched_bucket_is_separate():
     sc = S.batched_scenes(nscenes=8, nmax=64)
-    assert autotune.bucket(sc, 1).endswith("|p1|batched")
+    assert "|p1|batched|scenes" in autotune.bucket(sc, 1)
+
+
+def test_scene_size_buckets_split_and_key_the_tuning():
+    """split_scenes groups a batch by scene size ([2, 64), [64, 1024), [1024, 8192]): every
+    particle lands in exactly one bucket with its scene's wall and parameters, scenes keep their
+    order, and each bucket has a tuning key of its own."""
+    import numpy as np
+    sc = S.batched_scenes(nscenes=60, nmax=3000, seed=4)
+    parts = S.split_scenes(sc)
+    assert [b for b, _, _ in parts] == sorted(b for b, _, _ in parts)
+    rows = np.concatenate([sub.extra["rows"] for _, sub, _ in parts])
+    assert np.array_equal(np.sort(rows), np.arange(sc.state.n))
+    keys = {}
+    for b, sub, ids in parts:
+        counts = sc.extra["counts"][ids]
+        assert all(S.scene_bucket_of(int(c)) == b for c in counts)
+        assert np.array_equal(sub.state.x, sc.state.x[sub.extra["rows"]])
+        assert [sub.extra["scene_params"][k] for k in range(len(ids))] == [sc.extra["scene_params"][k] for k in ids]
+        assert np.array_equal(sub.walls.normal, sc.walls.normal[ids])
+        keys[b] = autotune.bucket(sub, 1)
+    assert len(set(keys.values())) == len(parts)
+    assert all(k.endswith("|scenes%d" % b) for b, k in keys.items())

@@ -76,3 +76,24 @@ def test_full_batch_mixed_matches_fp64():
     assert np.all(np.isfinite(fb))
     assert np.abs(fb - fa).max() <= 1e-5 * np.abs(fa).max()
     assert np.array_equal(a.particles.get("tng_count"), b.particles.get("tng_count"))
+
+
+def test_size_buckets_with_their_own_settings_equal_one_batch():
+    """The batch split by scene size into buckets, each bucket a solver with launch settings of
+    its own on its own stream, run concurrently (api.BatchRunner): the merged state equals the
+    whole batch run as one solver bit for bit."""
+    sc = S.batched_scenes(nscenes=40, nmax=3000, seed=17, nsteps=300)
+    one = api.from_scenario(S.batched_scenes(nscenes=40, nmax=3000, seed=17, nsteps=300))
+    one.run_steps(300)
+    ref = one.particles.download()
+    configs = {0: dict(contact_lanes=1, stream_block=64),
+               1: dict(contact_lanes=8, steps_per_launch=32),
+               2: dict(dense_form=2, skin_factor=0.5)}
+    runner = api.BatchRunner(sc, configs=configs)
+    assert len(runner.parts) >= 2
+    runner.run_steps(120)
+    runner.run_steps(180)
+    got = runner.download()
+    for f in STATE:
+        assert np.array_equal(getattr(got, f), getattr(ref, f)), f
+    runner.close()
