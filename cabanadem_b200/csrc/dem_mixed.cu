@@ -141,14 +141,17 @@ static int fill_blocks(const void *kernel, int block, long work) {
 template <bool MESH>
 static void pairs_mixed_t(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
                           const PairConst *pw, const WallGeom *walls, cudaStream_t s) {
-    static int g1 = 0, g2 = 0, g3 = 0, last_n = -1;
+    static int g2 = 0, g3 = 0, sms = 0, last_n = -1;
     if (last_n != P.n) {
-        g1 = fill_blocks((const void *)k_pairs_find<true>, kPairsBlock, P.n);
         g2 = fill_blocks((const void *)k_pairs_eval<true>, kPairsBlock, 8L * P.n);
         g3 = fill_blocks((const void *)k_pairs_sum<true, MESH>, kPairsBlock, P.n);
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
         last_n = P.n;
     }
-    k_pairs_find<true><<<g1, kPairsBlock, 0, s>>>(P, L, ctl, fc);
+    launch_pairs_find<true>(P, L, ctl, fc, sms, s);
     k_pairs_eval<true><<<g2, kPairsBlock, 0, s>>>(P, L, ctl, fc, pp);
     k_pairs_sum<true, MESH><<<g3, kPairsBlock, 0, s>>>(P, L, ctl, fc, pw, walls);
 }

@@ -550,14 +550,17 @@ static void launch_step_t(const Particles &P, const NbrList &L, Ctl *ctl, const 
         if (fc.mixed) {
             launch_pairs_mixed(P, L, ctl, fc, pp, pw, walls, MESH, s);
         } else {
-            static int g1 = 0, g2 = 0, g3 = 0, last_np = -1;
+            static int g2 = 0, g3 = 0, sms = 0, last_np = -1;
             if (last_np != P.n) {
-                g1 = persistent_blocks((const void *)k_pairs_find<false>, kPairsBlock, P.n);
                 g2 = persistent_blocks((const void *)k_pairs_eval<false>, kPairsBlock, 8 * P.n);
                 g3 = persistent_blocks((const void *)k_pairs_sum<false, MESH>, kPairsBlock, P.n);
+                int dev = 0;
+                cudaGetDevice(&dev);
+                cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+                if (sms <= 0) sms = 148;
                 last_np = P.n;
             }
-            k_pairs_find<false><<<g1, kPairsBlock, 0, s>>>(P, L, ctl, fc);
+            launch_pairs_find<false>(P, L, ctl, fc, sms, s);
             k_pairs_eval<false><<<g2, kPairsBlock, 0, s>>>(P, L, ctl, fc, pp);
             k_pairs_sum<false, MESH><<<g3, kPairsBlock, 0, s>>>(P, L, ctl, fc, pw, walls);
         }
