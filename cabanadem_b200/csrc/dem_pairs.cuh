@@ -27,22 +27,10 @@ namespace b200dem {
 namespace {
 
 constexpr int kPairsBlock = 128;
-// resident blocks the per-contact and the summing kernels are compiled for (register caps of
-// 80 and 64 per thread)
-#ifndef PAIRS_EVAL_MIN_BLOCKS
-#define PAIRS_EVAL_MIN_BLOCKS 6
-#endif
-#ifndef PAIRS_SUM_MIN_BLOCKS
-#define PAIRS_SUM_MIN_BLOCKS 8
-#endif
-constexpr int kPairsEvalMinBlocks = PAIRS_EVAL_MIN_BLOCKS;
-constexpr int kPairsSumMinBlocks = PAIRS_SUM_MIN_BLOCKS;
-// lanes per particle of the contact search: 1 (k_pairs_find) or 4 / 8 (k_pairs_find_coop, used
-// while MaxCnts <= kCoopSlots)
-#ifndef PAIRS_FIND_LANES
-#define PAIRS_FIND_LANES 1
-#endif
-constexpr int kPairsFindLanes = PAIRS_FIND_LANES;
+// The three kernels are compiled without a register cap: on the dam-break state (B200) caps of
+// 80 / 64 registers for the per-contact and summing kernels (more resident blocks, spills) ran
+// the step in 102.3 us against 95.1 us, and a contact search with 4 or 8 lanes per particle
+// (the closed-form compaction of dem_contact_coop.cuh) in 114-132 us.
 
 template <bool MIXED>
 __global__ void __launch_bounds__(kPairsBlock) k_pairs_find(Particles P, NbrList L, Ctl *ctl, ForceConsts fc) {
@@ -165,197 +153,8 @@ __global__ void __launch_bounds__(kPairsBlock) k_pairs_find(Particles P, NbrList
     if (status) atomicOr(&ctl->status, status);
 }
 
-// k_pairs_find with NL lanes per particle: the lanes of a group load the tracked slots, the
-// list entries and the partners' positions of one particle at once (the closed-form
-// compaction and the ballot-ranked new slots of the cooperative contact kernel,
-// dem_contact_coop.cuh), then write the particle's items in list order.  Same items, slots and
-// history as the one-thread form.  MaxCnts <= kCoopSlots.
-template <int NL>
-__global__ void __launch_bounds__(kPairsBlock) k_pairs_find_coop(Particles P, NbrList L, Ctl *ctl, ForceConsts fc) {
-    constexpr unsigned FULL = 0xffffffffu;
-    constexpr unsigned GLOW = NL == 32 ? 0xffffffffu : ((1u << NL) - 1u);
-    constexpr int R = kCoopSlots / NL;
-    __shared__ int s_tidx_all[kPairsBlock / NL][kCoopSlots + 1];
-    __shared__ double s_h_all[kPairsBlock / NL][3 * kCoopSlots];
-    const CtlSnap c = read_ctl(ctl, true);
-    if (!c.go) return;
-    const int cap = P.cap, n = P.n;
-    const double4 *__restrict__ pc = P.pos[c.cur];
-    const int lane = threadIdx.x & 31, gl = lane % NL, gbase = lane - gl;
-    const unsigned below = (1u << gl) - 1u;
-    const int grp = threadIdx.x / NL;
-    int *s_tidx = s_tidx_all[grp];
-    double *s_h = s_h_all[grp];
-    int status = 0;
-    for (int b = blockIdx.x * (kPairsBlock / NL); b < n; b += gridDim.x * (kPairsBlock / NL)) {   // block-uniform
-        const int i = b + grp;
-        const bool act = i < n;
-        const int ii = act ? i : 0;
-        D4 pi = {0., 0., 0., 0.};
-        int cs0 = 0, nn = 0;
-        if (act) {
-            pi = ld4_early(pc, i);
-            cs0 = ld_early_i(P.cstate + i);
-            nn = ld_early_i(L.nn + i);
-        }
-        const int cnt0 = cs0 & 0xff;
-        int *tidx = P.tidx + ii;
-        double *thx = P.th + ii;
-        double *thy = P.th + (long)P.mc * cap + ii;
-        double *thz = P.th + 2L * P.mc * cap + ii;
-        // ---- compaction (Force.hpp:364-441): the closed form of the swap-with-last loop
-        const int rc = (int)__reduce_max_sync(FULL, (unsigned)((cnt0 + NL - 1) / NL));
-        unsigned keep = 0u;
-        for (int r = 0; r < rc; ++r) {
-            const int s = gl + r * NL;
-            bool kp = false;
-            if (s < cnt0) {
-                const long a = (long)s * cap;
-                const int sidx = tidx[a];
-                s_tidx[s] = sidx;
-                s_h[s] = thx[a];
-                s_h[kCoopSlots + s] = thy[a];
-                s_h[2 * kCoopSlots + s] = thz[a];
-                kp = true;
-                if ((unsigned)sidx < (unsigned)n) {
-                    const D4 pj = ld4(pc, sidx);
-                    const double px = pi.x - pj.x, py = pi.y - pj.y, pz = pi.z - pj.z;
-                    const double r2ij = px * px + py * py + pz * pz;
-                    const double rij = sqrt(r2ij);
-                    const double overlap = pi.w + pj.w - rij;
-                    kp = !(overlap <= 0.);
-                }
-            }
-            keep |= ((__ballot_sync(FULL, kp) >> gbase) & GLOW) << (r * NL);
-        }
-        __syncwarp();
-        const int K = __popc(keep);
-        if (rc > 0) {
-            const unsigned lowK = K >= 32 ? FULL : ((1u << K) - 1u);
-            const unsigned holes = ~keep & lowK;
-            const unsigned back = keep & ~lowK;
-            int ft[R];
-            double f0[R], f1[R], f2[R];
-            bool mv[R];
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const int p = gl + r * NL;
-                mv[r] = false;
-                ft[r] = -1;
-                f0[r] = f1[r] = f2[r] = 0.;
-                if (r < rc && p < cnt0) {
-                    if (p < K) {
-                        if (!((keep >> p) & 1u)) {
-                            const int src = nth_high_bit(back, __popc(holes & ((1u << p) - 1u)));
-                            ft[r] = s_tidx[src];
-                            f0[r] = s_h[src];
-                            f1[r] = s_h[kCoopSlots + src];
-                            f2[r] = s_h[2 * kCoopSlots + src];
-                            mv[r] = true;
-                        }
-                    } else {
-                        mv[r] = true;   // emptied: index -1, zero history
-                    }
-                }
-            }
-            __syncwarp();
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const int p = gl + r * NL;
-                if (mv[r]) {
-                    const long a = (long)p * cap;
-                    s_tidx[p] = ft[r];
-                    tidx[a] = ft[r];
-                    thx[a] = f0[r];
-                    thy[a] = f1[r];
-                    thz[a] = f2[r];
-                }
-            }
-            __syncwarp();
-        }
-        // ---- pass A: overlap test over the list, new contacts take slots in list order
-        int cnt = K, ncont = 0;
-        unsigned conbits = 0u;   // bit r: this lane's entry of round r is a contact
-        const int rn = (int)__reduce_max_sync(FULL, (unsigned)((nn + NL - 1) / NL));
-        for (int r = 0; r < rn; ++r) {
-            const int kk = gl + r * NL;
-            bool con = false;
-            int j = 0;
-            if (kk < nn) {
-                j = L.idx[(long)kk * cap + i];
-                const D4 pj = ld4(pc, j);
-                const double px = pi.x - pj.x, py = pi.y - pj.y, pz = pi.z - pj.z;
-                const double r2ij = px * px + py * py + pz * pz;
-                const double sr = pi.w + pj.w;
-                if (!(r2ij >= sr * sr * 1.0000000001)) {
-                    const double rij = sqrt(r2ij);
-                    const double overlap = sr - rij;
-                    con = overlap > 0.;
-                }
-            }
-            int found_at = -1;
-            if (con)
-                for (int s = 0; s < K; ++s)
-                    if (s_tidx[s] == j) found_at = s;
-            const bool isnew = con && found_at < 0;
-            const unsigned nb = (__ballot_sync(FULL, isnew) >> gbase) & GLOW;
-            if (isnew) {
-                const int slot = cnt + __popc(nb & below);
-                if (slot < P.mc) {
-                    const long a = (long)slot * cap;
-                    tidx[a] = j;
-                    thx[a] = 0.;
-                    thy[a] = 0.;
-                    thz[a] = 0.;
-                    s_tidx[slot] = j;
-                } else {
-                    status |= DEM_ERR_CONTACT_OVERFLOW;
-                }
-            }
-            cnt = min(cnt + __popc(nb), P.mc);
-            conbits |= (con ? 1u : 0u) << r;
-            ncont += __popc((__ballot_sync(FULL, con) >> gbase) & GLOW);
-        }
-        __syncwarp();
-        // ---- items of the warp's particles: one atomic per warp, groups in lane order
-        const int gcount = gl == 0 ? ncont : 0;
-        int incl = gcount;
-        for (int o = 1; o < 32; o <<= 1) {
-            const int v = __shfl_up_sync(FULL, incl, o);
-            if (lane >= o) incl += v;
-        }
-        const int wtotal = __shfl_sync(FULL, incl, 31);
-        int wbase = 0;
-        if (lane == 31 && wtotal) wbase = atomicAdd(&ctl->npairs, wtotal);
-        wbase = __shfl_sync(FULL, wbase, 31);
-        const int gstart = wbase + __shfl_sync(FULL, incl - gcount, gbase);
-        // ---- pass B: each contact's item in list order
-        int before = 0;
-        for (int r = 0; r < rn; ++r) {
-            const bool con = (conbits >> r) & 1u;
-            const unsigned cb = (__ballot_sync(FULL, con) >> gbase) & GLOW;
-            if (con) {
-                const int kk = gl + r * NL;
-                const int j = L.idx[(long)kk * cap + i];
-                int found_at = -1;
-                for (int s = 0; s < cnt; ++s)
-                    if (s_tidx[s] == j) found_at = s;
-                L.pitem[gstart + before + __popc(cb & below)] = make_int4(i, j, found_at, 0);
-            }
-            before += __popc(cb);
-        }
-        if (act && gl == 0) {
-            L.prec[i] = make_int4(gstart, ncont, cs0, 0);
-            const int cs1 = (cs0 & ~0xff) | cnt;
-            if (cs1 != cs0) P.cstate[i] = cs1;
-        }
-        __syncwarp();
-    }
-    if (status) atomicOr(&ctl->status, status);
-}
-
 template <bool MIXED>
-__global__ void __launch_bounds__(kPairsBlock, kPairsEvalMinBlocks) k_pairs_eval(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
+__global__ void __launch_bounds__(kPairsBlock) k_pairs_eval(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
                                                             const PairConst *__restrict__ pp) {
     const CtlSnap c = read_ctl(ctl, true);
     if (!c.go) return;
@@ -438,7 +237,7 @@ __device__ __noinline__ int mesh_contacts(const Particles &P, const ForceConsts 
 }
 
 template <bool MIXED, bool MESH>
-__global__ void __launch_bounds__(kPairsBlock, kPairsSumMinBlocks) k_pairs_sum(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
+__global__ void __launch_bounds__(kPairsBlock) k_pairs_sum(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
                                                            const PairConst *__restrict__ pw,
                                                            const WallGeom *__restrict__ walls) {
     const CtlSnap c = read_ctl(ctl, true);
@@ -584,24 +383,15 @@ __global__ void __launch_bounds__(kPairsBlock, kPairsSumMinBlocks) k_pairs_sum(P
 
 namespace b200dem {
 namespace {
-// Launches the contact search of the pair-parallel step with the configured lanes per particle.
+// Launches the contact search of the pair-parallel step on a persistent grid.
 template <bool MIXED>
 inline void launch_pairs_find(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, int sms,
                               cudaStream_t s) {
-    if (kPairsFindLanes > 1 && P.mc <= kCoopSlots) {
-        constexpr int NL = kPairsFindLanes > 1 ? kPairsFindLanes : 4;
-        int per = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pairs_find_coop<NL>, kPairsBlock, 0);
-        const long need = ((long)P.n * NL + kPairsBlock - 1) / kPairsBlock;
-        const long g = need < (long)sms * (per > 0 ? per : 1) ? need : (long)sms * (per > 0 ? per : 1);
-        k_pairs_find_coop<NL><<<(int)(g > 0 ? g : 1), kPairsBlock, 0, s>>>(P, L, ctl, fc);
-    } else {
-        int per = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pairs_find<MIXED>, kPairsBlock, 0);
-        const long need = ((long)P.n + kPairsBlock - 1) / kPairsBlock;
-        const long g = need < (long)sms * (per > 0 ? per : 1) ? need : (long)sms * (per > 0 ? per : 1);
-        k_pairs_find<MIXED><<<(int)(g > 0 ? g : 1), kPairsBlock, 0, s>>>(P, L, ctl, fc);
-    }
+    int per = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pairs_find<MIXED>, kPairsBlock, 0);
+    const long need = ((long)P.n + kPairsBlock - 1) / kPairsBlock;
+    const long g = need < (long)sms * (per > 0 ? per : 1) ? need : (long)sms * (per > 0 ? per : 1);
+    k_pairs_find<MIXED><<<(int)(g > 0 ? g : 1), kPairsBlock, 0, s>>>(P, L, ctl, fc);
 }
 }  // namespace
 }  // namespace b200dem

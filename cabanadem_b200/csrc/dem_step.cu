@@ -360,14 +360,21 @@ __global__ void __launch_bounds__(kBlock) k_prologue(Particles P, Ctl *ctl, Forc
     const int cap = P.cap;
     double vmax2 = 0.0;
     if (i < P.n) {
-        const double2 mIi = load_mI(P, i);
-        const double m_inverse = 1. / mIi.x, I_inverse = 1. / mIi.y, h = fc.half_dt;
+        const double m_inverse = 1. / P.mI[i], h = fc.half_dt;
         double *vc = P.vel[vcur], *wc = P.omg[vcur];
         double u[3];
         for (int d = 0; d < 3; ++d) {
             u[d] = vc[d * cap + i] + h * P.force[d * cap + i] * m_inverse;
             vc[d * cap + i] = u[d];
-            wc[d * cap + i] = wc[d * cap + i] + h * P.torque[d * cap + i] * I_inverse;
+        }
+        // zero torque leaves omega as it is (the streaming kernel's rule for particles without
+        // pair or wall contacts): omega and I are read only for particles with a torque
+        const double t0 = P.torque[i], t1 = P.torque[cap + i], t2 = P.torque[2 * cap + i];
+        if (t0 != 0. || t1 != 0. || t2 != 0.) {
+            const double I_inverse = 1. / P.mI[cap + i];
+            wc[i] = wc[i] + h * t0 * I_inverse;
+            wc[cap + i] = wc[cap + i] + h * t1 * I_inverse;
+            wc[2 * cap + i] = wc[2 * cap + i] + h * t2 * I_inverse;
         }
         D4 p = ld4(P.pos[cur], i);
         p.x += fc.dt * u[0];
