@@ -272,7 +272,6 @@ __global__ void k_loop_begin(Ctl *ctl) {
     if (threadIdx.x == 0) ctl->loop_iter = 0;
 }
 __global__ void k_loop_ctl(Ctl *ctl, cudaGraphConditionalHandle h, int n, int dense) {
-    asm volatile("griddepcontrol.wait;" ::: "memory");   // launched as a dependent of the last step kernel
     if (threadIdx.x != 0) return;
     const int it = ++ctl->loop_iter;
     bool go = it <= ctl->target && ctl->steps_done < ctl->target && ctl->disp < ctl->half_skin &&
@@ -1099,7 +1098,7 @@ int capture_loop_graph(dem_solver *s) {
             }
             launch_step(s->p->P, s->L, s->p->ctl, s->fc, s->d_pp, s->d_pw, s->d_walls, MODE_FUSED, st, s->aux);
         }
-        launch_k(k_loop_ctl, 1, 32, st, s->p->ctl, h, s->p->P.n, s->fc.dense);
+        k_loop_ctl<<<1, 32, 0, st>>>(s->p->ctl, h, s->p->P.n, s->fc.dense);
         e = cudaStreamEndCapture(st, &body);
     }
     if (e == cudaSuccess) e = cudaGraphInstantiate(&s->graph, g, 0);

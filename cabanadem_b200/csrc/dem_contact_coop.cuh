@@ -372,7 +372,6 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contact_coop(Particles P, NbrL
     // one row per group, padded by one word so that the groups of a warp fall in different banks
     __shared__ int s_tidx[kBlock / NL][kCoopSlots + 1];
     __shared__ double s_h[kBlock / NL][3 * kCoopSlots + 1];
-    pdl_wait();
     if (ctl->steps_done >= ctl->target || (ctl->status & DEM_ERR_NEIGHBOR_OVERFLOW) || !(ctl->disp < ctl->half_skin))
         return;
     const int nd = ctl->ndefer;
@@ -393,7 +392,6 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contact_coop(Particles P, NbrL
                                  status);
         vmax2 = fmax(vmax2, v2);
     }
-    pdl_trigger();
     warp_vmax(ctl, P.vslots, vmax2, status);
 }
 

@@ -17,37 +17,11 @@
 //   perm      sorted index -> caller index; rank: caller index -> sorted index
 #pragma once
 #include <cstdint>
-#include <utility>
 #include <cuda_runtime.h>
 
 #include "b200dem.h"
 
 namespace b200dem {
-
-// Launch of a kernel of the step chain: with programmatic stream serialisation, so that its
-// blocks may be scheduled before the previous kernel has drained (the kernel waits for that
-// kernel's completion itself, pdl_wait).  B200DEM_PDL=0 builds plain launches.
-#ifndef B200DEM_PDL
-#define B200DEM_PDL 1
-#endif
-template <typename... KArgs, typename... Args>
-inline void launch_k(void (*kernel)(KArgs...), int grid, int block, cudaStream_t s, Args &&...args) {
-#if B200DEM_PDL
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(block);
-    cfg.dynamicSmemBytes = 0;
-    cfg.stream = s;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
-#else
-    kernel<<<grid, block, 0, s>>>(std::forward<Args>(args)...);
-#endif
-}
 
 constexpr int kMaxWalls = 24;
 constexpr int kMaxMat = 32;

@@ -19,7 +19,6 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contact_mixed(Particles P, Nbr
                                                           const PairConst *__restrict__ pp,
                                                           const PairConst *__restrict__ pw,
                                                           const WallGeom *__restrict__ walls) {
-    pdl_wait();
     if (ctl->steps_done >= ctl->target || (ctl->status & DEM_ERR_NEIGHBOR_OVERFLOW) || !(ctl->disp < ctl->half_skin))
         return;
     const int nd = ctl->ndefer;
@@ -34,7 +33,6 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contact_mixed(Particles P, Nbr
                                               status);
         vmax2 = fmax(vmax2, v2);
     }
-    pdl_trigger();
     block_vmax(ctl, P.vslots, vmax2, status);
 }
 
@@ -44,7 +42,6 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contact_mixed_all(Particles P,
                                                               const PairConst *__restrict__ pp,
                                                               const PairConst *__restrict__ pw,
                                                               const WallGeom *__restrict__ walls) {
-    pdl_wait();
     const CtlSnap c = read_ctl(ctl, true);
     if (!c.go) return;
     const int vcur = ctl->vcur;
@@ -58,7 +55,6 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contact_mixed_all(Particles P,
         vmax2 = fmax(vmax2, v2);
         active += a;
     }
-    pdl_trigger();
     finish_step_counted(ctl, P.vslots, vmax2, fc.dt, status, active, fc, !c.last);
 }
 
@@ -83,13 +79,13 @@ template <bool MESH>
 static void contact_mixed_t(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
                             const PairConst *pw, const WallGeom *walls, int blocks, cudaStream_t s) {
     if (fc.coop == 8)
-        launch_k(k_contact_coop<8, kCoopMinBlocks, true, MESH>, blocks, kBlock, s, P, L, ctl, fc, pp, pw, walls);
+        k_contact_coop<8, kCoopMinBlocks, true, MESH><<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
     else if (fc.coop == 4)
-        launch_k(k_contact_coop<4, kCoopMinBlocks, true, MESH>, blocks, kBlock, s, P, L, ctl, fc, pp, pw, walls);
+        k_contact_coop<4, kCoopMinBlocks, true, MESH><<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
     else if (fc.dense)
-        launch_k(k_contact_mixed<kContactMixedMinBlocksDense, MESH>, blocks, kBlock, s, P, L, ctl, fc, pp, pw, walls);
+        k_contact_mixed<kContactMixedMinBlocksDense, MESH><<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
     else
-        launch_k(k_contact_mixed<1, MESH>, blocks, kBlock, s, P, L, ctl, fc, pp, pw, walls);
+        k_contact_mixed<1, MESH><<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
 }
 
 void launch_contact_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
@@ -104,9 +100,9 @@ void launch_contact_mixed_all(const Particles &P, const NbrList &L, Ctl *ctl, co
                               const PairConst *pp, const PairConst *pw, const WallGeom *walls, int blocks, bool mesh,
                               cudaStream_t s) {
     if (mesh)
-        launch_k(k_contact_mixed_all<kContactMixedMinBlocksDense, true>, blocks, kBlock, s, P, L, ctl, fc, pp, pw, walls);
+        k_contact_mixed_all<kContactMixedMinBlocksDense, true><<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
     else
-        launch_k(k_contact_mixed_all<kContactMixedMinBlocksDense, false>, blocks, kBlock, s, P, L, ctl, fc, pp, pw, walls);
+        k_contact_mixed_all<kContactMixedMinBlocksDense, false><<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
 }
 
 const void *contact_mixed_all_kernel(bool mesh) {
@@ -156,8 +152,8 @@ static void pairs_mixed_t(const Particles &P, const NbrList &L, Ctl *ctl, const 
         last_n = P.n;
     }
     launch_pairs_find<true>(P, L, ctl, fc, sms, s);
-    launch_k(k_pairs_eval<true>, g2, kPairsBlock, s, P, L, ctl, fc, pp);
-    launch_k(k_pairs_sum<true, MESH>, g3, kPairsBlock, s, P, L, ctl, fc, pw, walls);
+    k_pairs_eval<true><<<g2, kPairsBlock, 0, s>>>(P, L, ctl, fc, pp);
+    k_pairs_sum<true, MESH><<<g3, kPairsBlock, 0, s>>>(P, L, ctl, fc, pw, walls);
 }
 
 void launch_pairs_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,

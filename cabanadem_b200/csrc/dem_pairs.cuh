@@ -34,7 +34,6 @@ constexpr int kPairsBlock = 128;
 
 template <bool MIXED>
 __global__ void __launch_bounds__(kPairsBlock) k_pairs_find(Particles P, NbrList L, Ctl *ctl, ForceConsts fc) {
-    pdl_wait();
     const CtlSnap c = read_ctl(ctl, true);
     if (!c.go) return;
     const int cap = P.cap, n = P.n;
@@ -151,14 +150,12 @@ __global__ void __launch_bounds__(kPairsBlock) k_pairs_find(Particles P, NbrList
             if (cs1 != cs0) P.cstate[i] = cs1;
         }
     }
-    pdl_trigger();
     if (status) atomicOr(&ctl->status, status);
 }
 
 template <bool MIXED>
 __global__ void __launch_bounds__(kPairsBlock) k_pairs_eval(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
                                                             const PairConst *__restrict__ pp) {
-    pdl_wait();
     const CtlSnap c = read_ctl(ctl, true);
     if (!c.go) return;
     const int np = ctl->npairs, cap = P.cap;
@@ -207,7 +204,6 @@ __global__ void __launch_bounds__(kPairsBlock) k_pairs_eval(Particles P, NbrList
         term[1] = make_double2(cf[2], cf[3]);
         term[2] = make_double2(cf[4], cf[5]);
     }
-    pdl_trigger();
 }
 
 // One wall contact of k_pairs_sum, out of line: few particles touch a wall, and inlined the
@@ -244,7 +240,6 @@ template <bool MIXED, bool MESH>
 __global__ void __launch_bounds__(kPairsBlock) k_pairs_sum(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
                                                            const PairConst *__restrict__ pw,
                                                            const WallGeom *__restrict__ walls) {
-    pdl_wait();
     const CtlSnap c = read_ctl(ctl, true);
     if (!c.go) return;
     const int cap = P.cap, vcur = ctl->vcur, nxt = c.cur ^ 1;
@@ -380,7 +375,6 @@ __global__ void __launch_bounds__(kPairsBlock) k_pairs_sum(Particles P, NbrList 
         wn[cap + i] = wi1;
         wn[2 * cap + i] = wi2;
     }
-    pdl_trigger();
     finish_step_counted(ctl, P.vslots, vmax2, fc.dt, status, active, fc, !c.last);
 }
 
@@ -397,7 +391,7 @@ inline void launch_pairs_find(const Particles &P, const NbrList &L, Ctl *ctl, co
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pairs_find<MIXED>, kPairsBlock, 0);
     const long need = ((long)P.n + kPairsBlock - 1) / kPairsBlock;
     const long g = need < (long)sms * (per > 0 ? per : 1) ? need : (long)sms * (per > 0 ? per : 1);
-    launch_k(k_pairs_find<MIXED>, (int)(g > 0 ? g : 1), kPairsBlock, s, P, L, ctl, fc);
+    k_pairs_find<MIXED><<<(int)(g > 0 ? g : 1), kPairsBlock, 0, s>>>(P, L, ctl, fc);
 }
 }  // namespace
 }  // namespace b200dem

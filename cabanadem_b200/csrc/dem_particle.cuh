@@ -33,14 +33,6 @@ __device__ __forceinline__ D4 ld4(const double4 *p, int i) {
 }
 __device__ __forceinline__ void st4(double4 *p, int i, D4 v) { reinterpret_cast<D4 *>(p)[i] = v; }
 
-// Programmatic dependent launch (the kernels of a step are launched with it, see launch_k):
-// pdl_wait blocks until the previous kernel of the stream has completed and its writes are
-// visible (it returns at once for a kernel launched without the attribute), so every kernel of
-// the step chain calls it before its first access; pdl_trigger, at the end of a block's work,
-// lets the next kernel's blocks be scheduled while this kernel's last blocks drain.
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
-
 // Read-only loads issued where they are written: volatile asm is neither sunk into a later
 // branch nor merged, so all of a particle's loads are in flight together.
 __device__ __forceinline__ double ld_early(const double *p) {

@@ -204,7 +204,6 @@ __device__ __forceinline__ bool stream_particle(const Particles &P, const NbrLis
 template <int BS, int MINB>
 __global__ void __launch_bounds__(BS, MINB) k_stream(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
                                                      const WallGeom *__restrict__ walls) {
-    pdl_wait();
     if (!step_gate(ctl)) return;
     const StreamCtl c = stream_ctl(ctl, P.n);
     double vmax2 = 0.0;
@@ -212,7 +211,6 @@ __global__ void __launch_bounds__(BS, MINB) k_stream(Particles P, NbrList L, Ctl
     bool defer = false;
     if (i < P.n) defer = stream_particle(P, L, fc, walls, c, i, vmax2);
     defer_append(ctl, L, defer, i);
-    pdl_trigger();
     warp_vmax(ctl, P.vslots, vmax2, 0);
 }
 
@@ -223,7 +221,6 @@ __global__ void __launch_bounds__(BS, MINB) k_stream(Particles P, NbrList L, Ctl
 template <int BS>
 __global__ void __launch_bounds__(BS, 1536 / BS) k_stream_lone(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
                                                                const WallGeom *__restrict__ walls) {
-    pdl_wait();
     if (!step_gate(ctl)) return;
     const StreamCtl c = stream_ctl(ctl, P.n);
     const int cap = P.cap;
@@ -243,7 +240,6 @@ __global__ void __launch_bounds__(BS, 1536 / BS) k_stream_lone(Particles P, NbrL
         }
         defer_append(ctl, L, defer, i);
     }
-    pdl_trigger();
     warp_vmax(ctl, P.vslots, vmax2, 0);
 }
 
@@ -252,7 +248,6 @@ __global__ void __launch_bounds__(BS, 1536 / BS) k_stream_lone(Particles P, NbrL
 template <int BS, int MINB>
 __global__ void __launch_bounds__(BS, MINB) k_stream_rest(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
                                                           const WallGeom *__restrict__ walls) {
-    pdl_wait();
     if (!step_gate(ctl)) return;
     const StreamCtl c = stream_ctl(ctl, P.n);
     double vmax2 = 0.0;
@@ -262,7 +257,6 @@ __global__ void __launch_bounds__(BS, MINB) k_stream_rest(Particles P, NbrList L
         if (i < P.n) defer = stream_particle(P, L, fc, walls, c, i, vmax2);
         defer_append(ctl, L, defer, i);
     }
-    pdl_trigger();
     warp_vmax(ctl, P.vslots, vmax2, 0);
 }
 
@@ -272,7 +266,6 @@ template <int MINB, bool MESH = false>
 __global__ void __launch_bounds__(kBlock, MINB) k_contact(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
                                                     const PairConst *__restrict__ pp, const PairConst *__restrict__ pw,
                                                     const WallGeom *__restrict__ walls) {
-    pdl_wait();
     if (!step_gate(ctl)) return;
     const int nd = ctl->ndefer;
     if ((long)blockIdx.x * blockDim.x >= nd) return;
@@ -286,7 +279,6 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contact(Particles P, NbrList L
                                          status);
         vmax2 = fmax(vmax2, v2);
     }
-    pdl_trigger();
     block_vmax(ctl, P.vslots, vmax2, status);
 }
 
@@ -298,7 +290,6 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contact_all(Particles P, NbrLi
                                                         const PairConst *__restrict__ pp,
                                                         const PairConst *__restrict__ pw,
                                                         const WallGeom *__restrict__ walls) {
-    pdl_wait();
     const CtlSnap c = read_ctl(ctl, true);
     if (!c.go) return;
     const int vcur = ctl->vcur;
@@ -312,7 +303,6 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contact_all(Particles P, NbrLi
         vmax2 = fmax(vmax2, v2);
         active += a;
     }
-    pdl_trigger();
     finish_step_counted(ctl, P.vslots, vmax2, fc.dt, status, active, fc, !c.last);
 }
 
@@ -322,7 +312,6 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contact_all(Particles P, NbrLi
 // reset cannot cut another block's copy short.
 __global__ void __launch_bounds__(kApplyBlock) k_apply(Particles P, NbrList L, Ctl *ctl, ForceConsts fc) {
     __shared__ int s_nd, s_go, s_last;
-    pdl_wait();
     if (threadIdx.x == 0) {
         s_go = step_gate(ctl);
         s_nd = ctl->ndefer;
@@ -338,7 +327,6 @@ __global__ void __launch_bounds__(kApplyBlock) k_apply(Particles P, NbrList L, C
             wc[d * cap + i] = L.defer_w[d * cap + t];
         }
     }
-    pdl_trigger();
     if (threadIdx.x == 0) {
         __threadfence();
         const unsigned tk = atomicAdd(&ctl->ticket, 1u);
@@ -580,8 +568,8 @@ static void launch_step_t(const Particles &P, const NbrList &L, Ctl *ctl, const 
                 last_np = P.n;
             }
             launch_pairs_find<false>(P, L, ctl, fc, sms, s);
-            launch_k(k_pairs_eval<false>, g2, kPairsBlock, s, P, L, ctl, fc, pp);
-            launch_k(k_pairs_sum<false, MESH>, g3, kPairsBlock, s, P, L, ctl, fc, pw, walls);
+            k_pairs_eval<false><<<g2, kPairsBlock, 0, s>>>(P, L, ctl, fc, pp);
+            k_pairs_sum<false, MESH><<<g3, kPairsBlock, 0, s>>>(P, L, ctl, fc, pw, walls);
         }
     } else if (mode == MODE_FUSED && fc.all) {
         static int ga = 0, gma = 0, last_na = -1;
@@ -593,7 +581,7 @@ static void launch_step_t(const Particles &P, const NbrList &L, Ctl *ctl, const 
         if (fc.mixed)
             launch_contact_mixed_all(P, L, ctl, fc, pp, pw, walls, gma, MESH, s);
         else
-            launch_k(k_contact_all<kContactMinBlocksDense, MESH>, ga, kBlock, s, P, L, ctl, fc, pp, pw, walls);
+            k_contact_all<kContactMinBlocksDense, MESH><<<ga, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
     } else if (mode == MODE_FUSED) {
         static int gc = 0, gm = 0, gcd = 0, gmd = 0, gk4 = 0, gk8 = 0, gkm4 = 0, gkm8 = 0, last_n = -1;
         if (last_n != P.n) {
@@ -635,23 +623,23 @@ static void launch_step_t(const Particles &P, const NbrList &L, Ctl *ctl, const 
                 k_stream_rest<128, 9><<<grest, 128, 0, s>>>(P, L, ctl, fc, walls);
             }
         } else if (fc.stream_block == 64)
-            launch_k(k_stream<64, 16>, (P.n + 63) / 64, 64, s, P, L, ctl, fc, walls);
+            k_stream<64, 16><<<(P.n + 63) / 64, 64, 0, s>>>(P, L, ctl, fc, walls);
         else if (fc.stream_block == 256)
-            launch_k(k_stream<256, 4>, (P.n + 255) / 256, 256, s, P, L, ctl, fc, walls);
+            k_stream<256, 4><<<(P.n + 255) / 256, 256, 0, s>>>(P, L, ctl, fc, walls);
         else
-            launch_k(k_stream<128, 10>, (P.n + 127) / 128, 128, s, P, L, ctl, fc, walls);
+            k_stream<128, 10><<<(P.n + 127) / 128, 128, 0, s>>>(P, L, ctl, fc, walls);
         if (fc.mixed)
             launch_contact_mixed(P, L, ctl, fc, pp, pw, walls, MESH,
                                  fc.coop == 8 ? gkm8 : fc.coop == 4 ? gkm4 : fc.dense ? gmd : gm, s);
         else if (fc.coop == 8)
-            launch_k(k_contact_coop<8, kCoopMinBlocks, false, MESH>, gk8, kBlock, s, P, L, ctl, fc, pp, pw, walls);
+            k_contact_coop<8, kCoopMinBlocks, false, MESH><<<gk8, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
         else if (fc.coop == 4)
-            launch_k(k_contact_coop<4, kCoopMinBlocks, false, MESH>, gk4, kBlock, s, P, L, ctl, fc, pp, pw, walls);
+            k_contact_coop<4, kCoopMinBlocks, false, MESH><<<gk4, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
         else if (fc.dense)
-            launch_k(k_contact<kContactMinBlocksDense, MESH>, gcd, kBlock, s, P, L, ctl, fc, pp, pw, walls);
+            k_contact<kContactMinBlocksDense, MESH><<<gcd, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
         else
-            launch_k(k_contact<1, MESH>, gc, kBlock, s, P, L, ctl, fc, pp, pw, walls);
-        launch_k(k_apply, fc.dense ? 4 * 148 : 148, kApplyBlock, s, P, L, ctl, fc);
+            k_contact<1, MESH><<<gc, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+        k_apply<<<fc.dense ? 4 * 148 : 148, kApplyBlock, 0, s>>>(P, L, ctl, fc);
     } else if (fc.mixed) {
         launch_force_mixed(P, L, ctl, fc, pp, pw, walls, MESH, s);
     } else {
