@@ -524,7 +524,7 @@ def main():
     prec = DEM_FP64 if args.precision == "fp64" else DEM_MIXED
     sc = workload(args.n, seed=2 + rank)
     ctx = api.Context(local)
-    solver = api.from_scenario(sc, ctx=ctx, precision=prec)
+    solver = api.from_scenario(sc, ctx=ctx, precision=prec, steps_per_launch=args.steps_per_launch)
     stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=torch.device("cuda", local))
 
     def barrier():
