@@ -262,25 +262,41 @@ __global__ void k_run_begin(Ctl *ctl, int target, double half_skin) {
         ctl->npairs = 0;
     }
 }
-// Step loop of a graph replay (a conditional while node): the loop counter is reset by the
-// replay's first node, and after every step one thread decides whether the body runs again --
-// while steps remain, the list is still valid, no list overflowed and the density regime the
-// kernels were chosen for still holds.  At most target + 1 iterations per replay, so the loop
-// ends even if some step made no progress.  An iteration runs several steps (kLoopUnroll);
-// those past a stop condition are gated no-ops.
-__global__ void k_loop_begin(Ctl *ctl) {
-    if (threadIdx.x == 0) ctl->loop_iter = 0;
-}
-__global__ void k_loop_ctl(Ctl *ctl, cudaGraphConditionalHandle h, int n, int dense) {
-    if (threadIdx.x != 0) return;
-    const int it = ++ctl->loop_iter;
-    bool go = it <= ctl->target && ctl->steps_done < ctl->target && ctl->disp < ctl->half_skin &&
-              !(ctl->status & DEM_ERR_NEIGHBOR_OVERFLOW);   // (at least one step per iteration)
+// Step loop of a graph replay: two conditional while nodes, the first running kLoopUnroll
+// steps per iteration while at least that many steps remain, the second one step per
+// iteration for the rest, so that no step of a replay past the target is launched (a gated
+// streaming kernel still costs its block launches).  A loop continues while steps remain, the
+// list is still valid, no list overflowed and the density regime the kernels were chosen for
+// still holds.  Each loop's condition is set before it by a node of the replay (k_loop_begin,
+// k_loop_mid) and after every iteration by one thread of its body (k_loop_ctl); an iteration
+// counter bounds every loop by target + 1 iterations, so a replay ends even if some step made
+// no progress.
+__device__ __forceinline__ bool loop_go(const Ctl *ctl, int n, int dense, int min_left) {
+    bool go = ctl->steps_done + min_left <= ctl->target && ctl->disp < ctl->half_skin &&
+              !(ctl->status & DEM_ERR_NEIGHBOR_OVERFLOW) && ctl->loop_iter <= ctl->target;
     if (go && n > 0) {   // the thresholds of adapt_density: leave the loop to switch kernel forms
         const double f = (double)ctl->last_ndefer / n;
         go = dense ? f >= 0.10 : !(f > 0.30);
     }
+    return go;
+}
+__global__ void k_loop_begin(Ctl *ctl, cudaGraphConditionalHandle h, int n, int dense, int min_left) {
+    if (threadIdx.x != 0) return;
+    ctl->loop_iter = 0;
+    // the first step of a run is always taken (the density of the step before the run does
+    // not decide the form of the run's first steps)
+    const bool go = ctl->steps_done + min_left <= ctl->target && ctl->disp < ctl->half_skin &&
+                    !(ctl->status & DEM_ERR_NEIGHBOR_OVERFLOW);
     cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+__global__ void k_loop_mid(Ctl *ctl, cudaGraphConditionalHandle h, int n, int dense) {
+    if (threadIdx.x != 0) return;
+    cudaGraphSetConditional(h, loop_go(ctl, n, dense, 1) ? 1u : 0u);
+}
+__global__ void k_loop_ctl(Ctl *ctl, cudaGraphConditionalHandle h, int n, int dense, int min_left) {
+    if (threadIdx.x != 0) return;
+    ++ctl->loop_iter;
+    cudaGraphSetConditional(h, loop_go(ctl, n, dense, min_left) ? 1u : 0u);
 }
 __global__ void k_invalidate(Ctl *ctl) {
     if (threadIdx.x == 0) ctl->disp = 1e300;
@@ -1050,14 +1066,70 @@ int capture_graph(dem_solver *s, int steps) {
     return DEM_OK;
 }
 
-// Steps per iteration of the graph while-loop: each iteration pays for the conditional and the
-// control kernel (about 5 us on a B200 with one step per iteration); steps past the target in
-// the last iteration are gated no-ops.
+// Steps per iteration of the first graph while-loop: each iteration pays for the conditional
+// and the control kernel (about 5 us on a B200).
 constexpr int kLoopUnroll = 8;
 
-// The step loop as one graph: a node resetting the loop counter, then a while node whose body
-// is kLoopUnroll steps (each with the neighbour build first in the rebuild-every-step mode) and
-// k_loop_ctl.
+// `steps` fused steps (each with the neighbour build first in the rebuild-every-step mode).
+static void capture_steps(dem_solver *s, int steps, cudaStream_t st) {
+    for (int k = 0; k < steps; ++k) {
+        if (ref_mode(s)) {
+            launch_build(s->p->P, s->p->alt, s->L, s->B, s->p->ctl, s->sp.delta, s->sp.skin, false, true, st);
+            if (s->mesh_nt > 0) launch_mesh_candidates(s->p->P, s->fc.mesh, s->p->ctl, s->sp.delta, s->sp.skin, st);
+        }
+        launch_step(s->p->P, s->L, s->p->ctl, s->fc, s->d_pp, s->d_pw, s->d_walls, MODE_FUSED, st, s->aux);
+    }
+}
+
+// Adds a while node after `dep` whose body is `steps` fused steps and k_loop_ctl.
+static cudaError_t add_loop(dem_solver *s, cudaGraph_t g, cudaGraphNode_t dep, cudaGraphConditionalHandle h, int steps,
+                            cudaGraphNode_t *node) {
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaError_t e = cudaGraphAddNode(node, g, &dep, 1, &cp);
+    if (e != cudaSuccess) return e;
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    cudaStream_t st = s->ctx->stream;
+    e = cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    capture_steps(s, steps, st);
+    k_loop_ctl<<<1, 32, 0, st>>>(s->p->ctl, h, s->p->P.n, s->fc.dense, steps);
+    return cudaStreamEndCapture(st, &body);
+}
+
+// One kernel node after `dep` (nullptr: a root node), captured from a launch on the stream.
+template <typename F>
+static cudaError_t add_kernel(cudaGraph_t g, cudaGraphNode_t dep, cudaStream_t st, F launch, cudaGraphNode_t *node) {
+    cudaError_t e = cudaStreamBeginCaptureToGraph(st, g, dep ? &dep : nullptr, nullptr, dep ? 1 : 0,
+                                                  cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    launch();
+    cudaGraph_t out = g;
+    e = cudaStreamEndCapture(st, &out);
+    if (e != cudaSuccess) return e;
+    // the node just added is the one without a dependent
+    size_t nn = 0;
+    e = cudaGraphGetNodes(g, nullptr, &nn);
+    if (e != cudaSuccess) return e;
+    std::vector<cudaGraphNode_t> nodes(nn);
+    e = cudaGraphGetNodes(g, nodes.data(), &nn);
+    if (e != cudaSuccess) return e;
+    for (cudaGraphNode_t c : nodes) {
+        size_t nd = 0;
+        if (cudaGraphNodeGetDependentNodes(c, nullptr, &nd) == cudaSuccess && nd == 0 && c != dep) {
+            cudaGraphNodeType t;
+            if (cudaGraphNodeGetType(c, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) *node = c;
+        }
+    }
+    return cudaSuccess;
+}
+
+// The step loop as one graph: k_loop_begin (loop counter reset, condition of the first loop),
+// a while node of kLoopUnroll steps per iteration, k_loop_mid (condition of the second loop),
+// a while node of one step per iteration.
 int capture_loop_graph(dem_solver *s) {
     dem_ctx *ctx = s->ctx;
     cudaStream_t st = ctx->stream;
@@ -1071,42 +1143,22 @@ int capture_loop_graph(dem_solver *s) {
     }
     cudaGraph_t g = nullptr;
     CK(cudaGraphCreate(&g, 0));
-    cudaGraphConditionalHandle h;
-    cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
-    if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
-    if (e == cudaSuccess) {
-        k_loop_begin<<<1, 32, 0, st>>>(s->p->ctl);
-        e = cudaStreamEndCapture(st, &g);
-    }
-    cudaGraphNode_t begin = nullptr;
-    size_t nnodes = 1;
-    if (e == cudaSuccess) e = cudaGraphGetNodes(g, &begin, &nnodes);
-    cudaGraphNodeParams cp = {};
-    cp.type = cudaGraphNodeTypeConditional;
-    cp.conditional.handle = h;
-    cp.conditional.type = cudaGraphCondTypeWhile;
-    cp.conditional.size = 1;
-    cudaGraphNode_t cnode = nullptr;
-    if (e == cudaSuccess) e = cudaGraphAddNode(&cnode, g, &begin, 1, &cp);
-    cudaGraph_t body = e == cudaSuccess ? cp.conditional.phGraph_out[0] : nullptr;
-    if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
-    if (e == cudaSuccess) {
-        for (int k = 0; k < kLoopUnroll; ++k) {
-            if (ref_mode(s)) {
-                launch_build(s->p->P, s->p->alt, s->L, s->B, s->p->ctl, s->sp.delta, s->sp.skin, false, true, st);
-                if (s->mesh_nt > 0) launch_mesh_candidates(s->p->P, s->fc.mesh, s->p->ctl, s->sp.delta, s->sp.skin, st);
-            }
-            launch_step(s->p->P, s->L, s->p->ctl, s->fc, s->d_pp, s->d_pw, s->d_walls, MODE_FUSED, st, s->aux);
-        }
-        k_loop_ctl<<<1, 32, 0, st>>>(s->p->ctl, h, s->p->P.n, s->fc.dense);
-        e = cudaStreamEndCapture(st, &body);
-    }
+    cudaGraphConditionalHandle h8, h1;
+    cudaError_t e = cudaGraphConditionalHandleCreate(&h8, g, 0, cudaGraphCondAssignDefault);
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h1, g, 0, cudaGraphCondAssignDefault);
+    const int n = s->p->P.n, dense = s->fc.dense;
+    Ctl *ctl = s->p->ctl;
+    cudaGraphNode_t begin = nullptr, loop8 = nullptr, mid = nullptr, loop1 = nullptr;
+    if (e == cudaSuccess)
+        e = add_kernel(g, nullptr, st, [&] { k_loop_begin<<<1, 32, 0, st>>>(ctl, h8, n, dense, kLoopUnroll); }, &begin);
+    if (e == cudaSuccess) e = add_loop(s, g, begin, h8, kLoopUnroll, &loop8);
+    if (e == cudaSuccess)
+        e = add_kernel(g, loop8, st, [&] { k_loop_mid<<<1, 32, 0, st>>>(ctl, h1, n, dense); }, &mid);
+    if (e == cudaSuccess) e = add_loop(s, g, mid, h1, 1, &loop1);
     if (e == cudaSuccess) e = cudaGraphInstantiate(&s->graph, g, 0);
     cudaGraphDestroy(g);
     CK(e);
-    s->graph_nodes = kLoopUnroll * (kernels_per_step(s->fc) +
-                                    (ref_mode(s) ? build_kernel_count(false) + (s->mesh_nt > 0 ? 1 : 0) : 0)) +
-                     1;   // per iteration
+    s->graph_nodes = kernels_per_step(s->fc) + (ref_mode(s) ? build_kernel_count(false) + (s->mesh_nt > 0 ? 1 : 0) : 0);
     s->graph_steps = -1;
     s->graph_version = s->version;
     return DEM_OK;
@@ -1308,7 +1360,12 @@ extern "C" int dem_solver_run(dem_solver *s, int nsteps) {
         return DEM_OK;
     };
     // kernels one replay launched: per iteration of the loop graph, per captured step otherwise
-    auto count_launches = [&](const Ctl &c) { s->launches += s->loop ? 1 + (long)c.loop_iter * s->graph_nodes : s->graph_nodes; };
+    // (loop graph: every step's kernels, a control kernel per iteration, the two condition nodes)
+    int steps_before = 0;
+    auto count_launches = [&](const Ctl &c) {
+        s->launches += s->loop ? 2 + (long)(c.steps_done - steps_before) * s->graph_nodes + c.loop_iter : s->graph_nodes;
+        steps_before = c.steps_done;
+    };
     if (ref_mode(s)) {
         // rebuild before every force pass, inside the graph (no re-sort)
         for (;;) {
