@@ -8,7 +8,9 @@ caller-index order, whatever its cutoff or the re-sort):
                         particle in dense steps, 8 in sparse ones), 1, 4 or 8 (the three-kernel
                         step with that cooperative width)
 * ``dense_form``        dense steps as one kernel (1) or as the pair-parallel three kernels (2)
-* ``stream_block``      block size (tile) of the streaming kernel (64, 128, 256)
+* ``stream_split``      streaming pass: 0 automatic (one persistent kernel over tiles staged in
+                        shared memory) or 1 (one thread per particle, ``stream_block`` wide blocks)
+* ``stream_block``      block size of the one-thread-per-particle streaming kernel (64, 128, 256)
 * ``steps_per_launch``  0: the step loop as a graph while-loop; else fused steps per captured graph
 * ``skin``              Verlet skin, i.e. the rebuild cadence
 
@@ -28,10 +30,11 @@ import time
 
 from . import api
 
-DEFAULTS = dict(contact_lanes=0, dense_form=0, stream_block=128, steps_per_launch=0, skin_factor=1.0)
-CANDIDATES = dict(contact_lanes=(0, 1, 4, 8), dense_form=(1, 2), stream_block=(64, 128, 256),
+DEFAULTS = dict(contact_lanes=0, dense_form=0, stream_split=0, stream_block=128, steps_per_launch=0,
+                skin_factor=1.0)
+CANDIDATES = dict(contact_lanes=(0, 1, 4, 8), dense_form=(1, 2), stream_split=(0, 1), stream_block=(64, 128, 256),
                   steps_per_launch=(0, 32), skin_factor=(0.5, 1.0, 2.0))
-ORDER = ("contact_lanes", "dense_form", "stream_block", "steps_per_launch", "skin_factor")
+ORDER = ("contact_lanes", "dense_form", "stream_split", "stream_block", "steps_per_launch", "skin_factor")
 
 
 def cache_path():
@@ -113,7 +116,7 @@ def _solver_kwargs(cfg):
     full = dict(DEFAULTS)
     full.update(cfg)
     return dict(stream_block=full["stream_block"], steps_per_launch=full["steps_per_launch"],
-                contact_lanes=full["contact_lanes"], dense_form=full["dense_form"])
+                contact_lanes=full["contact_lanes"], dense_form=full["dense_form"], stream_split=full["stream_split"])
 
 
 def apply(sc, cfg):

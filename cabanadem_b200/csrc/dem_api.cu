@@ -14,6 +14,7 @@
 #include <string>
 #include <tuple>
 #include <limits>
+#include <thread>
 #include <vector>
 
 #include "b200dem.h"
@@ -129,6 +130,30 @@ cudaError_t dalloc(T **p, size_t count) {
     *p = nullptr;
     if (count == 0) count = 1;
     return cudaMalloc((void **)p, count * sizeof(T));
+}
+
+// Runs f(begin, end) over [0, n) split across the host's cores (at most 32 threads, at least
+// 256k elements each); smaller ranges run on the calling thread.  For the host-side passes over
+// per-particle arrays that sit between the copies of a set/run/get cycle.
+template <typename F>
+void host_parallel(long n, F f) {
+    const long kMinChunk = 1L << 18;
+    long nt = std::min<long>(std::max(1u, std::thread::hardware_concurrency()), 32);
+    nt = std::min(nt, (n + kMinChunk - 1) / kMinChunk);
+    if (nt <= 1) {
+        f(0L, n, 0);
+        return;
+    }
+    const long chunk = (n + nt - 1) / nt;
+    std::vector<std::thread> th;
+    for (long t = 1; t < nt; ++t) th.emplace_back(f, std::min(n, t * chunk), std::min(n, (t + 1) * chunk), (int)t);
+    f(0L, std::min(n, chunk), 0);
+    for (auto &x : th) x.join();
+}
+int host_threads(long n) {
+    const long kMinChunk = 1L << 18;
+    long nt = std::min<long>(std::max(1u, std::thread::hardware_concurrency()), 32);
+    return (int)std::max(1L, std::min(nt, (n + kMinChunk - 1) / kMinChunk));
 }
 
 // ---- staging kernels (caller order <-> sorted order) --------------------------------
@@ -252,8 +277,11 @@ __global__ void k_init_particles(Particles P) {
         for (int k = 0; k < P.mc; ++k) P.tidx[(long)k * P.cap + i] = -1;
     }
 }
-__global__ void k_run_begin(Ctl *ctl, int target, double half_skin) {
+// `fresh_list`: every step builds its list first (the rebuild-every-step mode), so a list
+// invalidated by a change of the particles is not stale for the run's first step.
+__global__ void k_run_begin(Ctl *ctl, int target, double half_skin, int fresh_list = 0) {
     if (threadIdx.x == 0) {
+        if (fresh_list) ctl->disp = 0.0;
         ctl->steps_done = 0;
         ctl->target = target;
         ctl->half_skin = half_skin;
@@ -271,10 +299,11 @@ __global__ void k_run_begin(Ctl *ctl, int target, double half_skin) {
 // k_loop_mid) and after every iteration by one thread of its body (k_loop_ctl); an iteration
 // counter bounds every loop by target + 1 iterations, so a replay ends even if some step made
 // no progress.
+// `dense` < 0: the kernel forms do not depend on the density (no density exit).
 __device__ __forceinline__ bool loop_go(const Ctl *ctl, int n, int dense, int min_left) {
     bool go = ctl->steps_done + min_left <= ctl->target && ctl->disp < ctl->half_skin &&
-              !(ctl->status & DEM_ERR_NEIGHBOR_OVERFLOW) && ctl->loop_iter <= ctl->target;
-    if (go && n > 0) {   // the thresholds of adapt_density: leave the loop to switch kernel forms
+              !(ctl->status & kStopBits) && ctl->loop_iter <= ctl->target;
+    if (go && n > 0 && dense >= 0) {   // the thresholds of adapt_density: leave the loop to switch kernel forms
         const double f = (double)ctl->last_ndefer / n;
         go = dense ? f >= 0.10 : !(f > 0.30);
     }
@@ -286,12 +315,14 @@ __global__ void k_loop_begin(Ctl *ctl, cudaGraphConditionalHandle h, int n, int 
     // the first step of a run is always taken (the density of the step before the run does
     // not decide the form of the run's first steps)
     const bool go = ctl->steps_done + min_left <= ctl->target && ctl->disp < ctl->half_skin &&
-                    !(ctl->status & DEM_ERR_NEIGHBOR_OVERFLOW);
+                    !(ctl->status & kStopBits);
     cudaGraphSetConditional(h, go ? 1u : 0u);
 }
 __global__ void k_loop_mid(Ctl *ctl, cudaGraphConditionalHandle h, int n, int dense) {
     if (threadIdx.x != 0) return;
-    cudaGraphSetConditional(h, loop_go(ctl, n, dense, 1) ? 1u : 0u);
+    // no iteration of the first loop (fewer steps left than it takes): the replay's first step
+    // is taken here, whatever the density (as in k_loop_begin)
+    cudaGraphSetConditional(h, loop_go(ctl, n, ctl->loop_iter == 0 ? -1 : dense, 1) ? 1u : 0u);
 }
 __global__ void k_loop_ctl(Ctl *ctl, cudaGraphConditionalHandle h, int n, int dense, int min_left) {
     if (threadIdx.x != 0) return;
@@ -489,9 +520,17 @@ extern "C" int dem_particles_set(dem_particles *p, int field, const void *host, 
     cudaStream_t s = ctx->stream;
     Particles &P = p->P;
     if (field == DEM_F_RHO || field == DEM_F_E || field == DEM_F_NU || field == DEM_F_G) {
+        // host copies; the material table is re-derived only when E, nu or G changed
         std::vector<double> &dst = field == DEM_F_RHO ? p->rho : field == DEM_F_E ? p->E : field == DEM_F_NU ? p->nu : p->G;
-        std::memcpy(dst.data(), host, sizeof(double) * n);
-        if (field != DEM_F_RHO) p->mat_dirty = true;
+        const double *src = (const double *)host;
+        std::vector<char> changed(host_threads(n), 0);
+        host_parallel(n, [&](long b, long e, int t) {
+            if (e > b && std::memcmp(dst.data() + b, src + b, sizeof(double) * (e - b)) != 0) {
+                std::memcpy(dst.data() + b, src + b, sizeof(double) * (e - b));
+                changed[t] = 1;
+            }
+        });
+        if (field != DEM_F_RHO && std::find(changed.begin(), changed.end(), 1) != changed.end()) p->mat_dirty = true;
         return DEM_OK;
     }
     void *tmp = p->stage;
@@ -503,8 +542,13 @@ extern "C" int dem_particles_set(dem_particles *p, int field, const void *host, 
         case DEM_F_RAD: {
             k_scatter_pos<<<kGS, kTB, 0, s>>>((double *)tmp, P.pos[cur], n, P.rank, 1);
             const double *r = (const double *)host;
-            p->rmax = 0.0;
-            for (int i = 0; i < n; ++i) p->rmax = std::max(p->rmax, r[i]);
+            std::vector<double> part(host_threads(n), 0.0);
+            host_parallel(n, [&](long b, long e, int t) {
+                double m = 0.0;
+                for (long i = b; i < e; ++i) m = std::max(m, r[i]);
+                part[t] = m;
+            });
+            p->rmax = *std::max_element(part.begin(), part.end());
             break;
         }
         case DEM_F_U: k_scatter_d<<<kGS, kTB, 0, s>>>((double *)tmp, P.vel[vcur], n, 3, P.cap, P.rank); break;
@@ -733,27 +777,55 @@ int prepare(dem_solver *s) {
     cudaStream_t st = ctx->stream;
     const int n = p->P.n;
     if (p->mat_dirty) {
-        std::map<std::tuple<double, double, double>, int> ids;
+        // materials = distinct (E, nu, G) in order of first appearance in caller order: each
+        // host thread lists those of its range in order, the lists are merged in range order,
+        // then each thread writes its particles' material ids
+        using Mat = std::tuple<double, double, double>;
+        const int nt = host_threads(n);
+        std::vector<std::vector<Mat>> found(nt);
+        auto index_of = [](const std::vector<Mat> &v, const Mat &k) {
+            for (size_t a = 0; a < v.size(); ++a)
+                if (v[a] == k) return (int)a;
+            return -1;
+        };
+        host_parallel(n, [&](long b, long e, int t) {
+            std::vector<Mat> &mine = found[t];
+            int last = -1;   // neighbours in caller order usually share a material: test it first
+            for (long i = b; i < e && (int)mine.size() <= kMaxMat; ++i) {
+                const Mat k(p->E[i], p->nu[i], p->G[i]);
+                if (last >= 0 && mine[last] == k) continue;
+                last = index_of(mine, k);
+                if (last < 0) {
+                    last = (int)mine.size();
+                    mine.push_back(k);
+                }
+            }
+        });
         p->mats.clear();
-        p->mat.assign(n, 0);
-        int last = -1;   // neighbours in caller order usually share a material: test it first
-        for (int i = 0; i < n; ++i) {
-            const double E = p->E[i], nu = p->nu[i], G = p->G[i];
-            if (last >= 0 && std::get<0>(p->mats[last]) == E && std::get<1>(p->mats[last]) == nu &&
-                std::get<2>(p->mats[last]) == G) {
+        for (const auto &mine : found)
+            for (const Mat &k : mine)
+                if (index_of(p->mats, k) < 0) p->mats.push_back(k);
+        if ((int)p->mats.size() > kMaxMat) {
+            p->mats.clear();
+            return fail(ctx, DEM_ERR_UNSUPPORTED, "more than 32 distinct (E, nu, G) materials");
+        }
+        p->mat.resize(n);
+        std::vector<char> nan(nt, 0);   // a NaN constant equals no material (not even its own)
+        host_parallel(n, [&](long b, long e, int t) {
+            int last = 0;
+            for (long i = b; i < e; ++i) {
+                const Mat k(p->E[i], p->nu[i], p->G[i]);
+                if (!(p->mats[last] == k)) last = index_of(p->mats, k);
+                if (last < 0) {
+                    nan[t] = 1;
+                    last = 0;
+                }
                 p->mat[i] = (uint8_t)last;
-                continue;
             }
-            auto key = std::make_tuple(E, nu, G);
-            auto it = ids.find(key);
-            if (it == ids.end()) {
-                if ((int)p->mats.size() >= kMaxMat)
-                    return fail(ctx, DEM_ERR_UNSUPPORTED, "more than 32 distinct (E, nu, G) materials");
-                it = ids.emplace(key, (int)p->mats.size()).first;
-                p->mats.push_back(key);
-            }
-            last = it->second;
-            p->mat[i] = (uint8_t)last;
+        });
+        if (std::find(nan.begin(), nan.end(), 1) != nan.end()) {
+            p->mats.clear();
+            return fail(ctx, DEM_ERR_INVALID, "a particle's E, nu or G is not a number");
         }
         // through the staging buffer (cap * 24 bytes or more) of the particle set
         uint8_t *tmp = (uint8_t *)p->stage;
@@ -861,9 +933,10 @@ int prepare(dem_solver *s) {
     fc.has_fix = p->any_fix ? 1 : 0;
     fc.mixed = s->sp.precision == DEM_MIXED ? 1 : 0;
     fc.stream_block = (s->sp.stream_block == 64 || s->sp.stream_block == 256) ? s->sp.stream_block : 128;
-    // one streaming kernel unless asked: on the 2M lattice (B200) the split forms ran the step in
-    // 76.5 us (two kernels) and 78.4 us (two branches) against 67.6 us
-    fc.split = (s->sp.stream_split >= 1 && s->sp.stream_split <= 3) ? s->sp.stream_split : 1;
+    // the staged streaming kernel unless asked: on the 2M lattice (B200, kernel time per step over
+    // 1,000 steps) 64.1 us against 68.1 us with one thread per particle; the split forms ran the
+    // step in 76.5 us (two kernels) and 78.4 us (two branches)
+    fc.split = (s->sp.stream_split >= 1 && s->sp.stream_split <= 4) ? s->sp.stream_split : 4;
     pick_contact_kernel(s);
     fc.scenes = s->nscenes > 0 ? s->d_scenes : nullptr;
     fc.wps = s->nscenes > 0 ? s->wps : 0;
@@ -889,12 +962,13 @@ void free_pairs(dem_solver *s) {
     s->L.prec = nullptr;
 }
 
-// Work-item buffers of the pair-parallel dense step: one item per list entry at most, so
-// maxnb * cap items (16 B each, and 48 B of force/torque terms).
+// Work-item buffers of the pair-parallel dense step: one item per list entry and one per wall
+// at most, so (maxnb + mw) * cap items (16 B each, and 48 B of force/torque terms); the item
+// count cannot pass the buffer.
 int ensure_pairs(dem_solver *s) {
     if (s->L.pitem) return DEM_OK;
     dem_ctx *ctx = s->ctx;
-    const size_t items = (size_t)s->L.maxnb * s->p->P.cap;
+    const size_t items = ((size_t)s->L.maxnb + std::max(s->p->P.mw, 0)) * s->p->P.cap;
     CK(dalloc(&s->L.pitem, items));
     CK(dalloc(&s->L.pterm, 3 * items));
     CK(dalloc(&s->L.prec, (size_t)s->p->P.cap));
@@ -969,10 +1043,17 @@ void pick_contact_kernel(dem_solver *s) {
     }
 }
 
+// Whether the kernel forms depend on the density: not for small systems (one kernel per step
+// at any density) nor for a pair-parallel step the caller forced (dense_form 2).
+bool density_matters(const dem_solver *s) {
+    return s->fc.all == 0 || (s->p->P.n > kOneKernelMaxN && s->sp.dense_form != 2);
+}
+
 // Pick the contact-kernel build for the next graph from the last step's deferred count: the
 // dense build (more resident blocks, wider apply grid) above 30 % of the particles, back to
 // the sparse one below 10 %.  Same arithmetic either way; a switch re-captures the graph.
 void adapt_density(dem_solver *s, const Ctl &c) {
+    if (!density_matters(s)) return;
     const int n = s->p->P.n;
     const double f = n > 0 ? (double)c.last_ndefer / n : 0.0;
     const int want = s->fc.dense ? (f >= 0.10 ? 1 : 0) : (f > 0.30 ? 1 : 0);
@@ -1083,7 +1164,7 @@ static void capture_steps(dem_solver *s, int steps, cudaStream_t st) {
 
 // Adds a while node after `dep` whose body is `steps` fused steps and k_loop_ctl.
 static cudaError_t add_loop(dem_solver *s, cudaGraph_t g, cudaGraphNode_t dep, cudaGraphConditionalHandle h, int steps,
-                            cudaGraphNode_t *node) {
+                            int dense, cudaGraphNode_t *node) {
     cudaGraphNodeParams cp = {};
     cp.type = cudaGraphNodeTypeConditional;
     cp.conditional.handle = h;
@@ -1096,7 +1177,7 @@ static cudaError_t add_loop(dem_solver *s, cudaGraph_t g, cudaGraphNode_t dep, c
     e = cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return e;
     capture_steps(s, steps, st);
-    k_loop_ctl<<<1, 32, 0, st>>>(s->p->ctl, h, s->p->P.n, s->fc.dense, steps);
+    k_loop_ctl<<<1, 32, 0, st>>>(s->p->ctl, h, s->p->P.n, dense, steps);
     return cudaStreamEndCapture(st, &body);
 }
 
@@ -1146,15 +1227,15 @@ int capture_loop_graph(dem_solver *s) {
     cudaGraphConditionalHandle h8, h1;
     cudaError_t e = cudaGraphConditionalHandleCreate(&h8, g, 0, cudaGraphCondAssignDefault);
     if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h1, g, 0, cudaGraphCondAssignDefault);
-    const int n = s->p->P.n, dense = s->fc.dense;
+    const int n = s->p->P.n, dense = density_matters(s) ? s->fc.dense : -1;
     Ctl *ctl = s->p->ctl;
     cudaGraphNode_t begin = nullptr, loop8 = nullptr, mid = nullptr, loop1 = nullptr;
     if (e == cudaSuccess)
         e = add_kernel(g, nullptr, st, [&] { k_loop_begin<<<1, 32, 0, st>>>(ctl, h8, n, dense, kLoopUnroll); }, &begin);
-    if (e == cudaSuccess) e = add_loop(s, g, begin, h8, kLoopUnroll, &loop8);
+    if (e == cudaSuccess) e = add_loop(s, g, begin, h8, kLoopUnroll, dense, &loop8);
     if (e == cudaSuccess)
         e = add_kernel(g, loop8, st, [&] { k_loop_mid<<<1, 32, 0, st>>>(ctl, h1, n, dense); }, &mid);
-    if (e == cudaSuccess) e = add_loop(s, g, mid, h1, 1, &loop1);
+    if (e == cudaSuccess) e = add_loop(s, g, mid, h1, 1, dense, &loop1);
     if (e == cudaSuccess) e = cudaGraphInstantiate(&s->graph, g, 0);
     cudaGraphDestroy(g);
     CK(e);
@@ -1344,7 +1425,7 @@ extern "C" int dem_solver_run(dem_solver *s, int nsteps) {
     if (ref_mode(s)) half_skin = 1e300;
     else if (s->sp.delta > 0.0) half_skin = std::max(0.0, s->sp.delta - 2.0 * s->p->rmax) / 2.0;
     else half_skin = s->sp.skin / 2.0;
-    k_run_begin<<<1, 32, 0, st>>>(s->p->ctl, nsteps, half_skin);
+    k_run_begin<<<1, 32, 0, st>>>(s->p->ctl, nsteps, half_skin, ref_mode(s) ? 1 : 0);
     launch_prologue(s->p->P, s->p->ctl, s->fc, st);
     s->launches += 2;
     s->graph_done_mark = 0;
@@ -1379,6 +1460,7 @@ extern "C" int dem_solver_run(dem_solver *s, int nsteps) {
                 CK(cudaGraphLaunch(s->graph, st));
                 c = read_ctl(s);
                 count_launches(c);
+                if (c.status & DEM_ERR_TIMEOUT) return fail(ctx, DEM_ERR_TIMEOUT, "a bounded device wait gave up");
                 adapt_density(s, c);
                 if (c.steps_done >= c.target || (c.status & DEM_ERR_NEIGHBOR_OVERFLOW) || c.steps_done == done_before)
                     break;
@@ -1419,6 +1501,7 @@ extern "C" int dem_solver_run(dem_solver *s, int nsteps) {
             Ctl c = read_ctl(s);
             CK(cudaGetLastError());
             count_launches(c);
+            if (c.status & DEM_ERR_TIMEOUT) return fail(ctx, DEM_ERR_TIMEOUT, "a bounded device wait gave up");
             adapt_density(s, c);
             {
                 float ms = 0.f;

@@ -372,7 +372,7 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contact_coop(Particles P, NbrL
     // one row per group, padded by one word so that the groups of a warp fall in different banks
     __shared__ int s_tidx[kBlock / NL][kCoopSlots + 1];
     __shared__ double s_h[kBlock / NL][3 * kCoopSlots + 1];
-    if (ctl->steps_done >= ctl->target || (ctl->status & DEM_ERR_NEIGHBOR_OVERFLOW) || !(ctl->disp < ctl->half_skin))
+    if (ctl->steps_done >= ctl->target || (ctl->status & kStopBits) || !(ctl->disp < ctl->half_skin))
         return;
     const int nd = ctl->ndefer;
     const int warp = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);

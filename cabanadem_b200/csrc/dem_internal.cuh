@@ -73,6 +73,10 @@ __host__ __device__ __forceinline__ double2 load_mI(const Particles &P, int i) {
     return make_double2(P.mI[i], P.mI[(long)P.cap + i]);
 }
 
+// Status bits that stop a run's steps (every gated kernel exits, the step loop ends): a list
+// that overflowed (the host grows it and continues) and a bounded device wait that gave up (the
+// run returns DEM_ERR_TIMEOUT).
+constexpr int kStopBits = DEM_ERR_NEIGHBOR_OVERFLOW | DEM_ERR_TIMEOUT;
 constexpr int kCoopSlots = 32;   // largest MaxCnts the cooperative contact kernel stages in shared memory
 constexpr int kOneKernelMaxN = 65536;   // particle count up to which the step is always one kernel
 constexpr int kVmaxSlots = 32;   // blocks fold their max into slot blockIdx % 32 (word 32 * slot)
@@ -123,7 +127,8 @@ struct ForceConsts {
     int stream_block;          // k_stream block size: 64, 128 or 256
     int split;                 // streaming pass: 1 one kernel over every particle (k_stream);
                                // 2 the lone particles and the rest in two persistent kernels
-                               // (k_stream_lone, k_stream_rest); 3 the same as concurrent branches
+                               // (k_stream_lone, k_stream_rest); 3 the same as concurrent branches;
+                               // 4 one persistent kernel over bulk-staged tiles (k_stream_bulk)
     int dense;                 // 1: most particles are in contact -- contact kernels compiled for
                                // more resident blocks, wider apply grid (same arithmetic)
     int coop;                  // lanes per deferred particle in the contact kernel: 4 or 8
@@ -152,9 +157,10 @@ struct NbrList {
     int *defer;  // [cap] particles deferred to the contact kernel in the current step
     double *defer_v, *defer_w;  // [3][cap] new u, omega of deferred particle t (slot t)
     // pair-parallel dense step (dem_pairs.cuh), allocated when that form is first used:
-    int4 *pitem;     // [maxnb * cap] contact work items (i, j, history slot or -1, -)
-    double2 *pterm;  // [3][maxnb * cap]: per item F (3) and tau (3) of particle i
-    int4 *prec;      // [cap] first item, item count, contact word at the step's start
+    int4 *pitem;     // [(maxnb + mw) * cap] contact work items: (i, j, history slot or -1, 0) or, for
+                     // a wall, (i, -1 - wall, scene-local wall, wall history flag)
+    double2 *pterm;  // [3][(maxnb + mw) * cap]: per item F (3) and tau (3) of particle i
+    int4 *prec;      // [cap] first item, pair items, contact word at the step's start, wall items
 };
 
 struct Grid {                 // one per scene, computed on the device at every build

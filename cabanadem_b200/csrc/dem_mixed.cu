@@ -19,7 +19,7 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contact_mixed(Particles P, Nbr
                                                           const PairConst *__restrict__ pp,
                                                           const PairConst *__restrict__ pw,
                                                           const WallGeom *__restrict__ walls) {
-    if (ctl->steps_done >= ctl->target || (ctl->status & DEM_ERR_NEIGHBOR_OVERFLOW) || !(ctl->disp < ctl->half_skin))
+    if (ctl->steps_done >= ctl->target || (ctl->status & kStopBits) || !(ctl->disp < ctl->half_skin))
         return;
     const int nd = ctl->ndefer;
     if ((long)blockIdx.x * blockDim.x >= nd) return;
@@ -141,7 +141,7 @@ static int fill_blocks(const void *kernel, int block, long work) {
 template <bool MESH>
 static void pairs_mixed_t(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
                           const PairConst *pw, const WallGeom *walls, cudaStream_t s) {
-    static int g2 = 0, g3 = 0, sms = 0, last_n = -1;
+    static thread_local int g2 = 0, g3 = 0, sms = 0, last_n = -1;
     if (last_n != P.n) {
         g2 = fill_blocks((const void *)k_pairs_eval<true>, kPairsBlock, 8L * P.n);
         g3 = fill_blocks((const void *)k_pairs_sum<true, MESH>, kPairsBlock, P.n);
@@ -151,9 +151,9 @@ static void pairs_mixed_t(const Particles &P, const NbrList &L, Ctl *ctl, const 
         if (sms <= 0) sms = 148;
         last_n = P.n;
     }
-    launch_pairs_find<true>(P, L, ctl, fc, sms, s);
-    k_pairs_eval<true><<<g2, kPairsBlock, 0, s>>>(P, L, ctl, fc, pp);
-    k_pairs_sum<true, MESH><<<g3, kPairsBlock, 0, s>>>(P, L, ctl, fc, pw, walls);
+    launch_pairs_find<true>(P, L, ctl, fc, walls, sms, s);
+    k_pairs_eval<true><<<g2, kPairsBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+    k_pairs_sum<true, MESH><<<g3, kPairsBlock, 0, s>>>(P, L, ctl, fc);
 }
 
 void launch_pairs_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,

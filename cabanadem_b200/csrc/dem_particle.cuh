@@ -90,7 +90,7 @@ __device__ __forceinline__ CtlSnap read_ctl(const Ctl *ctl, bool gated) {
         c.cur = ctl->cur;
         if (gated) {
             const bool stale = !(ctl->disp < ctl->half_skin);
-            c.go = (ctl->steps_done < ctl->target) && !(ctl->status & DEM_ERR_NEIGHBOR_OVERFLOW) && !stale;
+            c.go = (ctl->steps_done < ctl->target) && !(ctl->status & kStopBits) && !stale;
             c.last = (ctl->steps_done + 1 >= ctl->target);
         } else {
             c.go = !(ctl->status & DEM_ERR_NEIGHBOR_OVERFLOW);

@@ -16,6 +16,7 @@
 #include "b200dem.h"
 
 #include "dem_particle.cuh"
+#include "dem_bulk.cuh"
 #include "dem_contact_coop.cuh"
 #include "dem_pairs.cuh"
 
@@ -38,7 +39,7 @@ __global__ void __launch_bounds__(kBlock) k_force(Particles P, NbrList L, Ctl *c
 }
 
 __device__ __forceinline__ bool step_gate(const Ctl *ctl) {
-    return ctl->steps_done < ctl->target && !(ctl->status & DEM_ERR_NEIGHBOR_OVERFLOW) && ctl->disp < ctl->half_skin;
+    return ctl->steps_done < ctl->target && !(ctl->status & kStopBits) && ctl->disp < ctl->half_skin;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -256,6 +257,126 @@ __global__ void __launch_bounds__(BS, MINB) k_stream_rest(Particles P, NbrList L
         bool defer = false;
         if (i < P.n) defer = stream_particle(P, L, fc, walls, c, i, vmax2);
         defer_append(ctl, L, defer, i);
+    }
+    warp_vmax(ctl, P.vslots, vmax2, 0);
+}
+
+// Staged streaming pass (split 4): the body of k_stream over tiles of T consecutive particles,
+// their own state brought into shared memory by bulk asynchronous copies.  A persistent block
+// walks the tiles blockIdx.x, blockIdx.x + gridDim.x, ...; thread 0 keeps S tiles in flight
+// (each tile's rows -- position, velocity x/y/z, mass, contact word and, where the tile
+// reaches past the clear class, list length and the first two list rows -- as one copy per
+// row completing on the tile's barrier), so the HBM reads of the next tiles overlap the
+// partner loads and stores of the current one instead of waiting on per-thread loads.
+// Waits are bounded: a wait that gives up sets DEM_ERR_TIMEOUT, waits (bounded again) for
+// the block's copies still in flight and leaves the step unfinished.
+constexpr int kBulkWaitLimit = 1 << 18;
+
+template <int T>
+struct BulkTile {
+    static constexpr int POS = 0;                 // double4 [T]
+    static constexpr int VEL = POS + 32 * T;      // double [3][T]
+    static constexpr int MASS = VEL + 24 * T;     // double [T]
+    static constexpr int CS = MASS + 8 * T;       // int [T]
+    static constexpr int NN = CS + 4 * T;         // int [T]
+    static constexpr int IDX = NN + 4 * T;        // int [2][T]
+    static constexpr int BYTES = IDX + 8 * T;
+};
+
+#ifndef STREAM_BULK_MINB
+#define STREAM_BULK_MINB 1
+#endif
+template <int T, int S>
+__global__ void __launch_bounds__(T, STREAM_BULK_MINB) k_stream_bulk(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
+                                                   const WallGeom *__restrict__ walls) {
+    using B = BulkTile<T>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ uint64_t full[S];
+    __shared__ int s_fail;
+    if (!step_gate(ctl)) return;
+    const StreamCtl c = stream_ctl(ctl, P.n);
+    const int cap = P.cap;
+    const double4 *__restrict__ pc = P.pos[c.cur];
+    double *vc = P.vel[c.vcur];
+    const int ntiles = (P.n + T - 1) / T;
+    const int mine = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < S; ++k) bulk::bar_init(&full[k], 1);
+        bulk::bar_init_fence();
+        s_fail = 0;
+    }
+    __syncthreads();
+    // thread 0: the copies of this block's k-th tile into stage k % S
+    auto issue = [&](int k) {
+        const int i0 = (blockIdx.x + k * gridDim.x) * T;
+        const int m = min(T, cap - i0);   // cap is a multiple of 64, i0 of T: m is 64 or T
+        const bool lists = i0 + m > c.nclear_end;
+        const int rows = lists ? (L.maxnb > 1 ? 2 : L.maxnb) : 0;
+        unsigned char *sb = smem + (k % S) * B::BYTES;
+        uint64_t *bar = &full[k % S];
+        bulk::bar_arrive_expect(bar, (uint32_t)m * (32u + 24u + 8u + 4u + (lists ? 4u : 0u) + 4u * rows));
+        bulk::copy_g2s(sb + B::POS, pc + i0, 32u * m, bar);
+        for (int d = 0; d < 3; ++d) bulk::copy_g2s(sb + B::VEL + 8 * T * d, vc + (long)d * cap + i0, 8u * m, bar);
+        bulk::copy_g2s(sb + B::MASS, P.mI + i0, 8u * m, bar);
+        bulk::copy_g2s(sb + B::CS, P.cstate + i0, 4u * m, bar);
+        if (lists) bulk::copy_g2s(sb + B::NN, L.nn + i0, 4u * m, bar);
+        for (int r = 0; r < rows; ++r) bulk::copy_g2s(sb + B::IDX + 4 * T * r, L.idx + (long)r * cap + i0, 4u * m, bar);
+    };
+    if (threadIdx.x == 0)
+        for (int k = 0; k < S && k < mine; ++k) issue(k);
+    double vmax2 = 0.0;
+    int k = 0;
+    for (; k < mine; ++k) {
+        if (!bulk::bar_wait(&full[k % S], (k / S) & 1, kBulkWaitLimit)) s_fail = 1;
+        __syncthreads();
+        if (s_fail) break;
+        const unsigned char *sb = smem + (k % S) * B::BYTES;
+        const int t = threadIdx.x;
+        const int i = (blockIdx.x + k * gridDim.x) * T + t;
+        bool defer = false;
+        if (i < P.n) {
+            const D4 pi = reinterpret_cast<const D4 *>(sb + B::POS)[t];
+            const double *sv = reinterpret_cast<const double *>(sb + B::VEL);
+            const double ui0 = sv[t], ui1 = sv[T + t], ui2 = sv[2 * T + t];
+            const double m = reinterpret_cast<const double *>(sb + B::MASS)[t];
+            defer = reinterpret_cast<const int *>(sb + B::CS)[t] != 0;
+            // lone and clear particles: no listed neighbour can touch them this step
+            const int nn = i >= c.nclear_end ? reinterpret_cast<const int *>(sb + B::NN)[t] : 0;
+            if (!defer && nn > 0) {
+                const int *sidx = reinterpret_cast<const int *>(sb + B::IDX);
+                const D4 pa = ld4(pc, sidx[t]);
+                D4 pb = pa;
+                if (nn > 1) pb = ld4(pc, sidx[T + t]);
+                const double ax = pi.x - pa.x, ay = pi.y - pa.y, az = pi.z - pa.z;
+                const double sa = pi.w + pa.w;
+                defer = !(ax * ax + ay * ay + az * az >= sa * sa * 1.0000000001);
+                if (nn > 1) {
+                    const double bx = pi.x - pb.x, by = pi.y - pb.y, bz = pi.z - pb.z;
+                    const double sb2 = pi.w + pb.w;
+                    defer = defer || !(bx * bx + by * by + bz * bz >= sb2 * sb2 * 1.0000000001);
+                }
+            }
+            for (int kk = 2; kk < nn && !defer; ++kk) {
+                const int j = L.idx[(long)kk * cap + i];
+                const D4 pj = ld4(pc, j);
+                const double px = pi.x - pj.x, py = pi.y - pj.y, pz = pi.z - pj.z;
+                const double r2ij = px * px + py * py + pz * pz;
+                const double sr = pi.w + pj.w;
+                defer = !(r2ij >= sr * sr * 1.0000000001);
+            }
+            defer = wall_defer(P, fc, walls, i, pi, defer);
+            if (!defer) stream_free_step(P, fc, c, vc, i, pi, m, ui0, ui1, ui2, vmax2);
+        }
+        defer_append(ctl, L, defer, i);
+        __syncthreads();   // stage k % S consumed: thread 0 refills it
+        if (threadIdx.x == 0 && k + S < mine) issue(k + S);
+    }
+    if (k < mine) {   // a wait gave up: report, and let the copies in flight land before exiting
+        if (threadIdx.x == 0) {
+            atomicOr(&ctl->status, DEM_ERR_TIMEOUT);
+            for (int q = k; q < k + S && q < mine; ++q) bulk::bar_wait(&full[q % S], (q / S) & 1, kBulkWaitLimit);
+        }
+        return;
     }
     warp_vmax(ctl, P.vslots, vmax2, 0);
 }
@@ -532,11 +653,38 @@ void launch_prologue(const Particles &P, Ctl *ctl, const ForceConsts &fc, cudaSt
 
 int kernels_per_step(const ForceConsts &fc) {
     if (fc.all) return fc.all == 2 ? 3 : 1;
-    return fc.split >= 2 ? 4 : 3;
+    return fc.split == 2 || fc.split == 3 ? 4 : 3;
+}
+
+#ifndef STREAM_BULK_STAGES
+#define STREAM_BULK_STAGES 2
+#endif
+#ifndef STREAM_BULK_T
+#define STREAM_BULK_T 128
+#endif
+constexpr int kBulkT = STREAM_BULK_T, kBulkS = STREAM_BULK_STAGES;
+
+// Persistent grid of the staged streaming kernel: every block the SMs hold at its shared
+// memory, at most one per tile.
+static int bulk_blocks(int n) {
+    static thread_local int per = -1, sms = 0;
+    if (per < 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+        const int smem = kBulkS * BulkTile<kBulkT>::BYTES;
+        cudaFuncSetAttribute((const void *)k_stream_bulk<kBulkT, kBulkS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_stream_bulk<kBulkT, kBulkS>, kBulkT, smem);
+        if (per <= 0) per = 1;
+    }
+    const int tiles = (n + kBulkT - 1) / kBulkT;
+    return std::max(1, std::min(tiles, sms * per));
 }
 
 static int persistent_blocks(const void *kernel, int block, int n) {
-    static int sms = 0;
+    static thread_local int sms = 0;   // per host thread: solvers run concurrently from threads
     if (!sms) {
         int dev = 0;
         cudaGetDevice(&dev);
@@ -557,7 +705,7 @@ static void launch_step_t(const Particles &P, const NbrList &L, Ctl *ctl, const 
         if (fc.mixed) {
             launch_pairs_mixed(P, L, ctl, fc, pp, pw, walls, MESH, s);
         } else {
-            static int g2 = 0, g3 = 0, sms = 0, last_np = -1;
+            static thread_local int g2 = 0, g3 = 0, sms = 0, last_np = -1;
             if (last_np != P.n) {
                 g2 = persistent_blocks((const void *)k_pairs_eval<false>, kPairsBlock, 8 * P.n);
                 g3 = persistent_blocks((const void *)k_pairs_sum<false, MESH>, kPairsBlock, P.n);
@@ -567,12 +715,12 @@ static void launch_step_t(const Particles &P, const NbrList &L, Ctl *ctl, const 
                 if (sms <= 0) sms = 148;
                 last_np = P.n;
             }
-            launch_pairs_find<false>(P, L, ctl, fc, sms, s);
-            k_pairs_eval<false><<<g2, kPairsBlock, 0, s>>>(P, L, ctl, fc, pp);
-            k_pairs_sum<false, MESH><<<g3, kPairsBlock, 0, s>>>(P, L, ctl, fc, pw, walls);
+            launch_pairs_find<false>(P, L, ctl, fc, walls, sms, s);
+            k_pairs_eval<false><<<g2, kPairsBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+            k_pairs_sum<false, MESH><<<g3, kPairsBlock, 0, s>>>(P, L, ctl, fc);
         }
     } else if (mode == MODE_FUSED && fc.all) {
-        static int ga = 0, gma = 0, last_na = -1;
+        static thread_local int ga = 0, gma = 0, last_na = -1;
         if (last_na != P.n) {
             ga = persistent_blocks((const void *)k_contact_all<kContactMinBlocksDense, MESH>, kBlock, P.n);
             gma = persistent_blocks(contact_mixed_all_kernel(MESH), kBlock, P.n);
@@ -583,7 +731,7 @@ static void launch_step_t(const Particles &P, const NbrList &L, Ctl *ctl, const 
         else
             k_contact_all<kContactMinBlocksDense, MESH><<<ga, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
     } else if (mode == MODE_FUSED) {
-        static int gc = 0, gm = 0, gcd = 0, gmd = 0, gk4 = 0, gk8 = 0, gkm4 = 0, gkm8 = 0, last_n = -1;
+        static thread_local int gc = 0, gm = 0, gcd = 0, gmd = 0, gk4 = 0, gk8 = 0, gkm4 = 0, gkm8 = 0, last_n = -1;
         if (last_n != P.n) {
             // contact kernels: every block the SMs hold (a dense packing defers nearly every
             // particle; blocks past the deferred count exit at once); the apply kernel copies
@@ -599,10 +747,10 @@ static void launch_step_t(const Particles &P, const NbrList &L, Ctl *ctl, const 
             gkm8 = persistent_blocks(contact_mixed_kernel(0, 8, MESH), kBlock, 8 * P.n);
             last_n = P.n;
         }
-        if (fc.split >= 2) {
+        if (fc.split == 2 || fc.split == 3) {
             // lone particles and the rest in two persistent kernels; with the concurrent form
             // (split 3, an aux stream given) as two graph branches whose grids share the SMs
-            static int sms = 0;
+            static thread_local int sms = 0;
             if (!sms) {
                 int dev = 0;
                 cudaGetDevice(&dev);
@@ -622,6 +770,9 @@ static void launch_step_t(const Particles &P, const NbrList &L, Ctl *ctl, const 
                 k_stream_lone<128><<<glone, 128, 0, s>>>(P, L, ctl, fc, walls);
                 k_stream_rest<128, 9><<<grest, 128, 0, s>>>(P, L, ctl, fc, walls);
             }
+        } else if (fc.split == 4) {
+            k_stream_bulk<kBulkT, kBulkS><<<bulk_blocks(P.n), kBulkT, kBulkS * BulkTile<kBulkT>::BYTES, s>>>(
+                P, L, ctl, fc, walls);
         } else if (fc.stream_block == 64)
             k_stream<64, 16><<<(P.n + 63) / 64, 64, 0, s>>>(P, L, ctl, fc, walls);
         else if (fc.stream_block == 256)

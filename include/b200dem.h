@@ -118,10 +118,12 @@ typedef struct dem_solver_params {
                             * an apply kernel per step; while most are, one kernel over every
                             * particle.  1, 4 or 8: always the three-kernel step, its contact
                             * kernel with that many lanes per particle.  Same results.        */
-    int stream_split;      /* streaming pass of the three-kernel step: 0 = automatic (1), 1 one
+    int stream_split;      /* streaming pass of the three-kernel step: 0 = automatic (4), 1 one
                             * kernel over every particle, 2 the particles without listed
                             * neighbours and the rest in two kernels, 3 the same two kernels as
-                            * concurrent branches.  Same results.                              */
+                            * concurrent branches, 4 one persistent kernel whose tiles of
+                            * particles are staged in shared memory by bulk asynchronous
+                            * copies.  Same results.                                           */
     int dense_form;        /* step of a dense flow (most particles in contact, contact_lanes 0):
                             * 0 = automatic (2 above 65,536 particles, else 1), 1 one kernel
                             * with a thread per particle, 2 three kernels: contact search per

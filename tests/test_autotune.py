@@ -9,15 +9,16 @@ from cabanadem_b200 import autotune, scenarios as S
 
 
 def _cost(cfg):
-    # separable, minimum at contact_lanes 4, dense_form 2, stream_block 256, steps_per_launch 32,
-    # skin_factor 0.5
+    # separable, minimum at contact_lanes 4, dense_form 2, stream_split 1, stream_block 256,
+    # steps_per_launch 32, skin_factor 0.5
     return ({0: 4.0, 1: 3.0, 4: 1.0, 8: 2.0}[cfg["contact_lanes"]] + {0: 3.0, 1: 2.0, 2: 1.0}[cfg["dense_form"]]
+            + {0: 2.0, 1: 1.0}[cfg["stream_split"]]
             + {64: 3.0, 128: 2.0, 256: 1.0}[cfg["stream_block"]] + {0: 2.0, 32: 1.0}[cfg["steps_per_launch"]]
             + {0.5: 1.0, 1.0: 2.0, 2.0: 3.0}[cfg["skin_factor"]])
 
 
-BEST = dict(contact_lanes=4, dense_form=2, stream_block=256, steps_per_launch=32, skin_factor=0.5)
-NTRIALS = 1 + 3 + 2 + 2 + 1 + 2     # defaults + every other candidate of each knob
+BEST = dict(contact_lanes=4, dense_form=2, stream_split=1, stream_block=256, steps_per_launch=32, skin_factor=0.5)
+NTRIALS = 1 + 3 + 2 + 1 + 2 + 1 + 2     # defaults + every other candidate of each knob
 
 
 def test_coordinate_search_and_cache(tmp_path, monkeypatch):
@@ -34,14 +35,14 @@ def test_coordinate_search_and_cache(tmp_path, monkeypatch):
     assert calls[0] == autotune.DEFAULTS and len(calls) == NTRIALS
     table = json.loads((tmp_path / "tune.json").read_text())
     key = autotune.bucket(sc, 0)
-    assert key == "n2^8|p0|single" and table[key]["config"] == cfg and table[key]["s_per_step"] == 5.0
+    assert key == "n2^8|p0|single" and table[key]["config"] == cfg and table[key]["s_per_step"] == 6.0
     calls.clear()
     assert autotune.tune(S.random_box(n=400), precision=0) == cfg and calls == []   # same bucket: cached
     autotune.tune(sc, precision=1)
     assert len(calls) == NTRIALS                                      # another precision: tuned anew
     sc_skin = sc.skin
     kw = autotune.apply(sc, cfg)
-    assert kw == dict(stream_block=256, steps_per_launch=32, contact_lanes=4, dense_form=2)
+    assert kw == dict(stream_block=256, steps_per_launch=32, contact_lanes=4, dense_form=2, stream_split=1)
     assert sc.skin == sc_skin * 0.5
 
 

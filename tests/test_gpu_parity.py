@@ -155,14 +155,16 @@ def test_pair_parallel_contact_overflow():
     _assert_bitwise(s.particles.download(), ref, where="pairs overflow")
 
 
-@pytest.mark.parametrize("split", [1, 2, 3], ids=["one_kernel", "two_kernels", "two_branches"])
+@pytest.mark.parametrize("split", [1, 2, 3, 4], ids=["one_kernel", "two_kernels", "two_branches", "staged"])
 @pytest.mark.parametrize("packing", [1.0, 0.7], ids=["gas", "compressed"])
 def test_streaming_pass_forms_bitwise(split, packing):
     """The three-kernel step with each form of its streaming pass (one kernel; the particles
     without listed neighbours and the rest in two persistent kernels, in sequence or as
-    concurrent graph branches): bit-identical to the oracle over 1,500 steps with rebuilds,
-    on the C1 gas (most particles without a listed neighbour) and on a compressed box."""
-    sc = S.random_box(n=4096, nsteps=1500)
+    concurrent graph branches; one persistent kernel over tiles staged in shared memory):
+    bit-identical to the oracle over 1,500 steps with rebuilds, on the C1 gas (most particles
+    without a listed neighbour) and on a compressed box.  4,133 particles: the last staged
+    tile is a partial one."""
+    sc = S.random_box(n=4133, nsteps=1500)
     c = sc.state.x.mean(axis=0)
     sc.state.x[:] = c + (sc.state.x - c) * packing
     ref, _ = _oracle(sc, 1500)
@@ -173,11 +175,12 @@ def test_streaming_pass_forms_bitwise(split, packing):
     assert s.stats()["rebuilds"] >= 1
 
 
-@pytest.mark.parametrize("lanes", [0, 1, 8], ids=["auto", "per_thread", "coop8"])
+@pytest.mark.parametrize("lanes", [0, 1, 8, "pairs"], ids=["auto", "per_thread", "coop8", "pairs"])
 def test_moving_wall_bitwise(lanes):
     """A kinematic piston (DEM_Q6_WALL_STATIC clear) driven into a compressed box at 5 m/s,
     400 steps in three runs (each run's last step must not move the walls, its next run's
-    first drift must): particles and wall positions bit-identical to the oracle."""
+    first drift must): particles and wall positions bit-identical to the oracle.  "pairs" is
+    the pair-parallel step, whose wall contacts are work items of their own."""
     sc = S.piston_box(n=4096, speed=5.0, nsteps=400)
     c = sc.state.x.mean(axis=0)
     sc.state.x[:] = c + (sc.state.x - c) * 0.8
@@ -185,10 +188,10 @@ def test_moving_wall_bitwise(lanes):
     ref = sc.state.copy()
     w = sc.walls.copy()
     O.run(ref, w, sc.params, sc.dt, 400, skin=sc.skin, gravity=sc.gravity, pow_mode=O.POW_SQRT)
-    s = api.from_scenario(sc, contact_lanes=lanes)
+    s = api.from_scenario(sc, **(dict(dense_form=2) if lanes == "pairs" else dict(contact_lanes=lanes)))
     for n in (150, 101, 149):
         s.run_steps(n)
-    _assert_bitwise(s.particles.download(), ref, where="piston%d" % lanes)
+    _assert_bitwise(s.particles.download(), ref, where="piston%s" % lanes)
     assert np.array_equal(s.wall_positions(), w.x)
     assert w.x[1, 0] < sc.walls.x[1, 0]
     # particles in sliding contact with the piston (history tangential to its normal, -x)
