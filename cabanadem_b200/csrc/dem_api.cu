@@ -887,6 +887,8 @@ int prepare(dem_solver *s) {
     CK(cudaMemcpyAsync(s->d_pp, pp.data(), pp.size() * sizeof(PairConst), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(s->d_pw, pw.data(), pw.size() * sizeof(PairConst), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(s->d_walls, wg.data(), wg.size() * sizeof(WallGeom), cudaMemcpyHostToDevice, st));
+    // the wall-gap flags of the last build were taken against the previous walls
+    CK(cudaMemsetAsync(&p->ctl->wfar_build, 0xff, sizeof(long long), st));
     // mesh: particle materials against the mesh's, in the plane walls' expression order
     cudaFree(s->d_mesh_pm);
     s->d_mesh_pm = nullptr;
@@ -982,6 +984,7 @@ int alloc_lists(dem_solver *s, int maxnb) {
     cudaFree(s->L.defer);
     cudaFree(s->L.defer_v);
     cudaFree(s->L.defer_w);
+    cudaFree(s->L.wfar);
     const bool pairs = s->L.pitem != nullptr;
     free_pairs(s);
     s->L.maxnb = maxnb;
@@ -990,7 +993,9 @@ int alloc_lists(dem_solver *s, int maxnb) {
     CK(dalloc(&s->L.defer, s->p->P.cap));
     CK(dalloc(&s->L.defer_v, 3 * (size_t)s->p->P.cap));
     CK(dalloc(&s->L.defer_w, 3 * (size_t)s->p->P.cap));
+    CK(dalloc(&s->L.wfar, (size_t)s->p->P.cap));
     CK(cudaMemsetAsync(s->L.nn, 0, sizeof(int) * s->p->P.cap, ctx->stream));
+    CK(cudaMemsetAsync(s->L.wfar, 0, s->p->P.cap, ctx->stream));
     if (pairs) {
         const int st = ensure_pairs(s);
         if (st) return st;
@@ -1100,6 +1105,14 @@ int build_with(dem_solver *s, bool resort, double delta, double skin) {
         if (!(c.status & DEM_ERR_NEIGHBOR_OVERFLOW)) {
             if (s->mesh_nt > 0) {
                 launch_mesh_candidates(s->p->P, s->fc.mesh, s->p->ctl, delta, skin, ctx->stream);
+                s->launches += 1;
+                CK(cudaGetLastError());
+            }
+            // wall-gap flags against the stale threshold of the solver's runs
+            const double half = s->sp.delta > 0.0 ? std::max(0.0, s->sp.delta - 2.0 * s->p->rmax) / 2.0
+                                                  : s->sp.skin / 2.0;
+            if (s->d_walls && s->fc.nwall > 0) {
+                launch_wall_far(s->p->P, s->L, s->p->ctl, s->fc, s->d_walls, half, ctx->stream);
                 s->launches += 1;
                 CK(cudaGetLastError());
             }
@@ -1331,6 +1344,7 @@ extern "C" int dem_solver_destroy(dem_solver *s) {
     if (s->aux.join) cudaEventDestroy(s->aux.join);
     cudaFree(s->d_pp); cudaFree(s->d_pw); cudaFree(s->d_walls); cudaFree(s->d_scenes);
     cudaFree(s->L.nn); cudaFree(s->L.idx); cudaFree(s->L.defer); cudaFree(s->L.defer_v); cudaFree(s->L.defer_w);
+    cudaFree(s->L.wfar);
     free_pairs(s);
     BuildBuffers &B = s->B;
     cudaFree(B.grid); cudaFree(B.total); cudaFree(B.key); cudaFree(B.cell_start); cudaFree(B.cell_fill); cudaFree(B.cell_items);

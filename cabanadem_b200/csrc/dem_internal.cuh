@@ -47,6 +47,7 @@ struct Ctl {
                               // exceeded skin/2 at the last build (placed second)
     int npairs;               // contact work items of the current step (pair-parallel dense step)
     int loop_iter;            // iterations of the step loop in the current graph replay
+    long long wfar_build;     // value of `rebuilds` when NbrList::wfar was last computed
 };
 
 struct Particles {
@@ -161,6 +162,8 @@ struct NbrList {
                      // a wall, (i, -1 - wall, scene-local wall, wall history flag)
     double2 *pterm;  // [3][(maxnb + mw) * cap]: per item F (3) and tau (3) of particle i
     int4 *prec;      // [cap] first item, pair items, contact word at the step's start, wall items
+    uint8_t *wfar;   // [cap] 1: at the last build every wall was farther than the stale threshold
+                     // (valid while Ctl::wfar_build == Ctl::rebuilds and 2 disp < half_skin)
 };
 
 struct Grid {                 // one per scene, computed on the device at every build
@@ -234,6 +237,9 @@ struct AuxStream {
     cudaStream_t stream = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr;
 };
+// Wall-gap flags of every particle after a build (static walls, no mesh): NbrList::wfar.
+void launch_wall_far(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const WallGeom *walls,
+                     double half_skin, cudaStream_t s);
 void launch_step(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
                  const PairConst *pw, const WallGeom *walls, int mode, cudaStream_t s, const AuxStream &aux = AuxStream());
 // the pair-parallel dense step in mixed precision (dem_mixed.cu)

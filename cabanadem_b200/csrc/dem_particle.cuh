@@ -102,6 +102,19 @@ __device__ __forceinline__ CtlSnap read_ctl(const Ctl *ctl, bool gated) {
     return s;
 }
 
+// Last-block election of a kernel: each block's thread 0 takes a ticket once the block's
+// writes are done (a block barrier before it); the block with ticket gridDim.x - 1 finalises.
+// The ticket is an acq_rel atomic at GPU scope: it orders the block's earlier memory
+// operations before the ticket (release; the barrier extends that to the block's other
+// threads), and the last block's later reads after it (acquire; its other threads follow
+// through a block barrier).  The finalising block's own writes reach the next kernel at the
+// kernel boundary, so neither side needs a separate fence.
+__device__ __forceinline__ unsigned take_ticket(unsigned *ticket) {
+    unsigned old;
+    asm volatile("atom.acq_rel.gpu.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(ticket) : "memory");
+    return old;
+}
+
 __device__ __forceinline__ void vmax_fold(unsigned long long *slots, double m) {
     if (m > 0.0) atomicMax(&slots[(blockIdx.x % kVmaxSlots) * 32], (unsigned long long)__double_as_longlong(m));
 }
@@ -152,13 +165,11 @@ __device__ __forceinline__ void finish_step(Ctl *ctl, unsigned long long *slots,
         double m = red[0];
         for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, red[w]);
         vmax_fold(slots, m);
-        __threadfence();
-        const unsigned t = atomicAdd(&ctl->ticket, 1u);
+        const unsigned t = take_ticket(&ctl->ticket);
         am_last = (t == gridDim.x - 1);
     }
     __syncthreads();
     if (am_last && threadIdx.x < 32) {
-        __threadfence();
         double v2 = vmax_collect_warp(slots);
         if (kin) {
             advance_kinematics(*kin);
@@ -173,7 +184,6 @@ __device__ __forceinline__ void finish_step(Ctl *ctl, unsigned long long *slots,
                 ctl->steps_done += 1;
                 ctl->total_steps += 1;
             }
-            __threadfence();
             ctl->ticket = 0u;
         }
     }
@@ -206,13 +216,11 @@ __device__ __forceinline__ void finish_step_counted(Ctl *ctl, unsigned long long
         }
         if (t) atomicAdd(&ctl->ndefer, t);
         vmax_fold(slots, m);
-        __threadfence();
-        const unsigned tk = atomicAdd(&ctl->ticket, 1u);
+        const unsigned tk = take_ticket(&ctl->ticket);
         am_last = (tk == gridDim.x - 1);
     }
     __syncthreads();
     if (am_last && threadIdx.x < 32) {
-        __threadfence();
         const double v2 = fmax(vmax_collect_warp(slots), mesh_speed2(fc));
         if (advance) advance_kinematics(fc);   // not on the last step of a run (no next drift)
         if (threadIdx.x == 0) {
@@ -224,7 +232,6 @@ __device__ __forceinline__ void finish_step_counted(Ctl *ctl, unsigned long long
             ctl->vcur ^= 1;
             ctl->steps_done += 1;
             ctl->total_steps += 1;
-            __threadfence();
             ctl->ticket = 0u;
         }
     }

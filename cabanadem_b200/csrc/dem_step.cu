@@ -59,6 +59,7 @@ __device__ __forceinline__ bool step_gate(const Ctl *ctl) {
 struct StreamCtl {
     int cur, vcur, nlone, nclear_end, n;
     bool last;
+    bool wfar;   // the wall-gap flags of the last build hold (see k_wall_far)
 };
 __device__ __forceinline__ StreamCtl stream_ctl(const Ctl *ctl, int n) {
     StreamCtl c;
@@ -68,6 +69,7 @@ __device__ __forceinline__ StreamCtl stream_ctl(const Ctl *ctl, int n) {
     // particles [nlone, nclear_end) had every listed neighbour at a gap above skin/2: while
     // twice the displacement bound stays below skin/2 none of them can touch
     c.nclear_end = (2.0 * ctl->disp < ctl->half_skin) ? c.nlone + ctl->nclear : c.nlone;
+    c.wfar = ctl->wfar_build == ctl->rebuilds && 2.0 * ctl->disp < ctl->half_skin;
     c.last = ctl->steps_done + 1 >= ctl->target;
     c.n = n;
     return c;
@@ -149,6 +151,36 @@ __device__ __forceinline__ bool wall_defer(const Particles &P, const ForceConsts
         defer = (pi.w - tmp) > 0.;
     }
     return defer;
+}
+
+// Wall-gap flags after a build: wfar[i] = 1 when every wall of particle i's scene is farther
+// than half_skin (the overlap r_i - (x_i - x_w).n_w of wall_defer below -half_skin).  While
+// twice the displacement bound stays below half_skin (walls static) such a particle cannot
+// reach a wall, so the staged streaming kernel skips its wall test -- the same rule as the
+// clear class of the re-sort for listed neighbours.  Non-finite positions give 0.
+__global__ void k_wall_far(Particles P, NbrList L, Ctl *ctl, ForceConsts fc, const WallGeom *__restrict__ walls,
+                           double half_skin) {
+    const double4 *__restrict__ pc = P.pos[ctl->cur];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += gridDim.x * blockDim.x) {
+        const D4 pi = ld4(pc, i);
+        const int scene_i = P.scene ? P.scene[i] : 0;
+        const int wall0 = fc.wps ? scene_i * fc.wps : 0;
+        const int wall1 = fc.wps ? wall0 + fc.wps : fc.nwall;
+        bool far = true;
+        for (int w = wall0; w < wall1; ++w) {
+            const WallGeom &g = walls[w];
+            const double tmp = (pi.x - g.x[0]) * g.n[0] + (pi.y - g.x[1]) * g.n[1] + (pi.z - g.x[2]) * g.n[2];
+            far = far && (pi.w - tmp) < -half_skin;
+        }
+        L.wfar[i] = far ? 1 : 0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->wfar_build = ctl->rebuilds;
+}
+
+void launch_wall_far(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const WallGeom *walls,
+                     double half_skin, cudaStream_t s) {
+    if (!L.wfar || fc.mwalls || fc.mesh.nt || !(half_skin > 0.0) || P.n <= 0) return;
+    k_wall_far<<<148 * 8, 256, 0, s>>>(P, L, ctl, fc, walls, half_skin);
 }
 
 // Streaming body for one particle i (any class); returns whether it is deferred.
@@ -280,11 +312,12 @@ struct BulkTile {
     static constexpr int CS = MASS + 8 * T;       // int [T]
     static constexpr int NN = CS + 4 * T;         // int [T]
     static constexpr int IDX = NN + 4 * T;        // int [2][T]
-    static constexpr int BYTES = IDX + 8 * T;
+    static constexpr int WFAR = IDX + 8 * T;      // uint8 [T]
+    static constexpr int BYTES = WFAR + T;
 };
 
 #ifndef STREAM_BULK_MINB
-#define STREAM_BULK_MINB 1
+#define STREAM_BULK_MINB 9
 #endif
 template <int T, int S>
 __global__ void __launch_bounds__(T, STREAM_BULK_MINB) k_stream_bulk(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
@@ -314,13 +347,14 @@ __global__ void __launch_bounds__(T, STREAM_BULK_MINB) k_stream_bulk(Particles P
         const int rows = lists ? (L.maxnb > 1 ? 2 : L.maxnb) : 0;
         unsigned char *sb = smem + (k % S) * B::BYTES;
         uint64_t *bar = &full[k % S];
-        bulk::bar_arrive_expect(bar, (uint32_t)m * (32u + 24u + 8u + 4u + (lists ? 4u : 0u) + 4u * rows));
+        bulk::bar_arrive_expect(bar, (uint32_t)m * (32u + 24u + 8u + 4u + (lists ? 4u : 0u) + 4u * rows + (c.wfar ? 1u : 0u)));
         bulk::copy_g2s(sb + B::POS, pc + i0, 32u * m, bar);
         for (int d = 0; d < 3; ++d) bulk::copy_g2s(sb + B::VEL + 8 * T * d, vc + (long)d * cap + i0, 8u * m, bar);
         bulk::copy_g2s(sb + B::MASS, P.mI + i0, 8u * m, bar);
         bulk::copy_g2s(sb + B::CS, P.cstate + i0, 4u * m, bar);
         if (lists) bulk::copy_g2s(sb + B::NN, L.nn + i0, 4u * m, bar);
         for (int r = 0; r < rows; ++r) bulk::copy_g2s(sb + B::IDX + 4 * T * r, L.idx + (long)r * cap + i0, 4u * m, bar);
+        if (c.wfar) bulk::copy_g2s(sb + B::WFAR, L.wfar + i0, (uint32_t)m, bar);
     };
     if (threadIdx.x == 0)
         for (int k = 0; k < S && k < mine; ++k) issue(k);
@@ -364,7 +398,8 @@ __global__ void __launch_bounds__(T, STREAM_BULK_MINB) k_stream_bulk(Particles P
                 const double sr = pi.w + pj.w;
                 defer = !(r2ij >= sr * sr * 1.0000000001);
             }
-            defer = wall_defer(P, fc, walls, i, pi, defer);
+            // the wall test, unless the last build found every wall beyond reach
+            if (!(c.wfar && sb[B::WFAR + t])) defer = wall_defer(P, fc, walls, i, pi, defer);
             if (!defer) stream_free_step(P, fc, c, vc, i, pi, m, ui0, ui1, ui2, vmax2);
         }
         defer_append(ctl, L, defer, i);
@@ -448,14 +483,13 @@ __global__ void __launch_bounds__(kApplyBlock) k_apply(Particles P, NbrList L, C
             wc[d * cap + i] = L.defer_w[d * cap + t];
         }
     }
+    __syncthreads();
     if (threadIdx.x == 0) {
-        __threadfence();
-        const unsigned tk = atomicAdd(&ctl->ticket, 1u);
+        const unsigned tk = take_ticket(&ctl->ticket);
         s_last = (tk == gridDim.x - 1);
     }
     __syncthreads();
     if (s_last && threadIdx.x < 32) {   // every block has taken its ticket: the slots are quiescent
-        __threadfence();
         const double v2 = fmax(vmax_collect_warp(P.vslots), mesh_speed2(fc));
         // walls and mesh drift with the particles' stage2 of the next step (none after a run's last step)
         if (ctl->steps_done + 1 < ctl->target) advance_kinematics(fc);
@@ -466,7 +500,6 @@ __global__ void __launch_bounds__(kApplyBlock) k_apply(Particles P, NbrList L, C
             ctl->cur ^= 1;
             ctl->steps_done += 1;
             ctl->total_steps += 1;
-            __threadfence();
             ctl->ticket = 0u;
         }
     }
