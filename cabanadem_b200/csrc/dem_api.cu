@@ -194,7 +194,11 @@ __global__ void k_gather_i(const int *src, int *dst, int n, int ncomp, int cap, 
         dst[t] = v;
     }
 }
-__global__ void k_scatter_pos(const double *src, double4 *pos, int n, const int *rank, int rad) {
+// Ping-pong buffers picked on the device from the control word (`sel` = &ctl->cur or
+// &ctl->vcur), so that a set or get queues behind the steps without a host round trip.
+__global__ void k_scatter_pos_sel(const double *src, double4 *pos0, double4 *pos1, const int *sel, int n,
+                                  const int *rank, int rad) {
+    double4 *pos = *sel ? pos1 : pos0;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
         double4 &p = pos[rank[c]];
         if (rad) p.w = src[c];
@@ -205,7 +209,9 @@ __global__ void k_scatter_pos(const double *src, double4 *pos, int n, const int 
         }
     }
 }
-__global__ void k_gather_pos(const double4 *pos, double *dst, int n, const int *rank, int rad) {
+__global__ void k_gather_pos_sel(const double4 *pos0, const double4 *pos1, const int *sel, double *dst, int n,
+                                 const int *rank, int rad) {
+    const double4 *pos = *sel ? pos1 : pos0;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
         const double4 p = pos[rank[c]];
         if (rad) dst[c] = p.w;
@@ -214,6 +220,22 @@ __global__ void k_gather_pos(const double4 *pos, double *dst, int n, const int *
             dst[3 * c + 1] = p.y;
             dst[3 * c + 2] = p.z;
         }
+    }
+}
+__global__ void k_scatter_d_sel(const double *src, double *d0, double *d1, const int *sel, int n, int ncomp, int cap,
+                                const int *rank) {
+    double *dst = *sel ? d1 : d0;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < (long)n * ncomp; t += (long)gridDim.x * blockDim.x) {
+        const int c = (int)(t / ncomp), k = (int)(t % ncomp);
+        dst[(long)k * cap + rank[c]] = src[t];
+    }
+}
+__global__ void k_gather_d_sel(const double *s0, const double *s1, const int *sel, double *dst, int n, int ncomp,
+                               int cap, const int *rank) {
+    const double *src = *sel ? s1 : s0;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < (long)n * ncomp; t += (long)gridDim.x * blockDim.x) {
+        const int c = (int)(t / ncomp), k = (int)(t % ncomp);
+        dst[t] = src[(long)k * cap + rank[c]];
     }
 }
 __global__ void k_scatter_mI(const double *src, double *mI, int n, int cap, const int *rank, int which) {
@@ -353,13 +375,6 @@ bool field_layout(const dem_particles *p, int field, long *count, int *esize) {
     }
 }
 
-int host_cur(dem_particles *p, int *vcur) {
-    int cv[2] = {0, 0};
-    cudaMemcpyAsync(cv, &p->ctl->cur, 2 * sizeof(int), cudaMemcpyDeviceToHost, p->ctx->stream);
-    cudaStreamSynchronize(p->ctx->stream);
-    *vcur = cv[1];
-    return cv[0];
-}
 
 }  // namespace
 
@@ -535,12 +550,11 @@ extern "C" int dem_particles_set(dem_particles *p, int field, const void *host, 
     }
     void *tmp = p->stage;
     CK(cudaMemcpyAsync(tmp, host, (size_t)need * es, cudaMemcpyHostToDevice, s));
-    int vcur = 0;
-    const int cur = host_cur(p, &vcur);
+    const int *cur = &p->ctl->cur, *vcur = &p->ctl->vcur;
     switch (field) {
-        case DEM_F_X: k_scatter_pos<<<kGS, kTB, 0, s>>>((double *)tmp, P.pos[cur], n, P.rank, 0); break;
+        case DEM_F_X: k_scatter_pos_sel<<<kGS, kTB, 0, s>>>((double *)tmp, P.pos[0], P.pos[1], cur, n, P.rank, 0); break;
         case DEM_F_RAD: {
-            k_scatter_pos<<<kGS, kTB, 0, s>>>((double *)tmp, P.pos[cur], n, P.rank, 1);
+            k_scatter_pos_sel<<<kGS, kTB, 0, s>>>((double *)tmp, P.pos[0], P.pos[1], cur, n, P.rank, 1);
             const double *r = (const double *)host;
             std::vector<double> part(host_threads(n), 0.0);
             host_parallel(n, [&](long b, long e, int t) {
@@ -551,8 +565,12 @@ extern "C" int dem_particles_set(dem_particles *p, int field, const void *host, 
             p->rmax = *std::max_element(part.begin(), part.end());
             break;
         }
-        case DEM_F_U: k_scatter_d<<<kGS, kTB, 0, s>>>((double *)tmp, P.vel[vcur], n, 3, P.cap, P.rank); break;
-        case DEM_F_OMEGA: k_scatter_d<<<kGS, kTB, 0, s>>>((double *)tmp, P.omg[vcur], n, 3, P.cap, P.rank); break;
+        case DEM_F_U:
+            k_scatter_d_sel<<<kGS, kTB, 0, s>>>((double *)tmp, P.vel[0], P.vel[1], vcur, n, 3, P.cap, P.rank);
+            break;
+        case DEM_F_OMEGA:
+            k_scatter_d_sel<<<kGS, kTB, 0, s>>>((double *)tmp, P.omg[0], P.omg[1], vcur, n, 3, P.cap, P.rank);
+            break;
         case DEM_F_FORCE: k_scatter_d<<<kGS, kTB, 0, s>>>((double *)tmp, P.force, n, 3, P.cap, P.rank); break;
         case DEM_F_TORQUE: k_scatter_d<<<kGS, kTB, 0, s>>>((double *)tmp, P.torque, n, 3, P.cap, P.rank); break;
         case DEM_F_EXT_FORCE:
@@ -655,13 +673,16 @@ static int particles_get_impl(dem_particles *p, int field, void *host, long coun
         return DEM_OK;
     }
     void *tmp = p->stage;
-    int vcur = 0;
-    const int cur = host_cur(p, &vcur);
+    const int *cur = &p->ctl->cur, *vcur = &p->ctl->vcur;
     switch (field) {
-        case DEM_F_X: k_gather_pos<<<kGS, kTB, 0, s>>>(P.pos[cur], (double *)tmp, n, P.rank, 0); break;
-        case DEM_F_RAD: k_gather_pos<<<kGS, kTB, 0, s>>>(P.pos[cur], (double *)tmp, n, P.rank, 1); break;
-        case DEM_F_U: k_gather_d<<<kGS, kTB, 0, s>>>(P.vel[vcur], (double *)tmp, n, 3, P.cap, P.rank); break;
-        case DEM_F_OMEGA: k_gather_d<<<kGS, kTB, 0, s>>>(P.omg[vcur], (double *)tmp, n, 3, P.cap, P.rank); break;
+        case DEM_F_X: k_gather_pos_sel<<<kGS, kTB, 0, s>>>(P.pos[0], P.pos[1], cur, (double *)tmp, n, P.rank, 0); break;
+        case DEM_F_RAD: k_gather_pos_sel<<<kGS, kTB, 0, s>>>(P.pos[0], P.pos[1], cur, (double *)tmp, n, P.rank, 1); break;
+        case DEM_F_U:
+            k_gather_d_sel<<<kGS, kTB, 0, s>>>(P.vel[0], P.vel[1], vcur, (double *)tmp, n, 3, P.cap, P.rank);
+            break;
+        case DEM_F_OMEGA:
+            k_gather_d_sel<<<kGS, kTB, 0, s>>>(P.omg[0], P.omg[1], vcur, (double *)tmp, n, 3, P.cap, P.rank);
+            break;
         case DEM_F_FORCE: k_gather_d<<<kGS, kTB, 0, s>>>(P.force, (double *)tmp, n, 3, P.cap, P.rank); break;
         case DEM_F_TORQUE: k_gather_d<<<kGS, kTB, 0, s>>>(P.torque, (double *)tmp, n, 3, P.cap, P.rank); break;
         case DEM_F_EXT_FORCE: k_gather_d<<<kGS, kTB, 0, s>>>(P.ext, (double *)tmp, n, 3, P.cap, P.rank); break;

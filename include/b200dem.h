@@ -17,6 +17,10 @@
  *    Morton curve; that order never shows through this interface.
  *  - One dem_ctx owns one CUDA stream; calls on it are stream-ordered, *_get and
  *    dem_ctx_sync synchronise.  A context is used by one host thread at a time.
+ *  - dem_particles_set reads a pageable host array before it returns.  From page-locked
+ *    (pinned) host memory the copy is queued on the context's stream instead, so that
+ *    several uploads overlap: keep such an array unchanged until a call that synchronises
+ *    (any *_get, dem_solver_run, dem_ctx_sync).
  */
 #ifndef B200DEM_H
 #define B200DEM_H
@@ -159,7 +163,8 @@ void *dem_ctx_stream(dem_ctx *ctx);
 int dem_particles_create(dem_ctx *ctx, int n, int max_contacts, int max_walls, dem_particles **out);
 int dem_particles_destroy(dem_particles *p);
 /* slice*() + updateParticles (src/CabanaDEM_Particles.hpp:91-271): SoA upload/download.
- * count = number of elements in `host` (e.g. 3*n for DEM_F_X). */
+ * count = number of elements in `host` (e.g. 3*n for DEM_F_X).  A set from pinned host
+ * memory is asynchronous (see Conventions). */
 int dem_particles_set(dem_particles *p, int field, const void *host, long count);
 int dem_particles_get(dem_particles *p, int field, void *host, long count);
 /* As dem_particles_get into device memory `dev` (same layout and caller order), queued on
