@@ -13,8 +13,8 @@ Verlet skin 0.1 r_mean with rebuild when the displacement bound reaches skin/2
 The other workloads (one JSON line each, device-timed particle-steps/s):
   random_box  4,096 r = 1 mm spheres in a 5 cm walled cube, dt 1e-7 (latency-bound size)
   batched     1,024 independent scenes of log-uniform [2, 8192] spheres fired at their own
-              walls, one launch per step for all scenes, FP32 forces / FP64 state, launch
-              settings from the autotuner
+              walls, FP32 forces / FP64 state, grouped by scene size, each group a solver with
+              launch settings from the autotuner, the groups concurrent
   bonded      256 x 64 x 8 bonded bar pulled at both ends, FP64
   dam_break   200,000 quasi-2D disks: full DEM rollout vs the learned surrogate with DEM
               fallback over the same simulated time (wall-clock of each, runout front and
@@ -35,7 +35,10 @@ rebuild-every-step mode) on a bounded sample of the same workload.  Three device
 sub-measurements follow the timed region on the same GPU and are reported beside it:
 `mixed` (the same lattice with FP32 contact forces), `dense` (the 200,000-disk dam break
 at t = 0.3 s, a contact-dense flow, FP64 and mixed) and `rebuild` (one full neighbour
-rebuild of the 2,000,000-sphere state).
+rebuild of the 2,000,000-sphere state); then the other configurations, each measured as its
+own workload above measures it: `c1` (random_box), `c3` (batched, with the packaged B200
+launch settings), `c4` (bonded) and `c5` (dam_break over --seconds; --seconds 0 skips it).
+--no-configs skips those four.
 """
 from __future__ import annotations
 
@@ -85,6 +88,8 @@ def parse():
     ap.add_argument("--dense-advance", type=int, default=300_000,
                     help="steps of the dam break run before the dense measurement (0: no dense measurement)")
     ap.add_argument("--no-sub", action="store_true", help="skip the mixed, dense and rebuild sub-measurements")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the C1, C3, C4 and C5 sub-measurements of the headline line")
     return ap.parse_args()
 
 
@@ -495,6 +500,57 @@ def measure_dense(ctx, args, stream, peak, n_steps):
     return out
 
 
+def measure_configs(local, ctx, stream, args):
+    """The other configurations of the suite, each device-timed on this GPU after the headline
+    (so that the driver's line records them): C1 (4,096 spheres in a walled box), C3 (the
+    1,024-scene batch, mixed, size buckets with the packaged B200 settings, wall-clock over the
+    concurrent buckets), C4 (the bonded bar, FP64) and C5 (learned surrogate against plain DEM on
+    the 200k-disk dam break, --seconds simulated)."""
+    import torch
+    from cabanadem_b200 import api, scenarios as S, surrogate as SG
+    from cabanadem_b200._lib import DEM_MIXED
+    steps = max(args.steps, args.sub_steps)
+    out = {}
+    sc = S.random_box(seed=1)
+    s = api.from_scenario(sc, ctx=ctx)
+    s.run_steps(max(3, args.warmup))
+    ms = _device_ms(stream, lambda: s.run_steps(steps))
+    out["c1"] = {"workload": "random_box_4096: 4096 r=1 mm spheres, 5 cm cube, 6 walls, gravity, dt 1e-7 s, FP64",
+                 "value": sc.state.n * steps / (ms / 1e3), "ms_per_step": round(ms / steps, 5), "steps": steps}
+    s.close()
+    s.particles.close()
+    sc = S.batched_scenes(seed=3)
+    runner = api.BatchRunner(sc, precision=DEM_MIXED, device=local)
+    runner.run_steps(max(3, args.warmup))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    runner.run_steps(steps)
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t0) * 1e3
+    out["c3"] = {"workload": "batched_1024_scenes: %d spheres in 1024 scenes (log-uniform [2,8192]), mixed; size "
+                             "buckets with the packaged B200 settings, concurrent; wall-clock" % sc.state.n,
+                 "value": sc.state.n * steps / (ms / 1e3), "ms_per_step": round(ms / steps, 5), "steps": steps}
+    runner.close()
+    case = S.bonded_bar()
+    b = api.bonded_from_case(case, ctx=ctx)
+    b.run_steps(max(3, args.warmup))
+    ms = _device_ms(stream, lambda: b.run_steps(steps))
+    out["c4"] = {"workload": "bonded_bar_256x64x8: %d spheres, 6-neighbour bonds, ends pulled, FP64" % case["state"].n,
+                 "value": case["state"].n * steps / (ms / 1e3), "ms_per_step": round(ms / steps, 5), "steps": steps}
+    b.close()
+    if args.seconds > 0:
+        mk = lambda: S.dam_break(n=200_000, aspect=2.0, seed=101)
+        sg = SG.load(ctx, os.path.join(ROOT, "cabanadem_b200", "data", "dam_break_surrogate.npz"), mk())
+        res = SG.evaluate(sg, mk, args.seconds, ctx)
+        out["c5"] = {"workload": "dam_break_200000, %.2f s simulated: learned surrogate (200-step strides) against "
+                                 "plain FP64 DEM" % args.seconds,
+                     "value": res["surrogate_particle_steps_per_s"], "dem_value": res["dem_particle_steps_per_s"],
+                     "speedup": round(res["speedup"], 3), "front_error": round(res["front_error"], 4),
+                     "surrogate_wall_s": round(res["surrogate_wall_s"], 3), "dem_wall_s": round(res["dem_wall_s"], 3)}
+        sg.close()
+    return out
+
+
 def measure_rebuild(solver, stream, state, off, peak, n):
     """One full rebuild of the solver's state (Morton re-sort with history remap, new list),
     device-timed; algorithmic bytes per particle 24 + 2*168 + 4 n_nbr + 56 n_c."""
@@ -581,6 +637,8 @@ def main():
             sub["mixed"] = measure_mixed(ctx, args, stream, peak, sub_steps, fp64_ms)
         if args.dense_advance > 0:
             sub["dense"] = measure_dense(ctx, args, stream, peak, sub_steps)
+        if not args.no_configs:
+            sub.update(measure_configs(local, ctx, stream, args))
 
     # end to end through the C ABI with host buffers (pinned): a new run sets positions,
     # velocities, spins, radii, masses, inertias and material constants, clears the contact

@@ -480,8 +480,9 @@ def from_scenario(sc, ctx: Context | None = None, rebuild_every_step=False, prec
 class BatchRunner:
     """Independent scenes of a batched set (scenarios.batched_scenes) grouped by scene size
     (scenarios.split_scenes): each size bucket is one solver, with the launch settings tuned for
-    that bucket (autotune.tune on the bucket's scenes, or `configs[bucket]`), on a context of its
-    own, so on a CUDA stream of its own.  run_steps advances every bucket at once: one host
+    that bucket (`configs[bucket]`; else autotune.tune on the bucket's scenes when `tune`; else
+    the B200 settings shipped with the package for that bucket, autotune.packaged, or the
+    defaults), on a context of its own, so on a CUDA stream of its own.  run_steps advances every bucket at once: one host
     thread per bucket, each a graph-looped run of its solver, the buckets' kernels running
     concurrently on the GPU.  Scenes never interact, so every scene evolves as it does alone."""
 
@@ -493,6 +494,8 @@ class BatchRunner:
             cfg = (configs or {}).get(b)
             if cfg is None and tune:
                 cfg = autotune.tune(sub, precision=precision, warmup=5, steps=tune_steps)
+            elif cfg is None:
+                cfg = autotune.packaged(sub, precision)   # B200 settings shipped with the package
             cfg = dict(autotune.DEFAULTS, **(cfg or {}))
             kw = autotune.apply(sub, cfg)
             ctx = Context(device)

@@ -112,6 +112,19 @@ def tune(sc, precision=0, warmup=20, steps=200, use_cache=True, ctx=None):
     return dict(best)
 
 
+def packaged(sc, precision):
+    """The B200 settings shipped with the package for this workload's bucket
+    (``data/autotune_b200.json``, found by ``tune`` on a B200), or None."""
+    path = os.path.join(os.path.dirname(__file__), "data", "autotune_b200.json")
+    try:
+        with open(path) as f:
+            table = json.load(f)
+    except (OSError, ValueError):
+        return None
+    cfg = table.get(bucket(sc, precision))
+    return dict(cfg) if isinstance(cfg, dict) else None
+
+
 def _solver_kwargs(cfg):
     full = dict(DEFAULTS)
     full.update(cfg)

@@ -312,12 +312,13 @@ __global__ void k_run_begin(Ctl *ctl, int target, double half_skin, int fresh_li
         ctl->npairs = 0;
     }
 }
-// Step loop of a graph replay: two conditional while nodes, the first running kLoopUnroll
-// steps per iteration while at least that many steps remain, the second one step per
-// iteration for the rest, so that no step of a replay past the target is launched (a gated
-// streaming kernel still costs its block launches).  A loop continues while steps remain, the
-// list is still valid, no list overflowed and the density regime the kernels were chosen for
-// still holds.  Each loop's condition is set before it by a node of the replay (k_loop_begin,
+// Step loop of a graph replay: conditional while nodes of 8, 4, 2 and 1 steps per iteration,
+// each running while at least that many steps remain, so that no step of a replay past the
+// target is launched (a gated streaming kernel still costs its block launches) and a run's
+// tail takes at most one iteration of each short loop (an iteration's conditional turn-around
+// costs about 5 us).  A loop continues while steps remain, the list is still valid, no list
+// overflowed, no bounded wait gave up and the density regime the kernels were chosen for still
+// holds.  Each loop's condition is set before it by a node of the replay (k_loop_begin,
 // k_loop_mid) and after every iteration by one thread of its body (k_loop_ctl); an iteration
 // counter bounds every loop by target + 1 iterations, so a replay ends even if some step made
 // no progress.
@@ -340,11 +341,11 @@ __global__ void k_loop_begin(Ctl *ctl, cudaGraphConditionalHandle h, int n, int 
                     !(ctl->status & kStopBits);
     cudaGraphSetConditional(h, go ? 1u : 0u);
 }
-__global__ void k_loop_mid(Ctl *ctl, cudaGraphConditionalHandle h, int n, int dense) {
+__global__ void k_loop_mid(Ctl *ctl, cudaGraphConditionalHandle h, int n, int dense, int min_left) {
     if (threadIdx.x != 0) return;
-    // no iteration of the first loop (fewer steps left than it takes): the replay's first step
-    // is taken here, whatever the density (as in k_loop_begin)
-    cudaGraphSetConditional(h, loop_go(ctl, n, ctl->loop_iter == 0 ? -1 : dense, 1) ? 1u : 0u);
+    // no iteration of an earlier loop (fewer steps left than they take): the replay's first
+    // step is taken here, whatever the density (as in k_loop_begin)
+    cudaGraphSetConditional(h, loop_go(ctl, n, ctl->loop_iter == 0 ? -1 : dense, min_left) ? 1u : 0u);
 }
 __global__ void k_loop_ctl(Ctl *ctl, cudaGraphConditionalHandle h, int n, int dense, int min_left) {
     if (threadIdx.x != 0) return;
@@ -1181,9 +1182,11 @@ int capture_graph(dem_solver *s, int steps) {
     return DEM_OK;
 }
 
-// Steps per iteration of the first graph while-loop: each iteration pays for the conditional
-// and the control kernel (about 5 us on a B200).
+// Steps per iteration of the graph while-loops, longest first: each iteration pays for the
+// conditional and the control kernel (about 5 us on a B200).
 constexpr int kLoopUnroll = 8;
+constexpr int kLoopUnits[] = {kLoopUnroll, 4, 2, 1};
+constexpr int kLoopLevels = sizeof(kLoopUnits) / sizeof(kLoopUnits[0]);
 
 // `steps` fused steps (each with the neighbour build first in the rebuild-every-step mode).
 static void capture_steps(dem_solver *s, int steps, cudaStream_t st) {
@@ -1243,8 +1246,8 @@ static cudaError_t add_kernel(cudaGraph_t g, cudaGraphNode_t dep, cudaStream_t s
 }
 
 // The step loop as one graph: k_loop_begin (loop counter reset, condition of the first loop),
-// a while node of kLoopUnroll steps per iteration, k_loop_mid (condition of the second loop),
-// a while node of one step per iteration.
+// a while node of kLoopUnroll steps per iteration, then for 4, 2 and 1 steps a k_loop_mid
+// (condition of the next loop) and a while node of that many steps per iteration.
 int capture_loop_graph(dem_solver *s) {
     dem_ctx *ctx = s->ctx;
     cudaStream_t st = ctx->stream;
@@ -1258,18 +1261,23 @@ int capture_loop_graph(dem_solver *s) {
     }
     cudaGraph_t g = nullptr;
     CK(cudaGraphCreate(&g, 0));
-    cudaGraphConditionalHandle h8, h1;
-    cudaError_t e = cudaGraphConditionalHandleCreate(&h8, g, 0, cudaGraphCondAssignDefault);
-    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h1, g, 0, cudaGraphCondAssignDefault);
+    cudaGraphConditionalHandle h[kLoopLevels];
+    cudaError_t e = cudaSuccess;
+    for (int l = 0; l < kLoopLevels && e == cudaSuccess; ++l)
+        e = cudaGraphConditionalHandleCreate(&h[l], g, 0, cudaGraphCondAssignDefault);
     const int n = s->p->P.n, dense = density_matters(s) ? s->fc.dense : -1;
     Ctl *ctl = s->p->ctl;
-    cudaGraphNode_t begin = nullptr, loop8 = nullptr, mid = nullptr, loop1 = nullptr;
+    cudaGraphNode_t cond = nullptr, loop = nullptr;
     if (e == cudaSuccess)
-        e = add_kernel(g, nullptr, st, [&] { k_loop_begin<<<1, 32, 0, st>>>(ctl, h8, n, dense, kLoopUnroll); }, &begin);
-    if (e == cudaSuccess) e = add_loop(s, g, begin, h8, kLoopUnroll, dense, &loop8);
-    if (e == cudaSuccess)
-        e = add_kernel(g, loop8, st, [&] { k_loop_mid<<<1, 32, 0, st>>>(ctl, h1, n, dense); }, &mid);
-    if (e == cudaSuccess) e = add_loop(s, g, mid, h1, 1, dense, &loop1);
+        e = add_kernel(g, nullptr, st, [&] { k_loop_begin<<<1, 32, 0, st>>>(ctl, h[0], n, dense, kLoopUnits[0]); },
+                       &cond);
+    if (e == cudaSuccess) e = add_loop(s, g, cond, h[0], kLoopUnits[0], dense, &loop);
+    for (int l = 1; l < kLoopLevels && e == cudaSuccess; ++l) {
+        const cudaGraphConditionalHandle hl = h[l];
+        const int unit = kLoopUnits[l];
+        e = add_kernel(g, loop, st, [&] { k_loop_mid<<<1, 32, 0, st>>>(ctl, hl, n, dense, unit); }, &cond);
+        if (e == cudaSuccess) e = add_loop(s, g, cond, hl, unit, dense, &loop);
+    }
     if (e == cudaSuccess) e = cudaGraphInstantiate(&s->graph, g, 0);
     cudaGraphDestroy(g);
     CK(e);
@@ -1479,7 +1487,8 @@ extern "C" int dem_solver_run(dem_solver *s, int nsteps) {
     // (loop graph: every step's kernels, a control kernel per iteration, the two condition nodes)
     int steps_before = 0;
     auto count_launches = [&](const Ctl &c) {
-        s->launches += s->loop ? 2 + (long)(c.steps_done - steps_before) * s->graph_nodes + c.loop_iter : s->graph_nodes;
+        s->launches += s->loop ? kLoopLevels + (long)(c.steps_done - steps_before) * s->graph_nodes + c.loop_iter
+                               : s->graph_nodes;
         steps_before = c.steps_done;
     };
     if (ref_mode(s)) {

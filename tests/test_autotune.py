@@ -71,3 +71,19 @@ def test_scene_size_buckets_split_and_key_the_tuning():
         keys[b] = autotune.bucket(sub, 1)
     assert len(set(keys.values())) == len(parts)
     assert all(k.endswith("|scenes%d" % b) for b, k in keys.items())
+
+
+def test_packaged_b200_settings_cover_the_batch_buckets():
+    """The launch settings shipped for B200 (used by BatchRunner when neither configurations nor
+    tuning are given) cover every size bucket of the 1,024-scene batch, and every value is one
+    the tuner could have kept (a default or a candidate)."""
+    from cabanadem_b200._lib import DEM_MIXED
+    sc = S.batched_scenes(seed=3)
+    parts = S.split_scenes(sc)
+    assert len(parts) == 3
+    for b, sub, ids in parts:
+        cfg = autotune.packaged(sub, DEM_MIXED)
+        assert cfg is not None, autotune.bucket(sub, DEM_MIXED)
+        assert set(cfg) == set(autotune.DEFAULTS)
+        assert all(cfg[k] in autotune.CANDIDATES[k] or cfg[k] == autotune.DEFAULTS[k] for k in cfg)
+    assert autotune.packaged(S.random_box(n=300), 0) is None
