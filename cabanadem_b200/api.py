@@ -155,6 +155,9 @@ class Particles:
 
     # ---- field access
     def set(self, field: str, arr):
+        """Upload a field in caller order.  From page-locked (pinned) memory the copy is queued
+        on the context's stream: keep `arr` unchanged until a call that synchronises (get, a
+        run, Context.sync); other arrays are read before set returns."""
         dt = _F_DTYPE.get(field, np.float64)
         a = np.ascontiguousarray(arr, dtype=dt)
         exp = _shape(field, self.n, self.max_cnts, self.max_walls)

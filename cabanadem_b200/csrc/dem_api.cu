@@ -1007,6 +1007,8 @@ int alloc_lists(dem_solver *s, int maxnb) {
     cudaFree(s->L.defer_v);
     cudaFree(s->L.defer_w);
     cudaFree(s->L.wfar);
+    cudaFree(s->L.nn_old);
+    cudaFree(s->L.idx_old);
     const bool pairs = s->L.pitem != nullptr;
     free_pairs(s);
     s->L.maxnb = maxnb;
@@ -1016,6 +1018,8 @@ int alloc_lists(dem_solver *s, int maxnb) {
     CK(dalloc(&s->L.defer_v, 3 * (size_t)s->p->P.cap));
     CK(dalloc(&s->L.defer_w, 3 * (size_t)s->p->P.cap));
     CK(dalloc(&s->L.wfar, (size_t)s->p->P.cap));
+    CK(dalloc(&s->L.nn_old, (size_t)s->p->P.cap));
+    CK(dalloc(&s->L.idx_old, (size_t)maxnb * s->p->P.cap));
     CK(cudaMemsetAsync(s->L.nn, 0, sizeof(int) * s->p->P.cap, ctx->stream));
     CK(cudaMemsetAsync(s->L.wfar, 0, s->p->P.cap, ctx->stream));
     if (pairs) {
@@ -1373,7 +1377,7 @@ extern "C" int dem_solver_destroy(dem_solver *s) {
     if (s->aux.join) cudaEventDestroy(s->aux.join);
     cudaFree(s->d_pp); cudaFree(s->d_pw); cudaFree(s->d_walls); cudaFree(s->d_scenes);
     cudaFree(s->L.nn); cudaFree(s->L.idx); cudaFree(s->L.defer); cudaFree(s->L.defer_v); cudaFree(s->L.defer_w);
-    cudaFree(s->L.wfar);
+    cudaFree(s->L.wfar); cudaFree(s->L.nn_old); cudaFree(s->L.idx_old);
     free_pairs(s);
     BuildBuffers &B = s->B;
     cudaFree(B.grid); cudaFree(B.total); cudaFree(B.key); cudaFree(B.cell_start); cudaFree(B.cell_fill); cudaFree(B.cell_items);

@@ -155,6 +155,8 @@ struct NbrList {
     int *nn;     // [cap] list length
     int *idx;    // [maxnb][cap] sorted indices, ascending caller id
     int maxnb;
+    int *nn_old, *idx_old;   // the lists of a re-sorting build in the old storage order ([cap],
+                             // [maxnb][cap]), re-indexed into nn / idx after the permutation
     int *defer;  // [cap] particles deferred to the contact kernel in the current step
     double *defer_v, *defer_w;  // [3][cap] new u, omega of deferred particle t (slot t)
     // pair-parallel dense step (dem_pairs.cuh), allocated when that form is first used:

@@ -549,6 +549,107 @@ __global__ void __launch_bounds__(kPartBlock) k_part_flag(Particles P, const Ctl
     if (threadIdx.x < 2) sums[threadIdx.x * (nb + 1) + blockIdx.x] = cnt[threadIdx.x];
 }
 
+// Re-sort partition, pass 1 with the lists: the class of cell slot s as k_part_flag gives it,
+// from the full list search of k_list done here, in the old storage order -- the list of the
+// particle q = items[s] goes to nn_old[q], idx_old[k][q] (old indices, ascending caller index),
+// and k_list_remap re-indexes it into the new order after the permutation, instead of a second
+// 27-cell search over the permuted storage.  Same candidates, same order, same overflow rule as
+// k_list (kMaxCand kept, DEM_ERR_NEIGHBOR_OVERFLOW when a list exceeds the capacity).
+__global__ void __launch_bounds__(kPartBlock) k_part_list(Particles P, NbrList L, Ctl *ctl, const Grid *g,
+                                                          const int *start, const int *items, double delta,
+                                                          double skin, int *cls, int *sums, int nb) {
+    const int cur = ctl->cur, n = P.n, cap = P.cap;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool invalid = (ctl->status & DEM_ERR_NAN) != 0;
+    int c_s = 2, count = 0;
+    if (s < n && invalid) L.nn_old[items[s]] = 0;
+    if (s < n && !invalid) {
+        const int q = items[s];
+        const Grid G = g[scene_of(P, q)];
+        const double4 *pc = P.pos[cur];
+        const D4 pi = ld4(pc, q);
+        const bool skin_mode = !(delta > 0.0) && skin > 0.0;
+        int c[3];
+        cell_of(G, pi, c);
+        int cand[kMaxCand];
+        int ckey[kMaxCand];
+        bool near = false;
+        for (int dz = -1; dz <= 1; ++dz) {
+            const int z = c[2] + dz;
+            if (z < 0 || z >= G.dims[2]) continue;
+            for (int dy = -1; dy <= 1; ++dy) {
+                const int y = c[1] + dy;
+                if (y < 0 || y >= G.dims[1]) continue;
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const int x = c[0] + dx;
+                    if (x < 0 || x >= G.dims[0]) continue;
+                    const int key = cell_key(G, x, y, z);
+                    const int e = start[key + 1];
+                    for (int t = start[key]; t < e; ++t) {
+                        const int j = items[t];
+                        if (j == q) continue;
+                        const D4 pj = ld4(pc, j);
+                        const double px = pi.x - pj.x, py = pi.y - pj.y, pz = pi.z - pj.z;
+                        const double r2 = px * px + py * py + pz * pz;
+                        const double cut = delta > 0.0 ? delta : pi.w + pj.w + skin;
+                        if (r2 <= cut * cut) {
+                            if (!skin_mode || !(sqrt(r2) - (pi.w + pj.w) > 0.5 * skin)) near = true;
+                            if (count < kMaxCand) {
+                                // insertion by caller index
+                                const int kj = P.perm[j];
+                                int u = count - 1;
+                                while (u >= 0 && ckey[u] > kj) {
+                                    ckey[u + 1] = ckey[u];
+                                    cand[u + 1] = cand[u];
+                                    --u;
+                                }
+                                ckey[u + 1] = kj;
+                                cand[u + 1] = j;
+                            }
+                            ++count;
+                        }
+                    }
+                }
+            }
+        }
+        const int lim = L.maxnb < kMaxCand ? L.maxnb : kMaxCand;
+        const int keep = count < lim ? count : lim;
+        for (int k = 0; k < keep; ++k) L.idx_old[(long)k * cap + q] = cand[k];
+        L.nn_old[q] = keep;
+        c_s = count == 0 ? 0 : (near ? 2 : 1);
+    }
+    if (s < n) cls[s] = c_s;
+    __shared__ int cnt[2];
+    __shared__ int smax;
+    if (threadIdx.x < 2) cnt[threadIdx.x] = 0;
+    if (threadIdx.x == 0) smax = 0;
+    __syncthreads();
+    const int w0 = __popc(__ballot_sync(0xffffffffu, s < n && c_s == 0));
+    const int w1 = __popc(__ballot_sync(0xffffffffu, s < n && c_s == 1));
+    if ((threadIdx.x & 31) == 0) {
+        if (w0) atomicAdd(&cnt[0], w0);
+        if (w1) atomicAdd(&cnt[1], w1);
+    }
+    atomicMax(&smax, count);
+    __syncthreads();
+    if (threadIdx.x < 2) sums[threadIdx.x * (nb + 1) + blockIdx.x] = cnt[threadIdx.x];
+    if (threadIdx.x == 0) {
+        atomicMax(&ctl->max_nbr, smax);
+        if (smax > L.maxnb || smax > kMaxCand) atomicOr(&ctl->status, DEM_ERR_NEIGHBOR_OVERFLOW);
+    }
+}
+
+// The lists of k_part_list into the new order: new position p holds old particle
+// newitems[p]; partners are renamed by dst (old index -> new position).
+__global__ void k_list_remap(int n, int cap, NbrList L, const int *newitems, const int *dst) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const int q = newitems[p];
+        const int c = L.nn_old[q];
+        for (int k = 0; k < c; ++k) L.idx[(long)k * cap + p] = dst[L.idx_old[(long)k * cap + q]];
+        L.nn[p] = c;
+    }
+}
+
 // Pass 2, one block: exclusive scans of both per-block counts (block order); totals into
 // nlone and nclear.
 __global__ void __launch_bounds__(1024) k_part_scan(int *sums, int nb, Ctl *ctl) {
@@ -654,8 +755,12 @@ void launch_build(const Particles &P, Particles &alt, const NbrList &L, BuildBuf
         // particles whose listed neighbours all keep a gap above skin/2, and the rest, so that
         // the streaming kernel's leading warps load no list and the next ones no partner
         const int nb = (n + kPartBlock - 1) / kPartBlock;
-        k_part_flag<<<nb, kPartBlock, 0, s>>>(P, ctl, B.grid, B.cell_fill, B.cell_items, delta, skin, B.src,
-                                              B.part_sums, nb);
+        if (L.idx_old)   // the lists too, in the old order (re-indexed below)
+            k_part_list<<<nb, kPartBlock, 0, s>>>(P, L, ctl, B.grid, B.cell_fill, B.cell_items, delta, skin, B.src,
+                                                  B.part_sums, nb);
+        else
+            k_part_flag<<<nb, kPartBlock, 0, s>>>(P, ctl, B.grid, B.cell_fill, B.cell_items, delta, skin, B.src,
+                                                  B.part_sums, nb);
         k_part_scan<<<1, 1024, 0, s>>>(B.part_sums, nb, ctl);
         k_part_place<<<nb, kPartBlock, 0, s>>>(n, B.src, B.part_sums, nb, ctl, B.cell_items, B.key);
         k_make_dst<<<gs, kB, 0, s>>>(n, B.key, B.dst);
@@ -673,7 +778,10 @@ void launch_build(const Particles &P, Particles &alt, const NbrList &L, BuildBuf
         if (P.scene) cudaMemcpyAsync(P.scene, alt.scene, cap * sizeof(int), cudaMemcpyDeviceToDevice, s);
         k_flip<<<1, 32, 0, s>>>(ctl);
     }
-    k_list<<<(n + 127) / 128, 128, 0, s>>>(P, L, ctl, B.grid, B.cell_fill, B.cell_items, delta, skin);
+    if (resort && L.idx_old)
+        k_list_remap<<<gs, kB, 0, s>>>(n, P.cap, L, B.key, B.dst);
+    else
+        k_list<<<(n + 127) / 128, 128, 0, s>>>(P, L, ctl, B.grid, B.cell_fill, B.cell_items, delta, skin);
     k_build_end<<<1, 32, 0, s>>>(ctl);
 }
 
