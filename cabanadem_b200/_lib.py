@@ -141,6 +141,7 @@ _PROTOS = {
                              _VP, _VP, _VP], C.c_int),
     "dem_nn_status": ([_VP, C.POINTER(C.c_int)], C.c_int),
     "dem_nn_debug_waits": ([_VP, C.c_int, C.c_int], C.c_int),
+    "dem_solver_debug_stream_waits": ([_VP, C.c_int, C.c_int], C.c_int),
     "dem_particles_get_device": ([_VP, C.c_int, _VP, C.c_long], C.c_int),
     "dem_particles_clear_contacts": ([_VP], C.c_int),
     "dem_checkpoint_save": ([_VP, C.c_char_p], C.c_int),

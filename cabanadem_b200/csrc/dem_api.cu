@@ -304,6 +304,7 @@ __global__ void k_init_particles(Particles P) {
 __global__ void k_run_begin(Ctl *ctl, int target, double half_skin, int fresh_list = 0) {
     if (threadIdx.x == 0) {
         if (fresh_list) ctl->disp = 0.0;
+        ctl->ndefer = 0;   // a run starts at a step boundary (a step stopped by an error left its list)
         ctl->steps_done = 0;
         ctl->target = target;
         ctl->half_skin = half_skin;
@@ -2118,6 +2119,18 @@ extern "C" int dem_nn_mlp_backward(dem_ctx *ctx, const dem_nn_mlp *m, long rows,
                          ctx->d_err, ctx->stream);
     if (st == DEM_ERR_UNSUPPORTED) return fail(ctx, st, "dem_nn_mlp_backward: unsupported (kin, nout)");
     if (st) return cuda_check(ctx, cudaGetLastError(), "dem_nn_mlp_backward");
+    return DEM_OK;
+}
+
+extern "C" int dem_solver_debug_stream_waits(dem_solver *s, int poll_limit, int drop_copies) {
+    if (!s || poll_limit < 0) return DEM_ERR_INVALID;
+    dem_ctx *ctx = s->ctx;
+    s->fc.wait_polls = poll_limit;
+    s->fc.drop_copies = drop_copies ? 1 : 0;
+    s->version++;   // graphs are captured again with the new settings
+    if (!drop_copies) k_clear_status<<<1, 32, 0, ctx->stream>>>(s->p->ctl, DEM_ERR_TIMEOUT);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->stream));
     return DEM_OK;
 }
 

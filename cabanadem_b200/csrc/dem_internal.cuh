@@ -125,6 +125,8 @@ struct ForceConsts {
     int has_ext;
     int has_fix;
     int mixed;                 // 1: FP32 contact forces (dem_mixed.cu)
+    int wait_polls;            // polls per bounded wait of the staged streaming kernel (0: default)
+    int drop_copies;           // testing only: the staged kernel arms its barriers but copies nothing
     int stream_block;          // k_stream block size: 64, 128 or 256
     int split;                 // streaming pass: 1 one kernel over every particle (k_stream);
                                // 2 the lone particles and the rest in two persistent kernels

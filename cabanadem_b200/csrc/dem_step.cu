@@ -348,6 +348,7 @@ __global__ void __launch_bounds__(T, STREAM_BULK_MINB) k_stream_bulk(Particles P
         unsigned char *sb = smem + (k % S) * B::BYTES;
         uint64_t *bar = &full[k % S];
         bulk::bar_arrive_expect(bar, (uint32_t)m * (32u + 24u + 8u + 4u + (lists ? 4u : 0u) + 4u * rows + (c.wfar ? 1u : 0u)));
+        if (fc.drop_copies) return;   // testing the bounded waits: nothing will arrive
         bulk::copy_g2s(sb + B::POS, pc + i0, 32u * m, bar);
         for (int d = 0; d < 3; ++d) bulk::copy_g2s(sb + B::VEL + 8 * T * d, vc + (long)d * cap + i0, 8u * m, bar);
         bulk::copy_g2s(sb + B::MASS, P.mI + i0, 8u * m, bar);
@@ -358,10 +359,11 @@ __global__ void __launch_bounds__(T, STREAM_BULK_MINB) k_stream_bulk(Particles P
     };
     if (threadIdx.x == 0)
         for (int k = 0; k < S && k < mine; ++k) issue(k);
+    const int limit = fc.wait_polls > 0 ? fc.wait_polls : kBulkWaitLimit;
     double vmax2 = 0.0;
     int k = 0;
     for (; k < mine; ++k) {
-        if (!bulk::bar_wait(&full[k % S], (k / S) & 1, kBulkWaitLimit)) s_fail = 1;
+        if (!bulk::bar_wait(&full[k % S], (k / S) & 1, limit)) s_fail = 1;
         __syncthreads();
         if (s_fail) break;
         const unsigned char *sb = smem + (k % S) * B::BYTES;
@@ -409,7 +411,7 @@ __global__ void __launch_bounds__(T, STREAM_BULK_MINB) k_stream_bulk(Particles P
     if (k < mine) {   // a wait gave up: report, and let the copies in flight land before exiting
         if (threadIdx.x == 0) {
             atomicOr(&ctl->status, DEM_ERR_TIMEOUT);
-            for (int q = k; q < k + S && q < mine; ++q) bulk::bar_wait(&full[q % S], (q / S) & 1, kBulkWaitLimit);
+            for (int q = k; q < k + S && q < mine; ++q) bulk::bar_wait(&full[q % S], (q / S) & 1, limit);
         }
         return;
     }

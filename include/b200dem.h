@@ -405,6 +405,14 @@ int dem_nn_status(dem_ctx *ctx, int *status);
  * and sets DEM_ERR_TIMEOUT in the word dem_nn_status returns.  The setting is per device and
  * process-wide; it takes effect for kernels queued after the call. */
 int dem_nn_debug_waits(dem_ctx *ctx, int poll_limit, int drop_mma);
+/* Bounds of the staged streaming kernel's waits (stream_split 4), for testing that a wait which
+ * runs out stops the run with DEM_ERR_TIMEOUT and leaves the context usable (no reference
+ * counterpart).  poll_limit: polls of a tile's copy barrier per wait (0 = the default, about
+ * 260,000); drop_copies != 0: the kernel arms its barriers but issues no copy, so every wait
+ * runs out with nothing in flight.  A run then returns DEM_ERR_TIMEOUT with its step
+ * unfinished (the particle state must be set again).  Calling with drop_copies = 0 also clears
+ * the DEM_ERR_TIMEOUT bit of the solver's control word. */
+int dem_solver_debug_stream_waits(dem_solver *s, int poll_limit, int drop_copies);
 
 /* ---- Learned surrogate: message-passing network over the contact graph -------------------
  * Quasi-2D (x, y) particles.  One network stride replaces `steps_per_stride` DEM steps:

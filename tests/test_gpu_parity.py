@@ -178,6 +178,28 @@ def test_streaming_pass_forms_bitwise(split, packing):
     assert s.stats()["rebuilds"] >= 1
 
 
+def test_staged_streaming_wait_that_runs_out_stops_the_run():
+    """The staged streaming kernel's bounded waits: with dem_solver_debug_stream_waits(drop_copies=1)
+    it arms its tile barriers but issues no copy, so every wait gives up after the poll limit with
+    nothing in flight, and the run stops with DEM_ERR_TIMEOUT (no hang, no fault).  With the
+    default bounds back and the state set again, the same solver steps bit-identically to the
+    oracle: the context stayed usable."""
+    from cabanadem_b200 import _lib
+    sc = S.random_box(n=4133, nsteps=60)
+    ref, _ = _oracle(sc, 60)
+    s = api.from_scenario(sc, contact_lanes=8, stream_split=4)
+    L = _lib.lib()
+    assert L.dem_solver_debug_stream_waits(s.h, 64, 1) == 0
+    try:
+        with pytest.raises(_lib.DemError, match="DEM_ERR_TIMEOUT"):
+            s.run_steps(5)
+    finally:
+        assert L.dem_solver_debug_stream_waits(s.h, 0, 0) == 0
+    s.particles.upload(sc.state)
+    s.run_steps(60)
+    _assert_bitwise(s.particles.download(), ref, where="after a timed-out run")
+
+
 @pytest.mark.parametrize("lanes", [0, 1, 8, "pairs"], ids=["auto", "per_thread", "coop8", "pairs"])
 def test_moving_wall_bitwise(lanes):
     """A kinematic piston (DEM_Q6_WALL_STATIC clear) driven into a compressed box at 5 m/s,
