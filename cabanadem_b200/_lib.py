@@ -37,7 +37,7 @@ class SolverParams(C.Structure):
     _fields_ = [("dt", C.c_double), ("delta", C.c_double), ("skin", C.c_double), ("rebuild_every_step", C.c_int),
                 ("precision", C.c_int), ("gravity", C.c_double * 3), ("max_neighbors", C.c_int),
                 ("steps_per_launch", C.c_int), ("stream_block", C.c_int), ("contact_lanes", C.c_int),
-                ("stream_split", C.c_int), ("dense_form", C.c_int)]
+                ("stream_split", C.c_int), ("dense_form", C.c_int), ("scene_kernel", C.c_int)]
 
 
 class SceneParams(C.Structure):

@@ -43,6 +43,7 @@ struct dem_particles {
     bool has_bonds = false;  // bond slots hold sorted indices: no re-sort from now on
     bool any_fix = false;    // some particle carries a DEM_FIX_* flag
     int nscenes = 1;         // 1 + largest DEM_F_SCENE value
+    int max_scene = 0;       // particles of the largest scene (DEM_F_SCENE set), else 0
     void *stage = nullptr;   // device staging buffer for set/get (largest field)
     size_t stage_bytes = 0;
     std::vector<uint8_t> mat;   // caller order
@@ -93,6 +94,12 @@ struct dem_solver {
     double graph_ms = 0.0;                      // device time of the replays
     long graph_steps_run = 0;                   // steps those replays advanced
     int graph_done_mark = 0;                    // steps_done before the current replay
+    // batched small scenes in one persistent launch per run (scene_kernel 0)
+    int2 *d_scene_table = nullptr;              // [nscenes] first storage index, count
+    int *d_scene_counts = nullptr, *d_scene_bad = nullptr;
+    int scene_table_n = 0;                      // scenes the table holds
+    bool scenes_ready = false;                  // the table matches the storage order
+    bool scenes_unfit = false;                  // a scene was found not contiguous: per-step form
 };
 
 struct dem_bonds {
@@ -608,6 +615,11 @@ extern "C" int dem_particles_set(dem_particles *p, int field, const void *host, 
             }
             k_scatter_i<<<kGS, kTB, 0, s>>>((int *)tmp, P.scene, n, 1, P.cap, P.rank, 0);
             p->nscenes = mx + 1;
+            {
+                std::vector<int> cnt(p->nscenes, 0);
+                for (int i = 0; i < n; ++i) ++cnt[sc[i]];
+                p->max_scene = *std::max_element(cnt.begin(), cnt.end());
+            }
             p->mat_dirty = true;
             break;
         }
@@ -1112,6 +1124,7 @@ int build_now(dem_solver *s, bool resort) { return build_with(s, resort, s->sp.d
 
 int build_with(dem_solver *s, bool resort, double delta, double skin) {
     dem_ctx *ctx = s->ctx;
+    s->scenes_ready = false;   // this build's order partitions the storage by class, not by scene
     if (s->p->has_bonds) resort = false;
     for (int attempt = 0; attempt < 8; ++attempt) {
         launch_build(s->p->P, s->p->alt, s->L, s->B, s->p->ctl, delta, skin, resort, false, ctx->stream);
@@ -1377,6 +1390,7 @@ extern "C" int dem_solver_destroy(dem_solver *s) {
     if (s->aux.fork) cudaEventDestroy(s->aux.fork);
     if (s->aux.join) cudaEventDestroy(s->aux.join);
     cudaFree(s->d_pp); cudaFree(s->d_pw); cudaFree(s->d_walls); cudaFree(s->d_scenes);
+    cudaFree(s->d_scene_table); cudaFree(s->d_scene_counts); cudaFree(s->d_scene_bad);
     cudaFree(s->L.nn); cudaFree(s->L.idx); cudaFree(s->L.defer); cudaFree(s->L.defer_v); cudaFree(s->L.defer_w);
     cudaFree(s->L.wfar); cudaFree(s->L.nn_old); cudaFree(s->L.idx_old);
     free_pairs(s);
@@ -1456,6 +1470,74 @@ extern "C" int dem_solver_mesh_translation(dem_solver *s, double *host3) {
     return DEM_OK;
 }
 
+namespace {
+// Whether a run takes the persistent per-scene form: batched scenes of at most
+// kSceneMaxParticles particles, the Verlet-skin mode, static walls, no mesh, no bonds, the
+// per-step forms not chosen by the caller.
+bool scenes_persistent(const dem_solver *s) {
+    return s->sp.scene_kernel == 0 && s->nscenes > 0 && s->p->P.scene && s->p->max_scene > 0 &&
+           s->p->max_scene <= kSceneMaxParticles && !ref_mode(s) && s->mesh_nt == 0 && !s->fc.mwalls &&
+           !s->p->has_bonds && s->sp.contact_lanes == 0 && s->sp.dense_form == 0 && !s->scenes_unfit;
+}
+
+// A run in one persistent launch (dem_scenes.cuh).  Returns DEM_ERR_UNSUPPORTED, with nothing
+// changed, when the storage turns out not to hold every scene contiguously (the caller then
+// takes the per-step form).
+int run_scenes(dem_solver *s, int nsteps) {
+    dem_ctx *ctx = s->ctx;
+    cudaStream_t st = ctx->stream;
+    if (s->L.maxnb < kSceneMaxParticles) {
+        const int e = alloc_lists(s, kSceneMaxParticles);
+        if (e) return e;
+    }
+    if (!s->scenes_ready || s->p->dirty) {
+        // re-sort in plain cell order (scene-major keys): every scene contiguous
+        for (int attempt = 0;; ++attempt) {
+            launch_build(s->p->P, s->p->alt, s->L, s->B, s->p->ctl, s->sp.delta, s->sp.skin, true, false, st, false);
+            s->launches += build_kernel_count(true);
+            const Ctl c = read_ctl(s);
+            if (!(c.status & DEM_ERR_NEIGHBOR_OVERFLOW)) break;
+            if (attempt >= 2 || c.max_nbr > 128) return fail(ctx, DEM_ERR_NEIGHBOR_OVERFLOW, "neighbour list overflow");
+            const int e = alloc_lists(s, std::min(std::max(2 * s->L.maxnb, c.max_nbr + 8), 128));
+            if (e) return e;
+            k_clear_status<<<1, 32, 0, st>>>(s->p->ctl, DEM_ERR_NEIGHBOR_OVERFLOW);
+        }
+        s->p->dirty = false;
+        const int ns = s->p->nscenes;
+        if (s->scene_table_n < ns) {
+            cudaFree(s->d_scene_table);
+            cudaFree(s->d_scene_counts);
+            cudaFree(s->d_scene_bad);
+            s->d_scene_table = nullptr;
+            s->d_scene_counts = s->d_scene_bad = nullptr;
+            CK(dalloc(&s->d_scene_table, (size_t)ns));
+            CK(dalloc(&s->d_scene_counts, (size_t)ns));
+            CK(dalloc(&s->d_scene_bad, 1));
+            s->scene_table_n = ns;
+        }
+        if (!launch_scene_table(s->p->P, ns, s->d_scene_table, s->d_scene_counts, s->d_scene_bad, st)) {
+            CK(cudaGetLastError());
+            s->scenes_unfit = true;
+            s->built = false;
+            return DEM_ERR_UNSUPPORTED;
+        }
+        s->scenes_ready = true;
+    }
+    const double half_skin = 1e300;   // lists are rebuilt inside the launch, every step
+    k_run_begin<<<1, 32, 0, st>>>(s->p->ctl, nsteps, half_skin);
+    launch_prologue(s->p->P, s->p->ctl, s->fc, st);
+    launch_scene_steps(s->p->P, s->L, s->p->ctl, s->fc, s->d_pp, s->d_pw, s->d_walls, s->d_scene_table,
+                       s->p->nscenes, nsteps, s->sp.delta, s->sp.skin, st);
+    s->launches += 4;
+    CK(cudaGetLastError());
+    const Ctl c = read_ctl(s);
+    CK(cudaGetLastError());
+    s->built = false;   // the lists are per-scene lists of the last step, not a Verlet list
+    if (c.status & DEM_ERR_NEIGHBOR_OVERFLOW) return fail(ctx, DEM_ERR_NEIGHBOR_OVERFLOW, "scene list overflow");
+    return c.status & (DEM_ERR_CONTACT_OVERFLOW | DEM_ERR_NAN);
+}
+}  // namespace
+
 extern "C" int dem_solver_run(dem_solver *s, int nsteps) {
     if (!s) return DEM_ERR_INVALID;
     if (nsteps <= 0) return DEM_OK;
@@ -1467,6 +1549,10 @@ extern "C" int dem_solver_run(dem_solver *s, int nsteps) {
     {
         const int wst = check_walls(s);
         if (wst) return wst;
+    }
+    if (scenes_persistent(s)) {
+        const int e = run_scenes(s, nsteps);
+        if (e != DEM_ERR_UNSUPPORTED) return e;
     }
     cudaStream_t st = ctx->stream;
     double half_skin;

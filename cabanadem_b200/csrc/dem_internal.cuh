@@ -267,8 +267,21 @@ void launch_energy(const Particles &P, const NbrList &L, Ctl *ctl, const ForceCo
 // ---- launchers (dem_nbr.cu) -------------------------------------------------------
 // Builds the neighbour list of the current order; with `resort` the particles are first
 // re-ordered by Morton cell key (state permuted, contact partners remapped).
+// classes = false: a re-sort keeps the plain cell order (scene-major for batched scenes), without
+// the partition into particles with no listed neighbour, clear ones and the rest.
 void launch_build(const Particles &P, Particles &alt, const NbrList &L, BuildBuffers &B, Ctl *ctl, double delta,
-                  double skin, bool resort, bool check_run, cudaStream_t s);
+                  double skin, bool resort, bool check_run, cudaStream_t s, bool classes = true);
+// Batched small scenes in one persistent launch per run (dem_scenes.cuh): the scene table of
+// the current storage (false when some scene is not contiguous or exceeds the block), and the
+// run's steps.
+bool launch_scene_table(const Particles &P, int nscenes, int2 *table, int *counts, int *bad, cudaStream_t s);
+void launch_scene_steps(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
+                        const PairConst *pw, const WallGeom *walls, const int2 *table, int nscenes, int nsteps,
+                        double delta, double skin, cudaStream_t s);
+void launch_scene_steps_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc,
+                              const PairConst *pp, const PairConst *pw, const WallGeom *walls, const int2 *table,
+                              int nscenes, int nsteps, double delta, double skin, cudaStream_t s);
+constexpr int kSceneMaxParticles = 64;   // largest scene of the persistent form
 
 // dense layers of the surrogate (dem_nn.cu)
 int nn_mlp_forward(const dem_nn_mlp &m, long rows, const dem_nn_rows *src, int nsrc, const void *resid, void *out,

@@ -9,6 +9,7 @@
 #include "dem_particle.cuh"
 #include "dem_contact_coop.cuh"
 #include "dem_pairs.cuh"
+#include "dem_scenes.cuh"
 
 namespace b200dem {
 
@@ -166,6 +167,13 @@ void launch_pairs_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const Fo
 
 const void *contact_mixed_kernel(int dense, int coop, bool mesh) {
     return mesh ? contact_mixed_kernel_t<true>(dense, coop) : contact_mixed_kernel_t<false>(dense, coop);
+}
+
+void launch_scene_steps_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc,
+                              const PairConst *pp, const PairConst *pw, const WallGeom *walls, const int2 *table,
+                              int nscenes, int nsteps, double delta, double skin, cudaStream_t s) {
+    k_scene_steps<true><<<nscenes, kSceneBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls, table, nsteps, delta, skin);
+    k_scene_run_end<<<1, 32, 0, s>>>(ctl, nsteps);
 }
 
 }  // namespace b200dem

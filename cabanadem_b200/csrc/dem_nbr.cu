@@ -491,11 +491,11 @@ __global__ void __launch_bounds__(128) k_list(Particles P, NbrList L, Ctl *ctl, 
 // else 2.  Per-block counts of classes 0 and 1 into sums[0][b], sums[1][b].
 __global__ void __launch_bounds__(kPartBlock) k_part_flag(Particles P, const Ctl *ctl, const Grid *g, const int *start,
                                                           const int *items, double delta, double skin, int *cls,
-                                                          int *sums, int nb) {
+                                                          int *sums, int nb, int classes) {
     const int cur = ctl->cur, n = P.n;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     int c_s = 2;
-    if (s < n && !(ctl->status & DEM_ERR_NAN)) {
+    if (s < n && classes && !(ctl->status & DEM_ERR_NAN)) {
         const int q = items[s];
         const Grid G = g[scene_of(P, q)];
         const double4 *pc = P.pos[cur];
@@ -557,7 +557,7 @@ __global__ void __launch_bounds__(kPartBlock) k_part_flag(Particles P, const Ctl
 // k_list (kMaxCand kept, DEM_ERR_NEIGHBOR_OVERFLOW when a list exceeds the capacity).
 __global__ void __launch_bounds__(kPartBlock) k_part_list(Particles P, NbrList L, Ctl *ctl, const Grid *g,
                                                           const int *start, const int *items, double delta,
-                                                          double skin, int *cls, int *sums, int nb) {
+                                                          double skin, int *cls, int *sums, int nb, int classes) {
     const int cur = ctl->cur, n = P.n, cap = P.cap;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     const bool invalid = (ctl->status & DEM_ERR_NAN) != 0;
@@ -616,7 +616,7 @@ __global__ void __launch_bounds__(kPartBlock) k_part_list(Particles P, NbrList L
         const int keep = count < lim ? count : lim;
         for (int k = 0; k < keep; ++k) L.idx_old[(long)k * cap + q] = cand[k];
         L.nn_old[q] = keep;
-        c_s = count == 0 ? 0 : (near ? 2 : 1);
+        c_s = !classes ? 2 : count == 0 ? 0 : (near ? 2 : 1);
     }
     if (s < n) cls[s] = c_s;
     __shared__ int cnt[2];
@@ -732,7 +732,7 @@ __global__ void k_build_end(Ctl *ctl) {
 }  // namespace
 
 void launch_build(const Particles &P, Particles &alt, const NbrList &L, BuildBuffers &B, Ctl *ctl, double delta,
-                  double skin, bool resort, bool check_run, cudaStream_t s) {
+                  double skin, bool resort, bool check_run, cudaStream_t s, bool classes) {
     (void)check_run;
     const int n = P.n;
     const int gs = 148 * 8;
@@ -757,10 +757,10 @@ void launch_build(const Particles &P, Particles &alt, const NbrList &L, BuildBuf
         const int nb = (n + kPartBlock - 1) / kPartBlock;
         if (L.idx_old)   // the lists too, in the old order (re-indexed below)
             k_part_list<<<nb, kPartBlock, 0, s>>>(P, L, ctl, B.grid, B.cell_fill, B.cell_items, delta, skin, B.src,
-                                                  B.part_sums, nb);
+                                                  B.part_sums, nb, classes ? 1 : 0);
         else
             k_part_flag<<<nb, kPartBlock, 0, s>>>(P, ctl, B.grid, B.cell_fill, B.cell_items, delta, skin, B.src,
-                                                  B.part_sums, nb);
+                                                  B.part_sums, nb, classes ? 1 : 0);
         k_part_scan<<<1, 1024, 0, s>>>(B.part_sums, nb, ctl);
         k_part_place<<<nb, kPartBlock, 0, s>>>(n, B.src, B.part_sums, nb, ctl, B.cell_items, B.key);
         k_make_dst<<<gs, kB, 0, s>>>(n, B.key, B.dst);

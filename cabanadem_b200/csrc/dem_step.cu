@@ -19,6 +19,7 @@
 #include "dem_bulk.cuh"
 #include "dem_contact_coop.cuh"
 #include "dem_pairs.cuh"
+#include "dem_scenes.cuh"
 
 namespace b200dem {
 
@@ -850,6 +851,31 @@ void launch_energy(const Particles &P, const NbrList &L, Ctl *ctl, const ForceCo
                    cudaStream_t s) {
     k_energy_partials<<<nparts, kBlock, 0, s>>>(P, L, fc, pp, pw, walls, ctl, partials);
     k_energy_final<<<1, 32, 0, s>>>(partials, nparts, out);
+}
+
+bool launch_scene_table(const Particles &P, int nscenes, int2 *table, int *counts, int *bad, cudaStream_t s) {
+    if (!P.scene || nscenes <= 0) return false;
+    cudaMemsetAsync(counts, 0, sizeof(int) * nscenes, s);
+    cudaMemsetAsync(bad, 0, sizeof(int), s);
+    const int g = (P.n + 255) / 256 < 148 * 8 ? (P.n + 255) / 256 : 148 * 8;
+    k_scene_hist<<<g > 0 ? g : 1, 256, 0, s>>>(P.scene, P.n, counts);
+    k_scene_bounds<<<g > 0 ? g : 1, 256, 0, s>>>(P.scene, P.n, table);
+    k_scene_check<<<(nscenes + 255) / 256, 256, 0, s>>>(nscenes, table, counts, bad);
+    int h = 1;
+    if (cudaMemcpyAsync(&h, bad, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess) return false;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return false;
+    return h == 0;
+}
+
+void launch_scene_steps(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
+                        const PairConst *pw, const WallGeom *walls, const int2 *table, int nscenes, int nsteps,
+                        double delta, double skin, cudaStream_t s) {
+    if (fc.mixed) {
+        launch_scene_steps_mixed(P, L, ctl, fc, pp, pw, walls, table, nscenes, nsteps, delta, skin, s);
+        return;
+    }
+    k_scene_steps<false><<<nscenes, kSceneBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls, table, nsteps, delta, skin);
+    k_scene_run_end<<<1, 32, 0, s>>>(ctl, nsteps);
 }
 
 }  // namespace b200dem

@@ -133,6 +133,11 @@ typedef struct dem_solver_params {
                             * with a thread per particle, 2 three kernels: contact search per
                             * particle, the pair law per contact, sums and integration per
                             * particle; 2 is also used at every density.  Same results.         */
+    int scene_kernel;      /* batched scenes (dem_solver_set_scenes) of at most 64 particles each:
+                            * 0 = automatic (a run is one persistent launch, a block per scene,
+                            * every step inside it; with the Verlet-skin mode, static walls, no
+                            * mesh, contact_lanes and dense_form 0), 1 = the per-step kernels.
+                            * Same results.                                                    */
 } dem_solver_params;
 
 typedef struct dem_run_stats {

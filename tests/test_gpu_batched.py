@@ -97,3 +97,34 @@ def test_size_buckets_with_their_own_settings_equal_one_batch():
     for f in STATE:
         assert np.array_equal(getattr(got, f), getattr(ref, f)), f
     runner.close()
+
+
+@pytest.mark.parametrize("precision", [DEM_FP64, DEM_MIXED], ids=["fp64", "mixed"])
+def test_small_scenes_in_one_persistent_launch(precision):
+    """Scenes of at most 64 particles: a run is one launch, a block per scene with every step
+    inside it (scene_kernel 0).  The state equals that of the per-step kernels (scene_kernel 1)
+    bit for bit, over runs of odd and even length (the buffer parity of the launch), and in FP64
+    every scene equals the oracle run on that scene alone."""
+    nsteps = (101, 200)
+    sc = S.batched_scenes(nscenes=48, nmax=64, seed=31, nsteps=sum(nsteps))
+    a = api.from_scenario(S.batched_scenes(nscenes=48, nmax=64, seed=31, nsteps=sum(nsteps)), precision=precision)
+    b = api.from_scenario(S.batched_scenes(nscenes=48, nmax=64, seed=31, nsteps=sum(nsteps)), precision=precision,
+                          scene_kernel=1)
+    for k in nsteps:
+        a.run_steps(k)
+        b.run_steps(k)
+    ga, gb = a.particles.download(), b.particles.download()
+    for f in STATE:
+        assert np.array_equal(getattr(ga, f), getattr(gb, f)), f
+    assert a.stats()["launches"] * 10 < b.stats()["launches"]     # one launch per run, not per step
+    assert ga.tng_count.sum() > 0                                  # contacts formed
+    if precision == DEM_FP64:
+        counts = sc.extra["counts"]
+        starts = np.concatenate([[0], np.cumsum(counts)])
+        for k in range(0, len(counts), 7):
+            sub = S.scene_subset(sc, k)
+            ref = sub.state.copy()
+            O.run(ref, sub.walls, sub.params, sub.dt, sum(nsteps), skin=sub.skin, pow_mode=O.POW_SQRT)
+            mine = _scene_slice(ga, starts[k], counts[k])
+            for f in STATE:
+                assert np.array_equal(mine[f], getattr(ref, f)), (k, f)
