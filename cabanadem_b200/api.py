@@ -490,14 +490,16 @@ class BatchRunner:
     thread per bucket, each a graph-looped run of its solver, the buckets' kernels running
     concurrently on the GPU.  Scenes never interact, so every scene evolves as it does alone."""
 
-    def __init__(self, sc, precision=_lib.DEM_FP64, configs=None, tune=False, device=0, tune_steps=40):
+    def __init__(self, sc, precision=_lib.DEM_FP64, configs=None, tune=False, device=0, tune_steps=300):
         from . import autotune, scenarios as S
         self.n = sc.state.n
         self.parts = []
         for b, sub, ids in S.split_scenes(sc):
             cfg = (configs or {}).get(b)
             if cfg is None and tune:
-                cfg = autotune.tune(sub, precision=precision, warmup=5, steps=tune_steps)
+                # long enough trials to see the rebuild cadence each skin gives (a rebuild every
+                # 50-100 steps in the fired clusters)
+                cfg = autotune.tune(sub, precision=precision, warmup=20, steps=tune_steps)
             elif cfg is None:
                 cfg = autotune.packaged(sub, precision)   # B200 settings shipped with the package
             cfg = dict(autotune.DEFAULTS, **(cfg or {}))

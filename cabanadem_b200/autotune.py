@@ -12,7 +12,8 @@ caller-index order, whatever its cutoff or the re-sort):
                         shared memory) or 1 (one thread per particle, ``stream_block`` wide blocks)
 * ``stream_block``      block size of the one-thread-per-particle streaming kernel (64, 128, 256)
 * ``steps_per_launch``  0: the step loop as a graph while-loop; else fused steps per captured graph
-* ``skin``              Verlet skin, i.e. the rebuild cadence
+* ``skin``              Verlet skin (0.5, 1, 2 or 4 times the scenario's), i.e. the rebuild cadence
+                        against the listed neighbours a streaming pass checks
 
 ``tune`` times short runs of the caller's workload for each candidate, one setting at a time
 (coordinate search from the defaults), and caches the winner per size bucket (log2 of the
@@ -33,7 +34,7 @@ from . import api
 DEFAULTS = dict(contact_lanes=0, dense_form=0, stream_split=0, stream_block=128, steps_per_launch=0,
                 skin_factor=1.0)
 CANDIDATES = dict(contact_lanes=(0, 1, 4, 8), dense_form=(1, 2), stream_split=(0, 1), stream_block=(64, 128, 256),
-                  steps_per_launch=(0, 32), skin_factor=(0.5, 1.0, 2.0))
+                  steps_per_launch=(0, 32), skin_factor=(0.5, 1.0, 2.0, 4.0))
 ORDER = ("contact_lanes", "dense_form", "stream_split", "stream_block", "steps_per_launch", "skin_factor")
 
 

@@ -14,11 +14,11 @@ def _cost(cfg):
     return ({0: 4.0, 1: 3.0, 4: 1.0, 8: 2.0}[cfg["contact_lanes"]] + {0: 3.0, 1: 2.0, 2: 1.0}[cfg["dense_form"]]
             + {0: 2.0, 1: 1.0}[cfg["stream_split"]]
             + {64: 3.0, 128: 2.0, 256: 1.0}[cfg["stream_block"]] + {0: 2.0, 32: 1.0}[cfg["steps_per_launch"]]
-            + {0.5: 1.0, 1.0: 2.0, 2.0: 3.0}[cfg["skin_factor"]])
+            + {0.5: 1.0, 1.0: 2.0, 2.0: 3.0, 4.0: 4.0}[cfg["skin_factor"]])
 
 
 BEST = dict(contact_lanes=4, dense_form=2, stream_split=1, stream_block=256, steps_per_launch=32, skin_factor=0.5)
-NTRIALS = 1 + 3 + 2 + 1 + 2 + 1 + 2     # defaults + every other candidate of each knob
+NTRIALS = 1 + 3 + 2 + 1 + 2 + 1 + 3     # defaults + every other candidate of each knob
 
 
 def test_coordinate_search_and_cache(tmp_path, monkeypatch):
