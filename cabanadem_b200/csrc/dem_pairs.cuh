@@ -35,7 +35,8 @@ constexpr int kPairsBlock = 128;
 // List entries the contact search tests per round: their index loads, then their position
 // loads, are issued together (B200, dam-break state, FP64 step: 79.2 us with one entry per round,
 // 76.8 us with two, 81.9 us with four -- more registers, fewer resident warps; testing the
-// tracked slots the same way before the compaction cost more registers than it saved).
+// tracked slots the same way before the compaction, or prefetching the first two tracked
+// partners with the own state, cost more registers than they saved: 82.1 and 83.8 us).
 constexpr int kFindBatch = 2;
 // The three kernels are compiled without a register cap: on the dam-break state (B200) caps of
 // 80 / 64 registers for the per-contact and summing kernels (more resident blocks, spills) ran

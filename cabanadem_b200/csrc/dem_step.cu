@@ -511,12 +511,13 @@ __global__ void __launch_bounds__(kApplyBlock) k_apply(Particles P, NbrList L, C
 // Prologue of a run: stage1 + stage2 of its first step with the stored F, tau
 // (src/CabanaDEM_Integrator.hpp:31-74).  u and omega in place; positions to the next
 // buffer, which becomes current.
+// Persistent grid-stride form: the step finalisation takes one ticket per block, so a grid of
+// one block per 128 particles (15,625 on the 2M lattice) would queue as many atomics on one word.
 __global__ void __launch_bounds__(kBlock) k_prologue(Particles P, Ctl *ctl, ForceConsts fc) {
     const int cur = ctl->cur, nxt = cur ^ 1, vcur = ctl->vcur;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int cap = P.cap;
     double vmax2 = 0.0;
-    if (i < P.n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += gridDim.x * blockDim.x) {
         const double m_inverse = 1. / P.mI[i], h = fc.half_dt;
         double *vc = P.vel[vcur], *wc = P.omg[vcur];
         double u[3];
@@ -537,7 +538,7 @@ __global__ void __launch_bounds__(kBlock) k_prologue(Particles P, Ctl *ctl, Forc
         p.x += fc.dt * u[0];
         p.y += fc.dt * u[1];
         p.z += fc.dt * u[2];
-        vmax2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+        vmax2 = fmax(vmax2, u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
         st4(P.pos[nxt], i, p);
     }
     finish_step(ctl, P.vslots, vmax2, fc.dt, 0, false, false, &fc);
@@ -684,7 +685,8 @@ void launch_permute_mesh(const MeshDev &M, const MeshDev &A, int n, int cap, con
 }
 
 void launch_prologue(const Particles &P, Ctl *ctl, const ForceConsts &fc, cudaStream_t s) {
-    k_prologue<<<nblocks(P.n), kBlock, 0, s>>>(P, ctl, fc);
+    const int g = nblocks(P.n) < 148 * 12 ? nblocks(P.n) : 148 * 12;
+    k_prologue<<<g > 0 ? g : 1, kBlock, 0, s>>>(P, ctl, fc);
 }
 
 int kernels_per_step(const ForceConsts &fc) {
