@@ -642,7 +642,8 @@ def main():
 
     # end to end through the C ABI with host buffers (pinned): a new run sets positions,
     # velocities, spins, radii, masses, inertias and material constants, clears the contact
-    # state on the device (dem_particles_clear_contacts), steps, and reads the state back
+    # state and the stored force and torque on the device (a fresh start, as new particles
+    # have them), steps, and reads the state back
     barrier()
     host = sc.state.copy()
     pinned = []
@@ -661,6 +662,7 @@ def main():
         for f in up_fields:
             solver.particles.set(f, getattr(host, f))
         solver.particles.clear_contacts()
+        solver.particles.clear_forces()
         solver.run_steps(args.steps)
         return {f: solver.particles.get(f, out=outbuf[f]) for f in outbuf}
 
@@ -681,7 +683,7 @@ def main():
     e2e = {"value": ws * n * args.steps / (e2e_ms / 1e3), "unit": METRIC,
            "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
            "wall_ms": round(wall_ms, 2),
-           "uploaded": list(up_fields) + ["(contact state cleared on the device)"], "downloaded": list(outbuf)}
+           "uploaded": list(up_fields) + ["(contact state, force and torque cleared on the device)"], "downloaded": list(outbuf)}
     ck = clocks.stop()
     ck["window"] = "timed region, the sub-measurements and the end-to-end run (the timed region alone: timed_region)"
 

@@ -144,6 +144,7 @@ _PROTOS = {
     "dem_solver_debug_stream_waits": ([_VP, C.c_int, C.c_int], C.c_int),
     "dem_particles_get_device": ([_VP, C.c_int, _VP, C.c_long], C.c_int),
     "dem_particles_clear_contacts": ([_VP], C.c_int),
+    "dem_particles_clear_forces": ([_VP], C.c_int),
     "dem_checkpoint_save": ([_VP, C.c_char_p], C.c_int),
     "dem_checkpoint_load": ([_VP, C.c_char_p], C.c_int),
     "dem_surrogate_create": ([_VP, C.POINTER(SurrogateParams), C.POINTER(_VP)], C.c_int),

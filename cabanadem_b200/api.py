@@ -199,6 +199,11 @@ class Particles:
         (dem_particles_clear_contacts): a fresh start without uploading zero history."""
         check(lib().dem_particles_clear_contacts(self.h), self.ctx.h, "dem_particles_clear_contacts")
 
+    def clear_forces(self):
+        """Force and torque zero on the device (dem_particles_clear_forces), as new particles have
+        them: with clear_contacts, a fresh start from uploaded positions and velocities."""
+        check(lib().dem_particles_clear_forces(self.h), self.ctx.h, "dem_particles_clear_forces")
+
     def upload(self, s: ParticleState):
         for f in ("rad", "x", "u", "omega", "force", "torque", "m", "I", "rho", "E", "nu", "G",
                   "tng_idx", "tng_ss_x", "tng_ss_y", "tng_ss_z", "tng_count"):

@@ -661,6 +661,15 @@ extern "C" int dem_particles_clear_contacts(dem_particles *p) {
     return DEM_OK;
 }
 
+extern "C" int dem_particles_clear_forces(dem_particles *p) {
+    if (!p) return DEM_ERR_INVALID;
+    dem_ctx *ctx = p->ctx;
+    const size_t cn = (size_t)p->P.cap;
+    CK(cudaMemsetAsync(p->P.force, 0, sizeof(double) * 3 * cn, ctx->stream));
+    CK(cudaMemsetAsync(p->P.torque, 0, sizeof(double) * 3 * cn, ctx->stream));
+    return DEM_OK;
+}
+
 static int particles_get_impl(dem_particles *p, int field, void *host, long count, bool device) {
     if (!p || !host) return DEM_ERR_INVALID;
     dem_ctx *ctx = p->ctx;

@@ -205,6 +205,69 @@ __global__ void __launch_bounds__(kPairsBlock) k_pairs_find(Particles P, NbrList
     if (status) atomicOr(&ctl->status, status);
 }
 
+// One work item (k_pairs_find): the pair law with the pair's history slot, or the wall law with
+// the wall's history; cf receives the item's F (0..2) and tau (3..5) on particle i.
+template <bool MIXED>
+__device__ __forceinline__ void pairs_item(const Particles &P, const ForceConsts &fc, const PairConst *__restrict__ pp,
+                                           const PairConst *__restrict__ pw, const WallGeom *__restrict__ walls,
+                                           const double4 *__restrict__ pc, const double *__restrict__ vc,
+                                           const double *__restrict__ wc, const int4 it, double (&cf)[6]) {
+    const int cap = P.cap;
+    const unsigned q = fc.quirks;
+    const int i = it.x, j = it.y, slot = it.z;
+    const D4 pi = ld4(pc, i);
+    const double ui0 = vc[i], ui1 = vc[cap + i], ui2 = vc[2 * cap + i];
+    const double wi0 = wc[i], wi1 = wc[cap + i], wi2 = wc[2 * cap + i];
+    const double m_i = P.mI[i];
+    const int scene_i = P.scene ? P.scene[i] : 0;
+    const SceneConst *scn = fc.scenes ? fc.scenes + scene_i : nullptr;
+    const int mi = fc.nmat > 1 ? (int)P.mat[i] : 0;
+    if (j < 0) {
+        // wall item: j = -1 - wall, slot = the scene-local wall, it.w = wall history flag
+        // (Force.hpp:475-673, pw_wall)
+        const int w = -1 - j;
+        const WallGeom *g = walls + w;
+        const double px = pi.x - __ldg(&g->x[0]), py = pi.y - __ldg(&g->x[1]), pz = pi.z - __ldg(&g->x[2]);
+        const double nx = __ldg(&g->n[0]), ny = __ldg(&g->n[1]), nz = __ldg(&g->n[2]);
+        const double tmp = px * nx + py * ny + pz * nz;
+        const double overlap = pi.w - tmp;
+        const double K_n_pw = scn ? scn->K_n_pw : fc.K_n_pw, K_t_pw = scn ? scn->K_t_pw : fc.K_t_pw;
+        const double mu_pw = scn ? scn->mu_pw : fc.mu_pw;
+        double *swx = P.sw + (long)slot * cap + i;
+        double *swy = P.sw + (long)(P.mw + slot) * cap + i;
+        double *swz = P.sw + (long)(2 * P.mw + slot) * cap + i;
+        pw_wall<MIXED>(q, pi, nx, ny, nz, overlap, ui0, ui1, ui2, wi0, wi1, wi2, __ldg(&g->u[0]), __ldg(&g->u[1]),
+                       __ldg(&g->u[2]), m_i, pw[mi * fc.nwall + w], K_n_pw, K_t_pw, mu_pw, fc.dt, it.w != 0, swx,
+                       swy, swz, cf);
+    } else {
+        const D4 pj = ld4(pc, j);
+        const double K_n_pp = scn ? scn->K_n_pp : fc.K_n_pp, K_t_pp = scn ? scn->K_t_pp : fc.K_t_pp;
+        const double mu_pp = scn ? scn->mu_pp : fc.mu_pp;
+        const int mj = fc.nmat > 1 ? (int)P.mat[j] : 0;
+        const double px = pi.x - pj.x, py = pi.y - pj.y, pz = pi.z - pj.z;
+        const double r2ij = px * px + py * py + pz * pz;
+        const double sr = pi.w + pj.w;
+        const double rij = sqrt(r2ij);
+        const double overlap = sr - rij;
+        double *hx = P.th + (long)slot * cap + i;
+        double *hy = P.th + ((long)P.mc + slot) * cap + i;
+        double *hz = P.th + (2L * P.mc + slot) * cap + i;
+        double h0 = 0., h1 = 0., h2 = 0.;
+        if (slot >= 0) {
+            h0 = *hx;
+            h1 = *hy;
+            h2 = *hz;
+        }
+        pp_pair<MIXED>(P.mI, vc, wc, cap, q, pi, pj, j, px, py, pz, rij, overlap, ui0, ui1, ui2, wi0, wi1, wi2,
+                       m_i, pp[mi * fc.nmat + mj], K_n_pp, K_t_pp, mu_pp, fc.dt, h0, h1, h2, cf);
+        if (slot >= 0) {
+            *hx = h0;
+            *hy = h1;
+            *hz = h2;
+        }
+    }
+}
+
 template <bool MIXED>
 __global__ void __launch_bounds__(kPairsBlock) k_pairs_eval(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
                                                             const PairConst *__restrict__ pp,
@@ -212,67 +275,14 @@ __global__ void __launch_bounds__(kPairsBlock) k_pairs_eval(Particles P, NbrList
                                                             const WallGeom *__restrict__ walls) {
     const CtlSnap c = read_ctl(ctl, true);
     if (!c.go) return;
-    const int np = ctl->npairs, cap = P.cap;
-    const unsigned q = fc.quirks;
+    const int np = ctl->npairs;
     const double4 *__restrict__ pc = P.pos[c.cur];
     const int vcur = ctl->vcur;
     const double *__restrict__ vc = P.vel[vcur];
     const double *__restrict__ wc = P.omg[vcur];
     for (int t = blockIdx.x * kPairsBlock + threadIdx.x; t < np; t += gridDim.x * kPairsBlock) {
-        const int4 it = L.pitem[t];
-        const int i = it.x, j = it.y, slot = it.z;
-        const D4 pi = ld4(pc, i);
-        const double ui0 = vc[i], ui1 = vc[cap + i], ui2 = vc[2 * cap + i];
-        const double wi0 = wc[i], wi1 = wc[cap + i], wi2 = wc[2 * cap + i];
-        const double m_i = P.mI[i];
-        const int scene_i = P.scene ? P.scene[i] : 0;
-        const SceneConst *scn = fc.scenes ? fc.scenes + scene_i : nullptr;
-        const int mi = fc.nmat > 1 ? (int)P.mat[i] : 0;
         double cf[6];
-        if (j < 0) {
-            // wall item: j = -1 - wall, slot = the scene-local wall, it.w = wall history flag
-            // (Force.hpp:475-673, pw_wall)
-            const int w = -1 - j;
-            const WallGeom *g = walls + w;
-            const double px = pi.x - __ldg(&g->x[0]), py = pi.y - __ldg(&g->x[1]), pz = pi.z - __ldg(&g->x[2]);
-            const double nx = __ldg(&g->n[0]), ny = __ldg(&g->n[1]), nz = __ldg(&g->n[2]);
-            const double tmp = px * nx + py * ny + pz * nz;
-            const double overlap = pi.w - tmp;
-            const double K_n_pw = scn ? scn->K_n_pw : fc.K_n_pw, K_t_pw = scn ? scn->K_t_pw : fc.K_t_pw;
-            const double mu_pw = scn ? scn->mu_pw : fc.mu_pw;
-            double *swx = P.sw + (long)slot * cap + i;
-            double *swy = P.sw + (long)(P.mw + slot) * cap + i;
-            double *swz = P.sw + (long)(2 * P.mw + slot) * cap + i;
-            pw_wall<MIXED>(q, pi, nx, ny, nz, overlap, ui0, ui1, ui2, wi0, wi1, wi2, __ldg(&g->u[0]), __ldg(&g->u[1]),
-                           __ldg(&g->u[2]), m_i, pw[mi * fc.nwall + w], K_n_pw, K_t_pw, mu_pw, fc.dt, it.w != 0, swx,
-                           swy, swz, cf);
-        } else {
-            const D4 pj = ld4(pc, j);
-            const double K_n_pp = scn ? scn->K_n_pp : fc.K_n_pp, K_t_pp = scn ? scn->K_t_pp : fc.K_t_pp;
-            const double mu_pp = scn ? scn->mu_pp : fc.mu_pp;
-            const int mj = fc.nmat > 1 ? (int)P.mat[j] : 0;
-            const double px = pi.x - pj.x, py = pi.y - pj.y, pz = pi.z - pj.z;
-            const double r2ij = px * px + py * py + pz * pz;
-            const double sr = pi.w + pj.w;
-            const double rij = sqrt(r2ij);
-            const double overlap = sr - rij;
-            double *hx = P.th + (long)slot * cap + i;
-            double *hy = P.th + ((long)P.mc + slot) * cap + i;
-            double *hz = P.th + (2L * P.mc + slot) * cap + i;
-            double h0 = 0., h1 = 0., h2 = 0.;
-            if (slot >= 0) {
-                h0 = *hx;
-                h1 = *hy;
-                h2 = *hz;
-            }
-            pp_pair<MIXED>(P.mI, vc, wc, cap, q, pi, pj, j, px, py, pz, rij, overlap, ui0, ui1, ui2, wi0, wi1, wi2,
-                           m_i, pp[mi * fc.nmat + mj], K_n_pp, K_t_pp, mu_pp, fc.dt, h0, h1, h2, cf);
-            if (slot >= 0) {
-                *hx = h0;
-                *hy = h1;
-                *hz = h2;
-            }
-        }
+        pairs_item<MIXED>(P, fc, pp, pw, walls, pc, vc, wc, L.pitem[t], cf);
         double2 *term = L.pterm + 3L * t;
         term[0] = make_double2(cf[0], cf[1]);
         term[1] = make_double2(cf[2], cf[3]);
@@ -292,11 +302,71 @@ __device__ __noinline__ int mesh_contacts(const Particles &P, const ForceConsts 
     return mesh_pass<MIXED>(P, fc, i, pi, ui0, ui1, ui2, wi0, wi1, wi2, m_i, mi, K_n_pw, K_t_pw, mu_pw, FT, status);
 }
 
+// The hooks after the pair forces and the velocity-Verlet update of particle i (stage3 of this
+// step, stage1 + stage2 of the next, or F and tau stored after the run's last step); positions
+// and velocities to the other buffers.
+__device__ __forceinline__ void pairs_integrate(const Particles &P, const ForceConsts &fc, const CtlSnap &c,
+                                                const int vcur, const int i, const D4 &pi, double ui0, double ui1,
+                                                double ui2, double wi0, double wi1, double wi2, const double2 mIi,
+                                                double F0, double F1, double F2, double T0, double T1, double T2,
+                                                double &vmax2) {
+    const int cap = P.cap, nxt = c.cur ^ 1;
+    if (fc.has_gravity) {
+        F0 = dadd(F0, dmul(mIi.x, fc.g[0]));
+        F1 = dadd(F1, dmul(mIi.x, fc.g[1]));
+        F2 = dadd(F2, dmul(mIi.x, fc.g[2]));
+    }
+    if (fc.has_fix) {
+        const int f = P.fix[i];
+        if (f & DEM_FIX_FORCE) F0 = F1 = F2 = 0.;
+        if (f & DEM_FIX_TORQUE) T0 = T1 = T2 = 0.;
+    }
+    const double m_inverse = 1. / mIi.x;
+    const double I_inverse = 1. / mIi.y;
+    const double h = fc.half_dt;
+    // stage3 of this step
+    ui0 = dadd(ui0, dmul(dmul(h, F0), m_inverse));
+    ui1 = dadd(ui1, dmul(dmul(h, F1), m_inverse));
+    ui2 = dadd(ui2, dmul(dmul(h, F2), m_inverse));
+    wi0 = dadd(wi0, dmul(dmul(h, T0), I_inverse));
+    wi1 = dadd(wi1, dmul(dmul(h, T1), I_inverse));
+    wi2 = dadd(wi2, dmul(dmul(h, T2), I_inverse));
+    D4 pn = pi;
+    if (c.last) {
+        P.force[i] = F0;
+        P.force[cap + i] = F1;
+        P.force[2 * cap + i] = F2;
+        P.torque[i] = T0;
+        P.torque[cap + i] = T1;
+        P.torque[2 * cap + i] = T2;
+    } else {
+        // stage1 + stage2 of the next step
+        ui0 = dadd(ui0, dmul(dmul(h, F0), m_inverse));
+        ui1 = dadd(ui1, dmul(dmul(h, F1), m_inverse));
+        ui2 = dadd(ui2, dmul(dmul(h, F2), m_inverse));
+        wi0 = dadd(wi0, dmul(dmul(h, T0), I_inverse));
+        wi1 = dadd(wi1, dmul(dmul(h, T1), I_inverse));
+        wi2 = dadd(wi2, dmul(dmul(h, T2), I_inverse));
+        pn.x = dadd(pn.x, dmul(fc.dt, ui0));
+        pn.y = dadd(pn.y, dmul(fc.dt, ui1));
+        pn.z = dadd(pn.z, dmul(fc.dt, ui2));
+        vmax2 = fmax(vmax2, dadd(dadd(dmul(ui0, ui0), dmul(ui1, ui1)), dmul(ui2, ui2)));
+    }
+    st4(P.pos[nxt], i, pn);
+    double *vn = P.vel[vcur ^ 1], *wn = P.omg[vcur ^ 1];
+    vn[i] = ui0;
+    vn[cap + i] = ui1;
+    vn[2 * cap + i] = ui2;
+    wn[i] = wi0;
+    wn[cap + i] = wi1;
+    wn[2 * cap + i] = wi2;
+}
+
 template <bool MIXED, bool MESH>
 __global__ void __launch_bounds__(kPairsBlock) k_pairs_sum(Particles P, NbrList L, Ctl *ctl, ForceConsts fc) {
     const CtlSnap c = read_ctl(ctl, true);
     if (!c.go) return;
-    const int cap = P.cap, vcur = ctl->vcur, nxt = c.cur ^ 1;
+    const int cap = P.cap, vcur = ctl->vcur;
     const unsigned q = fc.quirks;
     const double4 *__restrict__ pc = P.pos[c.cur];
     const double *__restrict__ vc = P.vel[vcur];
@@ -353,59 +423,11 @@ __global__ void __launch_bounds__(kPairsBlock) k_pairs_sum(Particles P, NbrList 
             T2 = FT[5];
         }
         active += ((rec.z | cs) != 0 || mcnt != 0) ? 1 : 0;
-        // ---- hooks after the pair forces
-        if (fc.has_gravity) {
-            F0 = dadd(F0, dmul(mIi.x, fc.g[0]));
-            F1 = dadd(F1, dmul(mIi.x, fc.g[1]));
-            F2 = dadd(F2, dmul(mIi.x, fc.g[2]));
-        }
-        if (fc.has_fix) {
-            const int f = P.fix[i];
-            if (f & DEM_FIX_FORCE) F0 = F1 = F2 = 0.;
-            if (f & DEM_FIX_TORQUE) T0 = T1 = T2 = 0.;
-        }
-        const double m_inverse = 1. / mIi.x;
-        const double I_inverse = 1. / mIi.y;
-        const double h = fc.half_dt;
-        // stage3 of this step
-        ui0 = dadd(ui0, dmul(dmul(h, F0), m_inverse));
-        ui1 = dadd(ui1, dmul(dmul(h, F1), m_inverse));
-        ui2 = dadd(ui2, dmul(dmul(h, F2), m_inverse));
-        wi0 = dadd(wi0, dmul(dmul(h, T0), I_inverse));
-        wi1 = dadd(wi1, dmul(dmul(h, T1), I_inverse));
-        wi2 = dadd(wi2, dmul(dmul(h, T2), I_inverse));
-        D4 pn = pi;
-        if (c.last) {
-            P.force[i] = F0;
-            P.force[cap + i] = F1;
-            P.force[2 * cap + i] = F2;
-            P.torque[i] = T0;
-            P.torque[cap + i] = T1;
-            P.torque[2 * cap + i] = T2;
-        } else {
-            // stage1 + stage2 of the next step
-            ui0 = dadd(ui0, dmul(dmul(h, F0), m_inverse));
-            ui1 = dadd(ui1, dmul(dmul(h, F1), m_inverse));
-            ui2 = dadd(ui2, dmul(dmul(h, F2), m_inverse));
-            wi0 = dadd(wi0, dmul(dmul(h, T0), I_inverse));
-            wi1 = dadd(wi1, dmul(dmul(h, T1), I_inverse));
-            wi2 = dadd(wi2, dmul(dmul(h, T2), I_inverse));
-            pn.x = dadd(pn.x, dmul(fc.dt, ui0));
-            pn.y = dadd(pn.y, dmul(fc.dt, ui1));
-            pn.z = dadd(pn.z, dmul(fc.dt, ui2));
-            vmax2 = fmax(vmax2, dadd(dadd(dmul(ui0, ui0), dmul(ui1, ui1)), dmul(ui2, ui2)));
-        }
-        st4(P.pos[nxt], i, pn);
-        double *vn = P.vel[vcur ^ 1], *wn = P.omg[vcur ^ 1];
-        vn[i] = ui0;
-        vn[cap + i] = ui1;
-        vn[2 * cap + i] = ui2;
-        wn[i] = wi0;
-        wn[cap + i] = wi1;
-        wn[2 * cap + i] = wi2;
+        pairs_integrate(P, fc, c, vcur, i, pi, ui0, ui1, ui2, wi0, wi1, wi2, mIi, F0, F1, F2, T0, T1, T2, vmax2);
     }
     finish_step_counted(ctl, P.vslots, vmax2, fc.dt, status, active, fc, !c.last);
 }
+
 
 }  // namespace
 }  // namespace b200dem

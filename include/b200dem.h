@@ -181,6 +181,10 @@ int dem_particles_get_device(dem_particles *p, int field, void *dev, long count)
  * Device-side, no host copy: a caller starting a new run from fresh positions and
  * velocities sets those fields and calls this instead of uploading zero history arrays. */
 int dem_particles_clear_contacts(dem_particles *p);
+/* Force and torque zero, on the device, as newly created particles have them (the reference's
+ * AoSoA is zero-initialised, src/CabanaDEM_Particles.hpp:22-71): with dem_particles_clear_contacts
+ * the fresh start of a new run from uploaded positions and velocities. */
+int dem_particles_clear_forces(dem_particles *p);
 int dem_particles_size(dem_particles *p);
 
 /* ---- walls: Wall<Mem,3>(exec, n, out) (src/CabanaDEM_Wall.hpp:22-153) ------------- */
