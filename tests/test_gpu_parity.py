@@ -405,3 +405,38 @@ def test_sliding_sphere_on_floor(quirks):
     g.run_steps(3000)
     _assert_bitwise(g.particles.download(), ref, where="sliding%d" % quirks)
     assert ref.u[0, 0] < 1.0 - 0.5 * 9.81 * 2e-3        # slowing down by friction
+
+
+def test_uploads_from_pinned_memory_equal_pageable_ones():
+    """A set from page-locked host memory is queued on the stream without waiting (the ping-pong
+    buffer it writes is picked on the device): a run after such uploads, and reads into pinned
+    buffers, give the same bits as the same calls with ordinary arrays."""
+    import torch
+    sc = S.random_box(n=4133, nsteps=200)
+    outs = []
+    for pinned in (False, True):
+        s = api.from_scenario(sc, contact_lanes=8)
+        s.run_steps(37)                    # an odd count: the current buffers are the second ones
+        keep = []
+        for f in ("rad", "x", "u", "omega", "m", "I"):
+            a = np.ascontiguousarray(getattr(sc.state, f))
+            if pinned:
+                t = torch.from_numpy(a.copy()).pin_memory()
+                keep.append(t)
+                a = t.numpy()
+            s.particles.set(f, a)
+        s.particles.clear_contacts()
+        s.particles.clear_forces()
+        s.run_steps(150)
+        got = {}
+        for f in ("x", "u", "omega", "force", "torque", "tng_count"):
+            ref = s.particles.get(f)
+            if pinned:
+                buf = torch.empty(ref.shape, dtype=torch.from_numpy(ref).dtype).pin_memory()
+                got[f] = s.particles.get(f, out=buf.numpy()).copy()
+            else:
+                got[f] = ref
+        outs.append(got)
+        s.close()
+    for f in outs[0]:
+        assert np.array_equal(outs[0][f], outs[1][f]), f
