@@ -37,7 +37,8 @@ class SolverParams(C.Structure):
     _fields_ = [("dt", C.c_double), ("delta", C.c_double), ("skin", C.c_double), ("rebuild_every_step", C.c_int),
                 ("precision", C.c_int), ("gravity", C.c_double * 3), ("max_neighbors", C.c_int),
                 ("steps_per_launch", C.c_int), ("stream_block", C.c_int), ("contact_lanes", C.c_int),
-                ("stream_split", C.c_int), ("dense_form", C.c_int), ("scene_kernel", C.c_int)]
+                ("stream_split", C.c_int), ("dense_form", C.c_int), ("scene_kernel", C.c_int),
+                ("launch_overlap", C.c_int)]
 
 
 class SceneParams(C.Structure):
@@ -56,7 +57,8 @@ BFIELD = {name: k for k, name in enumerate(
 class RunStats(C.Structure):
     _fields_ = [("steps", C.c_long), ("rebuilds", C.c_long), ("max_neighbors", C.c_int),
                 ("neighbor_capacity", C.c_int), ("status", C.c_int), ("disp_bound", C.c_double),
-                ("launches", C.c_long), ("graph_ms", C.c_double), ("graph_steps", C.c_long)]
+                ("launches", C.c_long), ("graph_ms", C.c_double), ("graph_steps", C.c_long),
+                ("launch_overlap", C.c_int)]
 
 
 class NnRows(C.Structure):

@@ -311,7 +311,8 @@ class SolverDEM:
                  skin: float = 0.0, rebuild_every_step: bool = False, gravity=(0.0, 0.0, 0.0),
                  precision: int = _lib.DEM_FP64, num_steps: int = 0, output_frequency: int = 0,
                  max_neighbors: int = 0, steps_per_launch: int = 0, stream_block: int = 0,
-                 contact_lanes: int = 0, stream_split: int = 0, dense_form: int = 0, scene_kernel: int = 0):
+                 contact_lanes: int = 0, stream_split: int = 0, dense_form: int = 0, scene_kernel: int = 0,
+                 launch_overlap: int = 0):
         self.particles, self.wall, self.force = particles, wall, force
         self.dt, self.num_steps, self.output_frequency = float(dt), int(num_steps), int(output_frequency)
         sp = _lib.SolverParams()
@@ -326,6 +327,7 @@ class SolverDEM:
         sp.stream_split = int(stream_split)
         sp.dense_form = int(dense_form)
         sp.scene_kernel = int(scene_kernel)
+        sp.launch_overlap = int(launch_overlap)
         fp = force.params()
         h = C.c_void_p()
         check(lib().dem_solver_create(particles.ctx.h, particles.h, wall.h if wall else None, C.byref(fp),
@@ -459,7 +461,7 @@ def createSolverDEM(inputs: Inputs, particles: Particles, wall: Wall, force: For
 
 def from_scenario(sc, ctx: Context | None = None, rebuild_every_step=False, precision=_lib.DEM_FP64,
                   steps_per_launch=0, max_neighbors=0, stream_block=0, contact_lanes=0, stream_split=0,
-                  dense_form=0, scene_kernel=0):
+                  dense_form=0, scene_kernel=0, launch_overlap=0):
     """Particles + Wall + SolverDEM on the device for a scenarios.Scenario."""
     st = sc.state
     nwalls = sc.walls.n if sc.walls is not None else 0
@@ -476,7 +478,8 @@ def from_scenario(sc, ctx: Context | None = None, rebuild_every_step=False, prec
     s = SolverDEM(p, w, f, sc.dt, delta=sc.delta, skin=sc.skin, rebuild_every_step=rebuild_every_step,
                   gravity=sc.gravity, precision=precision, steps_per_launch=steps_per_launch,
                   max_neighbors=max_neighbors, stream_block=stream_block, contact_lanes=contact_lanes,
-                  stream_split=stream_split, dense_form=dense_form, scene_kernel=scene_kernel)
+                  stream_split=stream_split, dense_form=dense_form, scene_kernel=scene_kernel,
+                  launch_overlap=launch_overlap)
     if sc.extra.get("scene") is not None:
         p.set("scene", sc.extra["scene"])
         s.set_scenes(sc.extra["scene_params"], sc.extra["walls_per_scene"])
@@ -631,7 +634,8 @@ class Bonds:
             pass
 
 
-def bonded_from_case(case: dict, ctx: Context | None = None, steps_per_launch=0, precision=_lib.DEM_FP64):
+def bonded_from_case(case: dict, ctx: Context | None = None, steps_per_launch=0, precision=_lib.DEM_FP64,
+                     launch_overlap=0):
     """Particles + SolverDEM + Bonds on the device for a scenarios.bonded_bar /
     bdem_two_particles case (bonds set up).  precision DEM_MIXED keeps the bond
     force/moment history in FP32 (strain, geometry and integration stay FP64)."""
@@ -643,7 +647,7 @@ def bonded_from_case(case: dict, ctx: Context | None = None, steps_per_launch=0,
     if case.get("fix_flags") is not None:
         p.set("fix", case["fix_flags"])
     s = SolverDEM(p, None, Force(1.0, 1.0, 0.0, 0.0), case["dt"], skin=0.0, steps_per_launch=steps_per_launch,
-                  precision=precision)
+                  precision=precision, launch_overlap=launch_overlap)
     bp = case["bparams"]
     b = Bonds(s, case["bonds"].max_bonds, quirks=bp["quirks"], beta=bp["beta"], radius_factor=bp["radius_factor"],
               kn=bp["kn"], kt=bp["kt"], break_strain=bp["break_strain"])

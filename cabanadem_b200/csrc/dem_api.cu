@@ -100,6 +100,7 @@ struct dem_solver {
     int scene_table_n = 0;                      // scenes the table holds
     bool scenes_ready = false;                  // the table matches the storage order
     bool scenes_unfit = false;                  // a scene was found not contiguous: per-step form
+    bool no_overlap = false;                    // a step graph with dependent launches failed to build
 };
 
 struct dem_bonds {
@@ -356,6 +357,8 @@ __global__ void k_loop_mid(Ctl *ctl, cudaGraphConditionalHandle h, int n, int de
     cudaGraphSetConditional(h, loop_go(ctl, n, ctl->loop_iter == 0 ? -1 : dense, min_left) ? 1u : 0u);
 }
 __global__ void k_loop_ctl(Ctl *ctl, cudaGraphConditionalHandle h, int n, int dense, int min_left) {
+    grid_dep_wait();   // launched as a dependent (launch_k): the kernel before has completed
+    grid_dep_release();
     if (threadIdx.x != 0) return;
     ++ctl->loop_iter;
     cudaGraphSetConditional(h, loop_go(ctl, n, dense, min_left) ? 1u : 0u);
@@ -983,6 +986,9 @@ int prepare(dem_solver *s) {
     // 1,000 steps) 64.1 us against 68.1 us with one thread per particle; the split forms ran the
     // step in 76.5 us (two kernels) and 78.4 us (two branches)
     fc.split = (s->sp.stream_split >= 1 && s->sp.stream_split <= 4) ? s->sp.stream_split : 4;
+    // each step kernel launched as the dependent of the one before (launch_k), unless asked not
+    // to or a graph with such launches failed to build on this device (s->no_overlap)
+    fc.pdl = (s->sp.launch_overlap != 2 && !s->no_overlap) ? 1 : 0;
     pick_contact_kernel(s);
     fc.scenes = s->nscenes > 0 ? s->d_scenes : nullptr;
     fc.wps = s->nscenes > 0 ? s->wps : 0;
@@ -1241,7 +1247,7 @@ static cudaError_t add_loop(dem_solver *s, cudaGraph_t g, cudaGraphNode_t dep, c
     e = cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return e;
     capture_steps(s, steps, st);
-    k_loop_ctl<<<1, 32, 0, st>>>(s->p->ctl, h, s->p->P.n, dense, steps);
+    launch_k(k_loop_ctl, 1, 32, 0, st, s->fc.pdl != 0, s->p->ctl, h, s->p->P.n, dense, steps);
     return cudaStreamEndCapture(st, &body);
 }
 
@@ -1576,12 +1582,17 @@ extern "C" int dem_solver_run(dem_solver *s, int nsteps) {
     const int chunk = s->sp.steps_per_launch;
     // the graph of the next replay: the step loop (while node), or `chunk` gated steps
     auto ensure_graph = [&]() -> int {
-        if (s->loop) {
-            if (!s->graph || s->graph_version != s->version || s->graph_steps != -1) return capture_loop_graph(s);
-        } else if (!s->graph || s->graph_version != s->version || s->graph_steps != chunk) {
-            return capture_graph(s, chunk);
+        const bool loop_stale = !s->graph || s->graph_version != s->version || s->graph_steps != -1;
+        const bool chunk_stale = !s->graph || s->graph_version != s->version || s->graph_steps != chunk;
+        if (s->loop ? !loop_stale : !chunk_stale) return DEM_OK;
+        int e = s->loop ? capture_loop_graph(s) : capture_graph(s, chunk);
+        if (e != DEM_OK && s->fc.pdl) {   // dependent launches refused in a graph: capture without them
+            (void)cudaGetLastError();
+            s->no_overlap = true;
+            s->fc.pdl = 0;
+            e = s->loop ? capture_loop_graph(s) : capture_graph(s, chunk);
         }
-        return DEM_OK;
+        return e;
     };
     // kernels one replay launched: per iteration of the loop graph, per captured step otherwise
     // (loop graph: every step's kernels, a control kernel per iteration, the two condition nodes)
@@ -1697,6 +1708,7 @@ extern "C" int dem_solver_stats(dem_solver *s, dem_run_stats *out) {
     out->launches = s->launches;
     out->graph_ms = s->graph_ms;
     out->graph_steps = s->graph_steps_run;
+    out->launch_overlap = s->fc.pdl;
     return DEM_OK;
 }
 
@@ -2140,12 +2152,24 @@ extern "C" int dem_bonded_run(dem_bonds *b, int nsteps) {
             cudaGraphExecDestroy(b->graph);
             b->graph = nullptr;
         }
-        cudaGraph_t g = nullptr;
-        CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        for (int k = 0; k < chunk; ++k) launch_bond_step(s->p->P, b->B, s->p->ctl, s->fc, b->bc, st);
-        CK(cudaStreamEndCapture(st, &g));
-        cudaError_t e = cudaGraphInstantiate(&b->graph, g, 0);
-        cudaGraphDestroy(g);
+        auto capture = [&]() -> cudaError_t {
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+            if (e != cudaSuccess) return e;
+            for (int k = 0; k < chunk; ++k) launch_bond_step(s->p->P, b->B, s->p->ctl, s->fc, b->bc, st);
+            e = cudaStreamEndCapture(st, &g);
+            if (e != cudaSuccess) return e;
+            e = cudaGraphInstantiate(&b->graph, g, 0);
+            cudaGraphDestroy(g);
+            return e;
+        };
+        cudaError_t e = capture();
+        if (e != cudaSuccess && s->fc.pdl) {   // dependent launches refused in a graph: without them
+            (void)cudaGetLastError();
+            s->no_overlap = true;
+            s->fc.pdl = 0;
+            e = capture();
+        }
         CK(e);
         b->graph_steps = chunk;
         b->graph_version = s->version;

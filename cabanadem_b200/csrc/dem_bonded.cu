@@ -276,6 +276,8 @@ __device__ __forceinline__ void bond_finish_particle(const Particles &P, const F
 
 template <typename R>
 __global__ void __launch_bounds__(kBondBlock) k_bond_step(Particles P, Bonds B, Ctl *ctl, ForceConsts fc, BondConsts bc) {
+    grid_dep_wait();   // launched as a dependent (launch_k): the kernel before has completed
+    grid_dep_release();
     R *__restrict__ hist = bond_hist<R>(B);
     const CtlSnap cs_ = read_ctl(ctl, true);
     if (!cs_.go) return;
@@ -406,10 +408,11 @@ void launch_bond_setup(const Particles &P, const NbrList &L, const Bonds &B, Ctl
 
 void launch_bond_step(const Particles &P, const Bonds &B, Ctl *ctl, const ForceConsts &fc, const BondConsts &bc,
                       cudaStream_t s) {
+    const int g = (P.n + kBondBlock - 1) / kBondBlock;
     if (B.hist32)
-        k_bond_step<float><<<(P.n + kBondBlock - 1) / kBondBlock, kBondBlock, 0, s>>>(P, B, ctl, fc, bc);
+        launch_k(k_bond_step<float>, g, kBondBlock, 0, s, fc.pdl, P, B, ctl, fc, bc);
     else
-        k_bond_step<double><<<(P.n + kBondBlock - 1) / kBondBlock, kBondBlock, 0, s>>>(P, B, ctl, fc, bc);
+        launch_k(k_bond_step<double>, g, kBondBlock, 0, s, fc.pdl, P, B, ctl, fc, bc);
 }
 
 void launch_bond_force(const Particles &P, const Bonds &B, Ctl *ctl, const BondConsts &bc, double dt, cudaStream_t s) {

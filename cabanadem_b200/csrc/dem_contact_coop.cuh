@@ -368,6 +368,8 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contact_coop(Particles P, NbrL
                                                                const PairConst *__restrict__ pp,
                                                                const PairConst *__restrict__ pw,
                                                                const WallGeom *__restrict__ walls) {
+    grid_dep_wait();   // launched as a dependent (launch_k): the kernel before has completed
+    grid_dep_release();
     constexpr int G = 32 / NL;
     // one row per group, padded by one word so that the groups of a warp fall in different banks
     __shared__ int s_tidx[kBlock / NL][kCoopSlots + 1];

@@ -145,7 +145,40 @@ struct ForceConsts {
                                // 2: the same step as three pair-parallel kernels (dem_pairs.cuh)
     const struct SceneConst *scenes;   // per-scene damping/friction, null: the scalars above
     int wps;                   // walls per scene (> 0 with scenes): scene s owns [s*wps, s*wps+wps)
+    int pdl;                   // 1: the step kernels are launched with programmatic stream
+                               // serialisation (launch_k), each the dependent of the one before
 };
+
+// ---- programmatic dependent launch ---------------------------------------------------
+// A step kernel launched with programmatic stream serialisation may be scheduled while the
+// kernel before it in the stream is still running, so that its launch overlaps that kernel's
+// tail instead of following its completion.  Every kernel launched that way starts with
+// grid_dep_wait(), which returns once the grids it depends on have completed and their memory
+// operations are visible (at once for a kernel launched without the attribute), before it
+// touches any device state; grid_dep_release() then lets the kernel after it be scheduled.
+// A kernel whose blocks have all released (or exited) lets its dependent launch; that
+// dependent's blocks wait in grid_dep_wait, so every grid waits only on grids whose blocks are
+// all resident or done, and the chain always makes progress.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// One launch of `kernel` on stream s; with `overlap`, programmatic stream serialisation
+// against the kernel before it (the kernel must begin with grid_dep_wait).
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_k(void (*kernel)(KArgs...), int grid, int block, size_t smem, cudaStream_t s, bool overlap,
+                            Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = overlap ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
 
 // Per-scene force constants of batched independent scenes.
 struct SceneConst {

@@ -20,6 +20,8 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contact_mixed(Particles P, Nbr
                                                           const PairConst *__restrict__ pp,
                                                           const PairConst *__restrict__ pw,
                                                           const WallGeom *__restrict__ walls) {
+    grid_dep_wait();   // launched as a dependent (launch_k): the kernel before has completed
+    grid_dep_release();
     if (ctl->steps_done >= ctl->target || (ctl->status & kStopBits) || !(ctl->disp < ctl->half_skin))
         return;
     const int nd = ctl->ndefer;
@@ -43,6 +45,8 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contact_mixed_all(Particles P,
                                                               const PairConst *__restrict__ pp,
                                                               const PairConst *__restrict__ pw,
                                                               const WallGeom *__restrict__ walls) {
+    grid_dep_wait();   // launched as a dependent (launch_k): the kernel before has completed
+    grid_dep_release();
     const CtlSnap c = read_ctl(ctl, true);
     if (!c.go) return;
     const int vcur = ctl->vcur;
@@ -79,14 +83,16 @@ __global__ void __launch_bounds__(kBlock) k_force_mixed(Particles P, NbrList L, 
 template <bool MESH>
 static void contact_mixed_t(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
                             const PairConst *pw, const WallGeom *walls, int blocks, cudaStream_t s) {
+    const bool dep = fc.pdl && fc.split != 3;   // not after the concurrent streaming branches' join
     if (fc.coop == 8)
-        k_contact_coop<8, kCoopMinBlocks, true, MESH><<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+        launch_k(k_contact_coop<8, kCoopMinBlocks, true, MESH>, blocks, kBlock, 0, s, dep, P, L, ctl, fc, pp, pw, walls);
     else if (fc.coop == 4)
-        k_contact_coop<4, kCoopMinBlocks, true, MESH><<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+        launch_k(k_contact_coop<4, kCoopMinBlocks, true, MESH>, blocks, kBlock, 0, s, dep, P, L, ctl, fc, pp, pw, walls);
     else if (fc.dense)
-        k_contact_mixed<kContactMixedMinBlocksDense, MESH><<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+        launch_k(k_contact_mixed<kContactMixedMinBlocksDense, MESH>, blocks, kBlock, 0, s, dep, P, L, ctl, fc, pp, pw,
+                 walls);
     else
-        k_contact_mixed<1, MESH><<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+        launch_k(k_contact_mixed<1, MESH>, blocks, kBlock, 0, s, dep, P, L, ctl, fc, pp, pw, walls);
 }
 
 void launch_contact_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
@@ -101,9 +107,11 @@ void launch_contact_mixed_all(const Particles &P, const NbrList &L, Ctl *ctl, co
                               const PairConst *pp, const PairConst *pw, const WallGeom *walls, int blocks, bool mesh,
                               cudaStream_t s) {
     if (mesh)
-        k_contact_mixed_all<kContactMixedMinBlocksDense, true><<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+        launch_k(k_contact_mixed_all<kContactMixedMinBlocksDense, true>, blocks, kBlock, 0, s, fc.pdl, P, L, ctl, fc, pp,
+                 pw, walls);
     else
-        k_contact_mixed_all<kContactMixedMinBlocksDense, false><<<blocks, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+        launch_k(k_contact_mixed_all<kContactMixedMinBlocksDense, false>, blocks, kBlock, 0, s, fc.pdl, P, L, ctl, fc, pp,
+                 pw, walls);
 }
 
 const void *contact_mixed_all_kernel(bool mesh) {
@@ -153,8 +161,8 @@ static void pairs_mixed_t(const Particles &P, const NbrList &L, Ctl *ctl, const 
         last_n = P.n;
     }
     launch_pairs_find<true>(P, L, ctl, fc, walls, sms, s);
-    k_pairs_eval<true><<<g2, kPairsBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
-    k_pairs_sum<true, MESH><<<g3, kPairsBlock, 0, s>>>(P, L, ctl, fc);
+    launch_k(k_pairs_eval<true>, g2, kPairsBlock, 0, s, fc.pdl, P, L, ctl, fc, pp, pw, walls);
+    launch_k(k_pairs_sum<true, MESH>, g3, kPairsBlock, 0, s, fc.pdl, P, L, ctl, fc);
 }
 
 void launch_pairs_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,

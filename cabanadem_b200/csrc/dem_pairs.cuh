@@ -46,6 +46,8 @@ constexpr int kFindBatch = 2;
 template <bool MIXED>
 __global__ void __launch_bounds__(kPairsBlock) k_pairs_find(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
                                                             const WallGeom *__restrict__ walls) {
+    grid_dep_wait();   // launched as a dependent (launch_k): the kernel before has completed
+    grid_dep_release();
     const CtlSnap c = read_ctl(ctl, true);
     if (!c.go) return;
     const int cap = P.cap, n = P.n;
@@ -273,6 +275,8 @@ __global__ void __launch_bounds__(kPairsBlock) k_pairs_eval(Particles P, NbrList
                                                             const PairConst *__restrict__ pp,
                                                             const PairConst *__restrict__ pw,
                                                             const WallGeom *__restrict__ walls) {
+    grid_dep_wait();   // launched as a dependent (launch_k): the kernel before has completed
+    grid_dep_release();
     const CtlSnap c = read_ctl(ctl, true);
     if (!c.go) return;
     const int np = ctl->npairs;
@@ -364,6 +368,8 @@ __device__ __forceinline__ void pairs_integrate(const Particles &P, const ForceC
 
 template <bool MIXED, bool MESH>
 __global__ void __launch_bounds__(kPairsBlock) k_pairs_sum(Particles P, NbrList L, Ctl *ctl, ForceConsts fc) {
+    grid_dep_wait();   // launched as a dependent (launch_k): the kernel before has completed
+    grid_dep_release();
     const CtlSnap c = read_ctl(ctl, true);
     if (!c.go) return;
     const int cap = P.cap, vcur = ctl->vcur;
@@ -442,7 +448,7 @@ inline void launch_pairs_find(const Particles &P, const NbrList &L, Ctl *ctl, co
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pairs_find<MIXED>, kPairsBlock, 0);
     const long need = ((long)P.n + kPairsBlock - 1) / kPairsBlock;
     const long g = need < (long)sms * (per > 0 ? per : 1) ? need : (long)sms * (per > 0 ? per : 1);
-    k_pairs_find<MIXED><<<(int)(g > 0 ? g : 1), kPairsBlock, 0, s>>>(P, L, ctl, fc, walls);
+    launch_k(k_pairs_find<MIXED>, (int)(g > 0 ? g : 1), kPairsBlock, 0, s, fc.pdl, P, L, ctl, fc, walls);
 }
 }  // namespace
 }  // namespace b200dem

@@ -238,6 +238,8 @@ __device__ __forceinline__ bool stream_particle(const Particles &P, const NbrLis
 template <int BS, int MINB>
 __global__ void __launch_bounds__(BS, MINB) k_stream(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
                                                      const WallGeom *__restrict__ walls) {
+    grid_dep_wait();   // launched as a dependent (launch_k): the kernel before has completed
+    grid_dep_release();
     if (!step_gate(ctl)) return;
     const StreamCtl c = stream_ctl(ctl, P.n);
     double vmax2 = 0.0;
@@ -323,6 +325,8 @@ struct BulkTile {
 template <int T, int S>
 __global__ void __launch_bounds__(T, STREAM_BULK_MINB) k_stream_bulk(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
                                                    const WallGeom *__restrict__ walls) {
+    grid_dep_wait();   // launched as a dependent (launch_k): the kernel before has completed
+    grid_dep_release();
     using B = BulkTile<T>;
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint64_t full[S];
@@ -425,6 +429,8 @@ template <int MINB, bool MESH = false>
 __global__ void __launch_bounds__(kBlock, MINB) k_contact(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
                                                     const PairConst *__restrict__ pp, const PairConst *__restrict__ pw,
                                                     const WallGeom *__restrict__ walls) {
+    grid_dep_wait();   // launched as a dependent (launch_k): the kernel before has completed
+    grid_dep_release();
     if (!step_gate(ctl)) return;
     const int nd = ctl->ndefer;
     if ((long)blockIdx.x * blockDim.x >= nd) return;
@@ -449,6 +455,8 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contact_all(Particles P, NbrLi
                                                         const PairConst *__restrict__ pp,
                                                         const PairConst *__restrict__ pw,
                                                         const WallGeom *__restrict__ walls) {
+    grid_dep_wait();   // launched as a dependent (launch_k): the kernel before has completed
+    grid_dep_release();
     const CtlSnap c = read_ctl(ctl, true);
     if (!c.go) return;
     const int vcur = ctl->vcur;
@@ -470,6 +478,8 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contact_all(Particles P, NbrLi
 // step counter, deferred-list reset).  Each block copies ndefer before its ticket, so the
 // reset cannot cut another block's copy short.
 __global__ void __launch_bounds__(kApplyBlock) k_apply(Particles P, NbrList L, Ctl *ctl, ForceConsts fc) {
+    grid_dep_wait();   // launched as a dependent (launch_k): the kernel before has completed
+    grid_dep_release();
     __shared__ int s_nd, s_go, s_last;
     if (threadIdx.x == 0) {
         s_go = step_gate(ctl);
@@ -754,8 +764,8 @@ static void launch_step_t(const Particles &P, const NbrList &L, Ctl *ctl, const 
                 last_np = P.n;
             }
             launch_pairs_find<false>(P, L, ctl, fc, walls, sms, s);
-            k_pairs_eval<false><<<g2, kPairsBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
-            k_pairs_sum<false, MESH><<<g3, kPairsBlock, 0, s>>>(P, L, ctl, fc);
+            launch_k(k_pairs_eval<false>, g2, kPairsBlock, 0, s, fc.pdl, P, L, ctl, fc, pp, pw, walls);
+            launch_k(k_pairs_sum<false, MESH>, g3, kPairsBlock, 0, s, fc.pdl, P, L, ctl, fc);
         }
     } else if (mode == MODE_FUSED && fc.all) {
         static thread_local int ga = 0, gma = 0, last_na = -1;
@@ -767,7 +777,7 @@ static void launch_step_t(const Particles &P, const NbrList &L, Ctl *ctl, const 
         if (fc.mixed)
             launch_contact_mixed_all(P, L, ctl, fc, pp, pw, walls, gma, MESH, s);
         else
-            k_contact_all<kContactMinBlocksDense, MESH><<<ga, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+            launch_k(k_contact_all<kContactMinBlocksDense, MESH>, ga, kBlock, 0, s, fc.pdl, P, L, ctl, fc, pp, pw, walls);
     } else if (mode == MODE_FUSED) {
         static thread_local int gc = 0, gm = 0, gcd = 0, gmd = 0, gk4 = 0, gk8 = 0, gkm4 = 0, gkm8 = 0, last_n = -1;
         if (last_n != P.n) {
@@ -809,26 +819,29 @@ static void launch_step_t(const Particles &P, const NbrList &L, Ctl *ctl, const 
                 k_stream_rest<128, 9><<<grest, 128, 0, s>>>(P, L, ctl, fc, walls);
             }
         } else if (fc.split == 4) {
-            k_stream_bulk<kBulkT, kBulkS><<<bulk_blocks(P.n), kBulkT, kBulkS * BulkTile<kBulkT>::BYTES, s>>>(
-                P, L, ctl, fc, walls);
+            launch_k(k_stream_bulk<kBulkT, kBulkS>, bulk_blocks(P.n), kBulkT, kBulkS * BulkTile<kBulkT>::BYTES, s,
+                     fc.pdl, P, L, ctl, fc, walls);
         } else if (fc.stream_block == 64)
-            k_stream<64, 16><<<(P.n + 63) / 64, 64, 0, s>>>(P, L, ctl, fc, walls);
+            launch_k(k_stream<64, 16>, (P.n + 63) / 64, 64, 0, s, fc.pdl, P, L, ctl, fc, walls);
         else if (fc.stream_block == 256)
-            k_stream<256, 4><<<(P.n + 255) / 256, 256, 0, s>>>(P, L, ctl, fc, walls);
+            launch_k(k_stream<256, 4>, (P.n + 255) / 256, 256, 0, s, fc.pdl, P, L, ctl, fc, walls);
         else
-            k_stream<128, 10><<<(P.n + 127) / 128, 128, 0, s>>>(P, L, ctl, fc, walls);
+            launch_k(k_stream<128, 10>, (P.n + 127) / 128, 128, 0, s, fc.pdl, P, L, ctl, fc, walls);
+        // the contact and apply kernels follow the streaming pass as its dependents, except after
+        // the concurrent form's join (a kernel after two branches)
+        const bool dep = fc.pdl && fc.split != 3;
         if (fc.mixed)
             launch_contact_mixed(P, L, ctl, fc, pp, pw, walls, MESH,
                                  fc.coop == 8 ? gkm8 : fc.coop == 4 ? gkm4 : fc.dense ? gmd : gm, s);
         else if (fc.coop == 8)
-            k_contact_coop<8, kCoopMinBlocks, false, MESH><<<gk8, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+            launch_k(k_contact_coop<8, kCoopMinBlocks, false, MESH>, gk8, kBlock, 0, s, dep, P, L, ctl, fc, pp, pw, walls);
         else if (fc.coop == 4)
-            k_contact_coop<4, kCoopMinBlocks, false, MESH><<<gk4, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+            launch_k(k_contact_coop<4, kCoopMinBlocks, false, MESH>, gk4, kBlock, 0, s, dep, P, L, ctl, fc, pp, pw, walls);
         else if (fc.dense)
-            k_contact<kContactMinBlocksDense, MESH><<<gcd, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
+            launch_k(k_contact<kContactMinBlocksDense, MESH>, gcd, kBlock, 0, s, dep, P, L, ctl, fc, pp, pw, walls);
         else
-            k_contact<1, MESH><<<gc, kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
-        k_apply<<<fc.dense ? 4 * 148 : 148, kApplyBlock, 0, s>>>(P, L, ctl, fc);
+            launch_k(k_contact<1, MESH>, gc, kBlock, 0, s, dep, P, L, ctl, fc, pp, pw, walls);
+        launch_k(k_apply, fc.dense ? 4 * 148 : 148, kApplyBlock, 0, s, fc.pdl, P, L, ctl, fc);
     } else if (fc.mixed) {
         launch_force_mixed(P, L, ctl, fc, pp, pw, walls, MESH, s);
     } else {

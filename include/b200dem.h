@@ -138,6 +138,11 @@ typedef struct dem_solver_params {
                             * every step inside it; with the Verlet-skin mode, static walls, no
                             * mesh, contact_lanes and dense_form 0), 1 = the per-step kernels.
                             * Same results.                                                    */
+    int launch_overlap;    /* 0 = automatic (on), 1 on: each kernel of a step is launched as the
+                            * programmatic dependent of the kernel before it, so that its launch
+                            * overlaps that kernel's tail (it waits for that kernel's completion
+                            * before it touches any state); 2 off: plain stream order.  Same
+                            * results.                                                         */
 } dem_solver_params;
 
 typedef struct dem_run_stats {
@@ -151,6 +156,7 @@ typedef struct dem_run_stats {
     double graph_ms;       /* device time of the step graphs replayed by dem_solver_run (CUDA
                             * events around each replay; host gaps and rebuilds excluded)  */
     long graph_steps;      /* fused steps those replays advanced                          */
+    int launch_overlap;    /* 1: the step kernels are launched as programmatic dependents      */
 } dem_run_stats;
 
 /* ---- context ------------------------------------------------------------------- */

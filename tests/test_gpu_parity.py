@@ -440,3 +440,33 @@ def test_uploads_from_pinned_memory_equal_pageable_ones():
         s.close()
     for f in outs[0]:
         assert np.array_equal(outs[0][f], outs[1][f]), f
+
+
+@pytest.mark.parametrize("form", ["staged", "pairs", "one_kernel", "mixed_coop", "chunked"])
+def test_dependent_launches_equal_plain_stream_order(form):
+    """Every kernel of a step launched as the programmatic dependent of the kernel before it
+    (launch_overlap 0, the default: its launch overlaps that kernel's tail, and it waits for
+    that kernel's completion before it touches any state) against plain stream order
+    (launch_overlap 2): the same trajectory bit for bit through rebuilds, for the three-kernel
+    step with the staged streaming pass, the pair-parallel step, the one-kernel dense step, the
+    mixed-precision cooperative step and graphs of a fixed number of steps; FP64 forms also
+    against the oracle."""
+    from cabanadem_b200._lib import DEM_MIXED
+    sc = S.random_box(n=4133, nsteps=600)
+    c = sc.state.x.mean(axis=0)
+    sc.state.x[:] = c + (sc.state.x - c) * (0.6 if form == "one_kernel" else 0.7)
+    kw = {"staged": dict(contact_lanes=8, stream_split=4), "pairs": dict(dense_form=2), "one_kernel": dict(),
+          "mixed_coop": dict(contact_lanes=8, precision=DEM_MIXED),
+          "chunked": dict(contact_lanes=8, steps_per_launch=16)}[form]
+    a = api.from_scenario(sc, **kw)
+    b = api.from_scenario(sc, launch_overlap=2, **kw)
+    for n in (250, 350):
+        a.run_steps(n)
+        b.run_steps(n)
+    got = a.particles.download()
+    _assert_bitwise(got, b.particles.download(), where="overlap %s" % form)
+    assert a.stats()["rebuilds"] == b.stats()["rebuilds"] >= 1
+    if form != "mixed_coop":
+        ref, _ = _oracle(sc, 600)
+        _assert_bitwise(got, ref, where="overlap %s vs oracle" % form)
+    assert a.stats()["launch_overlap"] == 1 and b.stats()["launch_overlap"] == 0
