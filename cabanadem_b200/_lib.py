@@ -141,6 +141,7 @@ _PROTOS = {
                            C.c_int),
     "dem_nn_mlp_backward": ([_VP, C.POINTER(NnMlp), C.c_long, C.POINTER(NnRows), C.c_int, _VP, _VP, _VP, _VP, _VP,
                              _VP, _VP, _VP], C.c_int),
+    "dem_nn_edge_forward": ([_VP, C.c_long, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, C.c_int], C.c_int),
     "dem_nn_status": ([_VP, C.POINTER(C.c_int)], C.c_int),
     "dem_nn_debug_waits": ([_VP, C.c_int, C.c_int], C.c_int),
     "dem_solver_debug_stream_waits": ([_VP, C.c_int, C.c_int], C.c_int),

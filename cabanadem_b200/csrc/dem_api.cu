@@ -2241,6 +2241,20 @@ extern "C" int dem_nn_mlp_backward(dem_ctx *ctx, const dem_nn_mlp *m, long rows,
     return DEM_OK;
 }
 
+extern "C" int dem_nn_edge_forward(dem_ctx *ctx, long rows, const void *e, const void *pq, const int *recv,
+                                   const int *send, const void *w1e_t, const float *b1, const void *w2t,
+                                   const float *b2, void *out, void *h1, int form) {
+    if (!ctx) return DEM_ERR_INVALID;
+    if (rows < 0 || (rows > 0 && (!e || !pq || !recv || !send || !w1e_t || !b1 || !w2t || !b2 || !out)) ||
+        (form != 0 && form != 1))
+        return fail(ctx, DEM_ERR_INVALID, "dem_nn_edge_forward: bad arguments");
+    int st = nn_prepare(ctx, 0);
+    if (st) return st;
+    st = nn_edge_forward(rows, e, pq, recv, send, w1e_t, b1, w2t, b2, out, h1, ctx->d_err, ctx->stream, form);
+    if (st) return cuda_check(ctx, cudaGetLastError(), "dem_nn_edge_forward");
+    return DEM_OK;
+}
+
 extern "C" int dem_solver_debug_stream_waits(dem_solver *s, int poll_limit, int drop_copies) {
     if (!s || poll_limit < 0) return DEM_ERR_INVALID;
     dem_ctx *ctx = s->ctx;

@@ -330,7 +330,8 @@ int nn_linear_pq_backward(long rows, const void *dpq, const void *w1ij, float *d
 int nn_linear_pq_wgrad(long rows, const void *dpq, const void *h, float *g_w1t, int ld, int col0, float *part,
                        int *err, cudaStream_t s);
 int nn_edge_forward(long rows, const void *e, const void *pq, const int *recv, const int *send, const void *w1e_t,
-                    const float *b1, const void *w2t, const float *b2, void *out, void *h1, int *err, cudaStream_t s);
+                    const float *b1, const void *w2t, const float *b2, void *out, void *h1, int *err, cudaStream_t s,
+                    int form = -1);
 long nn_linear_wgrad_scratch();
 
 // internal access to a solver's device state (dem_api.cu), used by the surrogate

@@ -18,6 +18,7 @@
 // is TMEM lane t of the M = 128 accumulators.  One elected thread issues tcgen05.mma and
 // commits to an mbarrier; every wait is bounded and a timeout raises the context's error
 // word instead of hanging.
+#include <cuda.h>   // CUtensorMap (encoded on the host through the driver entry point)
 #include <cuda_bf16.h>
 #include <cstdint>
 
@@ -171,6 +172,10 @@ __device__ int g_tc_drop_mma = 0;
 __device__ __forceinline__ void mma_issue(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
                                           uint32_t accumulate) {
     if (!g_tc_drop_mma) tc::mma_bf16(tmem_d, adesc, bdesc, idesc, accumulate);
+}
+__device__ __forceinline__ void mma_issue_tmem_a(uint32_t tmem_d, uint32_t tmem_a, uint64_t bdesc, uint32_t idesc,
+                                                 uint32_t accumulate) {
+    if (!g_tc_drop_mma) tc::mma_bf16_tmem_a(tmem_d, tmem_a, bdesc, idesc, accumulate);
 }
 __device__ __forceinline__ void mma_commit_issue(uint64_t *mbar) {
     if (!g_tc_drop_mma) tc::mma_commit(mbar);
@@ -795,6 +800,184 @@ __global__ void __launch_bounds__(kFwdThreads, 2) k_edge_fwd(EdgeArgs a) {
     tc_teardown(tm, 128, ok, a.err, mbar, phase);
 }
 
+// The same layer with its row tiles brought in by the tensor copy engine and the hidden tile
+// kept in tensor memory, so that the next tile's input is in flight during this tile's
+// products and epilogues.  Per CTA (two per SM, 256 threads): the e tile of 128 rows arrives as
+// two 64-feature boxes of a tiled tensor copy in the 128-byte swizzle layout (one elected thread
+// issues them on an mbarrier, one tile ahead: as soon as the first product of the current tile
+// has read the buffer); the first product reads it from shared memory; the epilogue writes the
+// hidden activations as BF16 pairs into tensor memory (tcgen05.st), which is the A operand of
+// the second product; the second epilogue stores each thread's half row straight to global
+// memory.  Same arithmetic, in the same order, as k_edge_fwd.
+constexpr size_t edge_tma_smem() { return 1024 + 3 * (size_t)kRows * kHidden * 2 + 64; }
+
+__global__ void __launch_bounds__(kFwdThreads, 2) k_edge_fwd_tma(const __grid_constant__ CUtensorMap tm_e, EdgeArgs a) {
+    // 1,024-byte alignment by hand: an extern array declared with it would raise the alignment of
+    // every kernel's dynamic shared memory in this file (and their static padding with it)
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    constexpr uint32_t T = (uint32_t)kRows * kHidden * 2;   // one 128 x 128 BF16 tile
+    unsigned char *sE = smem_raw + ((1024u - (tc::smem_u32(smem_raw) & 1023u)) & 1023u);   // 1,024-byte aligned
+    unsigned char *sW1 = sE + T;   // W1e^T 128 x 128 (row tile)
+    unsigned char *sW2 = sW1 + T;  // W2^T 128 x 128 (row tile)
+    uint64_t *bar_mma = reinterpret_cast<uint64_t *>(sW2 + T);
+    uint64_t *bar_e = bar_mma + 1;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(bar_e + 1);
+    __shared__ float s_b1[kHidden], s_b2[kHidden];
+    const int tid = threadIdx.x;
+    const int t = tid & (kRows - 1);   // tile row (TMEM lane)
+    const int half = tid >> 7;         // features [64 half, 64 half + 64)
+    if (half == 0) s_b1[t] = a.b1[t];
+    else s_b2[t] = a.b2[t];
+    stage_dense(sW1, a.w1e_t, kHidden, kHidden, 0, kHidden);
+    stage_dense(sW2, a.w2t, kHidden, kHidden, 0, kHidden);
+    cp_wait_all();
+    if (tid == 0) {
+        tc::mbar_init(bar_mma, 1);
+        tc::mbar_init(bar_e, 1);
+        tc::mbar_init_fence();
+    }
+    if (tid < 32) {
+        tc::tmem_alloc(tslot, 256);
+        tc::tmem_relinquish();
+    }
+    tc::fence_async_smem();   // the weight tiles, complete, visible to the tensor core
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tm = *tslot;
+    const uint32_t tacc = tm;         // accumulator, 128 columns (both products)
+    const uint32_t ta = tm + 128;     // hidden tile as the second product's A operand, 64 columns
+    const uint32_t aE = tc::smem_u32(sE), aW1 = tc::smem_u32(sW1), aW2 = tc::smem_u32(sW2);
+    constexpr uint32_t id = tc::idesc_bf16(kRows, kHidden, false, false);
+    const long ntiles = (a.rows + kRows - 1) / kRows;
+    auto issue_e = [&](long tile) {   // thread 0: the tile's two feature boxes
+        tc::mbar_arrive_expect(bar_e, T);
+        tc::tma_load_2d(sE, &tm_e, 0, (int)(tile * kRows), bar_e);
+        tc::tma_load_2d(sE + T / 2, &tm_e, 64, (int)(tile * kRows), bar_e);
+    };
+    uint32_t ph_mma = 0, ph_e = 0;
+    bool ok = true, e_pending = false;   // e_pending: thread 0 has a tile copy not yet waited for
+    if (tid == 0 && (long)blockIdx.x < ntiles) {
+        issue_e(blockIdx.x);
+        e_pending = true;
+    }
+    for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const long row0 = tile * kRows, grow = row0 + t;
+        const bool live = grow < a.rows;
+        uint4 p[8], q[8];
+        {
+            const long r = live ? a.recv[grow] : 0, c = live ? a.send[grow] : 0;
+            const uint4 *ps = reinterpret_cast<const uint4 *>(a.pq + r * 2 * kHidden + half * 64);
+            const uint4 *qs = reinterpret_cast<const uint4 *>(a.pq + c * 2 * kHidden + kHidden + half * 64);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                p[k] = ps[k];
+                q[k] = qs[k];
+            }
+        }
+        // the e tile; the block barrier also orders every thread's reads of the previous tile's
+        // accumulator before this tile's first product
+        const bool e_ok = tc::mbar_wait(bar_e, ph_e, g_tc_wait_limit);
+        if (!__syncthreads_and(e_ok)) {
+            ok = false;
+            break;
+        }
+        ph_e ^= 1u;
+        if (tid == 0) {
+            e_pending = false;
+            tc::fence_after_sync();
+            for (int ks = 0; ks < kHidden / 16; ++ks)
+                mma_issue(tacc, tc::sdesc_sw128(aE + (uint32_t)(ks >> 2) * (T / 2) + (uint32_t)(ks & 3) * 32u),
+                          tc::kmajor_desc(aW1, kHidden, ks), id, ks > 0);
+            mma_commit_issue(bar_mma);
+        }
+        ok = mma_wait(bar_mma, ph_mma);
+        if (!ok) break;
+        // the first product has read the e tile: the next tile's copy goes into its buffer
+        if (tid == 0 && tile + gridDim.x < ntiles) {
+            issue_e(tile + gridDim.x);
+            e_pending = true;
+        }
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {   // two batches of 32 columns keep the P/Q registers live
+            float w[32];
+            acc32(tacc, half * 64 + b * 32, w);
+            uint32_t hw[16];
+#pragma unroll
+            for (int c2 = 0; c2 < 2; ++c2) {
+                const int cc = 2 * b + c2;
+                const int c = half * 4 + cc;   // 16-feature group
+                float *v = w + 16 * c2, pf[8], qf[8];
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    tc::unpack8(p[2 * cc + h], pf);
+                    tc::unpack8(q[2 * cc + h], qf);
+                    for (int k = 0; k < 8; ++k)
+                        v[8 * h + k] = fmaxf(v[8 * h + k] + s_b1[c * 16 + 8 * h + k] + pf[k] + qf[k], 0.f);
+                }
+                const uint4 lo = tc::pack8(v), hi = tc::pack8(v + 8);
+                hw[8 * c2 + 0] = lo.x;
+                hw[8 * c2 + 1] = lo.y;
+                hw[8 * c2 + 2] = lo.z;
+                hw[8 * c2 + 3] = lo.w;
+                hw[8 * c2 + 4] = hi.x;
+                hw[8 * c2 + 5] = hi.y;
+                hw[8 * c2 + 6] = hi.z;
+                hw[8 * c2 + 7] = hi.w;
+                if (a.h1 && live) {
+                    uint4 *dst = reinterpret_cast<uint4 *>(a.h1 + grow * kHidden + c * 16);
+                    dst[0] = lo;
+                    dst[1] = hi;
+                }
+            }
+            // features [64 half + 32 b, + 32) as 16 columns of BF16 pairs
+            tc::tmem_st16(tc::tmem_warp_addr(ta, half * 32 + b * 16), hw);
+        }
+        tc::tmem_wait_st();
+        tc::fence_before_sync();
+        __syncthreads();
+        if (tid == 0) {
+            tc::fence_after_sync();
+            for (int ks = 0; ks < kHidden / 16; ++ks)
+                mma_issue_tmem_a(tacc, ta + (uint32_t)ks * 8u, tc::kmajor_desc(aW2, kHidden, ks), id, ks > 0);
+            mma_commit_issue(bar_mma);
+        }
+        {   // residual half row while the second product runs
+            const uint4 *es = reinterpret_cast<const uint4 *>(a.e + (live ? grow : 0) * kHidden + half * 64);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) p[k] = es[k];
+        }
+        ok = mma_wait(bar_mma, ph_mma);
+        if (!ok) break;
+        {
+            float w[64];
+            acc64(tacc, half * 64, w);
+            uint4 o[8];
+#pragma unroll
+            for (int cc = 0; cc < 4; ++cc) {
+                const int c = half * 4 + cc;
+                float *v = w + 16 * cc, r[8];
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    tc::unpack8(p[2 * cc + h], r);
+                    for (int k = 0; k < 8; ++k) v[8 * h + k] += s_b2[c * 16 + 8 * h + k] + r[k];
+                }
+                o[2 * cc] = tc::pack8(v);
+                o[2 * cc + 1] = tc::pack8(v + 8);
+            }
+            if (live) {
+                uint4 *dst = reinterpret_cast<uint4 *>(a.out + grow * kHidden + half * 64);
+#pragma unroll
+                for (int k = 0; k < 8; ++k) dst[k] = o[k];
+            }
+        }
+        tc::fence_before_sync();
+    }
+    // a wait gave up with a tile copy in flight: let it land before the block's memory goes
+    if (tid == 0 && e_pending) (void)tc::mbar_wait(bar_e, ph_e, g_tc_wait_limit);
+    tc_teardown(tm, 256, ok, a.err, bar_mma, ph_mma);
+}
+
 // dW^T [256][128] partials: D_half[o][k] = sum_rows A[row][128 half + o] B[row][k]
 struct LinWgradArgs {
     long rows;
@@ -977,10 +1160,63 @@ int nn_linear_pq_wgrad(long rows, const void *dpq, const void *h, float *g_w1t, 
     return cudaGetLastError() == cudaSuccess ? DEM_OK : DEM_ERR_CUDA;
 }
 
+namespace {
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against the driver
+// library); null when the driver does not provide it.
+using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                 const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiled encode_tiled() {
+    static EncodeTiled fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return (EncodeTiled) nullptr;
+        return reinterpret_cast<EncodeTiled>(p);
+    }();
+    return fn;
+}
+
+// Tensor map of e [rows][128] BF16 with 64 x 128 boxes in the 128-byte swizzle layout.
+bool edge_map(CUtensorMap *m, const void *e, long rows) {
+    const EncodeTiled enc = encode_tiled();
+    if (!enc || (reinterpret_cast<uintptr_t>(e) & 15u) || rows <= 0 || rows > 0x7FFFFFFFL - kRows) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)kHidden, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)kHidden * 2};
+    const cuuint32_t box[2] = {64u, (cuuint32_t)kRows};
+    const cuuint32_t elem[2] = {1u, 1u};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(e), dims, strides, box, elem,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+}  // namespace
+
+// form 0: the tensor-copy kernel (k_edge_fwd_tma) where the tensor map can be made, else the
+// staged kernel; form 1: the staged kernel (k_edge_fwd); -1: the build's default
+// (EDGE_FORM_DEFAULT).  Same results.
+#ifndef EDGE_FORM_DEFAULT
+#define EDGE_FORM_DEFAULT 0
+#endif
 int nn_edge_forward(long rows, const void *e, const void *pq, const int *recv, const int *send, const void *w1e_t,
-                    const float *b1, const void *w2t, const float *b2, void *out, void *h1, int *err, cudaStream_t s) {
+                    const float *b1, const void *w2t, const float *b2, void *out, void *h1, int *err, cudaStream_t s,
+                    int form) {
     EdgeArgs a{rows, (const bf16 *)e, (const bf16 *)pq, recv, send, (const bf16 *)w1e_t, b1, (const bf16 *)w2t, b2,
                (bf16 *)out, (bf16 *)h1, err};
+    if (rows <= 0) return DEM_OK;
+    if (form < 0) form = EDGE_FORM_DEFAULT;
+    CUtensorMap m;
+    if (form == 0 && edge_map(&m, e, rows)) {
+        const size_t smem = edge_tma_smem();
+        if (cudaFuncSetAttribute(k_edge_fwd_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            return DEM_ERR_CUDA;
+        int sms = 148, dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const long ntiles = (rows + kRows - 1) / kRows, cap = 2L * (sms > 0 ? sms : 148);   // two CTAs per SM
+        k_edge_fwd_tma<<<(int)(ntiles < cap ? ntiles : cap), kFwdThreads, smem, s>>>(m, a);
+        return cudaGetLastError() == cudaSuccess ? DEM_OK : DEM_ERR_CUDA;
+    }
     return launch_tc(k_edge_fwd, edge_smem(), 128, rows, a, s, 0, kFwdThreads);
 }
 

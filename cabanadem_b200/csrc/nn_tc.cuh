@@ -52,6 +52,23 @@ __device__ __forceinline__ uint64_t mnmajor_desc(uint32_t base, int R, int kstep
     return sdesc(base + (uint32_t)(kstep * 256), 128u, (uint32_t)(R * 16));
 }
 
+// Descriptor of a K-major operand block in the 128-byte swizzle layout that a tiled tensor copy
+// with CU_TENSOR_MAP_SWIZZLE_128B writes: rows of 128 bytes (64 BF16 features), the 16-byte
+// chunks of row r at chunk position c ^ (r % 8), 8-row groups 1,024 bytes apart (SBO); the block
+// starts on a 1,024-byte boundary.  Layout type [61,64) = 2 (128-byte swizzle); the leading byte
+// offset is not used by this layout (16 bytes).  The K step s (16 features, 32 bytes) inside the
+// 128-byte row starts at + 32 s: the swizzle is applied to the address bits, so the same rows
+// are read.
+__device__ __forceinline__ uint64_t sdesc_sw128(uint32_t addr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+    d |= (uint64_t)1 << 16;
+    d |= (uint64_t)(1024u >> 4) << 32;
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)2 << 61;
+    return d;
+}
+
 // ---- TMEM allocation (one full warp; power-of-two column count >= 32) ----
 __device__ __forceinline__ void tmem_alloc(uint32_t *smem_dst, int ncols) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(smem_dst)),
@@ -75,6 +92,20 @@ __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t"
         "}\n" ::"r"(tmem_d),
         "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(m0), "r"(m1), "r"(m2), "r"(m3));
+}
+
+// The same with A in tensor memory (rows = TMEM lanes, two BF16 features per 32-bit column,
+// the lower-indexed feature in the low half).
+__device__ __forceinline__ void mma_bf16_tmem_a(uint32_t tmem_d, uint32_t tmem_a, uint64_t bdesc, uint32_t idesc,
+                                                uint32_t accumulate) {
+    const uint32_t m0 = 0, m1 = 0, m2 = 0, m3 = 0;
+    asm volatile(
+        "{\n\t"
+        ".reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t"
+        "}\n" ::"r"(tmem_d),
+        "r"(tmem_a), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(m0), "r"(m1), "r"(m2), "r"(m3));
 }
 
 // Arrive once on the mbarrier when every MMA issued so far by this thread has completed.
@@ -139,6 +170,37 @@ __device__ __forceinline__ void tmem_ld32_nowait(uint32_t taddr, uint32_t r[32])
           "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
           "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
         : "r"(taddr));
+}
+
+// Registers -> this warp's 32 lanes, 16 consecutive 32-bit columns; tmem_wait_st before the
+// values are read by an MMA (then the tcgen05 fences around the thread barrier).
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t r[16]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
+        "{%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16};" ::"r"(taddr),
+        "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]),
+        "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
+        : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// ---- tiled tensor copies (TMA), global -> shared, completing on an mbarrier ----
+__device__ __forceinline__ void mbar_init_fence() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect(uint64_t *mbar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mbar)), "r"(bytes)
+                 : "memory");
+}
+// Box at element coordinates (x, y) of a 2-D tensor map (a kernel parameter) into dst; x times
+// the element size is a multiple of 16 bytes.  No multicast.
+__device__ __forceinline__ void tma_load_2d(void *dst, const void *tmap, int x, int y, uint64_t *mbar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+            "r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(smem_u32(mbar))
+        : "memory");
 }
 
 // TMEM address of (lane = 32 * (warp % 4), column col) for this warp's quarter.

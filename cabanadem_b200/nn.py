@@ -77,3 +77,14 @@ def status(ctx) -> int:
     v = C.c_int(0)
     check(lib().dem_nn_status(ctx.h, C.byref(v)), ctx.h, "dem_nn_status")
     return v.value
+
+
+def edge_forward(ctx, e, pq, recv, send, w1e_t, b1, w2t, b2, out, h1=None, form: int = 0):
+    """The factorised message layer (``dem_nn_edge_forward``): out = e + b2 + W2 relu(W1e e + b1
+    + P[recv] + Q[send]), PQ = [W1i h | W1j h] per node.  Tensors on the context's device: e, out
+    bf16 [rows][128], pq bf16 [nodes][256], recv/send int32 [rows], w1e_t/w2t bf16 [128][128],
+    b1/b2 float32 [128], h1 bf16 [rows][128] or None.  form 0: tensor-copy tiles and the hidden
+    tile in tensor memory; 1: per-thread staged copies (same results)."""
+    st = lib().dem_nn_edge_forward(ctx.h, int(e.shape[0]), _ptr(e), _ptr(pq), _ptr(recv), _ptr(send), _ptr(w1e_t),
+                                   _ptr(b1), _ptr(w2t), _ptr(b2), _ptr(out), _ptr(h1), int(form))
+    check(st, ctx.h, "dem_nn_edge_forward")

@@ -408,6 +408,17 @@ int dem_nn_mlp_forward(dem_ctx *ctx, const dem_nn_mlp *m, long rows, const dem_n
 int dem_nn_mlp_backward(dem_ctx *ctx, const dem_nn_mlp *m, long rows, const dem_nn_rows *src, int nsrc,
                         const void *dy, const void *h1, void *dz1, float *dx, float *g_w1t, float *g_b1,
                         float *g_w2t, float *g_b2);
+/* The message (edge) layer in its factorised form: out = e + b2 + W2 relu(W1e e + b1 + P[recv]
+ * + Q[send]) with PQ = [W1i h | W1j h] per node (bf16 [nodes][256]), e and out bf16
+ * [rows][128], recv/send int [rows], w1e_t and w2t bf16 [128][128] (out x in), h1 (bf16
+ * [rows][128], null: not written) the hidden activations.  form 0: the tile copies of e by the
+ * tensor copy engine, one tile ahead, and the hidden tile in tensor memory (falls back to form
+ * 1 when the driver cannot encode the tensor map); form 1: e staged by per-thread asynchronous
+ * copies, the hidden tile in shared memory.  Same results.  Device pointers, the context's
+ * stream (no reference counterpart). */
+int dem_nn_edge_forward(dem_ctx *ctx, long rows, const void *e, const void *pq, const int *recv, const int *send,
+                        const void *w1e_t, const float *b1, const void *w2t, const float *b2, void *out, void *h1,
+                        int form);
 /* Device error word of the context's tensor-core kernels (DEM_ERR_TIMEOUT when a bounded
  * wait gave up); synchronises, returns it in *status and clears it. */
 int dem_nn_status(dem_ctx *ctx, int *status);

@@ -156,3 +156,84 @@ def test_wait_that_runs_out_is_reported_and_the_next_call_succeeds():
         ref = h @ m.w2t_bf.float().t() + m.b2
         assert (out32 - ref).abs().max().item() <= 1e-2 * ref.abs().max().item()
     ctx.close()
+
+
+def _edge_case(rows, gen, dev):
+    bf = dict(device=dev, dtype=torch.bfloat16)
+    nodes = max(rows // 3, 7)
+    e = torch.randn(rows, 128, generator=gen).to(**bf)
+    pq = (torch.randn(nodes, 256, generator=gen) * 0.5).to(**bf)
+    recv = torch.randint(0, nodes, (rows,), generator=gen, dtype=torch.int32).to(dev)
+    send = torch.randint(0, nodes, (rows,), generator=gen, dtype=torch.int32).to(dev)
+    w1e_t = (torch.randn(128, 128, generator=gen) / 128 ** 0.5).to(**bf)
+    w2t = (torch.randn(128, 128, generator=gen) / 128 ** 0.5).to(**bf)
+    b1 = (torch.randn(128, generator=gen) * 0.1).to(dev)
+    b2 = (torch.randn(128, generator=gen) * 0.1).to(dev)
+    return e, pq, recv, send, w1e_t, b1, w2t, b2
+
+
+@pytest.mark.parametrize("rows", [37, 1000, 2 * 148 * 128 + 200, 1_200_017])
+def test_edge_layer_forms_match_torch_fp32(rows):
+    """The factorised message layer, out = e + b2 + W2 relu(W1e e + b1 + P[recv] + Q[send]):
+    the form whose e tiles come by tiled tensor copies (128-byte swizzle, one tile ahead) with
+    the hidden tile in tensor memory as the second product's A operand, and the form staged by
+    per-thread copies with the hidden tile in shared memory -- the same bits (outputs and hidden
+    activations), and both equal to a PyTorch FP32 reference of the same operation on the same
+    BF16 operands (hidden rounded to BF16 as in the kernels).  Row counts: a partial single tile,
+    several tiles, more tiles than CTAs with a ragged last tile, and the 200k dam break's edge
+    count."""
+    dev = torch.device("cuda:0")
+    ctx = api.Context(0)
+    gen = torch.Generator().manual_seed(rows)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr())
+    with torch.cuda.stream(stream):
+        e, pq, recv, send, w1e_t, b1, w2t, b2 = _edge_case(rows, gen, dev)
+        outs = []
+        for form in (0, 1):
+            out = torch.full((rows, 128), 3.0, device=dev, dtype=torch.bfloat16)
+            h1 = torch.full((rows, 128), 3.0, device=dev, dtype=torch.bfloat16)
+            nn.edge_forward(ctx, e, pq, recv, send, w1e_t, b1, w2t, b2, out, h1, form=form)
+            outs.append((out, h1))
+        assert nn.status(ctx) == 0
+        assert torch.equal(outs[0][0], outs[1][0]) and torch.equal(outs[0][1], outs[1][1])
+        ef, pqf = e.float(), pq.float()
+        z = ef @ w1e_t.float().t() + b1 + pqf[recv.long(), :128] + pqf[send.long(), 128:]
+        h = torch.relu(z).to(torch.bfloat16).float()
+        ref = h @ w2t.float().t() + b2 + ef
+        got = outs[0][0].float()
+        assert (got - ref).abs().max().item() <= 2e-2 * ref.abs().max().item()
+        # hidden activations: equal up to a BF16 rounding of values on a rounding edge
+        dh = (outs[0][1].float() - h).abs()
+        assert dh.max().item() <= 2e-2 * h.abs().max().item()
+        assert (dh > 0).float().mean().item() < 1e-3
+    ctx.close()
+
+
+def test_edge_layer_wait_that_runs_out_is_reported():
+    """The tensor-copy form with dem_nn_debug_waits(drop_mma=1): the tile copies arrive, no MMA
+    is issued, each block's wait on the product gives up; the call reports DEM_ERR_TIMEOUT and
+    writes nothing, and with the default bounds restored the same call gives the staged form's
+    bits."""
+    from cabanadem_b200 import _lib
+    dev = torch.device("cuda:0")
+    ctx = api.Context(0)
+    gen = torch.Generator().manual_seed(5)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr())
+    rows = 148 * 2 * 128 + 99
+    L = _lib.lib()
+    with torch.cuda.stream(stream):
+        args = _edge_case(rows, gen, dev)
+        out = torch.full((rows, 128), 7.0, device=dev, dtype=torch.bfloat16)
+        assert L.dem_nn_debug_waits(ctx.h, 1000, 1) == 0
+        try:
+            nn.edge_forward(ctx, *args, out, None, form=0)
+            assert nn.status(ctx) == 0x020           # DEM_ERR_TIMEOUT
+            assert bool((out.float() == 7.0).all())
+        finally:
+            assert L.dem_nn_debug_waits(ctx.h, 0, 0) == 0
+        ref = torch.empty_like(out)
+        nn.edge_forward(ctx, *args, out, None, form=0)
+        nn.edge_forward(ctx, *args, ref, None, form=1)
+        assert nn.status(ctx) == 0
+        assert torch.equal(out, ref)
+    ctx.close()
