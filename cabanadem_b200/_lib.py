@@ -38,7 +38,7 @@ class SolverParams(C.Structure):
                 ("precision", C.c_int), ("gravity", C.c_double * 3), ("max_neighbors", C.c_int),
                 ("steps_per_launch", C.c_int), ("stream_block", C.c_int), ("contact_lanes", C.c_int),
                 ("stream_split", C.c_int), ("dense_form", C.c_int), ("scene_kernel", C.c_int),
-                ("launch_overlap", C.c_int)]
+                ("launch_overlap", C.c_int), ("cooperative_loop", C.c_int)]
 
 
 class SceneParams(C.Structure):
@@ -58,7 +58,7 @@ class RunStats(C.Structure):
     _fields_ = [("steps", C.c_long), ("rebuilds", C.c_long), ("max_neighbors", C.c_int),
                 ("neighbor_capacity", C.c_int), ("status", C.c_int), ("disp_bound", C.c_double),
                 ("launches", C.c_long), ("graph_ms", C.c_double), ("graph_steps", C.c_long),
-                ("launch_overlap", C.c_int)]
+                ("launch_overlap", C.c_int), ("cooperative_loop", C.c_int)]
 
 
 class NnRows(C.Structure):

@@ -312,7 +312,7 @@ class SolverDEM:
                  precision: int = _lib.DEM_FP64, num_steps: int = 0, output_frequency: int = 0,
                  max_neighbors: int = 0, steps_per_launch: int = 0, stream_block: int = 0,
                  contact_lanes: int = 0, stream_split: int = 0, dense_form: int = 0, scene_kernel: int = 0,
-                 launch_overlap: int = 0):
+                 launch_overlap: int = 0, cooperative_loop: int = 0):
         self.particles, self.wall, self.force = particles, wall, force
         self.dt, self.num_steps, self.output_frequency = float(dt), int(num_steps), int(output_frequency)
         sp = _lib.SolverParams()
@@ -328,6 +328,7 @@ class SolverDEM:
         sp.dense_form = int(dense_form)
         sp.scene_kernel = int(scene_kernel)
         sp.launch_overlap = int(launch_overlap)
+        sp.cooperative_loop = int(cooperative_loop)
         fp = force.params()
         h = C.c_void_p()
         check(lib().dem_solver_create(particles.ctx.h, particles.h, wall.h if wall else None, C.byref(fp),
@@ -461,7 +462,7 @@ def createSolverDEM(inputs: Inputs, particles: Particles, wall: Wall, force: For
 
 def from_scenario(sc, ctx: Context | None = None, rebuild_every_step=False, precision=_lib.DEM_FP64,
                   steps_per_launch=0, max_neighbors=0, stream_block=0, contact_lanes=0, stream_split=0,
-                  dense_form=0, scene_kernel=0, launch_overlap=0):
+                  dense_form=0, scene_kernel=0, launch_overlap=0, cooperative_loop=0):
     """Particles + Wall + SolverDEM on the device for a scenarios.Scenario."""
     st = sc.state
     nwalls = sc.walls.n if sc.walls is not None else 0
@@ -479,7 +480,7 @@ def from_scenario(sc, ctx: Context | None = None, rebuild_every_step=False, prec
                   gravity=sc.gravity, precision=precision, steps_per_launch=steps_per_launch,
                   max_neighbors=max_neighbors, stream_block=stream_block, contact_lanes=contact_lanes,
                   stream_split=stream_split, dense_form=dense_form, scene_kernel=scene_kernel,
-                  launch_overlap=launch_overlap)
+                  launch_overlap=launch_overlap, cooperative_loop=cooperative_loop)
     if sc.extra.get("scene") is not None:
         p.set("scene", sc.extra["scene"])
         s.set_scenes(sc.extra["scene_params"], sc.extra["walls_per_scene"])

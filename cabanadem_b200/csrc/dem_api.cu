@@ -101,6 +101,8 @@ struct dem_solver {
     bool scenes_ready = false;                  // the table matches the storage order
     bool scenes_unfit = false;                  // a scene was found not contiguous: per-step form
     bool no_overlap = false;                    // a step graph with dependent launches failed to build
+    bool coop_refused = false;                  // a cooperative launch of the step loop was refused
+    bool coop_ran = false;                      // the last run's steps ran in cooperative launches
 };
 
 struct dem_bonds {
@@ -1553,6 +1555,14 @@ int run_scenes(dem_solver *s, int nsteps) {
 }
 }  // namespace
 
+// The run's steps in cooperative launches (dem_persist.cuh) rather than graph replays: the
+// one-kernel step of a small system in the Verlet-skin mode, with the step loop in while-loop
+// graphs (steps_per_launch 0, so no profiler asked for fixed graphs).
+bool coop_loop(const dem_solver *s) {
+    return s->sp.cooperative_loop != 2 && !s->coop_refused && s->fc.all == 1 && s->p->P.n <= kCoopMaxN &&
+           s->loop && !ref_mode(s);
+}
+
 extern "C" int dem_solver_run(dem_solver *s, int nsteps) {
     if (!s) return DEM_ERR_INVALID;
     if (nsteps <= 0) return DEM_OK;
@@ -1644,7 +1654,39 @@ extern "C" int dem_solver_run(dem_solver *s, int nsteps) {
             CK(cudaEventCreate(&s->ev0));
             CK(cudaEventCreate(&s->ev1));
         }
+        s->coop_ran = false;
         for (int guard = 0;; ++guard) {
+            if (coop_loop(s)) {   // every step until the target or a stale list in one launch
+                CK(cudaEventRecord(s->ev0, st));
+                const cudaError_t le = launch_steps_coop(s->p->P, s->L, s->p->ctl, s->fc, s->d_pp, s->d_pw, s->d_walls,
+                                                         nsteps, st);
+                if (le != cudaSuccess) {   // not resident at once (or refused): graph replays from here on
+                    (void)cudaGetLastError();
+                    s->coop_refused = true;
+                    continue;
+                }
+                CK(cudaEventRecord(s->ev1, st));
+                s->coop_ran = true;
+                s->launches += 1;
+                const int done_before = s->graph_done_mark;
+                Ctl c = read_ctl(s);
+                CK(cudaGetLastError());
+                if (c.status & DEM_ERR_TIMEOUT) return fail(ctx, DEM_ERR_TIMEOUT, "a bounded device wait gave up");
+                float ms = 0.f;
+                CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+                s->graph_ms += ms;
+                s->graph_steps_run += c.steps_done - done_before;
+                s->graph_done_mark = c.steps_done;
+                if (c.steps_done >= c.target) break;
+                if (!(c.disp < c.half_skin)) {
+                    int e = build_now(s, true);
+                    if (e) return e;
+                } else if (c.steps_done == done_before) {
+                    return fail(ctx, DEM_ERR_CUDA, "solver made no progress");
+                }
+                if (guard > 4 * (nsteps + 4)) return fail(ctx, DEM_ERR_CUDA, "solver made no progress");
+                continue;
+            }
             {
                 int e = ensure_graph();
                 if (e) return e;
@@ -1709,6 +1751,7 @@ extern "C" int dem_solver_stats(dem_solver *s, dem_run_stats *out) {
     out->graph_ms = s->graph_ms;
     out->graph_steps = s->graph_steps_run;
     out->launch_overlap = s->fc.pdl;
+    out->cooperative_loop = s->coop_ran ? 1 : 0;
     return DEM_OK;
 }
 

@@ -48,6 +48,7 @@ struct Ctl {
     int npairs;               // contact work items of the current step (pair-parallel dense step)
     int loop_iter;            // iterations of the step loop in the current graph replay
     long long wfar_build;     // value of `rebuilds` when NbrList::wfar was last computed
+    unsigned gen;             // step generation of the cooperative step loop (dem_persist.cuh)
 };
 
 struct Particles {
@@ -315,6 +316,15 @@ void launch_scene_steps_mixed(const Particles &P, const NbrList &L, Ctl *ctl, co
                               const PairConst *pp, const PairConst *pw, const WallGeom *walls, const int2 *table,
                               int nscenes, int nsteps, double delta, double skin, cudaStream_t s);
 constexpr int kSceneMaxParticles = 64;   // largest scene of the persistent form
+// The one-kernel step's run in one cooperative launch (dem_persist.cuh): at most `max_steps`
+// steps, ending at the target, a stale list or a stop bit.  An error when the launch is refused
+// (e.g. the grid cannot be resident at once).
+constexpr int kCoopMaxN = 32768;   // largest system the cooperative step loop takes
+cudaError_t launch_steps_coop(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
+                              const PairConst *pw, const WallGeom *walls, int max_steps, cudaStream_t s);
+cudaError_t launch_steps_coop_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc,
+                                    const PairConst *pp, const PairConst *pw, const WallGeom *walls, int max_steps,
+                                    cudaStream_t s);
 
 // dense layers of the surrogate (dem_nn.cu)
 int nn_mlp_forward(const dem_nn_mlp &m, long rows, const dem_nn_rows *src, int nsrc, const void *resid, void *out,

@@ -9,6 +9,7 @@
 #include "dem_particle.cuh"
 #include "dem_contact_coop.cuh"
 #include "dem_pairs.cuh"
+#include "dem_persist.cuh"
 #include "dem_scenes.cuh"
 
 namespace b200dem {
@@ -175,6 +176,36 @@ void launch_pairs_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const Fo
 
 const void *contact_mixed_kernel(int dense, int coop, bool mesh) {
     return mesh ? contact_mixed_kernel_t<true>(dense, coop) : contact_mixed_kernel_t<false>(dense, coop);
+}
+
+// Cooperative launch of the step loop (dem_persist.cuh): a grid-stride grid of at most the
+// blocks the SMs hold at once.
+template <bool MIXED, bool MESH>
+static cudaError_t steps_coop_t(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc,
+                                const PairConst *pp, const PairConst *pw, const WallGeom *walls, int max_steps,
+                                cudaStream_t s) {
+    static thread_local int fit = 0;   // resident blocks of this instantiation, per host thread
+    if (!fit) {
+        int dev = 0, sms = 0, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_steps_coop<MIXED, MESH>, kBlock, 0);
+        fit = (sms > 0 ? sms : 148) * (per > 0 ? per : 1);
+    }
+    const int need = (P.n + kBlock - 1) / kBlock;
+    const int grid = need < fit ? (need > 0 ? need : 1) : fit;
+    Particles p = P;
+    NbrList l = L;
+    ForceConsts f = fc;
+    void *args[] = {&p, &l, &ctl, &f, (void *)&pp, (void *)&pw, (void *)&walls, &max_steps};
+    return cudaLaunchCooperativeKernel((const void *)k_steps_coop<MIXED, MESH>, dim3(grid), dim3(kBlock), args, 0, s);
+}
+
+cudaError_t launch_steps_coop_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc,
+                                    const PairConst *pp, const PairConst *pw, const WallGeom *walls, int max_steps,
+                                    cudaStream_t s) {
+    return fc.mesh.nt ? steps_coop_t<true, true>(P, L, ctl, fc, pp, pw, walls, max_steps, s)
+                      : steps_coop_t<true, false>(P, L, ctl, fc, pp, pw, walls, max_steps, s);
 }
 
 void launch_scene_steps_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc,

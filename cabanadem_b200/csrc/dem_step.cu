@@ -19,6 +19,7 @@
 #include "dem_bulk.cuh"
 #include "dem_contact_coop.cuh"
 #include "dem_pairs.cuh"
+#include "dem_persist.cuh"
 #include "dem_scenes.cuh"
 
 namespace b200dem {
@@ -476,7 +477,10 @@ __global__ void __launch_bounds__(kBlock, MINB) k_contact_all(Particles P, NbrLi
 // Fused step, kernel 3 of 3: commit the deferred particles' u and omega, then the last
 // block to take a ticket finalises the step (displacement bound, position-buffer flip,
 // step counter, deferred-list reset).  Each block copies ndefer before its ticket, so the
-// reset cannot cut another block's copy short.
+// reset cannot cut another block's copy short.  With at most kApplyOneBlock deferred particles
+// (a sparse step: tens on the 2M lattice) block 0 alone commits and finalises, and the other
+// blocks leave at once: no ticket chain on the step's path.
+constexpr int kApplyOneBlock = 8 * kApplyBlock;
 __global__ void __launch_bounds__(kApplyBlock) k_apply(Particles P, NbrList L, Ctl *ctl, ForceConsts fc) {
     grid_dep_wait();   // launched as a dependent (launch_k): the kernel before has completed
     grid_dep_release();
@@ -488,8 +492,11 @@ __global__ void __launch_bounds__(kApplyBlock) k_apply(Particles P, NbrList L, C
     __syncthreads();
     if (!s_go) return;
     const int nd = s_nd, cap = P.cap, vcur = ctl->vcur;
+    const bool one = nd <= kApplyOneBlock;   // the same in every block
+    if (one && blockIdx.x != 0) return;
     double *vc = P.vel[vcur], *wc = P.omg[vcur];
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nd; t += gridDim.x * blockDim.x) {
+    const int stride = one ? blockDim.x : gridDim.x * blockDim.x;
+    for (int t = (one ? 0 : blockIdx.x * blockDim.x) + threadIdx.x; t < nd; t += stride) {
         const int i = L.defer[t];
         for (int d = 0; d < 3; ++d) {
             vc[d * cap + i] = L.defer_v[d * cap + t];
@@ -498,8 +505,12 @@ __global__ void __launch_bounds__(kApplyBlock) k_apply(Particles P, NbrList L, C
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        const unsigned tk = take_ticket(&ctl->ticket);
-        s_last = (tk == gridDim.x - 1);
+        if (one) {
+            s_last = 1;
+        } else {
+            const unsigned tk = take_ticket(&ctl->ticket);
+            s_last = (tk == gridDim.x - 1);
+        }
     }
     __syncthreads();
     if (s_last && threadIdx.x < 32) {   // every block has taken its ticket: the slots are quiescent
@@ -847,6 +858,36 @@ static void launch_step_t(const Particles &P, const NbrList &L, Ctl *ctl, const 
     } else {
         k_force<MESH><<<nblocks(P.n), kBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls);
     }
+}
+
+// Cooperative launch of the step loop (dem_persist.cuh): a grid-stride grid of at most the
+// blocks the SMs hold at once.
+template <bool MIXED, bool MESH>
+static cudaError_t steps_coop_t(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc,
+                                const PairConst *pp, const PairConst *pw, const WallGeom *walls, int max_steps,
+                                cudaStream_t s) {
+    static thread_local int fit = 0;   // resident blocks of this instantiation, per host thread
+    if (!fit) {
+        int dev = 0, sms = 0, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_steps_coop<MIXED, MESH>, kBlock, 0);
+        fit = (sms > 0 ? sms : 148) * (per > 0 ? per : 1);
+    }
+    const int need = (P.n + kBlock - 1) / kBlock;
+    const int grid = need < fit ? (need > 0 ? need : 1) : fit;
+    Particles p = P;
+    NbrList l = L;
+    ForceConsts f = fc;
+    void *args[] = {&p, &l, &ctl, &f, (void *)&pp, (void *)&pw, (void *)&walls, &max_steps};
+    return cudaLaunchCooperativeKernel((const void *)k_steps_coop<MIXED, MESH>, dim3(grid), dim3(kBlock), args, 0, s);
+}
+
+cudaError_t launch_steps_coop(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
+                              const PairConst *pw, const WallGeom *walls, int max_steps, cudaStream_t s) {
+    if (fc.mixed) return launch_steps_coop_mixed(P, L, ctl, fc, pp, pw, walls, max_steps, s);
+    return fc.mesh.nt ? steps_coop_t<false, true>(P, L, ctl, fc, pp, pw, walls, max_steps, s)
+                      : steps_coop_t<false, false>(P, L, ctl, fc, pp, pw, walls, max_steps, s);
 }
 
 void launch_step(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,

@@ -143,6 +143,12 @@ typedef struct dem_solver_params {
                             * overlaps that kernel's tail (it waits for that kernel's completion
                             * before it touches any state); 2 off: plain stream order.  Same
                             * results.                                                         */
+    int cooperative_loop;  /* 0 = automatic (on), 1 on: while the step is one kernel over every
+                            * particle (at most 32,768 particles, Verlet-skin mode, the graph
+                            * while-loop, steps_per_launch 0), a run's steps between neighbour
+                            * builds are one cooperative launch with a grid barrier between
+                            * steps instead of a graph replay of per-step kernels; 2 off.  Same
+                            * results.                                                         */
 } dem_solver_params;
 
 typedef struct dem_run_stats {
@@ -157,6 +163,7 @@ typedef struct dem_run_stats {
                             * events around each replay; host gaps and rebuilds excluded)  */
     long graph_steps;      /* fused steps those replays advanced                          */
     int launch_overlap;    /* 1: the step kernels are launched as programmatic dependents      */
+    int cooperative_loop;  /* 1: the last run's steps ran in cooperative launches             */
 } dem_run_stats;
 
 /* ---- context ------------------------------------------------------------------- */

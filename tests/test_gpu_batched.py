@@ -102,14 +102,14 @@ def test_size_buckets_with_their_own_settings_equal_one_batch():
 @pytest.mark.parametrize("precision", [DEM_FP64, DEM_MIXED], ids=["fp64", "mixed"])
 def test_small_scenes_in_one_persistent_launch(precision):
     """Scenes of at most 64 particles: a run is one launch, a block per scene with every step
-    inside it (scene_kernel 0).  The state equals that of the per-step kernels (scene_kernel 1)
-    bit for bit, over runs of odd and even length (the buffer parity of the launch), and in FP64
-    every scene equals the oracle run on that scene alone."""
+    inside it (scene_kernel 0).  The state equals that of the per-step kernels (scene_kernel 1,
+    cooperative_loop 2) bit for bit, over runs of odd and even length (the buffer parity of the
+    launch), and in FP64 every scene equals the oracle run on that scene alone."""
     nsteps = (101, 200)
     sc = S.batched_scenes(nscenes=48, nmax=64, seed=31, nsteps=sum(nsteps))
     a = api.from_scenario(S.batched_scenes(nscenes=48, nmax=64, seed=31, nsteps=sum(nsteps)), precision=precision)
     b = api.from_scenario(S.batched_scenes(nscenes=48, nmax=64, seed=31, nsteps=sum(nsteps)), precision=precision,
-                          scene_kernel=1)
+                          scene_kernel=1, cooperative_loop=2)
     for k in nsteps:
         a.run_steps(k)
         b.run_steps(k)

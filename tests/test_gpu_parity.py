@@ -470,3 +470,47 @@ def test_dependent_launches_equal_plain_stream_order(form):
         ref, _ = _oracle(sc, 600)
         _assert_bitwise(got, ref, where="overlap %s vs oracle" % form)
     assert a.stats()["launch_overlap"] == 1 and b.stats()["launch_overlap"] == 0
+
+
+@pytest.mark.parametrize("case", ["gas", "compressed", "piston", "mixed", "overflow"])
+def test_cooperative_step_loop_equals_graph_loop(case):
+    """The one-kernel step of a small system with a run's steps in one cooperative launch and a
+    grid barrier between steps (cooperative_loop 0, the default) against graph replays of the
+    per-step kernel (cooperative_loop 2): the same trajectory bit for bit through rebuilds,
+    runs split unevenly, a kinematic piston (each run's last step leaves the walls, the next
+    run's first drift moves them), mixed precision and contact-slot overflow (MaxCnts 2), and
+    the oracle's in FP64."""
+    from cabanadem_b200._lib import DEM_MIXED
+    if case == "piston":
+        sc = S.piston_box(n=4096, speed=5.0, nsteps=400)
+        c = sc.state.x.mean(axis=0)
+        sc.state.x[:] = c + (sc.state.x - c) * 0.8
+        sc.walls.x[1, 0] = float((sc.state.x[:, 0] + sc.state.rad).max())
+    else:
+        sc = S.random_box(n=4133, nsteps=400, **(dict(max_cnts=2) if case == "overflow" else {}))
+        c = sc.state.x.mean(axis=0)
+        sc.state.x[:] = c + (sc.state.x - c) * (1.0 if case == "gas" else 0.6)
+    kw = dict(precision=DEM_MIXED) if case == "mixed" else {}
+    a = api.from_scenario(sc, **kw)
+    b = api.from_scenario(sc, cooperative_loop=2, **kw)
+    for n in (150, 101, 149):
+        a.run_steps(n)
+        b.run_steps(n)
+    got = a.particles.download()
+    _assert_bitwise(got, b.particles.download(), where="coop %s" % case)
+    sa, sb = a.stats(), b.stats()
+    assert sa["cooperative_loop"] == 1 and sb["cooperative_loop"] == 0
+    assert sa["rebuilds"] == sb["rebuilds"] and sa["steps"] == sb["steps"] == 400
+    assert sa["launches"] < sb["launches"]
+    assert a.last_status == b.last_status
+    if case == "overflow":
+        assert a.last_status & 0x004
+    if case == "piston":
+        assert np.array_equal(a.wall_positions(), b.wall_positions())
+    if case != "mixed":
+        ref = sc.state.copy()
+        w = sc.walls.copy()
+        O.run(ref, w, sc.params, sc.dt, 400, skin=sc.skin, gravity=sc.gravity, pow_mode=O.POW_SQRT)
+        _assert_bitwise(got, ref, where="coop %s vs oracle" % case)
+        if case == "piston":
+            assert np.array_equal(a.wall_positions(), w.x)
