@@ -103,6 +103,7 @@ struct dem_solver {
     bool no_overlap = false;                    // a step graph with dependent launches failed to build
     bool coop_refused = false;                  // a cooperative launch of the step loop was refused
     bool coop_ran = false;                      // the last run's steps ran in cooperative launches
+    unsigned long long *d_coop = nullptr;       // kCoopScratch words: barrier counter and slots
 };
 
 struct dem_bonds {
@@ -1416,6 +1417,7 @@ extern "C" int dem_solver_destroy(dem_solver *s) {
     cudaFree(B.block_sums); cudaFree(B.bbox); cudaFree(B.src); cudaFree(B.dst);
     cudaFree(B.part_sums);
     cudaFree(s->d_epart); cudaFree(s->d_eout);
+    cudaFree(s->d_coop);
     free_mesh(s);
     delete s;
     return DEM_OK;
@@ -1657,9 +1659,10 @@ extern "C" int dem_solver_run(dem_solver *s, int nsteps) {
         s->coop_ran = false;
         for (int guard = 0;; ++guard) {
             if (coop_loop(s)) {   // every step until the target or a stale list in one launch
+                if (!s->d_coop) CK(dalloc(&s->d_coop, (size_t)kCoopScratch));
                 CK(cudaEventRecord(s->ev0, st));
                 const cudaError_t le = launch_steps_coop(s->p->P, s->L, s->p->ctl, s->fc, s->d_pp, s->d_pw, s->d_walls,
-                                                         nsteps, st);
+                                                         nsteps, s->d_coop, st);
                 if (le != cudaSuccess) {   // not resident at once (or refused): graph replays from here on
                     (void)cudaGetLastError();
                     s->coop_refused = true;

@@ -319,12 +319,16 @@ constexpr int kSceneMaxParticles = 64;   // largest scene of the persistent form
 // The one-kernel step's run in one cooperative launch (dem_persist.cuh): at most `max_steps`
 // steps, ending at the target, a stale list or a stop bit.  An error when the launch is refused
 // (e.g. the grid cannot be resident at once).
-constexpr int kCoopMaxN = 32768;   // largest system the cooperative step loop takes
+constexpr int kCoopMaxN = 65536;   // largest system the cooperative step loop takes
+// scratch: kCoopScratch words of device memory for the symmetric barrier (static walls, no
+// moving mesh).
+constexpr int kCoopScratch = 1 + 4 * (kCoopMaxN / 128);
 cudaError_t launch_steps_coop(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc, const PairConst *pp,
-                              const PairConst *pw, const WallGeom *walls, int max_steps, cudaStream_t s);
+                              const PairConst *pw, const WallGeom *walls, int max_steps, unsigned long long *scratch,
+                              cudaStream_t s);
 cudaError_t launch_steps_coop_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc,
                                     const PairConst *pp, const PairConst *pw, const WallGeom *walls, int max_steps,
-                                    cudaStream_t s);
+                                    unsigned long long *scratch, cudaStream_t s);
 
 // dense layers of the surrogate (dem_nn.cu)
 int nn_mlp_forward(const dem_nn_mlp &m, long rows, const dem_nn_rows *src, int nsrc, const void *resid, void *out,

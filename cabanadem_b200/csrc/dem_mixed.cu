@@ -180,32 +180,43 @@ const void *contact_mixed_kernel(int dense, int coop, bool mesh) {
 
 // Cooperative launch of the step loop (dem_persist.cuh): a grid-stride grid of at most the
 // blocks the SMs hold at once.
+// With static walls and no moving mesh the symmetric-barrier form (its arrival counter zeroed
+// first on the stream).
 template <bool MIXED, bool MESH>
 static cudaError_t steps_coop_t(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc,
                                 const PairConst *pp, const PairConst *pw, const WallGeom *walls, int max_steps,
-                                cudaStream_t s) {
-    static thread_local int fit = 0;   // resident blocks of this instantiation, per host thread
-    if (!fit) {
+                                unsigned long long *scratch, cudaStream_t s) {
+    const bool lean = !fc.mwalls && !fc.mesh_moving && scratch;
+    const void *kernel = lean ? (const void *)k_steps_coop_lean<MIXED, MESH> : (const void *)k_steps_coop<MIXED, MESH>;
+    static thread_local int fit[2] = {0, 0};   // resident blocks of each form, per host thread
+    if (!fit[lean]) {
         int dev = 0, sms = 0, per = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_steps_coop<MIXED, MESH>, kBlock, 0);
-        fit = (sms > 0 ? sms : 148) * (per > 0 ? per : 1);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kBlock, 0);
+        fit[lean] = (sms > 0 ? sms : 148) * (per > 0 ? per : 1);
     }
     const int need = (P.n + kBlock - 1) / kBlock;
-    const int grid = need < fit ? (need > 0 ? need : 1) : fit;
+    int grid = need < fit[lean] ? (need > 0 ? need : 1) : fit[lean];
+    if (lean && grid > kCoopMaxBlocks) grid = kCoopMaxBlocks;   // the scratch holds that many slots
     Particles p = P;
     NbrList l = L;
     ForceConsts f = fc;
-    void *args[] = {&p, &l, &ctl, &f, (void *)&pp, (void *)&pw, (void *)&walls, &max_steps};
-    return cudaLaunchCooperativeKernel((const void *)k_steps_coop<MIXED, MESH>, dim3(grid), dim3(kBlock), args, 0, s);
+    if (!lean) {
+        void *args[] = {&p, &l, &ctl, &f, (void *)&pp, (void *)&pw, (void *)&walls, &max_steps};
+        return cudaLaunchCooperativeKernel(kernel, dim3(grid), dim3(kBlock), args, 0, s);
+    }
+    const cudaError_t e = cudaMemsetAsync(scratch, 0, sizeof(unsigned long long), s);
+    if (e != cudaSuccess) return e;
+    void *args[] = {&p, &l, &ctl, &f, (void *)&pp, (void *)&pw, (void *)&walls, &max_steps, &scratch};
+    return cudaLaunchCooperativeKernel(kernel, dim3(grid), dim3(kBlock), args, 0, s);
 }
 
 cudaError_t launch_steps_coop_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc,
                                     const PairConst *pp, const PairConst *pw, const WallGeom *walls, int max_steps,
-                                    cudaStream_t s) {
-    return fc.mesh.nt ? steps_coop_t<true, true>(P, L, ctl, fc, pp, pw, walls, max_steps, s)
-                      : steps_coop_t<true, false>(P, L, ctl, fc, pp, pw, walls, max_steps, s);
+                                    unsigned long long *scratch, cudaStream_t s) {
+    return fc.mesh.nt ? steps_coop_t<true, true>(P, L, ctl, fc, pp, pw, walls, max_steps, scratch, s)
+                      : steps_coop_t<true, false>(P, L, ctl, fc, pp, pw, walls, max_steps, scratch, s);
 }
 
 void launch_scene_steps_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc,

@@ -123,5 +123,131 @@ __global__ void __launch_bounds__(kBlock) k_steps_coop(Particles P, NbrList L, C
     }
 }
 
+// The same loop with static walls and no moving mesh, where nothing but the particles changes
+// between steps: every block keeps the step counters, the buffer parity and the displacement
+// bound itself, and the barrier is symmetric.  Per step each block stores its largest |u|^2
+// and its in-contact count in its own slot (two sets of slots, by step parity), then arrives on
+// one counter with a release atomic and polls it with acquire loads until every block has
+// arrived (bounded); then one warp of each block reads the step's slots and every block computes
+// the same bound, disp + dt sqrt(max |u|^2) (1 + 1e-9), as the finaliser does.  Two dependent
+// round trips fewer per step than a ticket, a finaliser and its generation (the control word is
+// read once at the start and written once at the end, by block 0).  scratch: the arrival
+// counter (zeroed before the launch), then 2 x gridDim.x slots of |u|^2 bits and 2 x gridDim.x
+// counts.
+constexpr int kCoopMaxBlocks = kCoopMaxN / kBlock;
+
+template <bool MIXED, bool MESH>
+__global__ void __launch_bounds__(kBlock) k_steps_coop_lean(Particles P, NbrList L, Ctl *ctl, ForceConsts fc,
+                                                            const PairConst *__restrict__ pp,
+                                                            const PairConst *__restrict__ pw,
+                                                            const WallGeom *__restrict__ walls, int max_steps,
+                                                            unsigned long long *scratch) {
+    __shared__ int s_cur, s_vcur, s_done, s_target, s_stop, s_ok, s_cnt;
+    __shared__ double s_disp, s_half, s_v2;
+    __shared__ int cnt_s[32];
+    __shared__ double red[32];
+    if (threadIdx.x == 0) {
+        s_cur = ctl->cur;
+        s_vcur = ctl->vcur;
+        s_done = ctl->steps_done;
+        s_target = ctl->target;
+        s_stop = ctl->status & kStopBits;
+        s_disp = ctl->disp;
+        s_half = ctl->half_skin;
+        s_ok = 1;
+        s_cnt = 0;
+    }
+    __syncthreads();
+    unsigned *arrive = reinterpret_cast<unsigned *>(scratch);
+    unsigned long long *vslot = scratch + 1, *cslot = scratch + 1 + 2 * gridDim.x;
+    const int G = gridDim.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int cur = s_cur, vcur = s_vcur, done = s_done;
+    const int target = s_target;
+    double disp = s_disp;
+    const double half = s_half;
+    int steps = 0;
+    for (int k = 0; k < max_steps; ++k) {
+        if (!(done < target && !s_stop && disp < half && s_ok)) break;   // the same in every block
+        const int last = done + 1 >= target;
+        double vmax2 = 0.0;
+        int status = 0, active = 0;
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += gridDim.x * blockDim.x) {
+            double v2 = 0.0;
+            int a = 0;
+            particle_full<MODE_FUSED_DIRECT, MIXED, MESH>(P, L, fc, pp, pw, walls, cur, cur ^ 1, vcur, last, i, i, v2,
+                                                          status, &a);
+            vmax2 = fmax(vmax2, v2);
+            active += a;
+        }
+        int c = active;
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        for (int o = 16; o > 0; o >>= 1) vmax2 = fmax(vmax2, __shfl_xor_sync(0xffffffffu, vmax2, o));
+        if (status) atomicOr(&ctl->status, status);
+        if (lane == 0) {
+            cnt_s[warp] = c;
+            red[warp] = vmax2;
+        }
+        __syncthreads();
+        const int par = (k & 1) * G;
+        if (threadIdx.x == 0) {
+            int t = 0;
+            double m = red[0];
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+                t += cnt_s[w];
+                m = fmax(m, red[w]);
+            }
+            vslot[par + blockIdx.x] = (unsigned long long)__double_as_longlong(m);
+            cslot[par + blockIdx.x] = (unsigned long long)t;
+            unsigned old;   // the slots before the arrival
+            asm volatile("atom.release.gpu.global.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(arrive) : "memory");
+            const unsigned want = (unsigned)G * (unsigned)(k + 1);
+            int n = 0;
+            while (ld_acquire_u32(arrive) < want && n < kCoopWaitPolls) {
+                __nanosleep(32);
+                ++n;
+            }
+            if (n == kCoopWaitPolls) {
+                atomicOr(&ctl->status, DEM_ERR_TIMEOUT);
+                s_ok = 0;
+            }
+        }
+        __syncthreads();   // every block has arrived (or this one gave up): the slots are complete
+        if (!s_ok) break;
+        if (warp == 0) {   // every block's slots of this step, read by one warp after thread 0's acquire
+            unsigned long long v = 0ull, n = 0ull;
+            for (int b = lane; b < G; b += 32) {
+                const unsigned long long x = *reinterpret_cast<volatile unsigned long long *>(vslot + par + b);
+                v = x > v ? x : v;
+                n += *reinterpret_cast<volatile unsigned long long *>(cslot + par + b);
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+                v = w > v ? w : v;
+                n += __shfl_xor_sync(0xffffffffu, n, o);
+            }
+            if (lane == 0) {
+                s_v2 = __longlong_as_double((long long)v);
+                s_cnt = (int)n;
+            }
+        }
+        __syncthreads();
+        disp = disp + fc.dt * sqrt(s_v2) * (1.0 + 1e-9);
+        cur ^= 1;
+        vcur ^= 1;
+        done += 1;
+        steps += 1;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {   // the control word as the per-step finaliser leaves it
+        ctl->cur = cur;
+        ctl->vcur = vcur;
+        ctl->steps_done = done;
+        ctl->total_steps += steps;
+        ctl->disp = disp;
+        if (steps > 0) ctl->last_ndefer = s_cnt;
+        ctl->ndefer = 0;
+        ctl->npairs = 0;
+    }
+}
+
 }  // namespace
 }  // namespace b200dem

@@ -144,7 +144,7 @@ typedef struct dem_solver_params {
                             * before it touches any state); 2 off: plain stream order.  Same
                             * results.                                                         */
     int cooperative_loop;  /* 0 = automatic (on), 1 on: while the step is one kernel over every
-                            * particle (at most 32,768 particles, Verlet-skin mode, the graph
+                            * particle (at most 65,536 particles, Verlet-skin mode, the graph
                             * while-loop, steps_per_launch 0), a run's steps between neighbour
                             * builds are one cooperative launch with a grid barrier between
                             * steps instead of a graph replay of per-step kernels; 2 off.  Same
