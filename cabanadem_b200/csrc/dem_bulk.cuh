@@ -38,6 +38,25 @@ __device__ __forceinline__ void copy_g2s(void *dst, const void *src, uint32_t by
         : "memory");
 }
 
+// L2 cache policy for data that every step reads again (the particle masses, contact words and
+// neighbour lists between builds): its lines are evicted after the step's streaming data, so
+// that they stay in L2 from one step to the next instead of coming from HBM each time.
+__device__ __forceinline__ uint64_t policy_keep() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+// copy_g2s with an L2 cache policy for the source lines.
+__device__ __forceinline__ void copy_g2s_hint(void *dst, const void *src, uint32_t bytes, uint64_t *bar,
+                                              uint64_t policy) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::
+            "r"(saddr(dst)),
+        "l"(src), "r"(bytes), "r"(saddr(bar)), "l"(policy)
+        : "memory");
+}
+
 __device__ __forceinline__ bool bar_try_wait(uint64_t *bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(

@@ -357,11 +357,16 @@ __global__ void __launch_bounds__(T, STREAM_BULK_MINB) k_stream_bulk(Particles P
         if (fc.drop_copies) return;   // testing the bounded waits: nothing will arrive
         bulk::copy_g2s(sb + B::POS, pc + i0, 32u * m, bar);
         for (int d = 0; d < 3; ++d) bulk::copy_g2s(sb + B::VEL + 8 * T * d, vc + (long)d * cap + i0, 8u * m, bar);
-        bulk::copy_g2s(sb + B::MASS, P.mI + i0, 8u * m, bar);
-        bulk::copy_g2s(sb + B::CS, P.cstate + i0, 4u * m, bar);
-        if (lists) bulk::copy_g2s(sb + B::NN, L.nn + i0, 4u * m, bar);
-        for (int r = 0; r < rows; ++r) bulk::copy_g2s(sb + B::IDX + 4 * T * r, L.idx + (long)r * cap + i0, 4u * m, bar);
-        if (c.wfar) bulk::copy_g2s(sb + B::WFAR, L.wfar + i0, (uint32_t)m, bar);
+        // rows every step reads again and (between builds) hardly anything writes: kept in L2 across
+        // steps (at most 25 bytes per particle, 50 MB on the 2M lattice; the velocities kept as well
+        // measured slower)
+        const uint64_t keep = bulk::policy_keep();
+        bulk::copy_g2s_hint(sb + B::MASS, P.mI + i0, 8u * m, bar, keep);
+        bulk::copy_g2s_hint(sb + B::CS, P.cstate + i0, 4u * m, bar, keep);
+        if (lists) bulk::copy_g2s_hint(sb + B::NN, L.nn + i0, 4u * m, bar, keep);
+        for (int r = 0; r < rows; ++r)
+            bulk::copy_g2s_hint(sb + B::IDX + 4 * T * r, L.idx + (long)r * cap + i0, 4u * m, bar, keep);
+        if (c.wfar) bulk::copy_g2s_hint(sb + B::WFAR, L.wfar + i0, (uint32_t)m, bar, keep);
     };
     if (threadIdx.x == 0)
         for (int k = 0; k < S && k < mine; ++k) issue(k);
