@@ -50,6 +50,7 @@ __global__ void __launch_bounds__(kSceneBlock) k_scene_steps(Particles P, NbrLis
                                                              const WallGeom *__restrict__ walls, const int2 *table,
                                                              int nsteps, double delta, double skin) {
     __shared__ int order[kSceneBlock];
+    __shared__ D4 spos[kSceneBlock];   // the scene's positions of the step, for the list search
     const int2 sc = table[blockIdx.x];
     const int first = sc.x, count = sc.y, t = threadIdx.x, cap = P.cap;
     if (count <= 0) return;   // block-uniform
@@ -64,15 +65,16 @@ __global__ void __launch_bounds__(kSceneBlock) k_scene_steps(Particles P, NbrLis
     int status = 0;
     for (int k = 0; k < nsteps; ++k) {
         __syncthreads();   // the previous step's positions and velocities (and `order`) are complete
+        if (t < count) spos[t] = ld4(P.pos[cur], first + t);   // one load per particle, then shared
+        __syncthreads();
         if (t < count) {
             const int i = first + t;
-            const double4 *__restrict__ pc = P.pos[cur];
-            const D4 pi = ld4(pc, i);
+            const D4 pi = spos[t];
             int nn = 0;
             for (int r = 0; r < count; ++r) {
                 const int j = order[r];
                 if (j == i) continue;
-                const D4 pj = ld4(pc, j);
+                const D4 pj = spos[j - first];
                 const double px = pi.x - pj.x, py = pi.y - pj.y, pz = pi.z - pj.z;
                 const double r2 = px * px + py * py + pz * pz;
                 const double cut = delta > 0.0 ? delta : pi.w + pj.w + skin;
