@@ -222,7 +222,14 @@ cudaError_t launch_steps_coop_mixed(const Particles &P, const NbrList &L, Ctl *c
 void launch_scene_steps_mixed(const Particles &P, const NbrList &L, Ctl *ctl, const ForceConsts &fc,
                               const PairConst *pp, const PairConst *pw, const WallGeom *walls, const int2 *table,
                               int nscenes, int nsteps, double delta, double skin, cudaStream_t s) {
-    k_scene_steps<true><<<nscenes, kSceneBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls, table, nsteps, delta, skin);
+    const SceneSmem o = scene_smem(P.mc, P.mw, P.ext != nullptr, P.fix != nullptr, fc.nmat > 1);
+    if (o.bytes <= kSceneSmemMax &&
+        cudaFuncSetAttribute(k_scene_steps_smem<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, o.bytes) ==
+            cudaSuccess)
+        k_scene_steps_smem<true><<<nscenes, kSceneBlock, o.bytes, s>>>(P, L, ctl, fc, pp, pw, walls, table, nsteps,
+                                                                       delta, skin);
+    else
+        k_scene_steps<true><<<nscenes, kSceneBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls, table, nsteps, delta, skin);
     k_scene_run_end<<<1, 32, 0, s>>>(ctl, nsteps);
 }
 

@@ -822,7 +822,9 @@ __device__ __noinline__ int mesh_pass(const Particles &P, const ForceConsts &fc,
 // unfused reference-order path); MODE_FUSED integrates into the next buffer.
 // ---------------------------------------------------------------------------------------
 // MESH: the solver has a triangle mesh (a separate build, so that meshless steps carry no call).
-template <int MODE, bool MIXED, bool MESH = false>
+// GLOBAL: the particle arrays are in global memory (the early list and slot loads take the
+// read-only path); false when they are a scene's copy in shared memory (generic loads).
+template <int MODE, bool MIXED, bool MESH = false, bool GLOBAL = true>
 __device__ __forceinline__ void particle_full(const Particles &P, const NbrList &L, const ForceConsts &fc,
                                               const PairConst *__restrict__ pp, const PairConst *__restrict__ pw,
                                               const WallGeom *__restrict__ walls, const int cur, const int nxt,
@@ -846,8 +848,10 @@ __device__ __forceinline__ void particle_full(const Particles &P, const NbrList 
     // positions.  Slots past the list length or count hold stale values; an index outside
     // [0, n) falls back to i, and a prefetched position is used only while its slot still
     // holds the same partner, so the arithmetic is that of the plain loop.
-    int lpf0 = L.maxnb > 0 ? ld_early_i(L.idx + i) : i, lpf1 = L.maxnb > 1 ? ld_early_i(L.idx + cap + i) : i;
-    int tpf0 = P.mc > 0 ? ld_early_i(P.tidx + i) : i, tpf1 = P.mc > 1 ? ld_early_i(P.tidx + cap + i) : i;
+    int lpf0 = L.maxnb > 0 ? (GLOBAL ? ld_early_i(L.idx + i) : L.idx[i]) : i;
+    int lpf1 = L.maxnb > 1 ? (GLOBAL ? ld_early_i(L.idx + cap + i) : L.idx[cap + i]) : i;
+    int tpf0 = P.mc > 0 ? (GLOBAL ? ld_early_i(P.tidx + i) : P.tidx[i]) : i;
+    int tpf1 = P.mc > 1 ? (GLOBAL ? ld_early_i(P.tidx + cap + i) : P.tidx[cap + i]) : i;
     lpf0 = (unsigned)lpf0 < (unsigned)P.n ? lpf0 : i;
     lpf1 = (unsigned)lpf1 < (unsigned)P.n ? lpf1 : i;
     tpf0 = (unsigned)tpf0 < (unsigned)P.n ? tpf0 : i;

@@ -947,7 +947,14 @@ void launch_scene_steps(const Particles &P, const NbrList &L, Ctl *ctl, const Fo
         launch_scene_steps_mixed(P, L, ctl, fc, pp, pw, walls, table, nscenes, nsteps, delta, skin, s);
         return;
     }
-    k_scene_steps<false><<<nscenes, kSceneBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls, table, nsteps, delta, skin);
+    const SceneSmem o = scene_smem(P.mc, P.mw, P.ext != nullptr, P.fix != nullptr, fc.nmat > 1);
+    if (o.bytes <= kSceneSmemMax &&
+        cudaFuncSetAttribute(k_scene_steps_smem<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, o.bytes) ==
+            cudaSuccess)
+        k_scene_steps_smem<false><<<nscenes, kSceneBlock, o.bytes, s>>>(P, L, ctl, fc, pp, pw, walls, table, nsteps,
+                                                                        delta, skin);
+    else
+        k_scene_steps<false><<<nscenes, kSceneBlock, 0, s>>>(P, L, ctl, fc, pp, pw, walls, table, nsteps, delta, skin);
     k_scene_run_end<<<1, 32, 0, s>>>(ctl, nsteps);
 }
 
