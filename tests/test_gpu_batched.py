@@ -128,3 +128,35 @@ def test_small_scenes_in_one_persistent_launch(precision):
             mine = _scene_slice(ga, starts[k], counts[k])
             for f in STATE:
                 assert np.array_equal(mine[f], getattr(ref, f)), (k, f)
+
+
+def test_small_scenes_in_shared_memory_with_hooks_and_force_readback():
+    """The scenes kept in shared memory for a run carry every per-particle field the step uses:
+    an external force on every particle and fix flags on some (force, torque or both zeroed
+    after the pair forces) give the same bits as the per-step kernels, and so do the force and
+    torque the run's last step leaves, the tracked slots' partners (renamed back to storage
+    indices) and the wall history, over runs that cross the scenes' own list rebuilds."""
+    nsteps = (150, 151)
+    mk = lambda: S.batched_scenes(nscenes=48, nmax=64, seed=31, nsteps=sum(nsteps))
+    n = mk().state.n
+    rng = np.random.default_rng(5)
+    ext = rng.normal(0.0, 1e-6, (n, 3))
+    fix = (rng.random(n) < 0.1).astype(np.uint8) * rng.integers(1, 4, n).astype(np.uint8)
+    solvers = []
+    for kw in ({}, dict(scene_kernel=1, cooperative_loop=2)):
+        s = api.from_scenario(mk(), **kw)
+        s.particles.set("ext_force", ext)
+        s.particles.set("fix", fix)
+        solvers.append(s)
+    for k in nsteps:
+        for s in solvers:
+            s.run_steps(k)
+    ga, gb = (s.particles.download() for s in solvers)
+    for f in STATE + ("tng_idx", "tng_ss_x", "tng_sw_x", "tng_sw_y"):
+        a, b = getattr(ga, f), getattr(gb, f)
+        if f in ("tng_idx", "tng_ss_x"):   # slots beyond the count are not part of the state
+            live = np.arange(a.shape[1])[None, :] < gb.tng_count[:, None]
+            a, b = np.where(live, a, 0), np.where(live, b, 0)
+        assert np.array_equal(a, b), f
+    assert ga.tng_count.sum() > 0
+    assert solvers[0].stats()["launches"] * 10 < solvers[1].stats()["launches"]
