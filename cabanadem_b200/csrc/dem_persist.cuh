@@ -166,7 +166,10 @@ __global__ void __launch_bounds__(kBlock) k_steps_coop_lean(Particles P, NbrList
     double disp = s_disp;
     const double half = s_half;
     int steps = 0;
-    for (int k = 0; k < max_steps; ++k) {
+    // the arrival count of step k is G (k + 1): at most 2^31 - 1 in one launch (the host
+    // launches again for the steps left)
+    const int kmax = max_steps < (int)(0x7FFFFFFFu / (unsigned)G) ? max_steps : (int)(0x7FFFFFFFu / (unsigned)G);
+    for (int k = 0; k < kmax; ++k) {
         if (!(done < target && !s_stop && disp < half && s_ok)) break;   // the same in every block
         const int last = done + 1 >= target;
         double vmax2 = 0.0;
